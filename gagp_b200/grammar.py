@@ -1,0 +1,426 @@
+"""Grammar admission: ``grammar-definition-v2`` -> resident phase tables.
+
+This is the cold host-side step that turns a user grammar into the flat tables
+the device engine searches with.  It restates, for the scalar-expression
+subset of the grammar language, three reference steps:
+
+* ``compile_grammar`` (``cpp/src/evolution/grammar/compiled.cpp:150-215``):
+  nonterminals and their alternatives are taken in sorted stable-id order
+  (``cpp/src/evolution/grammar/definition.cpp:104-110,434-464``) and every
+  expression is numbered in post order (``compiled.cpp:391-395``), so the ids
+  below equal the reference's expression ids;
+* ``compile_phase_grammar`` (``cpp/src/evolution/repro/gpu/phase_grammar.hpp:102-532``):
+  the per-expression generation records, the production ranges in visit order,
+  constant domains and the entry expression appended last;
+* the site-depth cost table (``phase_grammar.hpp:496-530``) and the static
+  weight normalisation (``phase_grammar.hpp:48-67``).
+
+A construct outside the subset raises :class:`Declined`, which is the
+reference's resident-admission decline (``std::invalid_argument`` at
+admission, ``cpp/src/evolution/evolve.cpp:45-49``).
+"""
+from __future__ import annotations
+
+import json
+import os
+import struct
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+NO_ID = 0xFFFFFFFF
+
+# ValueTag (cpp/include/gagp/core/value.hpp:16-27)
+TAG_INT, TAG_FLOAT, TAG_BOOL, TAG_INVALID = 0, 1, 2, 9
+TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL}
+
+# PhaseExpressionKind (device/phase_generate.cuh:25)
+EK_OPERATION, EK_CONSTANT, EK_BOUND, EK_REFERENCE, EK_INPUT, EK_ALIAS = range(6)
+# PhaseTreeKind (device/phase_compile.cuh:21)
+TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR = range(6)
+# Opcode (cpp/include/gagp/core/opcode.hpp:8-37)
+OP = {"push_const": 0, "load": 1, "store": 2, "neg": 3, "not": 4, "add": 5, "sub": 6, "mul": 7,
+      "div": 8, "mod": 9, "lt": 10, "le": 11, "gt": 12, "ge": 13, "eq": 14, "ne": 15, "jmp": 16,
+      "jmp_if_false": 17, "jmp_if_true": 18, "call_builtin": 19, "return": 20}
+# BuiltinId (cpp/include/gagp/core/builtin.hpp:13-45)
+BUILTIN = {"abs": 0, "min": 1, "max": 2, "clip": 3, "idiv0": 13, "imod0": 14,
+           "trunc_div0": 28, "trunc_mod0": 29}
+
+# Scalar primitives of the catalog (cpp/src/evolution/grammar/catalog.cpp:83-116):
+# name -> (argument types, result type, tree kind, opcode, builtin operand, printed name).
+def _scalar_catalog() -> Dict[str, tuple]:
+    cat = {}
+    for t in ("Int", "Bool"):
+        cat[f"if(Bool,{t},{t})->{t}"] = (("Bool", t, t), t, TK_IF, 0, 0, "if_expr")
+        cat[f"eq({t},{t})->Bool"] = ((t, t), "Bool", TK_OPERATION, OP["eq"], 0, "eq")
+        cat[f"ne({t},{t})->Bool"] = ((t, t), "Bool", TK_OPERATION, OP["ne"], 0, "ne")
+    for name in ("add", "sub", "mul", "mod"):
+        cat[f"{name}(Int,Int)->Int"] = (("Int", "Int"), "Int", TK_OPERATION, OP[name], 0, name)
+    cat["neg(Int)->Int"] = (("Int",), "Int", TK_OPERATION, OP["neg"], 0, "neg")
+    for name in ("lt", "le", "gt", "ge"):
+        cat[f"{name}(Int,Int)->Bool"] = (("Int", "Int"), "Bool", TK_OPERATION, OP[name], 0, name)
+    cat["not(Bool)->Bool"] = (("Bool",), "Bool", TK_OPERATION, OP["not"], 0, "not")
+    cat["and(Bool,Bool)->Bool"] = (("Bool", "Bool"), "Bool", TK_AND, 0, 0, "and")
+    cat["or(Bool,Bool)->Bool"] = (("Bool", "Bool"), "Bool", TK_OR, 0, 0, "or")
+    for name in ("min", "max"):
+        cat[f"{name}(Int,Int)->Int"] = (("Int", "Int"), "Int", TK_OPERATION, OP["call_builtin"], BUILTIN[name], name)
+    cat["abs(Int)->Int"] = (("Int",), "Int", TK_OPERATION, OP["call_builtin"], BUILTIN["abs"], "abs")
+    for name in ("idiv0", "imod0", "trunc_div0", "trunc_mod0"):
+        cat[f"{name}(Int,Int)->Int"] = (("Int", "Int"), "Int", TK_OPERATION, OP["call_builtin"], BUILTIN[name], name)
+    return cat
+
+
+CATALOG = _scalar_catalog()
+
+
+class Declined(ValueError):
+    """The resident engine cannot hold this grammar (an admission decline)."""
+
+
+@dataclass
+class Expression:
+    """One phase-grammar expression (``PhaseExpression``, phase_generate.cuh:79-92)."""
+
+    kind: int = EK_OPERATION
+    node_kind: int = TK_CONSTANT
+    opcode: int = 0
+    operand: int = 0
+    arity: int = 0
+    fuel: int = 1
+    merge_fuel: int = 1
+    type: int = TAG_INVALID
+    target: int = -1
+    children: List[int] = field(default_factory=lambda: [-1] * 8)
+    scope_count: int = 0
+    child_scope: List[int] = field(default_factory=lambda: [-1] * 8)
+    name: str = ""
+    result: str = ""          # grammar result type name
+
+
+@dataclass
+class Domain:
+    value_offset: int = 0
+    value_count: int = 0
+    integer_range: bool = False
+    minimum: int = 0
+    maximum: int = 0
+
+
+@dataclass
+class PhaseTables:
+    """Flat resident tables of one admitted search (one whole-program phase)."""
+
+    expressions: List[Expression]
+    productions: List[Tuple[int, float]]          # (expression, weight)
+    nonterminals: List[Tuple[int, int, int, bool, bool]]  # offset, count, scope, normalized, fixed
+    domains: List[Domain]
+    values: List[Tuple[int, int]]                 # (tag, payload)
+    minimum: List[int]
+    root_expression: int
+    depth_count: int
+    logical_depth_count: int
+    site_depth: int
+    # slot / layout
+    slot_max_depth: int
+    slot_type: int
+    local_types: List[int]
+    input_names: List[str]
+    max_nodes: int
+    fixed_nodes: int
+    fuel: int
+    names: List[str] = field(default_factory=list)  # printed name per expression
+
+
+def _parse_int(text) -> int:
+    if not isinstance(text, str):
+        raise Declined("Int constant must be a decimal string")
+    v = int(text, 10)
+    if v < -(1 << 63) or v >= (1 << 63):
+        raise Declined("Int constant out of range")
+    return v
+
+
+def load_definition(path: str) -> dict:
+    with open(path) as f:
+        return json.load(f)
+
+
+class _Compiler:
+    def __init__(self, doc: dict):
+        if doc.get("format_version") != "grammar-definition-v2":
+            raise Declined("grammar-definition-v2 required")
+        for key in ("imports", "templates", "locals"):
+            if doc.get(key):
+                raise Declined(f"grammar {key} are outside the resident scalar subset")
+        self.doc = doc
+        self.inputs = [(b["name"], b["type"]) for b in doc.get("inputs", [])]
+        rules = sorted(doc["nonterminals"], key=lambda r: r["id"])
+        self.rules = rules
+        self.nt_ids = {r["id"]: i for i, r in enumerate(rules)}
+        self.exprs: List[Expression] = []
+        self.domains: List[dict] = []
+        self.productions: List[Tuple[int, int, float]] = []  # (nonterminal, expression, weight)
+        self.nt_productions: List[List[int]] = [[] for _ in rules]
+
+    def expression(self, value: dict, nt_scope: int) -> int:
+        e = Expression()
+        if "constant" in value:
+            d = value["constant"]
+            if d.get("type") != "Int":
+                raise Declined("only Int constant domains are resident")
+            if "range" in d:
+                lo, hi = (_parse_int(x) for x in d["range"])
+                dom = {"integer_range": True, "minimum": lo, "maximum": hi}
+            elif "values" in d:
+                dom = {"integer_range": False, "values": [_parse_int(x) for x in d["values"]]}
+                if not dom["values"]:
+                    raise Declined("empty constant domain")
+            else:
+                raise Declined("constant sequence domains are not resident")
+            e.kind, e.node_kind, e.target = EK_CONSTANT, TK_CONSTANT, len(self.domains)
+            e.type, e.result, e.name = TAG_INT, "Int", "const"
+            self.domains.append(dom)
+        elif "input" in value:
+            names = [n for n, _ in self.inputs]
+            if value["input"] not in names:
+                raise Declined("unknown input")
+            idx = names.index(value["input"])
+            t = self.inputs[idx][1]
+            if t not in TYPE_TAGS:
+                raise Declined("only Int/Bool inputs are resident")
+            e.kind, e.node_kind, e.target = EK_INPUT, TK_LOCAL, idx
+            e.type, e.result, e.name = TYPE_TAGS[t], t, value["input"]
+        elif "ref" in value:
+            if value["ref"] not in self.nt_ids:
+                raise Declined("unknown nonterminal")
+            target = self.nt_ids[value["ref"]]
+            rule = self.rules[target]
+            if rule.get("scope"):
+                raise Declined("scoped nonterminals are outside the scalar subset")
+            e.kind, e.target, e.result = EK_REFERENCE, target, rule["type"]
+            e.type = TYPE_TAGS.get(rule["type"], TAG_INVALID)
+        elif "signature" in value:
+            sig = value["signature"]
+            if sig not in CATALOG:
+                raise Declined(f"primitive {sig} is outside the resident scalar subset")
+            arg_types, result, tree_kind, opcode, operand, name = CATALOG[sig]
+            args = value.get("args", [])
+            if len(args) != len(arg_types):
+                raise Declined("argument count mismatch")
+            children = [self.expression(a, nt_scope) for a in args]
+            for c, t in zip(children, arg_types):
+                if self.exprs[c].result != t:
+                    raise Declined("argument type mismatch")
+            e.kind, e.node_kind, e.opcode, e.operand = EK_OPERATION, tree_kind, opcode, operand
+            e.arity, e.type, e.result, e.name = len(children), TYPE_TAGS[result], result, name
+            for i, c in enumerate(children):
+                e.children[i] = c
+                e.child_scope[i] = nt_scope
+        else:
+            raise Declined("expression form outside the resident scalar subset")
+        if "fuel_events" in value:
+            raise Declined("fuel profiles are outside the resident scalar subset")
+        self.exprs.append(e)
+        return len(self.exprs) - 1
+
+    def compile(self):
+        for i, rule in enumerate(self.rules):
+            if rule.get("category", "Expression") != "Expression":
+                raise Declined("statement grammars are outside the scalar subset")
+            if rule["type"] not in TYPE_TAGS:
+                raise Declined("only Int/Bool nonterminals are resident")
+            for alt in sorted(rule["alternatives"], key=lambda a: a["id"]):
+                w = float(alt["weight"])
+                if not (w > 0) or w == float("inf"):
+                    raise Declined("production weight")
+                x = self.expression(alt["expression"], 0)
+                if self.exprs[x].result != rule["type"]:
+                    raise Declined("production result type mismatch")
+                self.nt_productions[i].append(len(self.productions))
+                self.productions.append((i, x, w))
+
+
+def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_depth: int = 7) -> PhaseTables:
+    """Admit ``doc`` and build the resident tables (one whole-program slot)."""
+    c = _Compiler(doc)
+    c.compile()
+    entry = doc["entry"]
+    if entry.get("category", "Expression") != "Expression":
+        raise Declined("Program-entry grammars are outside the scalar subset")
+    root_nt = c.nt_ids[entry["nonterminal"]]
+    limits = doc["search_limits"]
+    max_depth, max_nodes = int(limits["max_depth"]), int(limits["max_nodes"])
+    fuel = int(doc["execution_limits"]["fuel"])
+    if not (1 <= max_depth <= 64) or max_nodes > 2048 or not (0 <= site_depth <= 15):
+        raise Declined("depth/node capacity")
+    grammar_inputs = [n for n, _ in c.inputs]
+    names = sorted(grammar_inputs) if input_names is None else list(input_names)
+    if sorted(names) != sorted(grammar_inputs) or len(names) > 64:
+        raise Declined("input names must exactly cover grammar inputs")
+
+    # compile_phase_grammar: visit from the entry nonterminal.
+    n_expr = len(c.exprs)
+    out_expr = [Expression() for _ in range(n_expr)]
+    out_nts = [[0, 0, 0, False, False] for _ in c.rules]
+    out_prods: List[Tuple[int, float]] = []
+    out_domains = [Domain() for _ in c.domains]
+    out_values: List[Tuple[int, int]] = []
+    seen_nt, seen_expr, seen_dom = set(), set(), set()
+
+    def visit_nt(i: int):
+        if i in seen_nt:
+            return
+        seen_nt.add(i)
+        out_nts[i][0] = len(out_prods)
+        for p in c.nt_productions[i]:
+            _, x, w = c.productions[p]
+            out_prods.append((x, w))
+            out_nts[i][1] += 1
+        for p in c.nt_productions[i]:
+            visit_expr(c.productions[p][1])
+
+    def visit_expr(i: int):
+        if i in seen_expr:
+            return
+        seen_expr.add(i)
+        e = c.exprs[i]
+        x = out_expr[i]
+        x.kind, x.type, x.target, x.name, x.result = e.kind, e.type, e.target, e.name, e.result
+        if e.kind == EK_REFERENCE:
+            x.scope_count = 0
+            visit_nt(e.target)
+            return
+        x.node_kind, x.opcode, x.operand, x.arity = e.node_kind, e.opcode, e.operand, e.arity
+        x.children, x.child_scope = list(e.children), list(e.child_scope)
+        if e.kind == EK_CONSTANT and e.target not in seen_dom:
+            seen_dom.add(e.target)
+            d = c.domains[e.target]
+            dom = out_domains[e.target]
+            dom.integer_range = d["integer_range"]
+            if d["integer_range"]:
+                dom.minimum, dom.maximum = d["minimum"], d["maximum"]
+            else:
+                dom.value_offset, dom.value_count = len(out_values), len(d["values"])
+                out_values.extend((TAG_INT, v) for v in d["values"])
+        if e.kind == EK_INPUT:
+            position = names.index(grammar_inputs[e.target])
+            x.target = position
+            x.operand = position
+        for ch in e.children[: e.arity]:
+            visit_expr(ch)
+
+    visit_nt(root_nt)
+    # Productions may not share a root node and must resolve to a node.
+    resolved = set()
+    for x, _ in out_prods:
+        if out_expr[x].kind == EK_REFERENCE:
+            raise Declined("root aliases require native fallback")
+        if x in resolved:
+            raise Declined("productions sharing a root node require native fallback")
+        resolved.add(x)
+
+    depth_count = max_depth + 1
+    # An expression entry runs as program(block(return e)): the phase starts at
+    # AST depth 4 and keeps max_depth - 3 levels (phase_layout.hpp:131-134),
+    # and the four wrapper nodes are the layout's fixed nodes.
+    slot_max_depth = max_depth - 3
+    if slot_max_depth < 1:
+        raise Declined("max_depth leaves no room for the entry phase")
+    entry_expr = Expression(kind=EK_REFERENCE, target=root_nt, name="", result=c.rules[root_nt]["type"])
+    root_expression = n_expr
+    out_expr.append(entry_expr)
+    logical_count = site_depth + 1 if site_depth else 1
+    minimum = _minimum_table(out_expr, out_nts, out_prods, seen_expr | {root_expression}, depth_count,
+                             logical_count, site_depth > 0)
+    tables = PhaseTables(
+        expressions=out_expr, productions=out_prods,
+        nonterminals=[tuple(n) for n in out_nts], domains=out_domains, values=out_values,
+        minimum=minimum, root_expression=root_expression, depth_count=depth_count,
+        logical_depth_count=logical_count, site_depth=site_depth,
+        slot_max_depth=slot_max_depth, slot_type=TYPE_TAGS[c.rules[root_nt]["type"]],
+        local_types=[TYPE_TAGS[dict(c.inputs)[n]] for n in names], input_names=names,
+        max_nodes=max_nodes, fixed_nodes=4, fuel=fuel,
+        names=[e.name for e in out_expr])
+    _normalize_static_weights(tables)
+    return tables
+
+
+def _minimum_table(exprs, nts, prods, reachable, depth_count, logical_count, site_depth):
+    """Minimum nodes of each (expression, depth, site budget) (phase_grammar.hpp:496-530).
+
+    Without a site-depth limit the logical dimension has one entry and a
+    reference does not consume it.
+    """
+    size = len(exprs) * depth_count * logical_count
+    table = [NO_ID] * size
+    done = [False] * size
+
+    def cost(i: int, d: int, l: int) -> int:
+        key = (i * depth_count + d) * logical_count + l
+        if done[key]:
+            return table[key]
+        done[key] = True
+        e = exprs[i]
+        result = NO_ID
+        if e.kind == EK_REFERENCE:
+            if site_depth and not l:
+                return NO_ID
+            off, count = nts[e.target][0], nts[e.target][1]
+            nl = l - 1 if site_depth else l
+            for p in range(off, off + count):
+                result = min(result, cost(prods[p][0], d, nl))
+        elif d > 0:
+            total = 1
+            for k in range(e.arity):
+                total += cost(e.children[k], d - 1, l)
+            result = NO_ID if total >= NO_ID else total
+        table[key] = result
+        return result
+
+    import sys
+    old = sys.getrecursionlimit()
+    sys.setrecursionlimit(max(old, 100000))
+    try:
+        for i in sorted(reachable):
+            for d in range(depth_count):
+                for l in range(logical_count):
+                    cost(i, d, l)
+    finally:
+        sys.setrecursionlimit(old)
+    return table
+
+
+def _normalize_static_weights(t: PhaseTables) -> None:
+    """Divide weights by the maximum when a maximum-weight alternative is always
+    among the cheapest (phase_grammar.hpp:48-67)."""
+    per = t.depth_count * t.logical_depth_count
+    nts = [list(n) for n in t.nonterminals]
+    prods = list(t.productions)
+    for nt in nts:
+        off, count = nt[0], nt[1]
+        if not count:
+            continue
+        maximum = max(prods[off + i][1] for i in range(count))
+        proven = maximum > 0
+        for depth in range(per):
+            if not proven:
+                break
+            cheapest = max_weight_cheapest = NO_ID
+            for i in range(count):
+                x, w = prods[off + i]
+                cost = t.minimum[x * per + depth]
+                cheapest = min(cheapest, cost)
+                if w == maximum:
+                    max_weight_cheapest = min(max_weight_cheapest, cost)
+            proven = cheapest == max_weight_cheapest
+        if not proven:
+            continue
+        for i in range(count):
+            x, w = prods[off + i]
+            prods[off + i] = (x, w / maximum)
+        nt[3] = True
+    t.nonterminals = [tuple(n) for n in nts]
+    t.productions = prods
+
+
+def compile_file(path: str, input_names: Optional[List[str]] = None, site_depth: int = 7) -> PhaseTables:
+    return compile_tables(load_definition(path), input_names, site_depth)

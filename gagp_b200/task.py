@@ -1,0 +1,179 @@
+"""``gagp-task-v1`` / ``gagp-search-config-v1`` loading.
+
+Mirrors what ``gagp run`` assembles before a search
+(``cpp/src/cli/run.cpp:275-300``): the built-in default search
+(``run.cpp:36-49``, ``configs/search/default.json``) overlaid with the search
+file, penalty = the task's ``case_cap``, fuel = the grammar's execution fuel
+(a search file may only lower it), reduction lanes = 512 (``run.cpp:63``).
+Inputs are ordered by name, as ``prepare_case_set`` orders them
+(``cpp/src/evolution/case_set.cpp:48-55``).
+"""
+from __future__ import annotations
+
+import json
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import grammar as G
+from .abi import CasesBlob, SearchSettings
+
+DEFAULT_SEARCH = {
+    "format": "gagp-search-config-v1", "representation": "resident", "population_size": 1024,
+    "generations": 64, "selection": {"method": "tournament", "size": 2}, "elitism": 1,
+    "crossover": {"probability": 0.7, "attempts": 8}, "mutation": {"probability": 0.3},
+    "sites": {"scope": "uniform_phase", "draw": "counted"}, "limits": {"site_depth": 7},
+    "ranking": {"tie_break": "ast_nodes"}, "schedule": {"mode": "steady_state", "replacement_size": 2},
+}
+
+_TYPE_TAGS = {"int": G.TAG_INT, "bool": G.TAG_BOOL}
+
+
+@dataclass
+class LoadedTask:
+    name: str
+    tables: G.PhaseTables
+    cases: CasesBlob
+    settings: SearchSettings
+    test_cases: Optional[CasesBlob] = None
+
+
+def _case_values(doc: dict, names):
+    rows, expected, tags, etag = [], [], None, None
+    for case in doc["cases"]:
+        row, row_tags = [], []
+        for n in names:
+            v = case["inputs"][n]
+            if v["type"] not in _TYPE_TAGS:
+                raise G.Declined(f"input type {v['type']} is outside the resident scalar subset")
+            row_tags.append(_TYPE_TAGS[v["type"]])
+            row.append(int(v["value"]))
+        if tags is None:
+            tags = row_tags
+        elif tags != row_tags:
+            raise G.Declined("mixed input types")
+        e = case["expected"]
+        if e["type"] not in _TYPE_TAGS:
+            raise G.Declined(f"expected type {e['type']} is outside the resident scalar subset")
+        if etag is None:
+            etag = _TYPE_TAGS[e["type"]]
+        rows.append(row)
+        expected.append(int(e["value"]))
+    return np.array(rows, dtype=np.int64).reshape(len(expected), len(names)), tags or [], \
+        np.array(expected, dtype=np.int64), etag or 0
+
+
+def apply_search(settings: SearchSettings, doc: dict) -> None:
+    """Overlay a ``gagp-search-config-v1`` document (spec/search_config.md)."""
+    if doc.get("format") != "gagp-search-config-v1":
+        raise ValueError("gagp-search-config-v1 required")
+    if doc.get("representation", "resident") != "resident":
+        raise G.Declined("native_ast representation is not the resident engine")
+    s = settings
+    if "population_size" in doc:
+        s.population = int(doc["population_size"])
+    if "generations" in doc:
+        s.generations = int(doc["generations"])
+    if "seed" in doc:
+        s.seed = int(doc["seed"])
+    if "selection" in doc:
+        s.tournament_size = int(doc["selection"].get("size", s.tournament_size))
+    if "elitism" in doc:
+        s.elite_count = int(doc["elitism"])
+    explicit = any(k in doc for k in ("crossover", "sites")) or "max_subtree_nodes" in doc.get("mutation", {})
+    if explicit:
+        s.crossover_probability, s.crossover_attempts, s.mutation_max_nodes = 1.0, 8, 0
+        s.uniform_phase, s.counted_sites = False, False
+    if "crossover" in doc:
+        s.crossover_probability = float(doc["crossover"].get("probability", s.crossover_probability))
+        s.crossover_attempts = int(doc["crossover"].get("attempts", s.crossover_attempts))
+    if "mutation" in doc:
+        s.mutation_probability = float(doc["mutation"].get("probability", s.mutation_probability))
+        s.mutation_max_nodes = int(doc["mutation"].get("max_subtree_nodes", s.mutation_max_nodes))
+    if "sites" in doc:
+        s.uniform_phase = doc["sites"].get("scope", "genome") == "uniform_phase"
+        s.counted_sites = doc["sites"].get("draw", "reservoir") == "counted"
+    if "limits" in doc:
+        s.site_depth = int(doc["limits"].get("site_depth", s.site_depth))
+    if "ranking" in doc:
+        s.grammar_site_ranking = doc["ranking"].get("tie_break", "ast_nodes") == "grammar_sites"
+    if "fitness" in doc and "penalty" in doc["fitness"]:
+        s.penalty = float(doc["fitness"]["penalty"])
+    if "execution" in doc and "fuel" in doc["execution"]:
+        s.fuel = min(s.fuel, int(doc["execution"]["fuel"]))
+    if "schedule" in doc:
+        sc = doc["schedule"]
+        s.steady_state = sc.get("mode", "generational") == "steady_state"
+        s.batch = int(sc.get("batch", 0))
+        s.replacement_size = int(sc.get("replacement_size", 2))
+
+
+def load(task_path: str, search_path: Optional[str] = None, population: Optional[int] = None,
+         generations: Optional[int] = None, seed: Optional[int] = None) -> LoadedTask:
+    base = os.path.dirname(os.path.abspath(task_path))
+    with open(task_path) as f:
+        task = json.load(f)
+    if task.get("format") != "gagp-task-v1":
+        raise ValueError("gagp-task-v1 required")
+    grammar_doc = G.load_definition(os.path.join(base, task["grammar"]))
+    with open(os.path.join(base, task["train"])) as f:
+        train = json.load(f)
+    names = sorted({n for case in train["cases"] for n in case["inputs"]})
+    fitness = task["fitness"]
+    settings = SearchSettings()
+    settings.metric = fitness["metric"]
+    settings.penalty = float(fitness.get("case_cap", 1000))
+    settings.fuel = int(grammar_doc["execution_limits"]["fuel"])
+    apply_search(settings, DEFAULT_SEARCH)
+    if search_path:
+        with open(search_path) as f:
+            apply_search(settings, json.load(f))
+    if population:
+        settings.population = population
+    if generations:
+        settings.generations = generations
+    if seed is not None:
+        settings.seed = seed
+    if settings.metric not in ("absolute", "exact"):
+        raise G.Declined(f"metric {settings.metric} is outside the resident scalar subset")
+    if settings.site_depth < 1:
+        raise G.Declined("the resident engine here generates its population under a site-depth limit")
+    tables = G.compile_tables(grammar_doc, names, settings.site_depth)
+    inputs, tags, expected, etag = _case_values(train, names)
+    test = None
+    if task.get("test"):
+        with open(os.path.join(base, task["test"])) as f:
+            tdoc = json.load(f)
+        ti, tt, te, tet = _case_values(tdoc, names)
+        test = CasesBlob(ti, tt, te, tet)
+    return LoadedTask(task.get("name", os.path.basename(base)), tables, CasesBlob(inputs, tags, expected, etag),
+                      settings, test)
+
+
+def program_text(tables: G.PhaseTables, origins, constants) -> str:
+    """Prefix program text of a phase row (``cli_detail::program_text``,
+    ``cpp/src/cli/program_json.cpp:876-946``)."""
+    out = []
+    pos = [0]
+    k = [0]
+
+    def node():
+        e = tables.expressions[origins[pos[0]]]
+        pos[0] += 1
+        if e.kind == G.EK_CONSTANT:
+            out.append(str(constants[k[0]]))
+            k[0] += 1
+            return
+        if e.kind == G.EK_INPUT:
+            out.append(e.name)
+            return
+        out.append("(" + e.name)
+        for _ in range(e.arity):
+            out.append(" ")
+            node()
+        out.append(")")
+
+    node()
+    return "".join(out)

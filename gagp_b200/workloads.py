@@ -1,0 +1,150 @@
+"""Deterministic synthetic GAGP tasks in the reference's file formats.
+
+Every task is written as the reference's ``gagp-task-v1`` file set
+(``spec/task.md``): a ``grammar-definition-v2`` grammar, ``fitness-cases``
+train/test files and an absolute-error fitness policy, plus a
+``gagp-search-config-v1`` search file.  The same files drive the reference CPU
+engine (``gagp run --engine cpu``) and this engine, so both search the same
+problem from the same seed.
+
+Workloads:
+
+* ``polynomial``  -- scalar integer regression of y = x^3 - 2x + 1; x = -10..10
+  train cases, 40 test cases x ~ U[-50, 50]; grammar x (w3), constants {0,1,2}
+  (w2), add/sub/mul (w1); max 31 nodes, depth 8, fuel 1000.
+* ``poly4``       -- random integer polynomial of degree <= 4, coefficients
+  U{-5..5} from the seed; train x ~ U{-100..100}; grammar x, constants
+  -2..3, add/sub/mul/idiv0/imod0 and if(lt(E,E),E,E); max 64 nodes, depth 16,
+  fuel 1000.
+
+Inputs are generated with ``random.Random(seed)``.
+"""
+from __future__ import annotations
+
+import json
+import os
+import random
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+
+def _int_case(x: int, y: int) -> dict:
+    return {"inputs": {"x": {"type": "int", "value": x}}, "expected": {"type": "int", "value": y}}
+
+
+def _binary(name: str) -> dict:
+    return {"signature": f"{name}(Int,Int)->Int", "args": [{"ref": "Expr"}, {"ref": "Expr"}]}
+
+
+@dataclass
+class TaskFiles:
+    """An in-memory task: grammar, cases and search documents."""
+
+    name: str
+    grammar: dict
+    train: List[dict]
+    test: List[dict] = field(default_factory=list)
+    fitness: dict = field(default_factory=lambda: {"metric": "absolute", "case_cap": 1000})
+    search: dict = field(default_factory=dict)
+
+    def write(self, directory: str) -> str:
+        """Write the task file set into ``directory``; return the task path."""
+        os.makedirs(directory, exist_ok=True)
+        with open(os.path.join(directory, "grammar.json"), "w") as f:
+            json.dump(self.grammar, f, indent=1)
+        with open(os.path.join(directory, "train.cases.json"), "w") as f:
+            json.dump({"format_version": "fitness-cases", "cases": self.train}, f)
+        task = {"format": "gagp-task-v1", "name": self.name, "grammar": "grammar.json",
+                "train": "train.cases.json", "fitness": self.fitness}
+        if self.test:
+            with open(os.path.join(directory, "test.cases.json"), "w") as f:
+                json.dump({"format_version": "fitness-cases", "cases": self.test}, f)
+            task["test"] = "test.cases.json"
+        with open(os.path.join(directory, "task.json"), "w") as f:
+            json.dump(task, f, indent=1)
+        if self.search:
+            with open(os.path.join(directory, "search.json"), "w") as f:
+                json.dump(self.search, f, indent=1)
+        return os.path.join(directory, "task.json")
+
+
+def search_config(population: int, generations: int, seed: int, **extra) -> dict:
+    """A ``gagp-search-config-v1`` document; absent members keep gagp's defaults."""
+    doc = {"format": "gagp-search-config-v1", "population_size": population,
+           "generations": generations, "seed": str(seed)}
+    doc.update(extra)
+    return doc
+
+
+def polynomial_grammar(constants=("0", "1", "2"), max_nodes: int = 31, max_depth: int = 8,
+                       fuel: int = 1000) -> dict:
+    return {
+        "format_version": "grammar-definition-v2",
+        "entry": {"nonterminal": "Expr", "type": "Int"},
+        "inputs": [{"name": "x", "type": "Int"}],
+        "search_limits": {"max_nodes": max_nodes, "max_depth": max_depth},
+        "execution_limits": {"fuel": fuel},
+        "nonterminals": [{"id": "Expr", "type": "Int", "scope": [], "alternatives": [
+            {"id": "x", "weight": 3, "expression": {"input": "x"}},
+            {"id": "small", "weight": 2,
+             "expression": {"constant": {"type": "Int", "values": list(constants)}}},
+            {"id": "add", "weight": 1, "expression": _binary("add")},
+            {"id": "sub", "weight": 1, "expression": _binary("sub")},
+            {"id": "mul", "weight": 1, "expression": _binary("mul")},
+        ]}],
+    }
+
+
+def polynomial(population: int = 1024, generations: int = 64, seed: int = 0) -> TaskFiles:
+    """Scalar regression of y = x^3 - 2x + 1 (21 train cases, 40 test cases)."""
+    f = lambda x: x ** 3 - 2 * x + 1
+    rng = random.Random(seed)
+    test_x = [rng.randint(-50, 50) for _ in range(40)]
+    return TaskFiles(
+        name="polynomial", grammar=polynomial_grammar(),
+        train=[_int_case(x, f(x)) for x in range(-10, 11)],
+        test=[_int_case(x, f(x)) for x in test_x],
+        search=search_config(population, generations, seed))
+
+
+def poly4_grammar(max_nodes: int = 64, max_depth: int = 16, fuel: int = 1000) -> dict:
+    ref = {"ref": "Expr"}
+    return {
+        "format_version": "grammar-definition-v2",
+        "entry": {"nonterminal": "Expr", "type": "Int"},
+        "inputs": [{"name": "x", "type": "Int"}],
+        "search_limits": {"max_nodes": max_nodes, "max_depth": max_depth},
+        "execution_limits": {"fuel": fuel},
+        "nonterminals": [{"id": "Expr", "type": "Int", "scope": [], "alternatives": [
+            {"id": "x", "weight": 3, "expression": {"input": "x"}},
+            {"id": "c", "weight": 2, "expression": {"constant": {"type": "Int", "range": ["-2", "3"]}}},
+            {"id": "add", "weight": 1, "expression": _binary("add")},
+            {"id": "sub", "weight": 1, "expression": _binary("sub")},
+            {"id": "mul", "weight": 1, "expression": _binary("mul")},
+            {"id": "idiv0", "weight": 1, "expression": _binary("idiv0")},
+            {"id": "imod0", "weight": 1, "expression": _binary("imod0")},
+            {"id": "iflt", "weight": 1, "expression": {
+                "signature": "if(Bool,Int,Int)->Int",
+                "args": [{"signature": "lt(Int,Int)->Bool", "args": [ref, ref]}, ref, ref]}},
+        ]}],
+    }
+
+
+def poly4(population: int = 16384, generations: int = 128, seed: int = 0, cases: int = 256,
+          max_nodes: int = 64) -> TaskFiles:
+    """Random degree<=4 integer polynomial regression over ``cases`` train cases."""
+    rng = random.Random(seed)
+    coefficients = [rng.randint(-5, 5) for _ in range(5)]
+    xs = [rng.randint(-100, 100) for _ in range(cases)]
+    f = lambda x: sum(c * x ** k for k, c in enumerate(coefficients))
+    return TaskFiles(
+        name=f"poly4-s{seed}", grammar=poly4_grammar(max_nodes=max_nodes),
+        train=[_int_case(x, f(x)) for x in xs],
+        search=search_config(population, generations, seed))
+
+
+WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4}
+
+
+def make(name: str, **kwargs) -> TaskFiles:
+    return WORKLOADS[name](**kwargs)

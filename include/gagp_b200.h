@@ -1,0 +1,245 @@
+/*
+ * gagp_b200 -- C ABI of the B200 resident GAGP search engine.
+ *
+ * The engine replaces the reference's resident GPU owner
+ * (NativePhasePopulation, cpp/src/evolution/repro/gpu/phase_population.hpp:15-60)
+ * and the steady-state search loop that drives it
+ * (run_phase_population_steady, cpp/src/evolution/evolve.cpp:331-441).
+ * Plain pointers and sizes only; every device resource is owned by the
+ * engine handle.  Inputs are copied in; exports are copied into caller
+ * buffers.  API calls on one engine must be serialized by the caller.
+ *
+ * Data formats (the admitted phase tables) follow the reference's
+ * HostPhaseGrammar / DeviceSlot layout
+ * (cpp/src/evolution/repro/gpu/phase_grammar.hpp:17-40,
+ *  cpp/src/evolution/repro/gpu/phase_operators.cuh:25).
+ */
+#ifndef GAGP_B200_H
+#define GAGP_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status (reference: invalid_argument = decline, runtime_error = failure) */
+typedef int32_t gagp_status;
+enum {
+  GAGP_OK = 0,
+  GAGP_DECLINED = 1,          /* admission decline: rerun on the native representation */
+  GAGP_INVALID_ARGUMENT = 2,
+  GAGP_OUT_OF_MEMORY = 3,
+  GAGP_DEVICE_ERROR = 4,      /* the engine is poisoned; later calls are refused */
+  GAGP_TIMEOUT_CAP = 5,       /* a device loop hit its iteration cap */
+  GAGP_NOT_READY = 6,
+  GAGP_NO_EXTENSION = 7
+};
+
+#define GAGP_MAX_ARITY 8
+#define GAGP_MAX_LOCALS 64
+#define GAGP_PHASE_CAPACITY 1024  /* physical phase row capacity of the reference */
+
+/* ValueTag (cpp/include/gagp/core/value.hpp:16-27) */
+enum { GAGP_TAG_INT = 0, GAGP_TAG_FLOAT = 1, GAGP_TAG_BOOL = 2, GAGP_TAG_INVALID = 9 };
+
+/* One generation record (PhaseExpression, device/phase_generate.cuh:79-92).
+ * kind: PhaseExpressionKind; node_*: the PhaseTreeNode it emits
+ * (device/phase_compile.cuh:64-74). */
+typedef struct gagp_expression {
+  int32_t kind;
+  int32_t node_kind;
+  int32_t opcode;
+  int32_t operand;
+  int32_t arity;
+  uint32_t fuel;
+  uint32_t merge_fuel;
+  int32_t type;
+  int32_t target;
+  int32_t scope_count;
+  int32_t children[GAGP_MAX_ARITY];
+  int8_t child_scope[GAGP_MAX_ARITY];
+} gagp_expression;
+
+typedef struct gagp_production {   /* PhaseProduction */
+  int32_t expression;
+  int32_t reserved;
+  double weight;
+} gagp_production;
+
+typedef struct gagp_nonterminal {  /* PhaseNonterminal */
+  int32_t production_offset;
+  int32_t production_count;
+  int32_t scope_count;
+  int32_t normalized_weights;
+  int32_t fixed;
+} gagp_nonterminal;
+
+typedef struct gagp_domain {       /* PhaseDomain */
+  int32_t value_offset;
+  int32_t value_count;
+  int32_t integer_range;
+  int32_t reserved;
+  int64_t minimum;
+  int64_t maximum;
+} gagp_domain;
+
+typedef struct gagp_value {        /* scalar Value: tag + payload */
+  int64_t i;
+  int32_t tag;
+  int32_t reserved;
+} gagp_value;
+
+/* The admitted grammar of one search: phase tables plus its single
+ * whole-program slot (expression entry: program(block(return phase))). */
+typedef struct gagp_grammar {
+  const gagp_expression* expressions; int32_t expression_count;
+  const gagp_production* productions; int32_t production_count;
+  const gagp_nonterminal* nonterminals; int32_t nonterminal_count;
+  const gagp_domain* domains; int32_t domain_count;
+  const gagp_value* values; int32_t value_count;
+  const uint32_t* minimum;          /* [expression][depth][logical] */
+  int32_t depth_count;
+  int32_t logical_depth_count;
+  int32_t site_depth;               /* 0: no site-depth limit */
+  int32_t root_expression;
+  int32_t slot_max_depth;
+  int32_t slot_type;                /* ValueTag of the phase result */
+  int32_t local_count;              /* evaluator inputs, sorted by name */
+  int32_t local_types[GAGP_MAX_LOCALS];
+  int32_t max_nodes;                /* grammar search_limits.max_nodes */
+  int32_t fixed_nodes;              /* AST nodes outside the phase */
+  uint32_t return_fuel;             /* fuel of the appended RETURN */
+} gagp_grammar;
+
+/* Scalar fitness cases: inputs[case * input_count + j] is the payload of
+ * evaluator input j (an Int, or 0/1 for a Bool); tags per input. */
+typedef struct gagp_cases {
+  int32_t case_count;
+  int32_t input_count;
+  const int64_t* inputs;
+  const int32_t* input_tags;
+  const int64_t* expected;
+  int32_t expected_tag;
+} gagp_cases;
+
+/* FitnessMetric (cpp/include/gagp/core/fitness_policy.hpp:4) */
+enum { GAGP_METRIC_LEGACY = 0, GAGP_METRIC_ABSOLUTE = 1, GAGP_METRIC_EXACT = 2 };
+
+/* gagp-search-config-v1 semantics (spec/search_config.md) of a resident run. */
+typedef struct gagp_search_config {
+  int32_t population;
+  int32_t generations;
+  uint64_t seed;
+  int32_t tournament_size;
+  int32_t crossover_attempts;
+  double crossover_probability;
+  double mutation_probability;
+  int32_t mutation_max_nodes;
+  int32_t counted_sites;            /* sites.draw: counted (1) / reservoir (0) */
+  int32_t uniform_phase;            /* sites.scope: uniform_phase (1) / genome (0) */
+  int32_t steady_state;             /* schedule.mode: steady_state (1) / generational (0) */
+  int32_t batch;                    /* steady_state batch (0: population) */
+  int32_t replacement_size;
+  int32_t elite_count;              /* generational only */
+  int32_t fuel;
+  double penalty;                   /* case_cap */
+  int32_t metric;
+  int32_t grammar_site_ranking;     /* ranking.tie_break: grammar_sites */
+  int32_t reduction_lanes;          /* 512 in gagp run */
+  int32_t reserved;
+} gagp_search_config;
+
+/* A population of phase rows in transport form: row r has node_counts[r]
+ * nodes whose construction expressions are origins[r*stride + i] and
+ * constant_counts[r] Int constants constants[r*stride + k] in prefix order. */
+typedef struct gagp_rows {
+  int32_t count;
+  int32_t stride;
+  int32_t* node_counts;
+  int32_t* origins;
+  int32_t* constant_counts;
+  int64_t* constants;
+} gagp_rows;
+
+/* Result of one search (history per generation-equivalent, final ranked
+ * population), in caller-allocated arrays. */
+typedef struct gagp_search_result {
+  int32_t generations;              /* history entries written */
+  double* history_best_fitness;
+  double* history_mean_fitness;
+  int32_t* history_best_wrong;
+  int32_t* history_best_nodes;
+  gagp_rows history_best;           /* champion row per history entry */
+  int32_t population;
+  double* final_fitness;            /* ranked: best first */
+  int32_t* final_wrong;
+  int32_t* final_nodes;
+  gagp_rows final_rows;
+  uint64_t evaluated_programs;      /* program evaluations run */
+  uint64_t reused_programs;         /* children reusing a member's result */
+  uint64_t program_cases;           /* evaluated (program, case) pairs */
+} gagp_search_result;
+
+/* ------------------------------------------------------------------ engine */
+typedef struct gagp_engine gagp_engine;
+
+const char* gagp_b200_last_error(void);
+const char* gagp_b200_version(void);
+
+/* Creates the engine on `device`. `arena_bytes` bounds the device memory the
+ * engine may hold for resident searches (0: 80% of free memory). */
+gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_engine** out);
+void gagp_b200_engine_destroy(gagp_engine* engine);
+
+/* Device bytes a search with this grammar, case set and config needs. */
+gagp_status gagp_b200_search_bytes(const gagp_grammar* grammar, const gagp_cases* cases,
+                                   const gagp_search_config* config, uint64_t* out_bytes);
+
+/* Admits one search (NativePhasePopulation ctor, phase_population.cu:489-629):
+ * uploads its tables and cases and builds its initial population on the
+ * device -- from `initial` when given, otherwise generated from the seed as
+ * generate_phase_initial_population does (phase_population_cpu.cpp:54-113). */
+gagp_status gagp_b200_search_create(gagp_engine* engine, const gagp_grammar* grammar,
+                                    const gagp_cases* cases, const gagp_search_config* config,
+                                    const gagp_rows* initial, int32_t* out_search);
+gagp_status gagp_b200_search_destroy(gagp_engine* engine, int32_t search);
+
+/* Runs a search to completion on the device (the whole steady-state loop,
+ * evolve.cpp:331-441, with no host round trip per round). */
+gagp_status gagp_b200_search_run(gagp_engine* engine, int32_t search);
+
+/* Advances every listed search together, one generation-equivalent per
+ * launch sequence, until all have finished (batched engine). */
+gagp_status gagp_b200_batch_run(gagp_engine* engine, const int32_t* searches, int32_t count);
+
+/* Advances every listed unfinished search by one generation-equivalent;
+ * `finished[i]` is set to 1 once search i has completed. */
+gagp_status gagp_b200_batch_step(gagp_engine* engine, const int32_t* searches, int32_t count,
+                                 int32_t* finished);
+
+/* Copies a finished search's history and final ranked population out. */
+gagp_status gagp_b200_search_result(gagp_engine* engine, int32_t search, gagp_search_result* out);
+
+/* ---- owner interface: the reference's NativePhasePopulation calls, one at
+ * a time, with the host running the loop (evolve.cpp:331-441).  The plain
+ * one-search-per-launch path. */
+gagp_status gagp_b200_owner_evaluate(gagp_engine* engine, int32_t search, double* fitness,
+                                     uint32_t* wrong);
+gagp_status gagp_b200_owner_make_batch(gagp_engine* engine, int32_t search,
+                                       const double* selection_fitness, int32_t tournament_size,
+                                       double mutation_probability, uint64_t seed, int32_t* reuse);
+gagp_status gagp_b200_owner_evaluate_batch(gagp_engine* engine, int32_t search, const int32_t* reuse,
+                                           double* fitness, uint32_t* wrong);
+gagp_status gagp_b200_owner_node_counts(gagp_engine* engine, int32_t search, int32_t batch_rows,
+                                        uint32_t* nodes);
+gagp_status gagp_b200_owner_commit_batch(gagp_engine* engine, int32_t search,
+                                         const int32_t* placements, int32_t count);
+gagp_status gagp_b200_owner_export(gagp_engine* engine, int32_t search, int32_t batch_rows,
+                                   gagp_rows* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,80 @@
+"""Regenerates the golden fixtures of this directory from the reference's own
+CPU engine, compiled from its sources by ``make -C oracle ref``.
+
+Each fixture ``<name>.json.gz`` holds the task file set (grammar, train cases,
+search config) and the reference's outputs for it: the admitted phase tables
+and initial population rows (``ref_driver tables``) and one complete CPU
+search (``ref_driver run``: per-generation history and the final ranked
+population with fitness, wrong counts, node counts, program text and rows).
+
+Run here (the container with the reference tree):
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import gzip
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from gagp_b200 import workloads as W  # noqa: E402
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+
+# name, workload, workload arguments, search-config overrides
+CASES = [
+    ("polynomial_p1024_g64", "polynomial", dict(population=1024, generations=64, seed=0), {}),
+    ("poly4_p512_g12_s1", "poly4", dict(population=512, generations=12, seed=1, cases=100), {}),
+    ("poly4_genome_reservoir", "poly4", dict(population=256, generations=10, seed=2, cases=50),
+     {"sites": {"scope": "genome", "draw": "reservoir"}}),
+    ("poly4_gate1_mutcap5", "poly4", dict(population=256, generations=10, seed=3, cases=50),
+     {"crossover": {"probability": 1.0, "attempts": 3}, "mutation": {"probability": 0.5, "max_subtree_nodes": 5}}),
+    ("poly4_batch64_repl3", "poly4", dict(population=256, generations=10, seed=4, cases=50),
+     {"schedule": {"mode": "steady_state", "batch": 64, "replacement_size": 3}}),
+    ("poly4_sitedepth4_t4", "poly4", dict(population=300, generations=10, seed=5, cases=33),
+     {"limits": {"site_depth": 4}, "selection": {"method": "tournament", "size": 4}}),
+    ("poly4_sitedepth1", "poly4", dict(population=256, generations=8, seed=6, cases=40), {"limits": {"site_depth": 1}}),
+    ("polynomial_grammar_sites", "polynomial", dict(population=200, generations=20, seed=9),
+     {"ranking": {"tie_break": "grammar_sites"}}),
+    ("poly4_exact_metric", "poly4", dict(population=256, generations=6, seed=7, cases=64), {}),
+]
+
+
+def driver(*args) -> dict:
+    out = subprocess.run([DRIVER, *args], check=True, capture_output=True, text=True).stdout
+    return json.loads(out)
+
+
+def main() -> None:
+    if not os.path.exists(DRIVER):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    here = os.path.dirname(os.path.abspath(__file__))
+    for name, workload, kwargs, extra in CASES:
+        task = W.make(workload, **kwargs)
+        task.search.update(extra)
+        if name.endswith("exact_metric"):
+            task.fitness = {"metric": "exact"}
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            tables = driver("tables", tp, "--search", sp)
+            run = driver("run", tp, "--search", sp)
+        fixture = {
+            "name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+            "train": task.train, "test": task.test, "search": task.search,
+            "tables": {k: v for k, v in tables.items() if k != "initial"},
+            "initial": [rows[0] for rows in tables["initial"]],
+            "run": run,
+        }
+        with gzip.open(os.path.join(here, name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
+
+
+if __name__ == "__main__":
+    main()

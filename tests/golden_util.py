@@ -1,0 +1,56 @@
+"""Loads the golden fixtures of tests/golden (see make_golden.py)."""
+from __future__ import annotations
+
+import glob
+import gzip
+import json
+import os
+import tempfile
+
+from gagp_b200 import abi
+from gagp_b200 import task as T
+from gagp_b200 import workloads as W
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(os.path.basename(p)[: -len(".json.gz")] for p in glob.glob(os.path.join(HERE, "*.json.gz")))
+
+
+def fixture(name: str) -> dict:
+    with gzip.open(os.path.join(HERE, name + ".json.gz"), "rt") as f:
+        return json.load(f)
+
+
+def load_task(fx: dict) -> T.LoadedTask:
+    files = W.TaskFiles(name=fx["task"]["name"], grammar=fx["grammar"], train=fx["train"], test=fx["test"],
+                        fitness=fx["task"]["fitness"], search=fx["search"])
+    with tempfile.TemporaryDirectory() as d:
+        files.write(d)
+        return T.load(os.path.join(d, "task.json"), os.path.join(d, "search.json"))
+
+
+def reference_rows(rows, stride: int) -> abi.RowsBuffer:
+    return abi.RowsBuffer.from_rows([(r["origins"], [c[1] for c in r["constants"]]) for r in rows], stride)
+
+
+def compare_result(lt: T.LoadedTask, got: dict, run: dict, label: str = "") -> None:
+    """Asserts a search result equals the reference run bit for bit."""
+    ref_hist, ref_final = run["history"], run["final"]
+    assert len(got["history"]) == len(ref_hist), label
+    for i, (a, b) in enumerate(zip(got["history"], ref_hist)):
+        text = T.program_text(lt.tables, *a["row"])
+        assert a["best_fitness"] == b["best_fitness"], (label, "history", i, a["best_fitness"], b["best_fitness"])
+        assert a["mean_fitness"] == float.fromhex(b["mean_fitness"]), (label, "mean", i)
+        assert a["best_wrong"] == b["best_wrong"], (label, "wrong", i)
+        assert a["best_nodes"] == b["best_nodes"], (label, "nodes", i)
+        assert text == b["text"], (label, "champion", i, text, b["text"])
+    assert len(got["final"]) == len(ref_final), label
+    for i, (a, b) in enumerate(zip(got["final"], ref_final)):
+        r = b["rows"][0]
+        assert a["fitness"] == b["fitness"], (label, "final fitness", i, a["fitness"], b["fitness"])
+        assert a["wrong"] == b["wrong"], (label, "final wrong", i)
+        assert a["nodes"] == b["nodes"], (label, "final nodes", i)
+        assert list(a["row"][0]) == r["origins"], (label, "final origins", i)
+        assert list(a["row"][1]) == [c[1] for c in r["constants"]], (label, "final constants", i)
