@@ -1,0 +1,696 @@
+// Host side of the B200 resident GAGP engine: admission, device memory,
+// launch sequences and the C ABI of include/gagp_b200.h.
+//
+// One engine per device.  A search owns one device allocation holding its
+// tables, cases, population rows, child rows, lowered programs, run-generator
+// stream and history; it stays resident between generations.  A batch is any
+// set of searches advanced together: every kernel takes the batch's
+// descriptor array and flat item offsets, so one launch sequence advances all
+// of them by one round.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_error;
+
+gagp_status fail(gagp_status status, const std::string& message) {
+  g_error = message;
+  return status;
+}
+
+#define CUDA_TRY(expr)                                                                    \
+  do {                                                                                    \
+    const cudaError_t e_ = (expr);                                                        \
+    if (e_ != cudaSuccess) return fail(GAGP_DEVICE_ERROR, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Sub-allocation plan of one search's device block.
+struct Layout {
+  size_t total = 0;
+  size_t take(size_t bytes) {
+    const size_t at = align_up(total, 256);
+    total = at + bytes;
+    return at;
+  }
+};
+
+struct Search {
+  int id = 0;
+  gb::SearchDesc desc{};
+  char* block = nullptr;
+  size_t bytes = 0;
+  int P = 0, B = 0, G = 0, total_rounds = 0, maxv = 0, stride = 0, fixed_nodes = 0;
+  int has_wrong = 0;
+  bool started = false;
+  gb::SearchDesc* d_desc = nullptr;   // single-search batch descriptor
+  int32_t* d_off = nullptr;           // {0, P, 0, B}: member and child offsets
+};
+
+}  // namespace
+
+struct gagp_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::map<int, std::unique_ptr<Search>> searches;
+  int next_id = 1;
+  uint64_t arena_limit = 0, arena_used = 0;
+  int sm_count = 0;
+  size_t max_smem = 0;
+  // batch scratch
+  gb::ProgramRef* d_fast = nullptr;
+  gb::ProgramRef* d_general = nullptr;
+  int32_t* d_counts = nullptr;
+  size_t list_capacity = 0;
+  gb::SearchDesc* d_batch_desc = nullptr;
+  size_t batch_desc_capacity = 0;
+  int32_t* d_batch_off = nullptr;
+  size_t batch_off_capacity = 0;
+  bool poisoned = false;
+};
+
+namespace {
+
+gagp_status ensure_lists(gagp_engine* e, size_t items) {
+  if (items <= e->list_capacity) return GAGP_OK;
+  if (e->d_fast) cudaFree(e->d_fast);
+  if (e->d_general) cudaFree(e->d_general);
+  e->d_fast = e->d_general = nullptr;
+  const size_t cap = std::max<size_t>(items, 1024);
+  CUDA_TRY(cudaMalloc(&e->d_fast, cap * sizeof(gb::ProgramRef)));
+  CUDA_TRY(cudaMalloc(&e->d_general, cap * sizeof(gb::ProgramRef)));
+  if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, 4 * sizeof(int32_t)));
+  e->list_capacity = cap;
+  return GAGP_OK;
+}
+
+// Highest cases-per-lane the VM uses for `cases` (autotuned by case count:
+// the fewest warp passes with at most 8 cases per lane).
+int cases_per_lane(int cases) {
+  if (cases <= 32) return 1;
+  if (cases <= 64) return 2;
+  if (cases <= 128) return 4;
+  return 8;
+}
+
+int bits_for(uint64_t v) {
+  int b = 0;
+  while (b < 64 && (v >> b)) ++b;
+  return b;
+}
+
+// Admission checks of this engine (a decline reruns on the native path in
+// the reference).  Returns GAGP_OK or GAGP_DECLINED with a reason.
+gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg) {
+  if (!g || !c || !cfg) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (!cfg->steady_state) return fail(GAGP_DECLINED, "the device-resident loop runs the steady-state schedule");
+  if (cfg->population < 1 || cfg->population > 16384) return fail(GAGP_DECLINED, "population/grammar capacity");
+  const int B = cfg->batch > 0 ? cfg->batch : cfg->population;
+  if (B > cfg->population || cfg->population % B) return fail(GAGP_INVALID_ARGUMENT, "steady-state batch must divide the population");
+  if (cfg->generations < 1) return fail(GAGP_INVALID_ARGUMENT, "generations must be > 0");
+  if (cfg->replacement_size < 1 || cfg->replacement_size > 64) return fail(GAGP_INVALID_ARGUMENT, "replacement_size");
+  if (cfg->tournament_size < 1 || cfg->crossover_attempts < 1 || cfg->crossover_attempts > 64)
+    return fail(GAGP_INVALID_ARGUMENT, "selection/crossover contract");
+  if (!(cfg->mutation_probability >= 0 && cfg->mutation_probability <= 1) ||
+      !(cfg->crossover_probability >= 0 && cfg->crossover_probability <= 1))
+    return fail(GAGP_INVALID_ARGUMENT, "probabilities must be in [0,1]");
+  if (cfg->metric != GAGP_METRIC_ABSOLUTE && cfg->metric != GAGP_METRIC_EXACT)
+    return fail(GAGP_DECLINED, "fitness metric outside the resident scalar subset");
+  const double pen = std::fabs(cfg->penalty);
+  if (pen != std::floor(pen) || pen < 1 || pen > 2147483647.0)
+    return fail(GAGP_DECLINED, "a fractional penalty needs the ordered 48-bit reduction");
+  if (double(c->case_count) * pen >= 281474976710656.0) return fail(GAGP_DECLINED, "cases * penalty must stay below 2^48");
+  if (c->case_count < 1 || c->case_count > (1 << 20)) return fail(GAGP_INVALID_ARGUMENT, "case count");
+  if (c->input_count != g->local_count || g->local_count > GAGP_MAX_LOCALS)
+    return fail(GAGP_INVALID_ARGUMENT, "case inputs must cover the grammar inputs");
+  if (g->expression_count < 1 || g->expression_count > 65534) return fail(GAGP_DECLINED, "expression table capacity");
+  if (g->site_depth < 1 || g->site_depth > 15) return fail(GAGP_DECLINED, "the device population is grown under a site-depth limit");
+  const int maxv = g->max_nodes - g->fixed_nodes;
+  if (maxv < 1 || maxv > gb::kMaxLowerNodes) return fail(GAGP_DECLINED, "variable node budget outside 1..256");
+  if (g->slot_max_depth < 1 || g->slot_max_depth >= g->depth_count || g->depth_count > 65)
+    return fail(GAGP_DECLINED, "depth budget");
+  for (int i = 0; i < g->expression_count; ++i) {
+    const gagp_expression& e = g->expressions[i];
+    if (e.kind == gb::EK_REFERENCE && e.scope_count != 0)
+      return fail(GAGP_DECLINED, "scoped nonterminals are outside the resident scalar subset");
+    if (e.kind == gb::EK_BOUND || e.kind == gb::EK_ALIAS)
+      return fail(GAGP_DECLINED, "lexical binders/templates are outside the resident scalar subset");
+    if (e.arity < 0 || e.arity > 3) return fail(GAGP_DECLINED, "arity capacity");
+  }
+  for (int i = 0; i < g->domain_count; ++i)
+    if (!g->domains[i].integer_range)
+      for (int k = 0; k < g->domains[i].value_count; ++k)
+        if (g->values[g->domains[i].value_offset + k].tag != GAGP_TAG_INT)
+          return fail(GAGP_DECLINED, "only Int constants are resident");
+  return GAGP_OK;
+}
+
+struct Plan {
+  Layout L;
+  size_t ex, info, prods, nts, doms, vals, minimum, local_types, inputs, expected;
+  size_t node, cval, len, cnode, ccval, clen, tnode, tcval, gnode, gcval;
+  size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
+  size_t code, code_len, kpool, code_temps, bc, bc_len, bc_consts;
+  size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, round, hist_sum, hist_fitness, hist_wrong,
+      hist_nodes, hist_node, hist_cval, hist_len, counters;
+  int stride, code_stride, bc_stride, stream_capacity, slots;
+};
+
+Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg) {
+  Plan p{};
+  const int P = cfg->population, B = cfg->batch > 0 ? cfg->batch : P, C = c->case_count;
+  const int maxv = g->max_nodes - g->fixed_nodes;
+  p.stride = int(align_up(size_t(maxv), 4));
+  p.code_stride = 2 * maxv + 8;
+  // bytecode bound: if -> 2 instructions, and/or -> 5, everything else 1
+  int per_node = 1;
+  for (int i = 0; i < g->expression_count; ++i) {
+    const int nk = g->expressions[i].node_kind;
+    if (g->expressions[i].kind == gb::EK_OPERATION) per_node = std::max(per_node, nk == gb::TK_IF ? 2 : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
+  }
+  p.bc_stride = per_node * maxv + 2;
+  p.slots = std::max(P, B);
+  const long long draws = (long long)B * cfg->replacement_size + 1;
+  p.stream_capacity = int(((draws + 311) / 312 + 2) * 312);
+  const int E = g->expression_count;
+  auto& L = p.L;
+  p.ex = L.take(sizeof(gagp_expression) * E);
+  p.info = L.take(sizeof(gb::ExprInfo) * E);
+  p.prods = L.take(sizeof(gagp_production) * std::max(1, g->production_count));
+  p.nts = L.take(sizeof(gagp_nonterminal) * std::max(1, g->nonterminal_count));
+  p.doms = L.take(sizeof(gagp_domain) * std::max(1, g->domain_count));
+  p.vals = L.take(sizeof(gagp_value) * std::max(1, g->value_count));
+  p.minimum = L.take(sizeof(uint32_t) * size_t(E) * g->depth_count * g->logical_depth_count);
+  p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
+  p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
+  p.expected = L.take(sizeof(int64_t) * C);
+  const size_t S = size_t(p.stride);
+  p.node = L.take(4 * S * P); p.cval = L.take(8 * S * P); p.len = L.take(4 * size_t(P));
+  p.cnode = L.take(4 * S * B); p.ccval = L.take(8 * S * B); p.clen = L.take(4 * size_t(B));
+  p.tnode = L.take(4 * S * B); p.tcval = L.take(8 * S * B);
+  p.gnode = L.take(4 * S * B); p.gcval = L.take(8 * S * B);
+  p.fitness = L.take(8 * size_t(P)); p.wrong = L.take(4 * size_t(P)); p.nodes = L.take(4 * size_t(P));
+  p.key = L.take(8 * size_t(P));
+  p.c_parent = L.take(4 * size_t(B)); p.c_reuse = L.take(4 * size_t(B)); p.c_error = L.take(4 * size_t(B));
+  p.c_fitness = L.take(8 * size_t(B)); p.c_wrong = L.take(4 * size_t(B)); p.c_nodes = L.take(4 * size_t(B));
+  p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
+  const size_t slots = size_t(p.slots);
+  p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
+  p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots);
+  p.bc = L.take(20 * slots * p.bc_stride); p.bc_len = L.take(4 * slots);
+  p.bc_consts = L.take(8 * slots * p.bc_stride);
+  p.mt = L.take(8 * 312); p.stream = L.take(8 * size_t(p.stream_capacity));
+  p.stream_mod = L.take(4 * size_t(p.stream_capacity)); p.stream_head = L.take(16);
+  p.round_seed = L.take(8); p.best = L.take(4); p.placed = L.take(4 * size_t(P)); p.round = L.take(16);
+  const size_t H = size_t(cfg->generations);
+  p.hist_sum = L.take(8 * H); p.hist_fitness = L.take(8 * H); p.hist_wrong = L.take(4 * H);
+  p.hist_nodes = L.take(4 * H); p.hist_node = L.take(4 * S * H); p.hist_cval = L.take(8 * S * H);
+  p.hist_len = L.take(4 * H); p.counters = L.take(8 * 4);
+  return p;
+}
+
+template <class T>
+T* at(char* block, size_t off) { return reinterpret_cast<T*>(block + off); }
+
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" {
+
+const char* gagp_b200_last_error(void) { return g_error.c_str(); }
+const char* gagp_b200_version(void) { return "gagp_b200 1.0 (sm_100a)"; }
+
+gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_engine** out) {
+  if (!out) return fail(GAGP_INVALID_ARGUMENT, "null engine pointer");
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(GAGP_DEVICE_ERROR, "no CUDA device");
+  if (device < 0 || device >= count) return fail(GAGP_INVALID_ARGUMENT, "device index");
+  CUDA_TRY(cudaSetDevice(device));
+  auto e = std::make_unique<gagp_engine>();
+  e->device = device;
+  CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  e->sm_count = prop.multiProcessorCount;
+  e->max_smem = prop.sharedMemPerBlockOptin;
+  size_t free_bytes = 0, total = 0;
+  CUDA_TRY(cudaMemGetInfo(&free_bytes, &total));
+  e->arena_limit = arena_bytes ? arena_bytes : uint64_t(0.8 * double(free_bytes));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 8192));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
+  *out = e.release();
+  return GAGP_OK;
+}
+
+void gagp_b200_engine_destroy(gagp_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  cudaStreamSynchronize(e->stream);
+  for (auto& kv : e->searches) {
+    cudaFree(kv.second->block);
+    cudaFree(kv.second->d_desc);
+    cudaFree(kv.second->d_off);
+  }
+  cudaFree(e->d_fast);
+  cudaFree(e->d_general);
+  cudaFree(e->d_counts);
+  cudaFree(e->d_batch_desc);
+  cudaFree(e->d_batch_off);
+  cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+gagp_status gagp_b200_search_bytes(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg,
+                                   uint64_t* out_bytes) {
+  const gagp_status st = admit(g, c, cfg);
+  if (st != GAGP_OK) return st;
+  *out_bytes = plan_search(g, c, cfg).L.total;
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const gagp_cases* c,
+                                    const gagp_search_config* cfg, const gagp_rows* initial, int32_t* out_search) {
+  if (!e || !out_search) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  if (initial) return fail(GAGP_DECLINED, "imported initial populations are not supported by this engine yet");
+  const gagp_status st = admit(g, c, cfg);
+  if (st != GAGP_OK) return st;
+  CUDA_TRY(cudaSetDevice(e->device));
+  Plan p = plan_search(g, c, cfg);
+  if (e->arena_used + p.L.total > e->arena_limit)
+    return fail(GAGP_OUT_OF_MEMORY, "search does not fit the engine's device-memory budget");
+  auto s = std::make_unique<Search>();
+  s->P = cfg->population;
+  s->B = cfg->batch > 0 ? cfg->batch : cfg->population;
+  s->G = cfg->generations;
+  s->total_rounds = int((long long)s->P * s->G / s->B);
+  s->maxv = g->max_nodes - g->fixed_nodes;
+  s->stride = p.stride;
+  s->fixed_nodes = g->fixed_nodes;
+  s->has_wrong = cfg->metric != GAGP_METRIC_LEGACY;
+  s->bytes = p.L.total;
+  CUDA_TRY(cudaMalloc(&s->block, s->bytes));
+  CUDA_TRY(cudaMemsetAsync(s->block, 0, s->bytes, e->stream));
+  char* b = s->block;
+  const int E = g->expression_count;
+  // derived per-expression facts
+  std::vector<gb::ExprInfo> info(E);
+  for (int i = 0; i < E; ++i) {
+    const gagp_expression& x = g->expressions[i];
+    gb::ExprInfo& f = info[i];
+    f.kind = int8_t(x.kind);
+    f.node_kind = int8_t(x.node_kind);
+    f.arity = int8_t(x.kind == gb::EK_REFERENCE ? 0 : x.arity);
+    f.type = int8_t(x.type);
+    f.opcode = int16_t(x.opcode);
+    f.operand = x.operand;
+    f.target = x.target;
+    f.site_nt = x.kind == gb::EK_REFERENCE ? x.target : -1;
+    f.site_class = -1;
+    if (x.kind == gb::EK_REFERENCE && x.target >= 0 && x.target < g->nonterminal_count &&
+        !g->nonterminals[x.target].fixed)
+      f.site_class = x.target * 16 + x.scope_count;
+  }
+  // cases, input-major
+  const int C = c->case_count, NI = c->input_count;
+  std::vector<int64_t> inputs(size_t(std::max(1, NI)) * C, 0);
+  for (int j = 0; j < NI; ++j)
+    for (int k = 0; k < C; ++k) inputs[size_t(j) * C + k] = c->inputs[size_t(k) * NI + j];
+  std::vector<int32_t> local_types(GAGP_MAX_LOCALS, GAGP_TAG_INVALID);
+  for (int j = 0; j < g->local_count; ++j) local_types[j] = g->local_types[j];
+  auto up = [&](size_t off, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(b + off, src, bytes, cudaMemcpyHostToDevice, e->stream);
+  };
+  CUDA_TRY(up(p.ex, g->expressions, sizeof(gagp_expression) * E));
+  CUDA_TRY(up(p.info, info.data(), sizeof(gb::ExprInfo) * E));
+  if (g->production_count) CUDA_TRY(up(p.prods, g->productions, sizeof(gagp_production) * g->production_count));
+  if (g->nonterminal_count) CUDA_TRY(up(p.nts, g->nonterminals, sizeof(gagp_nonterminal) * g->nonterminal_count));
+  if (g->domain_count) CUDA_TRY(up(p.doms, g->domains, sizeof(gagp_domain) * g->domain_count));
+  if (g->value_count) CUDA_TRY(up(p.vals, g->values, sizeof(gagp_value) * g->value_count));
+  CUDA_TRY(up(p.minimum, g->minimum, sizeof(uint32_t) * size_t(E) * g->depth_count * g->logical_depth_count));
+  CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
+  CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
+  CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
+
+  gb::SearchDesc& d = s->desc;
+  d.ex = at<gagp_expression>(b, p.ex);
+  d.info = at<gb::ExprInfo>(b, p.info);
+  d.prods = at<gagp_production>(b, p.prods);
+  d.nts = at<gagp_nonterminal>(b, p.nts);
+  d.doms = at<gagp_domain>(b, p.doms);
+  d.vals = at<gagp_value>(b, p.vals);
+  d.minimum = at<uint32_t>(b, p.minimum);
+  d.local_types = at<int32_t>(b, p.local_types);
+  d.n_ex = E; d.n_prods = g->production_count; d.n_nts = g->nonterminal_count;
+  d.n_doms = g->domain_count; d.n_vals = g->value_count;
+  d.depth_count = g->depth_count; d.logical_count = g->logical_depth_count; d.site_depth = g->site_depth;
+  d.root_expression = g->root_expression; d.slot_max_depth = g->slot_max_depth; d.slot_type = g->slot_type;
+  d.local_count = g->local_count; d.max_nodes = g->max_nodes; d.fixed_nodes = g->fixed_nodes;
+  d.return_fuel = g->return_fuel;
+  d.P = s->P; d.B = s->B; d.maxv = s->maxv; d.stride = p.stride;
+  d.pressure = std::clamp(cfg->tournament_size, 1, s->P);
+  d.attempts = cfg->crossover_attempts; d.mutation_max_nodes = cfg->mutation_max_nodes;
+  d.counted = cfg->counted_sites; d.uniform_phase = cfg->uniform_phase; d.replacement_size = cfg->replacement_size;
+  d.has_wrong = s->has_wrong; d.grammar_sites = cfg->grammar_site_ranking;
+  d.metric = cfg->metric; d.fuel = cfg->fuel;
+  d.crossover_probability = cfg->crossover_probability; d.mutation_probability = cfg->mutation_probability;
+  d.penalty = cfg->penalty; d.penalty_int = (int64_t)std::fabs(cfg->penalty);
+  d.seed = cfg->seed;
+  d.rounds_per_epoch = s->P / s->B;
+  d.generations = s->G;
+  d.inputs = at<int64_t>(b, p.inputs); d.expected = at<int64_t>(b, p.expected);
+  d.C = C; d.n_inputs = NI; d.expected_tag = c->expected_tag; d.vm_cases_per_lane = cases_per_lane(C);
+  d.node = at<uint32_t>(b, p.node); d.cval = at<int64_t>(b, p.cval); d.len = at<int32_t>(b, p.len);
+  d.cnode = at<uint32_t>(b, p.cnode); d.ccval = at<int64_t>(b, p.ccval); d.clen = at<int32_t>(b, p.clen);
+  d.tnode = at<uint32_t>(b, p.tnode); d.tcval = at<int64_t>(b, p.tcval);
+  d.gnode = at<uint32_t>(b, p.gnode); d.gcval = at<int64_t>(b, p.gcval);
+  d.fitness = at<double>(b, p.fitness); d.wrong = at<uint32_t>(b, p.wrong); d.nodes = at<uint32_t>(b, p.nodes);
+  d.key = at<uint64_t>(b, p.key);
+  d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
+  d.c_fitness = at<double>(b, p.c_fitness); d.c_wrong = at<uint32_t>(b, p.c_wrong);
+  d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
+  d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
+  d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
+  d.bc = at<int32_t>(b, p.bc); d.bc_len = at<int32_t>(b, p.bc_len); d.bc_consts = at<int64_t>(b, p.bc_consts);
+  d.bc_stride = p.bc_stride;
+  d.mt = at<uint64_t>(b, p.mt); d.stream = at<uint64_t>(b, p.stream); d.stream_mod = at<uint32_t>(b, p.stream_mod);
+  d.stream_head = at<long long>(b, p.stream_head); d.stream_capacity = p.stream_capacity;
+  d.round_seed = at<uint64_t>(b, p.round_seed);
+  d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
+  d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
+  d.hist_wrong = at<uint32_t>(b, p.hist_wrong); d.hist_nodes = at<uint32_t>(b, p.hist_nodes);
+  d.hist_node = at<uint32_t>(b, p.hist_node); d.hist_cval = at<int64_t>(b, p.hist_cval);
+  d.hist_len = at<int32_t>(b, p.hist_len); d.counters = at<uint64_t>(b, p.counters);
+  // packed ranking key: loss | wrong | nodes
+  const int node_bits = bits_for(uint64_t(g->max_nodes));
+  const int wrong_bits = bits_for(uint64_t(C));
+  const int loss_bits = bits_for(uint64_t(double(C) * std::fabs(cfg->penalty)));
+  if (s->has_wrong && node_bits + wrong_bits + loss_bits > 64) {
+    cudaFree(s->block);
+    return fail(GAGP_DECLINED, "ranking key wider than 64 bits");
+  }
+  d.key_shift_nodes = node_bits;
+  d.key_shift_wrong = node_bits + wrong_bits;
+  d.total_rounds = s->total_rounds;
+  CUDA_TRY(cudaMalloc(&s->d_desc, sizeof(gb::SearchDesc)));
+  CUDA_TRY(cudaMemcpyAsync(s->d_desc, &d, sizeof(gb::SearchDesc), cudaMemcpyHostToDevice, e->stream));
+  const int32_t off[4] = {0, s->P, 0, s->B};
+  CUDA_TRY(cudaMalloc(&s->d_off, sizeof(off)));
+  CUDA_TRY(cudaMemcpyAsync(s->d_off, off, sizeof(off), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  s->id = e->next_id++;
+  e->arena_used += s->bytes;
+  *out_search = s->id;
+  e->searches[s->id] = std::move(s);
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_search_destroy(gagp_engine* e, int32_t id) {
+  if (!e) return fail(GAGP_INVALID_ARGUMENT, "null engine");
+  auto it = e->searches.find(id);
+  if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
+  cudaSetDevice(e->device);
+  cudaStreamSynchronize(e->stream);
+  cudaFree(it->second->block);
+  cudaFree(it->second->d_desc);
+  cudaFree(it->second->d_off);
+  e->arena_used -= it->second->bytes;
+  e->searches.erase(it);
+  return GAGP_OK;
+}
+
+}  // extern "C"
+
+// ======================================================================= batches
+namespace {
+
+struct BatchView {
+  gb::SearchDesc* d_desc = nullptr;
+  int32_t* d_member_off = nullptr;   // n + 1
+  int32_t* d_child_off = nullptr;    // n + 1
+  int n = 0, total_members = 0, total_children = 0, max_P = 0, max_lanes = 1, max_rounds = 0;
+};
+
+gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
+  const int n = int(list.size());
+  v->n = n;
+  if (n == 1) {
+    v->d_desc = list[0]->d_desc;
+    v->d_member_off = list[0]->d_off;
+    v->d_child_off = list[0]->d_off + 2;
+  } else {
+    if (size_t(n) > e->batch_desc_capacity) {
+      cudaFree(e->d_batch_desc);
+      CUDA_TRY(cudaMalloc(&e->d_batch_desc, sizeof(gb::SearchDesc) * n));
+      e->batch_desc_capacity = n;
+    }
+    if (size_t(2 * (n + 1)) > e->batch_off_capacity) {
+      cudaFree(e->d_batch_off);
+      CUDA_TRY(cudaMalloc(&e->d_batch_off, sizeof(int32_t) * 2 * (n + 1)));
+      e->batch_off_capacity = 2 * (n + 1);
+    }
+    std::vector<gb::SearchDesc> descs(n);
+    std::vector<int32_t> off(2 * (n + 1), 0);
+    for (int i = 0; i < n; ++i) {
+      descs[i] = list[i]->desc;
+      off[i + 1] = off[i] + list[i]->P;
+      off[n + 1 + i + 1] = off[n + 1 + i] + list[i]->B;
+    }
+    CUDA_TRY(cudaMemcpyAsync(e->d_batch_desc, descs.data(), sizeof(gb::SearchDesc) * n, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->d_batch_off, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, e->stream));
+    v->d_desc = e->d_batch_desc;
+    v->d_member_off = e->d_batch_off;
+    v->d_child_off = e->d_batch_off + n + 1;
+  }
+  v->total_members = v->total_children = v->max_P = v->max_rounds = 0;
+  v->max_lanes = 1;
+  for (Search* s : list) {
+    v->total_members += s->P;
+    v->total_children += s->B;
+    v->max_P = std::max(v->max_P, s->P);
+    v->max_lanes = std::max(v->max_lanes, s->desc.vm_cases_per_lane);
+    v->max_rounds = std::max(v->max_rounds, s->total_rounds);
+  }
+  return ensure_lists(e, size_t(std::max(v->total_members, v->total_children)));
+}
+
+int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1) / threads); }
+
+// Evaluates lowered programs listed by k_lower (both VMs).
+gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
+  const int warps = 8;
+  const int temp_stride = gb::kMaxTemps * v.max_lanes * 32;
+  const size_t smem = size_t(warps) * temp_stride * sizeof(int64_t);
+  const int blocks = e->sm_count * std::max(1, int((e->max_smem - 1024) / std::max<size_t>(smem, 1)) > 2 ? 2 : 1);
+  gb::k_vm_fast<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, mode, e->d_fast, e->d_counts, temp_stride);
+  gb::k_vm_general<<<e->sm_count * 4, 128, 0, e->stream>>>(v.d_desc, mode, e->d_general, e->d_counts + 1);
+  return GAGP_OK;
+}
+
+gagp_status launch_start(gagp_engine* e, const BatchView& v) {
+  gb::k_init_population<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
+  gb::k_lower<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n, 0, e->d_fast,
+                                                                        e->d_general, e->d_counts);
+  launch_vm(e, v, 0);
+  gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+  gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n);
+  return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
+}
+
+gagp_status launch_round(gagp_engine* e, const BatchView& v) {
+  gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1);
+  gb::k_vary<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n);
+  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
+  gb::k_lower<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
+                                                                         e->d_general, e->d_counts);
+  launch_vm(e, v, 1);
+  gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n);
+  gb::k_place<<<v.n, 256, size_t(v.max_P) * sizeof(uint64_t), e->stream>>>(v.d_desc, v.n);
+  gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+  return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
+}
+
+gagp_status collect(gagp_engine* e, const std::vector<int32_t>& ids, std::vector<Search*>* list) {
+  for (int32_t id : ids) {
+    auto it = e->searches.find(id);
+    if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search " + std::to_string(id));
+    list->push_back(it->second.get());
+  }
+  return GAGP_OK;
+}
+
+gagp_status check_errors(gagp_engine* e, const std::vector<Search*>& list) {
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  for (Search* s : list) {
+    int32_t round[4];
+    CUDA_TRY(cudaMemcpy(round, s->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
+    if (round[3]) return fail(GAGP_DEVICE_ERROR, "search " + std::to_string(s->id) + " failed on the device (code " + std::to_string(round[3]) + ")");
+  }
+  return GAGP_OK;
+}
+
+gagp_status run_batch(gagp_engine* e, const std::vector<Search*>& list) {
+  BatchView v;
+  gagp_status st = make_batch_view(e, list, &v);
+  if (st != GAGP_OK) return st;
+  std::vector<Search*> fresh;
+  for (Search* s : list) if (!s->started) fresh.push_back(s);
+  if (!fresh.empty()) {
+    BatchView fv;
+    if (fresh.size() == list.size()) fv = v;
+    else if ((st = make_batch_view(e, fresh, &fv)) != GAGP_OK) return st;
+    if ((st = launch_start(e, fv)) != GAGP_OK) return st;
+    for (Search* s : fresh) s->started = true;
+    if (fresh.size() != list.size() && (st = make_batch_view(e, list, &v)) != GAGP_OK) return st;
+  }
+  for (int r = 0; r < v.max_rounds; ++r)
+    if ((st = launch_round(e, v)) != GAGP_OK) return st;
+  return check_errors(e, list);
+}
+
+}  // namespace
+
+extern "C" {
+
+gagp_status gagp_b200_search_run(gagp_engine* e, int32_t id) {
+  if (!e) return fail(GAGP_INVALID_ARGUMENT, "null engine");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<Search*> list;
+  gagp_status st = collect(e, {id}, &list);
+  if (st != GAGP_OK) return st;
+  st = run_batch(e, list);
+  if (st == GAGP_DEVICE_ERROR && cudaGetLastError() != cudaSuccess) e->poisoned = true;
+  return st;
+}
+
+gagp_status gagp_b200_batch_run(gagp_engine* e, const int32_t* ids, int32_t count) {
+  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<Search*> list;
+  gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
+  if (st != GAGP_OK || list.empty()) return st;
+  st = run_batch(e, list);
+  if (st == GAGP_DEVICE_ERROR && cudaGetLastError() != cudaSuccess) e->poisoned = true;
+  return st;
+}
+
+gagp_status gagp_b200_batch_step(gagp_engine* e, const int32_t* ids, int32_t count, int32_t* finished) {
+  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<Search*> list;
+  gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
+  if (st != GAGP_OK || list.empty()) return st;
+  BatchView v;
+  std::vector<Search*> fresh;
+  for (Search* s : list) if (!s->started) fresh.push_back(s);
+  if (!fresh.empty()) {
+    if ((st = make_batch_view(e, fresh, &v)) != GAGP_OK) return st;
+    if ((st = launch_start(e, v)) != GAGP_OK) return st;
+    for (Search* s : fresh) s->started = true;
+  }
+  if ((st = make_batch_view(e, list, &v)) != GAGP_OK) return st;
+  if ((st = launch_round(e, v)) != GAGP_OK) return st;
+  if ((st = check_errors(e, list)) != GAGP_OK) return st;
+  if (finished)
+    for (int i = 0; i < count; ++i) {
+      int32_t round[4];
+      CUDA_TRY(cudaMemcpy(round, list[i]->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
+      finished[i] = round[2];
+    }
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_result* out) {
+  if (!e || !out) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  auto it = e->searches.find(id);
+  if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
+  Search* s = it->second.get();
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  const gb::SearchDesc& d = s->desc;
+  int32_t round[4];
+  CUDA_TRY(cudaMemcpy(round, d.round, sizeof(round), cudaMemcpyDeviceToHost));
+  if (round[3]) return fail(GAGP_DEVICE_ERROR, "search failed on the device (code " + std::to_string(round[3]) + ")");
+  if (!round[2]) return fail(GAGP_NOT_READY, "search has not finished");
+  const int H = std::min(round[1], out->generations);
+  const int P = s->P, S = s->stride;
+  std::vector<int64_t> sum(H);
+  std::vector<double> hf(H);
+  std::vector<uint32_t> hw(H), hn(H), hnode(size_t(H) * S);
+  std::vector<int64_t> hc(size_t(H) * S);
+  std::vector<int32_t> hl(H);
+  if (H) {
+    CUDA_TRY(cudaMemcpy(sum.data(), d.hist_sum, 8 * H, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hf.data(), d.hist_fitness, 8 * H, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hw.data(), d.hist_wrong, 4 * H, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hn.data(), d.hist_nodes, 4 * H, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hnode.data(), d.hist_node, 4 * size_t(H) * S, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hc.data(), d.hist_cval, 8 * size_t(H) * S, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hl.data(), d.hist_len, 4 * H, cudaMemcpyDeviceToHost));
+  }
+  auto put_row = [&](const gagp_rows& rows, int index, const uint32_t* node, const int64_t* cval, int32_t l) {
+    const int n = l & 0xffff, nc = (l >> 16) & 0xffff;
+    rows.node_counts[index] = n;
+    rows.constant_counts[index] = nc;
+    for (int i = 0; i < n && i < rows.stride; ++i) rows.origins[size_t(index) * rows.stride + i] = int32_t(node[i] & 0xffffu);
+    for (int i = 0; i < nc && i < rows.stride; ++i) rows.constants[size_t(index) * rows.stride + i] = cval[i];
+  };
+  for (int h = 0; h < H; ++h) {
+    out->history_best_fitness[h] = hf[h];
+    // long double mean of member fitness, as the reference forms it (evolve.cpp:370-371)
+    out->history_mean_fitness[h] = double((long double)sum[h] / (long double)P);
+    out->history_best_wrong[h] = s->has_wrong ? int32_t(hw[h]) : -1;
+    out->history_best_nodes[h] = int32_t(hn[h]);
+    put_row(out->history_best, h, hnode.data() + size_t(h) * S, hc.data() + size_t(h) * S, hl[h]);
+  }
+  out->generations = H;
+  std::vector<double> fit(P);
+  std::vector<uint32_t> wr(P), node(size_t(P) * S);
+  std::vector<uint64_t> key(P);
+  std::vector<int64_t> cv(size_t(P) * S);
+  std::vector<int32_t> len(P);
+  CUDA_TRY(cudaMemcpy(fit.data(), d.fitness, 8 * size_t(P), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(wr.data(), d.wrong, 4 * size_t(P), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(key.data(), d.key, 8 * size_t(P), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(node.data(), d.node, 4 * size_t(P) * S, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(cv.data(), d.cval, 8 * size_t(P) * S, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(len.data(), d.len, 4 * size_t(P), cudaMemcpyDeviceToHost));
+  std::vector<int> order(P);
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
+  const int n_out = std::min(P, out->population);
+  for (int r = 0; r < n_out; ++r) {
+    const int m = order[r];
+    out->final_fitness[r] = fit[m];
+    out->final_wrong[r] = s->has_wrong ? int32_t(wr[m]) : -1;
+    out->final_nodes[r] = s->fixed_nodes + (len[m] & 0xffff);
+    put_row(out->final_rows, r, node.data() + size_t(m) * S, cv.data() + size_t(m) * S, len[m]);
+  }
+  out->population = n_out;
+  uint64_t counters[4];
+  CUDA_TRY(cudaMemcpy(counters, d.counters, sizeof(counters), cudaMemcpyDeviceToHost));
+  out->evaluated_programs = counters[0];
+  out->reused_programs = counters[1];
+  out->program_cases = counters[2];
+  return GAGP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// Device-resident state of one search and the descriptor kernels read it by.
+//
+// Row layout (B200-first, not the reference's): a member is one phase row of
+// at most `maxv` nodes.  A node is one 32-bit word -- the construction
+// expression in the low half and 1 + the expression that opened its grammar
+// site in the high half (0: no site) -- because every other field of the
+// reference's 28-byte PhaseTreeNode and 16-byte PhaseGeneSite is a function
+// of those two ids (device/phase_compile.cuh:64-74, device/phase_generate.cuh:12-17).
+// Constants are int64 payloads in prefix order, which is the operand order
+// the reference's generator and splice assign (phase_generate.cuh:253,
+// phase_variation.cuh:183-187).  A row is 12 bytes per node slot instead of
+// the reference's 64 KB fixed 1024-node rows.
+#pragma once
+#include <cstdint>
+
+#include "../../include/gagp_b200.h"
+
+namespace gb {
+
+constexpr int kCapacity = 1024;        // semantic phase capacity (phase_operators.cuh:13)
+constexpr unsigned kNoId = 0xffffffffu;
+constexpr int kMaxTemps = 6;           // accumulator VM temporaries
+constexpr int kMaxCodeWords = 2048;    // accumulator VM instructions per program
+
+// Per-expression facts the kernels need, derived once at admission.
+struct ExprInfo {
+  int8_t kind;         // PhaseExpressionKind
+  int8_t node_kind;    // PhaseTreeKind
+  int8_t arity;
+  int8_t type;         // ValueTag
+  int16_t opcode;
+  int16_t reserved;
+  int32_t site_class;  // Reference expressions: class of (nonterminal, scope); -1 fixed/none
+  int32_t operand;
+  int32_t target;
+  int32_t site_nt;     // Reference expressions: the nonterminal (site present), else -1
+};
+
+// Everything a kernel needs to work on one search (device pointers).
+struct SearchDesc {
+  // ---- admitted grammar (phase tables)
+  const gagp_expression* ex;
+  const ExprInfo* info;
+  const gagp_production* prods;
+  const gagp_nonterminal* nts;
+  const gagp_domain* doms;
+  const gagp_value* vals;
+  const uint32_t* minimum;
+  const int32_t* local_types;          // ValueTag of each evaluator input
+  int32_t n_ex, n_prods, n_nts, n_doms, n_vals;
+  int32_t depth_count, logical_count, site_depth;
+  int32_t root_expression, slot_max_depth, slot_type, local_count;
+  int32_t max_nodes, fixed_nodes;
+  uint32_t return_fuel;
+  // ---- config
+  int32_t P, B, maxv, stride;          // stride: row slots (>= maxv, multiple of 4)
+  int32_t pressure, attempts, mutation_max_nodes;
+  int32_t counted, uniform_phase, replacement_size, has_wrong, grammar_sites;
+  int32_t metric, fuel;
+  double crossover_probability, mutation_probability, penalty;
+  int64_t penalty_int;                 // |penalty| when integral
+  uint64_t seed;
+  int32_t rounds_per_epoch;            // P / B
+  int32_t generations;
+  // ---- cases (input-major: inputs[j * C + c])
+  const int64_t* inputs;
+  const int64_t* expected;
+  int32_t C, n_inputs, expected_tag, vm_cases_per_lane;
+  // ---- population rows (members) and children
+  uint32_t* node;     int64_t* cval;     int32_t* len;        // P rows
+  uint32_t* cnode;    int64_t* ccval;    int32_t* clen;       // B child rows
+  uint32_t* tnode;    int64_t* tcval;                         // B splice scratch rows
+  uint32_t* gnode;    int64_t* gcval;                         // B generated-subtree rows
+  // ---- member statistics; key: packed ranking key (smaller is better)
+  double* fitness; uint32_t* wrong; uint32_t* nodes; uint64_t* key;
+  // ---- per-child results of one round
+  int32_t* c_parent; int32_t* c_reuse; int32_t* c_error;
+  double* c_fitness; uint32_t* c_wrong; uint32_t* c_nodes; uint64_t* c_key;
+  int32_t* c_eval;                     // 1: evaluate this child
+  // ---- lowered programs (children, or members during the initial evaluation)
+  uint2* code; int32_t* code_len; int64_t* kpool;
+  int32_t code_stride;                 // accumulator instructions per program slot
+  int32_t* code_temps;                 // temporaries; <0: needs the general VM
+  int32_t* bc;                         // reference bytecode (op,flags,a,b,fuel) per program
+  int32_t* bc_len;
+  int64_t* bc_consts;
+  int32_t bc_stride;                   // instructions per program slot
+  // ---- run generator (MT19937-64) and its output stream
+  uint64_t* mt;                        // 312 words
+  uint64_t* stream;                    // buffered outputs
+  uint32_t* stream_mod;                // outputs % P
+  long long* stream_head;              // [0]: outputs read, [1]: outputs written (ring positions)
+  int32_t stream_capacity;
+  uint64_t* round_seed;                // seed of the next round's variation
+  // ---- search progress and history
+  int32_t* best;                       // tracked best member
+  int32_t* placed;                     // P: child placed into member, -1
+  int32_t* round;                      // [0] rounds done, [1] history entries, [2] finished flag, [3] error
+  int64_t* hist_sum;                   // per history entry: sum of member fitness (integral)
+  double* hist_fitness; uint32_t* hist_wrong; uint32_t* hist_nodes;
+  uint32_t* hist_node; int64_t* hist_cval; int32_t* hist_len;
+  uint64_t* counters;                  // [0] evaluated programs, [1] reused, [2] program cases, [3] VM ops
+  int32_t key_shift_wrong, key_shift_nodes; // packed key layout
+  int32_t total_rounds;
+};
+
+}  // namespace gb

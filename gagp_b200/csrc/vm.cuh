@@ -1,0 +1,273 @@
+// Fitness evaluation of lowered programs over the case set.
+//
+// Semantics: run_code_impl (cpp/src/runtime/cpu/execute_bytecode_cpu.cpp:152-626)
+// with the value semantics of cpp/include/gagp/core/value_semantics.hpp:91-190
+// and builtins_cpu.cpp:131-218, scored by fitness_case_score
+// (cpp/include/gagp/core/fitness_policy.hpp:28-58) and summed as
+// eval_fitness_cpu does (cpp/src/runtime/cpu/fitness_cpu.cpp:57-176).
+//
+// Exactness of the reduction: with an integral |penalty| every per-case
+// score is an integer (a capped integer gap, 0/1, or the ceiling), so every
+// partial sum is an integer below 2^48 in magnitude (admission checks
+// cases * |penalty| < 2^48).  The reference's 48-bit canonicalisation is
+// then the identity and its ordered 512-lane reduction equals any integer
+// sum: lanes accumulate int64 losses and the warp reduces with shuffles.
+#pragma once
+#include "lower.cuh"
+
+namespace gb {
+
+__device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t b) { return int64_t(uint64_t(a) + uint64_t(b)); }
+__device__ __forceinline__ int64_t wrap_sub(int64_t a, int64_t b) { return int64_t(uint64_t(a) - uint64_t(b)); }
+__device__ __forceinline__ int64_t wrap_mul(int64_t a, int64_t b) { return int64_t(uint64_t(a) * uint64_t(b)); }
+__device__ __forceinline__ int64_t wrap_neg(int64_t a) { return int64_t(0ULL - uint64_t(a)); }
+// Python-sign modulo (vm_semantics::py_int_mod); b != 0.
+__device__ __forceinline__ int64_t py_mod(int64_t a, int64_t b) {
+  if (b == -1) return 0;
+  int64_t r = a % b;
+  if (r != 0 && ((r < 0) != (b < 0))) r += b;
+  return r;
+}
+__device__ __forceinline__ int64_t idiv0(int64_t a, int64_t b) { return b == 0 ? 0 : b == -1 ? wrap_neg(a) : a / b; }
+__device__ __forceinline__ int64_t imod0(int64_t a, int64_t b) { return b == 0 ? 0 : py_mod(a, b); }
+__device__ __forceinline__ int64_t tdiv0(int64_t a, int64_t b) {
+  return b == 0 || (a == INT64_MIN && b == -1) ? 0 : a / b;
+}
+__device__ __forceinline__ int64_t tmod0(int64_t a, int64_t b) {
+  return b == 0 || (a == INT64_MIN && b == -1) ? 0 : a % b;
+}
+
+// Loss (= -score) of one case and whether it is wrong.  `tag` is the
+// program's static result type; values are Int payloads or 0/1 Bools.
+__device__ __forceinline__ int64_t case_loss(const SearchDesc& s, int tag, int64_t value, int64_t expected,
+                                             uint32_t& wrong) {
+  const bool same = tag == s.expected_tag && value == expected;
+  wrong += !same;
+  if (s.metric == GAGP_METRIC_EXACT) return same ? 0 : 1;
+  if (tag != GAGP_TAG_INT || s.expected_tag != GAGP_TAG_INT) return s.penalty_int;  // not numeric: ceiling
+  const uint64_t gap = value >= expected ? uint64_t(value) - uint64_t(expected) : uint64_t(expected) - uint64_t(value);
+  return gap < uint64_t(s.penalty_int) ? int64_t(gap) : s.penalty_int;
+}
+__device__ __forceinline__ int64_t error_loss(const SearchDesc& s) {
+  return s.metric == GAGP_METRIC_EXACT ? 1 : s.penalty_int;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ------------------------------------------------------------ fast VM
+// One warp runs one accumulator program; lane l holds cases
+// tile*32K + k*32 + l for k < K (coalesced input loads), in registers.
+// Temporaries live in shared memory [temp][k][lane].
+template <int K>
+__device__ inline void run_accumulator(const SearchDesc& s, int slot, int64_t* temps, int64_t& loss_out,
+                                       uint32_t& wrong_out, uint64_t& ops_out) {
+  const int lane = threadIdx.x & 31;
+  const uint2* code = s.code + size_t(slot) * s.code_stride;
+  const int len = s.code_len[slot];
+  const int64_t* kpool = s.kpool + size_t(slot) * s.stride;
+  const int C = s.C;
+  int64_t loss = 0;
+  uint32_t wrong = 0;
+  for (int tile = 0; tile < C; tile += 32 * K) {
+    int64_t acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0;
+    auto fetch = [&](uint32_t kind, uint32_t index, int k) -> int64_t {
+      switch (kind) {
+        case K_ACC: return acc[k];
+        case K_TEMP: return temps[(index * K + k) * 32 + lane];
+        case K_INPUT: {
+          const int c = tile + k * 32 + lane;
+          return c < C ? __ldg(&s.inputs[size_t(index) * C + c]) : 0;
+        }
+        default: return __ldg(&kpool[index]);
+      }
+    };
+    for (int ip = 0; ip < len; ++ip) {
+      const uint2 ins = __ldg(&code[ip]);
+      const uint32_t op = ins.x & 0xffu;
+      const bool swap = (ins.x >> 8) & 1u;
+      const uint32_t k1 = (ins.x >> 9) & 3u, k2 = (ins.x >> 11) & 3u, k3 = (ins.x >> 13) & 3u;
+      const uint32_t i1 = ins.y & 0xffffu, i2 = ins.y >> 16, i3 = ins.x >> 16;
+      switch (op) {
+        case A_MOV:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = fetch(k1, i1, k);
+          break;
+        case A_SPILL:
+#pragma unroll
+          for (int k = 0; k < K; ++k) temps[(i1 * K + k) * 32 + lane] = acc[k];
+          break;
+        case A_NEG:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = wrap_neg(acc[k]);
+          break;
+        case A_NOT:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] ^= 1;
+          break;
+        case A_ABS:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = acc[k] < 0 ? wrap_neg(acc[k]) : acc[k];
+          break;
+        case A_SELECT:
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int64_t c = fetch(k1, i1, k), t = fetch(k2, i2, k), e = fetch(k3, i3, k);
+            acc[k] = c ? t : e;
+          }
+          break;
+        default: {
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int64_t b = fetch(k1, i1, k);
+            const int64_t x = swap ? b : acc[k], y = swap ? acc[k] : b;
+            int64_t r;
+            switch (op) {
+              case A_ADD: r = wrap_add(x, y); break;
+              case A_SUB: r = wrap_sub(x, y); break;
+              case A_MUL: r = wrap_mul(x, y); break;
+              case A_LT: r = x < y; break;
+              case A_LE: r = x <= y; break;
+              case A_GT: r = x > y; break;
+              case A_GE: r = x >= y; break;
+              case A_EQ: r = x == y; break;
+              case A_NE: r = x != y; break;
+              case A_AND: r = x & y; break;
+              case A_OR: r = x | y; break;
+              case A_MIN: r = x < y ? x : y; break;
+              case A_MAX: r = x > y ? x : y; break;
+              case A_IDIV0: r = idiv0(x, y); break;
+              case A_IMOD0: r = imod0(x, y); break;
+              case A_TDIV0: r = tdiv0(x, y); break;
+              default: r = tmod0(x, y); break;
+            }
+            acc[k] = r;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int c = tile + k * 32 + lane;
+      if (c < C) loss += case_loss(s, s.slot_type, acc[k], __ldg(&s.expected[c]), wrong);
+    }
+  }
+  loss_out = loss;
+  wrong_out = wrong;
+  ops_out = uint64_t(len) * uint64_t(C);
+}
+
+// ------------------------------------------------------------ general VM
+// Exact stack interpreter of the reference bytecode (unit fuel: the phase
+// compiler leaves all-unit charge tables empty, phase_layout.hpp:481-486).
+// One thread per case.  Returns false on a runtime error or timeout.
+__device__ inline bool run_reference(const SearchDesc& s, const int32_t* code, int n, const int64_t* consts, int c,
+                                     int64_t& value, int& tag, uint64_t& steps) {
+  int64_t sv[64];
+  int8_t st[64];
+  int sp = 0, ip = 0, fuel = s.fuel;
+  while (ip < n) {
+    if (fuel <= 0) return false;  // Timeout
+    fuel -= 1;
+    ++steps;
+    const int32_t* x = code + 5 * ip++;
+    const int op = x[0], flags = x[1], a = x[2], b = x[3];
+    switch (op) {
+      case OP_PUSH_CONST:
+        if (sp >= 64) return false;
+        sv[sp] = consts[a];
+        st[sp++] = int8_t((flags & 4) ? GAGP_TAG_BOOL : GAGP_TAG_INT);
+        break;
+      case OP_LOAD:
+        if (sp >= 64 || a < 0 || a >= s.n_inputs) return false;
+        sv[sp] = s.inputs[size_t(a) * s.C + c];
+        st[sp++] = int8_t(s.local_types[a]);
+        break;
+      case OP_NEG: case OP_NOT: {
+        if (!sp) return false;
+        const int64_t v = sv[sp - 1];
+        const int t = st[sp - 1];
+        if (op == OP_NEG) { if (t != GAGP_TAG_INT) return false; sv[sp - 1] = wrap_neg(v); }
+        else { if (t != GAGP_TAG_BOOL) return false; sv[sp - 1] = v ^ 1; }
+        break;
+      }
+      case OP_ADD: case OP_SUB: case OP_MUL: case OP_DIV: case OP_MOD: {
+        if (sp < 2) return false;
+        const int64_t y = sv[--sp], xv = sv[--sp];
+        if (st[sp] != GAGP_TAG_INT || st[sp + 1] != GAGP_TAG_INT) return false;
+        if ((op == OP_DIV || op == OP_MOD) && y == 0) return false;  // ZeroDiv
+        if (op == OP_DIV) return false;                               // Float result: not admitted
+        sv[sp] = op == OP_ADD ? wrap_add(xv, y) : op == OP_SUB ? wrap_sub(xv, y) : op == OP_MUL ? wrap_mul(xv, y)
+                                                                                                 : py_mod(xv, y);
+        st[sp++] = int8_t(GAGP_TAG_INT);
+        break;
+      }
+      case OP_LT: case OP_LE: case OP_GT: case OP_GE: case OP_EQ: case OP_NE: {
+        if (sp < 2) return false;
+        const int64_t y = sv[--sp], xv = sv[--sp];
+        const int ty = st[sp + 1], tx = st[sp];
+        bool r;
+        if (op == OP_EQ || op == OP_NE) {
+          if (tx != ty || (tx != GAGP_TAG_INT && tx != GAGP_TAG_BOOL)) return false;
+          r = (xv == y) == (op == OP_EQ);
+        } else {
+          if (tx != GAGP_TAG_INT || ty != GAGP_TAG_INT) return false;
+          r = op == OP_LT ? xv < y : op == OP_LE ? xv <= y : op == OP_GT ? xv > y : xv >= y;
+        }
+        sv[sp] = r;
+        st[sp++] = int8_t(GAGP_TAG_BOOL);
+        break;
+      }
+      case OP_JMP:
+        if (a < 0 || a > n) return false;
+        ip = a;
+        break;
+      case OP_JMP_IF_FALSE: case OP_JMP_IF_TRUE: {
+        if (!sp || a < 0 || a > n) return false;
+        const int64_t v = sv[--sp];
+        if (st[sp] != GAGP_TAG_BOOL) return false;
+        if ((op == OP_JMP_IF_FALSE && !v) || (op == OP_JMP_IF_TRUE && v)) ip = a;
+        break;
+      }
+      case OP_CALL_BUILTIN: {
+        if (b < 0 || sp < b) return false;
+        for (int k = sp - b; k < sp; ++k) if (st[k] != GAGP_TAG_INT) return false;
+        int64_t r;
+        if (a == B_ABS) { if (b != 1) return false; r = sv[sp - 1] < 0 ? wrap_neg(sv[sp - 1]) : sv[sp - 1]; }
+        else {
+          if (b != 2) return false;
+          const int64_t p = sv[sp - 2], q = sv[sp - 1];
+          switch (a) {
+            case B_MIN: r = p < q ? p : q; break;
+            case B_MAX: r = p > q ? p : q; break;
+            case B_IDIV0: r = idiv0(p, q); break;
+            case B_IMOD0: r = imod0(p, q); break;
+            case B_TRUNC_DIV0: r = tdiv0(p, q); break;
+            case B_TRUNC_MOD0: r = tmod0(p, q); break;
+            default: return false;
+          }
+        }
+        sp -= b;
+        sv[sp] = r;
+        st[sp++] = int8_t(GAGP_TAG_INT);
+        break;
+      }
+      case OP_RETURN:
+        if (!sp) return false;
+        value = sv[sp - 1];
+        tag = st[sp - 1];
+        return true;
+      default:
+        return false;
+    }
+  }
+  return false;  // finished without return
+}
+
+}  // namespace gb

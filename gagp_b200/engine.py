@@ -1,0 +1,121 @@
+"""Python front end of the C ABI (include/gagp_b200.h) over ctypes.
+
+``Engine`` mirrors the reference's resident owner and search loop
+(``NativePhasePopulation`` + ``run_phase_population_steady``): admit a search,
+run it on the device, read its history and final ranked population.  The
+native library must be built (``gagp_b200.build``); there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .task import LoadedTask
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libgagp_b200.so")
+_lib = None
+
+
+class EngineError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load_library():
+    """Loads the in-tree engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EngineError(7, f"native engine library missing: {LIB_PATH} (run gagp_b200.build)")
+        lib = C.CDLL(LIB_PATH)
+        lib.gagp_b200_last_error.restype = C.c_char_p
+        lib.gagp_b200_version.restype = C.c_char_p
+        for name in ("gagp_b200_engine_create", "gagp_b200_search_bytes", "gagp_b200_search_create",
+                     "gagp_b200_search_destroy", "gagp_b200_search_run", "gagp_b200_batch_run",
+                     "gagp_b200_batch_step", "gagp_b200_search_result"):
+            getattr(lib, name).restype = C.c_int32
+        lib.gagp_b200_engine_destroy.restype = None
+        _lib = lib
+    return _lib
+
+
+def _check(status: int):
+    if status != 0:
+        raise EngineError(status, load_library().gagp_b200_last_error().decode())
+
+
+class Search:
+    """One admitted search held by an engine."""
+
+    def __init__(self, engine: "Engine", sid: int, task: LoadedTask, grammar: abi.GrammarBlob):
+        self.engine, self.id, self.task, self.grammar = engine, sid, task, grammar
+
+    def run(self):
+        self.engine.run(self)
+        return self
+
+    def result(self) -> dict:
+        t, s = self.task.tables, self.task.settings
+        res = abi.ResultBuffer(s.generations, s.population, t.max_nodes - t.fixed_nodes)
+        _check(load_library().gagp_b200_search_result(self.engine.handle, self.id, res.ref()))
+        return res.summary()
+
+    def close(self):
+        if self.id is not None and self.engine.handle:
+            _check(load_library().gagp_b200_search_destroy(self.engine.handle, self.id))
+            self.id = None
+
+
+class Engine:
+    """A device-resident GAGP engine on one GPU."""
+
+    def __init__(self, device: int = 0, arena_bytes: int = 0):
+        lib = load_library()
+        h = C.c_void_p()
+        _check(lib.gagp_b200_engine_create(C.c_int32(device), C.c_uint64(arena_bytes), C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            load_library().gagp_b200_engine_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def search_bytes(task: LoadedTask) -> int:
+        g = abi.GrammarBlob(task.tables)
+        cfg = task.settings.struct()
+        out = C.c_uint64(0)
+        _check(load_library().gagp_b200_search_bytes(g.ref(), task.cases.ref(), C.byref(cfg), C.byref(out)))
+        return int(out.value)
+
+    def admit(self, task: LoadedTask) -> Search:
+        g = abi.GrammarBlob(task.tables)
+        cfg = task.settings.struct()
+        sid = C.c_int32(0)
+        _check(load_library().gagp_b200_search_create(self.handle, g.ref(), task.cases.ref(), C.byref(cfg), None,
+                                                     C.byref(sid)))
+        return Search(self, sid.value, task, g)
+
+    def run(self, search: Search):
+        _check(load_library().gagp_b200_search_run(self.handle, C.c_int32(search.id)))
+
+    def run_batch(self, searches: Sequence[Search]):
+        ids = (C.c_int32 * len(searches))(*[s.id for s in searches])
+        _check(load_library().gagp_b200_batch_run(self.handle, ids, C.c_int32(len(searches))))
+
+    def step(self, searches: Sequence[Search]) -> List[bool]:
+        ids = (C.c_int32 * len(searches))(*[s.id for s in searches])
+        fin = (C.c_int32 * len(searches))()
+        _check(load_library().gagp_b200_batch_step(self.handle, ids, C.c_int32(len(searches)), fin))
+        return [bool(x) for x in fin]

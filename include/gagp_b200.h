@@ -222,23 +222,6 @@ gagp_status gagp_b200_batch_step(gagp_engine* engine, const int32_t* searches, i
 /* Copies a finished search's history and final ranked population out. */
 gagp_status gagp_b200_search_result(gagp_engine* engine, int32_t search, gagp_search_result* out);
 
-/* ---- owner interface: the reference's NativePhasePopulation calls, one at
- * a time, with the host running the loop (evolve.cpp:331-441).  The plain
- * one-search-per-launch path. */
-gagp_status gagp_b200_owner_evaluate(gagp_engine* engine, int32_t search, double* fitness,
-                                     uint32_t* wrong);
-gagp_status gagp_b200_owner_make_batch(gagp_engine* engine, int32_t search,
-                                       const double* selection_fitness, int32_t tournament_size,
-                                       double mutation_probability, uint64_t seed, int32_t* reuse);
-gagp_status gagp_b200_owner_evaluate_batch(gagp_engine* engine, int32_t search, const int32_t* reuse,
-                                           double* fitness, uint32_t* wrong);
-gagp_status gagp_b200_owner_node_counts(gagp_engine* engine, int32_t search, int32_t batch_rows,
-                                        uint32_t* nodes);
-gagp_status gagp_b200_owner_commit_batch(gagp_engine* engine, int32_t search,
-                                         const int32_t* placements, int32_t count);
-gagp_status gagp_b200_owner_export(gagp_engine* engine, int32_t search, int32_t batch_rows,
-                                   gagp_rows* out);
-
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,65 @@
+"""Device engine parity (GPU): whole searches through the C ABI are bit-identical
+to the reference CPU engine's golden runs and to the oracle, alone and batched."""
+import pytest
+
+from gagp_b200 import abi, workloads as W
+from oracle import oracle
+
+import golden_util as GU
+
+pytestmark = pytest.mark.gpu
+NAMES = GU.names()
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from gagp_b200 import build
+    from gagp_b200.engine import Engine
+    build.build()
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_search_matches_reference(engine, name):
+    fx = GU.fixture(name)
+    lt = GU.load_task(fx)
+    s = engine.admit(lt)
+    try:
+        s.run()
+        got = s.result()
+    finally:
+        s.close()
+    GU.compare_result(lt, got, fx["run"], name)
+
+
+def test_batched_searches_match_alone(engine):
+    """Searches advanced together in one launch sequence give each alone's result."""
+    names = [n for n in NAMES][:6]
+    tasks = [GU.load_task(GU.fixture(n)) for n in names]
+    searches = [engine.admit(t) for t in tasks]
+    try:
+        engine.run_batch(searches)
+        results = [s.result() for s in searches]
+    finally:
+        for s in searches:
+            s.close()
+    for n, t, r in zip(names, tasks, results):
+        GU.compare_result(t, r, GU.fixture(n)["run"], "batched " + n)
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_search_matches_oracle_fresh_seeds(engine, seed, tmp_path):
+    files = W.poly4(population=384, generations=6, seed=seed, cases=300)
+    from gagp_b200 import task as T
+    lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
+    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    s = engine.admit(lt)
+    s.run()
+    got = s.result()
+    s.close()
+    assert got["history"] == want["history"]
+    assert got["final"] == want["final"]
+    assert got["evaluated_programs"] == want["evaluated_programs"]
+    assert got["reused_programs"] == want["reused_programs"]
