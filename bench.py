@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark of the resident GAGP search path on B200.
+
+Metric: VM program-case evaluations per second (whole job), on the
+large scalar-regression search: a random degree<=4 integer polynomial, 256
+train cases x ~ U{-100..100}, grammar x, constants -2..3, add/sub/mul/idiv0/
+imod0 and if(lt(E,E),E,E), max 64 nodes, population 16384, 128 generations,
+absolute error (cap 1000), gagp's default resident search (steady state,
+batch = population).  A step is one steady-state round: one batch of 16384
+children varied, lowered, evaluated on all cases and placed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Own arm: `value` is program-case evaluations per second of device time over K
+rounds (CUDA events on the engine stream, L2 flushed before every round,
+outside the timed region); `e2e` runs a whole search through the C ABI from
+host buffers (admission upload, device loop, result download).  Reference arm
+(--impl reference): the reference's own CPU engine compiled from its sources
+(oracle/_ref/ref_driver), one process per host core, each step a bounded
+sample search.  Several GPUs run independent replica searches (one per rank,
+seed + rank): the path has no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from gagp_b200 import workloads as W  # noqa: E402
+from gagp_b200 import task as T  # noqa: E402
+
+METRIC = "VM program-case evals/s"
+UNIT = "program-case evals/s"
+WORKLOAD = dict(population=16384, generations=128, cases=256, max_nodes=64)
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def make_task(seed: int, directory: str, **overrides) -> str:
+    cfg = dict(WORKLOAD)
+    cfg.update(overrides)
+    files = W.poly4(population=cfg["population"], generations=cfg["generations"], seed=seed, cases=cfg["cases"],
+                    max_nodes=cfg["max_nodes"])
+    return files.write(directory)
+
+
+def config_block(world: int, seed: int) -> dict:
+    return {"workload": "poly4 scalar regression (large): P=16384, G=128, C=256, max_nodes=64, seed=%d" % seed,
+            "population": WORKLOAD["population"], "generations": WORKLOAD["generations"],
+            "cases": WORKLOAD["cases"], "max_nodes": WORKLOAD["max_nodes"], "batch": WORKLOAD["population"],
+            "parallelism": "replicas%d" % world if world > 1 else "single-gpu",
+            "l2": "256 MiB buffer written before every timed round (outside the timed region)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for name, flag in zip(names, f[5:9]):
+                    if flag.lower().startswith("active"):
+                        reasons.add(name)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks() -> dict:
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return {"hbm_gbs": p["hbm_gbs"], "source": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def reference_sample(task_path: str, search_path: str, generations: int) -> dict:
+    """One reference CPU-engine search (single thread), timed by its own clock."""
+    driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    out = subprocess.run([driver, "run", task_path, "--search", search_path, "--generations", str(generations)],
+                         check=True, capture_output=True, text=True).stdout
+    d = json.loads(out)
+    return {"program_cases": d["program_cases"], "ms": d["time_ms"]}
+
+
+def cpu_baseline(directory: str) -> dict:
+    """The reference CPU engine on a bounded sample of the workload (1 thread)."""
+    driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if os.path.exists(driver):
+        r = reference_sample(os.path.join(directory, "task.json"), os.path.join(directory, "search.json"), 4)
+        return {"value": r["program_cases"] / (r["ms"] / 1000.0), "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "reference CPU engine (HostPhasePopulation, single-threaded), same task and seed, "
+                          "population 16384, 4 generations + initial evaluation (%d program-cases in %.1f s)" % (
+                              r["program_cases"], r["ms"] / 1000.0)}
+    sys.path.insert(0, ROOT)
+    from oracle import oracle  # noqa: WPS433 (checker only)
+    from gagp_b200 import abi
+    lt = T.load(os.path.join(directory, "task.json"), os.path.join(directory, "search.json"), generations=2)
+    t0 = time.perf_counter()
+    res = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    dt = time.perf_counter() - t0
+    return {"value": res["program_cases"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "C oracle restatement, population 16384, 2 generations + initial evaluation"}
+
+
+def run_reference_arm(args, rank: int, world: int):
+    """--impl reference: the reference CPU engine on all host cores."""
+    if rank != 0:
+        return
+    driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    seed = 0
+    if not os.path.exists(driver):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver was not built"}))
+        return
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        make_task(seed, d)
+        tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+        sample_generations = 2
+        make_task(seed, d, population=2048)
+
+        def step():
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen([driver, "run", tp, "--search", sp, "--generations", str(sample_generations),
+                                       "--seed", str(seed + i)], stdout=subprocess.PIPE, text=True)
+                     for i in range(cores)]
+            total = 0
+            for p in procs:
+                out, _ = p.communicate()
+                if p.returncode:
+                    raise RuntimeError("reference run failed")
+                total += json.loads(out)["program_cases"]
+            return total, time.perf_counter() - t0
+
+        for _ in range(args.warmup):
+            step()
+        cases, secs = 0, 0.0
+        for _ in range(args.steps):
+            c, s = step()
+            cases += c
+            secs += s
+    value = cases / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic", "config": config_block(1, seed),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": "per step: %d concurrent single-threaded reference CPU-engine searches "
+                                       "(population 2048, initial evaluation + %d generations, seeds 0..%d)" % (
+                                           cores, sample_generations, cores - 1)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def roofline_entry(stats: dict, counters: dict, peak: dict) -> dict:
+    """Roofline of the kernel with the largest device time."""
+    top = max(stats.items(), key=lambda kv: kv[1]["ms"])[0]
+    ms = stats[top]["ms"] / max(1, stats[top]["launches"])
+    entry = {"kernel": top, "avg_launch_ms": ms, "share": stats[top]["ms"] / max(1e-9, sum(v["ms"] for v in stats.values()))}
+    return entry
+
+
+def run_own_arm(args, rank: int, world: int, local: int):
+    import ctypes  # noqa: F401
+    from gagp_b200 import build
+    from gagp_b200.engine import Engine
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    build.build()
+    seed = rank
+    line = {}
+    with tempfile.TemporaryDirectory() as d:
+        make_task(seed, d)
+        tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+        with Engine(local if world > 1 else 0) as eng:
+            # e2e: a whole search through the C ABI from host buffers
+            lt = T.load(tp, sp)
+            t0 = time.perf_counter()
+            s = eng.admit(lt)
+            s.run()
+            res = s.result()
+            e2e_secs = time.perf_counter() - t0
+            s.close()
+            h2d = lt.cases.inputs.nbytes + lt.cases.expected.nbytes + len(lt.tables.minimum) * 4 + \
+                len(lt.tables.expressions) * 80
+            d2h = (WORKLOAD["generations"] * 3 + WORKLOAD["population"] * 4) * 8 + \
+                (WORKLOAD["generations"] + WORKLOAD["population"]) * (lt.tables.max_nodes - lt.tables.fixed_nodes) * 12
+            e2e = {"value": res["program_cases"] / e2e_secs, "unit": UNIT,
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": e2e_secs,
+                   "step": "one whole search (admission + %d rounds + result)" % WORKLOAD["generations"]}
+            # device-timed rounds
+            lt = T.load(tp, sp)
+            s = eng.admit(lt)
+            eng.start([s])
+            eng.advance([s], args.warmup, flush_l2=True)
+            before = eng.counters(s)
+            if dist:
+                import torch
+                dist.barrier()
+                torch.cuda.synchronize()
+            eng.profile(True)
+            with ClockSampler(local) as clocks:
+                ms = eng.advance([s], args.steps, flush_l2=True)
+            stats = eng.kernel_stats()
+            eng.profile(False)
+            after = eng.counters(s)
+            s.close()
+    cases = after["program_cases"] - before["program_cases"]
+    secs = ms / 1000.0
+    if dist:
+        import torch
+        t = torch.tensor([secs, float(cases)], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        tot = t.clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        secs, cases = float(mx[0]), float(tot[1])
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    launches = sum(v["launches"] for v in stats.values())
+    line = {"metric": METRIC, "value": cases / secs, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": config_block(world, seed), "e2e": e2e, "gpu_launches": launches,
+            "kernels": {k: {"ms_per_step": v["ms"] / args.steps, "launches": v["launches"]} for k, v in stats.items()},
+            "roofline": roofline_entry(stats, after, peaks()), "clocks": clocks.summary(),
+            "counters": {"program_cases": cases, "evaluated_programs": after["evaluated_programs"] - before["evaluated_programs"],
+                         "reused_programs": after["reused_programs"] - before["reused_programs"],
+                         "vm_ops": after["vm_ops"] - before["vm_ops"]}}
+    if world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as d:
+            make_task(seed, d)
+            line["cpu_baseline"] = cpu_baseline(d)
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.steps + args.warmup > WORKLOAD["generations"]:
+        raise SystemExit("steps + warmup must not exceed the search's %d rounds" % WORKLOAD["generations"])
+    rank, world, local = rank_info()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_own_arm(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

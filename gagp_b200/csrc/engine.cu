@@ -80,9 +80,64 @@ struct gagp_engine {
   int32_t* d_batch_off = nullptr;
   size_t batch_off_capacity = 0;
   bool poisoned = false;
+  // per-kernel CUDA-event timing (bench/profiling)
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;
+  size_t event_next = 0;
+  struct Pending { int kernel; cudaEvent_t start, stop; };
+  std::vector<Pending> pending;
+  double kernel_ms[16] = {};
+  long long kernel_launches[16] = {};
+  void* flush_buffer = nullptr;
+  size_t flush_bytes = 0;
 };
 
 namespace {
+
+enum KernelId {
+  KN_INIT, KN_LOWER, KN_VM_FAST, KN_VM_GENERAL, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
+  KN_COMMIT, KN_COUNT
+};
+const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast", "k_vm_general",
+                                            "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
+                                            "k_place", "k_commit"};
+
+cudaEvent_t take_event(gagp_engine* e) {
+  if (e->event_next == e->event_pool.size()) {
+    cudaEvent_t ev;
+    cudaEventCreate(&ev);
+    e->event_pool.push_back(ev);
+  }
+  return e->event_pool[e->event_next++];
+}
+// Brackets one kernel launch with events on the engine stream when profiling.
+struct Timed {
+  gagp_engine* e;
+  int kernel;
+  cudaEvent_t stop = nullptr;
+  Timed(gagp_engine* engine, int k) : e(engine), kernel(k) {
+    if (!e->profiling) return;
+    cudaEvent_t start = take_event(e);
+    stop = take_event(e);
+    cudaEventRecord(start, e->stream);
+    e->pending.push_back({kernel, start, stop});
+  }
+  ~Timed() {
+    if (stop) cudaEventRecord(stop, e->stream);
+  }
+};
+// Adds the elapsed times of completed launches (after a stream sync).
+void harvest(gagp_engine* e) {
+  for (const auto& p : e->pending) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+      e->kernel_ms[p.kernel] += ms;
+      e->kernel_launches[p.kernel] += 1;
+    }
+  }
+  e->pending.clear();
+  e->event_next = 0;
+}
 
 gagp_status ensure_lists(gagp_engine* e, size_t items) {
   if (items <= e->list_capacity) return GAGP_OK;
@@ -271,6 +326,8 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   cudaFree(e->d_counts);
   cudaFree(e->d_batch_desc);
   cudaFree(e->d_batch_off);
+  cudaFree(e->flush_buffer);
+  for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
   cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -496,33 +553,40 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
   const int warps = 8;
   const int temp_stride = gb::kMaxTemps * v.max_lanes * 32;
   const size_t smem = size_t(warps) * temp_stride * sizeof(int64_t);
-  const int blocks = e->sm_count * std::max(1, int((e->max_smem - 1024) / std::max<size_t>(smem, 1)) > 2 ? 2 : 1);
-  gb::k_vm_fast<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, mode, e->d_fast, e->d_counts, temp_stride);
-  gb::k_vm_general<<<e->sm_count * 4, 128, 0, e->stream>>>(v.d_desc, mode, e->d_general, e->d_counts + 1);
+  const int per_sm = std::max(1, std::min(4, int((e->max_smem - 1024) / std::max<size_t>(smem, 1))));
+  const int blocks = e->sm_count * per_sm;
+  {
+    Timed t(e, KN_VM_FAST);
+    gb::k_vm_fast<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, mode, e->d_fast, e->d_counts, temp_stride);
+  }
+  {
+    Timed t(e, KN_VM_GENERAL);
+    gb::k_vm_general<<<e->sm_count * 4, 128, 0, e->stream>>>(v.d_desc, mode, e->d_general, e->d_counts + 1);
+  }
   return GAGP_OK;
 }
 
 gagp_status launch_start(gagp_engine* e, const BatchView& v) {
-  gb::k_init_population<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+  { Timed t(e, KN_INIT); gb::k_init_population<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
-  gb::k_lower<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n, 0, e->d_fast,
-                                                                        e->d_general, e->d_counts);
+  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n, 0, e->d_fast,
+                                                                        e->d_general, e->d_counts); }
   launch_vm(e, v, 0);
-  gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
-  gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n);
+  { Timed t(e, KN_KEYS); gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
+  { Timed t(e, KN_START); gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
 }
 
 gagp_status launch_round(gagp_engine* e, const BatchView& v) {
-  gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1);
-  gb::k_vary<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n);
+  { Timed t(e, KN_RECORD); gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1); }
+  { Timed t(e, KN_VARY); gb::k_vary<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
-  gb::k_lower<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
-                                                                         e->d_general, e->d_counts);
+  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
+                                                                         e->d_general, e->d_counts); }
   launch_vm(e, v, 1);
-  gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n);
-  gb::k_place<<<v.n, 256, size_t(v.max_P) * sizeof(uint64_t), e->stream>>>(v.d_desc, v.n);
-  gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+  { Timed t(e, KN_CHILD); gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
+  { Timed t(e, KN_PLACE); gb::k_place<<<v.n, 256, size_t(v.max_P) * sizeof(uint64_t), e->stream>>>(v.d_desc, v.n); }
+  { Timed t(e, KN_COMMIT); gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
 }
 
@@ -537,6 +601,7 @@ gagp_status collect(gagp_engine* e, const std::vector<int32_t>& ids, std::vector
 
 gagp_status check_errors(gagp_engine* e, const std::vector<Search*>& list) {
   CUDA_TRY(cudaStreamSynchronize(e->stream));
+  harvest(e);
   for (Search* s : list) {
     int32_t round[4];
     CUDA_TRY(cudaMemcpy(round, s->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
@@ -615,6 +680,105 @@ gagp_status gagp_b200_batch_step(gagp_engine* e, const int32_t* ids, int32_t cou
       CUDA_TRY(cudaMemcpy(round, list[i]->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
       finished[i] = round[2];
     }
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_batch_start(gagp_engine* e, const int32_t* ids, int32_t count) {
+  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<Search*> list, fresh;
+  gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
+  if (st != GAGP_OK) return st;
+  for (Search* s : list) if (!s->started) fresh.push_back(s);
+  if (fresh.empty()) return GAGP_OK;
+  BatchView v;
+  if ((st = make_batch_view(e, fresh, &v)) != GAGP_OK) return st;
+  if ((st = launch_start(e, v)) != GAGP_OK) return st;
+  for (Search* s : fresh) s->started = true;
+  return check_errors(e, fresh);
+}
+
+gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t count, int32_t rounds,
+                                    int32_t flush_l2, double* device_ms) {
+  if (!e || (!ids && count) || rounds < 0) return fail(GAGP_INVALID_ARGUMENT, "bad argument");
+  CUDA_TRY(cudaSetDevice(e->device));
+  std::vector<Search*> list;
+  gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
+  if (st != GAGP_OK || list.empty()) return st;
+  for (Search* s : list)
+    if (!s->started) return fail(GAGP_INVALID_ARGUMENT, "start the searches first (gagp_b200_batch_start)");
+  BatchView v;
+  if ((st = make_batch_view(e, list, &v)) != GAGP_OK) return st;
+  if (flush_l2 && !e->flush_buffer) {
+    e->flush_bytes = size_t(256) << 20;  // twice the B200's 126 MB L2
+    CUDA_TRY(cudaMalloc(&e->flush_buffer, e->flush_bytes));
+  }
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks;
+  for (int r = 0; r < rounds; ++r) {
+    if (flush_l2) CUDA_TRY(cudaMemsetAsync(e->flush_buffer, r & 0xff, e->flush_bytes, e->stream));
+    cudaEvent_t a, b;
+    CUDA_TRY(cudaEventCreate(&a));
+    CUDA_TRY(cudaEventCreate(&b));
+    CUDA_TRY(cudaEventRecord(a, e->stream));
+    if ((st = launch_round(e, v)) != GAGP_OK) return st;
+    CUDA_TRY(cudaEventRecord(b, e->stream));
+    marks.push_back({a, b});
+  }
+  st = check_errors(e, list);
+  double total = 0;
+  for (auto& m : marks) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, m.first, m.second);
+    total += ms;
+    cudaEventDestroy(m.first);
+    cudaEventDestroy(m.second);
+  }
+  if (device_ms) *device_ms = total;
+  return st;
+}
+
+gagp_status gagp_b200_search_counters(gagp_engine* e, int32_t id, uint64_t* out4) {
+  if (!e || !out4) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  auto it = e->searches.find(id);
+  if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  CUDA_TRY(cudaMemcpy(out4, it->second->desc.counters, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_engine_profile(gagp_engine* e, int32_t enable) {
+  if (!e) return fail(GAGP_INVALID_ARGUMENT, "null engine");
+  e->profiling = enable != 0;
+  std::fill(std::begin(e->kernel_ms), std::end(e->kernel_ms), 0.0);
+  std::fill(std::begin(e->kernel_launches), std::end(e->kernel_launches), 0LL);
+  e->pending.clear();
+  e->event_next = 0;
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_engine_kernel_stats(gagp_engine* e, int32_t kernel, const char** name, double* total_ms,
+                                          int64_t* launches) {
+  if (!e || kernel < 0 || kernel >= KN_COUNT) return fail(GAGP_INVALID_ARGUMENT, "kernel index");
+  if (name) *name = kKernelNames[kernel];
+  if (total_ms) *total_ms = e->kernel_ms[kernel];
+  if (launches) *launches = e->kernel_launches[kernel];
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_search_progress(gagp_engine* e, int32_t id, int32_t* rounds_done, int32_t* total_rounds,
+                                      int32_t* finished) {
+  if (!e) return fail(GAGP_INVALID_ARGUMENT, "null engine");
+  auto it = e->searches.find(id);
+  if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  int32_t round[4];
+  CUDA_TRY(cudaMemcpy(round, it->second->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
+  if (rounds_done) *rounds_done = round[0];
+  if (total_rounds) *total_rounds = it->second->total_rounds;
+  if (finished) *finished = round[2];
+  if (round[3]) return fail(GAGP_DEVICE_ERROR, "search failed on the device (code " + std::to_string(round[3]) + ")");
   return GAGP_OK;
 }
 

@@ -37,7 +37,9 @@ def load_library():
         lib.gagp_b200_version.restype = C.c_char_p
         for name in ("gagp_b200_engine_create", "gagp_b200_search_bytes", "gagp_b200_search_create",
                      "gagp_b200_search_destroy", "gagp_b200_search_run", "gagp_b200_batch_run",
-                     "gagp_b200_batch_step", "gagp_b200_search_result"):
+                     "gagp_b200_batch_step", "gagp_b200_search_result", "gagp_b200_batch_start",
+                     "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters",
+                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats"):
             getattr(lib, name).restype = C.c_int32
         lib.gagp_b200_engine_destroy.restype = None
         _lib = lib
@@ -119,3 +121,41 @@ class Engine:
         fin = (C.c_int32 * len(searches))()
         _check(load_library().gagp_b200_batch_step(self.handle, ids, C.c_int32(len(searches)), fin))
         return [bool(x) for x in fin]
+
+    def start(self, searches: Sequence[Search]):
+        ids = (C.c_int32 * len(searches))(*[s.id for s in searches])
+        _check(load_library().gagp_b200_batch_start(self.handle, ids, C.c_int32(len(searches))))
+
+    def advance(self, searches: Sequence[Search], rounds: int, flush_l2: bool = False) -> float:
+        """Runs ``rounds`` rounds of the started searches; returns device milliseconds."""
+        ids = (C.c_int32 * len(searches))(*[s.id for s in searches])
+        ms = C.c_double(0)
+        _check(load_library().gagp_b200_batch_advance(self.handle, ids, C.c_int32(len(searches)), C.c_int32(rounds),
+                                                      C.c_int32(int(flush_l2)), C.byref(ms)))
+        return ms.value
+
+    def counters(self, search: Search) -> dict:
+        out = (C.c_uint64 * 4)()
+        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out))
+        return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2], "vm_ops": out[3]}
+
+    def progress(self, search: Search) -> tuple:
+        done, total, fin = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(load_library().gagp_b200_search_progress(self.handle, C.c_int32(search.id), C.byref(done),
+                                                        C.byref(total), C.byref(fin)))
+        return done.value, total.value, bool(fin.value)
+
+    def profile(self, enable: bool = True):
+        _check(load_library().gagp_b200_engine_profile(self.handle, C.c_int32(int(enable))))
+
+    def kernel_stats(self) -> Dict[str, dict]:
+        lib = load_library()
+        out = {}
+        i = 0
+        while True:
+            name, ms, n = C.c_char_p(), C.c_double(), C.c_int64()
+            if lib.gagp_b200_engine_kernel_stats(self.handle, C.c_int32(i), C.byref(name), C.byref(ms), C.byref(n)):
+                break
+            out[name.value.decode()] = {"ms": ms.value, "launches": n.value}
+            i += 1
+        return out

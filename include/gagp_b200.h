@@ -219,6 +219,33 @@ gagp_status gagp_b200_batch_run(gagp_engine* engine, const int32_t* searches, in
 gagp_status gagp_b200_batch_step(gagp_engine* engine, const int32_t* searches, int32_t count,
                                  int32_t* finished);
 
+/* Runs start-up (initial population, initial evaluation, run generator) of
+ * every listed search that has not started; synchronous. */
+gagp_status gagp_b200_batch_start(gagp_engine* engine, const int32_t* searches, int32_t count);
+
+/* Enqueues `rounds` steady-state rounds of the listed (started) searches and
+ * waits.  *device_ms: summed CUDA-event time of the rounds on the engine
+ * stream; with flush_l2 a 256 MiB buffer is written before each round,
+ * outside the timed region, so no round starts with a warm L2. */
+gagp_status gagp_b200_batch_advance(gagp_engine* engine, const int32_t* searches, int32_t count,
+                                    int32_t rounds, int32_t flush_l2, double* device_ms);
+
+/* Rounds done, total rounds and completion flag of a search (synchronous). */
+gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32_t* rounds_done,
+                                      int32_t* total_rounds, int32_t* finished);
+
+/* Work counters of a search so far: [0] program evaluations, [1] children
+ * that reused a member's result, [2] evaluated (program, case) pairs,
+ * [3] VM instructions executed over all cases (synchronous). */
+gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out4);
+
+/* Per-kernel CUDA-event timing: enable (resets) or disable, then read the
+ * accumulated time and launch count of kernel index 0.. (INVALID_ARGUMENT
+ * past the last kernel). */
+gagp_status gagp_b200_engine_profile(gagp_engine* engine, int32_t enable);
+gagp_status gagp_b200_engine_kernel_stats(gagp_engine* engine, int32_t kernel, const char** name,
+                                          double* total_ms, int64_t* launches);
+
 /* Copies a finished search's history and final ranked population out. */
 gagp_status gagp_b200_search_result(gagp_engine* engine, int32_t search, gagp_search_result* out);
 

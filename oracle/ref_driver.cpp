@@ -23,6 +23,7 @@
 #include <cinttypes>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <memory>
 #include <string>
 #include <vector>
@@ -256,8 +257,11 @@ int run_search(const Args& a) {
   const auto case_set = evo::prepare_case_set(cases);
   const auto result = evo::evolve_population(cases, cfg, nullptr);
   rp::NativePhaseGrammarProfiles profiles(grammar, case_set.input_names);
-  std::printf("{\"declined\":%s,\"time_ms\":%s,\"history\":[", quote(result.resident_declined).c_str(),
-              num(result.timing.total_ms).c_str());
+  const auto& totals = result.timing.evaluation_totals;
+  std::printf("{\"declined\":%s,\"time_ms\":%s,\"init_ms\":%s,\"program_cases\":%llu,\"reused_programs\":%llu,\"history\":[",
+              quote(result.resident_declined).c_str(), num(result.timing.total_ms).c_str(),
+              num(result.timing.init_population_ms).c_str(), (unsigned long long)totals.program_cases,
+              (unsigned long long)totals.fitness_reused_programs);
   for (std::size_t i = 0; i < result.history_best.size(); ++i) {
     const auto& h = result.history_best[i];
     std::printf("%s{\"best_fitness\":%s,\"mean_fitness\":\"%s\",\"best_wrong\":%d,\"best_nodes\":%zu,\"text\":%s}",
@@ -285,6 +289,10 @@ int run_search(const Args& a) {
 }  // namespace
 
 int main(int argc, char** argv) {
+  if (argc >= 2 && std::string(argv[1]) == "--nproc") {
+    std::printf("%u\n", std::thread::hardware_concurrency());
+    return 0;
+  }
   if (argc < 3) {
     std::fprintf(stderr, "usage: ref_driver tables|run TASK.json [--search F] [--population N] [--generations G] [--seed S]\n");
     return 2;
