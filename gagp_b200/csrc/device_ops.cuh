@@ -1,7 +1,20 @@
-// Device building blocks of the resident search: the grammar RNG, phase-row
-// primitives, typed subtree generation and splicing over the compact row
-// layout of search_state.h.  Each function names the reference function whose
-// semantics it reproduces exactly (paths relative to the reference root).
+// Device building blocks of the resident search: the grammar RNG, the
+// self-describing node word, typed subtree generation and warp-cooperative
+// row primitives.  Each function names the reference function whose results
+// it reproduces exactly (paths relative to the reference root).
+//
+// Node word (64 bits), B200-first layout of one phase-tree node:
+//   [0,16)  construction expression (the reference's origin)
+//   [16,32) 1 + the reference expression that opened the node's grammar
+//           site (0: no site) -- the whole PhaseGeneSite is a function of it
+//   [32,40) depth (root = 1), [40,48) site depth: grammar sites on the path
+//           from the root down to and including this node
+//   [48,52) arity, [52] constant, [53,64) crossover class of the site
+//           (nonterminal and scope; kNoClass: none or variation disabled)
+// Storing depth and site depth turns the reference's sequential stack walks
+// (phase_node_depth, phase_site_depth, phase_tree_depth) into lookups and
+// warp max-reductions: a splice shifts the donor subtree's depths by the
+// difference at the splice point and leaves every other node's unchanged.
 #pragma once
 #include <cstdint>
 
@@ -14,6 +27,8 @@ enum { EK_OPERATION = 0, EK_CONSTANT = 1, EK_BOUND = 2, EK_REFERENCE = 3, EK_INP
 enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5 };
 enum { ST_OK = 0, ST_INVALID = 1, ST_UNSUPPORTED = 2, ST_CAPACITY = 3 };
 constexpr int kFixedSite = 1 << 30;
+constexpr uint32_t kNoClass = 0x7ffu;
+constexpr unsigned kFull = 0xffffffffu;
 
 // ---------------------------------------------------------------- RNG
 // SplitMix64 stream with rejection-sampled bounds
@@ -53,184 +68,43 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
   return x ^ (x >> 31);
 }
 
-// ---------------------------------------------------------------- rows
-__device__ __forceinline__ int origin_of(uint32_t w) { return int(w & 0xffffu); }
-__device__ __forceinline__ int entry_of(uint32_t w) { return int(w >> 16) - 1; }
-__device__ __forceinline__ uint32_t make_word(int origin, int entry) {
-  return uint32_t(origin) | (uint32_t(entry + 1) << 16);
+// ---------------------------------------------------------------- node words
+__device__ __forceinline__ int w_origin(uint64_t w) { return int(w & 0xffffu); }
+__device__ __forceinline__ int w_entry(uint64_t w) { return int((w >> 16) & 0xffffu) - 1; }
+__device__ __forceinline__ int w_depth(uint64_t w) { return int((w >> 32) & 0xffu); }
+__device__ __forceinline__ int w_sval(uint64_t w) { return int((w >> 40) & 0xffu); }
+__device__ __forceinline__ int w_arity(uint64_t w) { return int((w >> 48) & 0xfu); }
+__device__ __forceinline__ bool w_const(uint64_t w) { return (w >> 52) & 1u; }
+__device__ __forceinline__ uint32_t w_class(uint64_t w) { return uint32_t(w >> 53); }
+__device__ __forceinline__ bool w_site(uint64_t w) { return ((w >> 16) & 0xffffu) != 0; }
+__device__ __forceinline__ uint64_t w_make(int origin, int entry, int depth, int sval, int arity, bool constant,
+                                           uint32_t cls) {
+  return uint64_t(uint32_t(origin) & 0xffffu) | (uint64_t(uint32_t(entry + 1) & 0xffffu) << 16) |
+         (uint64_t(uint32_t(depth) & 0xffu) << 32) | (uint64_t(uint32_t(sval) & 0xffu) << 40) |
+         (uint64_t(uint32_t(arity) & 0xfu) << 48) | (uint64_t(constant) << 52) | (uint64_t(cls & 0x7ffu) << 53);
+}
+// Shifts depth and site depth (a donor subtree moved under another parent).
+__device__ __forceinline__ uint64_t w_shift(uint64_t w, int ddepth, int dsval) {
+  const int d = w_depth(w) + ddepth, v = w_sval(w) + dsval;
+  return (w & ~(0xffffULL << 32)) | (uint64_t(uint32_t(d) & 0xffu) << 32) | (uint64_t(uint32_t(v) & 0xffu) << 40);
+}
+// Replaces the site (entry and class) of a word by another word's site.
+__device__ __forceinline__ uint64_t w_with_site(uint64_t w, uint64_t site_from) {
+  const uint64_t mask = (0xffffULL << 16) | (0x7ffULL << 53);
+  return (w & ~mask) | (site_from & mask);
 }
 __device__ __forceinline__ int len_nodes(int32_t l) { return l & 0xffff; }
 __device__ __forceinline__ int len_consts(int32_t l) { return (l >> 16) & 0xffff; }
 __device__ __forceinline__ int32_t make_len(int n, int c) { return n | (c << 16); }
 
-struct Row {
-  const uint32_t* node;
-  const int64_t* cval;
-  int n, nc;
-};
-struct MRow {
-  uint32_t* node;
-  int64_t* cval;
-};
-
-__device__ __forceinline__ Row row_of(const uint32_t* node, const int64_t* cval, const int32_t* len, int stride, int r) {
-  const int32_t l = len[r];
-  return Row{node + size_t(r) * stride, cval + size_t(r) * stride, len_nodes(l), len_consts(l)};
-}
-__device__ __forceinline__ MRow mrow_of(uint32_t* node, int64_t* cval, int stride, int r) {
-  return MRow{node + size_t(r) * stride, cval + size_t(r) * stride};
-}
-
-__device__ __forceinline__ int arity_of(const SearchDesc& s, uint32_t w) { return s.info[origin_of(w)].arity; }
-__device__ __forceinline__ bool is_constant(const SearchDesc& s, uint32_t w) {
-  return s.info[origin_of(w)].node_kind == TK_CONSTANT;
-}
-// PhaseGeneSite fields as functions of the site's entry expression.
-__device__ __forceinline__ int site_nt(const SearchDesc& s, int entry) { return entry < 0 ? -1 : s.info[entry].site_nt; }
-__device__ __forceinline__ int site_scope(const SearchDesc& s, int entry) {
-  if (entry < 0) return 0;
-  const gagp_expression& e = s.ex[entry];
-  const bool fixed = s.nts[e.target].fixed != 0;
-  return e.scope_count | (fixed ? kFixedSite : 0);
-}
-
-__device__ inline void copy_row(const Row& from, MRow to) {
-  for (int i = 0; i < from.n; ++i) to.node[i] = from.node[i];
-  for (int i = 0; i < from.nc; ++i) to.cval[i] = from.cval[i];
-}
-
-// phase_subtree_end (device/phase_variation.cuh:81-91)
-__device__ inline int subtree_end(const SearchDesc& s, const Row& t, int start) {
-  if (start < 0 || start >= t.n || t.n > kCapacity) return -1;
-  int pending = 1;
-  for (int i = start; i < t.n; ++i) {
-    const int a = arity_of(s, t.node[i]);
-    if (a < 0 || a > 8) return -1;
-    pending += a - 1;
-    if (!pending) return i + 1;
-  }
-  return -1;
-}
-// phase_node_depth (device/phase_variation.cuh:92-105)
-__device__ inline int node_depth(const SearchDesc& s, const Row& t, int position) {
-  if (position < 0 || position >= t.n || t.n > kCapacity) return -1;
-  int pending[64];
-  int depth = 1;
-  pending[0] = 1;
-  for (int i = 0; i <= position; ++i) {
-    while (depth && !pending[depth - 1]) --depth;
-    if (!depth) return -1;
-    if (i == position) return depth;
-    --pending[depth - 1];
-    const int a = arity_of(s, t.node[i]);
-    if (a < 0 || a > 8) return -1;
-    if (a) {
-      if (depth == 64) return -1;
-      pending[depth++] = a;
-    }
-  }
-  return -1;
-}
-// phase_site_depth (device/phase_variation.cuh:127-142); position < 0 gives
-// the height, otherwise the incoming depth at `position`.
-__device__ inline int site_depth_of(const SearchDesc& s, const uint32_t* node, int count, int position) {
-  if (count <= 0 || count > kCapacity || position >= count) return -1;
-  int pending[64], incoming[64];
-  int depth = 1, maximum = 0;
-  pending[0] = 1;
-  incoming[0] = 0;
-  for (int i = 0; i < count; ++i) {
-    while (depth && !pending[depth - 1]) --depth;
-    if (!depth) return -1;
-    if (i == position) return incoming[depth - 1];
-    const int a = arity_of(s, node[i]);
-    if (a < 0 || a > 8) return -1;
-    const int value = incoming[depth - 1] + (entry_of(node[i]) >= 0 ? 1 : 0);
-    maximum = value > maximum ? value : maximum;
-    --pending[depth - 1];
-    if (a) {
-      if (depth == 64) return -1;
-      pending[depth] = a;
-      incoming[depth++] = value;
-    }
-  }
-  while (depth && !pending[depth - 1]) --depth;
-  return depth ? -1 : maximum;
+// Crossover class of sites opened by reference expression `entry`.
+__device__ __forceinline__ uint32_t class_of_entry(const SearchDesc& s, int entry) {
+  return entry < 0 ? kNoClass : uint32_t(s.info[entry].site_class);
 }
 
 struct GenResult {
   int status, nodes, constants;
 };
-
-// splice_phase_tree<FusedDepth=true> (device/phase_variation.cuh:147-207).
-// Output constants are base[..dest) ++ donor subtree ++ base[end..), which is
-// the prefix renumbering the reference applies node by node.
-__device__ inline GenResult splice(const SearchDesc& s, const Row& base, int dest, const Row& donor, int src,
-                                   MRow out, int max_depth, int site_limit) {
-  GenResult r{ST_INVALID, 0, 0};
-  if (max_depth <= 0 || max_depth > 64 || base.n <= 0 || base.n > kCapacity || donor.n <= 0 ||
-      donor.n > kCapacity || base.nc < 0 || base.nc > base.n || donor.nc < 0 || donor.nc > donor.n || dest < 0 ||
-      dest >= base.n || src < 0 || src >= donor.n)
-    return r;
-  const int ea = entry_of(base.node[dest]), eb = entry_of(donor.node[src]);
-  const int na = site_nt(s, ea), nb = site_nt(s, eb);
-  if (na < 0 || na != nb || site_scope(s, ea) != site_scope(s, eb)) return r;
-  const int end = subtree_end(s, base, dest), donor_end = subtree_end(s, donor, src);
-  if (end < 0 || donor_end < 0) return r;
-  const int inserted = donor_end - src;
-  const int length = base.n - (end - dest) + inserted;
-  if (length > kCapacity) { r.status = ST_CAPACITY; return r; }
-  // Callers bound the output by the variable-node budget before splicing
-  // (crossover's total check, mutation's generation capacity); the row
-  // stride holds that budget.
-  if (length > s.stride) { r.status = ST_CAPACITY; return r; }
-  int pending[64];
-  int depth = 1, maximum = 1;
-  pending[0] = 1;
-  for (int i = 0; i < length; ++i) {
-    const bool incoming = i >= dest && i < dest + inserted;
-    uint32_t w = incoming ? donor.node[src + i - dest] : base.node[i < dest ? i : i + (end - dest) - inserted];
-    const int a = arity_of(s, w);
-    while (depth && !pending[depth - 1]) --depth;
-    if (!depth || a < 0 || a > 8) return r;
-    maximum = depth > maximum ? depth : maximum;
-    --pending[depth - 1];
-    if (a) {
-      if (depth == 64) return r;
-      pending[depth++] = a;
-    }
-    if (i == dest) w = (w & 0xffffu) | (uint32_t(ea + 1) << 16);
-    out.node[i] = w;
-  }
-  int bb = 0, be = 0, db = 0, dc = 0;
-  for (int i = 0; i < end; ++i) {
-    const int c = is_constant(s, base.node[i]);
-    be += c;
-    if (i < dest) bb += c;
-  }
-  for (int i = 0; i < donor_end; ++i) {
-    const int c = is_constant(s, donor.node[i]);
-    if (i < src) db += c; else dc += c;
-  }
-  if (be > base.nc || db + dc > donor.nc) return r;
-  int o = 0;
-  for (int k = 0; k < bb; ++k) out.cval[o++] = base.cval[k];
-  for (int k = 0; k < dc; ++k) out.cval[o++] = donor.cval[db + k];
-  for (int k = be; k < base.nc; ++k) out.cval[o++] = base.cval[k];
-  while (depth && !pending[depth - 1]) --depth;
-  if (depth) return r;
-  if (maximum > max_depth) { r.status = ST_CAPACITY; return r; }
-  if (site_limit) {
-    const int height = site_depth_of(s, out.node, length, -1);
-    if (height < 0) return r;
-    if (height > site_limit) { r.status = ST_CAPACITY; return r; }
-  }
-  r.status = ST_OK;
-  r.nodes = length;
-  r.constants = o;
-  return r;
-}
-
 
 // Minimum node cost of (expression, depth, site budget); kNoId when infeasible.
 __device__ __forceinline__ unsigned minimum_of(const SearchDesc& s, int e, int d, int l) {
@@ -238,15 +112,17 @@ __device__ __forceinline__ unsigned minimum_of(const SearchDesc& s, int e, int d
   return __ldg(&s.minimum[(size_t(e) * s.depth_count + d) * s.logical_count + l]);
 }
 
-// generate_phase<CompactTasks=true, EmitSites, Warp=false>
+// generate_phase<CompactTasks=true, EmitSites=true, Warp=false>
 // (cpp/src/evolution/repro/gpu/device/phase_generate.cuh:125-270): a typed
 // random subtree with min-cost feasibility and the FP64 weighted production
 // draw.  The draw uses round-to-nearest intrinsics so nothing is contracted
-// into an FMA; the reference host build rounds every operation the same way.
-// Tasks pack (expression:17, depth:7, scope_count:4, logical:4).
+// into an FMA; the reference's host build rounds every operation alike.
+// Tasks pack (expression:17, depth:7, scope_count:4, logical:4) in `pending`
+// (192 entries).  Emitted words carry depth relative to the generated root
+// (root = 1) and site depth relative to the budget `logical_depth`.
 __device__ inline GenResult generate(const SearchDesc& s, int root_expression, int scope_count, int depth,
-                                     int capacity, uint64_t seed, uint32_t* out_node, int64_t* out_cval,
-                                     int logical_depth, bool emit_sites) {
+                                     int capacity, uint64_t seed, uint64_t* out_node, int64_t* out_cval,
+                                     int logical_depth, uint32_t* pending) {
   GenResult result{ST_INVALID, 0, 0};
   int steps = 0;
   int next_site = -1;  // entry expression of a pending site
@@ -255,9 +131,8 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       depth >= s.depth_count || depth > 64 || logical_depth < 0 || logical_depth >= s.logical_count ||
       capacity <= 0 || capacity > kCapacity || s.n_ex > 131071)
     return result;
-  if (capacity > s.stride) capacity = s.stride;  // never reached: callers pass <= the node budget
+  if (capacity > s.stride) capacity = s.stride;  // callers pass at most the node budget
   const unsigned unselected = 131071u;
-  uint32_t pending[192];
   int count = 1;
   auto pack = [](unsigned e, unsigned d, unsigned n, unsigned l) -> uint32_t {
     return e | (d << 17) | (n << 24) | (l << 28);
@@ -280,10 +155,8 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       if (expression.target < 0 || expression.target >= s.n_nts || expression.scope_count < 0 ||
           expression.scope_count > 8)
         return result;
-      if (emit_sites) {
-        if (next_site >= 0) return result;
-        next_site = t_expr;
-      }
+      if (next_site >= 0) return result;
+      next_site = t_expr;
       const gagp_nonterminal nt = s.nts[expression.target];
       if (nt.scope_count != expression.scope_count || nt.production_offset < 0 || nt.production_count <= 0 ||
           nt.production_offset > s.n_prods || nt.production_count > s.n_prods - nt.production_offset)
@@ -351,7 +224,8 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
     } else if (info.kind != EK_OPERATION && info.kind != EK_INPUT) {
       return result;
     }
-    out_node[result.nodes++] = make_word(t_expr, emit_sites ? next_site : -1);
+    out_node[result.nodes++] = w_make(t_expr, next_site, depth - t_depth + 1, logical_depth - t_logical, arity,
+                                      info.kind == EK_CONSTANT, class_of_entry(s, next_site));
     next_site = -1;
     for (int i = arity - 1; i >= 0; --i) {
       if (count >= 192) { result.status = ST_CAPACITY; return result; }
@@ -369,6 +243,160 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
   if (reserved || !result.nodes) return result;
   result.status = ST_OK;
   return result;
+}
+
+// ------------------------------------------------------- warp row primitives
+// A row staged in shared memory: node words and constants.
+struct SRow {
+  uint64_t* node;
+  int64_t* cval;
+  int n, nc;
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+__device__ inline void warp_copy(const uint64_t* from_node, const int64_t* from_cval, int n, int nc, uint64_t* to_node,
+                                 int64_t* to_cval) {
+  for (int i = lane_id(); i < n; i += 32) to_node[i] = from_node[i];
+  for (int i = lane_id(); i < nc; i += 32) to_cval[i] = from_cval[i];
+  __syncwarp();
+}
+
+// site_matches (phase_operators.cuh:51-54): a variation site of class `cls`
+// (any class when cls == kNoClass).
+__device__ __forceinline__ bool site_matches(uint64_t w, uint32_t cls) {
+  const uint32_t c = w_class(w);
+  return c != kNoClass && (cls == kNoClass || c == cls);
+}
+
+// choose_site (phase_operators.cuh:55-83 and the counted warp variant
+// :95-117): the same count, draws and prefix-ordered rank; reservoir draws
+// visit matching sites in prefix order.  Every lane returns the same site.
+__device__ inline int warp_choose_site(const SRow& t, Rng& random, bool counted, uint32_t cls) {
+  const int lane = lane_id();
+  if (counted) {
+    unsigned count = 0;
+    for (int chunk = 0; chunk < t.n; chunk += 32) {
+      const int i = chunk + lane;
+      count += __popc(__ballot_sync(kFull, i < t.n && site_matches(t.node[i], cls)));
+    }
+    if (!count) return -1;
+    unsigned rank = unsigned(random.bounded(count));
+    for (int chunk = 0; chunk < t.n; chunk += 32) {
+      const int i = chunk + lane;
+      unsigned mask = __ballot_sync(kFull, i < t.n && site_matches(t.node[i], cls));
+      const unsigned c = __popc(mask);
+      if (rank < c) {
+        for (unsigned j = 0; j < rank; ++j) mask &= mask - 1;
+        return chunk + __ffs(mask) - 1;
+      }
+      rank -= c;
+    }
+    return -1;
+  }
+  int selected = -1;
+  unsigned count = 0;
+  for (int chunk = 0; chunk < t.n; chunk += 32) {
+    const int i = chunk + lane;
+    unsigned mask = __ballot_sync(kFull, i < t.n && site_matches(t.node[i], cls));
+    while (mask) {
+      const int bit = __ffs(mask) - 1;
+      mask &= mask - 1;
+      if (random.bounded(++count) == 0) selected = chunk + bit;
+    }
+  }
+  return selected;
+}
+
+// phase_subtree_end (device/phase_variation.cuh:81-91, warp form :213-229).
+__device__ inline int warp_subtree_end(const SRow& t, int start) {
+  if (start < 0 || start >= t.n) return -1;
+  const int lane = lane_id();
+  int pending = 1;
+  for (int chunk = start; chunk < t.n; chunk += 32) {
+    const int i = chunk + lane;
+    const bool live = i < t.n;
+    int scan = live ? w_arity(t.node[i]) - 1 : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int up = __shfl_up_sync(kFull, scan, o);
+      if (lane >= o) scan += up;
+    }
+    const unsigned hit = __ballot_sync(kFull, live && pending + scan == 0);
+    if (hit) return chunk + __ffs(hit);
+    pending += __shfl_sync(kFull, scan, 31);
+  }
+  return -1;
+}
+
+// Constant nodes among row positions [0, end).
+__device__ __forceinline__ int warp_count_constants(const SRow& t, int end) {
+  int c = 0;
+  for (int chunk = 0; chunk < end; chunk += 32) {
+    const int i = chunk + lane_id();
+    c += __popc(__ballot_sync(kFull, i < end && w_const(t.node[i])));
+  }
+  return c;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const T u = __shfl_xor_sync(kFull, v, o);
+    v = u > v ? u : v;
+  }
+  return v;
+}
+
+// splice_phase_tree (device/phase_variation.cuh:147-207): base with the
+// subtree at `dest` replaced by donor's subtree at `src`, into `out`.
+// Depth and site-depth limits are maxima of the output words; constants are
+// base[..dest) ++ donor subtree ++ base[end..), the prefix renumbering the
+// reference performs node by node.  Every lane returns the same result.
+__device__ inline GenResult warp_splice(const SRow& base, int dest, const SRow& donor, int src, SRow out, int stride,
+                                        int max_depth, int site_limit) {
+  GenResult r{ST_INVALID, 0, 0};
+  if (max_depth <= 0 || max_depth > 64 || base.n <= 0 || donor.n <= 0 || dest < 0 || dest >= base.n || src < 0 ||
+      src >= donor.n)
+    return r;
+  const uint64_t a = base.node[dest], b = donor.node[src];
+  if (!w_site(a) || w_class(a) != w_class(b)) return r;
+  const int end = warp_subtree_end(base, dest), donor_end = warp_subtree_end(donor, src);
+  if (end < 0 || donor_end < 0) return r;
+  const int inserted = donor_end - src;
+  const int length = base.n - (end - dest) + inserted;
+  if (length > kCapacity) { r.status = ST_CAPACITY; return r; }
+  if (length > stride) { r.status = ST_CAPACITY; return r; }  // never reached: callers bound by the node budget
+  const int ddepth = w_depth(a) - w_depth(b), dsval = w_sval(a) - w_sval(b);
+  int maxd = 0, maxs = 0;
+  for (int i = lane_id(); i < length; i += 32) {
+    uint64_t w;
+    if (i >= dest && i < dest + inserted) {
+      w = w_shift(donor.node[src + i - dest], ddepth, dsval);
+      if (i == dest) w = w_with_site(w, a);
+    } else {
+      w = base.node[i < dest ? i : i + (end - dest) - inserted];
+    }
+    out.node[i] = w;
+    maxd = max(maxd, w_depth(w));
+    maxs = max(maxs, w_sval(w));
+  }
+  const int bb = warp_count_constants(base, dest), be = warp_count_constants(base, end);
+  const int db = warp_count_constants(donor, src), de = warp_count_constants(donor, donor_end);
+  const int dc = de - db;
+  for (int k = lane_id(); k < bb; k += 32) out.cval[k] = base.cval[k];
+  for (int k = lane_id(); k < dc; k += 32) out.cval[bb + k] = donor.cval[db + k];
+  for (int k = lane_id(); k < base.nc - be; k += 32) out.cval[bb + dc + k] = base.cval[be + k];
+  maxd = warp_max(maxd);
+  maxs = warp_max(maxs);
+  __syncwarp();
+  if (maxd > max_depth) { r.status = ST_CAPACITY; return r; }
+  if (site_limit && maxs > site_limit) { r.status = ST_CAPACITY; return r; }
+  r.status = ST_OK;
+  r.nodes = length;
+  r.constants = bb + dc + (base.nc - be);
+  return r;
 }
 
 }  // namespace gb

@@ -216,7 +216,7 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
 struct Plan {
   Layout L;
   size_t ex, info, prods, nts, doms, vals, minimum, local_types, inputs, expected;
-  size_t node, cval, len, cnode, ccval, clen, tnode, tcval, gnode, gcval;
+  size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
   size_t code, code_len, kpool, code_temps, bc, bc_len, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, round, hist_sum, hist_fitness, hist_wrong,
@@ -253,10 +253,8 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
   p.expected = L.take(sizeof(int64_t) * C);
   const size_t S = size_t(p.stride);
-  p.node = L.take(4 * S * P); p.cval = L.take(8 * S * P); p.len = L.take(4 * size_t(P));
-  p.cnode = L.take(4 * S * B); p.ccval = L.take(8 * S * B); p.clen = L.take(4 * size_t(B));
-  p.tnode = L.take(4 * S * B); p.tcval = L.take(8 * S * B);
-  p.gnode = L.take(4 * S * B); p.gcval = L.take(8 * S * B);
+  p.node = L.take(8 * S * P); p.cval = L.take(8 * S * P); p.len = L.take(4 * size_t(P));
+  p.cnode = L.take(8 * S * B); p.ccval = L.take(8 * S * B); p.clen = L.take(4 * size_t(B));
   p.fitness = L.take(8 * size_t(P)); p.wrong = L.take(4 * size_t(P)); p.nodes = L.take(4 * size_t(P));
   p.key = L.take(8 * size_t(P));
   p.c_parent = L.take(4 * size_t(B)); p.c_reuse = L.take(4 * size_t(B)); p.c_error = L.take(4 * size_t(B));
@@ -272,7 +270,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.round_seed = L.take(8); p.best = L.take(4); p.placed = L.take(4 * size_t(P)); p.round = L.take(16);
   const size_t H = size_t(cfg->generations);
   p.hist_sum = L.take(8 * H); p.hist_fitness = L.take(8 * H); p.hist_wrong = L.take(4 * H);
-  p.hist_nodes = L.take(4 * H); p.hist_node = L.take(4 * S * H); p.hist_cval = L.take(8 * S * H);
+  p.hist_nodes = L.take(4 * H); p.hist_node = L.take(8 * S * H); p.hist_cval = L.take(8 * S * H);
   p.hist_len = L.take(4 * H); p.counters = L.take(8 * 4);
   return p;
 }
@@ -308,6 +306,7 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   e->arena_limit = arena_bytes ? arena_bytes : uint64_t(0.8 * double(free_bytes));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 8192));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_vary, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   *out = e.release();
   return GAGP_OK;
 }
@@ -432,10 +431,8 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.generations = s->G;
   d.inputs = at<int64_t>(b, p.inputs); d.expected = at<int64_t>(b, p.expected);
   d.C = C; d.n_inputs = NI; d.expected_tag = c->expected_tag; d.vm_cases_per_lane = cases_per_lane(C);
-  d.node = at<uint32_t>(b, p.node); d.cval = at<int64_t>(b, p.cval); d.len = at<int32_t>(b, p.len);
-  d.cnode = at<uint32_t>(b, p.cnode); d.ccval = at<int64_t>(b, p.ccval); d.clen = at<int32_t>(b, p.clen);
-  d.tnode = at<uint32_t>(b, p.tnode); d.tcval = at<int64_t>(b, p.tcval);
-  d.gnode = at<uint32_t>(b, p.gnode); d.gcval = at<int64_t>(b, p.gcval);
+  d.node = at<uint64_t>(b, p.node); d.cval = at<int64_t>(b, p.cval); d.len = at<int32_t>(b, p.len);
+  d.cnode = at<uint64_t>(b, p.cnode); d.ccval = at<int64_t>(b, p.ccval); d.clen = at<int32_t>(b, p.clen);
   d.fitness = at<double>(b, p.fitness); d.wrong = at<uint32_t>(b, p.wrong); d.nodes = at<uint32_t>(b, p.nodes);
   d.key = at<uint64_t>(b, p.key);
   d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
@@ -451,7 +448,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
   d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
   d.hist_wrong = at<uint32_t>(b, p.hist_wrong); d.hist_nodes = at<uint32_t>(b, p.hist_nodes);
-  d.hist_node = at<uint32_t>(b, p.hist_node); d.hist_cval = at<int64_t>(b, p.hist_cval);
+  d.hist_node = at<uint64_t>(b, p.hist_node); d.hist_cval = at<int64_t>(b, p.hist_cval);
   d.hist_len = at<int32_t>(b, p.hist_len); d.counters = at<uint64_t>(b, p.counters);
   // packed ranking key: loss | wrong | nodes
   const int node_bits = bits_for(uint64_t(g->max_nodes));
@@ -500,7 +497,9 @@ struct BatchView {
   gb::SearchDesc* d_desc = nullptr;
   int32_t* d_member_off = nullptr;   // n + 1
   int32_t* d_child_off = nullptr;    // n + 1
-  int n = 0, total_members = 0, total_children = 0, max_P = 0, max_lanes = 1, max_rounds = 0;
+  int n = 0, total_members = 0, total_children = 0, max_P = 0, max_lanes = 1, max_rounds = 0, max_stride = 4;
+  long long max_draws = 0;
+  int max_code_stride = 2;
 };
 
 gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
@@ -535,6 +534,9 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
     v->d_child_off = e->d_batch_off + n + 1;
   }
   v->total_members = v->total_children = v->max_P = v->max_rounds = 0;
+  v->max_stride = 4;
+  v->max_draws = 0;
+  v->max_code_stride = 2;
   v->max_lanes = 1;
   for (Search* s : list) {
     v->total_members += s->P;
@@ -542,6 +544,9 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
     v->max_P = std::max(v->max_P, s->P);
     v->max_lanes = std::max(v->max_lanes, s->desc.vm_cases_per_lane);
     v->max_rounds = std::max(v->max_rounds, s->total_rounds);
+    v->max_stride = std::max(v->max_stride, s->stride);
+    v->max_code_stride = std::max(v->max_code_stride, s->desc.code_stride);
+    v->max_draws = std::max(v->max_draws, (long long)s->B * s->desc.replacement_size + 1);
   }
   return ensure_lists(e, size_t(std::max(v->total_members, v->total_children)));
 }
@@ -552,12 +557,15 @@ int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1
 gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
   const int warps = 8;
   const int temp_stride = gb::kMaxTemps * v.max_lanes * 32;
-  const size_t smem = size_t(warps) * temp_stride * sizeof(int64_t);
+  const int code_stride = (v.max_code_stride + 1) & ~1;  // uint2 slots, in int64 units
+  const int const_stride = v.max_stride;
+  const size_t smem = size_t(warps) * (temp_stride + code_stride + const_stride) * sizeof(int64_t);
   const int per_sm = std::max(1, std::min(4, int((e->max_smem - 1024) / std::max<size_t>(smem, 1))));
   const int blocks = e->sm_count * per_sm;
   {
     Timed t(e, KN_VM_FAST);
-    gb::k_vm_fast<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, mode, e->d_fast, e->d_counts, temp_stride);
+    gb::k_vm_fast<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, mode, e->d_fast, e->d_counts, temp_stride,
+                                                            code_stride, const_stride);
   }
   {
     Timed t(e, KN_VM_GENERAL);
@@ -579,13 +587,26 @@ gagp_status launch_start(gagp_engine* e, const BatchView& v) {
 
 gagp_status launch_round(gagp_engine* e, const BatchView& v) {
   { Timed t(e, KN_RECORD); gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1); }
-  { Timed t(e, KN_VARY); gb::k_vary<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
+  {
+    Timed t(e, KN_VARY);
+    const int warps = 4;
+    const size_t smem = warps * gb::warp_rows_bytes(v.max_stride);
+    gb::k_vary<<<blocks_for(v.total_children, warps), warps * 32, smem, e->stream>>>(v.d_desc, v.d_child_off, v.n,
+                                                                                     v.max_stride);
+  }
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
   { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
                                                                          e->d_general, e->d_counts); }
   launch_vm(e, v, 1);
   { Timed t(e, KN_CHILD); gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
-  { Timed t(e, KN_PLACE); gb::k_place<<<v.n, 256, size_t(v.max_P) * sizeof(uint64_t), e->stream>>>(v.d_desc, v.n); }
+  {
+    Timed t(e, KN_PLACE);
+    // member keys plus as many 16-bit staged draws as fit (B * replacement + slack)
+    const size_t limit = e->max_smem - 8192;
+    size_t bytes = size_t(v.max_P) * sizeof(uint64_t) + size_t(v.max_draws + 64) * sizeof(uint16_t);
+    bytes = std::min(bytes, limit);
+    gb::k_place<<<v.n, 256, bytes, e->stream>>>(v.d_desc, v.n, int(bytes));
+  }
   { Timed t(e, KN_COMMIT); gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
 }
@@ -798,7 +819,8 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   const int P = s->P, S = s->stride;
   std::vector<int64_t> sum(H);
   std::vector<double> hf(H);
-  std::vector<uint32_t> hw(H), hn(H), hnode(size_t(H) * S);
+  std::vector<uint32_t> hw(H), hn(H);
+  std::vector<uint64_t> hnode(size_t(H) * S);
   std::vector<int64_t> hc(size_t(H) * S);
   std::vector<int32_t> hl(H);
   if (H) {
@@ -806,11 +828,11 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
     CUDA_TRY(cudaMemcpy(hf.data(), d.hist_fitness, 8 * H, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hw.data(), d.hist_wrong, 4 * H, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hn.data(), d.hist_nodes, 4 * H, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hnode.data(), d.hist_node, 4 * size_t(H) * S, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hnode.data(), d.hist_node, 8 * size_t(H) * S, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hc.data(), d.hist_cval, 8 * size_t(H) * S, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hl.data(), d.hist_len, 4 * H, cudaMemcpyDeviceToHost));
   }
-  auto put_row = [&](const gagp_rows& rows, int index, const uint32_t* node, const int64_t* cval, int32_t l) {
+  auto put_row = [&](const gagp_rows& rows, int index, const uint64_t* node, const int64_t* cval, int32_t l) {
     const int n = l & 0xffff, nc = (l >> 16) & 0xffff;
     rows.node_counts[index] = n;
     rows.constant_counts[index] = nc;
@@ -827,14 +849,15 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   }
   out->generations = H;
   std::vector<double> fit(P);
-  std::vector<uint32_t> wr(P), node(size_t(P) * S);
+  std::vector<uint32_t> wr(P);
+  std::vector<uint64_t> node(size_t(P) * S);
   std::vector<uint64_t> key(P);
   std::vector<int64_t> cv(size_t(P) * S);
   std::vector<int32_t> len(P);
   CUDA_TRY(cudaMemcpy(fit.data(), d.fitness, 8 * size_t(P), cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(wr.data(), d.wrong, 4 * size_t(P), cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(key.data(), d.key, 8 * size_t(P), cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(node.data(), d.node, 4 * size_t(P) * S, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(node.data(), d.node, 8 * size_t(P) * S, cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(cv.data(), d.cval, 8 * size_t(P) * S, cudaMemcpyDeviceToHost));
   CUDA_TRY(cudaMemcpy(len.data(), d.len, 4 * size_t(P), cudaMemcpyDeviceToHost));
   std::vector<int> order(P);

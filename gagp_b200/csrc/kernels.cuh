@@ -41,13 +41,14 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
   const int i = item - off[si];
   const int site_limit = s.site_depth;
   const int ramp = site_limit < 2 ? site_limit : 2 + i % (site_limit - 1);
-  uint32_t* node = s.node + size_t(i) * s.stride;
+  uint64_t* node = s.node + size_t(i) * s.stride;
   int64_t* cval = s.cval + size_t(i) * s.stride;
+  uint32_t pending[192];
   GenResult g{ST_INVALID, 0, 0};
   for (int logical = ramp, attempt = 0; g.status != ST_OK; ++attempt) {
     const int room = s.maxv < kCapacity ? s.maxv : kCapacity;
     g = generate(s, s.root_expression, 0, s.slot_max_depth, room,
-                 mix64(s.seed ^ mix64((uint64_t(i) * 8 + 0) * 64 + uint64_t(attempt))), node, cval, logical, true);
+                 mix64(s.seed ^ mix64((uint64_t(i) * 8 + 0) * 64 + uint64_t(attempt))), node, cval, logical, pending);
     if (g.status != ST_OK && attempt % 4 == 3 && logical < site_limit) ++logical;
     if (attempt >= 256 && g.status != ST_OK) {
       raise_error(s, 20);
@@ -55,6 +56,8 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
       return;
     }
   }
+  // site depths relative to the budget `logical` are absolute here: the root
+  // phase starts with no site above it
   s.len[i] = make_len(g.nodes, g.constants);
 }
 
@@ -69,12 +72,14 @@ __global__ void k_lower(const SearchDesc* descs, const int32_t* off, int n, int 
   const SearchDesc& s = descs[si];
   if (!search_live(s)) return;
   const int slot = item - off[si];
-  Row t;
+  LRow t;
   if (mode == 0) {
-    t = row_of(s.node, s.cval, s.len, s.stride, slot);
+    const int32_t l = s.len[slot];
+    t = LRow{s.node + size_t(slot) * s.stride, s.cval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
   } else {
     if (!s.c_eval[slot]) return;
-    t = row_of(s.cnode, s.ccval, s.clen, s.stride, slot);
+    const int32_t l = s.clen[slot];
+    t = LRow{s.cnode + size_t(slot) * s.stride, s.ccval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
   }
   int temps = 0, klen = 0;
   int len = lower_accumulator(s, t, s.code + size_t(slot) * s.code_stride, s.code_stride,
@@ -83,7 +88,7 @@ __global__ void k_lower(const SearchDesc* descs, const int32_t* off, int n, int 
     // exact bytecode length (a bound of every executed path) must fit the fuel
     int bytecode = 1;
     for (int i = 0; i < t.n; ++i) {
-      const int nk = s.info[origin_of(t.node[i])].node_kind;
+      const int nk = s.info[w_origin(t.node[i])].node_kind;
       bytecode += nk == TK_IF ? 2 : (nk == TK_AND || nk == TK_OR) ? 5 : 1;
     }
     if (bytecode > s.fuel) len = -1;
@@ -117,13 +122,26 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
   }
 }
 
-// Fast VM: persistent warps over the fast list.
+// Fast VM: persistent warps over the fast list.  Per warp shared memory:
+// temporaries (kMaxTemps x lanes x 32), the staged code (code_stride) and
+// constants (stride).
+template <int K>
+__device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWarpSmem& w, int64_t& loss,
+                                      uint32_t& wrong, uint64_t& ops) {
+  switch (s.n_inputs) {
+    case 1: run_accumulator<K, 1>(s, slot, w, loss, wrong, ops); break;
+    case 2: run_accumulator<K, 2>(s, slot, w, loss, wrong, ops); break;
+    default: run_accumulator<K, 0>(s, slot, w, loss, wrong, ops); break;
+  }
+}
 __global__ void k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list, const int32_t* list_count,
-                          int temp_stride) {
-  extern __shared__ int64_t smem_temps[];
+                          int temp_stride, int code_stride, int const_stride) {
+  extern __shared__ __align__(16) int64_t smem_vm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
-  int64_t* temps = smem_temps + size_t(warp) * temp_stride;
+  const size_t per_warp = size_t(temp_stride) + size_t(code_stride) + size_t(const_stride);  // int64 units
+  int64_t* base = smem_vm + size_t(warp) * per_warp;
+  const VmWarpSmem w{base, reinterpret_cast<uint2*>(base + temp_stride), base + temp_stride + code_stride};
   const int count = *list_count;
   for (int i = blockIdx.x * warps + warp; i < count; i += gridDim.x * warps) {
     const ProgramRef p = list[i];
@@ -132,10 +150,10 @@ __global__ void k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* l
     uint32_t wrong = 0;
     uint64_t ops = 0;
     switch (s.vm_cases_per_lane) {
-      case 1: run_accumulator<1>(s, p.slot, temps, loss, wrong, ops); break;
-      case 2: run_accumulator<2>(s, p.slot, temps, loss, wrong, ops); break;
-      case 4: run_accumulator<4>(s, p.slot, temps, loss, wrong, ops); break;
-      default: run_accumulator<8>(s, p.slot, temps, loss, wrong, ops); break;
+      case 1: run_k<1>(s, p.slot, w, loss, wrong, ops); break;
+      case 2: run_k<2>(s, p.slot, w, loss, wrong, ops); break;
+      case 4: run_k<4>(s, p.slot, w, loss, wrong, ops); break;
+      default: run_k<8>(s, p.slot, w, loss, wrong, ops); break;
     }
     loss = warp_sum(loss);
     wrong = warp_sum(wrong);
@@ -205,8 +223,7 @@ __global__ void k_member_keys(const SearchDesc* descs, const int32_t* off, int n
   const int si = find_search(off, n, item);
   const SearchDesc& s = descs[si];
   const int m = item - off[si];
-  const Row t = row_of(s.node, s.cval, s.len, s.stride, m);
-  const uint32_t nodes = s.has_wrong ? ranking_nodes(s, t.node, t.n) : 0;
+  const uint32_t nodes = s.has_wrong ? ranking_nodes(s, s.node + size_t(m) * s.stride, len_nodes(s.len[m])) : 0;
   s.nodes[m] = nodes;
   s.key[m] = pack_key(s, s.fitness[m], s.wrong[m], nodes);
 }
@@ -335,21 +352,27 @@ __global__ void k_record(const SearchDesc* descs, int n, int only_epoch_start) {
   }
 }
 
-// make_batch (phase_population_cpu.cpp:322-353): thread per child.
-__global__ void k_vary(const SearchDesc* descs, const int32_t* off, int n) {
-  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+// make_batch (phase_population_cpu.cpp:322-353): one warp per child, rows
+// staged in dynamic shared memory (warp_rows_bytes(stride) per warp).
+__global__ void k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max) {
+  extern __shared__ __align__(16) char smem_rows[];
+  const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  const int item = blockIdx.x * warps + warp;
   if (item >= off[n]) return;
   const int si = find_search(off, n, item);
   const SearchDesc& s = descs[si];
   if (!search_live(s)) return;
   const int child = item - off[si];
+  WarpRows rows = carve_rows(smem_rows + size_t(warp) * warp_rows_bytes(stride_max), s.stride);
   int reuse = -1, parent = -1;
-  const int error = vary_child(s, child, s.round_seed[0], &reuse, &parent);
-  s.c_parent[child] = parent;
-  s.c_reuse[child] = reuse;
-  s.c_error[child] = error;
-  s.c_eval[child] = error == 0 && reuse < 0;
-  if (error) raise_error(s, 100 + error);
+  const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent);
+  if ((threadIdx.x & 31) == 0) {
+    s.c_parent[child] = parent;
+    s.c_reuse[child] = reuse;
+    s.c_error[child] = error;
+    s.c_eval[child] = error == 0 && reuse < 0;
+    if (error) raise_error(s, 100 + error);
+  }
 }
 
 // Results of all children before any placement (evolve.cpp:403-413).
@@ -381,62 +404,124 @@ __global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int
 
 // Steady-state placement (evolve.cpp:414-427): children in order, each
 // replacing the worst of replacement_size uniform draws (redrawn when it is
-// the current best).  Keys of all members sit in shared memory; the run
-// generator's outputs (and their residues mod P) are pre-generated by the
-// block.  Then the next round's seed is drawn.  One block per search.
-__global__ void k_place(const SearchDesc* descs, int n) {
-  extern __shared__ uint64_t keys[];
+// the current best).  The block pre-generates the run generator's outputs
+// and stages their residues mod P as 16-bit draws in shared memory beside
+// the members' ranking keys; one thread then runs the sequential placement.
+// With the default replacement size 2 the next child's draws and keys are
+// loaded one child ahead and the current child's key store is forwarded to
+// them when they name the replaced member, so shared-memory latency leaves
+// the dependency chain.  Then the next round's seed is drawn.  One block per
+// search; `dyn_bytes`: dynamic shared memory of the launch.
+__global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
+  extern __shared__ __align__(16) uint64_t keys[];
   __shared__ uint64_t mt[312], nw[312];
   const SearchDesc& s = descs[blockIdx.x];
   if (!search_live(s)) return;
-  const int P = s.P, B = s.B;
+  const int P = s.P, B = s.B, rs = s.replacement_size, cap = s.stream_capacity;
+  uint16_t* draws = reinterpret_cast<uint16_t*>(keys + P);
+  const int slots = (dyn_bytes - int(sizeof(uint64_t)) * P) / int(sizeof(uint16_t));
+  int32_t* __restrict__ placed = s.placed;
   for (int m = threadIdx.x; m < P; m += blockDim.x) {
     keys[m] = s.key[m];
-    s.placed[m] = -1;
+    placed[m] = -1;
   }
   for (int i = threadIdx.x; i < 312; i += blockDim.x) mt[i] = s.mt[i];
   __syncthreads();
-  long long rp = stream_ptrs(s)[0], wp = stream_ptrs(s)[1];
-  const long long need = (long long)B * s.replacement_size + 1;
-  while (wp - rp < need && wp - rp + 312 <= s.stream_capacity) {
+  const long long rp = stream_ptrs(s)[0];
+  long long wp = stream_ptrs(s)[1];
+  const long long need = (long long)B * rs + 1;
+  while (wp - rp < need && wp - rp + 312 <= cap) {
     mt_block(s, mt, nw, wp);
     wp += 312;
   }
+  const int avail = int(min((long long)slots, wp - rp));
+  for (int i = threadIdx.x; i < avail; i += blockDim.x) draws[i] = uint16_t(s.stream_mod[(rp + i) % cap]);
+  __syncthreads();
   if (threadIdx.x == 0) {
-    int best = s.best[0];
-    auto take = [&]() -> long long {
-      if (rp == wp) {
-        mt_block_serial(s, mt, wp);
-        wp += 312;
+    const uint32_t* __restrict__ smod = s.stream_mod;
+    const uint64_t* __restrict__ ckey = s.c_key;
+    long long gen_wp = wp;
+    // residue of the draw `idx` positions after rp (staged, else the ring)
+    auto draw = [&](int idx) -> int {
+      if (idx < avail) return draws[idx];
+      const long long pos = rp + idx;
+      while (pos >= gen_wp) {  // ran ahead of the buffer: one serial block
+        mt_block_serial(s, mt, gen_wp);
+        gen_wp += 312;
       }
-      return rp++;
+      return int(smod[pos % cap]);
     };
-    auto better_m = [&](int a, int b) { return keys[a] < keys[b] || (keys[a] == keys[b] && a < b); };
-    for (int b = 0; b < B; ++b) {
-      int v;
-      for (int guard = 0;; ++guard) {
-        int worst = int(s.stream_mod[take() % s.stream_capacity]);
-        for (int i = 1; i < s.replacement_size; ++i) {
-          const int c = int(s.stream_mod[take() % s.stream_capacity]);
-          if (better_m(worst, c)) worst = c;
+    int best = s.best[0];
+    uint64_t best_key = keys[best];
+    int di = 0;
+    bool failed = false;
+    if (rs == 2) {
+      int d0 = draw(0), d1 = draw(1);
+      uint64_t k0 = keys[d0], k1 = keys[d1];
+      uint64_t ck = ckey[0];
+      for (int b = 0; b < B; ++b) {
+        di += 2;
+        const uint64_t ck_next = b + 1 < B ? ckey[b + 1] : 0;
+        // worst of the pair: the second replaces the first when the first is better
+        int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
+        for (int guard = 0; v == best; ++guard) {
+          if (guard > (1 << 20)) { failed = true; break; }
+          d0 = draw(di); d1 = draw(di + 1); di += 2;
+          k0 = keys[d0]; k1 = keys[d1];
+          v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
         }
-        if (worst != best) { v = worst; break; }
-        if (guard > (1 << 20)) { v = -1; break; }  // bounded: P == 1 only
+        if (failed) break;
+        int n0 = 0, n1 = 0;
+        uint64_t nk0 = 0, nk1 = 0;
+        if (b + 1 < B) {
+          n0 = draw(di);
+          n1 = draw(di + 1);
+          nk0 = keys[n0];
+          nk1 = keys[n1];
+        }
+        keys[v] = ck;
+        placed[v] = b;
+        if (n0 == v) nk0 = ck;
+        if (n1 == v) nk1 = ck;
+        if (ck < best_key || (ck == best_key && v < best)) { best = v; best_key = ck; }
+        d0 = n0; d1 = n1; k0 = nk0; k1 = nk1; ck = ck_next;
       }
-      if (v < 0) { raise_error(s, 40); break; }
-      keys[v] = s.c_key[b];
-      s.placed[v] = b;
-      if (better_m(v, best)) best = v;
+    } else {
+      for (int b = 0; b < B && !failed; ++b) {
+        const uint64_t ck = ckey[b];
+        int v = -1;
+        for (int guard = 0; guard < (1 << 20); ++guard) {
+          int worst = draw(di++);
+          uint64_t kw = keys[worst];
+          for (int i = 1; i < rs; ++i) {
+            const int c = draw(di++);
+            const uint64_t kc = keys[c];
+            if (kw < kc || (kw == kc && worst < c)) { worst = c; kw = kc; }
+          }
+          if (worst != best) { v = worst; break; }
+        }
+        if (v < 0) { failed = true; break; }
+        keys[v] = ck;
+        placed[v] = b;
+        if (ck < best_key || (ck == best_key && v < best)) { best = v; best_key = ck; }
+      }
     }
-    s.round_seed[0] = s.stream[take() % s.stream_capacity];
+    if (failed) raise_error(s, 40);
+    // the next round's variation seed: the raw output at the next position
+    const long long pos = rp + di;
+    while (pos >= gen_wp) {
+      mt_block_serial(s, mt, gen_wp);
+      gen_wp += 312;
+    }
+    s.round_seed[0] = s.stream[pos % cap];
     s.best[0] = best;
-    stream_ptrs(s)[0] = rp;
-    stream_ptrs(s)[1] = wp;
+    stream_ptrs(s)[0] = pos + 1;
+    stream_ptrs(s)[1] = gen_wp;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 312; i += blockDim.x) s.mt[i] = mt[i];
   for (int m = threadIdx.x; m < P; m += blockDim.x) {
-    const int b = s.placed[m];
+    const int b = placed[m];
     if (b >= 0) {
       s.key[m] = keys[m];
       s.fitness[m] = s.c_fitness[b];
@@ -450,10 +535,6 @@ __global__ void k_place(const SearchDesc* descs, int n) {
     if (r >= s.total_rounds) s.round[2] = 1;
   }
 }
-// The state read by the serial placement above must be the one left by the
-// previous block-wide generation; both happen inside one block, ordered by
-// __syncthreads.  The MT state written back is the state after the last
-// generated block, matching the stream's write counter.
 
 // commit_batch (phase_population_cpu.cpp:382-394): placed child rows replace
 // members.  Thread per member.
@@ -467,8 +548,12 @@ __global__ void k_commit(const SearchDesc* descs, const int32_t* off, int n) {
   const int b = s.placed[m];
   if (b < 0) return;
   const int32_t l = s.clen[b];
-  copy_row(Row{s.cnode + size_t(b) * s.stride, s.ccval + size_t(b) * s.stride, len_nodes(l), len_consts(l)},
-           mrow_of(s.node, s.cval, s.stride, m));
+  const uint64_t* from = s.cnode + size_t(b) * s.stride;
+  const int64_t* cfrom = s.ccval + size_t(b) * s.stride;
+  uint64_t* to = s.node + size_t(m) * s.stride;
+  int64_t* cto = s.cval + size_t(m) * s.stride;
+  for (int i = 0; i < len_nodes(l); ++i) to[i] = from[i];
+  for (int i = 0; i < len_consts(l); ++i) cto[i] = cfrom[i];
   s.len[m] = l;
 }
 

@@ -39,10 +39,17 @@ __device__ __forceinline__ uint2 a_instr(uint32_t op, bool swap, uint32_t k1, ui
 
 constexpr int kMaxLowerNodes = 256;
 
+// A row to lower: node words and prefix-ordered constants.
+struct LRow {
+  const uint64_t* node;
+  const int64_t* cval;
+  int n, nc;
+};
+
 // Reference bytecode of a value phase.  Returns the instruction count
 // (including the appended RETURN) or -1 when the compiler rejects the row.
 // Code: 5 ints per instruction (op, flags, a, b, fuel).
-__device__ inline int lower_reference(const SearchDesc& s, const Row& t, int32_t* code, int code_cap,
+__device__ inline int lower_reference(const SearchDesc& s, const LRow& t, int32_t* code, int code_cap,
                                       int64_t* consts, int* n_consts, int* stack_bound_out) {
   struct Frame { int node, base_stack, first_jump, second_jump, seen; int8_t args[3]; };
   Frame frames[64];
@@ -61,7 +68,7 @@ __device__ inline int lower_reference(const SearchDesc& s, const Row& t, int32_t
     if (!have_value) {
       if (cursor >= t.n) return -1;
       const int index = cursor++;
-      const gagp_expression& e = s.ex[origin_of(t.node[index])];
+      const gagp_expression& e = s.ex[w_origin(t.node[index])];
       if (e.node_kind == TK_CONSTANT) {
         // constants are Int payloads in prefix order
         if (nconst >= kCapacity) return -1;
@@ -93,7 +100,7 @@ __device__ inline int lower_reference(const SearchDesc& s, const Row& t, int32_t
       return count;
     }
     Frame& f = frames[depth - 1];
-    const gagp_expression& e = s.ex[origin_of(t.node[f.node])];
+    const gagp_expression& e = s.ex[w_origin(t.node[f.node])];
     if (f.seen < 3) f.args[f.seen] = int8_t(completed);
     ++f.seen;
     const bool branch = e.node_kind == TK_IF || e.node_kind == TK_AND || e.node_kind == TK_OR;
@@ -173,7 +180,7 @@ __device__ __forceinline__ uint32_t accumulator_op(const gagp_expression& e) {
 
 // Accumulator program of a row; returns the instruction count, or -1 when the
 // row needs the general VM.  *temps_out: temporaries used.
-__device__ inline int lower_accumulator(const SearchDesc& s, const Row& t, uint2* code, int code_cap,
+__device__ inline int lower_accumulator(const SearchDesc& s, const LRow& t, uint2* code, int code_cap,
                                         int64_t* kpool, int* kpool_len, int* temps_out) {
   (void)kpool_len;
   const int n = t.n;
@@ -184,10 +191,10 @@ __device__ inline int lower_accumulator(const SearchDesc& s, const Row& t, uint2
   int16_t constant_index[kMaxLowerNodes];
   {
     int k = 0;
-    for (int i = 0; i < n; ++i) constant_index[i] = is_constant(s, t.node[i]) ? int16_t(k++) : int16_t(-1);
+    for (int i = 0; i < n; ++i) constant_index[i] = w_const(t.node[i]) ? int16_t(k++) : int16_t(-1);
   }
   for (int i = n - 1; i >= 0; --i) {
-    const gagp_expression& e = s.ex[origin_of(t.node[i])];
+    const gagp_expression& e = s.ex[w_origin(t.node[i])];
     const int a = e.arity;
     if (a == 0) { end[i] = int16_t(i + 1); need[i] = 0; continue; }
     if (accumulator_op(e) == A_COUNT) return -1;
@@ -216,7 +223,7 @@ __device__ inline int lower_accumulator(const SearchDesc& s, const Row& t, uint2
     return constant_index[i] >= 0 ? K_CONST : K_INPUT;
   };
   auto leaf_index = [&](int i) -> uint32_t {
-    return constant_index[i] >= 0 ? uint32_t(constant_index[i]) : uint32_t(s.ex[origin_of(t.node[i])].operand);
+    return constant_index[i] >= 0 ? uint32_t(constant_index[i]) : uint32_t(s.ex[w_origin(t.node[i])].operand);
   };
   // explicit-stack post order emission
   struct Frame { int16_t node; int8_t stage, count, order[3], spilled[3]; int8_t temp_base; };
@@ -235,7 +242,7 @@ __device__ inline int lower_accumulator(const SearchDesc& s, const Row& t, uint2
     f.stage = 0;
     f.temp_base = int8_t(temp_top);
     // non-leaf children in evaluation order (decreasing need, stable)
-    const int a = s.ex[origin_of(t.node[node])].arity;
+    const int a = s.ex[w_origin(t.node[node])].arity;
     int c = node + 1, k = 0;
     int8_t kids[3];
     for (int x = 0; x < a; ++x) { kids[x] = int8_t(c - node); c = end[c]; }
@@ -277,7 +284,7 @@ __device__ inline int lower_accumulator(const SearchDesc& s, const Row& t, uint2
       continue;
     }
     // all non-leaf children evaluated: the last one (if any) is in ACC
-    const gagp_expression& e = s.ex[origin_of(t.node[node])];
+    const gagp_expression& e = s.ex[w_origin(t.node[node])];
     const uint32_t op = accumulator_op(e);
     const int a = e.arity;
     uint32_t kind[3] = {K_ACC, K_ACC, K_ACC}, idx[3] = {0, 0, 0};

@@ -1,7 +1,9 @@
 // Per-child selection and variation of one steady-state round
 // (crossover_child / mutate_child / compare_child,
-// cpp/src/evolution/repro/gpu/phase_operators.cuh:46-265), over the compact
-// row layout.  One whole-program phase per member (slot_count == 1), so the
+// cpp/src/evolution/repro/gpu/phase_operators.cuh:46-265), one warp per
+// child over rows staged in shared memory.  Every lane draws the same random
+// numbers (the reference's Warp=true contract); lanes split copies, counts
+// and scans.  One whole-program phase per member (slot_count == 1), so the
 // uniform-phase draw is bounded(1) and a row is a member.
 #pragma once
 #include "device_ops.cuh"
@@ -16,11 +18,6 @@ __device__ __forceinline__ bool selection_greater(const SearchDesc& s, const uin
   const uint64_t kc = key[c], kb = key[b];
   return kc < kb || (s.has_wrong && kc == kb && c < b);
 }
-// Ranking order `better` (evolve.cpp:351-355): strict total order.
-__device__ __forceinline__ bool better(const uint64_t* key, int a, int b) {
-  const uint64_t ka = key[a], kb = key[b];
-  return ka < kb || (ka == kb && a < b);
-}
 
 // tournament (phase_operators.cuh:46-50)
 __device__ inline int tournament(const SearchDesc& s, Rng& random) {
@@ -32,135 +29,141 @@ __device__ inline int tournament(const SearchDesc& s, Rng& random) {
   return best;
 }
 
-// site_matches (phase_operators.cuh:51-54): a variation site of class `cls`
-// (any class when cls < 0); fixed-nonterminal sites never match.
-__device__ __forceinline__ bool site_matches(const SearchDesc& s, uint32_t w, int cls) {
-  const int e = entry_of(w);
-  if (e < 0) return false;
-  const int c = s.info[e].site_class;
-  return c >= 0 && (cls < 0 || c == cls);
+// Shared-memory rows of one warp: parent, donor, child, splice output,
+// generated subtree; `pending` is the generator's task stack.
+struct WarpRows {
+  SRow parent, donor, child, out, gen;
+  uint32_t* pending;
+};
+
+__host__ __device__ __forceinline__ size_t warp_rows_bytes(int stride) {
+  return size_t(5) * stride * (sizeof(uint64_t) + sizeof(int64_t)) + 192 * sizeof(uint32_t);
+}
+__device__ inline WarpRows carve_rows(char* base, int stride) {
+  WarpRows r;
+  uint64_t* n = reinterpret_cast<uint64_t*>(base);
+  int64_t* c = reinterpret_cast<int64_t*>(n + 5 * stride);
+  r.parent = SRow{n, c, 0, 0};
+  r.donor = SRow{n + stride, c + stride, 0, 0};
+  r.child = SRow{n + 2 * stride, c + 2 * stride, 0, 0};
+  r.out = SRow{n + 3 * stride, c + 3 * stride, 0, 0};
+  r.gen = SRow{n + 4 * stride, c + 4 * stride, 0, 0};
+  r.pending = reinterpret_cast<uint32_t*>(c + 5 * stride);
+  return r;
 }
 
-// choose_site (phase_operators.cuh:55-83): counted rank draw or reservoir draws.
-__device__ inline int choose_site(const SearchDesc& s, const Row& t, Rng& random, bool counted, int cls) {
-  if (counted) {
-    unsigned count = 0;
-    for (int i = 0; i < t.n; ++i) count += site_matches(s, t.node[i], cls);
-    if (!count) return -1;
-    unsigned rank = unsigned(random.bounded(count));
-    for (int i = 0; i < t.n; ++i)
-      if (site_matches(s, t.node[i], cls)) {
-        if (rank == 0) return i;
-        --rank;
-      }
-    return -1;
-  }
-  int selected = -1;
-  unsigned count = 0;
-  for (int i = 0; i < t.n; ++i)
-    if (site_matches(s, t.node[i], cls))
-      if (random.bounded(++count) == 0) selected = i;
-  return selected;
+__device__ inline void load_member(const SearchDesc& s, int m, SRow& to) {
+  const int32_t l = s.len[m];
+  to.n = len_nodes(l);
+  to.nc = len_consts(l);
+  warp_copy(s.node + size_t(m) * s.stride, s.cval + size_t(m) * s.stride, to.n, to.nc, to.node, to.cval);
 }
 
-// One child: crossover into the child row, then mutation of the child row,
-// then the identity check against its first parent.  Returns the error code
-// of the reference's OperatorStats (0: none).
-__device__ inline int vary_child(const SearchDesc& s, int child, uint64_t seed, int* reuse_out, int* parent_out) {
-  const Row none{nullptr, nullptr, 0, 0};
-  (void)none;
+// One child, by one warp.  Writes the child row, its parent and reuse
+// source (the parent when the genotype is unchanged) and returns the
+// reference's OperatorStats error code (0: none).
+__device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t seed, WarpRows& w, int* reuse_out,
+                                      int* parent_out) {
+  const int lane = lane_id();
   *reuse_out = -1;
-  MRow crow = mrow_of(s.cnode, s.ccval, s.stride, child);
-  MRow tmp = mrow_of(s.tnode, s.tcval, s.stride, child);
   // ---- crossover_child
   Rng random(seed ^ (0x617089e168ULL + uint64_t(child)));
   const int parent = tournament(s, random), donor = tournament(s, random);
   *parent_out = parent;
-  const Row prow = row_of(s.node, s.cval, s.len, s.stride, parent);
-  const Row drow = row_of(s.node, s.cval, s.len, s.stride, donor);
-  if (prow.n <= 0 || prow.n > s.maxv || prow.nc > prow.n) return 1;
-  copy_row(prow, crow);
-  int n = prow.n, nc = prow.nc;
-  const int total = prow.n;
-  bool gated = s.crossover_probability < 1 && random.unit() >= s.crossover_probability;
+  load_member(s, parent, w.parent);
+  load_member(s, donor, w.donor);
+  if (w.parent.n <= 0 || w.parent.n > s.maxv || w.parent.nc > w.parent.n) return 1;
+  warp_copy(w.parent.node, w.parent.cval, w.parent.n, w.parent.nc, w.child.node, w.child.cval);
+  w.child.n = w.parent.n;
+  w.child.nc = w.parent.nc;
+  const int total = w.parent.n;
+  const bool gated = s.crossover_probability < 1 && random.unit() >= s.crossover_probability;
   if (!gated) {
     if (s.uniform_phase) (void)random.bounded(1);
     for (int attempt = 0; attempt < s.attempts; ++attempt) {
-      const int dest = choose_site(s, prow, random, s.counted, -1);
+      const int dest = warp_choose_site(w.parent, random, s.counted, kNoClass);
       if (dest < 0) break;
-      const int cls = s.info[entry_of(prow.node[dest])].site_class;
-      const int src = choose_site(s, drow, random, s.counted, cls);
+      const int src = warp_choose_site(w.donor, random, s.counted, w_class(w.parent.node[dest]));
       if (src < 0) continue;
-      const int ae = subtree_end(s, prow, dest), be = subtree_end(s, drow, src);
+      const int ae = warp_subtree_end(w.parent, dest), be = warp_subtree_end(w.donor, src);
       if (ae < 0 || be < 0) return 3;
       if (total - (ae - dest) + (be - src) > s.maxv) continue;
-      const GenResult r = splice(s, prow, dest, drow, src, tmp, s.slot_max_depth, s.site_depth);
+      const GenResult r = warp_splice(w.parent, dest, w.donor, src, w.out, s.stride, s.slot_max_depth, s.site_depth);
       if (r.status == ST_OK) {
-        copy_row(Row{tmp.node, tmp.cval, r.nodes, r.constants}, crow);
-        n = r.nodes;
-        nc = r.constants;
+        warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
+        w.child.n = r.nodes;
+        w.child.nc = r.constants;
         break;
       }
     }
   }
-  s.clen[child] = make_len(n, nc);
   // ---- mutate_child
   {
-    const Row c{crow.node, crow.cval, n, nc};
     Rng m(seed ^ (0x124ab512bf01ULL + uint64_t(child)));
     if (m.unit() < s.mutation_probability) {
       if (s.uniform_phase) (void)m.bounded(1);
-      const int dest = choose_site(s, c, m, s.counted, -1);
+      const int dest = warp_choose_site(w.child, m, s.counted, kNoClass);
       if (dest >= 0) {
-        const int end = subtree_end(s, c, dest), depth = node_depth(s, c, dest);
-        if (end < 0 || depth < 0) return 6;
-        const int entry = entry_of(c.node[dest]);
-        const int incoming = s.site_depth ? site_depth_of(s, c.node, c.n, dest) : 0;
+        const uint64_t a = w.child.node[dest];
+        const int end = warp_subtree_end(w.child, dest), depth = w_depth(a);
+        if (end < 0 || depth < 1) return 6;
+        const int entry = w_entry(a);
+        const int incoming = s.site_depth ? w_sval(a) - 1 : 0;
         if (incoming < 0 || incoming > s.site_depth) return 6;
         const int logical = s.site_depth - incoming;
         const int replaced = end - dest;
-        const int whole = s.maxv - (c.n - replaced), phase = kCapacity - (c.n - replaced);
+        const int whole = s.maxv - (w.child.n - replaced), phase = kCapacity - (w.child.n - replaced);
         const int available = whole < phase ? whole : phase, uncapped = available < kCapacity ? available : kCapacity;
         const bool capped = s.mutation_max_nodes > 0 && s.mutation_max_nodes < uncapped;
         const int bounded = capped ? s.mutation_max_nodes : uncapped;
-        uint32_t* gnode = s.gnode + size_t(child) * s.stride;
-        int64_t* gcval = s.gcval + size_t(child) * s.stride;
-        // parent_scope of a site: scoped nonterminals are declined at admission
-        const GenResult g = generate(s, entry, 0, s.slot_max_depth - depth + 1, bounded, m.next(), gnode, gcval,
-                                     logical, true);
+        const uint64_t gseed = m.next();
+        GenResult g{ST_INVALID, 0, 0};
+        if (lane == 0)
+          g = generate(s, entry, 0, s.slot_max_depth - depth + 1, bounded, gseed, w.gen.node, w.gen.cval, logical,
+                       w.pending);
+        g.status = __shfl_sync(kFull, g.status, 0);
+        g.nodes = __shfl_sync(kFull, g.nodes, 0);
+        g.constants = __shfl_sync(kFull, g.constants, 0);
+        __syncwarp();
         if (capped && g.status == ST_CAPACITY) {
           // a configured cap without a feasible derivation skips this mutation
         } else if (g.status != ST_OK) {
           return 7;
         } else {
-          const Row gen{gnode, gcval, g.nodes, g.constants};
-          const GenResult r = splice(s, c, dest, gen, 0, tmp, s.slot_max_depth, s.site_depth);
+          w.gen.n = g.nodes;
+          w.gen.nc = g.constants;
+          const GenResult r = warp_splice(w.child, dest, w.gen, 0, w.out, s.stride, s.slot_max_depth, s.site_depth);
           if (r.status != ST_OK) return 8;
-          copy_row(Row{tmp.node, tmp.cval, r.nodes, r.constants}, crow);
-          n = r.nodes;
-          nc = r.constants;
-          s.clen[child] = make_len(n, nc);
+          warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
+          w.child.n = r.nodes;
+          w.child.nc = r.constants;
         }
       }
     }
   }
-  // ---- compare_child: identical genotype (construction records + constants)
-  if (n == prow.n && nc == prow.nc) {
-    bool equal = true;
-    for (int i = 0; i < n && equal; ++i) equal = origin_of(crow.node[i]) == origin_of(prow.node[i]);
-    for (int i = 0; i < nc && equal; ++i) equal = crow.cval[i] == prow.cval[i];
-    if (equal) *reuse_out = parent;
+  // ---- compare_child: identical construction records and constants
+  bool equal = w.child.n == w.parent.n && w.child.nc == w.parent.nc;
+  if (equal) {
+    bool mine = true;
+    for (int i = lane; i < w.child.n; i += 32) mine &= w_origin(w.child.node[i]) == w_origin(w.parent.node[i]);
+    for (int i = lane; i < w.child.nc; i += 32) mine &= w.child.cval[i] == w.parent.cval[i];
+    equal = __all_sync(kFull, mine);
   }
+  if (equal) *reuse_out = parent;
+  // ---- publish the child row
+  for (int i = lane; i < w.child.n; i += 32) s.cnode[size_t(child) * s.stride + i] = w.child.node[i];
+  for (int i = lane; i < w.child.nc; i += 32) s.ccval[size_t(child) * s.stride + i] = w.child.cval[i];
+  if (lane == 0) s.clen[child] = make_len(w.child.n, w.child.nc);
   return 0;
 }
 
 // Member (or child) node count for ranking: AST nodes (fixed wrapper nodes +
 // phase nodes), or the mutable grammar sites under tie_break grammar_sites
 // (HostPhasePopulation::nodes, phase_population_cpu.cpp:165-173).
-__device__ inline uint32_t ranking_nodes(const SearchDesc& s, const uint32_t* node, int n) {
+__device__ inline uint32_t ranking_nodes(const SearchDesc& s, const uint64_t* node, int n) {
   if (!s.grammar_sites) return uint32_t(s.fixed_nodes + n);
   uint32_t count = 0;
-  for (int i = 0; i < n; ++i) count += entry_of(node[i]) >= 0;
+  for (int i = 0; i < n; ++i) count += w_site(node[i]);
   return count;
 }
 

@@ -1,14 +1,15 @@
 // Device-resident state of one search and the descriptor kernels read it by.
 //
 // Row layout (B200-first, not the reference's): a member is one phase row of
-// at most `maxv` nodes.  A node is one 32-bit word -- the construction
-// expression in the low half and 1 + the expression that opened its grammar
-// site in the high half (0: no site) -- because every other field of the
-// reference's 28-byte PhaseTreeNode and 16-byte PhaseGeneSite is a function
-// of those two ids (device/phase_compile.cuh:64-74, device/phase_generate.cuh:12-17).
+// at most `maxv` nodes.  A node is one 64-bit self-describing word (see
+// device_ops.cuh): the construction expression and the expression that
+// opened its grammar site -- every other field of the reference's 28-byte
+// PhaseTreeNode and 16-byte PhaseGeneSite is a function of those two ids
+// (device/phase_compile.cuh:64-74, device/phase_generate.cuh:12-17) -- plus
+// depth, site depth, arity, a constant flag and the site's crossover class.
 // Constants are int64 payloads in prefix order, which is the operand order
 // the reference's generator and splice assign (phase_generate.cuh:253,
-// phase_variation.cuh:183-187).  A row is 12 bytes per node slot instead of
+// phase_variation.cuh:183-187).  A row is 16 bytes per node slot instead of
 // the reference's 64 KB fixed 1024-node rows.
 #pragma once
 #include <cstdint>
@@ -67,10 +68,8 @@ struct SearchDesc {
   const int64_t* expected;
   int32_t C, n_inputs, expected_tag, vm_cases_per_lane;
   // ---- population rows (members) and children
-  uint32_t* node;     int64_t* cval;     int32_t* len;        // P rows
-  uint32_t* cnode;    int64_t* ccval;    int32_t* clen;       // B child rows
-  uint32_t* tnode;    int64_t* tcval;                         // B splice scratch rows
-  uint32_t* gnode;    int64_t* gcval;                         // B generated-subtree rows
+  uint64_t* node;     int64_t* cval;     int32_t* len;        // P member rows (node words, constants)
+  uint64_t* cnode;    int64_t* ccval;    int32_t* clen;       // B child rows
   // ---- member statistics; key: packed ranking key (smaller is better)
   double* fitness; uint32_t* wrong; uint32_t* nodes; uint64_t* key;
   // ---- per-child results of one round
@@ -98,7 +97,7 @@ struct SearchDesc {
   int32_t* round;                      // [0] rounds done, [1] history entries, [2] finished flag, [3] error
   int64_t* hist_sum;                   // per history entry: sum of member fitness (integral)
   double* hist_fitness; uint32_t* hist_wrong; uint32_t* hist_nodes;
-  uint32_t* hist_node; int64_t* hist_cval; int32_t* hist_len;
+  uint64_t* hist_node; int64_t* hist_cval; int32_t* hist_len;
   uint64_t* counters;                  // [0] evaluated programs, [1] reused, [2] program cases, [3] VM ops
   int32_t key_shift_wrong, key_shift_nodes; // packed key layout
   int32_t total_rounds;

@@ -61,39 +61,64 @@ __device__ __forceinline__ T warp_sum(T v) {
 
 // ------------------------------------------------------------ fast VM
 // One warp runs one accumulator program; lane l holds cases
-// tile*32K + k*32 + l for k < K (coalesced input loads), in registers.
-// Temporaries live in shared memory [temp][k][lane].
-template <int K>
-__device__ inline void run_accumulator(const SearchDesc& s, int slot, int64_t* temps, int64_t& loss_out,
+// tile*32K + k*32 + l for k < K (coalesced input loads).  The program's code
+// and constants are staged in shared memory; with NIN (1 or 2) inputs the
+// tile's input values live in registers, otherwise (NIN == 0) they are read
+// through L1.  Temporaries live in shared memory [temp][k][lane].
+struct VmWarpSmem {
+  int64_t* temps;
+  uint2* code;
+  int64_t* consts;
+};
+
+template <int K, int NIN>
+__device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWarpSmem& w, int64_t& loss_out,
                                        uint32_t& wrong_out, uint64_t& ops_out) {
   const int lane = threadIdx.x & 31;
-  const uint2* code = s.code + size_t(slot) * s.code_stride;
   const int len = s.code_len[slot];
-  const int64_t* kpool = s.kpool + size_t(slot) * s.stride;
+  {
+    const uint2* code = s.code + size_t(slot) * s.code_stride;
+    const int64_t* kpool = s.kpool + size_t(slot) * s.stride;
+    for (int i = lane; i < len; i += 32) w.code[i] = code[i];
+    for (int i = lane; i < s.stride; i += 32) w.consts[i] = kpool[i];
+    __syncwarp();
+  }
   const int C = s.C;
+  const int64_t* __restrict__ inputs = s.inputs;
+  int64_t* __restrict__ temps = w.temps;
   int64_t loss = 0;
   uint32_t wrong = 0;
   for (int tile = 0; tile < C; tile += 32 * K) {
     int64_t acc[K];
+    int64_t in0[K], in1[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] = 0;
+    for (int k = 0; k < K; ++k) {
+      acc[k] = 0;
+      const int c = tile + k * 32 + lane;
+      in0[k] = (NIN >= 1 && c < C) ? __ldg(&inputs[c]) : 0;
+      in1[k] = (NIN >= 2 && c < C) ? __ldg(&inputs[size_t(C) + c]) : 0;
+    }
     auto fetch = [&](uint32_t kind, uint32_t index, int k) -> int64_t {
       switch (kind) {
         case K_ACC: return acc[k];
         case K_TEMP: return temps[(index * K + k) * 32 + lane];
         case K_INPUT: {
+          if (NIN == 1) return in0[k];
+          if (NIN == 2) return index ? in1[k] : in0[k];
           const int c = tile + k * 32 + lane;
-          return c < C ? __ldg(&s.inputs[size_t(index) * C + c]) : 0;
+          return c < C ? __ldg(&inputs[size_t(index) * C + c]) : 0;
         }
-        default: return __ldg(&kpool[index]);
+        default: return w.consts[index];
       }
     };
+    uint2 ins = len ? w.code[0] : make_uint2(0, 0);
     for (int ip = 0; ip < len; ++ip) {
-      const uint2 ins = __ldg(&code[ip]);
-      const uint32_t op = ins.x & 0xffu;
-      const bool swap = (ins.x >> 8) & 1u;
-      const uint32_t k1 = (ins.x >> 9) & 3u, k2 = (ins.x >> 11) & 3u, k3 = (ins.x >> 13) & 3u;
-      const uint32_t i1 = ins.y & 0xffffu, i2 = ins.y >> 16, i3 = ins.x >> 16;
+      const uint2 cur = ins;
+      if (ip + 1 < len) ins = w.code[ip + 1];
+      const uint32_t op = cur.x & 0xffu;
+      const bool swap = (cur.x >> 8) & 1u;
+      const uint32_t k1 = (cur.x >> 9) & 3u, k2 = (cur.x >> 11) & 3u, k3 = (cur.x >> 13) & 3u;
+      const uint32_t i1 = cur.y & 0xffffu, i2 = cur.y >> 16, i3 = cur.x >> 16;
       switch (op) {
         case A_MOV:
 #pragma unroll
@@ -122,6 +147,21 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, int64_t* t
             acc[k] = c ? t : e;
           }
           break;
+        case A_ADD:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = wrap_add(acc[k], fetch(k1, i1, k));
+          break;
+        case A_SUB:
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int64_t b = fetch(k1, i1, k);
+            acc[k] = swap ? wrap_sub(b, acc[k]) : wrap_sub(acc[k], b);
+          }
+          break;
+        case A_MUL:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = wrap_mul(acc[k], fetch(k1, i1, k));
+          break;
         default: {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
@@ -129,9 +169,6 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, int64_t* t
             const int64_t x = swap ? b : acc[k], y = swap ? acc[k] : b;
             int64_t r;
             switch (op) {
-              case A_ADD: r = wrap_add(x, y); break;
-              case A_SUB: r = wrap_sub(x, y); break;
-              case A_MUL: r = wrap_mul(x, y); break;
               case A_LT: r = x < y; break;
               case A_LE: r = x <= y; break;
               case A_GT: r = x > y; break;
@@ -158,6 +195,7 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, int64_t* t
       if (c < C) loss += case_loss(s, s.slot_type, acc[k], __ldg(&s.expected[c]), wrong);
     }
   }
+  __syncwarp();
   loss_out = loss;
   wrong_out = wrong;
   ops_out = uint64_t(len) * uint64_t(C);
