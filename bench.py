@@ -239,9 +239,14 @@ def run_own_arm(args, rank: int, world: int, local: int):
             lt = T.load(tp, sp)
             t0 = time.perf_counter()
             s = eng.admit(lt)
+            t_admit = time.perf_counter()
             s.run()
-            res = s.result()
+            t_run = time.perf_counter()
+            res = s.result_buffer()
             e2e_secs = time.perf_counter() - t0
+            res = {"program_cases": int(res.struct.program_cases)}
+            e2e_parts = {"admit_s": t_admit - t0, "run_s": t_run - t_admit, "result_s": e2e_secs - (t_run - t0)}
+            e2e_counters = eng.counters(s)
             s.close()
             h2d = lt.cases.inputs.nbytes + lt.cases.expected.nbytes + len(lt.tables.minimum) * 4 + \
                 len(lt.tables.expressions) * 80
@@ -249,7 +254,8 @@ def run_own_arm(args, rank: int, world: int, local: int):
                 (WORKLOAD["generations"] + WORKLOAD["population"]) * (lt.tables.max_nodes - lt.tables.fixed_nodes) * 12
             e2e = {"value": res["program_cases"] / e2e_secs, "unit": UNIT,
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": e2e_secs,
-                   "step": "one whole search (admission + %d rounds + result)" % WORKLOAD["generations"]}
+                   "step": "one whole search (admission + %d rounds + result)" % WORKLOAD["generations"],
+                   "parts": e2e_parts, "place_levels": e2e_counters.get("place_levels")}
             # device-timed rounds
             lt = T.load(tp, sp)
             s = eng.admit(lt)
@@ -290,7 +296,10 @@ def run_own_arm(args, rank: int, world: int, local: int):
             "roofline": roofline_entry(stats, after, peaks()), "clocks": clocks.summary(),
             "counters": {"program_cases": cases, "evaluated_programs": after["evaluated_programs"] - before["evaluated_programs"],
                          "reused_programs": after["reused_programs"] - before["reused_programs"],
-                         "vm_ops": after["vm_ops"] - before["vm_ops"]}}
+                         "vm_ops": after["vm_ops"] - before["vm_ops"],
+                         "place_cycles_per_step": {k: (after[k] - before[k]) / args.steps for k in
+                                                   ("place_generate_cycles", "place_stage_cycles",
+                                                    "place_serial_cycles", "place_levels")}}}
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as d:
             make_task(seed, d)

@@ -152,13 +152,12 @@ gagp_status ensure_lists(gagp_engine* e, size_t items) {
   return GAGP_OK;
 }
 
-// Highest cases-per-lane the VM uses for `cases` (autotuned by case count:
-// the fewest warp passes with at most 8 cases per lane).
+// Cases per lane of the fast VM for `cases` (the fewest warp passes with at
+// most 4 cases per lane, the register budget of two resident blocks per SM).
 int cases_per_lane(int cases) {
   if (cases <= 32) return 1;
   if (cases <= 64) return 2;
-  if (cases <= 128) return 4;
-  return 8;
+  return 4;
 }
 
 int bits_for(uint64_t v) {
@@ -217,7 +216,7 @@ struct Plan {
   Layout L;
   size_t ex, info, prods, nts, doms, vals, minimum, local_types, inputs, expected;
   size_t node, cval, len, cnode, ccval, clen;
-  size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
+  size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval, c_victim;
   size_t code, code_len, kpool, code_temps, bc, bc_len, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, round, hist_sum, hist_fitness, hist_wrong,
       hist_nodes, hist_node, hist_cval, hist_len, counters;
@@ -259,7 +258,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.key = L.take(8 * size_t(P));
   p.c_parent = L.take(4 * size_t(B)); p.c_reuse = L.take(4 * size_t(B)); p.c_error = L.take(4 * size_t(B));
   p.c_fitness = L.take(8 * size_t(B)); p.c_wrong = L.take(4 * size_t(B)); p.c_nodes = L.take(4 * size_t(B));
-  p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
+  p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B)); p.c_victim = L.take(4 * size_t(B));
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
   p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots);
@@ -271,7 +270,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   const size_t H = size_t(cfg->generations);
   p.hist_sum = L.take(8 * H); p.hist_fitness = L.take(8 * H); p.hist_wrong = L.take(4 * H);
   p.hist_nodes = L.take(4 * H); p.hist_node = L.take(8 * S * H); p.hist_cval = L.take(8 * S * H);
-  p.hist_len = L.take(4 * H); p.counters = L.take(8 * 4);
+  p.hist_len = L.take(4 * H); p.counters = L.take(8 * 8);
   return p;
 }
 
@@ -304,7 +303,7 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   size_t free_bytes = 0, total = 0;
   CUDA_TRY(cudaMemGetInfo(&free_bytes, &total));
   e->arena_limit = arena_bytes ? arena_bytes : uint64_t(0.8 * double(free_bytes));
-  CUDA_TRY(cudaFuncSetAttribute(gb::k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 8192));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 16384));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vary, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   *out = e.release();
@@ -438,12 +437,14 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
   d.c_fitness = at<double>(b, p.c_fitness); d.c_wrong = at<uint32_t>(b, p.c_wrong);
   d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
+  d.c_victim = at<int32_t>(b, p.c_victim);
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
   d.bc = at<int32_t>(b, p.bc); d.bc_len = at<int32_t>(b, p.bc_len); d.bc_consts = at<int64_t>(b, p.bc_consts);
   d.bc_stride = p.bc_stride;
   d.mt = at<uint64_t>(b, p.mt); d.stream = at<uint64_t>(b, p.stream); d.stream_mod = at<uint32_t>(b, p.stream_mod);
   d.stream_head = at<long long>(b, p.stream_head); d.stream_capacity = p.stream_capacity;
+  d.mod_magic = ~0ULL / uint64_t(s->P);
   d.round_seed = at<uint64_t>(b, p.round_seed);
   d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
   d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
@@ -602,8 +603,10 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v) {
   {
     Timed t(e, KN_PLACE);
     // member keys plus as many 16-bit staged draws as fit (B * replacement + slack)
-    const size_t limit = e->max_smem - 8192;
-    size_t bytes = size_t(v.max_P) * sizeof(uint64_t) + size_t(v.max_draws + 64) * sizeof(uint16_t);
+    const size_t limit = e->max_smem - 16384;  // static shared memory of k_place: ~13 KB
+    // keys, then either the level owners (4 bytes per member) or the staged draws
+    size_t bytes = size_t(v.max_P) * sizeof(uint64_t) +
+                   std::max(size_t(v.max_P) * sizeof(int32_t), size_t(v.max_draws + 64) * sizeof(uint16_t));
     bytes = std::min(bytes, limit);
     gb::k_place<<<v.n, 256, bytes, e->stream>>>(v.d_desc, v.n, int(bytes));
   }
@@ -758,13 +761,13 @@ gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t 
   return st;
 }
 
-gagp_status gagp_b200_search_counters(gagp_engine* e, int32_t id, uint64_t* out4) {
-  if (!e || !out4) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+gagp_status gagp_b200_search_counters(gagp_engine* e, int32_t id, uint64_t* out8) {
+  if (!e || !out8) return fail(GAGP_INVALID_ARGUMENT, "null argument");
   auto it = e->searches.find(id);
   if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
-  CUDA_TRY(cudaMemcpy(out4, it->second->desc.counters, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(out8, it->second->desc.counters, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return GAGP_OK;
 }
 

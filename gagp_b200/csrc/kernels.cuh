@@ -82,8 +82,11 @@ __global__ void k_lower(const SearchDesc* descs, const int32_t* off, int n, int 
     t = LRow{s.cnode + size_t(slot) * s.stride, s.ccval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
   }
   int temps = 0, klen = 0;
-  int len = lower_accumulator(s, t, s.code + size_t(slot) * s.code_stride, s.code_stride,
-                              s.kpool + size_t(slot) * s.stride, &klen, &temps);
+  int len = s.maxv <= 64 ? lower_accumulator<64>(s, t, s.code + size_t(slot) * s.code_stride, s.code_stride,
+                                                 s.kpool + size_t(slot) * s.stride, &klen, &temps)
+                         : lower_accumulator<kMaxLowerNodes>(s, t, s.code + size_t(slot) * s.code_stride,
+                                                             s.code_stride, s.kpool + size_t(slot) * s.stride, &klen,
+                                                             &temps);
   if (len >= 0) {
     // exact bytecode length (a bound of every executed path) must fit the fuel
     int bytecode = 1;
@@ -152,8 +155,7 @@ __global__ void k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* l
     switch (s.vm_cases_per_lane) {
       case 1: run_k<1>(s, p.slot, w, loss, wrong, ops); break;
       case 2: run_k<2>(s, p.slot, w, loss, wrong, ops); break;
-      case 4: run_k<4>(s, p.slot, w, loss, wrong, ops); break;
-      default: run_k<8>(s, p.slot, w, loss, wrong, ops); break;
+      default: run_k<4>(s, p.slot, w, loss, wrong, ops); break;
     }
     loss = warp_sum(loss);
     wrong = warp_sum(wrong);
@@ -244,8 +246,16 @@ __device__ __forceinline__ uint64_t mt_mix(uint64_t upper_src, uint64_t lower_sr
   const uint64_t x = (upper_src & 0xFFFFFFFF80000000ULL) | (lower_src & 0x7FFFFFFFULL);
   return far ^ (x >> 1) ^ ((x & 1) ? 0xB5026F5AA96619E9ULL : 0);
 }
+// x mod P from a multiply-high quotient estimate (Barrett): the estimate
+// is at most two below floor(x / P), so at most two corrections follow.
+__device__ __forceinline__ uint32_t mod_p(uint64_t x, uint64_t magic, uint32_t P) {
+  const uint64_t q = __umul64hi(x, magic);
+  uint64_t r = x - q * P;
+  while (r >= P) r -= P;
+  return uint32_t(r);
+}
 // Twists `mt` (smem, 312 words) using scratch `nw` (312 words) and appends
-// the tempered block to the stream ring at `wp`.
+// the tempered block to the stream ring at stream position `wp`.
 __device__ inline void mt_block(const SearchDesc& s, uint64_t* mt, uint64_t* nw, long long wp) {
   for (int i = threadIdx.x; i < 156; i += blockDim.x) nw[i] = mt_mix(mt[i], mt[i + 1], mt[i + 156]);
   __syncthreads();
@@ -253,23 +263,27 @@ __device__ inline void mt_block(const SearchDesc& s, uint64_t* mt, uint64_t* nw,
   __syncthreads();
   if (threadIdx.x == 0) nw[311] = mt_mix(mt[311], nw[0], nw[155]);
   __syncthreads();
+  const int base = int(wp % s.stream_capacity);
   for (int i = threadIdx.x; i < 312; i += blockDim.x) {
     mt[i] = nw[i];
     const uint64_t out = mt_temper(nw[i]);
-    const long long pos = (wp + i) % s.stream_capacity;
+    int pos = base + i;
+    if (pos >= s.stream_capacity) pos -= s.stream_capacity;
     s.stream[pos] = out;
-    s.stream_mod[pos] = uint32_t(out % uint64_t(s.P));
+    s.stream_mod[pos] = mod_p(out, s.mod_magic, uint32_t(s.P));
   }
   __syncthreads();
 }
 // Serial fallback of one block, for a consumer that ran ahead of the buffer.
 __device__ inline void mt_block_serial(const SearchDesc& s, uint64_t* mt, long long wp) {
   for (int i = 0; i < 312; ++i) mt[i] = mt_mix(mt[i], mt[(i + 1) % 312], mt[(i + 156) % 312]);
+  const int base = int(wp % s.stream_capacity);
   for (int i = 0; i < 312; ++i) {
     const uint64_t out = mt_temper(mt[i]);
-    const long long pos = (wp + i) % s.stream_capacity;
+    int pos = base + i;
+    if (pos >= s.stream_capacity) pos -= s.stream_capacity;
     s.stream[pos] = out;
-    s.stream_mod[pos] = uint32_t(out % uint64_t(s.P));
+    s.stream_mod[pos] = mod_p(out, s.mod_magic, uint32_t(s.P));
   }
 }
 
@@ -402,30 +416,99 @@ __global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int
   s.c_key[b] = pack_key(s, f, w, nodes);
 }
 
+// Windowed placement step over lanes [seg_begin, seg_end) of a window whose
+// children's draws do not overlap (every lane's members differ from every
+// earlier active lane's): victims from the current keys equal the
+// sequential ones, the best member before each lane is an exclusive prefix
+// minimum of (key, member), and the lanes commit up to the first whose
+// victim is the current best (a redraw).  Returns the committed count.
+__device__ __forceinline__ int place_segment(uint64_t* keys, int32_t* placed, int b0, int seg_begin, int seg_end,
+                                             int d0, int d1, uint64_t ck, int& best, uint64_t& best_key) {
+  const int lane = threadIdx.x & 31;
+  const bool live = lane >= seg_begin && lane < seg_end;
+  const uint64_t k0 = live ? keys[d0] : 0, k1 = live ? keys[d1] : 0;
+  // worst of the pair: the second replaces the first when the first is better
+  const int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
+  uint64_t pk = live ? ck : ~0ULL;
+  int pv = live ? v : 0x7fffffff;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t uk = __shfl_up_sync(kFull, pk, o);
+    const int uv = __shfl_up_sync(kFull, pv, o);
+    if (lane >= o && (uk < pk || (uk == pk && uv < pv))) { pk = uk; pv = uv; }
+  }
+  uint64_t ek = __shfl_up_sync(kFull, pk, 1);
+  int ev = __shfl_up_sync(kFull, pv, 1);
+  if (lane == 0 || best_key < ek || (best_key == ek && best < ev)) { ek = best_key; ev = best; }
+  const unsigned rmask = __ballot_sync(kFull, live && v == ev);
+  const int stop = rmask ? __ffs(rmask) - 1 : seg_end;
+  const int valid = stop - seg_begin;
+  if (valid <= 0) return 0;
+  if (live && lane < stop) {
+    keys[v] = ck;
+    placed[v] = b0 + lane;
+  }
+  uint64_t nk = __shfl_sync(kFull, pk, stop - 1);
+  int nv = __shfl_sync(kFull, pv, stop - 1);
+  if (best_key < nk || (best_key == nk && best < nv)) { nk = best_key; nv = best; }
+  best_key = nk;
+  best = nv;
+  __syncwarp();
+  return valid;
+}
+
+// Lanes of a 32-child window whose draws overlap an earlier lane's: bit j
+// set when child j draws a member that some child i < j of the window drew.
+__device__ __forceinline__ int latest_overlap(int d0, int d1) {
+  const int lane = threadIdx.x & 31;
+  int latest = -1;
+#pragma unroll 8
+  for (int o = 1; o < 32; ++o) {
+    const int e0 = __shfl_up_sync(kFull, d0, o), e1 = __shfl_up_sync(kFull, d1, o);
+    if (lane >= o && ((e0 == d0) | (e0 == d1) | (e1 == d0) | (e1 == d1))) latest = max(latest, lane - o);
+  }
+  return latest;
+}
+
 // Steady-state placement (evolve.cpp:414-427): children in order, each
 // replacing the worst of replacement_size uniform draws (redrawn when it is
-// the current best).  The block pre-generates the run generator's outputs
-// and stages their residues mod P as 16-bit draws in shared memory beside
-// the members' ranking keys; one thread then runs the sequential placement.
-// With the default replacement size 2 the next child's draws and keys are
-// loaded one child ahead and the current child's key store is forwarded to
-// them when they name the replaced member, so shared-memory latency leaves
-// the dependency chain.  Then the next round's seed is drawn.  One block per
-// search; `dyn_bytes`: dynamic shared memory of the launch.
+// the current best).  One block per search; `dyn_bytes`: dynamic shared
+// memory of the launch (member keys, then the level owners or staged draws).
+//
+// Level-parallel path (replacement size 2): without a redraw child j draws
+// stream positions 2j and 2j+1.  A child is ready once it is the earliest
+// unplaced child drawing each of its members; the ready children of a level
+// draw disjoint members, so they read exactly the keys the sequential loop
+// would and place at once.  The best member before each child is then a
+// prefix minimum of (key, member) in child order; a child whose victim is
+// that best member would have redrawn (both its draws are the best member),
+// and then the round is replayed on the exact windowed path.
+//
+// Windowed path (warp 0): 32 children per step, one per lane, over draws
+// staged in shared memory; a step commits the lanes before the first lane
+// drawing a member an earlier lane drew, or before the first redraw, which
+// the sequential loop then takes.  Other replacement sizes and the end of
+// the staged draws run the sequential loop.
+// Finally the next round's seed is drawn.
 __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
   extern __shared__ __align__(16) uint64_t keys[];
   __shared__ uint64_t mt[312], nw[312];
+  __shared__ uint64_t ck_stage[1024];
+  __shared__ uint64_t scan_key[256];
+  __shared__ int scan_idx[256];
+  __shared__ long long shared_pos, shared_wp;
+  __shared__ int shared_best, shared_fail, level_ready, level_left, redraw_at;
   const SearchDesc& s = descs[blockIdx.x];
   if (!search_live(s)) return;
+  const long long t0 = clock64();
   const int P = s.P, B = s.B, rs = s.replacement_size, cap = s.stream_capacity;
-  uint16_t* draws = reinterpret_cast<uint16_t*>(keys + P);
-  const int slots = (dyn_bytes - int(sizeof(uint64_t)) * P) / int(sizeof(uint16_t));
+  const int tid = threadIdx.x;
   int32_t* __restrict__ placed = s.placed;
-  for (int m = threadIdx.x; m < P; m += blockDim.x) {
+  for (int m = tid; m < P; m += blockDim.x) {
     keys[m] = s.key[m];
     placed[m] = -1;
   }
-  for (int i = threadIdx.x; i < 312; i += blockDim.x) mt[i] = s.mt[i];
+  for (int i = tid; i < 312; i += blockDim.x) mt[i] = s.mt[i];
   __syncthreads();
   const long long rp = stream_ptrs(s)[0];
   long long wp = stream_ptrs(s)[1];
@@ -434,105 +517,276 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
     mt_block(s, mt, nw, wp);
     wp += 312;
   }
+  const long long t1 = clock64();
+  // ---------------------------------------------------- level-parallel path
+  constexpr int kPerThread = 64;
+  int32_t* owner = reinterpret_cast<int32_t*>(keys + P);
+  const bool parallel_path = rs == 2 && blockDim.x == 256 && B <= 256 * kPerThread && wp - rp >= need &&
+                             dyn_bytes >= int(sizeof(uint64_t) + sizeof(int32_t)) * P;
+  bool parallel_done = false;
+  if (parallel_path) {
+    const int base = int(rp % cap);
+    uint32_t cand[kPerThread];
+    uint64_t pending = 0;
+#pragma unroll
+    for (int t = 0; t < kPerThread; ++t) {
+      const int j = tid + 256 * t;
+      cand[t] = 0;
+      if (j < B) {
+        int p0 = base + 2 * j, p1 = p0 + 1;
+        if (p0 >= cap) p0 -= cap;
+        if (p1 >= cap) p1 -= cap;
+        cand[t] = s.stream_mod[p0] | (s.stream_mod[p1] << 16);
+        pending |= 1ULL << t;
+      }
+    }
+    if (tid == 0) {
+      level_left = B;
+      redraw_at = 0x7fffffff;
+    }
+    __syncthreads();
+    int levels_run = 0;
+    for (int level = 0; level <= B; ++level) {
+      ++levels_run;
+#pragma unroll
+      for (int t = 0; t < kPerThread; ++t)
+        if (pending >> t & 1) {
+          owner[cand[t] & 0xffff] = 0x7fffffff;
+          owner[cand[t] >> 16] = 0x7fffffff;
+        }
+      if (tid == 0) level_ready = 0;
+      __syncthreads();
+#pragma unroll
+      for (int t = 0; t < kPerThread; ++t)
+        if (pending >> t & 1) {
+          const int j = tid + 256 * t;
+          atomicMin(&owner[cand[t] & 0xffff], j);
+          atomicMin(&owner[cand[t] >> 16], j);
+        }
+      __syncthreads();
+      int ready = 0;
+#pragma unroll
+      for (int t = 0; t < kPerThread; ++t)
+        if (pending >> t & 1) {
+          const int j = tid + 256 * t;
+          const int d0 = int(cand[t] & 0xffff), d1 = int(cand[t] >> 16);
+          if (owner[d0] == j && owner[d1] == j) {
+            const uint64_t k0 = keys[d0], k1 = keys[d1];
+            // worst of the pair: the second replaces the first when the first is better
+            const int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
+            keys[v] = s.c_key[j];
+            placed[v] = j;
+            s.c_victim[j] = v;
+            pending &= ~(1ULL << t);
+            ++ready;
+          }
+        }
+      if (ready) atomicAdd(&level_ready, ready);
+      __syncthreads();
+      if (tid == 0) level_left -= level_ready;
+      __syncthreads();
+      if (level_left == 0) break;
+    }
+    // best member before each child (child order): thread t scans children
+    // [64t, 64t+64); a block scan of the per-thread minima gives each
+    // thread's incoming best
+    const int begin = tid * kPerThread, stop = min(B, begin + kPerThread);
+    uint64_t mk = ~0ULL;
+    int mv = 0x7fffffff;
+    for (int j = begin; j < stop; ++j) {
+      const uint64_t k = s.c_key[j];
+      const int v = s.c_victim[j];
+      if (k < mk || (k == mk && v < mv)) { mk = k; mv = v; }
+    }
+    scan_key[tid] = mk;
+    scan_idx[tid] = mv;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+      uint64_t uk = 0;
+      int uv = 0;
+      const bool take = tid >= o;
+      if (take) { uk = scan_key[tid - o]; uv = scan_idx[tid - o]; }
+      __syncthreads();
+      if (take && (uk < scan_key[tid] || (uk == scan_key[tid] && uv < scan_idx[tid]))) {
+        scan_key[tid] = uk;
+        scan_idx[tid] = uv;
+      }
+      __syncthreads();
+    }
+    const int best0 = s.best[0];
+    const uint64_t best0_key = s.key[best0];
+    int bv = best0;
+    uint64_t bk = best0_key;
+    if (tid > 0 && (scan_key[tid - 1] < bk || (scan_key[tid - 1] == bk && scan_idx[tid - 1] < bv))) {
+      bk = scan_key[tid - 1];
+      bv = scan_idx[tid - 1];
+    }
+    for (int j = begin; j < stop; ++j) {
+      const int v = s.c_victim[j];
+      if (v == bv) { atomicMin(&redraw_at, j); break; }
+      const uint64_t k = s.c_key[j];
+      if (k < bk || (k == bk && v < bv)) { bk = k; bv = v; }
+    }
+    __syncthreads();
+    parallel_done = redraw_at == 0x7fffffff;
+    if (tid == 0)  // levels of the parallel path; a replay adds 2^20
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[7]),
+                (unsigned long long)(B - level_left >= 0 ? levels_run : 0) + (parallel_done ? 0ULL : (1ULL << 20)));
+    if (parallel_done) {
+      if (tid == 0) {
+        int fv = best0;
+        uint64_t fk = best0_key;
+        if (scan_key[255] < fk || (scan_key[255] == fk && scan_idx[255] < fv)) { fk = scan_key[255]; fv = scan_idx[255]; }
+        shared_best = fv;
+        shared_fail = 0;
+        // the next round's seed: the raw output after the 2B placement draws
+        const long long pos = rp + 2LL * B;
+        s.round_seed[0] = s.stream[pos % cap];
+        shared_pos = pos + 1;
+        shared_wp = wp;
+      }
+    } else {
+      // replay the round on the exact windowed path from the round's keys
+      for (int m = tid; m < P; m += blockDim.x) {
+        keys[m] = s.key[m];
+        placed[m] = -1;
+      }
+    }
+    __syncthreads();
+  }
+  // ---------------------------------------------------- windowed path
+  uint16_t* draws = reinterpret_cast<uint16_t*>(keys + P);
+  const int slots = (dyn_bytes - int(sizeof(uint64_t)) * P) / int(sizeof(uint16_t));
   const int avail = int(min((long long)slots, wp - rp));
-  for (int i = threadIdx.x; i < avail; i += blockDim.x) draws[i] = uint16_t(s.stream_mod[(rp + i) % cap]);
+  if (!parallel_done) {
+    const int base = int(rp % cap);
+    for (int i = tid; i < avail; i += blockDim.x) {
+      int pos = base + i;
+      if (pos >= cap) pos -= cap;
+      draws[i] = uint16_t(s.stream_mod[pos]);
+    }
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  const long long t2 = clock64();
+  if (!parallel_done && tid < 32) {
+    const int lane = tid;
     const uint32_t* __restrict__ smod = s.stream_mod;
     const uint64_t* __restrict__ ckey = s.c_key;
     long long gen_wp = wp;
-    // residue of the draw `idx` positions after rp (staged, else the ring)
-    auto draw = [&](int idx) -> int {
-      if (idx < avail) return draws[idx];
-      const long long pos = rp + idx;
-      while (pos >= gen_wp) {  // ran ahead of the buffer: one serial block
+    int best = s.best[0];
+    uint64_t best_key = keys[best];
+    int di = 0, b = 0;
+    int failed = 0;
+    int stage_begin = 0, stage_end = 0;
+    auto stage = [&]() {  // child keys [b, b + 1024) into shared memory
+      __syncwarp();
+      stage_begin = b;
+      stage_end = min(B, b + 1024);
+      for (int i = lane; i < stage_end - stage_begin; i += 32) ck_stage[i] = ckey[stage_begin + i];
+      __syncwarp();
+    };
+    while (b < B && !failed) {
+      while (rs == 2 && b < B && di + 64 <= avail) {
+        if (b + 32 > stage_end) stage();
+        const int cnt = min(32, B - b);
+        const bool live = lane < cnt;
+        const int d0 = live ? int(draws[di + 2 * lane]) : -1 - 2 * lane;
+        const int d1 = live ? int(draws[di + 2 * lane + 1]) : -2 - 2 * lane;
+        const int latest = latest_overlap(d0, d1);
+        const unsigned omask = __ballot_sync(kFull, live && latest >= 0);
+        const int first_overlap = omask ? __ffs(omask) - 1 : cnt;
+        const uint64_t ck = live ? ck_stage[b - stage_begin + lane] : ~0ULL;
+        const int valid = place_segment(keys, placed, b, 0, first_overlap, max(d0, 0), max(d1, 0), ck, best,
+                                        best_key);
+        if (valid == 0) break;  // lane 0's victim is the best: the sequential loop redraws
+        b += valid;
+        di += 2 * valid;
+      }
+      if (b >= B) break;
+      // sequential placement (lane 0): one child after a window stop, or every
+      // remaining child past the staged draws / with another replacement size
+      __syncwarp();
+      if (lane == 0) {
+        auto draw = [&](int idx) -> int {
+          if (idx < avail) return draws[idx];
+          const long long pos = rp + idx;
+          while (pos >= gen_wp) {  // ran ahead of the buffer: one serial block
+            mt_block_serial(s, mt, gen_wp);
+            gen_wp += 312;
+          }
+          return int(smod[pos % cap]);
+        };
+        const bool rest = rs != 2 || di + 64 > avail;
+        do {
+          const uint64_t ck = ckey[b];
+          int v = -1;
+          for (int guard = 0; guard < (1 << 20); ++guard) {
+            int worst = draw(di++);
+            uint64_t kw = keys[worst];
+            for (int i = 1; i < rs; ++i) {
+              const int c = draw(di++);
+              const uint64_t kc = keys[c];
+              if (kw < kc || (kw == kc && worst < c)) { worst = c; kw = kc; }
+            }
+            if (worst != best) { v = worst; break; }
+          }
+          if (v < 0) { failed = 1; break; }
+          keys[v] = ck;
+          placed[v] = b;
+          if (ck < best_key || (ck == best_key && v < best)) { best = v; best_key = ck; }
+          ++b;
+        } while (rest && b < B);
+      }
+      __syncwarp();
+      b = __shfl_sync(kFull, b, 0);
+      di = __shfl_sync(kFull, di, 0);
+      best = __shfl_sync(kFull, best, 0);
+      best_key = __shfl_sync(kFull, best_key, 0);
+      gen_wp = __shfl_sync(kFull, gen_wp, 0);
+      failed = __shfl_sync(kFull, failed, 0);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      // the next round's variation seed: the raw output at the next position
+      const long long pos = rp + di;
+      while (pos >= gen_wp) {
         mt_block_serial(s, mt, gen_wp);
         gen_wp += 312;
       }
-      return int(smod[pos % cap]);
-    };
-    int best = s.best[0];
-    uint64_t best_key = keys[best];
-    int di = 0;
-    bool failed = false;
-    if (rs == 2) {
-      int d0 = draw(0), d1 = draw(1);
-      uint64_t k0 = keys[d0], k1 = keys[d1];
-      uint64_t ck = ckey[0];
-      for (int b = 0; b < B; ++b) {
-        di += 2;
-        const uint64_t ck_next = b + 1 < B ? ckey[b + 1] : 0;
-        // worst of the pair: the second replaces the first when the first is better
-        int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
-        for (int guard = 0; v == best; ++guard) {
-          if (guard > (1 << 20)) { failed = true; break; }
-          d0 = draw(di); d1 = draw(di + 1); di += 2;
-          k0 = keys[d0]; k1 = keys[d1];
-          v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
-        }
-        if (failed) break;
-        int n0 = 0, n1 = 0;
-        uint64_t nk0 = 0, nk1 = 0;
-        if (b + 1 < B) {
-          n0 = draw(di);
-          n1 = draw(di + 1);
-          nk0 = keys[n0];
-          nk1 = keys[n1];
-        }
-        keys[v] = ck;
-        placed[v] = b;
-        if (n0 == v) nk0 = ck;
-        if (n1 == v) nk1 = ck;
-        if (ck < best_key || (ck == best_key && v < best)) { best = v; best_key = ck; }
-        d0 = n0; d1 = n1; k0 = nk0; k1 = nk1; ck = ck_next;
-      }
-    } else {
-      for (int b = 0; b < B && !failed; ++b) {
-        const uint64_t ck = ckey[b];
-        int v = -1;
-        for (int guard = 0; guard < (1 << 20); ++guard) {
-          int worst = draw(di++);
-          uint64_t kw = keys[worst];
-          for (int i = 1; i < rs; ++i) {
-            const int c = draw(di++);
-            const uint64_t kc = keys[c];
-            if (kw < kc || (kw == kc && worst < c)) { worst = c; kw = kc; }
-          }
-          if (worst != best) { v = worst; break; }
-        }
-        if (v < 0) { failed = true; break; }
-        keys[v] = ck;
-        placed[v] = b;
-        if (ck < best_key || (ck == best_key && v < best)) { best = v; best_key = ck; }
-      }
+      s.round_seed[0] = s.stream[pos % cap];
+      shared_best = best;
+      shared_pos = pos + 1;
+      shared_wp = gen_wp;
+      shared_fail = failed;
     }
-    if (failed) raise_error(s, 40);
-    // the next round's variation seed: the raw output at the next position
-    const long long pos = rp + di;
-    while (pos >= gen_wp) {
-      mt_block_serial(s, mt, gen_wp);
-      gen_wp += 312;
-    }
-    s.round_seed[0] = s.stream[pos % cap];
-    s.best[0] = best;
-    stream_ptrs(s)[0] = pos + 1;
-    stream_ptrs(s)[1] = gen_wp;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 312; i += blockDim.x) s.mt[i] = mt[i];
-  for (int m = threadIdx.x; m < P; m += blockDim.x) {
-    const int b = placed[m];
-    if (b >= 0) {
+  const long long t3 = clock64();
+  if (tid == 0) {
+    if (shared_fail) raise_error(s, 40);
+    s.best[0] = shared_best;
+    stream_ptrs(s)[0] = shared_pos;
+    stream_ptrs(s)[1] = shared_wp;
+  }
+  for (int i = tid; i < 312; i += blockDim.x) s.mt[i] = mt[i];
+  for (int m = tid; m < P; m += blockDim.x) {
+    const int c = placed[m];
+    if (c >= 0) {
       s.key[m] = keys[m];
-      s.fitness[m] = s.c_fitness[b];
-      s.wrong[m] = s.c_wrong[b];
-      s.nodes[m] = s.c_nodes[b];
+      s.fitness[m] = s.c_fitness[c];
+      s.wrong[m] = s.c_wrong[c];
+      s.nodes[m] = s.c_nodes[c];
     }
   }
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     const int r = s.round[0] + 1;
     s.round[0] = r;
     if (r >= s.total_rounds) s.round[2] = 1;
+    // SM clock cycles of the placement phases: generation, parallel
+    // placement (and draw staging), windowed placement
+    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[4]), (unsigned long long)(t1 - t0));
+    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[5]), (unsigned long long)(t2 - t1));
+    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[6]), (unsigned long long)(t3 - t2));
   }
 }
 

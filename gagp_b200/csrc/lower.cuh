@@ -179,16 +179,18 @@ __device__ __forceinline__ uint32_t accumulator_op(const gagp_expression& e) {
 }
 
 // Accumulator program of a row; returns the instruction count, or -1 when the
-// row needs the general VM.  *temps_out: temporaries used.
+// row needs the general VM.  *temps_out: temporaries used.  MAXN bounds the
+// row length (the per-thread working arrays).
+template <int MAXN>
 __device__ inline int lower_accumulator(const SearchDesc& s, const LRow& t, uint2* code, int code_cap,
                                         int64_t* kpool, int* kpool_len, int* temps_out) {
   (void)kpool_len;
   const int n = t.n;
-  if (n <= 0 || n > kMaxLowerNodes) return -1;
+  if (n <= 0 || n > MAXN) return -1;
   // child positions and Sethi-Ullman temporaries, children after parents
-  int16_t end[kMaxLowerNodes];
-  int8_t need[kMaxLowerNodes];
-  int16_t constant_index[kMaxLowerNodes];
+  int16_t end[MAXN];
+  int8_t need[MAXN];
+  int16_t constant_index[MAXN];
   {
     int k = 0;
     for (int i = 0; i < n; ++i) constant_index[i] = w_const(t.node[i]) ? int16_t(k++) : int16_t(-1);

@@ -76,6 +76,7 @@ struct SearchDesc {
   int32_t* c_parent; int32_t* c_reuse; int32_t* c_error;
   double* c_fitness; uint32_t* c_wrong; uint32_t* c_nodes; uint64_t* c_key;
   int32_t* c_eval;                     // 1: evaluate this child
+  int32_t* c_victim;                   // member each child replaced (level-parallel placement)
   // ---- lowered programs (children, or members during the initial evaluation)
   uint2* code; int32_t* code_len; int64_t* kpool;
   int32_t code_stride;                 // accumulator instructions per program slot
@@ -90,6 +91,7 @@ struct SearchDesc {
   uint32_t* stream_mod;                // outputs % P
   long long* stream_head;              // [0]: outputs read, [1]: outputs written (ring positions)
   int32_t stream_capacity;
+  uint64_t mod_magic;                  // floor((2^64 - 1) / P): exact residues by multiply-high
   uint64_t* round_seed;                // seed of the next round's variation
   // ---- search progress and history
   int32_t* best;                       // tracked best member

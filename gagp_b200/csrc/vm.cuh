@@ -98,17 +98,38 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
       in0[k] = (NIN >= 1 && c < C) ? __ldg(&inputs[c]) : 0;
       in1[k] = (NIN >= 2 && c < C) ? __ldg(&inputs[size_t(C) + c]) : 0;
     }
-    auto fetch = [&](uint32_t kind, uint32_t index, int k) -> int64_t {
+    // operand vector of one instruction: the kind switch is warp-uniform and
+    // taken once per instruction, not once per case
+    auto load = [&](uint32_t kind, uint32_t index, int64_t* v) {
       switch (kind) {
-        case K_ACC: return acc[k];
-        case K_TEMP: return temps[(index * K + k) * 32 + lane];
-        case K_INPUT: {
-          if (NIN == 1) return in0[k];
-          if (NIN == 2) return index ? in1[k] : in0[k];
-          const int c = tile + k * 32 + lane;
-          return c < C ? __ldg(&inputs[size_t(index) * C + c]) : 0;
+        case K_ACC:
+#pragma unroll
+          for (int k = 0; k < K; ++k) v[k] = acc[k];
+          break;
+        case K_TEMP:
+#pragma unroll
+          for (int k = 0; k < K; ++k) v[k] = temps[(index * K + k) * 32 + lane];
+          break;
+        case K_INPUT:
+          if (NIN == 1 || (NIN == 2 && index == 0)) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = in0[k];
+          } else if (NIN == 2) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) v[k] = in1[k];
+          } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+              const int c = tile + k * 32 + lane;
+              v[k] = c < C ? __ldg(&inputs[size_t(index) * C + c]) : 0;
+            }
+          }
+          break;
+        default: {
+          const int64_t x = w.consts[index];
+#pragma unroll
+          for (int k = 0; k < K; ++k) v[k] = x;
         }
-        default: return w.consts[index];
       }
     };
     uint2 ins = len ? w.code[0] : make_uint2(0, 0);
@@ -119,14 +140,17 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
       const bool swap = (cur.x >> 8) & 1u;
       const uint32_t k1 = (cur.x >> 9) & 3u, k2 = (cur.x >> 11) & 3u, k3 = (cur.x >> 13) & 3u;
       const uint32_t i1 = cur.y & 0xffffu, i2 = cur.y >> 16, i3 = cur.x >> 16;
+      if (op == A_SPILL) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) temps[(i1 * K + k) * 32 + lane] = acc[k];
+        continue;
+      }
+      int64_t b[K];
+      if (op != A_NEG && op != A_NOT && op != A_ABS) load(k1, i1, b);
       switch (op) {
         case A_MOV:
 #pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = fetch(k1, i1, k);
-          break;
-        case A_SPILL:
-#pragma unroll
-          for (int k = 0; k < K; ++k) temps[(i1 * K + k) * 32 + lane] = acc[k];
+          for (int k = 0; k < K; ++k) acc[k] = b[k];
           break;
         case A_NEG:
 #pragma unroll
@@ -140,51 +164,71 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] = acc[k] < 0 ? wrap_neg(acc[k]) : acc[k];
           break;
-        case A_SELECT:
+        case A_SELECT: {
+          int64_t t[K], e[K];
+          load(k2, i2, t);
+          load(k3, i3, e);
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int64_t c = fetch(k1, i1, k), t = fetch(k2, i2, k), e = fetch(k3, i3, k);
-            acc[k] = c ? t : e;
-          }
+          for (int k = 0; k < K; ++k) acc[k] = b[k] ? t[k] : e[k];
           break;
+        }
         case A_ADD:
 #pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = wrap_add(acc[k], fetch(k1, i1, k));
+          for (int k = 0; k < K; ++k) acc[k] = wrap_add(acc[k], b[k]);
           break;
         case A_SUB:
+          if (swap) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int64_t b = fetch(k1, i1, k);
-            acc[k] = swap ? wrap_sub(b, acc[k]) : wrap_sub(acc[k], b);
+            for (int k = 0; k < K; ++k) acc[k] = wrap_sub(b[k], acc[k]);
+          } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = wrap_sub(acc[k], b[k]);
           }
           break;
         case A_MUL:
 #pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = wrap_mul(acc[k], fetch(k1, i1, k));
+          for (int k = 0; k < K; ++k) acc[k] = wrap_mul(acc[k], b[k]);
+          break;
+        case A_LT: case A_LE: case A_GT: case A_GE: {
+          // ordered comparison of (x, y) = swap ? (b, acc) : (acc, b)
+          const bool gt = op == A_GT || op == A_GE, eq = op == A_LE || op == A_GE;
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const int64_t x = swap ? b[k] : acc[k], y = swap ? acc[k] : b[k];
+            acc[k] = gt ? (eq ? x >= y : x > y) : (eq ? x <= y : x < y);
+          }
+          break;
+        }
+        case A_EQ:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = acc[k] == b[k];
+          break;
+        case A_NE:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = acc[k] != b[k];
+          break;
+        case A_AND:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] &= b[k];
+          break;
+        case A_OR:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] |= b[k];
+          break;
+        case A_MIN:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = acc[k] < b[k] ? acc[k] : b[k];
+          break;
+        case A_MAX:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = acc[k] > b[k] ? acc[k] : b[k];
           break;
         default: {
 #pragma unroll
           for (int k = 0; k < K; ++k) {
-            const int64_t b = fetch(k1, i1, k);
-            const int64_t x = swap ? b : acc[k], y = swap ? acc[k] : b;
-            int64_t r;
-            switch (op) {
-              case A_LT: r = x < y; break;
-              case A_LE: r = x <= y; break;
-              case A_GT: r = x > y; break;
-              case A_GE: r = x >= y; break;
-              case A_EQ: r = x == y; break;
-              case A_NE: r = x != y; break;
-              case A_AND: r = x & y; break;
-              case A_OR: r = x | y; break;
-              case A_MIN: r = x < y ? x : y; break;
-              case A_MAX: r = x > y ? x : y; break;
-              case A_IDIV0: r = idiv0(x, y); break;
-              case A_IMOD0: r = imod0(x, y); break;
-              case A_TDIV0: r = tdiv0(x, y); break;
-              default: r = tmod0(x, y); break;
-            }
-            acc[k] = r;
+            const int64_t x = swap ? b[k] : acc[k], y = swap ? acc[k] : b[k];
+            acc[k] = op == A_IDIV0 ? idiv0(x, y) : op == A_IMOD0 ? imod0(x, y) : op == A_TDIV0 ? tdiv0(x, y)
+                                                                                               : tmod0(x, y);
           }
         }
       }

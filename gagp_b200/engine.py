@@ -61,11 +61,15 @@ class Search:
         self.engine.run(self)
         return self
 
-    def result(self) -> dict:
+    def result_buffer(self) -> abi.ResultBuffer:
+        """The finished search's history and ranked population, copied into numpy arrays."""
         t, s = self.task.tables, self.task.settings
         res = abi.ResultBuffer(s.generations, s.population, t.max_nodes - t.fixed_nodes)
         _check(load_library().gagp_b200_search_result(self.engine.handle, self.id, res.ref()))
-        return res.summary()
+        return res
+
+    def result(self) -> dict:
+        return self.result_buffer().summary()
 
     def close(self):
         if self.id is not None and self.engine.handle:
@@ -135,9 +139,11 @@ class Engine:
         return ms.value
 
     def counters(self, search: Search) -> dict:
-        out = (C.c_uint64 * 4)()
+        out = (C.c_uint64 * 8)()
         _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out))
-        return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2], "vm_ops": out[3]}
+        return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2], "vm_ops": out[3],
+                "place_generate_cycles": out[4], "place_stage_cycles": out[5], "place_serial_cycles": out[6],
+                "place_levels": out[7]}
 
     def progress(self, search: Search) -> tuple:
         done, total, fin = C.c_int32(), C.c_int32(), C.c_int32()

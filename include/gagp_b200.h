@@ -236,8 +236,10 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
 
 /* Work counters of a search so far: [0] program evaluations, [1] children
  * that reused a member's result, [2] evaluated (program, case) pairs,
- * [3] VM instructions executed over all cases (synchronous). */
-gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out4);
+ * [3] VM instructions executed over all cases, [4..6] SM clock cycles of
+ * the placement phases (stream generation, draw staging, placement),
+ * [7] reserved (synchronous). */
+gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out8);
 
 /* Per-kernel CUDA-event timing: enable (resets) or disable, then read the
  * accumulated time and launch count of kernel index 0.. (INVALID_ARGUMENT
