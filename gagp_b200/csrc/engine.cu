@@ -655,6 +655,211 @@ gagp_status run_batch(gagp_engine* e, const std::vector<Search*>& list) {
 
 }  // namespace
 
+// ======================================================================= row evaluation
+namespace {
+
+// Device layout of one row evaluation: grammar tables, cases, the rows as
+// node words, lowered programs, program lists and outputs, all carved from
+// one caller-provided device region.
+struct EvalPlan {
+  Layout L;
+  size_t desc, ex, info, minimum, local_types, inputs, expected, node, cval, len, code, code_len, kpool, code_temps,
+      bc, bc_len, bc_consts, fitness, wrong, counters, round, fast, general, counts, off;
+  int stride, code_stride, bc_stride;
+};
+
+EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
+  EvalPlan p{};
+  const int maxv = g->max_nodes - g->fixed_nodes;
+  p.stride = int(align_up(size_t(std::max(1, maxv)), 4));
+  p.code_stride = 2 * maxv + 8;
+  int per_node = 1;
+  for (int i = 0; i < g->expression_count; ++i) {
+    const int nk = g->expressions[i].node_kind;
+    if (g->expressions[i].kind == gb::EK_OPERATION)
+      per_node = std::max(per_node, nk == gb::TK_IF ? 2 : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
+  }
+  p.bc_stride = per_node * maxv + 2;
+  const int E = g->expression_count, C = c->case_count;
+  const size_t R = size_t(std::max(1, rows)), S = size_t(p.stride);
+  auto& L = p.L;
+  p.desc = L.take(sizeof(gb::SearchDesc));
+  p.ex = L.take(sizeof(gagp_expression) * E);
+  p.info = L.take(sizeof(gb::ExprInfo) * E);
+  p.minimum = L.take(sizeof(uint32_t));
+  p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
+  p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
+  p.expected = L.take(sizeof(int64_t) * C);
+  p.node = L.take(8 * S * R); p.cval = L.take(8 * S * R); p.len = L.take(4 * R);
+  p.code = L.take(8 * R * p.code_stride); p.code_len = L.take(4 * R); p.kpool = L.take(8 * R * S);
+  p.code_temps = L.take(4 * R);
+  p.bc = L.take(20 * R * p.bc_stride); p.bc_len = L.take(4 * R); p.bc_consts = L.take(8 * R * p.bc_stride);
+  p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.counters = L.take(8 * 8); p.round = L.take(16);
+  p.fast = L.take(sizeof(gb::ProgramRef) * R); p.general = L.take(sizeof(gb::ProgramRef) * R);
+  p.counts = L.take(16); p.off = L.take(8);
+  return p;
+}
+
+gagp_status eval_check(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg,
+                       const gagp_rows* rows) {
+  if (!g || !c || !cfg || !rows) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (cfg->metric != GAGP_METRIC_ABSOLUTE && cfg->metric != GAGP_METRIC_EXACT)
+    return fail(GAGP_DECLINED, "fitness metric outside the resident scalar subset");
+  const double pen = std::fabs(cfg->penalty);
+  if (pen != std::floor(pen) || pen < 1 || pen > 2147483647.0)
+    return fail(GAGP_DECLINED, "a fractional penalty needs the ordered 48-bit reduction");
+  if (c->case_count < 1 || double(c->case_count) * pen >= 281474976710656.0)
+    return fail(GAGP_DECLINED, "cases * penalty must stay below 2^48");
+  if (c->input_count != g->local_count || g->local_count > GAGP_MAX_LOCALS)
+    return fail(GAGP_INVALID_ARGUMENT, "case inputs must cover the grammar inputs");
+  if (g->expression_count < 1 || g->expression_count > 65534) return fail(GAGP_DECLINED, "expression table capacity");
+  const int maxv = g->max_nodes - g->fixed_nodes;
+  if (maxv < 1 || maxv > gb::kMaxLowerNodes) return fail(GAGP_DECLINED, "variable node budget outside 1..256");
+  if (rows->count < 0 || (rows->count && (!rows->node_counts || !rows->origins || !rows->constant_counts)))
+    return fail(GAGP_INVALID_ARGUMENT, "rows");
+  for (int r = 0; r < rows->count; ++r) {
+    const int n = rows->node_counts[r], nc = rows->constant_counts[r];
+    if (n < 1 || n > maxv || nc < 0 || nc > n || n > rows->stride)
+      return fail(GAGP_INVALID_ARGUMENT, "row " + std::to_string(r) + " outside the node budget");
+    for (int i = 0; i < n; ++i) {
+      const int o = rows->origins[size_t(r) * rows->stride + i];
+      if (o < 0 || o >= g->expression_count) return fail(GAGP_INVALID_ARGUMENT, "row origin out of range");
+    }
+  }
+  return GAGP_OK;
+}
+
+// Fills `region` (device, plan.L.total bytes) and evaluates every row on
+// `stream`; results are copied to the host arrays.  No device allocation.
+gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g, const gagp_cases* c,
+                         const gagp_search_config* cfg, const gagp_rows* rows, double* fitness, uint32_t* wrong,
+                         cudaStream_t stream, int sm_count, size_t max_smem) {
+  const int E = g->expression_count, C = c->case_count, NI = c->input_count, R = rows->count;
+  if (R == 0) return GAGP_OK;
+  char* b = region;
+  std::vector<gb::ExprInfo> info(E);
+  for (int i = 0; i < E; ++i) {
+    const gagp_expression& x = g->expressions[i];
+    gb::ExprInfo& f = info[i];
+    f.kind = int8_t(x.kind);
+    f.node_kind = int8_t(x.node_kind);
+    f.arity = int8_t(x.kind == gb::EK_REFERENCE ? 0 : x.arity);
+    f.type = int8_t(x.type);
+    f.opcode = int16_t(x.opcode);
+    f.operand = x.operand;
+    f.target = x.target;
+    f.site_nt = -1;
+    f.site_class = -1;
+  }
+  std::vector<int64_t> inputs(size_t(std::max(1, NI)) * C, 0);
+  for (int j = 0; j < NI; ++j)
+    for (int k = 0; k < C; ++k) inputs[size_t(j) * C + k] = c->inputs[size_t(k) * NI + j];
+  std::vector<int32_t> local_types(GAGP_MAX_LOCALS, GAGP_TAG_INVALID);
+  for (int j = 0; j < g->local_count; ++j) local_types[j] = g->local_types[j];
+  // rows as node words: evaluation reads the construction expression, arity
+  // and constant flag only
+  const size_t S = size_t(p.stride);
+  std::vector<uint64_t> node(S * R, 0);
+  std::vector<int64_t> cval(S * R, 0);
+  std::vector<int32_t> len(R);
+  for (int r = 0; r < R; ++r) {
+    const int n = rows->node_counts[r], nc = rows->constant_counts[r];
+    for (int i = 0; i < n; ++i) {
+      const int o = rows->origins[size_t(r) * rows->stride + i];
+      const gagp_expression& x = g->expressions[o];
+      node[S * r + i] = uint64_t(uint32_t(o)) | (uint64_t(uint32_t(x.arity) & 0xfu) << 48) |
+                        (uint64_t(x.kind == gb::EK_CONSTANT) << 52) | (uint64_t(gb::kNoClass) << 53);
+    }
+    for (int k = 0; k < nc; ++k) cval[S * r + k] = rows->constants[size_t(r) * rows->stride + k];
+    len[r] = n | (nc << 16);
+  }
+  gb::SearchDesc d{};
+  d.ex = at<gagp_expression>(b, p.ex);
+  d.info = at<gb::ExprInfo>(b, p.info);
+  d.minimum = at<uint32_t>(b, p.minimum);
+  d.local_types = at<int32_t>(b, p.local_types);
+  d.n_ex = E;
+  d.slot_type = g->slot_type;
+  d.local_count = g->local_count;
+  d.max_nodes = g->max_nodes;
+  d.fixed_nodes = g->fixed_nodes;
+  d.return_fuel = g->return_fuel;
+  d.P = R;
+  d.B = 1;
+  d.maxv = g->max_nodes - g->fixed_nodes;
+  d.stride = p.stride;
+  d.has_wrong = 1;
+  d.metric = cfg->metric;
+  d.fuel = cfg->fuel;
+  d.penalty = cfg->penalty;
+  d.penalty_int = (int64_t)std::fabs(cfg->penalty);
+  d.inputs = at<int64_t>(b, p.inputs);
+  d.expected = at<int64_t>(b, p.expected);
+  d.C = C;
+  d.n_inputs = NI;
+  d.expected_tag = c->expected_tag;
+  d.vm_cases_per_lane = cases_per_lane(C);
+  d.node = at<uint64_t>(b, p.node);
+  d.cval = at<int64_t>(b, p.cval);
+  d.len = at<int32_t>(b, p.len);
+  d.code = at<uint2>(b, p.code);
+  d.code_len = at<int32_t>(b, p.code_len);
+  d.kpool = at<int64_t>(b, p.kpool);
+  d.code_stride = p.code_stride;
+  d.code_temps = at<int32_t>(b, p.code_temps);
+  d.bc = at<int32_t>(b, p.bc);
+  d.bc_len = at<int32_t>(b, p.bc_len);
+  d.bc_consts = at<int64_t>(b, p.bc_consts);
+  d.bc_stride = p.bc_stride;
+  d.fitness = at<double>(b, p.fitness);
+  d.wrong = at<uint32_t>(b, p.wrong);
+  d.counters = at<uint64_t>(b, p.counters);
+  d.round = at<int32_t>(b, p.round);
+  const int32_t off[2] = {0, R};
+  auto up = [&](size_t at_off, const void* src, size_t bytes) {
+    return cudaMemcpyAsync(b + at_off, src, bytes, cudaMemcpyHostToDevice, stream);
+  };
+  CUDA_TRY(up(p.desc, &d, sizeof d));
+  CUDA_TRY(up(p.ex, g->expressions, sizeof(gagp_expression) * E));
+  CUDA_TRY(up(p.info, info.data(), sizeof(gb::ExprInfo) * E));
+  CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
+  CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
+  CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
+  CUDA_TRY(up(p.node, node.data(), 8 * node.size()));
+  CUDA_TRY(up(p.cval, cval.data(), 8 * cval.size()));
+  CUDA_TRY(up(p.len, len.data(), 4 * len.size()));
+  CUDA_TRY(up(p.off, off, sizeof off));
+  CUDA_TRY(cudaMemsetAsync(b + p.counters, 0, 8 * 8, stream));
+  CUDA_TRY(cudaMemsetAsync(b + p.round, 0, 16, stream));
+  CUDA_TRY(cudaMemsetAsync(b + p.counts, 0, 16, stream));
+  const gb::SearchDesc* dd = at<gb::SearchDesc>(b, p.desc);
+  const int32_t* doff = at<int32_t>(b, p.off);
+  gb::ProgramRef* fast = at<gb::ProgramRef>(b, p.fast);
+  gb::ProgramRef* general = at<gb::ProgramRef>(b, p.general);
+  int32_t* counts = at<int32_t>(b, p.counts);
+  gb::k_lower<<<blocks_for(R, 128), 128, 0, stream>>>(dd, doff, 1, 0, fast, general, counts);
+  const int warps = 8;
+  const int lanes = d.vm_cases_per_lane;
+  const int temp_stride = gb::kMaxTemps * lanes * 32;
+  const int code_stride = (p.code_stride + 1) & ~1;
+  const size_t smem = size_t(warps) * (temp_stride + code_stride + p.stride) * sizeof(int64_t);
+  if (smem > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the VM's shared memory");
+  const int per_sm = std::max(1, std::min(4, int((max_smem - 1024) / smem)));
+  gb::k_vm_fast<<<sm_count * per_sm, warps * 32, smem, stream>>>(dd, 0, fast, counts, temp_stride, code_stride,
+                                                                  p.stride);
+  gb::k_vm_general<<<sm_count * 4, 128, 0, stream>>>(dd, 0, general, counts + 1);
+  CUDA_TRY(cudaGetLastError());
+  int32_t round[4];
+  CUDA_TRY(cudaMemcpyAsync(round, b + p.round, sizeof round, cudaMemcpyDeviceToHost, stream));
+  CUDA_TRY(cudaMemcpyAsync(fitness, b + p.fitness, 8 * size_t(R), cudaMemcpyDeviceToHost, stream));
+  if (wrong) CUDA_TRY(cudaMemcpyAsync(wrong, b + p.wrong, 4 * size_t(R), cudaMemcpyDeviceToHost, stream));
+  CUDA_TRY(cudaStreamSynchronize(stream));
+  if (round[3]) return fail(GAGP_DEVICE_ERROR, "row evaluation failed on the device (code " + std::to_string(round[3]) + ")");
+  return GAGP_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 gagp_status gagp_b200_search_run(gagp_engine* e, int32_t id) {
@@ -804,6 +1009,22 @@ gagp_status gagp_b200_search_progress(gagp_engine* e, int32_t id, int32_t* round
   if (finished) *finished = round[2];
   if (round[3]) return fail(GAGP_DEVICE_ERROR, "search failed on the device (code " + std::to_string(round[3]) + ")");
   return GAGP_OK;
+}
+
+gagp_status gagp_b200_evaluate_rows(gagp_engine* e, const gagp_grammar* grammar, const gagp_cases* cases,
+                                    const gagp_search_config* config, const gagp_rows* rows, double* fitness,
+                                    uint32_t* wrong) {
+  if (!e || !fitness) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  gagp_status st = eval_check(grammar, cases, config, rows);
+  if (st != GAGP_OK) return st;
+  CUDA_TRY(cudaSetDevice(e->device));
+  const EvalPlan p = plan_eval(grammar, cases, rows->count);
+  char* region = nullptr;
+  CUDA_TRY(cudaMalloc(&region, p.L.total));
+  st = eval_rows_in(region, p, grammar, cases, config, rows, fitness, wrong, e->stream, e->sm_count, e->max_smem);
+  cudaFree(region);
+  return st;
 }
 
 gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_result* out) {

@@ -39,7 +39,7 @@ def load_library():
                      "gagp_b200_search_destroy", "gagp_b200_search_run", "gagp_b200_batch_run",
                      "gagp_b200_batch_step", "gagp_b200_search_result", "gagp_b200_batch_start",
                      "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters",
-                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats"):
+                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_evaluate_rows"):
             getattr(lib, name).restype = C.c_int32
         lib.gagp_b200_engine_destroy.restype = None
         _lib = lib
@@ -165,3 +165,14 @@ class Engine:
             out[name.value.decode()] = {"ms": ms.value, "launches": n.value}
             i += 1
         return out
+
+    def evaluate_rows(self, task: LoadedTask, rows: abi.RowsBuffer):
+        """Fitness and wrong counts of transport rows on the task's cases."""
+        g = abi.GrammarBlob(task.tables)
+        cfg = task.settings.struct()
+        fitness = np.zeros(rows.count, dtype=np.float64)
+        wrong = np.zeros(rows.count, dtype=np.uint32)
+        _check(load_library().gagp_b200_evaluate_rows(self.handle, g.ref(), task.cases.ref(), C.byref(cfg), rows.ref(),
+                                                      fitness.ctypes.data_as(C.POINTER(C.c_double)),
+                                                      wrong.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return fitness, wrong

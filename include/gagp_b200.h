@@ -248,6 +248,17 @@ gagp_status gagp_b200_engine_profile(gagp_engine* engine, int32_t enable);
 gagp_status gagp_b200_engine_kernel_stats(gagp_engine* engine, int32_t kernel, const char** name,
                                           double* total_ms, int64_t* launches);
 
+/* Fitness and wrong-case counts of phase rows (host `rows`) on a case set:
+ * each row is lowered on the device and run on every case, with the case
+ * scores of `config` (metric, penalty, fuel).  Replaces the reference's
+ * evaluator call over lowered owner programs, FitnessSessionGpu::eval_programs
+ * (cpp/include/gagp/runtime/gpu/fitness_gpu.hpp:91-121) as the resident owner
+ * uses it (NativePhasePopulation::evaluate, phase_population.cu:637-664).
+ * fitness[rows->count], wrong[rows->count] (wrong may be null). */
+gagp_status gagp_b200_evaluate_rows(gagp_engine* engine, const gagp_grammar* grammar, const gagp_cases* cases,
+                                    const gagp_search_config* config, const gagp_rows* rows, double* fitness,
+                                    uint32_t* wrong);
+
 /* Copies a finished search's history and final ranked population out. */
 gagp_status gagp_b200_search_result(gagp_engine* engine, int32_t search, gagp_search_result* out);
 
