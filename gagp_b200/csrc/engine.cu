@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -860,6 +861,49 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
 
 }  // namespace
 
+// ======================================================================= evaluation without device allocation
+namespace {
+
+// Device scratch of gagp_b200_evaluate_rows_static: every device that loads
+// this library holds these bytes until the process exits.  In host code the
+// name is only a handle for the symbol; its device address comes from
+// cudaGetSymbolAddress (static_scratch_on).
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+struct StaticDevice {
+  bool ready = false;
+  char* scratch = nullptr;  // device address of g_static_scratch on this device
+  int sm_count = 0;
+  size_t max_smem = 0;
+};
+std::mutex g_static_mutex;
+std::map<int, StaticDevice> g_static_devices;
+
+// Once per device, with that device current: the scratch's device address,
+// the SM count and the VM kernel's shared-memory opt-in.
+gagp_status static_scratch_on(int device, StaticDevice** out) {
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  StaticDevice& d = g_static_devices[device];
+  if (!d.ready) {
+    void* ptr = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (rc != cudaSuccess) return fail(GAGP_DEVICE_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(rc));
+    int sms = 0, smem = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    CUDA_TRY(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
+    d.scratch = static_cast<char*>(ptr);
+    d.sm_count = sms;
+    d.max_smem = size_t(smem);
+    d.ready = true;
+  }
+  *out = &d;
+  return GAGP_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 gagp_status gagp_b200_search_run(gagp_engine* e, int32_t id) {
@@ -1025,6 +1069,29 @@ gagp_status gagp_b200_evaluate_rows(gagp_engine* e, const gagp_grammar* grammar,
   st = eval_rows_in(region, p, grammar, cases, config, rows, fitness, wrong, e->stream, e->sm_count, e->max_smem);
   cudaFree(region);
   return st;
+}
+
+// Row evaluation for callers that may not allocate device memory: it runs the
+// same lowering and VM kernels as gagp_b200_evaluate_rows, but every device
+// buffer lives in the static scratch above.  See include/gagp_b200.h.
+gagp_status gagp_b200_evaluate_rows_static(const gagp_grammar* grammar, const gagp_cases* cases,
+                                           const gagp_search_config* config, const gagp_rows* rows,
+                                           double* fitness, uint32_t* wrong, void* stream) {
+  if (!fitness) return fail(GAGP_INVALID_ARGUMENT, "null fitness output");
+  gagp_status st = eval_check(grammar, cases, config, rows);
+  if (st != GAGP_OK) return st;
+  const EvalPlan p = plan_eval(grammar, cases, rows->count);
+  if (p.L.total > kStaticScratchBytes)
+    return fail(GAGP_INVALID_ARGUMENT, "this evaluation needs " + std::to_string(p.L.total) +
+                                           " bytes of device scratch; the static scratch holds " +
+                                           std::to_string(kStaticScratchBytes) +
+                                           " bytes: evaluate fewer rows or cases per call");
+  int device = 0;
+  CUDA_TRY(cudaGetDevice(&device));
+  StaticDevice* d = nullptr;
+  if ((st = static_scratch_on(device, &d)) != GAGP_OK) return st;
+  return eval_rows_in(d->scratch, p, grammar, cases, config, rows, fitness, wrong,
+                      static_cast<cudaStream_t>(stream), d->sm_count, d->max_smem);
 }
 
 gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_result* out) {

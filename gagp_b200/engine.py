@@ -39,7 +39,8 @@ def load_library():
                      "gagp_b200_search_destroy", "gagp_b200_search_run", "gagp_b200_batch_run",
                      "gagp_b200_batch_step", "gagp_b200_search_result", "gagp_b200_batch_start",
                      "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters",
-                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_evaluate_rows"):
+                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_evaluate_rows",
+                     "gagp_b200_evaluate_rows_static"):
             getattr(lib, name).restype = C.c_int32
         lib.gagp_b200_engine_destroy.restype = None
         _lib = lib
@@ -176,3 +177,19 @@ class Engine:
                                                       fitness.ctypes.data_as(C.POINTER(C.c_double)),
                                                       wrong.ctypes.data_as(C.POINTER(C.c_uint32))))
         return fitness, wrong
+
+
+def evaluate_rows_static(task: LoadedTask, rows: abi.RowsBuffer, stream: int = 0):
+    """Row evaluation that allocates no device memory (for callers that may not
+    allocate: inside a stream capture, under a foreign allocator, or in a
+    latency-critical loop).  All device buffers live in the library's static
+    32 MiB scratch; larger requests raise EngineError(INVALID_ARGUMENT).  Calls
+    share that scratch, so concurrent calls must be serialized by the caller."""
+    g = abi.GrammarBlob(task.tables)
+    cfg = task.settings.struct()
+    fitness = np.zeros(rows.count, dtype=np.float64)
+    wrong = np.zeros(rows.count, dtype=np.uint32)
+    _check(load_library().gagp_b200_evaluate_rows_static(
+        g.ref(), task.cases.ref(), C.byref(cfg), rows.ref(), fitness.ctypes.data_as(C.POINTER(C.c_double)),
+        wrong.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(stream)))
+    return fitness, wrong
