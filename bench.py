@@ -208,12 +208,56 @@ def run_reference_arm(args, rank: int, world: int):
     print(json.dumps(line))
 
 
-def roofline_entry(stats: dict, counters: dict, peak: dict) -> dict:
-    """Roofline of the kernel with the largest device time."""
+# Algorithmic bytes per launch of the bandwidth-bound kernels: the variation
+# and lowering kernels count theirs on the device (search counters 8 and 9);
+# placement reads every member key, resets and writes the placement map, and
+# per child reads its key and two stream draws and writes its placement.
+def algorithmic_bytes(kernel: str, delta: dict, steps: int, population: int, batch: int):
+    if kernel == "k_vary":
+        return delta["vary_bytes"] / steps
+    if kernel == "k_lower":
+        return delta["lower_bytes"] / steps
+    if kernel == "k_place":
+        return population * (8 + 4 + 8) + batch * (8 + 4 + 4 + 4)
+    return None
+
+
+def profiled_traffic(kernel: str):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "%s_poly4_p16384.txt" % kernel)
+    try:
+        for line in open(path):
+            f = line.split()
+            if len(f) == 3 and f[0] == "traffic_bytes_per_launch:" and f[1] == kernel:
+                return float(f[2])
+    except OSError:
+        pass
+    return None
+
+
+def roofline_entry(stats: dict, delta: dict, steps: int, peak: dict) -> dict:
+    """Roofline of the kernel with the largest device time (HBM-bound)."""
     top = max(stats.items(), key=lambda kv: kv[1]["ms"])[0]
-    ms = stats[top]["ms"] / max(1, stats[top]["launches"])
-    entry = {"kernel": top, "avg_launch_ms": ms, "share": stats[top]["ms"] / max(1e-9, sum(v["ms"] for v in stats.values()))}
-    return entry
+    launches = max(1, stats[top]["launches"])
+    ms = stats[top]["ms"] / launches
+    total = sum(v["ms"] for v in stats.values())
+    per_launch = algorithmic_bytes(top, delta, launches, WORKLOAD["population"], WORKLOAD["population"])
+    achieved = per_launch / (ms / 1000.0) / 1e9 if per_launch is not None else None
+    return {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peak["hbm_gbs"] if achieved is not None else None,
+            "traffic": profiled_traffic(top), "algorithmic_bytes_per_launch": per_launch,
+            "avg_launch_ms": ms, "share": stats[top]["ms"] / max(1e-9, total),
+            "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak["source"]}
+
+
+def vm_entry(stats: dict, delta: dict) -> dict:
+    """VM bytecode instructions and program-case evaluations per second of VM kernel time."""
+    ms = sum(stats[k]["ms"] for k in ("k_vm_fast", "k_vm_general") if k in stats)
+    if ms <= 0:
+        return {}
+    return {"kernel_ms": ms, "bytecode_ops_per_s": delta["vm_ops"] / (ms / 1000.0),
+            "program_cases_per_s": delta["program_cases"] / (ms / 1000.0),
+            "ops_per_program_case": delta["vm_ops"] / max(1, delta["program_cases"])}
 
 
 def run_own_arm(args, rank: int, world: int, local: int):
@@ -237,6 +281,7 @@ def run_own_arm(args, rank: int, world: int, local: int):
         with Engine(local if world > 1 else 0) as eng:
             # e2e: a whole search through the C ABI from host buffers
             lt = T.load(tp, sp)
+            moved0 = eng.transfers()
             t0 = time.perf_counter()
             s = eng.admit(lt)
             t_admit = time.perf_counter()
@@ -246,12 +291,10 @@ def run_own_arm(args, rank: int, world: int, local: int):
             e2e_secs = time.perf_counter() - t0
             res = {"program_cases": int(res.struct.program_cases)}
             e2e_parts = {"admit_s": t_admit - t0, "run_s": t_run - t_admit, "result_s": e2e_secs - (t_run - t0)}
+            moved1 = eng.transfers()
             e2e_counters = eng.counters(s)
             s.close()
-            h2d = lt.cases.inputs.nbytes + lt.cases.expected.nbytes + len(lt.tables.minimum) * 4 + \
-                len(lt.tables.expressions) * 80
-            d2h = (WORKLOAD["generations"] * 3 + WORKLOAD["population"] * 4) * 8 + \
-                (WORKLOAD["generations"] + WORKLOAD["population"]) * (lt.tables.max_nodes - lt.tables.fixed_nodes) * 12
+            h2d, d2h = moved1[0] - moved0[0], moved1[1] - moved0[1]
             e2e = {"value": res["program_cases"] / e2e_secs, "unit": UNIT,
                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "seconds": e2e_secs,
                    "step": "one whole search (admission + %d rounds + result)" % WORKLOAD["generations"],
@@ -288,12 +331,14 @@ def run_own_arm(args, rank: int, world: int, local: int):
     if rank != 0:
         return
     launches = sum(v["launches"] for v in stats.values())
+    delta = {k: after[k] - before[k] for k in after}
     line = {"metric": METRIC, "value": cases / secs, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             "config": config_block(world, seed), "e2e": e2e, "gpu_launches": launches,
             "kernels": {k: {"ms_per_step": v["ms"] / args.steps, "launches": v["launches"]} for k, v in stats.items()},
-            "roofline": roofline_entry(stats, after, peaks()), "clocks": clocks.summary(),
+            "vm": vm_entry(stats, delta),
+            "roofline": roofline_entry(stats, delta, args.steps, peaks()), "clocks": clocks.summary(),
             "counters": {"program_cases": cases, "evaluated_programs": after["evaluated_programs"] - before["evaluated_programs"],
                          "reused_programs": after["reused_programs"] - before["reused_programs"],
                          "vm_ops": after["vm_ops"] - before["vm_ops"],

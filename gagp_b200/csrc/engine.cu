@@ -66,6 +66,9 @@ struct Search {
 struct gagp_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // side stream of the run-generator top-up, forked from and joined to `stream`
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   std::map<int, std::unique_ptr<Search>> searches;
   int next_id = 1;
   uint64_t arena_limit = 0, arena_used = 0;
@@ -91,17 +94,31 @@ struct gagp_engine {
   long long kernel_launches[16] = {};
   void* flush_buffer = nullptr;
   size_t flush_bytes = 0;
+  // bytes copied host->device and device->host by this engine's API calls
+  uint64_t h2d_bytes = 0, d2h_bytes = 0;
 };
+
+namespace {
+// Engine copies, counted for gagp_b200_engine_transfers.
+cudaError_t copy_h2d(gagp_engine* e, void* dst, const void* src, size_t bytes) {
+  e->h2d_bytes += bytes;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, e->stream);
+}
+cudaError_t copy_d2h(gagp_engine* e, void* dst, const void* src, size_t bytes) {
+  e->d2h_bytes += bytes;
+  return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+}
+}  // namespace
 
 namespace {
 
 enum KernelId {
   KN_INIT, KN_LOWER, KN_VM_FAST, KN_VM_GENERAL, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
-  KN_COMMIT, KN_COUNT
+  KN_COMMIT, KN_STREAM, KN_COUNT
 };
 const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast", "k_vm_general",
                                             "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
-                                            "k_place", "k_commit"};
+                                            "k_place", "k_commit", "k_stream"};
 
 cudaEvent_t take_event(gagp_engine* e) {
   if (e->event_next == e->event_pool.size()) {
@@ -116,15 +133,16 @@ struct Timed {
   gagp_engine* e;
   int kernel;
   cudaEvent_t stop = nullptr;
-  Timed(gagp_engine* engine, int k) : e(engine), kernel(k) {
+  cudaStream_t stream;
+  Timed(gagp_engine* engine, int k, cudaStream_t on = nullptr) : e(engine), kernel(k), stream(on ? on : engine->stream) {
     if (!e->profiling) return;
     cudaEvent_t start = take_event(e);
     stop = take_event(e);
-    cudaEventRecord(start, e->stream);
+    cudaEventRecord(start, stream);
     e->pending.push_back({kernel, start, stop});
   }
   ~Timed() {
-    if (stop) cudaEventRecord(stop, e->stream);
+    if (stop) cudaEventRecord(stop, stream);
   }
 };
 // Adds the elapsed times of completed launches (after a stream sync).
@@ -271,7 +289,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   const size_t H = size_t(cfg->generations);
   p.hist_sum = L.take(8 * H); p.hist_fitness = L.take(8 * H); p.hist_wrong = L.take(4 * H);
   p.hist_nodes = L.take(4 * H); p.hist_node = L.take(8 * S * H); p.hist_cval = L.take(8 * S * H);
-  p.hist_len = L.take(4 * H); p.counters = L.take(8 * 8);
+  p.hist_len = L.take(4 * H); p.counters = L.take(8 * GAGP_COUNTERS);
   return p;
 }
 
@@ -297,6 +315,9 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   auto e = std::make_unique<gagp_engine>();
   e->device = device;
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming));
   cudaDeviceProp prop;
   CUDA_TRY(cudaGetDeviceProperties(&prop, device));
   e->sm_count = prop.multiProcessorCount;
@@ -328,6 +349,9 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   cudaFree(e->flush_buffer);
   for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
   cudaStreamDestroy(e->stream);
+  if (e->side) cudaStreamDestroy(e->side);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->join) cudaEventDestroy(e->join);
   delete e;
 }
 
@@ -390,7 +414,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   std::vector<int32_t> local_types(GAGP_MAX_LOCALS, GAGP_TAG_INVALID);
   for (int j = 0; j < g->local_count; ++j) local_types[j] = g->local_types[j];
   auto up = [&](size_t off, const void* src, size_t bytes) {
-    return cudaMemcpyAsync(b + off, src, bytes, cudaMemcpyHostToDevice, e->stream);
+    return copy_h2d(e, b + off, src, bytes);
   };
   CUDA_TRY(up(p.ex, g->expressions, sizeof(gagp_expression) * E));
   CUDA_TRY(up(p.info, info.data(), sizeof(gb::ExprInfo) * E));
@@ -464,10 +488,10 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.key_shift_wrong = node_bits + wrong_bits;
   d.total_rounds = s->total_rounds;
   CUDA_TRY(cudaMalloc(&s->d_desc, sizeof(gb::SearchDesc)));
-  CUDA_TRY(cudaMemcpyAsync(s->d_desc, &d, sizeof(gb::SearchDesc), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(copy_h2d(e, s->d_desc, &d, sizeof(gb::SearchDesc)));
   const int32_t off[4] = {0, s->P, 0, s->B};
   CUDA_TRY(cudaMalloc(&s->d_off, sizeof(off)));
-  CUDA_TRY(cudaMemcpyAsync(s->d_off, off, sizeof(off), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(copy_h2d(e, s->d_off, off, sizeof(off)));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   s->id = e->next_id++;
   e->arena_used += s->bytes;
@@ -529,8 +553,8 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
       off[i + 1] = off[i] + list[i]->P;
       off[n + 1 + i + 1] = off[n + 1 + i] + list[i]->B;
     }
-    CUDA_TRY(cudaMemcpyAsync(e->d_batch_desc, descs.data(), sizeof(gb::SearchDesc) * n, cudaMemcpyHostToDevice, e->stream));
-    CUDA_TRY(cudaMemcpyAsync(e->d_batch_off, off.data(), sizeof(int32_t) * off.size(), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(copy_h2d(e, e->d_batch_desc, descs.data(), sizeof(gb::SearchDesc) * n));
+    CUDA_TRY(copy_h2d(e, e->d_batch_off, off.data(), sizeof(int32_t) * off.size()));
     v->d_desc = e->d_batch_desc;
     v->d_member_off = e->d_batch_off;
     v->d_child_off = e->d_batch_off + n + 1;
@@ -588,15 +612,23 @@ gagp_status launch_start(gagp_engine* e, const BatchView& v) {
 }
 
 gagp_status launch_round(gagp_engine* e, const BatchView& v) {
+  // the run-generator top-up overlaps everything up to the placement
+  CUDA_TRY(cudaEventRecord(e->fork, e->stream));
+  CUDA_TRY(cudaStreamWaitEvent(e->side, e->fork, 0));
+  { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
+  CUDA_TRY(cudaEventRecord(e->join, e->side));
   { Timed t(e, KN_RECORD); gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1); }
+  // [0], [1]: lowered-program list sizes; [2]: next child of the variation warps
+  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 3 * sizeof(int32_t), e->stream));
   {
     Timed t(e, KN_VARY);
     const int warps = 4;
     const size_t smem = warps * gb::warp_rows_bytes(v.max_stride);
-    gb::k_vary<<<blocks_for(v.total_children, warps), warps * 32, smem, e->stream>>>(v.d_desc, v.d_child_off, v.n,
-                                                                                     v.max_stride);
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vary, warps * 32, smem));
+    const int blocks = std::min(blocks_for(v.total_children, warps), std::max(1, per_sm) * e->sm_count);
+    gb::k_vary<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, e->d_counts + 2);
   }
-  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
   { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
                                                                          e->d_general, e->d_counts); }
   launch_vm(e, v, 1);
@@ -609,7 +641,8 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v) {
     size_t bytes = size_t(v.max_P) * sizeof(uint64_t) +
                    std::max(size_t(v.max_P) * sizeof(int32_t), size_t(v.max_draws + 64) * sizeof(uint16_t));
     bytes = std::min(bytes, limit);
-    gb::k_place<<<v.n, 256, bytes, e->stream>>>(v.d_desc, v.n, int(bytes));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join, 0));
+    gb::k_place<<<v.n, gb::kPlaceThreads, bytes, e->stream>>>(v.d_desc, v.n, int(bytes));
   }
   { Timed t(e, KN_COMMIT); gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
@@ -629,7 +662,7 @@ gagp_status check_errors(gagp_engine* e, const std::vector<Search*>& list) {
   harvest(e);
   for (Search* s : list) {
     int32_t round[4];
-    CUDA_TRY(cudaMemcpy(round, s->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
+    CUDA_TRY(copy_d2h(e, round, s->desc.round, sizeof(round)));
     if (round[3]) return fail(GAGP_DEVICE_ERROR, "search " + std::to_string(s->id) + " failed on the device (code " + std::to_string(round[3]) + ")");
   }
   return GAGP_OK;
@@ -695,7 +728,7 @@ EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   p.code = L.take(8 * R * p.code_stride); p.code_len = L.take(4 * R); p.kpool = L.take(8 * R * S);
   p.code_temps = L.take(4 * R);
   p.bc = L.take(20 * R * p.bc_stride); p.bc_len = L.take(4 * R); p.bc_consts = L.take(8 * R * p.bc_stride);
-  p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.counters = L.take(8 * 8); p.round = L.take(16);
+  p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.counters = L.take(8 * GAGP_COUNTERS); p.round = L.take(16);
   p.fast = L.take(sizeof(gb::ProgramRef) * R); p.general = L.take(sizeof(gb::ProgramRef) * R);
   p.counts = L.take(16); p.off = L.take(8);
   return p;
@@ -830,7 +863,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   CUDA_TRY(up(p.cval, cval.data(), 8 * cval.size()));
   CUDA_TRY(up(p.len, len.data(), 4 * len.size()));
   CUDA_TRY(up(p.off, off, sizeof off));
-  CUDA_TRY(cudaMemsetAsync(b + p.counters, 0, 8 * 8, stream));
+  CUDA_TRY(cudaMemsetAsync(b + p.counters, 0, 8 * GAGP_COUNTERS, stream));
   CUDA_TRY(cudaMemsetAsync(b + p.round, 0, 16, stream));
   CUDA_TRY(cudaMemsetAsync(b + p.counts, 0, 16, stream));
   const gb::SearchDesc* dd = at<gb::SearchDesc>(b, p.desc);
@@ -950,7 +983,7 @@ gagp_status gagp_b200_batch_step(gagp_engine* e, const int32_t* ids, int32_t cou
   if (finished)
     for (int i = 0; i < count; ++i) {
       int32_t round[4];
-      CUDA_TRY(cudaMemcpy(round, list[i]->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
+      CUDA_TRY(copy_d2h(e, round, list[i]->desc.round, sizeof(round)));
       finished[i] = round[2];
     }
   return GAGP_OK;
@@ -1010,13 +1043,21 @@ gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t 
   return st;
 }
 
-gagp_status gagp_b200_search_counters(gagp_engine* e, int32_t id, uint64_t* out8) {
-  if (!e || !out8) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+gagp_status gagp_b200_engine_transfers(gagp_engine* e, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+  if (!e) return fail(GAGP_INVALID_ARGUMENT, "null engine");
+  if (h2d_bytes) *h2d_bytes = e->h2d_bytes;
+  if (d2h_bytes) *d2h_bytes = e->d2h_bytes;
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_search_counters(gagp_engine* e, int32_t id, uint64_t* out, int32_t count) {
+  if (!e || !out || count < 0) return fail(GAGP_INVALID_ARGUMENT, "null argument or negative count");
+  if (count > GAGP_COUNTERS) count = GAGP_COUNTERS;
   auto it = e->searches.find(id);
   if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
-  CUDA_TRY(cudaMemcpy(out8, it->second->desc.counters, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  CUDA_TRY(copy_d2h(e, out, it->second->desc.counters, size_t(count) * sizeof(uint64_t)));
   return GAGP_OK;
 }
 
@@ -1047,7 +1088,7 @@ gagp_status gagp_b200_search_progress(gagp_engine* e, int32_t id, int32_t* round
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   int32_t round[4];
-  CUDA_TRY(cudaMemcpy(round, it->second->desc.round, sizeof(round), cudaMemcpyDeviceToHost));
+  CUDA_TRY(copy_d2h(e, round, it->second->desc.round, sizeof(round)));
   if (rounds_done) *rounds_done = round[0];
   if (total_rounds) *total_rounds = it->second->total_rounds;
   if (finished) *finished = round[2];
@@ -1103,7 +1144,7 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   const gb::SearchDesc& d = s->desc;
   int32_t round[4];
-  CUDA_TRY(cudaMemcpy(round, d.round, sizeof(round), cudaMemcpyDeviceToHost));
+  CUDA_TRY(copy_d2h(e, round, d.round, sizeof(round)));
   if (round[3]) return fail(GAGP_DEVICE_ERROR, "search failed on the device (code " + std::to_string(round[3]) + ")");
   if (!round[2]) return fail(GAGP_NOT_READY, "search has not finished");
   const int H = std::min(round[1], out->generations);
@@ -1115,13 +1156,13 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   std::vector<int64_t> hc(size_t(H) * S);
   std::vector<int32_t> hl(H);
   if (H) {
-    CUDA_TRY(cudaMemcpy(sum.data(), d.hist_sum, 8 * H, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hf.data(), d.hist_fitness, 8 * H, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hw.data(), d.hist_wrong, 4 * H, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hn.data(), d.hist_nodes, 4 * H, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hnode.data(), d.hist_node, 8 * size_t(H) * S, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hc.data(), d.hist_cval, 8 * size_t(H) * S, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hl.data(), d.hist_len, 4 * H, cudaMemcpyDeviceToHost));
+    CUDA_TRY(copy_d2h(e, sum.data(), d.hist_sum, 8 * H));
+    CUDA_TRY(copy_d2h(e, hf.data(), d.hist_fitness, 8 * H));
+    CUDA_TRY(copy_d2h(e, hw.data(), d.hist_wrong, 4 * H));
+    CUDA_TRY(copy_d2h(e, hn.data(), d.hist_nodes, 4 * H));
+    CUDA_TRY(copy_d2h(e, hnode.data(), d.hist_node, 8 * size_t(H) * S));
+    CUDA_TRY(copy_d2h(e, hc.data(), d.hist_cval, 8 * size_t(H) * S));
+    CUDA_TRY(copy_d2h(e, hl.data(), d.hist_len, 4 * H));
   }
   auto put_row = [&](const gagp_rows& rows, int index, const uint64_t* node, const int64_t* cval, int32_t l) {
     const int n = l & 0xffff, nc = (l >> 16) & 0xffff;
@@ -1145,12 +1186,12 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   std::vector<uint64_t> key(P);
   std::vector<int64_t> cv(size_t(P) * S);
   std::vector<int32_t> len(P);
-  CUDA_TRY(cudaMemcpy(fit.data(), d.fitness, 8 * size_t(P), cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(wr.data(), d.wrong, 4 * size_t(P), cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(key.data(), d.key, 8 * size_t(P), cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(node.data(), d.node, 8 * size_t(P) * S, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(cv.data(), d.cval, 8 * size_t(P) * S, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemcpy(len.data(), d.len, 4 * size_t(P), cudaMemcpyDeviceToHost));
+  CUDA_TRY(copy_d2h(e, fit.data(), d.fitness, 8 * size_t(P)));
+  CUDA_TRY(copy_d2h(e, wr.data(), d.wrong, 4 * size_t(P)));
+  CUDA_TRY(copy_d2h(e, key.data(), d.key, 8 * size_t(P)));
+  CUDA_TRY(copy_d2h(e, node.data(), d.node, 8 * size_t(P) * S));
+  CUDA_TRY(copy_d2h(e, cv.data(), d.cval, 8 * size_t(P) * S));
+  CUDA_TRY(copy_d2h(e, len.data(), d.len, 4 * size_t(P)));
   std::vector<int> order(P);
   std::iota(order.begin(), order.end(), 0);
   std::sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
@@ -1164,7 +1205,7 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   }
   out->population = n_out;
   uint64_t counters[4];
-  CUDA_TRY(cudaMemcpy(counters, d.counters, sizeof(counters), cudaMemcpyDeviceToHost));
+  CUDA_TRY(copy_d2h(e, counters, d.counters, sizeof(counters)));
   out->evaluated_programs = counters[0];
   out->reused_programs = counters[1];
   out->program_cases = counters[2];

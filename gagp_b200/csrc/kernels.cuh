@@ -96,10 +96,14 @@ __global__ void k_lower(const SearchDesc* descs, const int32_t* off, int n, int 
     }
     if (bytecode > s.fuel) len = -1;
   }
+  // row and its length read; code words, constants, length, temps and list entry written
+  const uint64_t row_bytes = 8ull * (t.n + t.nc) + 4;
   if (len >= 0) {
     s.code_len[slot] = len;
     s.code_temps[slot] = temps;
     fast_list[atomicAdd(&list_count[0], 1)] = ProgramRef{si, slot};
+    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
+              (unsigned long long)(row_bytes + 8ull * (len + klen) + 16));
     return;
   }
   int nconst = 0, bound = 0;
@@ -112,6 +116,8 @@ __global__ void k_lower(const SearchDesc* descs, const int32_t* off, int n, int 
   s.bc_len[slot] = bl;
   s.code_temps[slot] = -1;
   general_list[atomicAdd(&list_count[1], 1)] = ProgramRef{si, slot};
+  atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
+            (unsigned long long)(row_bytes + 20ull * bl + 8ull * nconst + 16));
 }
 
 __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int slot, int64_t loss, uint32_t wrong) {
@@ -290,6 +296,27 @@ __device__ inline void mt_block_serial(const SearchDesc& s, uint64_t* mt, long l
 // stream_head as two 64-bit counters: [0] read, [1] written
 __device__ __forceinline__ long long* stream_ptrs(const SearchDesc& s) { return s.stream_head; }
 
+// Tops up each search's run-generator stream to the next placement's
+// 2B+1 draws (as far as the ring allows).  Launched on a side stream so the
+// generation overlaps the round's variation, lowering and evaluation; the
+// placement kernel waits for it and only generates what redraws add.
+__global__ void k_stream(const SearchDesc* descs, int n) {
+  __shared__ uint64_t mt[312], nw[312];
+  const SearchDesc& s = descs[blockIdx.x];
+  if (!search_live(s)) return;
+  for (int i = threadIdx.x; i < 312; i += blockDim.x) mt[i] = s.mt[i];
+  __syncthreads();
+  const long long rp = stream_ptrs(s)[0];
+  long long wp = stream_ptrs(s)[1];
+  const long long need = (long long)s.B * s.replacement_size + 1;
+  while (wp - rp < need && wp - rp + 312 <= s.stream_capacity) {
+    mt_block(s, mt, nw, wp);
+    wp += 312;
+  }
+  for (int i = threadIdx.x; i < 312; i += blockDim.x) s.mt[i] = mt[i];
+  if (threadIdx.x == 0) stream_ptrs(s)[1] = wp;
+}
+
 // Seeds the generator, tops up the stream, finds the best member and draws
 // the first round's variation seed.  One block per search.
 __global__ void k_start(const SearchDesc* descs, int n) {
@@ -368,24 +395,40 @@ __global__ void k_record(const SearchDesc* descs, int n, int only_epoch_start) {
 
 // make_batch (phase_population_cpu.cpp:322-353): one warp per child, rows
 // staged in dynamic shared memory (warp_rows_bytes(stride) per warp).
-__global__ void k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max) {
+// Persistent warps: each warp takes the next child index from `next_item`
+// (zeroed before the launch) until all children of the batch are varied, so
+// warps that drew short children go on to the next one instead of idling.
+__global__ void __launch_bounds__(128, 8) k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max,
+                                                 int32_t* next_item) {
   extern __shared__ __align__(16) char smem_rows[];
-  const int warps = blockDim.x >> 5, warp = threadIdx.x >> 5;
-  const int item = blockIdx.x * warps + warp;
-  if (item >= off[n]) return;
-  const int si = find_search(off, n, item);
-  const SearchDesc& s = descs[si];
-  if (!search_live(s)) return;
-  const int child = item - off[si];
-  WarpRows rows = carve_rows(smem_rows + size_t(warp) * warp_rows_bytes(stride_max), s.stride);
-  int reuse = -1, parent = -1;
-  const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent);
-  if ((threadIdx.x & 31) == 0) {
-    s.c_parent[child] = parent;
-    s.c_reuse[child] = reuse;
-    s.c_error[child] = error;
-    s.c_eval[child] = error == 0 && reuse < 0;
-    if (error) raise_error(s, 100 + error);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  char* base = smem_rows + size_t(warp) * warp_rows_bytes(stride_max);
+  const int total = off[n];
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(next_item, 1);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    const int si = find_search(off, n, item);
+    const SearchDesc& s = descs[si];
+    if (!search_live(s)) continue;
+    const int child = item - off[si];
+    WarpRows rows = carve_rows(base, s.stride);
+    int reuse = -1, parent = -1;
+    const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent);
+    if (lane == 0) {
+      s.c_parent[child] = parent;
+      s.c_reuse[child] = reuse;
+      s.c_error[child] = error;
+      s.c_eval[child] = error == 0 && reuse < 0;
+      if (error) raise_error(s, 100 + error);
+      // rows read (parent, donor) and written (child) with their lengths,
+      // 2 x pressure tournament keys, four per-child outputs
+      const uint64_t bytes = 8ull * (rows.parent.n + rows.parent.nc + rows.donor.n + rows.donor.nc + rows.child.n +
+                                     rows.child.nc + 2 * s.pressure) + 12 + 16;
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[8]), (unsigned long long)bytes);
+    }
+    __syncwarp();
   }
 }
 
@@ -490,12 +533,16 @@ __device__ __forceinline__ int latest_overlap(int d0, int d1) {
 // the sequential loop then takes.  Other replacement sizes and the end of
 // the staged draws run the sequential loop.
 // Finally the next round's seed is drawn.
-__global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
+constexpr int kPlaceThreads = 1024;
+__device__ __forceinline__ bool key_before(uint64_t ka, int va, uint64_t kb, int vb) {
+  return ka < kb || (ka == kb && va < vb);
+}
+__global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* descs, int n, int dyn_bytes) {
   extern __shared__ __align__(16) uint64_t keys[];
   __shared__ uint64_t mt[312], nw[312];
   __shared__ uint64_t ck_stage[1024];
-  __shared__ uint64_t scan_key[256];
-  __shared__ int scan_idx[256];
+  __shared__ uint64_t scan_key[32];
+  __shared__ int scan_idx[32];
   __shared__ long long shared_pos, shared_wp;
   __shared__ int shared_best, shared_fail, level_ready, level_left, redraw_at;
   const SearchDesc& s = descs[blockIdx.x];
@@ -519,25 +566,26 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
   }
   const long long t1 = clock64();
   // ---------------------------------------------------- level-parallel path
-  constexpr int kPerThread = 64;
+  constexpr int kPerThread = 16;
   int32_t* owner = reinterpret_cast<int32_t*>(keys + P);
-  const bool parallel_path = rs == 2 && blockDim.x == 256 && B <= 256 * kPerThread && wp - rp >= need &&
+  const bool parallel_path = rs == 2 && blockDim.x == kPlaceThreads && B <= kPlaceThreads * kPerThread &&
+                             wp - rp >= need &&
                              dyn_bytes >= int(sizeof(uint64_t) + sizeof(int32_t)) * P;
   bool parallel_done = false;
   if (parallel_path) {
     const int base = int(rp % cap);
     uint32_t cand[kPerThread];
-    uint64_t pending = 0;
+    uint32_t pending = 0;
 #pragma unroll
     for (int t = 0; t < kPerThread; ++t) {
-      const int j = tid + 256 * t;
+      const int j = tid + kPlaceThreads * t;
       cand[t] = 0;
       if (j < B) {
         int p0 = base + 2 * j, p1 = p0 + 1;
         if (p0 >= cap) p0 -= cap;
         if (p1 >= cap) p1 -= cap;
         cand[t] = s.stream_mod[p0] | (s.stream_mod[p1] << 16);
-        pending |= 1ULL << t;
+        pending |= 1u << t;
       }
     }
     if (tid == 0) {
@@ -559,7 +607,7 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
 #pragma unroll
       for (int t = 0; t < kPerThread; ++t)
         if (pending >> t & 1) {
-          const int j = tid + 256 * t;
+          const int j = tid + kPlaceThreads * t;
           atomicMin(&owner[cand[t] & 0xffff], j);
           atomicMin(&owner[cand[t] >> 16], j);
         }
@@ -568,7 +616,7 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
 #pragma unroll
       for (int t = 0; t < kPerThread; ++t)
         if (pending >> t & 1) {
-          const int j = tid + 256 * t;
+          const int j = tid + kPlaceThreads * t;
           const int d0 = int(cand[t] & 0xffff), d1 = int(cand[t] >> 16);
           if (owner[d0] == j && owner[d1] == j) {
             const uint64_t k0 = keys[d0], k1 = keys[d1];
@@ -577,7 +625,7 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
             keys[v] = s.c_key[j];
             placed[v] = j;
             s.c_victim[j] = v;
-            pending &= ~(1ULL << t);
+            pending &= ~(1u << t);
             ++ready;
           }
         }
@@ -588,38 +636,48 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
       if (level_left == 0) break;
     }
     // best member before each child (child order): thread t scans children
-    // [64t, 64t+64); a block scan of the per-thread minima gives each
-    // thread's incoming best
+    // [16t, 16t+16); a warp-shuffle scan, then a scan of the warp totals,
+    // gives each thread's incoming best
+    const int lane = tid & 31, warp = tid >> 5;
     const int begin = tid * kPerThread, stop = min(B, begin + kPerThread);
     uint64_t mk = ~0ULL;
     int mv = 0x7fffffff;
     for (int j = begin; j < stop; ++j) {
       const uint64_t k = s.c_key[j];
       const int v = s.c_victim[j];
-      if (k < mk || (k == mk && v < mv)) { mk = k; mv = v; }
+      if (key_before(k, v, mk, mv)) { mk = k; mv = v; }
     }
-    scan_key[tid] = mk;
-    scan_idx[tid] = mv;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t uk = __shfl_up_sync(kFull, mk, o);
+      const int uv = __shfl_up_sync(kFull, mv, o);
+      if (lane >= o && key_before(uk, uv, mk, mv)) { mk = uk; mv = uv; }
+    }
+    if (lane == 31) { scan_key[warp] = mk; scan_idx[warp] = mv; }
     __syncthreads();
-    for (int o = 1; o < 256; o <<= 1) {
-      uint64_t uk = 0;
-      int uv = 0;
-      const bool take = tid >= o;
-      if (take) { uk = scan_key[tid - o]; uv = scan_idx[tid - o]; }
-      __syncthreads();
-      if (take && (uk < scan_key[tid] || (uk == scan_key[tid] && uv < scan_idx[tid]))) {
-        scan_key[tid] = uk;
-        scan_idx[tid] = uv;
+    if (warp == 0) {
+      uint64_t wk = scan_key[lane];
+      int wv = scan_idx[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t uk = __shfl_up_sync(kFull, wk, o);
+        const int uv = __shfl_up_sync(kFull, wv, o);
+        if (lane >= o && key_before(uk, uv, wk, wv)) { wk = uk; wv = uv; }
       }
-      __syncthreads();
+      scan_key[lane] = wk;
+      scan_idx[lane] = wv;
     }
+    __syncthreads();
     const int best0 = s.best[0];
     const uint64_t best0_key = s.key[best0];
     int bv = best0;
     uint64_t bk = best0_key;
-    if (tid > 0 && (scan_key[tid - 1] < bk || (scan_key[tid - 1] == bk && scan_idx[tid - 1] < bv))) {
-      bk = scan_key[tid - 1];
-      bv = scan_idx[tid - 1];
+    {
+      const uint64_t lk = __shfl_up_sync(kFull, mk, 1);
+      const int lv = __shfl_up_sync(kFull, mv, 1);
+      if (lane > 0 && key_before(lk, lv, bk, bv)) { bk = lk; bv = lv; }
+      if (warp > 0 && key_before(scan_key[warp - 1], scan_idx[warp - 1], bk, bv)) {
+        bk = scan_key[warp - 1];
+        bv = scan_idx[warp - 1];
+      }
     }
     for (int j = begin; j < stop; ++j) {
       const int v = s.c_victim[j];
@@ -636,7 +694,7 @@ __global__ void k_place(const SearchDesc* descs, int n, int dyn_bytes) {
       if (tid == 0) {
         int fv = best0;
         uint64_t fk = best0_key;
-        if (scan_key[255] < fk || (scan_key[255] == fk && scan_idx[255] < fv)) { fk = scan_key[255]; fv = scan_idx[255]; }
+        if (key_before(scan_key[31], scan_idx[31], fk, fv)) { fk = scan_key[31]; fv = scan_idx[31]; }
         shared_best = fv;
         shared_fail = 0;
         // the next round's seed: the raw output after the 2B placement draws

@@ -100,7 +100,7 @@ struct SearchDesc {
   int64_t* hist_sum;                   // per history entry: sum of member fitness (integral)
   double* hist_fitness; uint32_t* hist_wrong; uint32_t* hist_nodes;
   uint64_t* hist_node; int64_t* hist_cval; int32_t* hist_len;
-  uint64_t* counters;                  // [0] evaluated programs, [1] reused, [2] program cases, [3] VM ops
+  uint64_t* counters;                  // GAGP_COUNTERS work counters (gagp_b200_search_counters)
   int32_t key_shift_wrong, key_shift_nodes; // packed key layout
   int32_t total_rounds;
 };

@@ -38,7 +38,7 @@ def load_library():
         for name in ("gagp_b200_engine_create", "gagp_b200_search_bytes", "gagp_b200_search_create",
                      "gagp_b200_search_destroy", "gagp_b200_search_run", "gagp_b200_batch_run",
                      "gagp_b200_batch_step", "gagp_b200_search_result", "gagp_b200_batch_start",
-                     "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters",
+                     "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters", "gagp_b200_engine_transfers",
                      "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_evaluate_rows",
                      "gagp_b200_evaluate_rows_static"):
             getattr(lib, name).restype = C.c_int32
@@ -140,11 +140,17 @@ class Engine:
         return ms.value
 
     def counters(self, search: Search) -> dict:
-        out = (C.c_uint64 * 8)()
-        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out))
+        out = (C.c_uint64 * 16)()
+        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out, C.c_int32(16)))
         return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2], "vm_ops": out[3],
                 "place_generate_cycles": out[4], "place_stage_cycles": out[5], "place_serial_cycles": out[6],
-                "place_levels": out[7]}
+                "place_levels": out[7], "vary_bytes": out[8], "lower_bytes": out[9]}
+
+    def transfers(self) -> tuple:
+        """(host->device, device->host) bytes copied by this engine so far."""
+        h2d, d2h = C.c_uint64(), C.c_uint64()
+        _check(load_library().gagp_b200_engine_transfers(self.handle, C.byref(h2d), C.byref(d2h)))
+        return h2d.value, d2h.value
 
     def progress(self, search: Search) -> tuple:
         done, total, fin = C.c_int32(), C.c_int32(), C.c_int32()

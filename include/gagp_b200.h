@@ -238,8 +238,18 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
  * that reused a member's result, [2] evaluated (program, case) pairs,
  * [3] VM instructions executed over all cases, [4..6] SM clock cycles of
  * the placement phases (stream generation, draw staging, placement),
- * [7] reserved (synchronous). */
-gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out8);
+ * [7] placement levels (+2^20 per sequential replay), [8] bytes the
+ * variation kernel moved (parent, donor and child rows, tournament keys,
+ * per-child outputs), [9] bytes the lowering kernel moved (rows read, code
+ * and constants written).  Copies min(count, GAGP_COUNTERS) entries
+ * (synchronous). */
+/* Bytes this engine's calls have copied host->device and device->host since
+ * it was created (uploads at admission and batch launches, progress and
+ * result reads). */
+gagp_status gagp_b200_engine_transfers(gagp_engine* engine, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+
+#define GAGP_COUNTERS 16
+gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out, int32_t count);
 
 /* Per-kernel CUDA-event timing: enable (resets) or disable, then read the
  * accumulated time and launch count of kernel index 0.. (INVALID_ARGUMENT
