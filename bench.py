@@ -331,7 +331,7 @@ def run_own_arm(args, rank: int, world: int, local: int):
     if rank != 0:
         return
     launches = sum(v["launches"] for v in stats.values())
-    delta = {k: after[k] - before[k] for k in after}
+    delta = {k: after[k] - before[k] for k in after if isinstance(after[k], int)}
     line = {"metric": METRIC, "value": cases / secs, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
@@ -344,7 +344,13 @@ def run_own_arm(args, rank: int, world: int, local: int):
                          "vm_ops": after["vm_ops"] - before["vm_ops"],
                          "place_cycles_per_step": {k: (after[k] - before[k]) / args.steps for k in
                                                    ("place_generate_cycles", "place_stage_cycles",
-                                                    "place_serial_cycles", "place_levels")}}}
+                                                    "place_serial_cycles", "place_levels", "place_level_cycles")},
+                         "vary_cycles_per_child": {k: (after[k] - before[k]) / max(1, args.steps * WORKLOAD["population"])
+                                                   for k in ("vary_select_cycles", "vary_crossover_cycles",
+                                                             "vary_generate_cycles", "vary_rest_cycles")},
+                         "vary_max_child_cycles": after["vary_max_child_cycles"],
+                         "vary_max_phase_cycles": after["vary_max_phase_cycles"],
+                         "vary_slow_children": after["vary_slow_children"] - before["vary_slow_children"]}}
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as d:
             make_task(seed, d)

@@ -124,12 +124,28 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
                                      int capacity, uint64_t seed, uint64_t* out_node, int64_t* out_cval,
                                      int logical_depth, uint32_t* pending) {
   GenResult result{ST_INVALID, 0, 0};
+  // the tables, read once into registers: every table load below is a
+  // read-only load through these
+  const gagp_expression* __restrict__ ex = s.ex;
+  const ExprInfo* __restrict__ info_tab = s.info;
+  const gagp_production* __restrict__ prods = s.prods;
+  const gagp_nonterminal* __restrict__ nts = s.nts;
+  const gagp_domain* __restrict__ doms = s.doms;
+  const gagp_value* __restrict__ vals = s.vals;
+  const uint32_t* __restrict__ minimum = s.minimum;
+  const uint32_t* __restrict__ prod_minimum = s.prod_minimum;
+  const int n_ex = s.n_ex, n_nts = s.n_nts, n_prods = s.n_prods, n_doms = s.n_doms, n_vals = s.n_vals;
+  const int depth_count = s.depth_count, logical_count = s.logical_count;
+  const bool site_limited = s.site_depth > 0;
+  auto min_of = [&](int e, int d, int l) -> unsigned {
+    if (e < 0 || e >= n_ex || d < 0 || d >= depth_count || l < 0 || l >= logical_count) return kNoId;
+    return __ldg(&minimum[(size_t(e) * depth_count + d) * logical_count + l]);
+  };
   int steps = 0;
   int next_site = -1;  // entry expression of a pending site
-  const bool site_limited = s.site_depth > 0;
-  if (root_expression < 0 || root_expression >= s.n_ex || scope_count < 0 || scope_count > 15 || depth <= 0 ||
-      depth >= s.depth_count || depth > 64 || logical_depth < 0 || logical_depth >= s.logical_count ||
-      capacity <= 0 || capacity > kCapacity || s.n_ex > 131071)
+  if (root_expression < 0 || root_expression >= n_ex || scope_count < 0 || scope_count > 15 || depth <= 0 ||
+      depth >= depth_count || depth > 64 || logical_depth < 0 || logical_depth >= logical_count ||
+      capacity <= 0 || capacity > kCapacity || n_ex > 131071)
     return result;
   if (capacity > s.stride) capacity = s.stride;  // callers pass at most the node budget
   const unsigned unselected = 131071u;
@@ -138,7 +154,7 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
     return e | (d << 17) | (n << 24) | (l << 28);
   };
   pending[0] = pack(unsigned(root_expression), unsigned(depth), unsigned(scope_count), unsigned(logical_depth));
-  unsigned reserved = minimum_of(s, root_expression, depth, logical_depth);
+  unsigned reserved = min_of(root_expression, depth, logical_depth);
   if (reserved > unsigned(capacity)) { result.status = ST_CAPACITY; return result; }
   Rng random(seed);
   while (count) {
@@ -146,96 +162,108 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
     const uint32_t task = pending[--count];
     const int t_expr = int(task & 0x1ffffu), t_depth = int((task >> 17) & 0x7fu);
     const int t_scope = int((task >> 24) & 0xfu), t_logical = int(task >> 28);
-    const unsigned required = minimum_of(s, t_expr, t_depth, t_logical);
+    const unsigned required = min_of(t_expr, t_depth, t_logical);
     if (required > reserved) return result;
     reserved -= required;
-    const gagp_expression& expression = s.ex[t_expr];
-    const ExprInfo info = s.info[t_expr];
-    if (info.kind == EK_REFERENCE) {
-      if (expression.target < 0 || expression.target >= s.n_nts || expression.scope_count < 0 ||
-          expression.scope_count > 8)
-        return result;
+    const gagp_expression* expression = ex + t_expr;
+    const int kind = __ldg(&info_tab[t_expr].kind);
+    if (kind == EK_REFERENCE) {
+      const int target = __ldg(&expression->target), e_scopes = __ldg(&expression->scope_count);
+      if (target < 0 || target >= n_nts || e_scopes < 0 || e_scopes > 8) return result;
       if (next_site >= 0) return result;
       next_site = t_expr;
-      const gagp_nonterminal nt = s.nts[expression.target];
-      if (nt.scope_count != expression.scope_count || nt.production_offset < 0 || nt.production_count <= 0 ||
-          nt.production_offset > s.n_prods || nt.production_count > s.n_prods - nt.production_offset)
+      const int nt_offset = __ldg(&nts[target].production_offset), nt_count = __ldg(&nts[target].production_count);
+      const bool normalized = __ldg(&nts[target].normalized_weights) != 0;
+      if (__ldg(&nts[target].scope_count) != e_scopes || nt_offset < 0 || nt_count <= 0 || nt_offset > n_prods ||
+          nt_count > n_prods - nt_offset)
         return result;
       if (site_limited && t_logical == 0) { result.status = ST_CAPACITY; return result; }
       const int n_logical = t_logical - (site_limited ? 1 : 0);
       unsigned next_expr = unselected;
       if (reserved > unsigned(capacity - result.nodes)) { result.status = ST_CAPACITY; return result; }
       const unsigned available = unsigned(capacity - result.nodes) - reserved;
-      double maximum = nt.normalized_weights ? 1.0 : 0.0, total = 0.0;
-      if (!nt.normalized_weights)
-        for (int i = 0; i < nt.production_count; ++i) {
-          const gagp_production p = s.prods[nt.production_offset + i];
-          if (minimum_of(s, p.expression, t_depth, n_logical) <= available && p.weight > maximum) maximum = p.weight;
+      // feasibility of each production (a bit mask for the first 64)
+      const uint32_t* __restrict__ prow = prod_minimum + (size_t(t_depth) * logical_count + n_logical) * n_prods + nt_offset;
+      uint64_t feasible_mask = 0;
+      for (int i = 0; i < nt_count && i < 64; ++i)
+        if (__ldg(&prow[i]) <= available) feasible_mask |= 1ULL << i;
+      auto feasible = [&](int i) -> bool { return i < 64 ? (feasible_mask >> i & 1) : __ldg(&prow[i]) <= available; };
+      double maximum = normalized ? 1.0 : 0.0, total = 0.0;
+      if (!normalized)
+        for (int i = 0; i < nt_count; ++i) {
+          const double w = __ldg(&prods[nt_offset + i].weight);
+          if (feasible(i) && w > maximum) maximum = w;
         }
       if (!(maximum > 0)) { result.status = ST_CAPACITY; return result; }
-      for (int i = 0; i < nt.production_count; ++i) {
-        const gagp_production p = s.prods[nt.production_offset + i];
-        if (minimum_of(s, p.expression, t_depth, n_logical) <= available)
-          total = __dadd_rn(total, nt.normalized_weights ? p.weight : __ddiv_rn(p.weight, maximum));
-      }
+      for (int i = 0; i < nt_count; ++i)
+        if (feasible(i)) {
+          const double w = __ldg(&prods[nt_offset + i].weight);
+          total = __dadd_rn(total, normalized ? w : __ddiv_rn(w, maximum));
+        }
       double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), total);
-      for (int i = 0; i < nt.production_count; ++i) {
-        const gagp_production p = s.prods[nt.production_offset + i];
-        if (minimum_of(s, p.expression, t_depth, n_logical) > available) continue;
-        if (p.expression < 0 || p.expression >= s.n_ex) return result;
-        next_expr = unsigned(p.expression);
-        choice = __dsub_rn(choice, nt.normalized_weights ? p.weight : __ddiv_rn(p.weight, maximum));
+      for (int i = 0; i < nt_count; ++i) {
+        if (!feasible(i)) continue;
+        const int pe = __ldg(&prods[nt_offset + i].expression);
+        if (pe < 0 || pe >= n_ex) return result;
+        next_expr = unsigned(pe);
+        const double w = __ldg(&prods[nt_offset + i].weight);
+        choice = __dsub_rn(choice, normalized ? w : __ddiv_rn(w, maximum));
         if (choice < 0) break;
       }
       if (next_expr == unselected || count >= 192) return result;
-      reserved += minimum_of(s, int(next_expr), t_depth, n_logical);
-      pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(expression.scope_count), unsigned(n_logical));
+      reserved += min_of(int(next_expr), t_depth, n_logical);
+      pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical));
       continue;
     }
-    if (info.kind == EK_ALIAS) {
-      const int child = expression.children[0];
-      if (child < 0 || child >= s.n_ex || count >= 192) return result;
-      const int scope = expression.child_scope[0] >= 0 ? expression.child_scope[0] : t_scope;
-      reserved += minimum_of(s, child, t_depth, t_logical);
+    if (kind == EK_ALIAS) {
+      const int child = __ldg(&expression->children[0]);
+      if (child < 0 || child >= n_ex || count >= 192) return result;
+      const int child_scope = __ldg(&expression->child_scope[0]);
+      const int scope = child_scope >= 0 ? child_scope : t_scope;
+      reserved += min_of(child, t_depth, t_logical);
       pending[count++] = pack(unsigned(child), unsigned(t_depth), unsigned(scope), unsigned(t_logical));
       continue;
     }
     if (t_depth <= 0 || result.nodes >= capacity) { result.status = ST_CAPACITY; return result; }
-    const int arity = info.arity;
+    const int arity = __ldg(&info_tab[t_expr].arity);
     if (arity < 0 || arity > 8) return result;
-    if (info.kind == EK_BOUND) {
-      if (arity != 0 || expression.operand < 0 || expression.operand >= 16) return result;
-    } else if (info.kind == EK_CONSTANT) {
-      if (expression.target < 0 || expression.target >= s.n_doms || arity != 0) return result;
-      const gagp_domain domain = s.doms[expression.target];
+    if (kind == EK_BOUND) {
+      const int operand = __ldg(&expression->operand);
+      if (arity != 0 || operand < 0 || operand >= 16) return result;
+    } else if (kind == EK_CONSTANT) {
+      const int target = __ldg(&expression->target);
+      if (target < 0 || target >= n_doms || arity != 0) return result;
+      const gagp_domain* domain = doms + target;
       int64_t value;
-      if (domain.integer_range) {
-        if (domain.minimum > domain.maximum) return result;
-        value = random.integer(domain.minimum, domain.maximum);
+      if (__ldg(&domain->integer_range)) {
+        const int64_t lo = __ldg(&domain->minimum), hi = __ldg(&domain->maximum);
+        if (lo > hi) return result;
+        value = random.integer(lo, hi);
       } else {
-        if (domain.value_offset < 0 || domain.value_count <= 0 || domain.value_offset > s.n_vals ||
-            domain.value_count > s.n_vals - domain.value_offset)
-          return result;
-        const gagp_value v = s.vals[domain.value_offset + random.bounded(uint64_t(domain.value_count))];
-        if (v.tag == GAGP_TAG_INVALID) return result;
-        value = v.i;
+        const int v_offset = __ldg(&domain->value_offset), v_count = __ldg(&domain->value_count);
+        if (v_offset < 0 || v_count <= 0 || v_offset > n_vals || v_count > n_vals - v_offset) return result;
+        const gagp_value* v = vals + v_offset + random.bounded(uint64_t(v_count));
+        if (__ldg(&v->tag) == GAGP_TAG_INVALID) return result;
+        value = __ldg(&v->i);
       }
       out_cval[result.constants++] = value;
-    } else if (info.kind != EK_OPERATION && info.kind != EK_INPUT) {
+    } else if (kind != EK_OPERATION && kind != EK_INPUT) {
       return result;
     }
+    const uint32_t cls = next_site < 0 ? kNoClass : uint32_t(__ldg(&info_tab[next_site].site_class));
     out_node[result.nodes++] = w_make(t_expr, next_site, depth - t_depth + 1, logical_depth - t_logical, arity,
-                                      info.kind == EK_CONSTANT, class_of_entry(s, next_site));
+                                      kind == EK_CONSTANT, cls);
     next_site = -1;
     for (int i = arity - 1; i >= 0; --i) {
       if (count >= 192) { result.status = ST_CAPACITY; return result; }
-      const int child = expression.children[i];
-      const unsigned need = minimum_of(s, child, t_depth - 1, t_logical);
+      const int child = __ldg(&expression->children[i]);
+      const unsigned need = min_of(child, t_depth - 1, t_logical);
       if (need > unsigned(capacity - result.nodes) || reserved > unsigned(capacity - result.nodes) - need) {
         result.status = ST_CAPACITY;
         return result;
       }
-      const int scope = expression.child_scope[i] >= 0 ? expression.child_scope[i] : t_scope;
+      const int child_scope = __ldg(&expression->child_scope[i]);
+      const int scope = child_scope >= 0 ? child_scope : t_scope;
       pending[count++] = pack(unsigned(child), unsigned(t_depth - 1), unsigned(scope), unsigned(t_logical));
       reserved += need;
     }

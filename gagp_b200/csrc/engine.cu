@@ -233,9 +233,9 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
 
 struct Plan {
   Layout L;
-  size_t ex, info, prods, nts, doms, vals, minimum, local_types, inputs, expected;
+  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, local_types, inputs, expected;
   size_t node, cval, len, cnode, ccval, clen;
-  size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval, c_victim;
+  size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
   size_t code, code_len, kpool, code_temps, bc, bc_len, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, round, hist_sum, hist_fitness, hist_wrong,
       hist_nodes, hist_node, hist_cval, hist_len, counters;
@@ -267,6 +267,8 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.doms = L.take(sizeof(gagp_domain) * std::max(1, g->domain_count));
   p.vals = L.take(sizeof(gagp_value) * std::max(1, g->value_count));
   p.minimum = L.take(sizeof(uint32_t) * size_t(E) * g->depth_count * g->logical_depth_count);
+  p.prod_minimum = L.take(sizeof(uint32_t) * size_t(std::max(1, g->production_count)) * g->depth_count *
+                          g->logical_depth_count);
   p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
   p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
   p.expected = L.take(sizeof(int64_t) * C);
@@ -277,7 +279,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.key = L.take(8 * size_t(P));
   p.c_parent = L.take(4 * size_t(B)); p.c_reuse = L.take(4 * size_t(B)); p.c_error = L.take(4 * size_t(B));
   p.c_fitness = L.take(8 * size_t(B)); p.c_wrong = L.take(4 * size_t(B)); p.c_nodes = L.take(4 * size_t(B));
-  p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B)); p.c_victim = L.take(4 * size_t(B));
+  p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
   p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots);
@@ -423,6 +425,17 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   if (g->domain_count) CUDA_TRY(up(p.doms, g->domains, sizeof(gagp_domain) * g->domain_count));
   if (g->value_count) CUDA_TRY(up(p.vals, g->values, sizeof(gagp_value) * g->value_count));
   CUDA_TRY(up(p.minimum, g->minimum, sizeof(uint32_t) * size_t(E) * g->depth_count * g->logical_depth_count));
+  // production-major copy of the minimum table: a nonterminal's productions
+  // are adjacent for each (depth, site budget)
+  const int PR = g->production_count, DC = g->depth_count, LC = g->logical_depth_count;
+  std::vector<uint32_t> prod_minimum(size_t(std::max(1, PR)) * DC * LC, gb::kNoId);
+  for (int d = 0; d < DC; ++d)
+    for (int l = 0; l < LC; ++l)
+      for (int q = 0; q < PR; ++q) {
+        const int pe = g->productions[q].expression;
+        if (pe >= 0 && pe < E) prod_minimum[(size_t(d) * LC + l) * PR + q] = g->minimum[(size_t(pe) * DC + d) * LC + l];
+      }
+  CUDA_TRY(up(p.prod_minimum, prod_minimum.data(), sizeof(uint32_t) * prod_minimum.size()));
   CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
   CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
   CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
@@ -435,6 +448,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.doms = at<gagp_domain>(b, p.doms);
   d.vals = at<gagp_value>(b, p.vals);
   d.minimum = at<uint32_t>(b, p.minimum);
+  d.prod_minimum = at<uint32_t>(b, p.prod_minimum);
   d.local_types = at<int32_t>(b, p.local_types);
   d.n_ex = E; d.n_prods = g->production_count; d.n_nts = g->nonterminal_count;
   d.n_doms = g->domain_count; d.n_vals = g->value_count;
@@ -462,7 +476,6 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
   d.c_fitness = at<double>(b, p.c_fitness); d.c_wrong = at<uint32_t>(b, p.c_wrong);
   d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
-  d.c_victim = at<int32_t>(b, p.c_victim);
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
   d.bc = at<int32_t>(b, p.bc); d.bc_len = at<int32_t>(b, p.bc_len); d.bc_consts = at<int64_t>(b, p.bc_consts);
@@ -603,7 +616,7 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
 gagp_status launch_start(gagp_engine* e, const BatchView& v) {
   { Timed t(e, KN_INIT); gb::k_init_population<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
-  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n, 0, e->d_fast,
+  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_members, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n, 0, e->d_fast,
                                                                         e->d_general, e->d_counts); }
   launch_vm(e, v, 0);
   { Timed t(e, KN_KEYS); gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
@@ -629,7 +642,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v) {
     const int blocks = std::min(blocks_for(v.total_children, warps), std::max(1, per_sm) * e->sm_count);
     gb::k_vary<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, e->d_counts + 2);
   }
-  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
+  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_children, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
                                                                          e->d_general, e->d_counts); }
   launch_vm(e, v, 1);
   { Timed t(e, KN_CHILD); gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
@@ -811,6 +824,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.ex = at<gagp_expression>(b, p.ex);
   d.info = at<gb::ExprInfo>(b, p.info);
   d.minimum = at<uint32_t>(b, p.minimum);
+  d.prod_minimum = d.minimum;  // no subtree generation in row evaluation
   d.local_types = at<int32_t>(b, p.local_types);
   d.n_ex = E;
   d.slot_type = g->slot_type;
@@ -871,7 +885,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   gb::ProgramRef* fast = at<gb::ProgramRef>(b, p.fast);
   gb::ProgramRef* general = at<gb::ProgramRef>(b, p.general);
   int32_t* counts = at<int32_t>(b, p.counts);
-  gb::k_lower<<<blocks_for(R, 128), 128, 0, stream>>>(dd, doff, 1, 0, fast, general, counts);
+  gb::k_lower<<<blocks_for(R, gb::kLowerWarps), gb::kLowerWarps * 32, 0, stream>>>(dd, doff, 1, 0, fast, general, counts);
   const int warps = 8;
   const int lanes = d.vm_cases_per_lane;
   const int temp_stride = gb::kMaxTemps * lanes * 32;

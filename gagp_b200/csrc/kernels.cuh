@@ -63,61 +63,61 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
 
 // ----------------------------------------------------------- lowering
 // mode 0: the members (initial evaluation); mode 1: this round's children
-// that reuse no member's result.
-__global__ void k_lower(const SearchDesc* descs, const int32_t* off, int n, int mode, ProgramRef* fast_list,
-                        ProgramRef* general_list, int32_t* list_count) {
-  const int item = blockIdx.x * blockDim.x + threadIdx.x;
-  if (item >= off[n]) return;
-  const int si = find_search(off, n, item);
-  const SearchDesc& s = descs[si];
-  if (!search_live(s)) return;
-  const int slot = item - off[si];
-  LRow t;
-  if (mode == 0) {
-    const int32_t l = s.len[slot];
-    t = LRow{s.node + size_t(slot) * s.stride, s.cval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
-  } else {
-    if (!s.c_eval[slot]) return;
-    const int32_t l = s.clen[slot];
-    t = LRow{s.cnode + size_t(slot) * s.stride, s.ccval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
-  }
-  int temps = 0, klen = 0;
-  int len = s.maxv <= 64 ? lower_accumulator<64>(s, t, s.code + size_t(slot) * s.code_stride, s.code_stride,
-                                                 s.kpool + size_t(slot) * s.stride, &klen, &temps)
-                         : lower_accumulator<kMaxLowerNodes>(s, t, s.code + size_t(slot) * s.code_stride,
-                                                             s.code_stride, s.kpool + size_t(slot) * s.stride, &klen,
-                                                             &temps);
-  if (len >= 0) {
-    // exact bytecode length (a bound of every executed path) must fit the fuel
-    int bytecode = 1;
-    for (int i = 0; i < t.n; ++i) {
-      const int nk = s.info[w_origin(t.node[i])].node_kind;
-      bytecode += nk == TK_IF ? 2 : (nk == TK_AND || nk == TK_OR) ? 5 : 1;
+// that reuse no member's result.  One warp per row: the accumulator program
+// when the row is total and fits the fuel, else the reference bytecode for
+// the general VM (lane 0).
+constexpr int kLowerWarps = 4;
+__global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* descs, const int32_t* off, int n,
+                                                            int mode, ProgramRef* fast_list, ProgramRef* general_list,
+                                                            int32_t* list_count) {
+  __shared__ LowerScratch scratch[kLowerWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total_items = off[n];
+  for (int item = blockIdx.x * kLowerWarps + warp; item < total_items; item += gridDim.x * kLowerWarps) {
+    const int si = find_search(off, n, item);
+    const SearchDesc& s = descs[si];
+    if (!search_live(s)) continue;
+    const int slot = item - off[si];
+    LRow t;
+    if (mode == 0) {
+      const int32_t l = s.len[slot];
+      t = LRow{s.node + size_t(slot) * s.stride, s.cval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
+    } else {
+      if (!s.c_eval[slot]) continue;
+      const int32_t l = s.clen[slot];
+      t = LRow{s.cnode + size_t(slot) * s.stride, s.ccval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
     }
-    if (bytecode > s.fuel) len = -1;
+    int temps = 0;
+    const int len = lower_accumulator_warp(s, t.node, t.n, t.cval, t.nc, s.code + size_t(slot) * s.code_stride,
+                                           s.code_stride, s.kpool + size_t(slot) * s.stride, scratch[warp], &temps);
+    // row and its length read; code words, constants, length, temps and list entry written
+    const uint64_t row_bytes = 8ull * (t.n + t.nc) + 4;
+    if (len >= 0) {
+      if (lane == 0) {
+        s.code_len[slot] = len;
+        s.code_temps[slot] = temps;
+        fast_list[atomicAdd(&list_count[0], 1)] = ProgramRef{si, slot};
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
+                  (unsigned long long)(row_bytes + 8ull * (len + t.nc) + 16));
+      }
+      continue;
+    }
+    if (lane == 0) {
+      int nconst = 0, bound = 0;
+      const int bl = lower_reference(s, t, s.bc + size_t(slot) * 5 * s.bc_stride, s.bc_stride,
+                                     s.bc_consts + size_t(slot) * s.bc_stride, &nconst, &bound);
+      if (bl < 0) {
+        raise_error(s, 30);  // the phase compiler rejected a constructed program
+      } else {
+        s.bc_len[slot] = bl;
+        s.code_temps[slot] = -1;
+        general_list[atomicAdd(&list_count[1], 1)] = ProgramRef{si, slot};
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
+                  (unsigned long long)(row_bytes + 20ull * bl + 8ull * nconst + 16));
+      }
+    }
+    __syncwarp();
   }
-  // row and its length read; code words, constants, length, temps and list entry written
-  const uint64_t row_bytes = 8ull * (t.n + t.nc) + 4;
-  if (len >= 0) {
-    s.code_len[slot] = len;
-    s.code_temps[slot] = temps;
-    fast_list[atomicAdd(&list_count[0], 1)] = ProgramRef{si, slot};
-    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
-              (unsigned long long)(row_bytes + 8ull * (len + klen) + 16));
-    return;
-  }
-  int nconst = 0, bound = 0;
-  const int bl = lower_reference(s, t, s.bc + size_t(slot) * 5 * s.bc_stride, s.bc_stride,
-                                 s.bc_consts + size_t(slot) * s.bc_stride, &nconst, &bound);
-  if (bl < 0) {
-    raise_error(s, 30);  // the phase compiler rejected a constructed program
-    return;
-  }
-  s.bc_len[slot] = bl;
-  s.code_temps[slot] = -1;
-  general_list[atomicAdd(&list_count[1], 1)] = ProgramRef{si, slot};
-  atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
-            (unsigned long long)(row_bytes + 20ull * bl + 8ull * nconst + 16));
 }
 
 __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int slot, int64_t loss, uint32_t wrong) {
@@ -398,7 +398,7 @@ __global__ void k_record(const SearchDesc* descs, int n, int only_epoch_start) {
 // Persistent warps: each warp takes the next child index from `next_item`
 // (zeroed before the launch) until all children of the batch are varied, so
 // warps that drew short children go on to the next one instead of idling.
-__global__ void __launch_bounds__(128, 8) k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max,
+__global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max,
                                                  int32_t* next_item) {
   extern __shared__ __align__(16) char smem_rows[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -415,8 +415,21 @@ __global__ void __launch_bounds__(128, 8) k_vary(const SearchDesc* descs, const 
     const int child = item - off[si];
     WarpRows rows = carve_rows(base, s.stride);
     int reuse = -1, parent = -1;
-    const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent);
+    long long stamp[4] = {0, 0, 0, 0};
+    const long long started = clock64();
+    const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent, stamp);
     if (lane == 0) {
+      // per-phase SM cycles: selection, crossover, subtree generation, rest
+      stamp[3] = clock64();
+      long long prev = started;
+      for (int k = 0; k < 4; ++k) {
+        if (stamp[k] == 0) stamp[k] = prev;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[10 + k]), (unsigned long long)(stamp[k] - prev));
+        atomicMax(reinterpret_cast<unsigned long long*>(&s.counters[16 + k]), (unsigned long long)(stamp[k] - prev));
+        prev = stamp[k];
+      }
+      atomicMax(reinterpret_cast<unsigned long long*>(&s.counters[15]), (unsigned long long)(stamp[3] - started));
+      if (stamp[3] - started > 200000) atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[20]), 1ULL);
       s.c_parent[child] = parent;
       s.c_reuse[child] = reuse;
       s.c_error[child] = error;
@@ -544,7 +557,7 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
   __shared__ uint64_t scan_key[32];
   __shared__ int scan_idx[32];
   __shared__ long long shared_pos, shared_wp;
-  __shared__ int shared_best, shared_fail, level_ready, level_left, redraw_at;
+  __shared__ int shared_best, shared_fail, ready_count[2], redraw_at;
   const SearchDesc& s = descs[blockIdx.x];
   if (!search_live(s)) return;
   const long long t0 = clock64();
@@ -573,12 +586,17 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
                              dyn_bytes >= int(sizeof(uint64_t) + sizeof(int32_t)) * P;
   bool parallel_done = false;
   if (parallel_path) {
+    // thread tid owns children [16 tid, 16 tid + 16): cand[t] holds child
+    // begin + t's two draws, and once it is placed, its victim
     const int base = int(rp % cap);
+    const int begin = tid * kPerThread;
+    constexpr int kBatch = 4;  // child keys loaded together
+    const uint64_t* __restrict__ ckey = s.c_key;
     uint32_t cand[kPerThread];
     uint32_t pending = 0;
 #pragma unroll
     for (int t = 0; t < kPerThread; ++t) {
-      const int j = tid + kPlaceThreads * t;
+      const int j = begin + t;
       cand[t] = 0;
       if (j < B) {
         int p0 = base + 2 * j, p1 = p0 + 1;
@@ -588,64 +606,81 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
         pending |= 1u << t;
       }
     }
+    // owner[m]: the earliest child of the current level that drew member m,
+    // tagged with the level so that no per-level reset is needed (a later
+    // level's tag is smaller than every earlier one's)
+    for (int m = tid; m < P; m += blockDim.x) owner[m] = 0x7fffffff;
     if (tid == 0) {
-      level_left = B;
+      ready_count[0] = ready_count[1] = 0;
       redraw_at = 0x7fffffff;
     }
     __syncthreads();
-    int levels_run = 0;
+    int levels_run = 0, left = B;
+    const long long level_start = clock64();
     for (int level = 0; level <= B; ++level) {
       ++levels_run;
+      const int tag = (0x7fff - level) << 16;
 #pragma unroll
       for (int t = 0; t < kPerThread; ++t)
         if (pending >> t & 1) {
-          owner[cand[t] & 0xffff] = 0x7fffffff;
-          owner[cand[t] >> 16] = 0x7fffffff;
+          atomicMin(&owner[cand[t] & 0xffff], tag | (begin + t));
+          atomicMin(&owner[cand[t] >> 16], tag | (begin + t));
         }
-      if (tid == 0) level_ready = 0;
       __syncthreads();
+      // children owning both their members are placed at this level; they
+      // touch disjoint members, so their order within the level is free
+      uint32_t ready = 0;
 #pragma unroll
       for (int t = 0; t < kPerThread; ++t)
-        if (pending >> t & 1) {
-          const int j = tid + kPlaceThreads * t;
-          atomicMin(&owner[cand[t] & 0xffff], j);
-          atomicMin(&owner[cand[t] >> 16], j);
-        }
-      __syncthreads();
-      int ready = 0;
+        if ((pending >> t & 1) && owner[cand[t] & 0xffff] == (tag | (begin + t)) &&
+            owner[cand[t] >> 16] == (tag | (begin + t)))
+          ready |= 1u << t;
+      if (ready) {
 #pragma unroll
-      for (int t = 0; t < kPerThread; ++t)
-        if (pending >> t & 1) {
-          const int j = tid + kPlaceThreads * t;
-          const int d0 = int(cand[t] & 0xffff), d1 = int(cand[t] >> 16);
-          if (owner[d0] == j && owner[d1] == j) {
-            const uint64_t k0 = keys[d0], k1 = keys[d1];
-            // worst of the pair: the second replaces the first when the first is better
-            const int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
-            keys[v] = s.c_key[j];
-            placed[v] = j;
-            s.c_victim[j] = v;
-            pending &= ~(1u << t);
-            ++ready;
-          }
+        for (int h = 0; h < kPerThread; h += kBatch) {
+          uint64_t kv[kBatch];
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u) kv[u] = (ready >> (h + u) & 1) ? ckey[begin + h + u] : 0;
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u)
+            if (ready >> (h + u) & 1) {
+              const int d0 = int(cand[h + u] & 0xffff), d1 = int(cand[h + u] >> 16);
+              const uint64_t k0 = keys[d0], k1 = keys[d1];
+              // worst of the pair: the second replaces the first when the first is better
+              const int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
+              keys[v] = kv[u];
+              placed[v] = begin + h + u;
+              cand[h + u] = uint32_t(v);
+            }
         }
-      if (ready) atomicAdd(&level_ready, ready);
+        pending &= ~ready;
+        atomicAdd(&ready_count[level & 1], __popc(ready));
+      }
+      if (tid == 0) ready_count[(level + 1) & 1] = 0;  // read by every thread before this level's first barrier
       __syncthreads();
-      if (tid == 0) level_left -= level_ready;
-      __syncthreads();
-      if (level_left == 0) break;
+      left -= ready_count[level & 1];
+      if (left == 0) break;
     }
-    // best member before each child (child order): thread t scans children
-    // [16t, 16t+16); a warp-shuffle scan, then a scan of the warp totals,
-    // gives each thread's incoming best
+    const int level_left = left;
+    if (tid == 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[14]), (unsigned long long)(clock64() - level_start));
+    // best member before each child (child order): each thread's minimum of
+    // (key, victim) over its children, a warp-shuffle scan, then a scan of
+    // the warp totals, gives each thread's incoming best
     const int lane = tid & 31, warp = tid >> 5;
-    const int begin = tid * kPerThread, stop = min(B, begin + kPerThread);
     uint64_t mk = ~0ULL;
     int mv = 0x7fffffff;
-    for (int j = begin; j < stop; ++j) {
-      const uint64_t k = s.c_key[j];
-      const int v = s.c_victim[j];
-      if (key_before(k, v, mk, mv)) { mk = k; mv = v; }
+#pragma unroll
+    for (int h = 0; h < kPerThread; h += kBatch) {
+      uint64_t kv[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) kv[u] = begin + h + u < B ? ckey[begin + h + u] : ~0ULL;
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u)
+        if (begin + h + u < B && key_before(kv[u], int(cand[h + u]), mk, mv)) {
+          mk = kv[u];
+          mv = int(cand[h + u]);
+        }
     }
     for (int o = 1; o < 32; o <<= 1) {
       const uint64_t uk = __shfl_up_sync(kFull, mk, o);
@@ -679,11 +714,25 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
         bv = scan_idx[warp - 1];
       }
     }
-    for (int j = begin; j < stop; ++j) {
-      const int v = s.c_victim[j];
-      if (v == bv) { atomicMin(&redraw_at, j); break; }
-      const uint64_t k = s.c_key[j];
-      if (k < bk || (k == bk && v < bv)) { bk = k; bv = v; }
+    // a child whose victim is the best member before it would have redrawn
+    bool hit = false;
+#pragma unroll
+    for (int h = 0; h < kPerThread; h += kBatch) {
+      uint64_t kv[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) kv[u] = begin + h + u < B ? ckey[begin + h + u] : 0;
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u)
+        if (!hit && begin + h + u < B) {
+          const int v = int(cand[h + u]);
+          if (v == bv) {
+            atomicMin(&redraw_at, begin + h + u);
+            hit = true;
+          } else if (key_before(kv[u], v, bk, bv)) {
+            bk = kv[u];
+            bv = v;
+          }
+        }
     }
     __syncthreads();
     parallel_done = redraw_at == 0x7fffffff;

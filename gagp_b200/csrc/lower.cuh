@@ -144,133 +144,85 @@ __device__ inline int lower_reference(const SearchDesc& s, const LRow& t, int32_
   }
 }
 
-// Accumulator op of a total operation node; A_COUNT when the node may raise
-// a runtime error (then the program runs on the general VM).
-__device__ __forceinline__ uint32_t accumulator_op(const gagp_expression& e) {
-  if (e.node_kind == TK_AND) return A_AND;
-  if (e.node_kind == TK_OR) return A_OR;
-  if (e.node_kind == TK_IF) return A_SELECT;
-  if (e.node_kind != TK_OPERATION) return A_COUNT;
-  switch (e.opcode) {
-    case OP_ADD: return A_ADD;
-    case OP_SUB: return A_SUB;
-    case OP_MUL: return A_MUL;
-    case OP_NEG: return A_NEG;
-    case OP_NOT: return A_NOT;
-    case OP_LT: return A_LT;
-    case OP_LE: return A_LE;
-    case OP_GT: return A_GT;
-    case OP_GE: return A_GE;
-    case OP_EQ: return A_EQ;
-    case OP_NE: return A_NE;
-    case OP_CALL_BUILTIN:
-      switch (e.operand) {
-        case B_ABS: return A_ABS;
-        case B_MIN: return A_MIN;
-        case B_MAX: return A_MAX;
-        case B_IDIV0: return A_IDIV0;
-        case B_IMOD0: return A_IMOD0;
-        case B_TRUNC_DIV0: return A_TDIV0;
-        case B_TRUNC_MOD0: return A_TMOD0;
-        default: return A_COUNT;
-      }
-    default: return A_COUNT;  // DIV (Float result), MOD (ZeroDiv error)
-  }
-}
+// Per-warp shared memory of the accumulator lowering: per-node tables
+// filled by the whole warp, then walked by lane 0.
+constexpr uint8_t kLeafOp = 0xff;
+struct LowerFrame { int16_t node; int8_t stage, count, order[3], spilled[3]; int8_t temp_base; };
+struct LowerScratch {
+  uint8_t aop[kMaxLowerNodes];    // accumulator op (A_COUNT: not total), kLeafOp for leaves
+  uint8_t arity[kMaxLowerNodes];
+  int8_t need[kMaxLowerNodes];    // Sethi-Ullman temporaries of the subtree
+  int16_t end[kMaxLowerNodes];    // one past the subtree
+  uint32_t leaf[kMaxLowerNodes];  // leaves: operand kind << 16 | index
+  LowerFrame st[64];
+};
 
-// Accumulator program of a row; returns the instruction count, or -1 when the
-// row needs the general VM.  *temps_out: temporaries used.  MAXN bounds the
-// row length (the per-thread working arrays).
-template <int MAXN>
-__device__ inline int lower_accumulator(const SearchDesc& s, const LRow& t, uint2* code, int code_cap,
-                                        int64_t* kpool, int* kpool_len, int* temps_out) {
-  (void)kpool_len;
-  const int n = t.n;
-  if (n <= 0 || n > MAXN) return -1;
+// Subtree ends, needs and code emission of lower_accumulator_warp (one lane).
+__device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code, int code_cap, int* temps_out) {
   // child positions and Sethi-Ullman temporaries, children after parents
-  int16_t end[MAXN];
-  int8_t need[MAXN];
-  int16_t constant_index[MAXN];
-  {
-    int k = 0;
-    for (int i = 0; i < n; ++i) constant_index[i] = w_const(t.node[i]) ? int16_t(k++) : int16_t(-1);
-  }
   for (int i = n - 1; i >= 0; --i) {
-    const gagp_expression& e = s.ex[w_origin(t.node[i])];
-    const int a = e.arity;
-    if (a == 0) { end[i] = int16_t(i + 1); need[i] = 0; continue; }
-    if (accumulator_op(e) == A_COUNT) return -1;
+    const int a = m.arity[i];
+    if (a == 0) { m.end[i] = int16_t(i + 1); m.need[i] = 0; continue; }
     int c = i + 1, needs[3], nonleaf = 0;
     for (int k = 0; k < a; ++k) {
       if (c >= n) return -1;
-      if (end[c] - c > 1) needs[nonleaf++] = need[c];
-      c = end[c];
+      if (m.end[c] - c > 1) needs[nonleaf++] = m.need[c];
+      c = m.end[c];
     }
-    end[i] = int16_t(c);
+    m.end[i] = int16_t(c);
     // temporaries: non-leaf children by decreasing need, all but the last spilled
     for (int x = 0; x < nonleaf; ++x)
       for (int y = x + 1; y < nonleaf; ++y)
         if (needs[y] > needs[x]) { const int tmp = needs[x]; needs[x] = needs[y]; needs[y] = tmp; }
-    int m = 0;
-    for (int x = 0; x < nonleaf; ++x) m = max(m, needs[x] + x);
-    need[i] = int8_t(min(m, 127));
+    int mx = 0;
+    for (int x = 0; x < nonleaf; ++x) mx = max(mx, needs[x] + x);
+    m.need[i] = int8_t(min(mx, 127));
   }
-  if (end[0] != n) return -1;
-  if (need[0] > kMaxTemps) return -1;
-  *temps_out = need[0];
-  // constant pool: the row constants in prefix order
-  for (int k = 0; k < t.nc; ++k) kpool[k] = t.cval[k];
-  *kpool_len = t.nc;
-  auto leaf_kind = [&](int i) -> uint32_t {
-    return constant_index[i] >= 0 ? K_CONST : K_INPUT;
-  };
-  auto leaf_index = [&](int i) -> uint32_t {
-    return constant_index[i] >= 0 ? uint32_t(constant_index[i]) : uint32_t(s.ex[w_origin(t.node[i])].operand);
-  };
-  // explicit-stack post order emission
-  struct Frame { int16_t node; int8_t stage, count, order[3], spilled[3]; int8_t temp_base; };
-  Frame st[64];
+  if (m.end[0] != n) return -1;
+  if (m.need[0] > kMaxTemps) return -1;
+  *temps_out = m.need[0];
   int sp = 0, len = 0, temp_top = 0;
   auto put = [&](uint2 x) -> bool { if (len >= code_cap) return false; code[len++] = x; return true; };
-  // a leaf root
-  if (end[0] - 0 == 1) {
+  auto leaf_kind = [&](int i) -> uint32_t { return m.leaf[i] >> 16; };
+  auto leaf_index = [&](int i) -> uint32_t { return m.leaf[i] & 0xffffu; };
+  if (m.end[0] == 1) {  // a leaf root
     if (!put(a_instr(A_MOV, false, leaf_kind(0), leaf_index(0)))) return -1;
     return len;
   }
-  auto push = [&](int node) -> bool {
+  auto child_at = [&](int nd, int x) -> int {
+    int c = nd + 1;
+    for (int k = 0; k < x; ++k) c = m.end[c];
+    return c;
+  };
+  auto push = [&](int nd) -> bool {
     if (sp >= 64) return false;
-    Frame& f = st[sp++];
-    f.node = int16_t(node);
+    LowerFrame& f = m.st[sp++];
+    f.node = int16_t(nd);
     f.stage = 0;
     f.temp_base = int8_t(temp_top);
     // non-leaf children in evaluation order (decreasing need, stable)
-    const int a = s.ex[w_origin(t.node[node])].arity;
-    int c = node + 1, k = 0;
+    const int a = m.arity[nd];
     int8_t kids[3];
-    for (int x = 0; x < a; ++x) { kids[x] = int8_t(c - node); c = end[c]; }
-    f.count = 0;
+    int c = nd + 1;
+    for (int x = 0; x < a; ++x) { kids[x] = int8_t(c - nd); c = m.end[c]; }
+    int count = 0;
     for (int x = 0; x < a; ++x) {
-      const int ch = node + kids[x];
-      if (end[ch] - ch > 1) f.order[f.count++] = int8_t(x);
+      const int ch = nd + kids[x];
+      if (m.end[ch] - ch > 1) f.order[count++] = int8_t(x);
     }
-    for (int x = 0; x < f.count; ++x)
-      for (int y = x + 1; y < f.count; ++y) {
-        const int cx = node + kids[f.order[x]], cy = node + kids[f.order[y]];
-        if (need[cy] > need[cx]) { const int8_t tmp = f.order[x]; f.order[x] = f.order[y]; f.order[y] = tmp; }
+    f.count = int8_t(count);
+    for (int x = 0; x < count; ++x)
+      for (int y = x + 1; y < count; ++y) {
+        const int cx = nd + kids[f.order[x]], cy = nd + kids[f.order[y]];
+        if (m.need[cy] > m.need[cx]) { const int8_t tmp = f.order[x]; f.order[x] = f.order[y]; f.order[y] = tmp; }
       }
     for (int x = 0; x < 3; ++x) f.spilled[x] = -1;
-    (void)k;
     return true;
-  };
-  auto child_at = [&](int node, int x) -> int {
-    int c = node + 1;
-    for (int k = 0; k < x; ++k) c = end[c];
-    return c;
   };
   if (!push(0)) return -1;
   while (sp) {
-    Frame& f = st[sp - 1];
-    const int node = f.node;
+    LowerFrame& f = m.st[sp - 1];
+    const int nd = f.node;
     if (f.stage < f.count) {
       // before evaluating the next non-leaf child, spill the previous one
       if (f.stage > 0) {
@@ -280,20 +232,19 @@ __device__ inline int lower_accumulator(const SearchDesc& s, const LRow& t, uint
         if (!put(a_instr(A_SPILL, false, K_TEMP, uint32_t(temp_top)))) return -1;
         ++temp_top;
       }
-      const int child = child_at(node, f.order[f.stage]);
+      const int child = child_at(nd, f.order[f.stage]);
       ++f.stage;
       if (!push(child)) return -1;
       continue;
     }
     // all non-leaf children evaluated: the last one (if any) is in ACC
-    const gagp_expression& e = s.ex[w_origin(t.node[node])];
-    const uint32_t op = accumulator_op(e);
-    const int a = e.arity;
+    const uint32_t op = m.aop[nd];
+    const int a = m.arity[nd];
     uint32_t kind[3] = {K_ACC, K_ACC, K_ACC}, idx[3] = {0, 0, 0};
     const int last = f.count ? f.order[f.count - 1] : -1;
     for (int x = 0; x < a; ++x) {
-      const int ch = child_at(node, x);
-      if (end[ch] - ch == 1) { kind[x] = leaf_kind(ch); idx[x] = leaf_index(ch); }
+      const int ch = child_at(nd, x);
+      if (m.end[ch] - ch == 1) { kind[x] = leaf_kind(ch); idx[x] = leaf_index(ch); }
       else if (x == last) { kind[x] = K_ACC; }
       else { kind[x] = K_TEMP; idx[x] = uint32_t(f.spilled[x]); }
     }
@@ -317,6 +268,88 @@ __device__ inline int lower_accumulator(const SearchDesc& s, const LRow& t, uint
     --sp;
   }
   return len;
+}
+
+__device__ __forceinline__ uint32_t accumulator_op_of(int node_kind, int opcode, int operand) {
+  if (node_kind == TK_AND) return A_AND;
+  if (node_kind == TK_OR) return A_OR;
+  if (node_kind == TK_IF) return A_SELECT;
+  if (node_kind != TK_OPERATION) return A_COUNT;
+  switch (opcode) {
+    case OP_ADD: return A_ADD;
+    case OP_SUB: return A_SUB;
+    case OP_MUL: return A_MUL;
+    case OP_NEG: return A_NEG;
+    case OP_NOT: return A_NOT;
+    case OP_LT: return A_LT;
+    case OP_LE: return A_LE;
+    case OP_GT: return A_GT;
+    case OP_GE: return A_GE;
+    case OP_EQ: return A_EQ;
+    case OP_NE: return A_NE;
+    case OP_CALL_BUILTIN:
+      switch (operand) {
+        case B_ABS: return A_ABS;
+        case B_MIN: return A_MIN;
+        case B_MAX: return A_MAX;
+        case B_IDIV0: return A_IDIV0;
+        case B_IMOD0: return A_IMOD0;
+        case B_TRUNC_DIV0: return A_TDIV0;
+        case B_TRUNC_MOD0: return A_TMOD0;
+        default: return A_COUNT;
+      }
+    default: return A_COUNT;  // DIV (Float result), MOD (ZeroDiv error)
+  }
+}
+
+// Accumulator program of a row, by one warp; returns the instruction count
+// (the same on every lane), or -1 when the row needs the general VM.
+// *temps_out: temporaries used.  The lanes classify the nodes, number the
+// constants, copy the constant pool and bound the bytecode length in
+// parallel; lane 0 then computes subtree ends and Sethi-Ullman needs and
+// emits the code, reading only shared memory.
+__device__ inline int lower_accumulator_warp(const SearchDesc& s, const uint64_t* node, int n, const int64_t* cval,
+                                             int nc, uint2* code, int code_cap, int64_t* kpool, LowerScratch& m,
+                                             int* temps_out) {
+  const int lane = threadIdx.x & 31;
+  if (n <= 0 || n > kMaxLowerNodes) return -1;
+  const ExprInfo* __restrict__ info = s.info;
+  bool total = true;
+  int bytecode = 0, constants = 0;
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    const uint64_t w = i < n ? node[i] : 0;
+    const bool is_const = i < n && w_const(w);
+    const unsigned const_mask = __ballot_sync(kFull, is_const);
+    if (i < n) {
+      const int o = w_origin(w);
+      const int arity = __ldg(&info[o].arity), nk = __ldg(&info[o].node_kind);
+      m.arity[i] = uint8_t(arity);
+      if (arity == 0) {
+        m.aop[i] = kLeafOp;
+      } else {
+        const uint32_t op = accumulator_op_of(nk, __ldg(&info[o].opcode), __ldg(&info[o].operand));
+        m.aop[i] = uint8_t(op);
+        total &= op != A_COUNT && arity <= 3;
+      }
+      bytecode += nk == TK_IF ? 2 : (nk == TK_AND || nk == TK_OR) ? 5 : 1;
+      // leaves: the row constants in prefix order, or the input operand
+      m.leaf[i] = is_const ? (K_CONST << 16) | uint32_t(constants + __popc(const_mask & ((1u << lane) - 1)))
+                           : (K_INPUT << 16) | uint32_t(__ldg(&info[o].operand) & 0xffff);
+    }
+    constants += __popc(const_mask);
+  }
+  for (int k = lane; k < nc; k += 32) kpool[k] = cval[k];
+  total = __all_sync(kFull, total);
+  for (int o = 16; o; o >>= 1) bytecode += __shfl_xor_sync(kFull, bytecode, o);
+  bytecode += 1;
+  __syncwarp();
+  // the exact bytecode length (a bound of every executed path) must fit the fuel
+  if (!total || bytecode > s.fuel) return -1;
+  int len = -1;
+  if (lane == 0) len = lower_accumulator_emit(m, n, code, code_cap, temps_out);
+  __syncwarp();
+  return __shfl_sync(kFull, len, 0);
 }
 
 }  // namespace gb

@@ -61,9 +61,11 @@ __device__ inline void load_member(const SearchDesc& s, int m, SRow& to) {
 
 // One child, by one warp.  Writes the child row, its parent and reuse
 // source (the parent when the genotype is unchanged) and returns the
-// reference's OperatorStats error code (0: none).
+// reference's OperatorStats error code (0: none).  stamp[0..2]: SM clock
+// after selection, after crossover, after the mutation's subtree generation
+// (left 0 for phases not reached).
 __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t seed, WarpRows& w, int* reuse_out,
-                                      int* parent_out) {
+                                      int* parent_out, long long* stamp) {
   const int lane = lane_id();
   *reuse_out = -1;
   // ---- crossover_child
@@ -72,6 +74,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
   *parent_out = parent;
   load_member(s, parent, w.parent);
   load_member(s, donor, w.donor);
+  stamp[0] = clock64();
   if (w.parent.n <= 0 || w.parent.n > s.maxv || w.parent.nc > w.parent.n) return 1;
   warp_copy(w.parent.node, w.parent.cval, w.parent.n, w.parent.nc, w.child.node, w.child.cval);
   w.child.n = w.parent.n;
@@ -97,6 +100,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
       }
     }
   }
+  stamp[1] = clock64();
   // ---- mutate_child
   {
     Rng m(seed ^ (0x124ab512bf01ULL + uint64_t(child)));
@@ -125,6 +129,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
         g.nodes = __shfl_sync(kFull, g.nodes, 0);
         g.constants = __shfl_sync(kFull, g.constants, 0);
         __syncwarp();
+        stamp[2] = clock64();
         if (capped && g.status == ST_CAPACITY) {
           // a configured cap without a feasible derivation skips this mutation
         } else if (g.status != ST_OK) {

@@ -47,6 +47,9 @@ struct SearchDesc {
   const gagp_domain* doms;
   const gagp_value* vals;
   const uint32_t* minimum;
+  // minimum of each production's expression, production-major per (depth,
+  // site budget): prod_minimum[(d * logical_count + l) * n_prods + p]
+  const uint32_t* prod_minimum;
   const int32_t* local_types;          // ValueTag of each evaluator input
   int32_t n_ex, n_prods, n_nts, n_doms, n_vals;
   int32_t depth_count, logical_count, site_depth;
@@ -76,7 +79,6 @@ struct SearchDesc {
   int32_t* c_parent; int32_t* c_reuse; int32_t* c_error;
   double* c_fitness; uint32_t* c_wrong; uint32_t* c_nodes; uint64_t* c_key;
   int32_t* c_eval;                     // 1: evaluate this child
-  int32_t* c_victim;                   // member each child replaced (level-parallel placement)
   // ---- lowered programs (children, or members during the initial evaluation)
   uint2* code; int32_t* code_len; int64_t* kpool;
   int32_t code_stride;                 // accumulator instructions per program slot

@@ -140,11 +140,14 @@ class Engine:
         return ms.value
 
     def counters(self, search: Search) -> dict:
-        out = (C.c_uint64 * 16)()
-        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out, C.c_int32(16)))
+        out = (C.c_uint64 * 24)()
+        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out, C.c_int32(24)))
         return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2], "vm_ops": out[3],
                 "place_generate_cycles": out[4], "place_stage_cycles": out[5], "place_serial_cycles": out[6],
-                "place_levels": out[7], "vary_bytes": out[8], "lower_bytes": out[9]}
+                "place_levels": out[7], "vary_bytes": out[8], "lower_bytes": out[9],
+                "vary_select_cycles": out[10], "vary_crossover_cycles": out[11], "vary_generate_cycles": out[12],
+                "vary_rest_cycles": out[13], "place_level_cycles": out[14], "vary_max_child_cycles": out[15],
+                "vary_max_phase_cycles": list(out[16:20]), "vary_slow_children": out[20]}
 
     def transfers(self) -> tuple:
         """(host->device, device->host) bytes copied by this engine so far."""

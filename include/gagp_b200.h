@@ -241,14 +241,20 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
  * [7] placement levels (+2^20 per sequential replay), [8] bytes the
  * variation kernel moved (parent, donor and child rows, tournament keys,
  * per-child outputs), [9] bytes the lowering kernel moved (rows read, code
- * and constants written).  Copies min(count, GAGP_COUNTERS) entries
+ * and constants written), [10..13] SM clock cycles of the variation warps
+ * summed over children (selection, crossover, mutation subtree generation,
+ * the rest), [14] cycles of the placement's level loop, [15] the most
+ * cycles one child's variation took, [16..19] the most cycles of one child
+ * in each variation phase, [20] children whose variation took over 200000
+ * cycles, [21..23] reserved.
+ * Copies min(count, GAGP_COUNTERS) entries
  * (synchronous). */
 /* Bytes this engine's calls have copied host->device and device->host since
  * it was created (uploads at admission and batch launches, progress and
  * result reads). */
 gagp_status gagp_b200_engine_transfers(gagp_engine* engine, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
-#define GAGP_COUNTERS 16
+#define GAGP_COUNTERS 24
 gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out, int32_t count);
 
 /* Per-kernel CUDA-event timing: enable (resets) or disable, then read the
