@@ -350,7 +350,11 @@ def run_own_arm(args, rank: int, world: int, local: int):
                                                              "vary_generate_cycles", "vary_rest_cycles")},
                          "vary_max_child_cycles": after["vary_max_child_cycles"],
                          "vary_max_phase_cycles": after["vary_max_phase_cycles"],
-                         "vary_slow_children": after["vary_slow_children"] - before["vary_slow_children"]}}
+                         "vary_slow_children": after["vary_slow_children"] - before["vary_slow_children"],
+                         "generate_steps_per_generation": (after["generate_steps"] - before["generate_steps"]) /
+                         max(1, after["generations"] - before["generations"]),
+                         "generations_per_step": (after["generations"] - before["generations"]) / args.steps,
+                         "generate_max_steps": after["generate_max_steps"]}}
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as d:
             make_task(seed, d)

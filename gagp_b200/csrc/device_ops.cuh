@@ -57,6 +57,20 @@ struct Rng {
     if (bits < sign) return int64_t(bits);
     return INT64_MIN + int64_t(bits - sign);
   }
+  // bounded(upper) for a fixed upper with its rejection bound
+  // ((2^64 - upper) mod upper) and magic floor((2^64 - 1) / upper) given:
+  // the residue comes from a multiply-high quotient estimate, at most two
+  // below the true quotient, and at most two corrections
+  __device__ __forceinline__ uint64_t bounded_fixed(uint64_t upper, uint64_t threshold, uint64_t magic) {
+    for (;;) {
+      const uint64_t v = next();
+      if (v >= threshold) {
+        uint64_t r = v - __umul64hi(v, magic) * upper;
+        while (r >= upper) r -= upper;
+        return r;
+      }
+    }
+  }
   // 53-bit uniform in [0,1): exact (a power-of-two scale)
   __device__ __forceinline__ double unit() { return __dmul_rn(double(next() >> 11), 0x1.0p-53); }
 };
@@ -104,6 +118,7 @@ __device__ __forceinline__ uint32_t class_of_entry(const SearchDesc& s, int entr
 
 struct GenResult {
   int status, nodes, constants;
+  int steps;  // tasks processed
 };
 
 // Minimum node cost of (expression, depth, site budget); kNoId when infeasible.
@@ -122,68 +137,100 @@ __device__ __forceinline__ unsigned minimum_of(const SearchDesc& s, int e, int d
 // (root = 1) and site depth relative to the budget `logical_depth`.
 __device__ inline GenResult generate(const SearchDesc& s, int root_expression, int scope_count, int depth,
                                      int capacity, uint64_t seed, uint64_t* out_node, int64_t* out_cval,
-                                     int logical_depth, uint32_t* pending) {
-  GenResult result{ST_INVALID, 0, 0};
+                                     int logical_depth, uint64_t* pending) {
+  GenResult result{ST_INVALID, 0, 0, 0};
   // the tables, read once into registers: every table load below is a
   // read-only load through these
-  const gagp_expression* __restrict__ ex = s.ex;
-  const ExprInfo* __restrict__ info_tab = s.info;
+  const GenExpr* __restrict__ gx = s.gen_expr;
+  const GenNt* __restrict__ gnt = s.gen_nt;
   const gagp_production* __restrict__ prods = s.prods;
-  const gagp_nonterminal* __restrict__ nts = s.nts;
   const gagp_domain* __restrict__ doms = s.doms;
   const gagp_value* __restrict__ vals = s.vals;
   const uint32_t* __restrict__ minimum = s.minimum;
   const uint32_t* __restrict__ prod_minimum = s.prod_minimum;
+  const uint32_t* __restrict__ nt_maxmin = s.nt_maxmin;
+  const double* __restrict__ nt_total = s.nt_total;
+  const double* __restrict__ prod_threshold = s.prod_threshold;
   const int n_ex = s.n_ex, n_nts = s.n_nts, n_prods = s.n_prods, n_doms = s.n_doms, n_vals = s.n_vals;
   const int depth_count = s.depth_count, logical_count = s.logical_count;
   const bool site_limited = s.site_depth > 0;
   auto min_of = [&](int e, int d, int l) -> unsigned {
     if (e < 0 || e >= n_ex || d < 0 || d >= depth_count || l < 0 || l >= logical_count) return kNoId;
-    return __ldg(&minimum[(size_t(e) * depth_count + d) * logical_count + l]);
+    return __ldg(&minimum[(e * depth_count + d) * logical_count + l]);
   };
-  int steps = 0;
   int next_site = -1;  // entry expression of a pending site
+  uint32_t next_class = kNoClass;
   if (root_expression < 0 || root_expression >= n_ex || scope_count < 0 || scope_count > 15 || depth <= 0 ||
       depth >= depth_count || depth > 64 || logical_depth < 0 || logical_depth >= logical_count ||
       capacity <= 0 || capacity > kCapacity || n_ex > 131071)
     return result;
   if (capacity > s.stride) capacity = s.stride;  // callers pass at most the node budget
-  const unsigned unselected = 131071u;
   int count = 1;
-  auto pack = [](unsigned e, unsigned d, unsigned n, unsigned l) -> uint32_t {
-    return e | (d << 17) | (n << 24) | (l << 28);
+  // a task: expression, depth, scope, site budget and its minimum cost (the
+  // reservation made when it was pushed)
+  auto pack = [](unsigned e, unsigned d, unsigned n, unsigned l, unsigned required) -> uint64_t {
+    return uint64_t(e | (d << 17) | (n << 24) | (l << 28)) | (uint64_t(required) << 32);
   };
-  pending[0] = pack(unsigned(root_expression), unsigned(depth), unsigned(scope_count), unsigned(logical_depth));
   unsigned reserved = min_of(root_expression, depth, logical_depth);
+  pending[0] = pack(unsigned(root_expression), unsigned(depth), unsigned(scope_count), unsigned(logical_depth),
+                    reserved);
   if (reserved > unsigned(capacity)) { result.status = ST_CAPACITY; return result; }
   Rng random(seed);
   while (count) {
-    if (++steps > 8192) { result.status = ST_CAPACITY; return result; }
-    const uint32_t task = pending[--count];
+    if (++result.steps > 8192) { result.status = ST_CAPACITY; return result; }
+    const uint64_t task = pending[--count];
     const int t_expr = int(task & 0x1ffffu), t_depth = int((task >> 17) & 0x7fu);
-    const int t_scope = int((task >> 24) & 0xfu), t_logical = int(task >> 28);
-    const unsigned required = min_of(t_expr, t_depth, t_logical);
+    const int t_scope = int((task >> 24) & 0xfu), t_logical = int((task >> 28) & 0xfu);
+    const unsigned required = unsigned(task >> 32);
     if (required > reserved) return result;
     reserved -= required;
-    const gagp_expression* expression = ex + t_expr;
-    const int kind = __ldg(&info_tab[t_expr].kind);
+    const int4 ra = __ldg(reinterpret_cast<const int4*>(gx + t_expr));      // children
+    const int4 rb = __ldg(reinterpret_cast<const int4*>(gx + t_expr) + 1);  // target, class, kinds, scopes
+    const int kind = int(int8_t(rb.z & 0xff)), arity = int(int8_t((rb.z >> 8) & 0xff));
+    const int e_scopes = int(int8_t((rb.z >> 16) & 0xff));
+    const int target = rb.x;
     if (kind == EK_REFERENCE) {
-      const int target = __ldg(&expression->target), e_scopes = __ldg(&expression->scope_count);
       if (target < 0 || target >= n_nts || e_scopes < 0 || e_scopes > 8) return result;
       if (next_site >= 0) return result;
       next_site = t_expr;
-      const int nt_offset = __ldg(&nts[target].production_offset), nt_count = __ldg(&nts[target].production_count);
-      const bool normalized = __ldg(&nts[target].normalized_weights) != 0;
-      if (__ldg(&nts[target].scope_count) != e_scopes || nt_offset < 0 || nt_count <= 0 || nt_offset > n_prods ||
-          nt_count > n_prods - nt_offset)
+      next_class = uint32_t(rb.y);
+      const int4 nt = __ldg(reinterpret_cast<const int4*>(gnt + target));
+      const int nt_offset = nt.x, nt_count = nt.y;
+      const bool normalized = nt.w != 0;
+      if (nt.z != e_scopes || nt_offset < 0 || nt_count <= 0 || nt_offset > n_prods || nt_count > n_prods - nt_offset)
         return result;
       if (site_limited && t_logical == 0) { result.status = ST_CAPACITY; return result; }
       const int n_logical = t_logical - (site_limited ? 1 : 0);
-      unsigned next_expr = unselected;
+      unsigned next_expr = 131071u;  // unselected
       if (reserved > unsigned(capacity - result.nodes)) { result.status = ST_CAPACITY; return result; }
       const unsigned available = unsigned(capacity - result.nodes) - reserved;
+      const uint32_t* __restrict__ prow = prod_minimum + (t_depth * logical_count + n_logical) * n_prods + nt_offset;
+      const double all_total = __ldg(&nt_total[target]);
+      if (__ldg(&nt_maxmin[(t_depth * logical_count + n_logical) * n_nts + target]) <= available &&
+          all_total == all_total) {
+        // every production feasible: the precomputed thresholds give the
+        // production the sequential subtraction stops at
+        const double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), all_total);
+        int pick = nt_count - 1;
+        if (nt_count <= 8) {
+          double th[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) th[k] = k < nt_count ? __ldg(&prod_threshold[nt_offset + k]) : 0.0;
+#pragma unroll
+          for (int k = 7; k >= 0; --k)
+            if (k < nt_count && choice < th[k]) pick = k;
+        } else {
+          for (int i = 0; i < nt_count; ++i)
+            if (choice < __ldg(&prod_threshold[nt_offset + i])) { pick = i; break; }
+        }
+        next_expr = unsigned(__ldg(&prods[nt_offset + pick].expression));
+        const unsigned need = __ldg(&prow[pick]);
+        if (count >= 192) return result;
+        reserved += need;
+        pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical), need);
+        continue;
+      }
       // feasibility of each production (a bit mask for the first 64)
-      const uint32_t* __restrict__ prow = prod_minimum + (size_t(t_depth) * logical_count + n_logical) * n_prods + nt_offset;
       uint64_t feasible_mask = 0;
       for (int i = 0; i < nt_count && i < 64; ++i)
         if (__ldg(&prow[i]) <= available) feasible_mask |= 1ULL << i;
@@ -210,28 +257,28 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
         choice = __dsub_rn(choice, normalized ? w : __ddiv_rn(w, maximum));
         if (choice < 0) break;
       }
-      if (next_expr == unselected || count >= 192) return result;
-      reserved += min_of(int(next_expr), t_depth, n_logical);
-      pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical));
+      if (next_expr == 131071u || count >= 192) return result;
+      const unsigned need = min_of(int(next_expr), t_depth, n_logical);
+      reserved += need;
+      pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical), need);
       continue;
     }
     if (kind == EK_ALIAS) {
-      const int child = __ldg(&expression->children[0]);
+      const int child = ra.x;
       if (child < 0 || child >= n_ex || count >= 192) return result;
-      const int child_scope = __ldg(&expression->child_scope[0]);
+      const int child_scope = int(int8_t(rb.w & 0xff));
       const int scope = child_scope >= 0 ? child_scope : t_scope;
-      reserved += min_of(child, t_depth, t_logical);
-      pending[count++] = pack(unsigned(child), unsigned(t_depth), unsigned(scope), unsigned(t_logical));
+      const unsigned need = min_of(child, t_depth, t_logical);
+      reserved += need;
+      pending[count++] = pack(unsigned(child), unsigned(t_depth), unsigned(scope), unsigned(t_logical), need);
       continue;
     }
     if (t_depth <= 0 || result.nodes >= capacity) { result.status = ST_CAPACITY; return result; }
-    const int arity = __ldg(&info_tab[t_expr].arity);
-    if (arity < 0 || arity > 8) return result;
+    if (arity < 0 || arity > 3) return result;  // admission bounds operation arity by 3
     if (kind == EK_BOUND) {
-      const int operand = __ldg(&expression->operand);
+      const int operand = __ldg(&s.ex[t_expr].operand);
       if (arity != 0 || operand < 0 || operand >= 16) return result;
     } else if (kind == EK_CONSTANT) {
-      const int target = __ldg(&expression->target);
       if (target < 0 || target >= n_doms || arity != 0) return result;
       const gagp_domain* domain = doms + target;
       int64_t value;
@@ -250,21 +297,25 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
     } else if (kind != EK_OPERATION && kind != EK_INPUT) {
       return result;
     }
-    const uint32_t cls = next_site < 0 ? kNoClass : uint32_t(__ldg(&info_tab[next_site].site_class));
     out_node[result.nodes++] = w_make(t_expr, next_site, depth - t_depth + 1, logical_depth - t_logical, arity,
-                                      kind == EK_CONSTANT, cls);
+                                      kind == EK_CONSTANT, next_class);
     next_site = -1;
+    next_class = kNoClass;
+    // the children's minimum costs, loaded together, then pushed last to first
+    const unsigned need0 = arity > 0 ? min_of(ra.x, t_depth - 1, t_logical) : 0;
+    const unsigned need1 = arity > 1 ? min_of(ra.y, t_depth - 1, t_logical) : 0;
+    const unsigned need2 = arity > 2 ? min_of(ra.z, t_depth - 1, t_logical) : 0;
     for (int i = arity - 1; i >= 0; --i) {
       if (count >= 192) { result.status = ST_CAPACITY; return result; }
-      const int child = __ldg(&expression->children[i]);
-      const unsigned need = min_of(child, t_depth - 1, t_logical);
+      const int child = i == 0 ? ra.x : i == 1 ? ra.y : ra.z;
+      const unsigned need = i == 0 ? need0 : i == 1 ? need1 : need2;
       if (need > unsigned(capacity - result.nodes) || reserved > unsigned(capacity - result.nodes) - need) {
         result.status = ST_CAPACITY;
         return result;
       }
-      const int child_scope = __ldg(&expression->child_scope[i]);
+      const int child_scope = int(int8_t((rb.w >> (8 * i)) & 0xff));
       const int scope = child_scope >= 0 ? child_scope : t_scope;
-      pending[count++] = pack(unsigned(child), unsigned(t_depth - 1), unsigned(scope), unsigned(t_logical));
+      pending[count++] = pack(unsigned(child), unsigned(t_depth - 1), unsigned(scope), unsigned(t_logical), need);
       reserved += need;
     }
   }

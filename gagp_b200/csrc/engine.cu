@@ -69,6 +69,12 @@ struct gagp_engine {
   // side stream of the run-generator top-up, forked from and joined to `stream`
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // the children of a round in kChunks ranges, each varied, lowered and
+  // evaluated on its own stream so that one range's slowest children
+  // overlap the other ranges' work
+  static constexpr int kChunks = 4;
+  cudaStream_t chunk_stream[kChunks] = {};
+  cudaEvent_t chunk_fork = nullptr, chunk_done[kChunks] = {};
   std::map<int, std::unique_ptr<Search>> searches;
   int next_id = 1;
   uint64_t arena_limit = 0, arena_used = 0;
@@ -166,7 +172,7 @@ gagp_status ensure_lists(gagp_engine* e, size_t items) {
   const size_t cap = std::max<size_t>(items, 1024);
   CUDA_TRY(cudaMalloc(&e->d_fast, cap * sizeof(gb::ProgramRef)));
   CUDA_TRY(cudaMalloc(&e->d_general, cap * sizeof(gb::ProgramRef)));
-  if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, 4 * sizeof(int32_t)));
+  if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, 4 * gagp_engine::kChunks * sizeof(int32_t)));
   e->list_capacity = cap;
   return GAGP_OK;
 }
@@ -231,9 +237,77 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
   return GAGP_OK;
 }
 
+// Precomputed production draws (generate_phase's weighted choice,
+// cpp/src/evolution/repro/gpu/device/phase_generate.cuh:125-270) for the
+// case where every production of a nonterminal is feasible.  The choice
+// value c = u * total is compared against thresholds instead of subtracting
+// the weights one by one: with f_i(c) = (((c - v_0) - v_1) ... - v_i), each
+// step rounded to nearest in double precision, f_i is non-decreasing in c,
+// so f_i(c) < 0 exactly when c is below the smallest double T_i with
+// f_i(T_i) >= 0, found here by bisection over the bit patterns of
+// non-negative doubles.  The first production whose threshold exceeds c is
+// the one the sequential loop stops at (the last one when none does).
+struct DrawTables {
+  std::vector<uint32_t> maxmin;
+  std::vector<double> total, threshold;
+};
+DrawTables draw_tables(const gagp_grammar* g) {
+  const int E = g->expression_count, PR = g->production_count, NT = g->nonterminal_count;
+  const int DC = g->depth_count, LC = g->logical_depth_count;
+  DrawTables t;
+  t.maxmin.assign(size_t(std::max(1, NT)) * DC * LC, gb::kNoId);
+  t.total.assign(size_t(std::max(1, NT)), std::nan(""));
+  t.threshold.assign(size_t(std::max(1, PR)), 0.0);
+  for (int nt = 0; nt < NT; ++nt) {
+    const gagp_nonterminal& n = g->nonterminals[nt];
+    const int off = n.production_offset, cnt = n.production_count;
+    if (cnt <= 0 || off < 0 || off > PR || cnt > PR - off) continue;
+    bool valid = true;
+    double maximum = n.normalized_weights ? 1.0 : 0.0;
+    for (int i = 0; i < cnt; ++i) {
+      const gagp_production& p = g->productions[off + i];
+      if (p.expression < 0 || p.expression >= E) valid = false;
+      if (!n.normalized_weights && p.weight > maximum) maximum = p.weight;
+    }
+    if (!valid || !(maximum > 0)) continue;
+    std::vector<double> v(cnt);
+    double total = 0.0;
+    for (int i = 0; i < cnt; ++i) {
+      const double w = g->productions[off + i].weight;
+      v[i] = n.normalized_weights ? w : w / maximum;
+      total = total + v[i];
+    }
+    auto f = [&](double c, int i) {
+      double x = c;
+      for (int k = 0; k <= i; ++k) x = x - v[k];
+      return x;
+    };
+    auto from_bits = [](uint64_t b) { double d; std::memcpy(&d, &b, sizeof d); return d; };
+    for (int i = 0; i < cnt; ++i) {
+      if (f(0.0, i) >= 0) { t.threshold[off + i] = 0.0; continue; }
+      uint64_t lo = 0, hi = 0x7ff0000000000000ULL;  // f_i(lo) < 0 <= f_i(hi)
+      while (hi - lo > 1) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        if (f(from_bits(mid), i) >= 0) hi = mid; else lo = mid;
+      }
+      t.threshold[off + i] = from_bits(hi);
+    }
+    t.total[nt] = total;
+    for (int d = 0; d < DC; ++d)
+      for (int l = 0; l < LC; ++l) {
+        uint32_t m = 0;
+        for (int i = 0; i < cnt; ++i)
+          m = std::max(m, g->minimum[(size_t(g->productions[off + i].expression) * DC + d) * LC + l]);
+        t.maxmin[(size_t(d) * LC + l) * NT + nt] = m;
+      }
+  }
+  return t;
+}
+
 struct Plan {
   Layout L;
-  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, local_types, inputs, expected;
+  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, nt_maxmin, nt_total, prod_threshold, gen_expr,
+      gen_nt, local_types, inputs, expected;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
   size_t code, code_len, kpool, code_temps, bc, bc_len, bc_consts;
@@ -269,6 +343,12 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.minimum = L.take(sizeof(uint32_t) * size_t(E) * g->depth_count * g->logical_depth_count);
   p.prod_minimum = L.take(sizeof(uint32_t) * size_t(std::max(1, g->production_count)) * g->depth_count *
                           g->logical_depth_count);
+  p.nt_maxmin = L.take(sizeof(uint32_t) * size_t(std::max(1, g->nonterminal_count)) * g->depth_count *
+                       g->logical_depth_count);
+  p.nt_total = L.take(sizeof(double) * size_t(std::max(1, g->nonterminal_count)));
+  p.prod_threshold = L.take(sizeof(double) * size_t(std::max(1, g->production_count)));
+  p.gen_expr = L.take(sizeof(gb::GenExpr) * size_t(E));
+  p.gen_nt = L.take(sizeof(gb::GenNt) * size_t(std::max(1, g->nonterminal_count)));
   p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
   p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
   p.expected = L.take(sizeof(int64_t) * C);
@@ -320,6 +400,11 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&e->chunk_fork, cudaEventDisableTiming));
+  for (int c = 0; c < gagp_engine::kChunks; ++c) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->chunk_stream[c], cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->chunk_done[c], cudaEventDisableTiming));
+  }
   cudaDeviceProp prop;
   CUDA_TRY(cudaGetDeviceProperties(&prop, device));
   e->sm_count = prop.multiProcessorCount;
@@ -354,6 +439,11 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   if (e->side) cudaStreamDestroy(e->side);
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->join) cudaEventDestroy(e->join);
+  if (e->chunk_fork) cudaEventDestroy(e->chunk_fork);
+  for (int c = 0; c < gagp_engine::kChunks; ++c) {
+    if (e->chunk_stream[c]) cudaStreamDestroy(e->chunk_stream[c]);
+    if (e->chunk_done[c]) cudaEventDestroy(e->chunk_done[c]);
+  }
   delete e;
 }
 
@@ -436,6 +526,33 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
         if (pe >= 0 && pe < E) prod_minimum[(size_t(d) * LC + l) * PR + q] = g->minimum[(size_t(pe) * DC + d) * LC + l];
       }
   CUDA_TRY(up(p.prod_minimum, prod_minimum.data(), sizeof(uint32_t) * prod_minimum.size()));
+  DrawTables draw = draw_tables(g);
+  CUDA_TRY(up(p.nt_maxmin, draw.maxmin.data(), sizeof(uint32_t) * draw.maxmin.size()));
+  CUDA_TRY(up(p.nt_total, draw.total.data(), sizeof(double) * draw.total.size()));
+  CUDA_TRY(up(p.prod_threshold, draw.threshold.data(), sizeof(double) * draw.threshold.size()));
+  std::vector<gb::GenExpr> gen_expr(E);
+  for (int i = 0; i < E; ++i) {
+    const gagp_expression& x = g->expressions[i];
+    gb::GenExpr& r = gen_expr[i];
+    for (int k = 0; k < 4; ++k) {
+      r.child[k] = k < GAGP_MAX_ARITY ? x.children[k] : -1;
+      r.child_scope[k] = k < GAGP_MAX_ARITY ? x.child_scope[k] : -1;
+    }
+    r.target = x.target;
+    r.site_class = info[i].site_class;
+    r.kind = int8_t(x.kind);
+    r.arity = info[i].arity;
+    // out-of-range counts keep their validity (admission bounds them anyway)
+    r.scope_count = int8_t(std::min(std::max(x.scope_count, -1), 100));
+    r.reserved = 0;
+  }
+  CUDA_TRY(up(p.gen_expr, gen_expr.data(), sizeof(gb::GenExpr) * gen_expr.size()));
+  std::vector<gb::GenNt> gen_nt(std::max(1, g->nonterminal_count));
+  for (int i = 0; i < g->nonterminal_count; ++i) {
+    const gagp_nonterminal& n = g->nonterminals[i];
+    gen_nt[i] = gb::GenNt{n.production_offset, n.production_count, n.scope_count, n.normalized_weights};
+  }
+  CUDA_TRY(up(p.gen_nt, gen_nt.data(), sizeof(gb::GenNt) * gen_nt.size()));
   CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
   CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
   CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
@@ -449,6 +566,11 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.vals = at<gagp_value>(b, p.vals);
   d.minimum = at<uint32_t>(b, p.minimum);
   d.prod_minimum = at<uint32_t>(b, p.prod_minimum);
+  d.nt_maxmin = at<uint32_t>(b, p.nt_maxmin);
+  d.nt_total = at<double>(b, p.nt_total);
+  d.prod_threshold = at<double>(b, p.prod_threshold);
+  d.gen_expr = at<gb::GenExpr>(b, p.gen_expr);
+  d.gen_nt = at<gb::GenNt>(b, p.gen_nt);
   d.local_types = at<int32_t>(b, p.local_types);
   d.n_ex = E; d.n_prods = g->production_count; d.n_nts = g->nonterminal_count;
   d.n_doms = g->domain_count; d.n_vals = g->value_count;
@@ -483,6 +605,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.mt = at<uint64_t>(b, p.mt); d.stream = at<uint64_t>(b, p.stream); d.stream_mod = at<uint32_t>(b, p.stream_mod);
   d.stream_head = at<long long>(b, p.stream_head); d.stream_capacity = p.stream_capacity;
   d.mod_magic = ~0ULL / uint64_t(s->P);
+  d.bounded_threshold = (0 - uint64_t(s->P)) % uint64_t(s->P);
   d.round_seed = at<uint64_t>(b, p.round_seed);
   d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
   d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
@@ -593,7 +716,8 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
 int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1) / threads); }
 
 // Evaluates lowered programs listed by k_lower (both VMs).
-gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
+gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t stream, const gb::ProgramRef* fast,
+                      const gb::ProgramRef* general, const int32_t* counts) {
   const int warps = 8;
   const int temp_stride = gb::kMaxTemps * v.max_lanes * 32;
   const int code_stride = (v.max_code_stride + 1) & ~1;  // uint2 slots, in int64 units
@@ -602,13 +726,13 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
   const int per_sm = std::max(1, std::min(4, int((e->max_smem - 1024) / std::max<size_t>(smem, 1))));
   const int blocks = e->sm_count * per_sm;
   {
-    Timed t(e, KN_VM_FAST);
-    gb::k_vm_fast<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, mode, e->d_fast, e->d_counts, temp_stride,
-                                                            code_stride, const_stride);
+    Timed t(e, KN_VM_FAST, stream);
+    gb::k_vm_fast<<<blocks, warps * 32, smem, stream>>>(v.d_desc, mode, fast, counts, temp_stride, code_stride,
+                                                         const_stride);
   }
   {
-    Timed t(e, KN_VM_GENERAL);
-    gb::k_vm_general<<<e->sm_count * 4, 128, 0, e->stream>>>(v.d_desc, mode, e->d_general, e->d_counts + 1);
+    Timed t(e, KN_VM_GENERAL, stream);
+    gb::k_vm_general<<<e->sm_count * 4, 128, 0, stream>>>(v.d_desc, mode, general, counts + 1);
   }
   return GAGP_OK;
 }
@@ -616,9 +740,12 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode) {
 gagp_status launch_start(gagp_engine* e, const BatchView& v) {
   { Timed t(e, KN_INIT); gb::k_init_population<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
-  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_members, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n, 0, e->d_fast,
-                                                                        e->d_general, e->d_counts); }
-  launch_vm(e, v, 0);
+  {
+    Timed t(e, KN_LOWER);
+    gb::k_lower<<<blocks_for(v.total_members, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(
+        v.d_desc, v.d_member_off, v.n, 0, e->d_fast, e->d_general, e->d_counts, 0, v.total_members);
+  }
+  launch_vm(e, v, 0, e->stream, e->d_fast, e->d_general, e->d_counts);
   { Timed t(e, KN_KEYS); gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   { Timed t(e, KN_START); gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
@@ -631,20 +758,37 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v) {
   { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
   CUDA_TRY(cudaEventRecord(e->join, e->side));
   { Timed t(e, KN_RECORD); gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1); }
-  // [0], [1]: lowered-program list sizes; [2]: next child of the variation warps
-  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 3 * sizeof(int32_t), e->stream));
-  {
-    Timed t(e, KN_VARY);
-    const int warps = 4;
-    const size_t smem = warps * gb::warp_rows_bytes(v.max_stride);
-    int per_sm = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vary, warps * 32, smem));
-    const int blocks = std::min(blocks_for(v.total_children, warps), std::max(1, per_sm) * e->sm_count);
-    gb::k_vary<<<blocks, warps * 32, smem, e->stream>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, e->d_counts + 2);
+  // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
+  // next child of the variation warps; range c's lists start at item lo
+  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));
+  CUDA_TRY(cudaEventRecord(e->chunk_fork, e->stream));
+  const int chunks = v.total_children >= 4096 ? gagp_engine::kChunks : 1;
+  const int warps = 4;
+  const size_t vary_smem = warps * gb::warp_rows_bytes(v.max_stride);
+  int per_sm = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vary, warps * 32, vary_smem));
+  for (int c = 0; c < chunks; ++c) {
+    const int lo = int(int64_t(v.total_children) * c / chunks), hi = int(int64_t(v.total_children) * (c + 1) / chunks);
+    cudaStream_t st = chunks == 1 ? e->stream : e->chunk_stream[c];
+    if (chunks > 1) CUDA_TRY(cudaStreamWaitEvent(st, e->chunk_fork, 0));
+    int32_t* counts = e->d_counts + 4 * c;
+    {
+      Timed t(e, KN_VARY, st);
+      const int blocks = std::min(blocks_for(hi - lo, warps), std::max(1, per_sm) * e->sm_count);
+      gb::k_vary<<<blocks, warps * 32, vary_smem, st>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, counts + 2, lo,
+                                                        hi);
+    }
+    {
+      Timed t(e, KN_LOWER, st);
+      gb::k_lower<<<blocks_for(hi - lo, gb::kLowerWarps), gb::kLowerWarps * 32, 0, st>>>(
+          v.d_desc, v.d_child_off, v.n, 1, e->d_fast + lo, e->d_general + lo, counts, lo, hi);
+    }
+    launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts);
+    if (chunks > 1) {
+      CUDA_TRY(cudaEventRecord(e->chunk_done[c], st));
+      CUDA_TRY(cudaStreamWaitEvent(e->stream, e->chunk_done[c], 0));
+    }
   }
-  { Timed t(e, KN_LOWER); gb::k_lower<<<blocks_for(v.total_children, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n, 1, e->d_fast,
-                                                                         e->d_general, e->d_counts); }
-  launch_vm(e, v, 1);
   { Timed t(e, KN_CHILD); gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
   {
     Timed t(e, KN_PLACE);
@@ -824,7 +968,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.ex = at<gagp_expression>(b, p.ex);
   d.info = at<gb::ExprInfo>(b, p.info);
   d.minimum = at<uint32_t>(b, p.minimum);
-  d.prod_minimum = d.minimum;  // no subtree generation in row evaluation
+  d.prod_minimum = d.nt_maxmin = d.minimum;  // no subtree generation in row evaluation
   d.local_types = at<int32_t>(b, p.local_types);
   d.n_ex = E;
   d.slot_type = g->slot_type;
@@ -885,7 +1029,8 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   gb::ProgramRef* fast = at<gb::ProgramRef>(b, p.fast);
   gb::ProgramRef* general = at<gb::ProgramRef>(b, p.general);
   int32_t* counts = at<int32_t>(b, p.counts);
-  gb::k_lower<<<blocks_for(R, gb::kLowerWarps), gb::kLowerWarps * 32, 0, stream>>>(dd, doff, 1, 0, fast, general, counts);
+  gb::k_lower<<<blocks_for(R, gb::kLowerWarps), gb::kLowerWarps * 32, 0, stream>>>(dd, doff, 1, 0, fast, general, counts,
+                                                                                  0, R);
   const int warps = 8;
   const int lanes = d.vm_cases_per_lane;
   const int temp_stride = gb::kMaxTemps * lanes * 32;

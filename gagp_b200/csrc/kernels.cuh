@@ -43,8 +43,8 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
   const int ramp = site_limit < 2 ? site_limit : 2 + i % (site_limit - 1);
   uint64_t* node = s.node + size_t(i) * s.stride;
   int64_t* cval = s.cval + size_t(i) * s.stride;
-  uint32_t pending[192];
-  GenResult g{ST_INVALID, 0, 0};
+  uint64_t pending[192];
+  GenResult g{ST_INVALID, 0, 0, 0};
   for (int logical = ramp, attempt = 0; g.status != ST_OK; ++attempt) {
     const int room = s.maxv < kCapacity ? s.maxv : kCapacity;
     g = generate(s, s.root_expression, 0, s.slot_max_depth, room,
@@ -63,17 +63,17 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
 
 // ----------------------------------------------------------- lowering
 // mode 0: the members (initial evaluation); mode 1: this round's children
-// that reuse no member's result.  One warp per row: the accumulator program
-// when the row is total and fits the fuel, else the reference bytecode for
-// the general VM (lane 0).
+// that reuse no member's result; batch items [lo, hi).  One warp per row:
+// the accumulator program when the row is total and fits the fuel, else the
+// reference bytecode for the general VM (lane 0).
 constexpr int kLowerWarps = 4;
 __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* descs, const int32_t* off, int n,
                                                             int mode, ProgramRef* fast_list, ProgramRef* general_list,
-                                                            int32_t* list_count) {
+                                                            int32_t* list_count, int lo, int hi) {
   __shared__ LowerScratch scratch[kLowerWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int total_items = off[n];
-  for (int item = blockIdx.x * kLowerWarps + warp; item < total_items; item += gridDim.x * kLowerWarps) {
+  const int total_items = min(off[n], hi);
+  for (int item = lo + blockIdx.x * kLowerWarps + warp; item < total_items; item += gridDim.x * kLowerWarps) {
     const int si = find_search(off, n, item);
     const SearchDesc& s = descs[si];
     if (!search_live(s)) continue;
@@ -395,18 +395,19 @@ __global__ void k_record(const SearchDesc* descs, int n, int only_epoch_start) {
 
 // make_batch (phase_population_cpu.cpp:322-353): one warp per child, rows
 // staged in dynamic shared memory (warp_rows_bytes(stride) per warp).
-// Persistent warps: each warp takes the next child index from `next_item`
-// (zeroed before the launch) until all children of the batch are varied, so
-// warps that drew short children go on to the next one instead of idling.
+// Persistent warps over the batch items [lo, hi): each warp takes the next
+// child from `next_item` (zeroed before the launch) until the range is
+// varied, so warps that drew short children go on to the next one instead
+// of idling.
 __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max,
-                                                 int32_t* next_item) {
+                                                 int32_t* next_item, int lo, int hi) {
   extern __shared__ __align__(16) char smem_rows[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   char* base = smem_rows + size_t(warp) * warp_rows_bytes(stride_max);
-  const int total = off[n];
+  const int total = min(off[n], hi);
   for (;;) {
     int item = 0;
-    if (lane == 0) item = atomicAdd(next_item, 1);
+    if (lane == 0) item = lo + atomicAdd(next_item, 1);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
     const int si = find_search(off, n, item);

@@ -21,9 +21,9 @@ __device__ __forceinline__ bool selection_greater(const SearchDesc& s, const uin
 
 // tournament (phase_operators.cuh:46-50)
 __device__ inline int tournament(const SearchDesc& s, Rng& random) {
-  int best = int(random.bounded(uint64_t(s.P)));
+  int best = int(random.bounded_fixed(uint64_t(s.P), s.bounded_threshold, s.mod_magic));
   for (int i = 1; i < s.pressure; ++i) {
-    const int c = int(random.bounded(uint64_t(s.P)));
+    const int c = int(random.bounded_fixed(uint64_t(s.P), s.bounded_threshold, s.mod_magic));
     if (selection_greater(s, s.key, c, best)) best = c;
   }
   return best;
@@ -33,11 +33,11 @@ __device__ inline int tournament(const SearchDesc& s, Rng& random) {
 // generated subtree; `pending` is the generator's task stack.
 struct WarpRows {
   SRow parent, donor, child, out, gen;
-  uint32_t* pending;
+  uint64_t* pending;
 };
 
 __host__ __device__ __forceinline__ size_t warp_rows_bytes(int stride) {
-  return size_t(5) * stride * (sizeof(uint64_t) + sizeof(int64_t)) + 192 * sizeof(uint32_t);
+  return size_t(5) * stride * (sizeof(uint64_t) + sizeof(int64_t)) + 192 * sizeof(uint64_t);
 }
 __device__ inline WarpRows carve_rows(char* base, int stride) {
   WarpRows r;
@@ -48,7 +48,7 @@ __device__ inline WarpRows carve_rows(char* base, int stride) {
   r.child = SRow{n + 2 * stride, c + 2 * stride, 0, 0};
   r.out = SRow{n + 3 * stride, c + 3 * stride, 0, 0};
   r.gen = SRow{n + 4 * stride, c + 4 * stride, 0, 0};
-  r.pending = reinterpret_cast<uint32_t*>(c + 5 * stride);
+  r.pending = reinterpret_cast<uint64_t*>(c + 5 * stride);
   return r;
 }
 
@@ -121,10 +121,14 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
         const bool capped = s.mutation_max_nodes > 0 && s.mutation_max_nodes < uncapped;
         const int bounded = capped ? s.mutation_max_nodes : uncapped;
         const uint64_t gseed = m.next();
-        GenResult g{ST_INVALID, 0, 0};
-        if (lane == 0)
+        GenResult g{ST_INVALID, 0, 0, 0};
+        if (lane == 0) {
           g = generate(s, entry, 0, s.slot_max_depth - depth + 1, bounded, gseed, w.gen.node, w.gen.cval, logical,
                        w.pending);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[21]), (unsigned long long)g.steps);
+          atomicMax(reinterpret_cast<unsigned long long*>(&s.counters[22]), (unsigned long long)g.steps);
+          atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[23]), 1ULL);
+        }
         g.status = __shfl_sync(kFull, g.status, 0);
         g.nodes = __shfl_sync(kFull, g.nodes, 0);
         g.constants = __shfl_sync(kFull, g.constants, 0);

@@ -37,6 +37,21 @@ struct ExprInfo {
   int32_t site_nt;     // Reference expressions: the nonterminal (site present), else -1
 };
 
+// Subtree-generation view of one expression, two 16-byte loads: the first
+// four children, then target (nonterminal or domain), the crossover class of
+// the sites it opens, kind / arity / scope count and the children's scopes.
+struct alignas(16) GenExpr {
+  int32_t child[4];
+  int32_t target;
+  int32_t site_class;
+  int8_t kind, arity, scope_count, reserved;
+  int8_t child_scope[4];
+};
+// A nonterminal in one 16-byte load.
+struct alignas(16) GenNt {
+  int32_t production_offset, production_count, scope_count, normalized_weights;
+};
+
 // Everything a kernel needs to work on one search (device pointers).
 struct SearchDesc {
   // ---- admitted grammar (phase tables)
@@ -50,6 +65,16 @@ struct SearchDesc {
   // minimum of each production's expression, production-major per (depth,
   // site budget): prod_minimum[(d * logical_count + l) * n_prods + p]
   const uint32_t* prod_minimum;
+  const GenExpr* gen_expr;
+  const GenNt* gen_nt;
+  // production draw when every production of a nonterminal is feasible:
+  // nt_maxmin[(d * logical_count + l) * n_nts + nt] = the largest production
+  // minimum (all feasible iff it fits), nt_total[nt] = the draw's weight sum
+  // (NaN: no precomputed draw), prod_threshold[p]: the smallest choice value
+  // whose running difference after production p is not negative
+  const uint32_t* nt_maxmin;
+  const double* nt_total;
+  const double* prod_threshold;
   const int32_t* local_types;          // ValueTag of each evaluator input
   int32_t n_ex, n_prods, n_nts, n_doms, n_vals;
   int32_t depth_count, logical_count, site_depth;
@@ -94,6 +119,7 @@ struct SearchDesc {
   long long* stream_head;              // [0]: outputs read, [1]: outputs written (ring positions)
   int32_t stream_capacity;
   uint64_t mod_magic;                  // floor((2^64 - 1) / P): exact residues by multiply-high
+  uint64_t bounded_threshold;          // (2^64 - P) mod P: rejection bound of bounded(P)
   uint64_t* round_seed;                // seed of the next round's variation
   // ---- search progress and history
   int32_t* best;                       // tracked best member

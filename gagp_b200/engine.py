@@ -147,7 +147,8 @@ class Engine:
                 "place_levels": out[7], "vary_bytes": out[8], "lower_bytes": out[9],
                 "vary_select_cycles": out[10], "vary_crossover_cycles": out[11], "vary_generate_cycles": out[12],
                 "vary_rest_cycles": out[13], "place_level_cycles": out[14], "vary_max_child_cycles": out[15],
-                "vary_max_phase_cycles": list(out[16:20]), "vary_slow_children": out[20]}
+                "vary_max_phase_cycles": list(out[16:20]), "vary_slow_children": out[20],
+                "generate_steps": out[21], "generate_max_steps": out[22], "generations": out[23]}
 
     def transfers(self) -> tuple:
         """(host->device, device->host) bytes copied by this engine so far."""

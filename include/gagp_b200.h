@@ -246,7 +246,8 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
  * the rest), [14] cycles of the placement's level loop, [15] the most
  * cycles one child's variation took, [16..19] the most cycles of one child
  * in each variation phase, [20] children whose variation took over 200000
- * cycles, [21..23] reserved.
+ * cycles, [21] subtree-generation steps (tasks) of mutations, [22] the
+ * most steps of one generation, [23] mutation subtree generations.
  * Copies min(count, GAGP_COUNTERS) entries
  * (synchronous). */
 /* Bytes this engine's calls have copied host->device and device->host since
