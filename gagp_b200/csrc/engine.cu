@@ -13,6 +13,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -102,6 +104,9 @@ struct gagp_engine {
   size_t flush_bytes = 0;
   // bytes copied host->device and device->host by this engine's API calls
   uint64_t h2d_bytes = 0, d2h_bytes = 0;
+  // stream-ordered pool of the searches' device blocks: admission and
+  // retirement neither allocate from the driver nor synchronize the device
+  cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -169,7 +174,7 @@ gagp_status ensure_lists(gagp_engine* e, size_t items) {
   if (e->d_fast) cudaFree(e->d_fast);
   if (e->d_general) cudaFree(e->d_general);
   e->d_fast = e->d_general = nullptr;
-  const size_t cap = std::max<size_t>(items, 1024);
+  const size_t cap = std::max<size_t>({items, size_t(1024), 2 * e->list_capacity});
   CUDA_TRY(cudaMalloc(&e->d_fast, cap * sizeof(gb::ProgramRef)));
   CUDA_TRY(cudaMalloc(&e->d_general, cap * sizeof(gb::ProgramRef)));
   if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, 4 * gagp_engine::kChunks * sizeof(int32_t)));
@@ -412,6 +417,13 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   size_t free_bytes = 0, total = 0;
   CUDA_TRY(cudaMemGetInfo(&free_bytes, &total));
   e->arena_limit = arena_bytes ? arena_bytes : uint64_t(0.8 * double(free_bytes));
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  CUDA_TRY(cudaMemPoolCreate(&e->pool, &props));
+  uint64_t keep = ~0ULL;  // freed blocks stay in the pool for the next admission
+  CUDA_TRY(cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 16384));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vary, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
@@ -424,10 +436,12 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   cudaSetDevice(e->device);
   cudaStreamSynchronize(e->stream);
   for (auto& kv : e->searches) {
-    cudaFree(kv.second->block);
-    cudaFree(kv.second->d_desc);
-    cudaFree(kv.second->d_off);
+    cudaFreeAsync(kv.second->block, e->stream);
+    cudaFreeAsync(kv.second->d_desc, e->stream);
+    cudaFreeAsync(kv.second->d_off, e->stream);
   }
+  cudaStreamSynchronize(e->stream);
+  if (e->pool) cudaMemPoolDestroy(e->pool);
   cudaFree(e->d_fast);
   cudaFree(e->d_general);
   cudaFree(e->d_counts);
@@ -476,7 +490,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   s->fixed_nodes = g->fixed_nodes;
   s->has_wrong = cfg->metric != GAGP_METRIC_LEGACY;
   s->bytes = p.L.total;
-  CUDA_TRY(cudaMalloc(&s->block, s->bytes));
+  CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->block), s->bytes, e->pool, e->stream));
   CUDA_TRY(cudaMemsetAsync(s->block, 0, s->bytes, e->stream));
   char* b = s->block;
   const int E = g->expression_count;
@@ -617,16 +631,16 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   const int wrong_bits = bits_for(uint64_t(C));
   const int loss_bits = bits_for(uint64_t(double(C) * std::fabs(cfg->penalty)));
   if (s->has_wrong && node_bits + wrong_bits + loss_bits > 64) {
-    cudaFree(s->block);
+    cudaFreeAsync(s->block, e->stream);
     return fail(GAGP_DECLINED, "ranking key wider than 64 bits");
   }
   d.key_shift_nodes = node_bits;
   d.key_shift_wrong = node_bits + wrong_bits;
   d.total_rounds = s->total_rounds;
-  CUDA_TRY(cudaMalloc(&s->d_desc, sizeof(gb::SearchDesc)));
+  CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->d_desc), sizeof(gb::SearchDesc), e->pool, e->stream));
   CUDA_TRY(copy_h2d(e, s->d_desc, &d, sizeof(gb::SearchDesc)));
   const int32_t off[4] = {0, s->P, 0, s->B};
-  CUDA_TRY(cudaMalloc(&s->d_off, sizeof(off)));
+  CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->d_off), sizeof(off), e->pool, e->stream));
   CUDA_TRY(copy_h2d(e, s->d_off, off, sizeof(off)));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   s->id = e->next_id++;
@@ -641,10 +655,11 @@ gagp_status gagp_b200_search_destroy(gagp_engine* e, int32_t id) {
   auto it = e->searches.find(id);
   if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search");
   cudaSetDevice(e->device);
-  cudaStreamSynchronize(e->stream);
-  cudaFree(it->second->block);
-  cudaFree(it->second->d_desc);
-  cudaFree(it->second->d_off);
+  // stream-ordered: the blocks return to the pool after the work queued on
+  // the engine stream (every kernel of the search) has run
+  cudaFreeAsync(it->second->block, e->stream);
+  cudaFreeAsync(it->second->d_desc, e->stream);
+  cudaFreeAsync(it->second->d_off, e->stream);
   e->arena_used -= it->second->bytes;
   e->searches.erase(it);
   return GAGP_OK;
@@ -672,15 +687,17 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
     v->d_member_off = list[0]->d_off;
     v->d_child_off = list[0]->d_off + 2;
   } else {
-    if (size_t(n) > e->batch_desc_capacity) {
+    if (size_t(n) > e->batch_desc_capacity) {  // grown geometrically: batches change size while serving
+      const size_t cap = std::max<size_t>(size_t(n), 2 * e->batch_desc_capacity);
       cudaFree(e->d_batch_desc);
-      CUDA_TRY(cudaMalloc(&e->d_batch_desc, sizeof(gb::SearchDesc) * n));
-      e->batch_desc_capacity = n;
+      CUDA_TRY(cudaMalloc(&e->d_batch_desc, sizeof(gb::SearchDesc) * cap));
+      e->batch_desc_capacity = cap;
     }
     if (size_t(2 * (n + 1)) > e->batch_off_capacity) {
+      const size_t cap = std::max<size_t>(size_t(2 * (n + 1)), 2 * e->batch_off_capacity);
       cudaFree(e->d_batch_off);
-      CUDA_TRY(cudaMalloc(&e->d_batch_off, sizeof(int32_t) * 2 * (n + 1)));
-      e->batch_off_capacity = 2 * (n + 1);
+      CUDA_TRY(cudaMalloc(&e->d_batch_off, sizeof(int32_t) * cap));
+      e->batch_off_capacity = cap;
     }
     std::vector<gb::SearchDesc> descs(n);
     std::vector<int32_t> off(2 * (n + 1), 0);
@@ -1368,6 +1385,322 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   out->evaluated_programs = counters[0];
   out->reused_programs = counters[1];
   out->program_cases = counters[2];
+  return GAGP_OK;
+}
+
+}  // extern "C"
+
+// ======================================================================= serving
+namespace {
+
+// A queued or running request: owned copies of the caller's blobs, then the
+// finished search's result read back to host memory.
+struct Request {
+  int64_t ticket = 0;
+  int32_t state = GAGP_REQUEST_QUEUED;
+  std::string error;
+  std::vector<gagp_expression> ex;
+  std::vector<gagp_production> prods;
+  std::vector<gagp_nonterminal> nts;
+  std::vector<gagp_domain> doms;
+  std::vector<gagp_value> vals;
+  std::vector<uint32_t> minimum;
+  std::vector<int64_t> inputs, expected;
+  std::vector<int32_t> tags;
+  gagp_grammar grammar{};
+  gagp_cases cases{};
+  gagp_search_config config{};
+  uint64_t bytes = 0;
+  int32_t search = -1;
+  double submitted = -1, admitted = -1, finished = -1;
+  // result (gagp_search_result layout)
+  int32_t generations = 0, population = 0, stride = 0;
+  std::vector<double> hbf, hmf, ff;
+  std::vector<int32_t> hbw, hbn, fw, fn;
+  std::vector<int32_t> h_nodes, h_orig, h_ncon, f_nodes, f_orig, f_ncon;
+  std::vector<int64_t> h_con, f_con;
+  uint64_t evaluated = 0, reused = 0, program_cases = 0;
+};
+
+template <class T>
+std::vector<T> copy_of(const T* p, int32_t n) {
+  return p && n > 0 ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+
+}  // namespace
+
+struct gagp_server {
+  gagp_engine* e = nullptr;
+  uint64_t budget = 0;
+  int32_t max_active = 0;
+  int64_t next_ticket = 1;
+  std::deque<int64_t> queue;
+  std::vector<int64_t> active;
+  std::map<int64_t, std::unique_ptr<Request>> requests;
+  int32_t* d_status = nullptr;
+  size_t status_capacity = 0;
+  std::chrono::steady_clock::time_point epoch = std::chrono::steady_clock::now();
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - epoch).count();
+  }
+};
+
+namespace {
+
+// Reads a finished search's result into the request, then frees the search.
+gagp_status retire(gagp_server* sv, Request& r) {
+  gagp_engine* e = sv->e;
+  Search* s = e->searches.at(r.search).get();
+  const int H = r.config.generations + 1, P = s->P, S = s->stride;
+  r.generations = H;
+  r.population = P;
+  r.stride = S;
+  r.hbf.assign(H, 0); r.hmf.assign(H, 0); r.hbw.assign(H, 0); r.hbn.assign(H, 0);
+  r.h_nodes.assign(H, 0); r.h_ncon.assign(H, 0); r.h_orig.assign(size_t(H) * S, -1); r.h_con.assign(size_t(H) * S, 0);
+  r.ff.assign(P, 0); r.fw.assign(P, 0); r.fn.assign(P, 0);
+  r.f_nodes.assign(P, 0); r.f_ncon.assign(P, 0); r.f_orig.assign(size_t(P) * S, -1); r.f_con.assign(size_t(P) * S, 0);
+  gagp_search_result out{};
+  out.generations = H;
+  out.history_best_fitness = r.hbf.data();
+  out.history_mean_fitness = r.hmf.data();
+  out.history_best_wrong = r.hbw.data();
+  out.history_best_nodes = r.hbn.data();
+  out.history_best = gagp_rows{H, S, r.h_nodes.data(), r.h_orig.data(), r.h_ncon.data(), r.h_con.data()};
+  out.population = P;
+  out.final_fitness = r.ff.data();
+  out.final_wrong = r.fw.data();
+  out.final_nodes = r.fn.data();
+  out.final_rows = gagp_rows{P, S, r.f_nodes.data(), r.f_orig.data(), r.f_ncon.data(), r.f_con.data()};
+  const gagp_status st = gagp_b200_search_result(e, r.search, &out);
+  if (st == GAGP_OK) {
+    r.generations = out.generations;
+    r.population = out.population;
+    r.evaluated = out.evaluated_programs;
+    r.reused = out.reused_programs;
+    r.program_cases = out.program_cases;
+    r.state = GAGP_REQUEST_DONE;
+  } else {
+    r.state = GAGP_REQUEST_FAILED;
+    r.error = gagp_b200_last_error();
+  }
+  gagp_b200_search_destroy(e, r.search);
+  r.search = -1;
+  r.finished = sv->now();
+  return st == GAGP_DEVICE_ERROR ? st : GAGP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+gagp_status gagp_b200_server_create(gagp_engine* e, uint64_t memory_budget, int32_t max_active, gagp_server** out) {
+  if (!e || !out || max_active < 0) return fail(GAGP_INVALID_ARGUMENT, "bad argument");
+  auto sv = std::make_unique<gagp_server>();
+  sv->e = e;
+  sv->budget = memory_budget ? std::min<uint64_t>(memory_budget, e->arena_limit) : e->arena_limit;
+  sv->max_active = max_active;
+  *out = sv.release();
+  return GAGP_OK;
+}
+
+void gagp_b200_server_destroy(gagp_server* sv) {
+  if (!sv) return;
+  for (int64_t t : sv->active) {
+    Request& r = *sv->requests.at(t);
+    if (r.search >= 0) gagp_b200_search_destroy(sv->e, r.search);
+  }
+  if (sv->d_status) {
+    cudaSetDevice(sv->e->device);
+    cudaFree(sv->d_status);
+  }
+  delete sv;
+}
+
+gagp_status gagp_b200_server_submit(gagp_server* sv, const gagp_grammar* g, const gagp_cases* c,
+                                    const gagp_search_config* cfg, int64_t* ticket) {
+  if (!sv || !g || !c || !cfg || !ticket) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  gagp_status st = admit(g, c, cfg);
+  if (st != GAGP_OK) return st;
+  const Plan p = plan_search(g, c, cfg);
+  if (p.L.total > sv->budget) return fail(GAGP_OUT_OF_MEMORY, "request larger than the server's memory budget");
+  auto r = std::make_unique<Request>();
+  r->ticket = sv->next_ticket++;
+  r->ex = copy_of(g->expressions, g->expression_count);
+  r->prods = copy_of(g->productions, g->production_count);
+  r->nts = copy_of(g->nonterminals, g->nonterminal_count);
+  r->doms = copy_of(g->domains, g->domain_count);
+  r->vals = copy_of(g->values, g->value_count);
+  r->minimum = copy_of(g->minimum, g->expression_count * g->depth_count * g->logical_depth_count);
+  r->grammar = *g;
+  r->grammar.expressions = r->ex.data();
+  r->grammar.productions = r->prods.data();
+  r->grammar.nonterminals = r->nts.data();
+  r->grammar.domains = r->doms.data();
+  r->grammar.values = r->vals.data();
+  r->grammar.minimum = r->minimum.data();
+  r->inputs = copy_of(c->inputs, c->case_count * c->input_count);
+  r->expected = copy_of(c->expected, c->case_count);
+  r->tags = copy_of(c->input_tags, c->input_count);
+  r->cases = *c;
+  r->cases.inputs = r->inputs.data();
+  r->cases.expected = r->expected.data();
+  r->cases.input_tags = r->tags.empty() ? nullptr : r->tags.data();
+  r->config = *cfg;
+  r->bytes = p.L.total;
+  r->submitted = sv->now();
+  *ticket = r->ticket;
+  sv->queue.push_back(r->ticket);
+  sv->requests[r->ticket] = std::move(r);
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_server_step(gagp_server* sv, int32_t* running, int32_t* queued, int32_t* finished_now) {
+  if (!sv) return fail(GAGP_INVALID_ARGUMENT, "null server");
+  gagp_engine* e = sv->e;
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  CUDA_TRY(cudaSetDevice(e->device));
+  // admission in arrival order while the head request fits
+  while (!sv->queue.empty() && (sv->max_active == 0 || int32_t(sv->active.size()) < sv->max_active)) {
+    Request& r = *sv->requests.at(sv->queue.front());
+    if (e->arena_used + r.bytes > sv->budget) break;
+    int32_t id = -1;
+    const gagp_status st = gagp_b200_search_create(e, &r.grammar, &r.cases, &r.config, nullptr, &id);
+    if (st == GAGP_OUT_OF_MEMORY) break;
+    sv->queue.pop_front();
+    if (st != GAGP_OK) {
+      r.state = GAGP_REQUEST_FAILED;
+      r.error = gagp_b200_last_error();
+      r.finished = sv->now();
+      if (st == GAGP_DEVICE_ERROR) return st;
+      continue;
+    }
+    r.search = id;
+    r.state = GAGP_REQUEST_RUNNING;
+    r.admitted = sv->now();
+    sv->active.push_back(r.ticket);
+  }
+  int32_t done = 0;
+  if (!sv->active.empty()) {
+    std::vector<Search*> list, fresh;
+    for (int64_t t : sv->active) list.push_back(e->searches.at(sv->requests.at(t)->search).get());
+    for (Search* s : list) if (!s->started) fresh.push_back(s);
+    BatchView v;
+    gagp_status st;
+    if (!fresh.empty()) {
+      if ((st = make_batch_view(e, fresh, &v)) != GAGP_OK) return st;
+      if ((st = launch_start(e, v)) != GAGP_OK) return st;
+      for (Search* s : fresh) s->started = true;
+    }
+    if ((st = make_batch_view(e, list, &v)) != GAGP_OK) return st;
+    if ((st = launch_round(e, v)) != GAGP_OK) return st;
+    const size_t n = list.size();
+    if (n > sv->status_capacity) {
+      const size_t cap = std::max(n, 2 * sv->status_capacity);
+      cudaFree(sv->d_status);
+      CUDA_TRY(cudaMalloc(&sv->d_status, cap * sizeof(int32_t)));
+      sv->status_capacity = cap;
+    }
+    gb::k_status<<<blocks_for(int(n), 256), 256, 0, e->stream>>>(v.d_desc, int(n), sv->d_status);
+    std::vector<int32_t> status(n);
+    CUDA_TRY(cudaMemcpyAsync(status.data(), sv->d_status, n * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    e->d2h_bytes += n * sizeof(int32_t);
+    harvest(e);
+    std::vector<int64_t> still;
+    for (size_t i = 0; i < n; ++i) {
+      Request& r = *sv->requests.at(sv->active[i]);
+      if (status[i] & 2) {
+        r.state = GAGP_REQUEST_FAILED;
+        r.error = "search failed on the device";
+        gagp_b200_search_destroy(e, r.search);
+        r.search = -1;
+        r.finished = sv->now();
+        ++done;
+      } else if (status[i] & 1) {
+        if ((st = retire(sv, r)) != GAGP_OK) return st;
+        ++done;
+      } else {
+        still.push_back(r.ticket);
+      }
+    }
+    sv->active.swap(still);
+  }
+  if (running) *running = int32_t(sv->active.size());
+  if (queued) *queued = int32_t(sv->queue.size());
+  if (finished_now) *finished_now = done;
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_server_poll(gagp_server* sv, int64_t ticket, int32_t* state) {
+  if (!sv || !state) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  auto it = sv->requests.find(ticket);
+  if (it == sv->requests.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown ticket");
+  *state = it->second->state;
+  if (it->second->state == GAGP_REQUEST_FAILED) return fail(GAGP_OK, it->second->error);
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_server_times(gagp_server* sv, int64_t ticket, double* submitted, double* admitted,
+                                   double* finished) {
+  if (!sv) return fail(GAGP_INVALID_ARGUMENT, "null server");
+  auto it = sv->requests.find(ticket);
+  if (it == sv->requests.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown ticket");
+  if (submitted) *submitted = it->second->submitted;
+  if (admitted) *admitted = it->second->admitted;
+  if (finished) *finished = it->second->finished;
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_server_result(gagp_server* sv, int64_t ticket, gagp_search_result* out) {
+  if (!sv || !out) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  auto it = sv->requests.find(ticket);
+  if (it == sv->requests.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown ticket");
+  Request& r = *it->second;
+  if (r.state == GAGP_REQUEST_FAILED) return fail(GAGP_DEVICE_ERROR, r.error);
+  if (r.state != GAGP_REQUEST_DONE) return fail(GAGP_NOT_READY, "request has not finished");
+  const int H = std::min(r.generations, out->generations), P = std::min(r.population, out->population);
+  auto rows = [&](const gagp_rows& to, int count, const std::vector<int32_t>& nodes, const std::vector<int32_t>& orig,
+                  const std::vector<int32_t>& ncon, const std::vector<int64_t>& con) {
+    for (int i = 0; i < count; ++i) {
+      to.node_counts[i] = nodes[i];
+      to.constant_counts[i] = ncon[i];
+      for (int k = 0; k < std::min(to.stride, r.stride); ++k) {
+        to.origins[size_t(i) * to.stride + k] = orig[size_t(i) * r.stride + k];
+        to.constants[size_t(i) * to.stride + k] = con[size_t(i) * r.stride + k];
+      }
+    }
+  };
+  for (int h = 0; h < H; ++h) {
+    out->history_best_fitness[h] = r.hbf[h];
+    out->history_mean_fitness[h] = r.hmf[h];
+    out->history_best_wrong[h] = r.hbw[h];
+    out->history_best_nodes[h] = r.hbn[h];
+  }
+  rows(out->history_best, H, r.h_nodes, r.h_orig, r.h_ncon, r.h_con);
+  for (int i = 0; i < P; ++i) {
+    out->final_fitness[i] = r.ff[i];
+    out->final_wrong[i] = r.fw[i];
+    out->final_nodes[i] = r.fn[i];
+  }
+  rows(out->final_rows, P, r.f_nodes, r.f_orig, r.f_ncon, r.f_con);
+  out->generations = H;
+  out->population = P;
+  out->evaluated_programs = r.evaluated;
+  out->reused_programs = r.reused;
+  out->program_cases = r.program_cases;
+  sv->requests.erase(it);
+  return GAGP_OK;
+}
+
+gagp_status gagp_b200_server_cancel(gagp_server* sv, int64_t ticket) {
+  if (!sv) return fail(GAGP_INVALID_ARGUMENT, "null server");
+  auto it = sv->requests.find(ticket);
+  if (it == sv->requests.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown ticket");
+  Request& r = *it->second;
+  if (r.search >= 0) gagp_b200_search_destroy(sv->e, r.search);
+  sv->queue.erase(std::remove(sv->queue.begin(), sv->queue.end(), ticket), sv->queue.end());
+  sv->active.erase(std::remove(sv->active.begin(), sv->active.end(), ticket), sv->active.end());
+  sv->requests.erase(it);
   return GAGP_OK;
 }
 

@@ -446,6 +446,15 @@ __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const 
   }
 }
 
+// State of every search of a batch in one array (bit 0: finished, bit 1:
+// failed), so that a serving step reads them with one copy.
+__global__ void k_status(const SearchDesc* descs, int n, int32_t* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const SearchDesc& s = descs[i];
+  out[i] = (s.round[2] ? 1 : 0) | (s.round[3] ? 2 : 0);
+}
+
 // Results of all children before any placement (evolve.cpp:403-413).
 __global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int n) {
   const int item = blockIdx.x * blockDim.x + threadIdx.x;

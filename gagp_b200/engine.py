@@ -40,9 +40,12 @@ def load_library():
                      "gagp_b200_batch_step", "gagp_b200_search_result", "gagp_b200_batch_start",
                      "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters", "gagp_b200_engine_transfers",
                      "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_evaluate_rows",
-                     "gagp_b200_evaluate_rows_static"):
+                     "gagp_b200_evaluate_rows_static", "gagp_b200_server_create", "gagp_b200_server_submit",
+                     "gagp_b200_server_step", "gagp_b200_server_poll", "gagp_b200_server_times",
+                     "gagp_b200_server_result", "gagp_b200_server_cancel"):
             getattr(lib, name).restype = C.c_int32
         lib.gagp_b200_engine_destroy.restype = None
+        lib.gagp_b200_server_destroy.restype = None
         _lib = lib
     return _lib
 
@@ -203,3 +206,74 @@ def evaluate_rows_static(task: LoadedTask, rows: abi.RowsBuffer, stream: int = 0
         g.ref(), task.cases.ref(), C.byref(cfg), rows.ref(), fitness.ctypes.data_as(C.POINTER(C.c_double)),
         wrong.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(stream)))
     return fitness, wrong
+
+
+REQUEST_QUEUED, REQUEST_RUNNING, REQUEST_DONE, REQUEST_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """Continuous-batching request loop over one engine (gagp_b200_server_*).
+
+    submit() queues a search; every step() admits queued requests in arrival
+    order while their device bytes fit `memory_budget`, runs one round of
+    every running search in one batched launch sequence and retires the
+    finished ones; result() returns a finished request's history and final
+    population exactly as Search.result() does for the search run alone."""
+
+    def __init__(self, engine: Engine, memory_budget: int = 0, max_active: int = 0):
+        h = C.c_void_p()
+        _check(load_library().gagp_b200_server_create(engine.handle, C.c_uint64(memory_budget),
+                                                      C.c_int32(max_active), C.byref(h)))
+        self.engine, self.handle, self.tasks = engine, h, {}
+
+    def close(self):
+        if self.handle:
+            load_library().gagp_b200_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, task: LoadedTask) -> int:
+        g = abi.GrammarBlob(task.tables)
+        cfg = task.settings.struct()
+        ticket = C.c_int64(0)
+        _check(load_library().gagp_b200_server_submit(self.handle, g.ref(), task.cases.ref(), C.byref(cfg),
+                                                      C.byref(ticket)))
+        self.tasks[ticket.value] = task
+        return ticket.value
+
+    def step(self) -> tuple:
+        """(running, queued, finished in this step)"""
+        running, queued, done = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(load_library().gagp_b200_server_step(self.handle, C.byref(running), C.byref(queued), C.byref(done)))
+        return running.value, queued.value, done.value
+
+    def poll(self, ticket: int) -> int:
+        state = C.c_int32()
+        _check(load_library().gagp_b200_server_poll(self.handle, C.c_int64(ticket), C.byref(state)))
+        return state.value
+
+    def times(self, ticket: int) -> tuple:
+        """(submitted, admitted, finished) seconds on the server clock; negative: not yet"""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _check(load_library().gagp_b200_server_times(self.handle, C.c_int64(ticket), C.byref(a), C.byref(b),
+                                                     C.byref(c)))
+        return a.value, b.value, c.value
+
+    def result_buffer(self, ticket: int) -> abi.ResultBuffer:
+        t = self.tasks.pop(ticket)
+        s = t.settings
+        res = abi.ResultBuffer(s.generations, s.population, t.tables.max_nodes - t.tables.fixed_nodes)
+        _check(load_library().gagp_b200_server_result(self.handle, C.c_int64(ticket), res.ref()))
+        return res
+
+    def result(self, ticket: int) -> dict:
+        return self.result_buffer(ticket).summary()
+
+    def cancel(self, ticket: int):
+        self.tasks.pop(ticket, None)
+        _check(load_library().gagp_b200_server_cancel(self.handle, C.c_int64(ticket)))

@@ -120,16 +120,32 @@ def load(task_path: str, search_path: Optional[str] = None, population: Optional
     grammar_doc = G.load_definition(os.path.join(base, task["grammar"]))
     with open(os.path.join(base, task["train"])) as f:
         train = json.load(f)
+    search = None
+    if search_path:
+        with open(search_path) as f:
+            search = json.load(f)
+    test = None
+    if task.get("test"):
+        with open(os.path.join(base, task["test"])) as f:
+            test = json.load(f)
+    return assemble(task.get("name", os.path.basename(base)), grammar_doc, train, task["fitness"], search, test,
+                    population, generations, seed)
+
+
+def assemble(name: str, grammar_doc: dict, train: dict, fitness: dict, search: Optional[dict] = None,
+             test: Optional[dict] = None, population: Optional[int] = None, generations: Optional[int] = None,
+             seed: Optional[int] = None, table_cache: Optional[dict] = None) -> LoadedTask:
+    """A loaded task from in-memory task documents (what load() reads from
+    files).  `table_cache` shares compiled phase tables between tasks with
+    the same grammar, inputs and site depth."""
     names = sorted({n for case in train["cases"] for n in case["inputs"]})
-    fitness = task["fitness"]
     settings = SearchSettings()
     settings.metric = fitness["metric"]
     settings.penalty = float(fitness.get("case_cap", 1000))
     settings.fuel = int(grammar_doc["execution_limits"]["fuel"])
     apply_search(settings, DEFAULT_SEARCH)
-    if search_path:
-        with open(search_path) as f:
-            apply_search(settings, json.load(f))
+    if search:
+        apply_search(settings, search)
     if population:
         settings.population = population
     if generations:
@@ -140,16 +156,26 @@ def load(task_path: str, search_path: Optional[str] = None, population: Optional
         raise G.Declined(f"metric {settings.metric} is outside the resident scalar subset")
     if settings.site_depth < 1:
         raise G.Declined("the resident engine here generates its population under a site-depth limit")
-    tables = G.compile_tables(grammar_doc, names, settings.site_depth)
+    key = (json.dumps(grammar_doc, sort_keys=True), tuple(names), settings.site_depth)
+    tables = table_cache.get(key) if table_cache is not None else None
+    if tables is None:
+        tables = G.compile_tables(grammar_doc, names, settings.site_depth)
+        if table_cache is not None:
+            table_cache[key] = tables
     inputs, tags, expected, etag = _case_values(train, names)
-    test = None
-    if task.get("test"):
-        with open(os.path.join(base, task["test"])) as f:
-            tdoc = json.load(f)
-        ti, tt, te, tet = _case_values(tdoc, names)
-        test = CasesBlob(ti, tt, te, tet)
-    return LoadedTask(task.get("name", os.path.basename(base)), tables, CasesBlob(inputs, tags, expected, etag),
-                      settings, test)
+    test_blob = None
+    if test:
+        ti, tt, te, tet = _case_values(test, names)
+        test_blob = CasesBlob(ti, tt, te, tet)
+    return LoadedTask(name, tables, CasesBlob(inputs, tags, expected, etag), settings, test_blob)
+
+
+def from_files(files, table_cache: Optional[dict] = None) -> LoadedTask:
+    """A loaded task straight from an in-memory ``workloads.TaskFiles``."""
+    train = {"format_version": "fitness-cases", "cases": files.train}
+    test = {"format_version": "fitness-cases", "cases": files.test} if files.test else None
+    return assemble(files.name, files.grammar, train, files.fitness, files.search or None, test,
+                    table_cache=table_cache)
 
 
 def program_text(tables: G.PhaseTables, origins, constants) -> str:

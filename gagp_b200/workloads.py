@@ -143,6 +143,50 @@ def poly4(population: int = 16384, generations: int = 128, seed: int = 0, cases:
         search=search_config(population, generations, seed))
 
 
+def _log_uniform_population(rng: random.Random, lo: int, hi: int) -> int:
+    # floor(lo * (hi / lo) ** u), u ~ U[0, 1)
+    return int(lo * (hi / lo) ** rng.random())
+
+
+def batch_mix(count: int = 64, generations: int = 64, max_population: int = 8192) -> List[dict]:
+    """The batching workload: `count` independent searches with seeds 0..count-1,
+    populations log-uniform in 256..max_population, case counts uniform in
+    16..1000.  Even indices are scalar regressions of a random integer
+    polynomial (the large scalar grammar); odd indices are list programs, which
+    this engine declines (entry ``files`` is None for them)."""
+    out = []
+    for i in range(count):
+        rng = random.Random(1000003 * i + 17)
+        population = _log_uniform_population(rng, 256, max_population)
+        cases = rng.randint(16, 1000)
+        entry = {"index": i, "seed": i, "population": population, "cases": cases, "generations": generations,
+                 "kind": "scalar" if i % 2 == 0 else "list", "files": None}
+        if i % 2 == 0:
+            entry["files"] = poly4(population=population, generations=generations, seed=i, cases=cases)
+        out.append(entry)
+    return out
+
+
+def serving_mix(count: int = 2000, seed: int = 0) -> List[dict]:
+    """The serving workload: `count` requests, populations log-uniform in
+    256..16384, case counts uniform in 16..2000, generations uniform in
+    32..128, half scalar regressions of a random integer polynomial and half
+    list programs (declined here: entry ``files`` is None)."""
+    rng = random.Random(seed)
+    out = []
+    for i in range(count):
+        population = _log_uniform_population(rng, 256, 16384)
+        cases = rng.randint(16, 2000)
+        generations = rng.randint(32, 128)
+        scalar = rng.random() < 0.5
+        entry = {"index": i, "seed": seed * 100003 + i, "population": population, "cases": cases,
+                 "generations": generations, "kind": "scalar" if scalar else "list", "files": None}
+        if scalar:
+            entry["files"] = poly4(population=population, generations=generations, seed=entry["seed"], cases=cases)
+        out.append(entry)
+    return out
+
+
 WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4}
 
 

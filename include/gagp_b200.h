@@ -296,6 +296,50 @@ gagp_status gagp_b200_evaluate_rows_static(const gagp_grammar* grammar, const ga
                                            const gagp_search_config* config, const gagp_rows* rows,
                                            double* fitness, uint32_t* wrong, void* stream);
 
+/* ----------------------------------------------------------------- serving
+ * A request loop over one engine with continuous batching.  No counterpart
+ * in the reference, which runs one search per process.  Requests are queued
+ * on submit; every gagp_b200_server_step admits queued requests in arrival
+ * order while their device bytes fit the server's memory budget (a request
+ * waits, it is not reordered), starts the newly admitted searches, runs one
+ * steady-state round of every running search in one batched launch
+ * sequence, and retires the searches that finished: their history and final
+ * population are copied to host memory and their device memory is released
+ * at once for the next admissions.  A request's result is the same as that
+ * search run alone (every kernel works per search; the batch only shares
+ * launches).  Calls on one server are serialized by the caller; the server
+ * uses its engine exclusively while it exists. */
+typedef struct gagp_server gagp_server;
+enum {
+  GAGP_REQUEST_QUEUED = 0,
+  GAGP_REQUEST_RUNNING = 1,
+  GAGP_REQUEST_DONE = 2,
+  GAGP_REQUEST_FAILED = 3
+};
+/* memory_budget: device bytes the running searches may hold (0: the
+ * engine's arena limit); max_active: running searches at most (0: no cap). */
+gagp_status gagp_b200_server_create(gagp_engine* engine, uint64_t memory_budget, int32_t max_active,
+                                    gagp_server** out);
+void gagp_b200_server_destroy(gagp_server* server);
+/* Queues a search request (the blobs are copied).  Declines at once what
+ * the engine would decline at admission (GAGP_DECLINED) and what can never
+ * fit the budget (GAGP_OUT_OF_MEMORY). */
+gagp_status gagp_b200_server_submit(gagp_server* server, const gagp_grammar* grammar, const gagp_cases* cases,
+                                    const gagp_search_config* config, int64_t* ticket);
+/* One serving step (see above); the counts after it. */
+gagp_status gagp_b200_server_step(gagp_server* server, int32_t* running, int32_t* queued, int32_t* finished_now);
+/* GAGP_REQUEST_* state of a ticket. */
+gagp_status gagp_b200_server_poll(gagp_server* server, int64_t ticket, int32_t* state);
+/* Seconds on the server's monotonic clock when the ticket was submitted,
+ * admitted and finished (negative: not yet). */
+gagp_status gagp_b200_server_times(gagp_server* server, int64_t ticket, double* submitted, double* admitted,
+                                   double* finished);
+/* Copies a finished request's result (as gagp_b200_search_result) and
+ * releases the ticket; GAGP_NOT_READY before it finishes. */
+gagp_status gagp_b200_server_result(gagp_server* server, int64_t ticket, gagp_search_result* out);
+/* Drops a ticket in any state (a running search is stopped and freed). */
+gagp_status gagp_b200_server_cancel(gagp_server* server, int64_t ticket);
+
 /* Copies a finished search's history and final ranked population out. */
 gagp_status gagp_b200_search_result(gagp_engine* engine, int32_t search, gagp_search_result* out);
 
