@@ -362,6 +362,154 @@ def run_own_arm(args, rank: int, world: int, local: int):
     print(json.dumps(line))
 
 
+def _mix_tasks(entries):
+    cache = {}
+    return [T.from_files(m["files"], cache) for m in entries if m["files"] is not None]
+
+
+def run_batch_workload(args, rank: int, world: int):
+    """Batching: the scalar half of 64 independent searches (populations
+    log-uniform 256..8192, 16..1000 cases, 64 generations, seeds 0..63) run
+    as one batch (one launch sequence per round, rounds replayed from a CUDA
+    graph) against the plain path (each search alone, one after another)."""
+    from gagp_b200 import build
+    from gagp_b200.engine import Engine
+    build.build()
+    mix = W.batch_mix(64)
+    tasks = _mix_tasks(mix)
+    declined = sum(1 for m in mix if m["files"] is None)
+    with Engine(0) as eng:
+        warm = [eng.admit(lt) for lt in tasks[:2]]  # driver and module warm-up
+        eng.run_batch(warm)
+        for s in warm:
+            s.close()
+        # batched: admission, the batch, results
+        t0 = time.perf_counter()
+        searches = [eng.admit(lt) for lt in tasks]
+        t1 = time.perf_counter()
+        eng.run_batch(searches)
+        t2 = time.perf_counter()
+        cases = sum(int(s.result_buffer().struct.program_cases) for s in searches)
+        t3 = time.perf_counter()
+        for s in searches:
+            s.close()
+        # plain: one search at a time through the same engine
+        p0 = time.perf_counter()
+        plain_run = 0.0
+        for lt in tasks:
+            s = eng.admit(lt)
+            r0 = time.perf_counter()
+            s.run()
+            plain_run += time.perf_counter() - r0
+            s.result_buffer()
+            s.close()
+        p1 = time.perf_counter()
+    n = len(tasks)
+    line = {"metric": "searches/s", "value": n / (t2 - t1), "unit": "searches/s", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": 1000.0 * (t2 - t1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": "batch of the scalar searches of a 64-search mix (populations log-uniform "
+                                   "256..8192, 16..1000 cases, 64 generations, seeds 0..63)",
+                       "searches": n, "declined_list_searches": declined, "parallelism": "single-gpu"},
+            "e2e": {"value": n / (t3 - t0), "unit": "searches/s", "seconds": t3 - t0},
+            "program_cases_per_s": cases / (t2 - t1),
+            "plain": {"searches_per_s": n / plain_run, "e2e_searches_per_s": n / (p1 - p0),
+                      "step": "each search alone, one after another, same engine"},
+            "speedup_vs_plain": (n / (t2 - t1)) / (n / plain_run)}
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_serve_workload(args, rank: int, world: int):
+    """Serving: an open-loop Poisson stream of the scalar requests of a
+    config-5 mix (populations log-uniform 256..16384, 16..2000 cases, 32..128
+    generations) through the continuous-batching server; searches/s and
+    p50/p99 time-to-result against the plain path."""
+    import random
+    from gagp_b200 import build
+    from gagp_b200.engine import Engine, Server
+    build.build()
+    mix = W.serving_mix(args.requests, seed=0)
+    entries = [m for m in mix if m["files"] is not None]
+    tasks = _mix_tasks(entries)
+    rng = random.Random(12345)
+    arrivals, t = [], 0.0
+    for _ in tasks:
+        t += rng.expovariate(args.rate)
+        arrivals.append(t)
+    n = len(tasks)
+    with Engine(0) as eng:
+        warm = [eng.admit(lt) for lt in tasks[:2]]
+        eng.run_batch(warm)
+        for s in warm:
+            s.close()
+        latencies, evals = [], 0
+        with Server(eng) as server:
+            outstanding = {}
+            nxt, done = 0, 0
+            t0 = time.perf_counter()
+            peak_running = 0
+            while done < n:
+                now = time.perf_counter() - t0
+                while nxt < n and arrivals[nxt] <= now:
+                    outstanding[server.submit(tasks[nxt])] = nxt
+                    nxt += 1
+                if not outstanding:
+                    time.sleep(max(0.0, arrivals[nxt] - now))
+                    continue
+                running, queued, finished = server.step()
+                peak_running = max(peak_running, running)
+                if finished:
+                    for ticket in list(outstanding):
+                        if server.poll(ticket) >= 2:
+                            sub, _adm, fin = server.times(ticket)
+                            latencies.append(fin - sub)
+                            evals += int(server.result_buffer(ticket).struct.program_cases)
+                            del outstanding[ticket]
+                            done += 1
+            makespan = time.perf_counter() - t0
+        # plain path: a sample of the requests, each alone
+        sample = tasks[:: max(1, n // 16)][:16]
+        plain_s, plain_evals = 0.0, 0
+        for lt in sample:
+            s = eng.admit(lt)
+            r0 = time.perf_counter()
+            s.run()
+            plain_s += time.perf_counter() - r0
+            plain_evals += int(s.result_buffer().struct.program_cases)
+            s.close()
+    latencies.sort()
+    pct = lambda q: latencies[min(len(latencies) - 1, int(q * len(latencies)))]
+    plain_rate = len(sample) / plain_s
+    # the plain path under the same arrivals: one search at a time, FIFO, each
+    # taking its work at the sample's measured program-case rate
+    per_eval = plain_s / max(1, plain_evals)
+    work = [lt.settings.population * lt.settings.generations * lt.cases.expected.shape[0] for lt in tasks]
+    scale = plain_evals / max(1, sum(work[i] for i in range(0, n, max(1, n // 16))[:16]))
+    clock, plain_lat = 0.0, []
+    for a, w in zip(arrivals, work):
+        clock = max(clock, a) + w * scale * per_eval
+        plain_lat.append(clock - a)
+    plain_lat.sort()
+    ppct = lambda q: plain_lat[min(len(plain_lat) - 1, int(q * len(plain_lat)))]
+    line = {"metric": "searches/s", "value": n / makespan, "unit": "searches/s", "n_gpus": 1, "steps": n,
+            "warmup": 1, "ms_per_step": 1000.0 * makespan / n, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": "open-loop Poisson stream of the scalar requests of a %d-request serving mix "
+                                   "(populations log-uniform 256..16384, 16..2000 cases, 32..128 generations)"
+                                   % args.requests,
+                       "requests": n, "declined_list_requests": args.requests - n, "arrival_rate_per_s": args.rate,
+                       "parallelism": "single-gpu"},
+            "latency_s": {"p50": pct(0.5), "p99": pct(0.99), "max": latencies[-1]},
+            "program_cases_per_s": evals / makespan, "peak_running": peak_running,
+            "plain": {"searches_per_s": plain_rate, "sample": len(sample),
+                      "latency_s_fifo_model": {"p50": ppct(0.5), "p99": ppct(0.99)},
+                      "step": "each search alone through the same engine; latency from a FIFO model of the same "
+                              "arrivals at the sample's measured rate"}}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -369,11 +517,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="poly4", choices=["poly4", "batch", "serve"],
+                    help="poly4: the large scalar search (default); batch: 64-search batching mix; "
+                         "serve: open-loop serving stream")
+    ap.add_argument("--requests", type=int, default=500, help="serve: requests in the mix")
+    ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrival rate (requests/s)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.steps + args.warmup > WORKLOAD["generations"]:
         raise SystemExit("steps + warmup must not exceed the search's %d rounds" % WORKLOAD["generations"])
     rank, world, local = rank_info()
+    if args.workload == "batch" and args.impl != "reference":
+        run_batch_workload(args, rank, world)
+        return
+    if args.workload == "serve" and args.impl != "reference":
+        run_serve_workload(args, rank, world)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
