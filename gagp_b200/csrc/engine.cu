@@ -107,6 +107,17 @@ struct gagp_engine {
   // stream-ordered pool of the searches' device blocks: admission and
   // retirement neither allocate from the driver nor synchronize the device
   cudaMemPool_t pool = nullptr;
+  // VM autotuner: per batch shape, the fast VM's cases per lane, chosen by
+  // timing each candidate on live rounds (results do not depend on it)
+  struct VmTune {
+    double ms[3] = {0, 0, 0};
+    int rounds[3] = {0, 0, 0};
+    int pending = 0;
+    int chosen = -1;
+  };
+  std::map<uint64_t, VmTune> vm_tune;
+  struct TuneMark { uint64_t key; int cand; cudaEvent_t start, stop; };
+  std::vector<TuneMark> tune_marks;
 };
 
 namespace {
@@ -157,6 +168,9 @@ struct Timed {
   }
 };
 // Adds the elapsed times of completed launches (after a stream sync).
+// Fast-VM cases per lane, the autotuner's candidates.
+constexpr int kVmLanes[3] = {1, 2, 4};
+
 void harvest(gagp_engine* e) {
   for (const auto& p : e->pending) {
     float ms = 0;
@@ -166,6 +180,23 @@ void harvest(gagp_engine* e) {
     }
   }
   e->pending.clear();
+  // VM autotuner: once every candidate's round has been timed, keep the
+  // fastest (mean fast-VM time per round)
+  for (const auto& m : e->tune_marks) {
+    float ms = 0;
+    auto& t = e->vm_tune[m.key];
+    if (cudaEventElapsedTime(&ms, m.start, m.stop) == cudaSuccess) t.ms[m.cand] += ms;
+    --t.pending;
+  }
+  for (const auto& m : e->tune_marks) {
+    auto& t = e->vm_tune[m.key];
+    if (t.chosen >= 0 || t.pending > 0 || !t.rounds[0] || !t.rounds[1] || !t.rounds[2]) continue;
+    int best = 0;
+    for (int c = 1; c < 3; ++c)
+      if (t.ms[c] / t.rounds[c] < t.ms[best] / t.rounds[best]) best = c;
+    t.chosen = best;
+  }
+  e->tune_marks.clear();
   e->event_next = 0;
 }
 
@@ -188,6 +219,14 @@ int cases_per_lane(int cases) {
   if (cases <= 32) return 1;
   if (cases <= 64) return 2;
   return 4;
+}
+
+// Batch shape of the VM autotuner: case count rounded up to a power of two
+// and the input count.
+uint64_t vm_key(int max_C, int max_inputs) {
+  uint64_t c = 1;
+  while (c < uint64_t(max_C)) c <<= 1;
+  return (c << 8) | uint64_t(max_inputs & 0xff);
 }
 
 int bits_for(uint64_t v) {
@@ -425,7 +464,9 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   uint64_t keep = ~0ULL;  // freed blocks stay in the pool for the next admission
   CUDA_TRY(cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 16384));
-  CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vary, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   *out = e.release();
   return GAGP_OK;
@@ -677,6 +718,7 @@ struct BatchView {
   int n = 0, total_members = 0, total_children = 0, max_P = 0, max_lanes = 1, max_rounds = 0, max_stride = 4;
   long long max_draws = 0;
   int max_code_stride = 2;
+  int max_C = 1, max_inputs = 0;
 };
 
 gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
@@ -717,7 +759,11 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
   v->max_draws = 0;
   v->max_code_stride = 2;
   v->max_lanes = 1;
+  v->max_C = 1;
+  v->max_inputs = 0;
   for (Search* s : list) {
+    v->max_C = std::max(v->max_C, s->desc.C);
+    v->max_inputs = std::max(v->max_inputs, s->desc.n_inputs);
     v->total_members += s->P;
     v->total_children += s->B;
     v->max_P = std::max(v->max_P, s->P);
@@ -733,19 +779,71 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
 int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1) / threads); }
 
 // Evaluates lowered programs listed by k_lower (both VMs).
+// Fast-VM launch of one instantiation.
+void vm_fast_launch(int lanes, int blocks, int threads, size_t smem, cudaStream_t stream, const gb::SearchDesc* descs,
+                    int mode, const gb::ProgramRef* list, const int32_t* count, int temp_stride, int code_stride,
+                    int const_stride) {
+  switch (lanes) {
+    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride); break;
+    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride); break;
+    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride); break;
+  }
+}
+
+// The VM configuration of one round: the tuned cases per lane, or the next
+// candidate to time (measure_key != 0) while the shape is being tuned.
+struct VmPlan {
+  int lanes = 4;
+  uint64_t measure_key = 0;
+  int cand = 0;
+};
+VmPlan plan_vm(gagp_engine* e, const BatchView& v, bool may_measure) {
+  VmPlan p;
+  const uint64_t key = vm_key(v.max_C, v.max_inputs);
+  auto& t = e->vm_tune[key];
+  if (t.chosen >= 0) { p.lanes = kVmLanes[t.chosen]; return p; }
+  p.lanes = v.max_lanes;  // the heuristic until the candidates are timed
+  if (!may_measure || e->profiling) return p;
+  for (int c = 0; c < 3; ++c)
+    if (!t.rounds[c]) {
+      p.lanes = kVmLanes[c];
+      p.cand = c;
+      p.measure_key = key;
+      ++t.rounds[c];
+      return p;
+    }
+  return p;
+}
+
 gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t stream, const gb::ProgramRef* fast,
-                      const gb::ProgramRef* general, const int32_t* counts) {
+                      const gb::ProgramRef* general, const int32_t* counts, const VmPlan& plan) {
   const int warps = 8;
-  const int temp_stride = gb::kMaxTemps * v.max_lanes * 32;
+  const int temp_stride = gb::kMaxTemps * plan.lanes * 32;
   const int code_stride = (v.max_code_stride + 1) & ~1;  // uint2 slots, in int64 units
   const int const_stride = v.max_stride;
   const size_t smem = size_t(warps) * (temp_stride + code_stride + const_stride) * sizeof(int64_t);
-  const int per_sm = std::max(1, std::min(4, int((e->max_smem - 1024) / std::max<size_t>(smem, 1))));
-  const int blocks = e->sm_count * per_sm;
+  // persistent: as many blocks as fit on every SM at once
+  int per_sm = 0;
+  const cudaError_t occ = plan.lanes == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vm_fast<1>, warps * 32, smem)
+                          : plan.lanes == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vm_fast<2>, warps * 32, smem)
+                                            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vm_fast<4>, warps * 32, smem);
+  if (occ != cudaSuccess) return fail(GAGP_DEVICE_ERROR, std::string("VM occupancy: ") + cudaGetErrorString(occ));
+  const int blocks = e->sm_count * std::max(1, per_sm);
+  cudaEvent_t mark_start = nullptr, mark_stop = nullptr;
+  if (plan.measure_key) {
+    mark_start = take_event(e);
+    mark_stop = take_event(e);
+    cudaEventRecord(mark_start, stream);
+  }
   {
     Timed t(e, KN_VM_FAST, stream);
-    gb::k_vm_fast<<<blocks, warps * 32, smem, stream>>>(v.d_desc, mode, fast, counts, temp_stride, code_stride,
-                                                         const_stride);
+    vm_fast_launch(plan.lanes, blocks, warps * 32, smem, stream, v.d_desc, mode, fast, counts, temp_stride, code_stride,
+                   const_stride);
+  }
+  if (plan.measure_key) {
+    cudaEventRecord(mark_stop, stream);
+    e->tune_marks.push_back({plan.measure_key, plan.cand, mark_start, mark_stop});
+    ++e->vm_tune[plan.measure_key].pending;
   }
   {
     Timed t(e, KN_VM_GENERAL, stream);
@@ -762,13 +860,16 @@ gagp_status launch_start(gagp_engine* e, const BatchView& v) {
     gb::k_lower<<<blocks_for(v.total_members, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(
         v.d_desc, v.d_member_off, v.n, 0, e->d_fast, e->d_general, e->d_counts, 0, v.total_members);
   }
-  launch_vm(e, v, 0, e->stream, e->d_fast, e->d_general, e->d_counts);
+  VmPlan start_plan;
+  start_plan.lanes = v.max_lanes;
+  launch_vm(e, v, 0, e->stream, e->d_fast, e->d_general, e->d_counts, start_plan);
   { Timed t(e, KN_KEYS); gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   { Timed t(e, KN_START); gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
 }
 
-gagp_status launch_round(gagp_engine* e, const BatchView& v) {
+gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = true) {
+  const VmPlan vm = plan_vm(e, v, may_measure);
   // the run-generator top-up overlaps everything up to the placement
   CUDA_TRY(cudaEventRecord(e->fork, e->stream));
   CUDA_TRY(cudaStreamWaitEvent(e->side, e->fork, 0));
@@ -800,7 +901,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v) {
       gb::k_lower<<<blocks_for(hi - lo, gb::kLowerWarps), gb::kLowerWarps * 32, 0, st>>>(
           v.d_desc, v.d_child_off, v.n, 1, e->d_fast + lo, e->d_general + lo, counts, lo, hi);
     }
-    launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts);
+    launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts, vm);
     if (chunks > 1) {
       CUDA_TRY(cudaEventRecord(e->chunk_done[c], st));
       CUDA_TRY(cudaStreamWaitEvent(e->stream, e->chunk_done[c], 0));
@@ -853,7 +954,7 @@ struct RoundGraph {
 };
 gagp_status capture_round(gagp_engine* e, const BatchView& v, RoundGraph* out) {
   CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-  const gagp_status st = launch_round(e, v);
+  const gagp_status st = launch_round(e, v, false);
   cudaGraph_t graph = nullptr;
   const cudaError_t ended = cudaStreamEndCapture(e->stream, &graph);  // always leaves capture mode
   if (st != GAGP_OK) {
@@ -877,10 +978,22 @@ gagp_status launch_rounds(gagp_engine* e, const BatchView& v, int rounds) {
     }
     return GAGP_OK;
   }
+  // an untuned batch shape times its VM candidates on the first rounds
+  int r = 0;
+  while (r < rounds && e->vm_tune[vm_key(v.max_C, v.max_inputs)].chosen < 0 && r < 3) {
+    const gagp_status st = launch_round(e, v);
+    if (st != GAGP_OK) return st;
+    ++r;
+  }
+  if (r) {
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    harvest(e);
+  }
+  if (r >= rounds) return GAGP_OK;
   RoundGraph g;
   const gagp_status st = capture_round(e, v, &g);
   if (st != GAGP_OK) return st;
-  for (int r = 0; r < rounds; ++r) CUDA_TRY(cudaGraphLaunch(g.exec, e->stream));
+  for (; r < rounds; ++r) CUDA_TRY(cudaGraphLaunch(g.exec, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));  // the graph is destroyed on return
   return GAGP_OK;
 }
@@ -1097,8 +1210,8 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   const size_t smem = size_t(warps) * (temp_stride + code_stride + p.stride) * sizeof(int64_t);
   if (smem > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the VM's shared memory");
   const int per_sm = std::max(1, std::min(4, int((max_smem - 1024) / smem)));
-  gb::k_vm_fast<<<sm_count * per_sm, warps * 32, smem, stream>>>(dd, 0, fast, counts, temp_stride, code_stride,
-                                                                  p.stride);
+  vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, counts, temp_stride, code_stride,
+                 p.stride);
   gb::k_vm_general<<<sm_count * 4, 128, 0, stream>>>(dd, 0, general, counts + 1);
   CUDA_TRY(cudaGetLastError());
   int32_t round[4];
@@ -1143,7 +1256,9 @@ gagp_status static_scratch_on(int device, StaticDevice** out) {
     int sms = 0, smem = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     CUDA_TRY(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-    CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
+    CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
+    CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
+    CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
     d.scratch = static_cast<char*>(ptr);
     d.sm_count = sms;
     d.max_smem = size_t(smem);
@@ -1239,7 +1354,7 @@ gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t 
   }
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks;
   RoundGraph graph;
-  const bool replay = !e->profiling && rounds > 1;
+  const bool replay = !e->profiling && rounds > 1 && e->vm_tune[vm_key(v.max_C, v.max_inputs)].chosen >= 0;
   if (replay && (st = capture_round(e, v, &graph)) != GAGP_OK) return st;
   for (int r = 0; r < rounds; ++r) {
     if (flush_l2) CUDA_TRY(cudaMemsetAsync(e->flush_buffer, r & 0xff, e->flush_bytes, e->stream));

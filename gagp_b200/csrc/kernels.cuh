@@ -132,7 +132,7 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
 }
 
 // Fast VM: persistent warps over the fast list.  Per warp shared memory:
-// temporaries (kMaxTemps x lanes x 32), the staged code (code_stride) and
+// temporaries (kMaxTemps x K x 32), the staged code (code_stride) and
 // constants (stride).
 template <int K>
 __device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWarpSmem& w, int64_t& loss,
@@ -143,8 +143,12 @@ __device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWar
     default: run_accumulator<K, 0>(s, slot, w, loss, wrong, ops); break;
   }
 }
-__global__ void k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list, const int32_t* list_count,
-                          int temp_stride, int code_stride, int const_stride) {
+// One instantiation per cases-per-lane K (each with its own register
+// budget); the engine's autotuner picks K per batch shape.
+template <int K>
+__global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list,
+                                                 const int32_t* list_count, int temp_stride, int code_stride,
+                                                 int const_stride) {
   extern __shared__ __align__(16) int64_t smem_vm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
@@ -158,11 +162,7 @@ __global__ void k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* l
     int64_t loss = 0;
     uint32_t wrong = 0;
     uint64_t ops = 0;
-    switch (s.vm_cases_per_lane) {
-      case 1: run_k<1>(s, p.slot, w, loss, wrong, ops); break;
-      case 2: run_k<2>(s, p.slot, w, loss, wrong, ops); break;
-      default: run_k<4>(s, p.slot, w, loss, wrong, ops); break;
-    }
+    run_k<K>(s, p.slot, w, loss, wrong, ops);
     loss = warp_sum(loss);
     wrong = warp_sum(wrong);
     if (lane == 0) {
