@@ -874,8 +874,9 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   CUDA_TRY(cudaEventRecord(e->fork, e->stream));
   CUDA_TRY(cudaStreamWaitEvent(e->side, e->fork, 0));
   { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
+  // the history entry reads only what the placement later rewrites
+  { Timed t(e, KN_RECORD, e->side); gb::k_record<<<v.n, 1024, 0, e->side>>>(v.d_desc, v.n, 1); }
   CUDA_TRY(cudaEventRecord(e->join, e->side));
-  { Timed t(e, KN_RECORD); gb::k_record<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n, 1); }
   // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
   // next child of the variation warps; range c's lists start at item lo
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));

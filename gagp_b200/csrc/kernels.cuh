@@ -361,8 +361,8 @@ __global__ void k_start(const SearchDesc* descs, int n) {
 // History entry before every population/batch rounds (record(),
 // evolve.cpp:360-371): the best member, its row, and the exact integer sum of
 // member fitness (the host forms the long double mean).
-__global__ void k_record(const SearchDesc* descs, int n, int only_epoch_start) {
-  __shared__ long long partial[256];
+__global__ void __launch_bounds__(1024) k_record(const SearchDesc* descs, int n, int only_epoch_start) {
+  __shared__ long long partial[1024];
   const SearchDesc& s = descs[blockIdx.x];
   if (!search_live(s)) return;
   const int round = s.round[0];
@@ -370,6 +370,7 @@ __global__ void k_record(const SearchDesc* descs, int n, int only_epoch_start) {
   const int entry = s.round[1];
   if (entry >= s.generations) return;
   long long sum = 0;
+#pragma unroll 4
   for (int m = threadIdx.x; m < s.P; m += blockDim.x) sum += (long long)s.fitness[m];
   partial[threadIdx.x] = sum;
   __syncthreads();
@@ -697,11 +698,12 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
       const int uv = __shfl_up_sync(kFull, mv, o);
       if (lane >= o && key_before(uk, uv, mk, mv)) { mk = uk; mv = uv; }
     }
+    constexpr int kWarps = kPlaceThreads / 32;
     if (lane == 31) { scan_key[warp] = mk; scan_idx[warp] = mv; }
     __syncthreads();
     if (warp == 0) {
-      uint64_t wk = scan_key[lane];
-      int wv = scan_idx[lane];
+      uint64_t wk = lane < kWarps ? scan_key[lane] : ~0ULL;
+      int wv = lane < kWarps ? scan_idx[lane] : 0x7fffffff;
       for (int o = 1; o < 32; o <<= 1) {
         const uint64_t uk = __shfl_up_sync(kFull, wk, o);
         const int uv = __shfl_up_sync(kFull, wv, o);
@@ -753,7 +755,10 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
       if (tid == 0) {
         int fv = best0;
         uint64_t fk = best0_key;
-        if (key_before(scan_key[31], scan_idx[31], fk, fv)) { fk = scan_key[31]; fv = scan_idx[31]; }
+        if (key_before(scan_key[kWarps - 1], scan_idx[kWarps - 1], fk, fv)) {
+          fk = scan_key[kWarps - 1];
+          fv = scan_idx[kWarps - 1];
+        }
         shared_best = fv;
         shared_fail = 0;
         // the next round's seed: the raw output after the 2B placement draws
