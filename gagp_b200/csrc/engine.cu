@@ -914,8 +914,8 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     // member keys plus as many 16-bit staged draws as fit (B * replacement + slack)
     const size_t limit = e->max_smem - 16384;  // static shared memory of k_place: ~13 KB
     // keys, then either the level owners (4 bytes per member) or the staged draws
-    size_t bytes = size_t(v.max_P) * sizeof(uint64_t) +
-                   std::max(size_t(v.max_P) * sizeof(int32_t), size_t(v.max_draws + 64) * sizeof(uint16_t));
+    size_t bytes = size_t(v.max_P + 1) * sizeof(uint64_t) +
+                   std::max(size_t(v.max_P) * sizeof(int32_t) + 64, size_t(v.max_draws + 64) * sizeof(uint16_t));
     bytes = std::min(bytes, limit);
     CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join, 0));
     gb::k_place<<<v.n, gb::kPlaceThreads, bytes, e->stream>>>(v.d_desc, v.n, int(bytes));

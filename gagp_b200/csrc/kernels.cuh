@@ -591,10 +591,12 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
   const long long t1 = clock64();
   // ---------------------------------------------------- level-parallel path
   constexpr int kPerThread = 16;
-  int32_t* owner = reinterpret_cast<int32_t*>(keys + P);
+  // owner area after the keys, 16-byte aligned, with 64 bytes of slack for
+  // the per-thread 16-byte reads of the staged draws
+  int32_t* owner = reinterpret_cast<int32_t*>(keys + P + (P & 1));
   const bool parallel_path = rs == 2 && blockDim.x == kPlaceThreads && B <= kPlaceThreads * kPerThread &&
                              wp - rp >= need &&
-                             dyn_bytes >= int(sizeof(uint64_t) + sizeof(int32_t)) * P;
+                             dyn_bytes >= int(sizeof(uint64_t)) * (P + 1) + int(sizeof(int32_t)) * P + 64;
   bool parallel_done = false;
   if (parallel_path) {
     // thread tid owns children [16 tid, 16 tid + 16): cand[t] holds child
@@ -603,20 +605,39 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
     const int begin = tid * kPerThread;
     constexpr int kBatch = 4;  // child keys loaded together
     const uint64_t* __restrict__ ckey = s.c_key;
-    uint32_t cand[kPerThread];
-    uint32_t pending = 0;
-#pragma unroll
-    for (int t = 0; t < kPerThread; ++t) {
-      const int j = begin + t;
-      cand[t] = 0;
-      if (j < B) {
-        int p0 = base + 2 * j, p1 = p0 + 1;
-        if (p0 >= cap) p0 -= cap;
-        if (p1 >= cap) p1 -= cap;
-        cand[t] = s.stream_mod[p0] | (s.stream_mod[p1] << 16);
-        pending |= 1u << t;
+    // the 2B draws (residues < P <= 65536), staged as 16-bit values in the
+    // owner area with coalesced loads, then read back per thread: child j's
+    // pair is the 32-bit word j
+    {
+      uint16_t* stage = reinterpret_cast<uint16_t*>(owner);
+      const uint32_t* __restrict__ smod = s.stream_mod;
+      for (int i = tid; i < 2 * B; i += blockDim.x) {
+        int pos = base + i;
+        if (pos >= cap) pos -= cap;
+        stage[i] = uint16_t(smod[pos]);
       }
     }
+    __syncthreads();
+    uint32_t cand[kPerThread];
+    uint32_t pending = 0;
+    {
+      static_assert(kPerThread % 4 == 0, "draw pairs are read four at a time");
+      const uint4* pairs = reinterpret_cast<const uint4*>(owner) + size_t(begin) / 4;
+#pragma unroll
+      for (int q = 0; q < kPerThread / 4; ++q) {
+        const uint4 v = begin < B ? pairs[q] : make_uint4(0, 0, 0, 0);
+        cand[4 * q] = v.x;
+        cand[4 * q + 1] = v.y;
+        cand[4 * q + 2] = v.z;
+        cand[4 * q + 3] = v.w;
+      }
+#pragma unroll
+      for (int t = 0; t < kPerThread; ++t) {
+        if (begin + t < B) pending |= 1u << t;
+        else cand[t] = 0;
+      }
+    }
+    __syncthreads();  // the owner area is reset below
     // owner[m]: the earliest child of the current level that drew member m,
     // tagged with the level so that no per-level reset is needed (a later
     // level's tag is smaller than every earlier one's)
@@ -891,13 +912,34 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
     stream_ptrs(s)[1] = shared_wp;
   }
   for (int i = tid; i < 312; i += blockDim.x) s.mt[i] = mt[i];
-  for (int m = tid; m < P; m += blockDim.x) {
-    const int c = placed[m];
-    if (c >= 0) {
-      s.key[m] = keys[m];
-      s.fitness[m] = s.c_fitness[c];
-      s.wrong[m] = s.c_wrong[c];
-      s.nodes[m] = s.c_nodes[c];
+  {
+    // placed members take their child's statistics; four members' loads in flight at once
+    const double* __restrict__ cfit = s.c_fitness;
+    const uint32_t* __restrict__ cwrong = s.c_wrong;
+    const uint32_t* __restrict__ cnodes = s.c_nodes;
+    const int stride = blockDim.x;
+    for (int m0 = tid; m0 < P; m0 += 4 * stride) {
+      int c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c[u] = m0 + u * stride < P ? placed[m0 + u * stride] : -1;
+      double f[4];
+      uint32_t w[4], nd[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c[u] >= 0) {
+          f[u] = cfit[c[u]];
+          w[u] = cwrong[c[u]];
+          nd[u] = cnodes[c[u]];
+        }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c[u] >= 0) {
+          const int m = m0 + u * stride;
+          s.key[m] = keys[m];
+          s.fitness[m] = f[u];
+          s.wrong[m] = w[u];
+          s.nodes[m] = nd[u];
+        }
     }
   }
   if (tid == 0) {
