@@ -40,6 +40,7 @@ from gagp_b200 import task as T  # noqa: E402
 METRIC = "VM program-case evals/s"
 UNIT = "program-case evals/s"
 WORKLOAD = dict(population=16384, generations=128, cases=256, max_nodes=64)
+PROFILE_ROUNDS = 3
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -336,12 +337,17 @@ def run_own_arm(args, rank: int, world: int, local: int):
                 import torch
                 dist.barrier()
                 torch.cuda.synchronize()
-            eng.profile(True)
             with ClockSampler(local) as clocks:
                 ms = eng.advance([s], args.steps, flush_l2=True)
+            after = eng.counters(s)
+            # per-kernel CUDA-event durations: PROFILE_ROUNDS further rounds of
+            # the same search right after the timed region (timing each launch
+            # needs direct launches, which the timed rounds avoid)
+            eng.profile(True)
+            eng.advance([s], PROFILE_ROUNDS, flush_l2=True)
             stats = eng.kernel_stats()
             eng.profile(False)
-            after = eng.counters(s)
+            profiled = eng.counters(s)
             s.close()
     cases = after["program_cases"] - before["program_cases"]
     secs = ms / 1000.0
@@ -351,15 +357,18 @@ def run_own_arm(args, rank: int, world: int, local: int):
         dist.destroy_process_group()
     if rank != 0:
         return
-    launches = sum(v["launches"] for v in stats.values())
+    launches = sum(v["launches"] for v in stats.values()) * args.steps // PROFILE_ROUNDS
     delta = {k: after[k] - before[k] for k in after if isinstance(after[k], int)}
+    pdelta = {k: profiled[k] - after[k] for k in after if isinstance(after[k], int)}
     line = {"metric": METRIC, "value": cases / secs, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
             "config": config_block(world, seed), "e2e": e2e, "gpu_launches": launches,
-            "kernels": {k: {"ms_per_step": v["ms"] / args.steps, "launches": v["launches"]} for k, v in stats.items()},
-            "vm": vm_entry(stats, delta),
-            "roofline": roofline_entry(stats, delta, args.steps, peaks()), "clocks": clocks.summary(),
+            "kernels": {k: {"ms_per_step": v["ms"] / PROFILE_ROUNDS, "launches_per_step": v["launches"] / PROFILE_ROUNDS}
+                        for k, v in stats.items()},
+            "kernel_timing": "CUDA events per launch over %d profiled rounds right after the timed region" % PROFILE_ROUNDS,
+            "vm": vm_entry(stats, pdelta),
+            "roofline": roofline_entry(stats, pdelta, PROFILE_ROUNDS, peaks()), "clocks": clocks.summary(),
             "counters": {"program_cases": cases, "evaluated_programs": after["evaluated_programs"] - before["evaluated_programs"],
                          "reused_programs": after["reused_programs"] - before["reused_programs"],
                          "vm_ops": after["vm_ops"] - before["vm_ops"],
@@ -554,8 +563,9 @@ def main():
     ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrival rate (requests/s)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.steps + args.warmup > WORKLOAD["generations"]:
-        raise SystemExit("steps + warmup must not exceed the search's %d rounds" % WORKLOAD["generations"])
+    if args.steps + args.warmup + PROFILE_ROUNDS > WORKLOAD["generations"]:
+        raise SystemExit("steps + warmup + %d profiled rounds must not exceed the search's %d rounds"
+                         % (PROFILE_ROUNDS, WORKLOAD["generations"]))
     rank, world, local = rank_info()
     if args.workload == "batch" and args.impl != "reference":
         run_batch_workload(args, rank, world)

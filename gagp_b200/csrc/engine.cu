@@ -74,7 +74,7 @@ struct gagp_engine {
   // the children of a round in kChunks ranges, each varied, lowered and
   // evaluated on its own stream so that one range's slowest children
   // overlap the other ranges' work
-  static constexpr int kChunks = 4;
+  static constexpr int kChunks = 8;
   cudaStream_t chunk_stream[kChunks] = {};
   cudaEvent_t chunk_fork = nullptr, chunk_done[kChunks] = {};
   std::map<int, std::unique_ptr<Search>> searches;
