@@ -354,7 +354,7 @@ struct Plan {
       gen_nt, local_types, inputs, expected;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
-  size_t code, code_len, kpool, code_temps, bc, bc_len, bc_consts;
+  size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, round, hist_sum, hist_fitness, hist_wrong,
       hist_nodes, hist_node, hist_cval, hist_len, counters;
   int stride, code_stride, bc_stride, stream_capacity, slots;
@@ -406,7 +406,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
-  p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots);
+  p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots); p.vm_acc = L.take(16 * slots);
   p.bc = L.take(20 * slots * p.bc_stride); p.bc_len = L.take(4 * slots);
   p.bc_consts = L.take(8 * slots * p.bc_stride);
   p.mt = L.take(8 * 312); p.stream = L.take(8 * size_t(p.stream_capacity));
@@ -655,6 +655,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
+  d.vm_acc = at<unsigned long long>(b, p.vm_acc);
   d.bc = at<int32_t>(b, p.bc); d.bc_len = at<int32_t>(b, p.bc_len); d.bc_consts = at<int64_t>(b, p.bc_consts);
   d.bc_stride = p.bc_stride;
   d.mt = at<uint64_t>(b, p.mt); d.stream = at<uint64_t>(b, p.stream); d.stream_mod = at<uint32_t>(b, p.stream_mod);
@@ -782,11 +783,12 @@ int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1
 // Fast-VM launch of one instantiation.
 void vm_fast_launch(int lanes, int blocks, int threads, size_t smem, cudaStream_t stream, const gb::SearchDesc* descs,
                     int mode, const gb::ProgramRef* list, const int32_t* count, int temp_stride, int code_stride,
-                    int const_stride) {
+                    int const_stride, int max_C) {
+  const int tiles = (max_C + 32 * lanes - 1) / (32 * lanes);
   switch (lanes) {
-    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride); break;
-    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride); break;
-    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride); break;
+    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride, tiles); break;
+    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride, tiles); break;
+    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride, tiles); break;
   }
 }
 
@@ -838,7 +840,7 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
   {
     Timed t(e, KN_VM_FAST, stream);
     vm_fast_launch(plan.lanes, blocks, warps * 32, smem, stream, v.d_desc, mode, fast, counts, temp_stride, code_stride,
-                   const_stride);
+                   const_stride, v.max_C);
   }
   if (plan.measure_key) {
     cudaEventRecord(mark_stop, stream);
@@ -1027,7 +1029,7 @@ namespace {
 // one caller-provided device region.
 struct EvalPlan {
   Layout L;
-  size_t desc, ex, info, minimum, local_types, inputs, expected, node, cval, len, code, code_len, kpool, code_temps,
+  size_t desc, ex, info, minimum, local_types, inputs, expected, node, cval, len, code, code_len, kpool, code_temps, vm_acc,
       bc, bc_len, bc_consts, fitness, wrong, counters, round, fast, general, counts, off;
   int stride, code_stride, bc_stride;
 };
@@ -1056,7 +1058,7 @@ EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   p.expected = L.take(sizeof(int64_t) * C);
   p.node = L.take(8 * S * R); p.cval = L.take(8 * S * R); p.len = L.take(4 * R);
   p.code = L.take(8 * R * p.code_stride); p.code_len = L.take(4 * R); p.kpool = L.take(8 * R * S);
-  p.code_temps = L.take(4 * R);
+  p.code_temps = L.take(4 * R); p.vm_acc = L.take(16 * R);
   p.bc = L.take(20 * R * p.bc_stride); p.bc_len = L.take(4 * R); p.bc_consts = L.take(8 * R * p.bc_stride);
   p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.counters = L.take(8 * GAGP_COUNTERS); p.round = L.take(16);
   p.fast = L.take(sizeof(gb::ProgramRef) * R); p.general = L.take(sizeof(gb::ProgramRef) * R);
@@ -1172,6 +1174,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride;
   d.code_temps = at<int32_t>(b, p.code_temps);
+  d.vm_acc = at<unsigned long long>(b, p.vm_acc);
   d.bc = at<int32_t>(b, p.bc);
   d.bc_len = at<int32_t>(b, p.bc_len);
   d.bc_consts = at<int64_t>(b, p.bc_consts);
@@ -1212,7 +1215,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   if (smem > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the VM's shared memory");
   const int per_sm = std::max(1, std::min(4, int((max_smem - 1024) / smem)));
   vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, counts, temp_stride, code_stride,
-                 p.stride);
+                 p.stride, C);
   gb::k_vm_general<<<sm_count * 4, 128, 0, stream>>>(dd, 0, general, counts + 1);
   CUDA_TRY(cudaGetLastError());
   int32_t round[4];

@@ -96,6 +96,8 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
       if (lane == 0) {
         s.code_len[slot] = len;
         s.code_temps[slot] = temps;
+        s.vm_acc[2 * size_t(slot)] = 0;
+        s.vm_acc[2 * size_t(slot) + 1] = 0;
         fast_list[atomicAdd(&list_count[0], 1)] = ProgramRef{si, slot};
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
                   (unsigned long long)(row_bytes + 8ull * (len + t.nc) + 16));
@@ -135,41 +137,56 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
 // temporaries (kMaxTemps x K x 32), the staged code (code_stride) and
 // constants (stride).
 template <int K>
-__device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWarpSmem& w, int64_t& loss,
-                                      uint32_t& wrong, uint64_t& ops) {
+__device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWarpSmem& w, int case_begin,
+                                      int case_end, int64_t& loss, uint32_t& wrong, uint64_t& ops) {
   switch (s.n_inputs) {
-    case 1: run_accumulator<K, 1>(s, slot, w, loss, wrong, ops); break;
-    case 2: run_accumulator<K, 2>(s, slot, w, loss, wrong, ops); break;
-    default: run_accumulator<K, 0>(s, slot, w, loss, wrong, ops); break;
+    case 1: run_accumulator<K, 1>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
+    case 2: run_accumulator<K, 2>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
+    default: run_accumulator<K, 0>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
   }
 }
 // One instantiation per cases-per-lane K (each with its own register
-// budget); the engine's autotuner picks K per batch shape.
+// budget); the engine's autotuner picks K per batch shape.  Work items are
+// (program, tile of 32 K cases), program-major, so that a round with fewer
+// programs than resident warps still fills the GPU; each tile adds its loss
+// and wrong count to the program's accumulators and the last tile to finish
+// stores the program's result (integer sums: the order does not matter).
 template <int K>
 __global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list,
                                                  const int32_t* list_count, int temp_stride, int code_stride,
-                                                 int const_stride) {
+                                                 int const_stride, int tiles_max) {
   extern __shared__ __align__(16) int64_t smem_vm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
   const size_t per_warp = size_t(temp_stride) + size_t(code_stride) + size_t(const_stride);  // int64 units
   int64_t* base = smem_vm + size_t(warp) * per_warp;
   const VmWarpSmem w{base, reinterpret_cast<uint2*>(base + temp_stride), base + temp_stride + code_stride};
-  const int count = *list_count;
-  for (int i = blockIdx.x * warps + warp; i < count; i += gridDim.x * warps) {
-    const ProgramRef p = list[i];
+  const long long items = (long long)(*list_count) * tiles_max;
+  for (long long item = (long long)blockIdx.x * warps + warp; item < items; item += (long long)gridDim.x * warps) {
+    const ProgramRef p = list[item / tiles_max];
+    const int case0 = int(item % tiles_max) * 32 * K;
     const SearchDesc& s = descs[p.search];
+    if (case0 >= s.C) continue;
     int64_t loss = 0;
     uint32_t wrong = 0;
     uint64_t ops = 0;
-    run_k<K>(s, p.slot, w, loss, wrong, ops);
+    run_k<K>(s, p.slot, w, case0, min(s.C, case0 + 32 * K), loss, wrong, ops);
     loss = warp_sum(loss);
     wrong = warp_sum(wrong);
     if (lane == 0) {
-      store_result(s, mode, p.slot, loss, wrong);
-      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
-      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
+      unsigned long long* acc = s.vm_acc + 2 * size_t(p.slot);
+      atomicAdd(&acc[0], (unsigned long long)loss);
+      __threadfence();
+      const unsigned long long before = atomicAdd(&acc[1], (unsigned long long)wrong | (1ULL << 32));
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), (unsigned long long)ops);
+      const unsigned tiles = unsigned((s.C + 32 * K - 1) / (32 * K));
+      if (unsigned(before >> 32) == tiles - 1) {  // the last tile of the program
+        __threadfence();
+        const int64_t total = int64_t(atomicAdd(&acc[0], 0ULL));
+        store_result(s, mode, p.slot, total, uint32_t(before) + wrong);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
+      }
     }
   }
 }

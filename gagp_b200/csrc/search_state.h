@@ -108,6 +108,9 @@ struct SearchDesc {
   uint2* code; int32_t* code_len; int64_t* kpool;
   int32_t code_stride;                 // accumulator instructions per program slot
   int32_t* code_temps;                 // temporaries; <0: needs the general VM
+  // per program slot, the fast VM's tile accumulators: [2 slot] the loss
+  // sum, [2 slot + 1] wrong cases (low 32 bits) | tiles done (high 32 bits)
+  unsigned long long* vm_acc;
   int32_t* bc;                         // reference bytecode (op,flags,a,b,fuel) per program
   int32_t* bc_len;
   int64_t* bc_consts;

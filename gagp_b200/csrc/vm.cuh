@@ -83,9 +83,10 @@ struct VmWarpSmem {
   int64_t* consts;
 };
 
+// Runs cases [case_begin, case_end) (tiles of 32 K from case_begin).
 template <int K, int NIN>
-__device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWarpSmem& w, int64_t& loss_out,
-                                       uint32_t& wrong_out, uint64_t& ops_out) {
+__device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWarpSmem& w, int case_begin,
+                                       int case_end, int64_t& loss_out, uint32_t& wrong_out, uint64_t& ops_out) {
   const int lane = threadIdx.x & 31;
   const int len = s.code_len[slot];
   {
@@ -95,20 +96,20 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
     for (int i = lane; i < s.stride; i += 32) w.consts[i] = kpool[i];
     __syncwarp();
   }
-  const int C = s.C;
+  const int C = s.C;  // input-major stride
   const int64_t* __restrict__ inputs = s.inputs;
   int64_t* __restrict__ temps = w.temps;
   int64_t loss = 0;
   uint32_t wrong = 0;
-  for (int tile = 0; tile < C; tile += 32 * K) {
+  for (int tile = case_begin; tile < case_end; tile += 32 * K) {
     int64_t acc[K];
     int64_t in0[K], in1[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       acc[k] = 0;
       const int c = tile + k * 32 + lane;
-      in0[k] = (NIN >= 1 && c < C) ? __ldg(&inputs[c]) : 0;
-      in1[k] = (NIN >= 2 && c < C) ? __ldg(&inputs[size_t(C) + c]) : 0;
+      in0[k] = (NIN >= 1 && c < case_end) ? __ldg(&inputs[c]) : 0;
+      in1[k] = (NIN >= 2 && c < case_end) ? __ldg(&inputs[size_t(C) + c]) : 0;
     }
     // operand vector of one instruction: the kind switch is warp-uniform and
     // taken once per instruction, not once per case
@@ -133,7 +134,7 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
 #pragma unroll
             for (int k = 0; k < K; ++k) {
               const int c = tile + k * 32 + lane;
-              v[k] = c < C ? __ldg(&inputs[size_t(index) * C + c]) : 0;
+              v[k] = c < case_end ? __ldg(&inputs[size_t(index) * C + c]) : 0;
             }
           }
           break;
@@ -248,13 +249,13 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int c = tile + k * 32 + lane;
-      if (c < C) loss += case_loss(s, s.slot_type, acc[k], __ldg(&s.expected[c]), wrong);
+      if (c < case_end) loss += case_loss(s, s.slot_type, acc[k], __ldg(&s.expected[c]), wrong);
     }
   }
   __syncwarp();
   loss_out = loss;
   wrong_out = wrong;
-  ops_out = uint64_t(len) * uint64_t(C);
+  ops_out = uint64_t(len) * uint64_t(case_end - case_begin);
 }
 
 // ------------------------------------------------------------ general VM
