@@ -145,129 +145,189 @@ __device__ inline int lower_reference(const SearchDesc& s, const LRow& t, int32_
 }
 
 // Per-warp shared memory of the accumulator lowering: per-node tables
-// filled by the whole warp, then walked by lane 0.
+// filled and read by the whole warp.
 constexpr uint8_t kLeafOp = 0xff;
-struct LowerFrame { int16_t node; int8_t stage, count, order[3], spilled[3]; int8_t temp_base; };
 struct LowerScratch {
   uint8_t aop[kMaxLowerNodes];    // accumulator op (A_COUNT: not total), kLeafOp for leaves
   uint8_t arity[kMaxLowerNodes];
-  int8_t need[kMaxLowerNodes];    // Sethi-Ullman temporaries of the subtree
+  int8_t need[kMaxLowerNodes];    // Sethi-Ullman temporaries of the subtree (-1: not yet known)
+  uint8_t order[kMaxLowerNodes];  // evaluation order of the non-leaf children: 3 x 2 bits | count << 6
   int16_t end[kMaxLowerNodes];    // one past the subtree
+  int16_t size[kMaxLowerNodes];   // code words of the subtree
+  int16_t start[kMaxLowerNodes];  // open slots before the node, then the subtree's first code word
+  int8_t temp_base[kMaxLowerNodes];
+  uint8_t depth[kMaxLowerNodes];  // non-leaf depth (root 1; 0: not yet placed)
   uint32_t leaf[kMaxLowerNodes];  // leaves: operand kind << 16 | index
-  LowerFrame st[64];
 };
 
-// Subtree ends, needs and code emission of lower_accumulator_warp (one lane).
+// Warp-parallel Sethi-Ullman code generation for lower_accumulator_warp.
+// Same code, failure conditions and temporaries as evaluating the tree with
+// an explicit stack (children in decreasing need, every non-leaf child but
+// the last spilled; a spill past kMaxTemps, code past code_cap or non-leaf
+// nesting past 64 frames fails), but computed with warp scans and
+// level-synchronous sweeps: subtree ends from the open-slot prefix sums,
+// needs and code sizes bottom-up, code positions and temporaries top-down,
+// and every node writing its own instructions.  All lanes return the same.
 __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code, int code_cap, int* temps_out) {
-  // child positions and Sethi-Ullman temporaries, children after parents
-  for (int i = n - 1; i >= 0; --i) {
-    const int a = m.arity[i];
-    if (a == 0) { m.end[i] = int16_t(i + 1); m.need[i] = 0; continue; }
-    int c = i + 1, needs[3], nonleaf = 0;
-    for (int k = 0; k < a; ++k) {
-      if (c >= n) return -1;
-      if (m.end[c] - c > 1) needs[nonleaf++] = m.need[c];
-      c = m.end[c];
+  const int lane = threadIdx.x & 31;
+  // open slots before node i: 1 + sum over earlier nodes of (arity - 1)
+  int carry = 1;
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    const int v = i < n ? int(m.arity[i]) - 1 : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
     }
-    m.end[i] = int16_t(c);
-    // temporaries: non-leaf children by decreasing need, all but the last spilled
-    for (int x = 0; x < nonleaf; ++x)
-      for (int y = x + 1; y < nonleaf; ++y)
-        if (needs[y] > needs[x]) { const int tmp = needs[x]; needs[x] = needs[y]; needs[y] = tmp; }
-    int mx = 0;
-    for (int x = 0; x < nonleaf; ++x) mx = max(mx, needs[x] + x);
-    m.need[i] = int8_t(min(mx, 127));
+    if (i < n) m.start[i] = int16_t(carry + incl - v);
+    carry += __shfl_sync(kFull, incl, 31);
   }
-  if (m.end[0] != n) return -1;
-  if (m.need[0] > kMaxTemps) return -1;
-  *temps_out = m.need[0];
-  int sp = 0, len = 0, temp_top = 0;
-  auto put = [&](uint2 x) -> bool { if (len >= code_cap) return false; code[len++] = x; return true; };
-  auto leaf_kind = [&](int i) -> uint32_t { return m.leaf[i] >> 16; };
-  auto leaf_index = [&](int i) -> uint32_t { return m.leaf[i] & 0xffffu; };
-  if (m.end[0] == 1) {  // a leaf root
-    if (!put(a_instr(A_MOV, false, leaf_kind(0), leaf_index(0)))) return -1;
-    return len;
+  __syncwarp();
+  // a subtree ends at the first later node with fewer open slots
+  for (int i = lane; i < n; i += 32) {
+    const int r = m.start[i];
+    int j = i + 1;
+    while (j < n && m.start[j] >= r) ++j;
+    m.end[i] = int16_t(j);
   }
-  auto child_at = [&](int nd, int x) -> int {
-    int c = nd + 1;
+  __syncwarp();
+  if (carry != 0 || m.end[0] != n) return -1;
+  auto child = [&](int i, int x) -> int {
+    int c = i + 1;
     for (int k = 0; k < x; ++k) c = m.end[c];
     return c;
   };
-  auto push = [&](int nd) -> bool {
-    if (sp >= 64) return false;
-    LowerFrame& f = m.st[sp++];
-    f.node = int16_t(nd);
-    f.stage = 0;
-    f.temp_base = int8_t(temp_top);
-    // non-leaf children in evaluation order (decreasing need, stable)
-    const int a = m.arity[nd];
-    int8_t kids[3];
-    int c = nd + 1;
-    for (int x = 0; x < a; ++x) { kids[x] = int8_t(c - nd); c = m.end[c]; }
-    int count = 0;
-    for (int x = 0; x < a; ++x) {
-      const int ch = nd + kids[x];
-      if (m.end[ch] - ch > 1) f.order[count++] = int8_t(x);
-    }
-    f.count = int8_t(count);
-    for (int x = 0; x < count; ++x)
-      for (int y = x + 1; y < count; ++y) {
-        const int cx = nd + kids[f.order[x]], cy = nd + kids[f.order[y]];
-        if (m.need[cy] > m.need[cx]) { const int8_t tmp = f.order[x]; f.order[x] = f.order[y]; f.order[y] = tmp; }
-      }
-    for (int x = 0; x < 3; ++x) f.spilled[x] = -1;
-    return true;
-  };
-  if (!push(0)) return -1;
-  while (sp) {
-    LowerFrame& f = m.st[sp - 1];
-    const int nd = f.node;
-    if (f.stage < f.count) {
-      // before evaluating the next non-leaf child, spill the previous one
-      if (f.stage > 0) {
-        const int prev = f.order[f.stage - 1];
-        if (temp_top >= kMaxTemps) return -1;
-        f.spilled[prev] = int8_t(temp_top);
-        if (!put(a_instr(A_SPILL, false, K_TEMP, uint32_t(temp_top)))) return -1;
-        ++temp_top;
-      }
-      const int child = child_at(nd, f.order[f.stage]);
-      ++f.stage;
-      if (!push(child)) return -1;
-      continue;
-    }
-    // all non-leaf children evaluated: the last one (if any) is in ACC
-    const uint32_t op = m.aop[nd];
-    const int a = m.arity[nd];
-    uint32_t kind[3] = {K_ACC, K_ACC, K_ACC}, idx[3] = {0, 0, 0};
-    const int last = f.count ? f.order[f.count - 1] : -1;
-    for (int x = 0; x < a; ++x) {
-      const int ch = child_at(nd, x);
-      if (m.end[ch] - ch == 1) { kind[x] = leaf_kind(ch); idx[x] = leaf_index(ch); }
-      else if (x == last) { kind[x] = K_ACC; }
-      else { kind[x] = K_TEMP; idx[x] = uint32_t(f.spilled[x]); }
-    }
-    bool ok = true;
-    if (a == 1) {
-      if (kind[0] != K_ACC) ok = put(a_instr(A_MOV, false, kind[0], idx[0]));
-      ok = ok && put(a_instr(op, false, K_ACC, 0));
-    } else if (a == 2) {
-      if (kind[0] != K_ACC && kind[1] != K_ACC) {
-        ok = put(a_instr(A_MOV, false, kind[0], idx[0])) && put(a_instr(op, false, kind[1], idx[1]));
-      } else if (kind[0] == K_ACC) {
-        ok = put(a_instr(op, false, kind[1], idx[1]));
-      } else {
-        ok = put(a_instr(op, true, kind[0], idx[0]));  // acc = op(first, acc)
-      }
-    } else {
-      ok = put(a_instr(A_SELECT, false, kind[0], idx[0], kind[1], idx[1], kind[2], idx[2]));
-    }
-    if (!ok) return -1;
-    temp_top = f.temp_base;
-    --sp;
+  // ---- bottom-up: need, size, evaluation order
+  uint32_t pend = 0;  // bit k: node lane + 32 k not yet computed
+  for (int k = 0; lane + 32 * k < n; ++k) {
+    const int i = lane + 32 * k;
+    m.depth[i] = 0;
+    if (m.arity[i] == 0) { m.need[i] = 0; m.size[i] = 0; }
+    else { m.need[i] = -1; pend |= 1u << k; }
   }
-  return len;
+  __syncwarp();
+  bool fail = false;
+  while (__any_sync(kFull, pend != 0)) {
+    uint32_t ready = 0;
+    for (uint32_t b = pend; b; b &= b - 1) {
+      const int k = __ffs(b) - 1, i = lane + 32 * k, a = m.arity[i];
+      bool ok = true;
+      for (int x = 0, c = i + 1; x < a; ++x) {
+        if (c >= n) { ok = false; fail = true; break; }
+        ok &= m.need[c] >= 0;
+        c = m.end[c];
+      }
+      if (ok) ready |= 1u << k;
+    }
+    __syncwarp();
+    if (!__any_sync(kFull, ready != 0) || __any_sync(kFull, fail)) { fail = true; break; }
+    for (uint32_t b = ready; b; b &= b - 1) {
+      const int k = __ffs(b) - 1, i = lane + 32 * k, a = m.arity[i];
+      int needs[3], idx[3], nonleaf = 0, sz = 0;
+      for (int x = 0, c = i + 1; x < a; ++x) {
+        if (m.end[c] - c > 1) { needs[nonleaf] = m.need[c]; idx[nonleaf] = x; ++nonleaf; sz += m.size[c]; }
+        c = m.end[c];
+      }
+      // the explicit-stack evaluator's exchange sort by decreasing need
+      for (int x = 0; x < nonleaf; ++x)
+        for (int y = x + 1; y < nonleaf; ++y)
+          if (needs[y] > needs[x]) {
+            const int tn = needs[x]; needs[x] = needs[y]; needs[y] = tn;
+            const int ti = idx[x]; idx[x] = idx[y]; idx[y] = ti;
+          }
+      int mx = 0;
+      for (int x = 0; x < nonleaf; ++x) mx = max(mx, needs[x] + x);
+      // own words: unary MOV + op when its child is a leaf; binary MOV + op
+      // when both children are leaves; otherwise one word
+      const bool leaf0 = m.end[i + 1] - (i + 1) == 1;
+      const int own = a == 1 ? (leaf0 ? 2 : 1) : a == 2 ? (nonleaf == 0 ? 2 : 1) : 1;
+      m.size[i] = int16_t(min(sz + max(nonleaf - 1, 0) + own, 32767));
+      m.order[i] = uint8_t((nonleaf << 6) | (nonleaf > 0 ? idx[0] : 0) | (nonleaf > 1 ? idx[1] << 2 : 0) |
+                           (nonleaf > 2 ? idx[2] << 4 : 0));
+      m.need[i] = int8_t(min(mx, 127));
+    }
+    pend &= ~ready;
+    __syncwarp();
+  }
+  if (__any_sync(kFull, fail)) return -1;
+  if (m.need[0] > kMaxTemps) return -1;
+  *temps_out = m.need[0];
+  if (m.end[0] == 1) {  // a leaf root
+    if (code_cap < 1) return -1;
+    if (lane == 0) code[0] = a_instr(A_MOV, false, m.leaf[0] >> 16, m.leaf[0] & 0xffffu);
+    __syncwarp();
+    return 1;
+  }
+  const int total = m.size[0];
+  if (total > code_cap) return -1;
+  // ---- top-down: code positions, temporaries and depth; each node writes its words
+  pend = 0;
+  for (int k = 0; lane + 32 * k < n; ++k)
+    if (m.arity[lane + 32 * k]) pend |= 1u << k;
+  if (lane == 0) { m.start[0] = 0; m.temp_base[0] = 0; m.depth[0] = 1; }
+  __syncwarp();
+  while (__any_sync(kFull, pend != 0)) {
+    uint32_t ready = 0;
+    for (uint32_t b = pend; b; b &= b - 1) {
+      const int k = __ffs(b) - 1;
+      if (m.depth[lane + 32 * k]) ready |= 1u << k;
+    }
+    __syncwarp();
+    if (!__any_sync(kFull, ready != 0)) { fail = true; break; }
+    for (uint32_t b = ready; b; b &= b - 1) {
+      const int k = __ffs(b) - 1, i = lane + 32 * k, a = m.arity[i];
+      if (m.depth[i] >= 65) fail = true;  // the 65th nested frame overflows the 64-frame stack
+      const int count = m.order[i] >> 6, tb = m.temp_base[i];
+      int pos = m.start[i];
+      int ord[3] = {m.order[i] & 3, (m.order[i] >> 2) & 3, (m.order[i] >> 4) & 3};
+      for (int q = 0; q < count; ++q) {
+        const int c = child(i, ord[q]);
+        if (q > 0) {
+          const int temp = tb + q - 1;
+          if (temp >= kMaxTemps) fail = true;
+          else code[pos] = a_instr(A_SPILL, false, K_TEMP, uint32_t(temp));
+          ++pos;
+        }
+        m.start[c] = int16_t(pos);
+        m.temp_base[c] = int8_t(tb + q);
+        m.depth[c] = uint8_t(min(int(m.depth[i]) + 1, 255));
+        pos += m.size[c];
+      }
+      const uint32_t op = m.aop[i];
+      uint32_t kind[3] = {K_ACC, K_ACC, K_ACC}, id[3] = {0, 0, 0};
+      const int last = count ? ord[count - 1] : -1;
+      for (int x = 0; x < a; ++x) {
+        const int c = child(i, x);
+        if (m.end[c] - c == 1) { kind[x] = m.leaf[c] >> 16; id[x] = m.leaf[c] & 0xffffu; }
+        else if (x == last) { kind[x] = K_ACC; }
+        else {
+          kind[x] = K_TEMP;
+          for (int q = 0; q < count - 1; ++q)
+            if (ord[q] == x) id[x] = uint32_t(tb + q);
+        }
+      }
+      if (a == 1) {
+        if (kind[0] != K_ACC) code[pos++] = a_instr(A_MOV, false, kind[0], id[0]);
+        code[pos] = a_instr(op, false, K_ACC, 0);
+      } else if (a == 2) {
+        if (kind[0] != K_ACC && kind[1] != K_ACC) {
+          code[pos++] = a_instr(A_MOV, false, kind[0], id[0]);
+          code[pos] = a_instr(op, false, kind[1], id[1]);
+        } else if (kind[0] == K_ACC) {
+          code[pos] = a_instr(op, false, kind[1], id[1]);
+        } else {
+          code[pos] = a_instr(op, true, kind[0], id[0]);  // acc = op(first, acc)
+        }
+      } else {
+        code[pos] = a_instr(A_SELECT, false, kind[0], id[0], kind[1], id[1], kind[2], id[2]);
+      }
+    }
+    pend &= ~ready;
+    __syncwarp();
+  }
+  if (__any_sync(kFull, fail)) return -1;
+  return total;
 }
 
 __device__ __forceinline__ uint32_t accumulator_op_of(int node_kind, int opcode, int operand) {
@@ -306,8 +366,7 @@ __device__ __forceinline__ uint32_t accumulator_op_of(int node_kind, int opcode,
 // (the same on every lane), or -1 when the row needs the general VM.
 // *temps_out: temporaries used.  The lanes classify the nodes, number the
 // constants, copy the constant pool and bound the bytecode length in
-// parallel; lane 0 then computes subtree ends and Sethi-Ullman needs and
-// emits the code, reading only shared memory.
+// parallel, then emit the code together (lower_accumulator_emit).
 __device__ inline int lower_accumulator_warp(const SearchDesc& s, const uint64_t* node, int n, const int64_t* cval,
                                              int nc, uint2* code, int code_cap, int64_t* kpool, LowerScratch& m,
                                              int* temps_out) {
@@ -346,10 +405,7 @@ __device__ inline int lower_accumulator_warp(const SearchDesc& s, const uint64_t
   __syncwarp();
   // the exact bytecode length (a bound of every executed path) must fit the fuel
   if (!total || bytecode > s.fuel) return -1;
-  int len = -1;
-  if (lane == 0) len = lower_accumulator_emit(m, n, code, code_cap, temps_out);
-  __syncwarp();
-  return __shfl_sync(kFull, len, 0);
+  return lower_accumulator_emit(m, n, code, code_cap, temps_out);
 }
 
 }  // namespace gb
