@@ -895,7 +895,10 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     int32_t* counts = e->d_counts + 4 * c;
     {
       Timed t(e, KN_VARY, st);
-      const int blocks = std::min(blocks_for(hi - lo, warps), std::max(1, per_sm) * e->sm_count);
+      // each range gets its share of the GPU, so that all ranges start at once
+      // and the slowest children of every range overlap one another
+      const int share = std::max(1, std::max(1, per_sm) * e->sm_count / chunks);
+      const int blocks = std::min(blocks_for(hi - lo, warps), share);
       gb::k_vary<<<blocks, warps * 32, vary_smem, st>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, counts + 2, lo,
                                                         hi);
     }
