@@ -703,7 +703,12 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
             }
         }
         pending &= ~ready;
-        atomicAdd(&ready_count[level & 1], __popc(ready));
+      }
+      {
+        // one shared-memory atomic per warp, not per thread
+        int placed_here = __popc(ready);
+        for (int o = 16; o; o >>= 1) placed_here += __shfl_xor_sync(kFull, placed_here, o);
+        if ((tid & 31) == 0 && placed_here) atomicAdd(&ready_count[level & 1], placed_here);
       }
       if (tid == 0) ready_count[(level + 1) & 1] = 0;  // read by every thread before this level's first barrier
       __syncthreads();
