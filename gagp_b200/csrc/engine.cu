@@ -77,9 +77,6 @@ struct gagp_engine {
   static constexpr int kChunks = 8;
   cudaStream_t chunk_stream[kChunks] = {};
   cudaEvent_t chunk_fork = nullptr, chunk_done[kChunks] = {};
-  // a range's general-VM programs run beside its fast-VM programs
-  cudaStream_t general_stream[kChunks] = {};
-  cudaEvent_t lowered[kChunks] = {}, general_done[kChunks] = {};
   std::map<int, std::unique_ptr<Search>> searches;
   int next_id = 1;
   uint64_t arena_limit = 0, arena_used = 0;
@@ -451,9 +448,6 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   for (int c = 0; c < gagp_engine::kChunks; ++c) {
     CUDA_TRY(cudaStreamCreateWithFlags(&e->chunk_stream[c], cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&e->chunk_done[c], cudaEventDisableTiming));
-    CUDA_TRY(cudaStreamCreateWithFlags(&e->general_stream[c], cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&e->lowered[c], cudaEventDisableTiming));
-    CUDA_TRY(cudaEventCreateWithFlags(&e->general_done[c], cudaEventDisableTiming));
   }
   cudaDeviceProp prop;
   CUDA_TRY(cudaGetDeviceProperties(&prop, device));
@@ -504,9 +498,6 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   for (int c = 0; c < gagp_engine::kChunks; ++c) {
     if (e->chunk_stream[c]) cudaStreamDestroy(e->chunk_stream[c]);
     if (e->chunk_done[c]) cudaEventDestroy(e->chunk_done[c]);
-    if (e->general_stream[c]) cudaStreamDestroy(e->general_stream[c]);
-    if (e->lowered[c]) cudaEventDestroy(e->lowered[c]);
-    if (e->general_done[c]) cudaEventDestroy(e->general_done[c]);
   }
   delete e;
 }
@@ -827,8 +818,7 @@ VmPlan plan_vm(gagp_engine* e, const BatchView& v, bool may_measure) {
 }
 
 gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t stream, const gb::ProgramRef* fast,
-                      const gb::ProgramRef* general, const int32_t* counts, const VmPlan& plan,
-                      cudaStream_t general_on = nullptr) {
+                      const gb::ProgramRef* general, const int32_t* counts, const VmPlan& plan) {
   const int warps = 8;
   const int temp_stride = gb::kMaxTemps * plan.lanes * 32;
   const int code_stride = (v.max_code_stride + 1) & ~1;  // uint2 slots, in int64 units
@@ -858,9 +848,8 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
     ++e->vm_tune[plan.measure_key].pending;
   }
   {
-    cudaStream_t gs = general_on ? general_on : stream;
-    Timed t(e, KN_VM_GENERAL, gs);
-    gb::k_vm_general<<<e->sm_count * 4, 128, 0, gs>>>(v.d_desc, mode, general, counts + 1);
+    Timed t(e, KN_VM_GENERAL, stream);
+    gb::k_vm_general<<<e->sm_count * 4, 128, 0, stream>>>(v.d_desc, mode, general, counts + 1);
   }
   return GAGP_OK;
 }
@@ -918,18 +907,10 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
       gb::k_lower<<<blocks_for(hi - lo, gb::kLowerWarps), gb::kLowerWarps * 32, 0, st>>>(
           v.d_desc, v.d_child_off, v.n, 1, e->d_fast + lo, e->d_general + lo, counts, lo, hi);
     }
-    cudaStream_t gs = nullptr;
-    if (chunks > 1) {
-      gs = e->general_stream[c];
-      CUDA_TRY(cudaEventRecord(e->lowered[c], st));
-      CUDA_TRY(cudaStreamWaitEvent(gs, e->lowered[c], 0));
-    }
-    launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts, vm, gs);
+    launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts, vm);
     if (chunks > 1) {
       CUDA_TRY(cudaEventRecord(e->chunk_done[c], st));
-      CUDA_TRY(cudaEventRecord(e->general_done[c], gs));
       CUDA_TRY(cudaStreamWaitEvent(e->stream, e->chunk_done[c], 0));
-      CUDA_TRY(cudaStreamWaitEvent(e->stream, e->general_done[c], 0));
     }
   }
   { Timed t(e, KN_CHILD); gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
