@@ -107,6 +107,9 @@ struct gagp_engine {
   // stream-ordered pool of the searches' device blocks: admission and
   // retirement neither allocate from the driver nor synchronize the device
   cudaMemPool_t pool = nullptr;
+  // pinned staging of result downloads (grown on demand)
+  char* pinned = nullptr;
+  size_t pinned_bytes = 0;
   // VM autotuner: per batch shape, the fast VM's cases per lane, chosen by
   // timing each candidate on live rounds (results do not depend on it)
   struct VmTune {
@@ -483,6 +486,7 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   }
   cudaStreamSynchronize(e->stream);
   if (e->pool) cudaMemPoolDestroy(e->pool);
+  if (e->pinned) cudaFreeHost(e->pinned);
   cudaFree(e->d_fast);
   cudaFree(e->d_general);
   cudaFree(e->d_counts);
@@ -1493,21 +1497,54 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   if (!round[2]) return fail(GAGP_NOT_READY, "search has not finished");
   const int H = std::min(round[1], out->generations);
   const int P = s->P, S = s->stride;
-  std::vector<int64_t> sum(H);
-  std::vector<double> hf(H);
-  std::vector<uint32_t> hw(H), hn(H);
-  std::vector<uint64_t> hnode(size_t(H) * S);
-  std::vector<int64_t> hc(size_t(H) * S);
-  std::vector<int32_t> hl(H);
-  if (H) {
-    CUDA_TRY(copy_d2h(e, sum.data(), d.hist_sum, 8 * H));
-    CUDA_TRY(copy_d2h(e, hf.data(), d.hist_fitness, 8 * H));
-    CUDA_TRY(copy_d2h(e, hw.data(), d.hist_wrong, 4 * H));
-    CUDA_TRY(copy_d2h(e, hn.data(), d.hist_nodes, 4 * H));
-    CUDA_TRY(copy_d2h(e, hnode.data(), d.hist_node, 8 * size_t(H) * S));
-    CUDA_TRY(copy_d2h(e, hc.data(), d.hist_cval, 8 * size_t(H) * S));
-    CUDA_TRY(copy_d2h(e, hl.data(), d.hist_len, 4 * H));
+  // every array in one pinned staging area, copied asynchronously, one sync
+  Layout L;
+  const size_t o_sum = L.take(8 * size_t(H)), o_hf = L.take(8 * size_t(H)), o_hw = L.take(4 * size_t(H)),
+               o_hn = L.take(4 * size_t(H)), o_hnode = L.take(8 * size_t(H) * S), o_hc = L.take(8 * size_t(H) * S),
+               o_hl = L.take(4 * size_t(H)), o_fit = L.take(8 * size_t(P)), o_wr = L.take(4 * size_t(P)),
+               o_key = L.take(8 * size_t(P)), o_node = L.take(8 * size_t(P) * S), o_cv = L.take(8 * size_t(P) * S),
+               o_len = L.take(4 * size_t(P)), o_cnt = L.take(8 * 4);
+  if (L.total > e->pinned_bytes) {
+    if (e->pinned) cudaFreeHost(e->pinned);
+    e->pinned = nullptr;
+    e->pinned_bytes = 0;
+    CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&e->pinned), L.total));
+    e->pinned_bytes = L.total;
   }
+  char* hb = e->pinned;
+  auto fetch = [&](size_t off, const void* src, size_t bytes) -> cudaError_t {
+    e->d2h_bytes += bytes;
+    return bytes ? cudaMemcpyAsync(hb + off, src, bytes, cudaMemcpyDeviceToHost, e->stream) : cudaSuccess;
+  };
+  CUDA_TRY(fetch(o_sum, d.hist_sum, 8 * size_t(H)));
+  CUDA_TRY(fetch(o_hf, d.hist_fitness, 8 * size_t(H)));
+  CUDA_TRY(fetch(o_hw, d.hist_wrong, 4 * size_t(H)));
+  CUDA_TRY(fetch(o_hn, d.hist_nodes, 4 * size_t(H)));
+  CUDA_TRY(fetch(o_hnode, d.hist_node, 8 * size_t(H) * S));
+  CUDA_TRY(fetch(o_hc, d.hist_cval, 8 * size_t(H) * S));
+  CUDA_TRY(fetch(o_hl, d.hist_len, 4 * size_t(H)));
+  CUDA_TRY(fetch(o_fit, d.fitness, 8 * size_t(P)));
+  CUDA_TRY(fetch(o_wr, d.wrong, 4 * size_t(P)));
+  CUDA_TRY(fetch(o_key, d.key, 8 * size_t(P)));
+  CUDA_TRY(fetch(o_node, d.node, 8 * size_t(P) * S));
+  CUDA_TRY(fetch(o_cv, d.cval, 8 * size_t(P) * S));
+  CUDA_TRY(fetch(o_len, d.len, 4 * size_t(P)));
+  CUDA_TRY(fetch(o_cnt, d.counters, 8 * 4));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  const int64_t* sum = reinterpret_cast<const int64_t*>(hb + o_sum);
+  const double* hf = reinterpret_cast<const double*>(hb + o_hf);
+  const uint32_t* hw = reinterpret_cast<const uint32_t*>(hb + o_hw);
+  const uint32_t* hn = reinterpret_cast<const uint32_t*>(hb + o_hn);
+  const uint64_t* hnode = reinterpret_cast<const uint64_t*>(hb + o_hnode);
+  const int64_t* hc = reinterpret_cast<const int64_t*>(hb + o_hc);
+  const int32_t* hl = reinterpret_cast<const int32_t*>(hb + o_hl);
+  const double* fit = reinterpret_cast<const double*>(hb + o_fit);
+  const uint32_t* wr = reinterpret_cast<const uint32_t*>(hb + o_wr);
+  const uint64_t* key = reinterpret_cast<const uint64_t*>(hb + o_key);
+  const uint64_t* node = reinterpret_cast<const uint64_t*>(hb + o_node);
+  const int64_t* cv = reinterpret_cast<const int64_t*>(hb + o_cv);
+  const int32_t* len = reinterpret_cast<const int32_t*>(hb + o_len);
+  const uint64_t* counters = reinterpret_cast<const uint64_t*>(hb + o_cnt);
   auto put_row = [&](const gagp_rows& rows, int index, const uint64_t* node, const int64_t* cval, int32_t l) {
     const int n = l & 0xffff, nc = (l >> 16) & 0xffff;
     rows.node_counts[index] = n;
@@ -1521,21 +1558,9 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
     out->history_mean_fitness[h] = double((long double)sum[h] / (long double)P);
     out->history_best_wrong[h] = s->has_wrong ? int32_t(hw[h]) : -1;
     out->history_best_nodes[h] = int32_t(hn[h]);
-    put_row(out->history_best, h, hnode.data() + size_t(h) * S, hc.data() + size_t(h) * S, hl[h]);
+    put_row(out->history_best, h, hnode + size_t(h) * S, hc + size_t(h) * S, hl[h]);
   }
   out->generations = H;
-  std::vector<double> fit(P);
-  std::vector<uint32_t> wr(P);
-  std::vector<uint64_t> node(size_t(P) * S);
-  std::vector<uint64_t> key(P);
-  std::vector<int64_t> cv(size_t(P) * S);
-  std::vector<int32_t> len(P);
-  CUDA_TRY(copy_d2h(e, fit.data(), d.fitness, 8 * size_t(P)));
-  CUDA_TRY(copy_d2h(e, wr.data(), d.wrong, 4 * size_t(P)));
-  CUDA_TRY(copy_d2h(e, key.data(), d.key, 8 * size_t(P)));
-  CUDA_TRY(copy_d2h(e, node.data(), d.node, 8 * size_t(P) * S));
-  CUDA_TRY(copy_d2h(e, cv.data(), d.cval, 8 * size_t(P) * S));
-  CUDA_TRY(copy_d2h(e, len.data(), d.len, 4 * size_t(P)));
   std::vector<int> order(P);
   std::iota(order.begin(), order.end(), 0);
   std::sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
@@ -1545,11 +1570,9 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
     out->final_fitness[r] = fit[m];
     out->final_wrong[r] = s->has_wrong ? int32_t(wr[m]) : -1;
     out->final_nodes[r] = s->fixed_nodes + (len[m] & 0xffff);
-    put_row(out->final_rows, r, node.data() + size_t(m) * S, cv.data() + size_t(m) * S, len[m]);
+    put_row(out->final_rows, r, node + size_t(m) * S, cv + size_t(m) * S, len[m]);
   }
   out->population = n_out;
-  uint64_t counters[4];
-  CUDA_TRY(copy_d2h(e, counters, d.counters, sizeof(counters)));
   out->evaluated_programs = counters[0];
   out->reused_programs = counters[1];
   out->program_cases = counters[2];
