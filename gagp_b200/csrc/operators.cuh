@@ -52,11 +52,29 @@ __device__ inline WarpRows carve_rows(char* base, int stride) {
   return r;
 }
 
-__device__ inline void load_member(const SearchDesc& s, int m, SRow& to) {
-  const int32_t l = s.len[m];
-  to.n = len_nodes(l);
-  to.nc = len_consts(l);
-  warp_copy(s.node + size_t(m) * s.stride, s.cval + size_t(m) * s.stride, to.n, to.nc, to.node, to.cval);
+// The parent's and the donor's rows into shared memory, their loads in
+// flight together.
+__device__ inline void load_members(const SearchDesc& s, int a, SRow& to_a, int b, SRow& to_b) {
+  const int32_t la = s.len[a], lb = s.len[b];
+  to_a.n = len_nodes(la);
+  to_a.nc = len_consts(la);
+  to_b.n = len_nodes(lb);
+  to_b.nc = len_consts(lb);
+  const uint64_t* na = s.node + size_t(a) * s.stride;
+  const uint64_t* nb = s.node + size_t(b) * s.stride;
+  const int64_t* ca = s.cval + size_t(a) * s.stride;
+  const int64_t* cb = s.cval + size_t(b) * s.stride;
+  const int n = max(max(to_a.n, to_b.n), max(to_a.nc, to_b.nc));
+  for (int i = lane_id(); i < n; i += 32) {
+    const bool na_ok = i < to_a.n, nb_ok = i < to_b.n, ca_ok = i < to_a.nc, cb_ok = i < to_b.nc;
+    const uint64_t x = na_ok ? na[i] : 0, y = nb_ok ? nb[i] : 0;
+    const int64_t u = ca_ok ? ca[i] : 0, v = cb_ok ? cb[i] : 0;
+    if (na_ok) to_a.node[i] = x;
+    if (nb_ok) to_b.node[i] = y;
+    if (ca_ok) to_a.cval[i] = u;
+    if (cb_ok) to_b.cval[i] = v;
+  }
+  __syncwarp();
 }
 
 // One child, by one warp.  Writes the child row, its parent and reuse
@@ -72,8 +90,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
   Rng random(seed ^ (0x617089e168ULL + uint64_t(child)));
   const int parent = tournament(s, random), donor = tournament(s, random);
   *parent_out = parent;
-  load_member(s, parent, w.parent);
-  load_member(s, donor, w.donor);
+  load_members(s, parent, w.parent, donor, w.donor);
   stamp[0] = clock64();
   if (w.parent.n <= 0 || w.parent.n > s.maxv || w.parent.nc > w.parent.n) return 1;
   warp_copy(w.parent.node, w.parent.cval, w.parent.n, w.parent.nc, w.child.node, w.child.cval);
