@@ -358,7 +358,8 @@ struct Plan {
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
   size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_consts;
-  size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, round, hist_sum, hist_fitness, hist_wrong,
+  size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, round, hist_sum, hist_fitness,
+      hist_wrong,
       hist_nodes, hist_node, hist_cval, hist_len, counters;
   int stride, code_stride, bc_stride, stream_capacity, slots;
 };
@@ -415,6 +416,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.mt = L.take(8 * 312); p.stream = L.take(8 * size_t(p.stream_capacity));
   p.stream_mod = L.take(4 * size_t(p.stream_capacity)); p.stream_head = L.take(16);
   p.round_seed = L.take(8); p.best = L.take(4); p.placed = L.take(4 * size_t(P)); p.round = L.take(16);
+  p.place_state = L.take(4);
   const size_t H = size_t(cfg->generations);
   p.hist_sum = L.take(8 * H); p.hist_fitness = L.take(8 * H); p.hist_wrong = L.take(4 * H);
   p.hist_nodes = L.take(4 * H); p.hist_node = L.take(8 * S * H); p.hist_cval = L.take(8 * S * H);
@@ -668,6 +670,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.bounded_threshold = (0 - uint64_t(s->P)) % uint64_t(s->P);
   d.round_seed = at<uint64_t>(b, p.round_seed);
   d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
+  d.place_state = at<int32_t>(b, p.place_state);
   d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
   d.hist_wrong = at<uint32_t>(b, p.hist_wrong); d.hist_nodes = at<uint32_t>(b, p.hist_nodes);
   d.hist_node = at<uint64_t>(b, p.hist_node); d.hist_cval = at<int64_t>(b, p.hist_cval);
@@ -927,7 +930,11 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
                    std::max(size_t(v.max_P) * sizeof(int32_t) + 64, size_t(v.max_draws + 64) * sizeof(uint16_t));
     bytes = std::min(bytes, limit);
     CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join, 0));
-    gb::k_place<<<v.n, gb::kPlaceThreads, bytes, e->stream>>>(v.d_desc, v.n, int(bytes));
+    // the cluster placement first; the single-block kernel replays what it could not place
+    const int local_P = (v.max_P + gb::kPlaceCtas - 1) / gb::kPlaceCtas;
+    const size_t cluster_bytes = size_t(local_P + 2) * (sizeof(uint64_t) + sizeof(int32_t)) + 16;
+    gb::k_place_cluster<<<v.n * gb::kPlaceCtas, gb::kClusterThreads, cluster_bytes, e->stream>>>(v.d_desc, v.n);
+    gb::k_place<<<v.n, gb::kPlaceThreads, bytes, e->stream>>>(v.d_desc, v.n, int(bytes), 1);
   }
   { Timed t(e, KN_COMMIT); gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));

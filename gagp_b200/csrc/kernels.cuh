@@ -8,10 +8,14 @@
 //   k_record (epoch start) -> k_vary -> k_lower -> k_vm_fast / k_vm_general
 //   -> k_child_results -> k_place -> k_commit
 #pragma once
+#include <cooperative_groups.h>
+
 #include "operators.cuh"
 #include "vm.cuh"
 
 namespace gb {
+
+namespace cg = cooperative_groups;
 
 struct ProgramRef {
   int32_t search, slot;
@@ -578,7 +582,10 @@ constexpr int kPlaceThreads = 1024;
 __device__ __forceinline__ bool key_before(uint64_t ka, int va, uint64_t kb, int vb) {
   return ka < kb || (ka == kb && va < vb);
 }
-__global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* descs, int n, int dyn_bytes) {
+// after_cluster: the cluster placement ran first; return if it placed the
+// round, else replay it on the exact windowed path.
+__global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* descs, int n, int dyn_bytes,
+                                                            int after_cluster) {
   extern __shared__ __align__(16) uint64_t keys[];
   __shared__ uint64_t mt[312], nw[312];
   __shared__ uint64_t ck_stage[1024];
@@ -588,6 +595,7 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
   __shared__ int shared_best, shared_fail, ready_count[2], redraw_at;
   const SearchDesc& s = descs[blockIdx.x];
   if (!search_live(s)) return;
+  if (after_cluster && *s.place_state) return;
   const long long t0 = clock64();
   const int P = s.P, B = s.B, rs = s.replacement_size, cap = s.stream_capacity;
   const int tid = threadIdx.x;
@@ -611,7 +619,7 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
   // owner area after the keys, 16-byte aligned, with 64 bytes of slack for
   // the per-thread 16-byte reads of the staged draws
   int32_t* owner = reinterpret_cast<int32_t*>(keys + P + (P & 1));
-  const bool parallel_path = rs == 2 && blockDim.x == kPlaceThreads && B <= kPlaceThreads * kPerThread &&
+  const bool parallel_path = !after_cluster && rs == 2 && blockDim.x == kPlaceThreads && B <= kPlaceThreads * kPerThread &&
                              wp - rp >= need &&
                              dyn_bytes >= int(sizeof(uint64_t)) * (P + 1) + int(sizeof(int32_t)) * P + 64;
   bool parallel_done = false;
@@ -973,6 +981,226 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
     atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[4]), (unsigned long long)(t1 - t0));
     atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[5]), (unsigned long long)(t2 - t1));
     atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[6]), (unsigned long long)(t3 - t2));
+  }
+}
+
+// Cluster placement: the level-parallel placement above, spread over a
+// cluster of kPlaceCtas blocks that share their shared memory.  Member m
+// lives in block m % kPlaceCtas (its key and level owner); thread g of the
+// cluster owns children [2g, 2g + 2), so the blocks hold the children in
+// order.  Each level is two cluster barriers: level-tagged atomicMin on the
+// owning block's owner word, then the ready children place (remote key
+// reads and writes).  The running best before each child is a scan inside
+// each block plus a prefix over the blocks' totals.  When a child would have
+// redrawn, or the stream holds too few draws, or the replacement size is not
+// 2, nothing is written back: place_state stays 0 and k_place replays the
+// round on the exact path.  On success this kernel finishes the round as
+// k_place does (statistics, best member, stream position, next seed).
+constexpr int kPlaceCtas = 8;
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterPer = 2;
+__global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThreads, 1)
+    k_place_cluster(const SearchDesc* descs, int n) {
+  extern __shared__ __align__(16) uint64_t cl_keys[];
+  __shared__ uint64_t scan_key[32];
+  __shared__ int scan_idx[32];
+  __shared__ uint64_t cta_key[kPlaceCtas];  // block totals (read from block 0)
+  __shared__ int cta_idx[kPlaceCtas];
+  __shared__ int ready_count[2], redraw_at;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = int(cluster.block_rank());
+  const SearchDesc& s = descs[blockIdx.x / kPlaceCtas];
+  if (!search_live(s)) return;  // the same for every block of the cluster
+  const long long t0 = clock64();
+  const int P = s.P, B = s.B, cap = s.stream_capacity;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long rp = stream_ptrs(s)[0], wp = stream_ptrs(s)[1];
+  if (s.replacement_size != 2 || B > kPlaceCtas * kClusterThreads * kClusterPer || wp - rp < 2LL * B + 1) {
+    if (rank == 0 && tid == 0) *s.place_state = 0;
+    return;  // the same decision in every block
+  }
+  const int local_P = (P + kPlaceCtas - 1) / kPlaceCtas;
+  uint64_t* keys = cl_keys;
+  int32_t* owner = reinterpret_cast<int32_t*>(cl_keys + local_P + (local_P & 1));
+  for (int i = tid; i < local_P; i += blockDim.x) {
+    const int m = i * kPlaceCtas + rank;
+    keys[i] = m < P ? s.key[m] : ~0ULL;
+    owner[i] = 0x7fffffff;
+  }
+  int32_t* __restrict__ placed = s.placed;
+  for (int m = rank * kClusterThreads + tid; m < P; m += kPlaceCtas * kClusterThreads) placed[m] = -1;
+  if (tid == 0) {
+    ready_count[0] = ready_count[1] = 0;
+    redraw_at = 0x7fffffff;
+  }
+  const int begin = (rank * kClusterThreads + tid) * kClusterPer;
+  const int base = int(rp % cap);
+  uint32_t cand[kClusterPer];
+  uint32_t pending = 0;
+#pragma unroll
+  for (int t = 0; t < kClusterPer; ++t) {
+    const int j = begin + t;
+    cand[t] = 0;
+    if (j < B) {
+      int p0 = base + 2 * j, p1 = p0 + 1;
+      if (p0 >= cap) p0 -= cap;
+      if (p1 >= cap) p1 -= cap;
+      cand[t] = s.stream_mod[p0] | (s.stream_mod[p1] << 16);
+      pending |= 1u << t;
+    }
+  }
+  auto owner_at = [&](int m) -> int* { return cluster.map_shared_rank(owner, m % kPlaceCtas) + m / kPlaceCtas; };
+  auto key_at = [&](int m) -> uint64_t* { return cluster.map_shared_rank(keys, m % kPlaceCtas) + m / kPlaceCtas; };
+  int* counter0 = cluster.map_shared_rank(ready_count, 0);
+  const uint64_t* __restrict__ ckey = s.c_key;
+  cluster.sync();
+  const long long level_start = clock64();
+  int left = B, levels_run = 0;
+  for (int level = 0; level <= B; ++level) {
+    ++levels_run;
+    const int tag = (0x7fff - level) << 16;
+#pragma unroll
+    for (int t = 0; t < kClusterPer; ++t)
+      if (pending >> t & 1) {
+        atomicMin(owner_at(int(cand[t] & 0xffff)), tag | (begin + t));
+        atomicMin(owner_at(int(cand[t] >> 16)), tag | (begin + t));
+      }
+    cluster.sync();
+    uint32_t ready = 0;
+#pragma unroll
+    for (int t = 0; t < kClusterPer; ++t)
+      if ((pending >> t & 1) && *owner_at(int(cand[t] & 0xffff)) == (tag | (begin + t)) &&
+          *owner_at(int(cand[t] >> 16)) == (tag | (begin + t)))
+        ready |= 1u << t;
+    uint64_t kv[kClusterPer];
+#pragma unroll
+    for (int t = 0; t < kClusterPer; ++t) kv[t] = (ready >> t & 1) ? ckey[begin + t] : 0;
+#pragma unroll
+    for (int t = 0; t < kClusterPer; ++t)
+      if (ready >> t & 1) {
+        const int d0 = int(cand[t] & 0xffff), d1 = int(cand[t] >> 16);
+        const uint64_t k0 = *key_at(d0), k1 = *key_at(d1);
+        // worst of the pair: the second replaces the first when the first is better
+        const int v = (k0 < k1 || (k0 == k1 && d0 < d1)) ? d1 : d0;
+        *key_at(v) = kv[t];
+        placed[v] = begin + t;
+        cand[t] = uint32_t(v);
+      }
+    pending &= ~ready;
+    int placed_here = __popc(ready);
+    for (int o = 16; o; o >>= 1) placed_here += __shfl_xor_sync(kFull, placed_here, o);
+    if (lane == 0 && placed_here) atomicAdd(counter0 + (level & 1), placed_here);
+    if (rank == 0 && tid == 0) ready_count[(level + 1) & 1] = 0;  // read by every thread before this level's first barrier
+    cluster.sync();
+    left -= counter0[level & 1];
+    if (left == 0) break;
+  }
+  const long long level_end = clock64();
+  // best member before each child: (key, victim) minimum of this thread's
+  // children, a warp scan, a block scan, then the blocks before this one
+  uint64_t mk = ~0ULL;
+  int mv = 0x7fffffff;
+#pragma unroll
+  for (int t = 0; t < kClusterPer; ++t)
+    if (begin + t < B) {
+      const uint64_t k = ckey[begin + t];
+      if (key_before(k, int(cand[t]), mk, mv)) { mk = k; mv = int(cand[t]); }
+    }
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t uk = __shfl_up_sync(kFull, mk, o);
+    const int uv = __shfl_up_sync(kFull, mv, o);
+    if (lane >= o && key_before(uk, uv, mk, mv)) { mk = uk; mv = uv; }
+  }
+  constexpr int kWarps = kClusterThreads / 32;
+  if (lane == 31) { scan_key[warp] = mk; scan_idx[warp] = mv; }
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t wk = lane < kWarps ? scan_key[lane] : ~0ULL;
+    int wv = lane < kWarps ? scan_idx[lane] : 0x7fffffff;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t uk = __shfl_up_sync(kFull, wk, o);
+      const int uv = __shfl_up_sync(kFull, wv, o);
+      if (lane >= o && key_before(uk, uv, wk, wv)) { wk = uk; wv = uv; }
+    }
+    scan_key[lane] = wk;
+    scan_idx[lane] = wv;
+    if (lane == kWarps - 1) {
+      *cluster.map_shared_rank(cta_key + rank, 0) = wk;
+      *cluster.map_shared_rank(cta_idx + rank, 0) = wv;
+    }
+  }
+  cluster.sync();
+  const int best0 = s.best[0];
+  const uint64_t best0_key = s.key[best0];
+  int bv = best0;
+  uint64_t bk = best0_key;
+  {
+    const uint64_t* tot_key = cluster.map_shared_rank(cta_key, 0);
+    const int* tot_idx = cluster.map_shared_rank(cta_idx, 0);
+    for (int r = 0; r < rank; ++r)
+      if (key_before(tot_key[r], tot_idx[r], bk, bv)) { bk = tot_key[r]; bv = tot_idx[r]; }
+    const uint64_t lk = __shfl_up_sync(kFull, mk, 1);
+    const int lv = __shfl_up_sync(kFull, mv, 1);
+    if (lane > 0 && key_before(lk, lv, bk, bv)) { bk = lk; bv = lv; }
+    if (warp > 0 && key_before(scan_key[warp - 1], scan_idx[warp - 1], bk, bv)) {
+      bk = scan_key[warp - 1];
+      bv = scan_idx[warp - 1];
+    }
+  }
+  // a child whose victim is the best member before it would have redrawn
+  int* redraw0 = cluster.map_shared_rank(&redraw_at, 0);
+  bool hit = false;
+#pragma unroll
+  for (int t = 0; t < kClusterPer; ++t)
+    if (!hit && begin + t < B) {
+      const int v = int(cand[t]);
+      if (v == bv) {
+        atomicMin(redraw0, begin + t);
+        hit = true;
+      } else {
+        const uint64_t k = ckey[begin + t];
+        if (key_before(k, v, bk, bv)) { bk = k; bv = v; }
+      }
+    }
+  cluster.sync();
+  const bool done = *redraw0 == 0x7fffffff;
+  if (done) {
+    // this block's members take their child's statistics
+    const double* __restrict__ cfit = s.c_fitness;
+    const uint32_t* __restrict__ cwrong = s.c_wrong;
+    const uint32_t* __restrict__ cnodes = s.c_nodes;
+    for (int i = tid; i < local_P; i += blockDim.x) {
+      const int m = i * kPlaceCtas + rank;
+      if (m >= P) continue;
+      const int c = placed[m];
+      if (c >= 0) {
+        s.key[m] = keys[i];
+        s.fitness[m] = cfit[c];
+        s.wrong[m] = cwrong[c];
+        s.nodes[m] = cnodes[c];
+      }
+    }
+  }
+  if (rank == 0 && tid == 0) {
+    *s.place_state = done ? 1 : 0;
+    if (done) {
+      const uint64_t* tot_key = cta_key;
+      int fv = best0;
+      uint64_t fk = best0_key;
+      for (int r = 0; r < kPlaceCtas; ++r)
+        if (key_before(tot_key[r], cta_idx[r], fk, fv)) { fk = tot_key[r]; fv = cta_idx[r]; }
+      s.best[0] = fv;
+      // the next round's seed: the raw output after the 2B placement draws
+      const long long pos = rp + 2LL * B;
+      s.round_seed[0] = s.stream[pos % cap];
+      stream_ptrs(s)[0] = pos + 1;
+      const int r = s.round[0] + 1;
+      s.round[0] = r;
+      if (r >= s.total_rounds) s.round[2] = 1;
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[5]), (unsigned long long)(clock64() - t0));
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[14]), (unsigned long long)(level_end - level_start));
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[7]), (unsigned long long)levels_run);
+    }
   }
 }
 

@@ -127,6 +127,7 @@ struct SearchDesc {
   // ---- search progress and history
   int32_t* best;                       // tracked best member
   int32_t* placed;                     // P: child placed into member, -1
+  int32_t* place_state;                // 1: the cluster placement placed this round
   int32_t* round;                      // [0] rounds done, [1] history entries, [2] finished flag, [3] error
   int64_t* hist_sum;                   // per history entry: sum of member fitness (integral)
   double* hist_fitness; uint32_t* hist_wrong; uint32_t* hist_nodes;
