@@ -1036,23 +1036,26 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   const int begin = (rank * kClusterThreads + tid) * kClusterPer;
   const int base = int(rp % cap);
   uint32_t cand[kClusterPer];
+  uint64_t kv[kClusterPer];  // the children's keys
   uint32_t pending = 0;
+  const uint64_t* __restrict__ ckey = s.c_key;
 #pragma unroll
   for (int t = 0; t < kClusterPer; ++t) {
     const int j = begin + t;
     cand[t] = 0;
+    kv[t] = ~0ULL;
     if (j < B) {
       int p0 = base + 2 * j, p1 = p0 + 1;
       if (p0 >= cap) p0 -= cap;
       if (p1 >= cap) p1 -= cap;
       cand[t] = s.stream_mod[p0] | (s.stream_mod[p1] << 16);
+      kv[t] = ckey[j];
       pending |= 1u << t;
     }
   }
   auto owner_at = [&](int m) -> int* { return cluster.map_shared_rank(owner, m % kPlaceCtas) + m / kPlaceCtas; };
   auto key_at = [&](int m) -> uint64_t* { return cluster.map_shared_rank(keys, m % kPlaceCtas) + m / kPlaceCtas; };
   int* counter0 = cluster.map_shared_rank(ready_count, 0);
-  const uint64_t* __restrict__ ckey = s.c_key;
   cluster.sync();
   const long long level_start = clock64();
   int left = B, levels_run = 0;
@@ -1072,9 +1075,6 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
       if ((pending >> t & 1) && *owner_at(int(cand[t] & 0xffff)) == (tag | (begin + t)) &&
           *owner_at(int(cand[t] >> 16)) == (tag | (begin + t)))
         ready |= 1u << t;
-    uint64_t kv[kClusterPer];
-#pragma unroll
-    for (int t = 0; t < kClusterPer; ++t) kv[t] = (ready >> t & 1) ? ckey[begin + t] : 0;
 #pragma unroll
     for (int t = 0; t < kClusterPer; ++t)
       if (ready >> t & 1) {
@@ -1102,10 +1102,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   int mv = 0x7fffffff;
 #pragma unroll
   for (int t = 0; t < kClusterPer; ++t)
-    if (begin + t < B) {
-      const uint64_t k = ckey[begin + t];
-      if (key_before(k, int(cand[t]), mk, mv)) { mk = k; mv = int(cand[t]); }
-    }
+    if (begin + t < B && key_before(kv[t], int(cand[t]), mk, mv)) { mk = kv[t]; mv = int(cand[t]); }
   for (int o = 1; o < 32; o <<= 1) {
     const uint64_t uk = __shfl_up_sync(kFull, mk, o);
     const int uv = __shfl_up_sync(kFull, mv, o);
@@ -1157,9 +1154,9 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
       if (v == bv) {
         atomicMin(redraw0, begin + t);
         hit = true;
-      } else {
-        const uint64_t k = ckey[begin + t];
-        if (key_before(k, v, bk, bv)) { bk = k; bv = v; }
+      } else if (key_before(kv[t], v, bk, bv)) {
+        bk = kv[t];
+        bv = v;
       }
     }
   cluster.sync();
