@@ -1006,7 +1006,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   __shared__ int scan_idx[32];
   __shared__ uint64_t cta_key[kPlaceCtas];  // block totals (read from block 0)
   __shared__ int cta_idx[kPlaceCtas];
-  __shared__ int ready_count[2], redraw_at;
+  __shared__ int ready_count[3], redraw_at;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = int(cluster.block_rank());
   const SearchDesc& s = descs[blockIdx.x / kPlaceCtas];
@@ -1030,7 +1030,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   int32_t* __restrict__ placed = s.placed;
   for (int m = rank * kClusterThreads + tid; m < P; m += kPlaceCtas * kClusterThreads) placed[m] = -1;
   if (tid == 0) {
-    ready_count[0] = ready_count[1] = 0;
+    ready_count[0] = ready_count[1] = ready_count[2] = 0;
     redraw_at = 0x7fffffff;
   }
   const int begin = (rank * kClusterThreads + tid) * kClusterPer;
@@ -1058,6 +1058,14 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   int* counter0 = cluster.map_shared_rank(ready_count, 0);
   cluster.sync();
   const long long level_start = clock64();
+  // One cluster barrier per level.  Level L claims members, passes barrier
+  // L, checks and places; a thread may then claim for level L + 1 while
+  // others still place for level L: its smaller tag never makes a level-L
+  // check succeed wrongly (it can only delay a child, which stays the
+  // earliest pending child of its members), and every level-L key write
+  // happens before barrier L + 1, ahead of every level-L+1 key read.  The
+  // level-L count is read after barrier L + 1 (slot L mod 3; the slot of
+  // level L - 1 is cleared for level L + 2 after barrier L + 1 too).
   int left = B, levels_run = 0;
   for (int level = 0; level <= B; ++level) {
     ++levels_run;
@@ -1069,6 +1077,11 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
         atomicMin(owner_at(int(cand[t] >> 16)), tag | (begin + t));
       }
     cluster.sync();
+    if (level > 0) {
+      left -= counter0[(level - 1) % 3];
+      if (left == 0) break;
+    }
+    if (rank == 0 && tid == 0) ready_count[(level + 1) % 3] = 0;
     uint32_t ready = 0;
 #pragma unroll
     for (int t = 0; t < kClusterPer; ++t)
@@ -1089,11 +1102,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
     pending &= ~ready;
     int placed_here = __popc(ready);
     for (int o = 16; o; o >>= 1) placed_here += __shfl_xor_sync(kFull, placed_here, o);
-    if (lane == 0 && placed_here) atomicAdd(counter0 + (level & 1), placed_here);
-    if (rank == 0 && tid == 0) ready_count[(level + 1) & 1] = 0;  // read by every thread before this level's first barrier
-    cluster.sync();
-    left -= counter0[level & 1];
-    if (left == 0) break;
+    if (lane == 0 && placed_here) atomicAdd(counter0 + level % 3, placed_here);
   }
   const long long level_end = clock64();
   // best member before each child: (key, victim) minimum of this thread's
