@@ -583,7 +583,8 @@ __device__ __forceinline__ bool key_before(uint64_t ka, int va, uint64_t kb, int
   return ka < kb || (ka == kb && va < vb);
 }
 // after_cluster: the cluster placement ran first; return if it placed the
-// round, else replay it on the exact windowed path.
+// round (place_state 1), replay it on the exact windowed path if it found a
+// redraw (2), or place it here if it did not take it (0).
 __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* descs, int n, int dyn_bytes,
                                                             int after_cluster) {
   extern __shared__ __align__(16) uint64_t keys[];
@@ -595,7 +596,8 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
   __shared__ int shared_best, shared_fail, ready_count[2], redraw_at;
   const SearchDesc& s = descs[blockIdx.x];
   if (!search_live(s)) return;
-  if (after_cluster && *s.place_state) return;
+  const int cluster_state = after_cluster ? *s.place_state : 0;
+  if (cluster_state == 1) return;
   const long long t0 = clock64();
   const int P = s.P, B = s.B, rs = s.replacement_size, cap = s.stream_capacity;
   const int tid = threadIdx.x;
@@ -619,7 +621,8 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
   // owner area after the keys, 16-byte aligned, with 64 bytes of slack for
   // the per-thread 16-byte reads of the staged draws
   int32_t* owner = reinterpret_cast<int32_t*>(keys + P + (P & 1));
-  const bool parallel_path = !after_cluster && rs == 2 && blockDim.x == kPlaceThreads && B <= kPlaceThreads * kPerThread &&
+  const bool parallel_path = cluster_state == 0 && rs == 2 && blockDim.x == kPlaceThreads &&
+                             B <= kPlaceThreads * kPerThread &&
                              wp - rp >= need &&
                              dyn_bytes >= int(sizeof(uint64_t)) * (P + 1) + int(sizeof(int32_t)) * P + 64;
   bool parallel_done = false;
@@ -992,13 +995,16 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
 // owning block's owner word, then the ready children place (remote key
 // reads and writes).  The running best before each child is a scan inside
 // each block plus a prefix over the blocks' totals.  When a child would have
-// redrawn, or the stream holds too few draws, or the replacement size is not
-// 2, nothing is written back: place_state stays 0 and k_place replays the
-// round on the exact path.  On success this kernel finishes the round as
-// k_place does (statistics, best member, stream position, next seed).
+// redrawn, nothing is written back (place_state 2) and k_place replays the
+// round on the exact path; a batch of fewer than kClusterMinChildren
+// children, another replacement size or a stream short of draws is left to
+// k_place (place_state 0), whose single block is then as fast.  On success
+// this kernel finishes the round as k_place does (statistics, best member,
+// stream position, next seed).
 constexpr int kPlaceCtas = 8;
 constexpr int kClusterThreads = 1024;
 constexpr int kClusterPer = 2;
+constexpr int kClusterMinChildren = 4096;
 __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThreads, 1)
     k_place_cluster(const SearchDesc* descs, int n) {
   extern __shared__ __align__(16) uint64_t cl_keys[];
@@ -1015,7 +1021,8 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   const int P = s.P, B = s.B, cap = s.stream_capacity;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long rp = stream_ptrs(s)[0], wp = stream_ptrs(s)[1];
-  if (s.replacement_size != 2 || B > kPlaceCtas * kClusterThreads * kClusterPer || wp - rp < 2LL * B + 1) {
+  if (s.replacement_size != 2 || B < kClusterMinChildren || B > kPlaceCtas * kClusterThreads * kClusterPer ||
+      wp - rp < 2LL * B + 1) {
     if (rank == 0 && tid == 0) *s.place_state = 0;
     return;  // the same decision in every block
   }
@@ -1188,7 +1195,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
     }
   }
   if (rank == 0 && tid == 0) {
-    *s.place_state = done ? 1 : 0;
+    *s.place_state = done ? 1 : 2;
     if (done) {
       const uint64_t* tot_key = cta_key;
       int fv = best0;
