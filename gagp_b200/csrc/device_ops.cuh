@@ -127,6 +127,18 @@ __device__ __forceinline__ unsigned minimum_of(const SearchDesc& s, int e, int d
   return __ldg(&s.minimum[(size_t(e) * s.depth_count + d) * s.logical_count + l]);
 }
 
+// A precomputed draw level (GenLevel) in registers.
+struct LevelView {
+  double total;
+  unsigned bound, entry;
+  int last, below;
+};
+__device__ __forceinline__ LevelView load_level(const GenLevel* p) {
+  const int4 a = __ldg(reinterpret_cast<const int4*>(p));
+  const int2 b = __ldg(reinterpret_cast<const int2*>(p) + 2);
+  return LevelView{__hiloint2double(a.y, a.x), unsigned(a.z), unsigned(a.w), b.x, b.y};
+}
+
 // generate_phase<CompactTasks=true, EmitSites=true, Warp=false>
 // (cpp/src/evolution/repro/gpu/device/phase_generate.cuh:125-270): a typed
 // random subtree with min-cost feasibility and the FP64 weighted production
@@ -148,9 +160,8 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
   const gagp_value* __restrict__ vals = s.vals;
   const uint32_t* __restrict__ minimum = s.minimum;
   const uint32_t* __restrict__ prod_minimum = s.prod_minimum;
-  const uint32_t* __restrict__ nt_maxmin = s.nt_maxmin;
-  const double* __restrict__ nt_total = s.nt_total;
-  const double* __restrict__ prod_threshold = s.prod_threshold;
+  const GenLevel* __restrict__ gen_level = s.gen_level;
+  const GenEntry* __restrict__ gen_entry = s.gen_entry;
   const int n_ex = s.n_ex, n_nts = s.n_nts, n_prods = s.n_prods, n_doms = s.n_doms, n_vals = s.n_vals;
   const int depth_count = s.depth_count, logical_count = s.logical_count;
   const bool site_limited = s.site_depth > 0;
@@ -205,29 +216,30 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       if (reserved > unsigned(capacity - result.nodes)) { result.status = ST_CAPACITY; return result; }
       const unsigned available = unsigned(capacity - result.nodes) - reserved;
       const uint32_t* __restrict__ prow = prod_minimum + (t_depth * logical_count + n_logical) * n_prods + nt_offset;
-      const double all_total = __ldg(&nt_total[target]);
-      if (__ldg(&nt_maxmin[(t_depth * logical_count + n_logical) * n_nts + target]) <= available &&
-          all_total == all_total) {
-        // every production feasible: the precomputed thresholds give the
-        // production the sequential subtraction stops at
-        const double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), all_total);
-        int pick = nt_count - 1;
+      // the widest precomputed level whose productions all fit
+      LevelView lv = load_level(gen_level + ((t_depth * logical_count + n_logical) * n_nts + target));
+      while (lv.bound > available && lv.below >= 0) lv = load_level(gen_level + lv.below);
+      if (lv.bound <= available && lv.total == lv.total) {
+        const double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), lv.total);
+        const GenEntry* __restrict__ en = gen_entry + lv.entry;
+        int pick = lv.last;
         if (nt_count <= 8) {
           double th[8];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) th[k] = k < nt_count ? __ldg(&prod_threshold[nt_offset + k]) : 0.0;
+          for (int k = 0; k < 8; ++k) th[k] = k < nt_count ? __ldg(&en[k].threshold) : 0.0;
 #pragma unroll
           for (int k = 7; k >= 0; --k)
             if (k < nt_count && choice < th[k]) pick = k;
         } else {
           for (int i = 0; i < nt_count; ++i)
-            if (choice < __ldg(&prod_threshold[nt_offset + i])) { pick = i; break; }
+            if (choice < __ldg(&en[i].threshold)) { pick = i; break; }
         }
-        next_expr = unsigned(__ldg(&prods[nt_offset + pick].expression));
-        const unsigned need = __ldg(&prow[pick]);
+        const int2 picked = __ldg(reinterpret_cast<const int2*>(en + pick) + 1);  // expression, need
+        const int pe = picked.x;
+        const unsigned need = unsigned(picked.y);
         if (count >= 192) return result;
         reserved += need;
-        pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical), need);
+        pending[count++] = pack(unsigned(pe), unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical), need);
         continue;
       }
       // feasibility of each production (a bit mask for the first 64)

@@ -285,75 +285,139 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
 }
 
 // Precomputed production draws (generate_phase's weighted choice,
-// cpp/src/evolution/repro/gpu/device/phase_generate.cuh:125-270) for the
-// case where every production of a nonterminal is feasible.  The choice
+// cpp/src/evolution/repro/gpu/device/phase_generate.cuh:125-270).  At a
+// given (depth, site budget) a production is feasible when its minimum cost
+// fits the room left, so the feasible productions of a nonterminal are
+// always those whose cost is at most one of the distinct costs among its
+// productions: one level per distinct cost.  For each level the choice
 // value c = u * total is compared against thresholds instead of subtracting
-// the weights one by one: with f_i(c) = (((c - v_0) - v_1) ... - v_i), each
-// step rounded to nearest in double precision, f_i is non-decreasing in c,
-// so f_i(c) < 0 exactly when c is below the smallest double T_i with
-// f_i(T_i) >= 0, found here by bisection over the bit patterns of
-// non-negative doubles.  The first production whose threshold exceeds c is
-// the one the sequential loop stops at (the last one when none does).
+// the weights one by one: with f_i(c) = (((c - v_0) - v_1) ... - v_i) over
+// the level's productions, each step rounded to nearest in double
+// precision, f_i is non-decreasing in c, so f_i(c) < 0 exactly when c is
+// below the smallest double T_i with f_i(T_i) >= 0, found by bisection over
+// the bit patterns of non-negative doubles.  The first production whose
+// threshold exceeds c is the one the sequential loop stops at (the last
+// feasible one when none does).  Levels with the same feasible set share
+// their draw; past kMaxDrawEntries the remaining nonterminals keep the
+// sequential draw.
+constexpr size_t kMaxDrawEntries = size_t(1) << 16;
+
 struct DrawTables {
-  std::vector<uint32_t> maxmin;
-  std::vector<double> total, threshold;
+  std::vector<gb::GenLevel> level;
+  std::vector<gb::GenEntry> entry;
 };
-DrawTables draw_tables(const gagp_grammar* g) {
+
+// `with_draws` false: only the table sizes (for the memory plan).
+DrawTables draw_tables(const gagp_grammar* g, bool with_draws) {
   const int E = g->expression_count, PR = g->production_count, NT = g->nonterminal_count;
   const int DC = g->depth_count, LC = g->logical_depth_count;
   DrawTables t;
-  t.maxmin.assign(size_t(std::max(1, NT)) * DC * LC, gb::kNoId);
-  t.total.assign(size_t(std::max(1, NT)), std::nan(""));
-  t.threshold.assign(size_t(std::max(1, PR)), 0.0);
+  const size_t heads = size_t(std::max(1, NT)) * DC * LC;
+  gb::GenLevel none{};
+  none.total = std::nan("");
+  none.bound = gb::kNoId;
+  none.entry = 0;
+  none.last = -1;
+  none.below = -1;
+  t.level.assign(heads, none);
+  struct Draw { double total; int last; std::vector<double> threshold; };
+  std::map<std::pair<int, std::vector<uint8_t>>, Draw> memo;
+  auto from_bits = [](uint64_t b) { double d; std::memcpy(&d, &b, sizeof d); return d; };
+  auto draw_of = [&](int nt, const std::vector<uint8_t>& feasible) -> const Draw& {
+    auto it = memo.find({nt, feasible});
+    if (it != memo.end()) return it->second;
+    const gagp_nonterminal& n = g->nonterminals[nt];
+    const int off = n.production_offset, cnt = n.production_count;
+    Draw dr{std::nan(""), -1, std::vector<double>(cnt, 0.0)};
+    double maximum = n.normalized_weights ? 1.0 : 0.0;
+    for (int i = 0; i < cnt; ++i)
+      if (feasible[i] && !n.normalized_weights && g->productions[off + i].weight > maximum)
+        maximum = g->productions[off + i].weight;
+    if (maximum > 0) {
+      std::vector<double> v(cnt, 0.0);
+      double total = 0.0;
+      for (int i = 0; i < cnt; ++i)
+        if (feasible[i]) {
+          const double w = g->productions[off + i].weight;
+          v[i] = n.normalized_weights ? w : w / maximum;
+          total = total + v[i];
+          dr.last = i;
+        }
+      auto f = [&](double c, int i) {
+        double x = c;
+        for (int k = 0; k <= i; ++k)
+          if (feasible[k]) x = x - v[k];
+        return x;
+      };
+      for (int i = 0; i < cnt; ++i) {
+        if (!feasible[i] || f(0.0, i) >= 0) continue;  // threshold 0: never picked
+        uint64_t lo = 0, hi = 0x7ff0000000000000ULL;   // f_i(lo) < 0 <= f_i(hi)
+        while (hi - lo > 1) {
+          const uint64_t mid = lo + (hi - lo) / 2;
+          if (f(from_bits(mid), i) >= 0) hi = mid; else lo = mid;
+        }
+        dr.threshold[i] = from_bits(hi);
+      }
+      dr.total = total;
+    }
+    return memo.emplace(std::make_pair(nt, feasible), std::move(dr)).first->second;
+  };
   for (int nt = 0; nt < NT; ++nt) {
     const gagp_nonterminal& n = g->nonterminals[nt];
     const int off = n.production_offset, cnt = n.production_count;
     if (cnt <= 0 || off < 0 || off > PR || cnt > PR - off) continue;
     bool valid = true;
-    double maximum = n.normalized_weights ? 1.0 : 0.0;
-    for (int i = 0; i < cnt; ++i) {
-      const gagp_production& p = g->productions[off + i];
-      if (p.expression < 0 || p.expression >= E) valid = false;
-      if (!n.normalized_weights && p.weight > maximum) maximum = p.weight;
-    }
-    if (!valid || !(maximum > 0)) continue;
-    std::vector<double> v(cnt);
-    double total = 0.0;
-    for (int i = 0; i < cnt; ++i) {
-      const double w = g->productions[off + i].weight;
-      v[i] = n.normalized_weights ? w : w / maximum;
-      total = total + v[i];
-    }
-    auto f = [&](double c, int i) {
-      double x = c;
-      for (int k = 0; k <= i; ++k) x = x - v[k];
-      return x;
-    };
-    auto from_bits = [](uint64_t b) { double d; std::memcpy(&d, &b, sizeof d); return d; };
-    for (int i = 0; i < cnt; ++i) {
-      if (f(0.0, i) >= 0) { t.threshold[off + i] = 0.0; continue; }
-      uint64_t lo = 0, hi = 0x7ff0000000000000ULL;  // f_i(lo) < 0 <= f_i(hi)
-      while (hi - lo > 1) {
-        const uint64_t mid = lo + (hi - lo) / 2;
-        if (f(from_bits(mid), i) >= 0) hi = mid; else lo = mid;
-      }
-      t.threshold[off + i] = from_bits(hi);
-    }
-    t.total[nt] = total;
+    for (int i = 0; i < cnt; ++i)
+      if (g->productions[off + i].expression < 0 || g->productions[off + i].expression >= E) valid = false;
+    if (!valid) continue;
     for (int d = 0; d < DC; ++d)
       for (int l = 0; l < LC; ++l) {
-        uint32_t m = 0;
+        std::vector<uint32_t> cost(cnt);
         for (int i = 0; i < cnt; ++i)
-          m = std::max(m, g->minimum[(size_t(g->productions[off + i].expression) * DC + d) * LC + l]);
-        t.maxmin[(size_t(d) * LC + l) * NT + nt] = m;
+          cost[i] = g->minimum[(size_t(g->productions[off + i].expression) * DC + d) * LC + l];
+        std::vector<uint32_t> bounds;
+        for (uint32_t c : cost)
+          if (c != gb::kNoId) bounds.push_back(c);
+        std::sort(bounds.begin(), bounds.end());
+        bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
+        if (bounds.empty() || t.entry.size() + bounds.size() * size_t(cnt) > kMaxDrawEntries) continue;
+        // widest level at the head, narrower ones appended and chained
+        int32_t slot = int32_t((size_t(d) * LC + l) * NT + nt);
+        for (int k = int(bounds.size()) - 1; k >= 0; --k) {
+          gb::GenLevel lv = none;
+          lv.bound = bounds[k];
+          lv.entry = uint32_t(t.entry.size());
+          std::vector<uint8_t> feasible(cnt);
+          for (int i = 0; i < cnt; ++i) feasible[i] = cost[i] <= bounds[k];
+          const Draw* dr = with_draws ? &draw_of(nt, feasible) : nullptr;
+          if (dr) {
+            lv.total = dr->total;
+            lv.last = dr->last;
+          }
+          for (int i = 0; i < cnt; ++i) {
+            gb::GenEntry en{};
+            en.threshold = dr ? dr->threshold[i] : 0.0;
+            en.expression = g->productions[off + i].expression;
+            en.need = cost[i];
+            t.entry.push_back(en);
+          }
+          if (k == int(bounds.size()) - 1) {
+            t.level[size_t(slot)] = lv;
+          } else {
+            t.level[size_t(slot)].below = int32_t(t.level.size());
+            slot = int32_t(t.level.size());
+            t.level.push_back(lv);
+          }
+        }
       }
   }
+  if (t.entry.empty()) t.entry.push_back(gb::GenEntry{});
   return t;
 }
 
 struct Plan {
   Layout L;
-  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, nt_maxmin, nt_total, prod_threshold, gen_expr,
+  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, gen_level, gen_entry, gen_expr,
       gen_nt, local_types, inputs, expected;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
@@ -391,10 +455,11 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.minimum = L.take(sizeof(uint32_t) * size_t(E) * g->depth_count * g->logical_depth_count);
   p.prod_minimum = L.take(sizeof(uint32_t) * size_t(std::max(1, g->production_count)) * g->depth_count *
                           g->logical_depth_count);
-  p.nt_maxmin = L.take(sizeof(uint32_t) * size_t(std::max(1, g->nonterminal_count)) * g->depth_count *
-                       g->logical_depth_count);
-  p.nt_total = L.take(sizeof(double) * size_t(std::max(1, g->nonterminal_count)));
-  p.prod_threshold = L.take(sizeof(double) * size_t(std::max(1, g->production_count)));
+  {
+    const DrawTables shape = draw_tables(g, false);
+    p.gen_level = L.take(sizeof(gb::GenLevel) * shape.level.size());
+    p.gen_entry = L.take(sizeof(gb::GenEntry) * shape.entry.size());
+  }
   p.gen_expr = L.take(sizeof(gb::GenExpr) * size_t(E));
   p.gen_nt = L.take(sizeof(gb::GenNt) * size_t(std::max(1, g->nonterminal_count)));
   p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
@@ -587,10 +652,9 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
         if (pe >= 0 && pe < E) prod_minimum[(size_t(d) * LC + l) * PR + q] = g->minimum[(size_t(pe) * DC + d) * LC + l];
       }
   CUDA_TRY(up(p.prod_minimum, prod_minimum.data(), sizeof(uint32_t) * prod_minimum.size()));
-  DrawTables draw = draw_tables(g);
-  CUDA_TRY(up(p.nt_maxmin, draw.maxmin.data(), sizeof(uint32_t) * draw.maxmin.size()));
-  CUDA_TRY(up(p.nt_total, draw.total.data(), sizeof(double) * draw.total.size()));
-  CUDA_TRY(up(p.prod_threshold, draw.threshold.data(), sizeof(double) * draw.threshold.size()));
+  const DrawTables draw = draw_tables(g, true);
+  CUDA_TRY(up(p.gen_level, draw.level.data(), sizeof(gb::GenLevel) * draw.level.size()));
+  CUDA_TRY(up(p.gen_entry, draw.entry.data(), sizeof(gb::GenEntry) * draw.entry.size()));
   std::vector<gb::GenExpr> gen_expr(E);
   for (int i = 0; i < E; ++i) {
     const gagp_expression& x = g->expressions[i];
@@ -627,9 +691,8 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.vals = at<gagp_value>(b, p.vals);
   d.minimum = at<uint32_t>(b, p.minimum);
   d.prod_minimum = at<uint32_t>(b, p.prod_minimum);
-  d.nt_maxmin = at<uint32_t>(b, p.nt_maxmin);
-  d.nt_total = at<double>(b, p.nt_total);
-  d.prod_threshold = at<double>(b, p.prod_threshold);
+  d.gen_level = at<gb::GenLevel>(b, p.gen_level);
+  d.gen_entry = at<gb::GenEntry>(b, p.gen_entry);
   d.gen_expr = at<gb::GenExpr>(b, p.gen_expr);
   d.gen_nt = at<gb::GenNt>(b, p.gen_nt);
   d.local_types = at<int32_t>(b, p.local_types);
@@ -1157,7 +1220,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.ex = at<gagp_expression>(b, p.ex);
   d.info = at<gb::ExprInfo>(b, p.info);
   d.minimum = at<uint32_t>(b, p.minimum);
-  d.prod_minimum = d.nt_maxmin = d.minimum;  // no subtree generation in row evaluation
+  d.prod_minimum = d.minimum;  // no subtree generation in row evaluation
   d.local_types = at<int32_t>(b, p.local_types);
   d.n_ex = E;
   d.slot_type = g->slot_type;

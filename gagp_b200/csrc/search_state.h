@@ -51,6 +51,29 @@ struct alignas(16) GenExpr {
 struct alignas(16) GenNt {
   int32_t production_offset, production_count, scope_count, normalized_weights;
 };
+// Precomputed production draw of one nonterminal at one (depth, site
+// budget) for one feasibility level: the productions whose minimum cost is at
+// most `bound` are the feasible ones, and the draw over them is decided by
+// comparing the choice value with per-production thresholds (GenEntry).  A
+// nonterminal's levels at one (depth, site budget) form a chain from the
+// widest (every production of finite cost) down through `below`.
+struct alignas(16) GenLevel {
+  double total;     // the draw's weight sum; NaN: no precomputed draw
+  uint32_t bound;   // largest minimum cost of a feasible production (kNoId: none)
+  uint32_t entry;   // first of the nonterminal's production_count GenEntry
+  int32_t last;     // the last feasible production: the pick when no threshold exceeds the choice
+  int32_t below;    // the next narrower level, -1: none
+  int32_t reserved[2];
+};
+// One production of a level's draw: the smallest choice value whose running
+// difference after this production is not negative (0: never picked), the
+// production's expression and its minimum cost at the level's (depth, site
+// budget).
+struct alignas(16) GenEntry {
+  double threshold;
+  int32_t expression;
+  uint32_t need;
+};
 
 // Everything a kernel needs to work on one search (device pointers).
 struct SearchDesc {
@@ -67,14 +90,11 @@ struct SearchDesc {
   const uint32_t* prod_minimum;
   const GenExpr* gen_expr;
   const GenNt* gen_nt;
-  // production draw when every production of a nonterminal is feasible:
-  // nt_maxmin[(d * logical_count + l) * n_nts + nt] = the largest production
-  // minimum (all feasible iff it fits), nt_total[nt] = the draw's weight sum
-  // (NaN: no precomputed draw), prod_threshold[p]: the smallest choice value
-  // whose running difference after production p is not negative
-  const uint32_t* nt_maxmin;
-  const double* nt_total;
-  const double* prod_threshold;
+  // precomputed production draws: gen_level[(d * logical_count + l) * n_nts
+  // + nt] is the widest level of nonterminal nt at (depth d, site budget l);
+  // narrower levels follow the first depth_count * logical_count * n_nts
+  const GenLevel* gen_level;
+  const GenEntry* gen_entry;
   const int32_t* local_types;          // ValueTag of each evaluator input
   int32_t n_ex, n_prods, n_nts, n_doms, n_vals;
   int32_t depth_count, logical_count, site_depth;
