@@ -31,6 +31,24 @@ constexpr uint32_t kNoClass = 0x7ffu;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---------------------------------------------------------------- RNG
+// Rejection bound ((2^64 - u) mod u) and reciprocal floor((2^64 - 1) / u) of
+// every range u <= kBoundTable, fixed at compile time: site counts, value
+// lists and small integer domains draw without a 64-bit division.
+constexpr int kBoundTable = 1024;
+struct BoundTable {
+  uint64_t threshold[kBoundTable + 1];
+  uint64_t magic[kBoundTable + 1];
+};
+constexpr BoundTable make_bound_table() {
+  BoundTable t{};
+  for (int u = 1; u <= kBoundTable; ++u) {
+    t.threshold[u] = (0 - uint64_t(u)) % uint64_t(u);
+    t.magic[u] = ~uint64_t(0) / uint64_t(u);
+  }
+  return t;
+}
+__device__ const BoundTable g_bounds = make_bound_table();
+
 // SplitMix64 stream with rejection-sampled bounds
 // (DGrammarRandom, cpp/src/evolution/repro/gpu/device/grammar_random.cuh:10-51).
 struct Rng {
@@ -43,6 +61,8 @@ struct Rng {
     return v ^ (v >> 31);
   }
   __device__ __forceinline__ uint64_t bounded(uint64_t upper) {
+    if (upper - 1 < uint64_t(kBoundTable))
+      return bounded_fixed(upper, __ldg(&g_bounds.threshold[upper]), __ldg(&g_bounds.magic[upper]));
     const uint64_t threshold = (0 - upper) % upper;
     for (;;) {
       const uint64_t v = next();
@@ -420,14 +440,17 @@ __device__ inline int warp_subtree_end(const SRow& t, int start) {
   return -1;
 }
 
-// Constant nodes among row positions [0, end).
-__device__ __forceinline__ int warp_count_constants(const SRow& t, int end) {
-  int c = 0;
-  for (int chunk = 0; chunk < end; chunk += 32) {
+// Constant nodes among row positions [0, first) and [0, second), first <= second.
+__device__ __forceinline__ void warp_count_constants2(const SRow& t, int first, int second, int* a, int* b) {
+  int ca = 0, cb = 0;
+  for (int chunk = 0; chunk < second; chunk += 32) {
     const int i = chunk + lane_id();
-    c += __popc(__ballot_sync(kFull, i < end && w_const(t.node[i])));
+    const bool c = i < second && w_const(t.node[i]);
+    ca += __popc(__ballot_sync(kFull, c && i < first));
+    cb += __popc(__ballot_sync(kFull, c));
   }
-  return c;
+  *a = ca;
+  *b = cb;
 }
 
 template <typename T>
@@ -441,20 +464,20 @@ __device__ __forceinline__ T warp_max(T v) {
 }
 
 // splice_phase_tree (device/phase_variation.cuh:147-207): base with the
-// subtree at `dest` replaced by donor's subtree at `src`, into `out`.
+// subtree [dest, end) replaced by donor's subtree [src, donor_end), into
+// `out`; the callers have found both subtree ends already.
 // Depth and site-depth limits are maxima of the output words; constants are
 // base[..dest) ++ donor subtree ++ base[end..), the prefix renumbering the
 // reference performs node by node.  Every lane returns the same result.
-__device__ inline GenResult warp_splice(const SRow& base, int dest, const SRow& donor, int src, SRow out, int stride,
-                                        int max_depth, int site_limit) {
+__device__ inline GenResult warp_splice(const SRow& base, int dest, int end, const SRow& donor, int src, int donor_end,
+                                        SRow out, int stride, int max_depth, int site_limit) {
   GenResult r{ST_INVALID, 0, 0};
   if (max_depth <= 0 || max_depth > 64 || base.n <= 0 || donor.n <= 0 || dest < 0 || dest >= base.n || src < 0 ||
       src >= donor.n)
     return r;
   const uint64_t a = base.node[dest], b = donor.node[src];
   if (!w_site(a) || w_class(a) != w_class(b)) return r;
-  const int end = warp_subtree_end(base, dest), donor_end = warp_subtree_end(donor, src);
-  if (end < 0 || donor_end < 0) return r;
+  if (end <= dest || end > base.n || donor_end <= src || donor_end > donor.n) return r;
   const int inserted = donor_end - src;
   const int length = base.n - (end - dest) + inserted;
   if (length > kCapacity) { r.status = ST_CAPACITY; return r; }
@@ -473,8 +496,9 @@ __device__ inline GenResult warp_splice(const SRow& base, int dest, const SRow& 
     maxd = max(maxd, w_depth(w));
     maxs = max(maxs, w_sval(w));
   }
-  const int bb = warp_count_constants(base, dest), be = warp_count_constants(base, end);
-  const int db = warp_count_constants(donor, src), de = warp_count_constants(donor, donor_end);
+  int bb, be, db, de;
+  warp_count_constants2(base, dest, end, &bb, &be);
+  warp_count_constants2(donor, src, donor_end, &db, &de);
   const int dc = de - db;
   for (int k = lane_id(); k < bb; k += 32) out.cval[k] = base.cval[k];
   for (int k = lane_id(); k < dc; k += 32) out.cval[bb + k] = donor.cval[db + k];

@@ -108,7 +108,8 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
       const int ae = warp_subtree_end(w.parent, dest), be = warp_subtree_end(w.donor, src);
       if (ae < 0 || be < 0) return 3;
       if (total - (ae - dest) + (be - src) > s.maxv) continue;
-      const GenResult r = warp_splice(w.parent, dest, w.donor, src, w.out, s.stride, s.slot_max_depth, s.site_depth);
+      const GenResult r = warp_splice(w.parent, dest, ae, w.donor, src, be, w.out, s.stride, s.slot_max_depth,
+                                      s.site_depth);
       if (r.status == ST_OK) {
         warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
         w.child.n = r.nodes;
@@ -158,7 +159,8 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
         } else {
           w.gen.n = g.nodes;
           w.gen.nc = g.constants;
-          const GenResult r = warp_splice(w.child, dest, w.gen, 0, w.out, s.stride, s.slot_max_depth, s.site_depth);
+          const GenResult r = warp_splice(w.child, dest, end, w.gen, 0, w.gen.n, w.out, s.stride, s.slot_max_depth,
+                                          s.site_depth);
           if (r.status != ST_OK) return 8;
           warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
           w.child.n = r.nodes;
