@@ -138,10 +138,10 @@ cudaError_t copy_d2h(gagp_engine* e, void* dst, const void* src, size_t bytes) {
 namespace {
 
 enum KernelId {
-  KN_INIT, KN_LOWER, KN_VM_FAST, KN_VM_GENERAL, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
+  KN_INIT, KN_LOWER, KN_VM_FAST, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
   KN_COMMIT, KN_STREAM, KN_COUNT
 };
-const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast", "k_vm_general",
+const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast",
                                             "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
                                             "k_place", "k_commit", "k_stream"};
 
@@ -851,14 +851,16 @@ int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1
 
 // Evaluates lowered programs listed by k_lower (both VMs).
 // Fast-VM launch of one instantiation.
+// One VM launch over both lists: counts[0] fast programs, counts[1] programs
+// that need the exact VM.
 void vm_fast_launch(int lanes, int blocks, int threads, size_t smem, cudaStream_t stream, const gb::SearchDesc* descs,
-                    int mode, const gb::ProgramRef* list, const int32_t* count, int temp_stride, int code_stride,
-                    int const_stride, int max_C) {
+                    int mode, const gb::ProgramRef* list, const gb::ProgramRef* general, const int32_t* counts,
+                    int temp_stride, int code_stride, int const_stride, int max_C) {
   const int tiles = (max_C + 32 * lanes - 1) / (32 * lanes);
   switch (lanes) {
-    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride, tiles); break;
-    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride, tiles); break;
-    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, count, temp_stride, code_stride, const_stride, tiles); break;
+    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, general, counts + 1, temp_stride, code_stride, const_stride, tiles); break;
+    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, general, counts + 1, temp_stride, code_stride, const_stride, tiles); break;
+    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, general, counts + 1, temp_stride, code_stride, const_stride, tiles); break;
   }
 }
 
@@ -909,17 +911,13 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
   }
   {
     Timed t(e, KN_VM_FAST, stream);
-    vm_fast_launch(plan.lanes, blocks, warps * 32, smem, stream, v.d_desc, mode, fast, counts, temp_stride, code_stride,
-                   const_stride, v.max_C);
+    vm_fast_launch(plan.lanes, blocks, warps * 32, smem, stream, v.d_desc, mode, fast, general, counts, temp_stride,
+                   code_stride, const_stride, v.max_C);
   }
   if (plan.measure_key) {
     cudaEventRecord(mark_stop, stream);
     e->tune_marks.push_back({plan.measure_key, plan.cand, mark_start, mark_stop});
     ++e->vm_tune[plan.measure_key].pending;
-  }
-  {
-    Timed t(e, KN_VM_GENERAL, stream);
-    gb::k_vm_general<<<e->sm_count * 4, 128, 0, stream>>>(v.d_desc, mode, general, counts + 1);
   }
   return GAGP_OK;
 }
@@ -1291,9 +1289,8 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   const size_t smem = size_t(warps) * (temp_stride + code_stride + p.stride) * sizeof(int64_t);
   if (smem > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the VM's shared memory");
   const int per_sm = std::max(1, std::min(4, int((max_smem - 1024) / smem)));
-  vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, counts, temp_stride, code_stride,
-                 p.stride, C);
-  gb::k_vm_general<<<sm_count * 4, 128, 0, stream>>>(dd, 0, general, counts + 1);
+  vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, general, counts, temp_stride,
+                 code_stride, p.stride, C);
   CUDA_TRY(cudaGetLastError());
   int32_t round[4];
   CUDA_TRY(cudaMemcpyAsync(round, b + p.round, sizeof round, cudaMemcpyDeviceToHost, stream));

@@ -5,7 +5,7 @@
 // offsets array (items of search i are [off[i], off[i+1])).  A single search
 // is a batch of one.  Per round (run_phase_population_steady,
 // cpp/src/evolution/evolve.cpp:388-427):
-//   k_record (epoch start) -> k_vary -> k_lower -> k_vm_fast / k_vm_general
+//   k_record (epoch start) -> k_vary -> k_lower -> k_vm_fast (exact-VM programs included)
 //   -> k_child_results -> k_place -> k_commit
 #pragma once
 #include <cooperative_groups.h>
@@ -137,69 +137,11 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
   }
 }
 
-// Fast VM: persistent warps over the fast list.  Per warp shared memory:
-// temporaries (kMaxTemps x K x 32), the staged code (code_stride) and
-// constants (stride).
-template <int K>
-__device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWarpSmem& w, int case_begin,
-                                      int case_end, int64_t& loss, uint32_t& wrong, uint64_t& ops) {
-  switch (s.n_inputs) {
-    case 1: run_accumulator<K, 1>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
-    case 2: run_accumulator<K, 2>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
-    default: run_accumulator<K, 0>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
-  }
-}
-// One instantiation per cases-per-lane K (each with its own register
-// budget); the engine's autotuner picks K per batch shape.  Work items are
-// (program, tile of 32 K cases), program-major, so that a round with fewer
-// programs than resident warps still fills the GPU; each tile adds its loss
-// and wrong count to the program's accumulators and the last tile to finish
-// stores the program's result (integer sums: the order does not matter).
-template <int K>
-__global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list,
-                                                 const int32_t* list_count, int temp_stride, int code_stride,
-                                                 int const_stride, int tiles_max) {
-  extern __shared__ __align__(16) int64_t smem_vm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int warps = blockDim.x >> 5;
-  const size_t per_warp = size_t(temp_stride) + size_t(code_stride) + size_t(const_stride);  // int64 units
-  int64_t* base = smem_vm + size_t(warp) * per_warp;
-  const VmWarpSmem w{base, reinterpret_cast<uint2*>(base + temp_stride), base + temp_stride + code_stride};
-  const long long items = (long long)(*list_count) * tiles_max;
-  for (long long item = (long long)blockIdx.x * warps + warp; item < items; item += (long long)gridDim.x * warps) {
-    const ProgramRef p = list[item / tiles_max];
-    const int case0 = int(item % tiles_max) * 32 * K;
-    const SearchDesc& s = descs[p.search];
-    if (case0 >= s.C) continue;
-    int64_t loss = 0;
-    uint32_t wrong = 0;
-    uint64_t ops = 0;
-    run_k<K>(s, p.slot, w, case0, min(s.C, case0 + 32 * K), loss, wrong, ops);
-    loss = warp_sum(loss);
-    wrong = warp_sum(wrong);
-    if (lane == 0) {
-      unsigned long long* acc = s.vm_acc + 2 * size_t(p.slot);
-      atomicAdd(&acc[0], (unsigned long long)loss);
-      __threadfence();
-      const unsigned long long before = atomicAdd(&acc[1], (unsigned long long)wrong | (1ULL << 32));
-      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), (unsigned long long)ops);
-      const unsigned tiles = unsigned((s.C + 32 * K - 1) / (32 * K));
-      if (unsigned(before >> 32) == tiles - 1) {  // the last tile of the program
-        __threadfence();
-        const int64_t total = int64_t(atomicAdd(&acc[0], 0ULL));
-        store_result(s, mode, p.slot, total, uint32_t(before) + wrong);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
-      }
-    }
-  }
-}
-
-// General VM: one block per program of the general list, threads over cases.
-__global__ void k_vm_general(const SearchDesc* descs, int mode, const ProgramRef* list, const int32_t* list_count) {
+// General VM: the block's threads run one program of the general list at a
+// time, thread per case (any block size that is a multiple of 32).
+__device__ inline void vm_general_programs(const SearchDesc* descs, int mode, const ProgramRef* list, int count) {
   __shared__ int64_t red_loss[32];
   __shared__ uint32_t red_wrong[32];
-  const int count = *list_count;
   for (int i = blockIdx.x; i < count; i += gridDim.x) {
     const ProgramRef p = list[i];
     const SearchDesc& s = descs[p.search];
@@ -235,6 +177,67 @@ __global__ void k_vm_general(const SearchDesc* descs, int mode, const ProgramRef
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
     }
     __syncthreads();
+  }
+}
+
+// Fast VM: persistent warps over the fast list.  Per warp shared memory:
+// temporaries (kMaxTemps x K x 32), the staged code (code_stride) and
+// constants (stride).
+template <int K>
+__device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWarpSmem& w, int case_begin,
+                                      int case_end, int64_t& loss, uint32_t& wrong, uint64_t& ops) {
+  switch (s.n_inputs) {
+    case 1: run_accumulator<K, 1>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
+    case 2: run_accumulator<K, 2>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
+    default: run_accumulator<K, 0>(s, slot, w, case_begin, case_end, loss, wrong, ops); break;
+  }
+}
+// One instantiation per cases-per-lane K (each with its own register
+// budget); the engine's autotuner picks K per batch shape.  Work items are
+// (program, tile of 32 K cases), program-major, so that a round with fewer
+// programs than resident warps still fills the GPU; each tile adds its loss
+// and wrong count to the program's accumulators and the last tile to finish
+// stores the program's result (integer sums: the order does not matter).
+template <int K>
+__global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list,
+                                                 const int32_t* list_count, const ProgramRef* general,
+                                                 const int32_t* general_count, int temp_stride, int code_stride,
+                                                 int const_stride, int tiles_max) {
+  extern __shared__ __align__(16) int64_t smem_vm[];
+  // the programs that need the exact VM first, a block each (rarely any)
+  vm_general_programs(descs, mode, general, *general_count);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  const size_t per_warp = size_t(temp_stride) + size_t(code_stride) + size_t(const_stride);  // int64 units
+  int64_t* base = smem_vm + size_t(warp) * per_warp;
+  const VmWarpSmem w{base, reinterpret_cast<uint2*>(base + temp_stride), base + temp_stride + code_stride};
+  const long long items = (long long)(*list_count) * tiles_max;
+  for (long long item = (long long)blockIdx.x * warps + warp; item < items; item += (long long)gridDim.x * warps) {
+    const ProgramRef p = list[item / tiles_max];
+    const int case0 = int(item % tiles_max) * 32 * K;
+    const SearchDesc& s = descs[p.search];
+    if (case0 >= s.C) continue;
+    int64_t loss = 0;
+    uint32_t wrong = 0;
+    uint64_t ops = 0;
+    run_k<K>(s, p.slot, w, case0, min(s.C, case0 + 32 * K), loss, wrong, ops);
+    loss = warp_sum(loss);
+    wrong = warp_sum(wrong);
+    if (lane == 0) {
+      unsigned long long* acc = s.vm_acc + 2 * size_t(p.slot);
+      atomicAdd(&acc[0], (unsigned long long)loss);
+      __threadfence();
+      const unsigned long long before = atomicAdd(&acc[1], (unsigned long long)wrong | (1ULL << 32));
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), (unsigned long long)ops);
+      const unsigned tiles = unsigned((s.C + 32 * K - 1) / (32 * K));
+      if (unsigned(before >> 32) == tiles - 1) {  // the last tile of the program
+        __threadfence();
+        const int64_t total = int64_t(atomicAdd(&acc[0], 0ULL));
+        store_result(s, mode, p.slot, total, uint32_t(before) + wrong);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
+      }
+    }
   }
 }
 
