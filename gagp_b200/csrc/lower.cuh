@@ -184,20 +184,30 @@ __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code
     carry += __shfl_sync(kFull, incl, 31);
   }
   __syncwarp();
-  // a subtree ends at the first later node with fewer open slots
-  for (int i = lane; i < n; i += 32) {
-    const int r = m.start[i];
-    int j = i + 1;
-    while (j < n && m.start[j] >= r) ++j;
-    m.end[i] = int16_t(j);
+  // a subtree ends at the first later node with fewer open slots: for 32
+  // nodes at a time, every lane holds one later node's slot count and each
+  // node's question is answered by one ballot per chunk
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    const int r = i < n ? m.start[i] : 0;
+    int e = n;
+    bool found = i >= n;
+    for (int cb = base; cb < n && __any_sync(kFull, !found); cb += 32) {
+      const int j = cb + lane;
+      const int slots = j < n ? m.start[j] : 0x7fffffff;
+      for (int q = 0; q < 32; ++q) {
+        const int rq = __shfl_sync(kFull, r, q);
+        const unsigned hit = __ballot_sync(kFull, j > base + q && slots < rq);
+        if (lane == q && !found && hit) {
+          e = cb + __ffs(hit) - 1;
+          found = true;
+        }
+      }
+    }
+    if (i < n) m.end[i] = int16_t(e);
   }
   __syncwarp();
   if (carry != 0 || m.end[0] != n) return -1;
-  auto child = [&](int i, int x) -> int {
-    int c = i + 1;
-    for (int k = 0; k < x; ++k) c = m.end[c];
-    return c;
-  };
   // ---- bottom-up: need, size, evaluation order
   uint32_t pend = 0;  // bit k: node lane + 32 k not yet computed
   for (int k = 0; lane + 32 * k < n; ++k) {
@@ -224,27 +234,38 @@ __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code
     if (!__any_sync(kFull, ready != 0) || __any_sync(kFull, fail)) { fail = true; break; }
     for (uint32_t b = ready; b; b &= b - 1) {
       const int k = __ffs(b) - 1, i = lane + 32 * k, a = m.arity[i];
-      int needs[3], idx[3], nonleaf = 0, sz = 0;
-      for (int x = 0, c = i + 1; x < a; ++x) {
-        if (m.end[c] - c > 1) { needs[nonleaf] = m.need[c]; idx[nonleaf] = x; ++nonleaf; sz += m.size[c]; }
-        c = m.end[c];
+      // the non-leaf children as (need << 2 | position), in child order, in
+      // registers (arity <= 3)
+      const int c0 = i + 1, c1 = a > 1 ? m.end[c0] : 0, c2 = a > 2 ? m.end[c1] : 0;
+      int e0 = 0, e1 = 0, e2 = 0, nonleaf = 0, sz = 0;
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        const int c = x == 0 ? c0 : x == 1 ? c1 : c2;
+        if (x < a && m.end[c] - c > 1) {
+          const int v = (int(m.need[c]) << 2) | x;
+          if (nonleaf == 0) e0 = v; else if (nonleaf == 1) e1 = v; else e2 = v;
+          ++nonleaf;
+          sz += m.size[c];
+        }
       }
-      // the explicit-stack evaluator's exchange sort by decreasing need
-      for (int x = 0; x < nonleaf; ++x)
-        for (int y = x + 1; y < nonleaf; ++y)
-          if (needs[y] > needs[x]) {
-            const int tn = needs[x]; needs[x] = needs[y]; needs[y] = tn;
-            const int ti = idx[x]; idx[x] = idx[y]; idx[y] = ti;
-          }
+      // the explicit-stack evaluator's exchange sort by decreasing need:
+      // pairs (0,1), (0,2), (1,2), swapping when the later need is larger
+      auto exchange = [](int& p, int& q) {
+        if ((q >> 2) > (p >> 2)) { const int t = p; p = q; q = t; }
+      };
+      if (nonleaf > 1) exchange(e0, e1);
+      if (nonleaf > 2) { exchange(e0, e2); exchange(e1, e2); }
       int mx = 0;
-      for (int x = 0; x < nonleaf; ++x) mx = max(mx, needs[x] + x);
+      if (nonleaf > 0) mx = max(mx, e0 >> 2);
+      if (nonleaf > 1) mx = max(mx, (e1 >> 2) + 1);
+      if (nonleaf > 2) mx = max(mx, (e2 >> 2) + 2);
       // own words: unary MOV + op when its child is a leaf; binary MOV + op
       // when both children are leaves; otherwise one word
-      const bool leaf0 = m.end[i + 1] - (i + 1) == 1;
+      const bool leaf0 = m.end[c0] - c0 == 1;
       const int own = a == 1 ? (leaf0 ? 2 : 1) : a == 2 ? (nonleaf == 0 ? 2 : 1) : 1;
       m.size[i] = int16_t(min(sz + max(nonleaf - 1, 0) + own, 32767));
-      m.order[i] = uint8_t((nonleaf << 6) | (nonleaf > 0 ? idx[0] : 0) | (nonleaf > 1 ? idx[1] << 2 : 0) |
-                           (nonleaf > 2 ? idx[2] << 4 : 0));
+      m.order[i] = uint8_t((nonleaf << 6) | (nonleaf > 0 ? e0 & 3 : 0) | (nonleaf > 1 ? (e1 & 3) << 2 : 0) |
+                           (nonleaf > 2 ? (e2 & 3) << 4 : 0));
       m.need[i] = int8_t(min(mx, 127));
     }
     pend &= ~ready;
@@ -278,49 +299,65 @@ __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code
     for (uint32_t b = ready; b; b &= b - 1) {
       const int k = __ffs(b) - 1, i = lane + 32 * k, a = m.arity[i];
       if (m.depth[i] >= 65) fail = true;  // the 65th nested frame overflows the 64-frame stack
-      const int count = m.order[i] >> 6, tb = m.temp_base[i];
+      const int ob = m.order[i], count = ob >> 6, tb = m.temp_base[i];
+      const int o0 = ob & 3, o1 = (ob >> 2) & 3, o2 = (ob >> 4) & 3;
+      const int c0 = i + 1, c1 = a > 1 ? m.end[c0] : 0, c2 = a > 2 ? m.end[c1] : 0;
+      auto child_at = [&](int x) { return x == 0 ? c0 : x == 1 ? c1 : c2; };
+      const int child_depth = min(int(m.depth[i]) + 1, 255);
       int pos = m.start[i];
-      int ord[3] = {m.order[i] & 3, (m.order[i] >> 2) & 3, (m.order[i] >> 4) & 3};
-      for (int q = 0; q < count; ++q) {
-        const int c = child(i, ord[q]);
-        if (q > 0) {
-          const int temp = tb + q - 1;
-          if (temp >= kMaxTemps) fail = true;
-          else code[pos] = a_instr(A_SPILL, false, K_TEMP, uint32_t(temp));
-          ++pos;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        if (q < count) {
+          const int c = child_at(q == 0 ? o0 : q == 1 ? o1 : o2);
+          if (q > 0) {
+            const int temp = tb + q - 1;
+            if (temp >= kMaxTemps) fail = true;
+            else code[pos] = a_instr(A_SPILL, false, K_TEMP, uint32_t(temp));
+            ++pos;
+          }
+          m.start[c] = int16_t(pos);
+          m.temp_base[c] = int8_t(tb + q);
+          m.depth[c] = uint8_t(child_depth);
+          pos += m.size[c];
         }
-        m.start[c] = int16_t(pos);
-        m.temp_base[c] = int8_t(tb + q);
-        m.depth[c] = uint8_t(min(int(m.depth[i]) + 1, 255));
-        pos += m.size[c];
       }
       const uint32_t op = m.aop[i];
-      uint32_t kind[3] = {K_ACC, K_ACC, K_ACC}, id[3] = {0, 0, 0};
-      const int last = count ? ord[count - 1] : -1;
-      for (int x = 0; x < a; ++x) {
-        const int c = child(i, x);
-        if (m.end[c] - c == 1) { kind[x] = m.leaf[c] >> 16; id[x] = m.leaf[c] & 0xffffu; }
-        else if (x == last) { kind[x] = K_ACC; }
-        else {
-          kind[x] = K_TEMP;
-          for (int q = 0; q < count - 1; ++q)
-            if (ord[q] == x) id[x] = uint32_t(tb + q);
+      const int last = count == 1 ? o0 : count == 2 ? o1 : count == 3 ? o2 : -1;
+      uint32_t kind0 = K_ACC, kind1 = K_ACC, kind2 = K_ACC, id0 = 0, id1 = 0, id2 = 0;
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        if (x < a) {
+          const int c = child_at(x);
+          uint32_t kind = K_ACC, id = 0;
+          if (m.end[c] - c == 1) {
+            const uint32_t leaf = m.leaf[c];
+            kind = leaf >> 16;
+            id = leaf & 0xffffu;
+          } else if (x != last) {
+            // a spilled non-leaf child: the temporary of its evaluation slot
+            kind = K_TEMP;
+            if (count > 1 && o0 == x) id = uint32_t(tb);
+            else if (count > 2 && o1 == x) id = uint32_t(tb + 1);
+          }
+          if (x == 0) { kind0 = kind; id0 = id; }
+          else if (x == 1) { kind1 = kind; id1 = id; }
+          else { kind2 = kind; id2 = id; }
         }
       }
       if (a == 1) {
-        if (kind[0] != K_ACC) code[pos++] = a_instr(A_MOV, false, kind[0], id[0]);
+        if (kind0 != K_ACC) code[pos++] = a_instr(A_MOV, false, kind0, id0);
         code[pos] = a_instr(op, false, K_ACC, 0);
       } else if (a == 2) {
-        if (kind[0] != K_ACC && kind[1] != K_ACC) {
-          code[pos++] = a_instr(A_MOV, false, kind[0], id[0]);
-          code[pos] = a_instr(op, false, kind[1], id[1]);
-        } else if (kind[0] == K_ACC) {
-          code[pos] = a_instr(op, false, kind[1], id[1]);
+        if (kind0 != K_ACC && kind1 != K_ACC) {
+          code[pos++] = a_instr(A_MOV, false, kind0, id0);
+          code[pos] = a_instr(op, false, kind1, id1);
+        } else if (kind0 == K_ACC) {
+          code[pos] = a_instr(op, false, kind1, id1);
         } else {
-          code[pos] = a_instr(op, true, kind[0], id[0]);  // acc = op(first, acc)
+          code[pos] = a_instr(op, true, kind0, id0);  // acc = op(first, acc)
         }
       } else {
-        code[pos] = a_instr(A_SELECT, false, kind[0], id[0], kind[1], id[1], kind[2], id[2]);
+        code[pos] = a_instr(A_SELECT, false, kind0, id0, kind1, id1, kind2, id2);
       }
     }
     pend &= ~ready;
