@@ -1163,15 +1163,16 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
       bv = scan_idx[warp - 1];
     }
   }
-  // a child whose victim is the best member before it would have redrawn
-  int* redraw0 = cluster.map_shared_rank(&redraw_at, 0);
+  // a child whose victim is the best member before it would have redrawn;
+  // the earliest such child is noted in every block, so that no block reads
+  // another's shared memory after the last cluster barrier
   bool hit = false;
 #pragma unroll
   for (int t = 0; t < kClusterPer; ++t)
     if (!hit && begin + t < B) {
       const int v = int(cand[t]);
       if (v == bv) {
-        atomicMin(redraw0, begin + t);
+        for (int r = 0; r < kPlaceCtas; ++r) atomicMin(cluster.map_shared_rank(&redraw_at, r), begin + t);
         hit = true;
       } else if (key_before(kv[t], v, bk, bv)) {
         bk = kv[t];
@@ -1179,7 +1180,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
       }
     }
   cluster.sync();
-  const bool done = *redraw0 == 0x7fffffff;
+  const bool done = redraw_at == 0x7fffffff;
   if (done) {
     // this block's members take their child's statistics
     const double* __restrict__ cfit = s.c_fitness;

@@ -88,6 +88,24 @@ template <int K, int NIN>
 __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWarpSmem& w, int case_begin,
                                        int case_end, int64_t& loss_out, uint32_t& wrong_out, uint64_t& ops_out) {
   const int lane = threadIdx.x & 31;
+  const int C = s.C;  // input-major stride
+  const int64_t* __restrict__ inputs = s.inputs;
+  const int64_t* __restrict__ expected = s.expected;
+  // a tile's inputs and expected values, loaded before they are needed: the
+  // first tile's ahead of the code staging, each next tile's ahead of the
+  // current tile's instructions, so that their latency overlaps other work
+  int64_t in0[K], in1[K], want[K];
+  auto fetch = [&](int tile) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int c = tile + k * 32 + lane;
+      const bool live = c < case_end;
+      in0[k] = (NIN >= 1 && live) ? __ldg(&inputs[c]) : 0;
+      in1[k] = (NIN >= 2 && live) ? __ldg(&inputs[size_t(C) + c]) : 0;
+      want[k] = live ? __ldg(&expected[c]) : 0;
+    }
+  };
+  fetch(case_begin);
   const int len = s.code_len[slot];
   {
     const uint2* code = s.code + size_t(slot) * s.code_stride;
@@ -96,21 +114,22 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
     for (int i = lane; i < s.stride; i += 32) w.consts[i] = kpool[i];
     __syncwarp();
   }
-  const int C = s.C;  // input-major stride
-  const int64_t* __restrict__ inputs = s.inputs;
   int64_t* __restrict__ temps = w.temps;
   int64_t loss = 0;
   uint32_t wrong = 0;
   for (int tile = case_begin; tile < case_end; tile += 32 * K) {
     int64_t acc[K];
-    int64_t in0[K], in1[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0;
+    // this tile's operands, and the next tile's loads in flight
+    int64_t cur0[K], cur1[K], cur_want[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      acc[k] = 0;
-      const int c = tile + k * 32 + lane;
-      in0[k] = (NIN >= 1 && c < case_end) ? __ldg(&inputs[c]) : 0;
-      in1[k] = (NIN >= 2 && c < case_end) ? __ldg(&inputs[size_t(C) + c]) : 0;
+      cur0[k] = in0[k];
+      cur1[k] = in1[k];
+      cur_want[k] = want[k];
     }
+    if (tile + 32 * K < case_end) fetch(tile + 32 * K);
     // operand vector of one instruction: the kind switch is warp-uniform and
     // taken once per instruction, not once per case
     auto load = [&](uint32_t kind, uint32_t index, int64_t* v) {
@@ -126,10 +145,10 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
         case K_INPUT:
           if (NIN == 1 || (NIN == 2 && index == 0)) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) v[k] = in0[k];
+            for (int k = 0; k < K; ++k) v[k] = cur0[k];
           } else if (NIN == 2) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) v[k] = in1[k];
+            for (int k = 0; k < K; ++k) v[k] = cur1[k];
           } else {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -249,7 +268,7 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int c = tile + k * 32 + lane;
-      if (c < case_end) loss += case_loss(s, s.slot_type, acc[k], __ldg(&s.expected[c]), wrong);
+      if (c < case_end) loss += case_loss(s, s.slot_type, acc[k], cur_want[k], wrong);
     }
   }
   __syncwarp();
