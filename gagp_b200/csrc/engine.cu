@@ -1564,13 +1564,26 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   if (!round[2]) return fail(GAGP_NOT_READY, "search has not finished");
   const int H = std::min(round[1], out->generations);
   const int P = s->P, S = s->stride;
+  // the final population ranked and in transport form on the device, so the
+  // host only copies it out
+  const int W = S;
+  Layout D;
+  const size_t d_rank = D.take(4 * size_t(P)), d_fit = D.take(8 * size_t(P)), d_wr = D.take(4 * size_t(P)),
+               d_nodes = D.take(4 * size_t(P)), d_nc = D.take(4 * size_t(P)), d_cc = D.take(4 * size_t(P)),
+               d_org = D.take(4 * size_t(P) * W), d_con = D.take(8 * size_t(P) * W);
+  char* db = nullptr;
+  CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&db), D.total, e->pool, e->stream));
+  gb::k_rank_members<<<blocks_for(P, 128), 128, 0, e->stream>>>(s->d_desc, at<int32_t>(db, d_rank));
+  gb::k_export_members<<<blocks_for(size_t(P) * 32, 256), 256, 0, e->stream>>>(
+      s->d_desc, at<int32_t>(db, d_rank), W, at<double>(db, d_fit), at<int32_t>(db, d_wr), at<int32_t>(db, d_nodes),
+      at<int32_t>(db, d_nc), at<int32_t>(db, d_cc), at<int32_t>(db, d_org), at<int64_t>(db, d_con));
   // every array in one pinned staging area, copied asynchronously, one sync
   Layout L;
   const size_t o_sum = L.take(8 * size_t(H)), o_hf = L.take(8 * size_t(H)), o_hw = L.take(4 * size_t(H)),
                o_hn = L.take(4 * size_t(H)), o_hnode = L.take(8 * size_t(H) * S), o_hc = L.take(8 * size_t(H) * S),
                o_hl = L.take(4 * size_t(H)), o_fit = L.take(8 * size_t(P)), o_wr = L.take(4 * size_t(P)),
-               o_key = L.take(8 * size_t(P)), o_node = L.take(8 * size_t(P) * S), o_cv = L.take(8 * size_t(P) * S),
-               o_len = L.take(4 * size_t(P)), o_cnt = L.take(8 * 4);
+               o_nodes = L.take(4 * size_t(P)), o_nc = L.take(4 * size_t(P)), o_cc = L.take(4 * size_t(P)),
+               o_org = L.take(4 * size_t(P) * W), o_con = L.take(8 * size_t(P) * W), o_cnt = L.take(8 * 4);
   if (L.total > e->pinned_bytes) {
     if (e->pinned) cudaFreeHost(e->pinned);
     e->pinned = nullptr;
@@ -1590,13 +1603,17 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   CUDA_TRY(fetch(o_hnode, d.hist_node, 8 * size_t(H) * S));
   CUDA_TRY(fetch(o_hc, d.hist_cval, 8 * size_t(H) * S));
   CUDA_TRY(fetch(o_hl, d.hist_len, 4 * size_t(H)));
-  CUDA_TRY(fetch(o_fit, d.fitness, 8 * size_t(P)));
-  CUDA_TRY(fetch(o_wr, d.wrong, 4 * size_t(P)));
-  CUDA_TRY(fetch(o_key, d.key, 8 * size_t(P)));
-  CUDA_TRY(fetch(o_node, d.node, 8 * size_t(P) * S));
-  CUDA_TRY(fetch(o_cv, d.cval, 8 * size_t(P) * S));
-  CUDA_TRY(fetch(o_len, d.len, 4 * size_t(P)));
+  // the ranked population: only the rows the caller asked for
+  const int n_out = std::min(P, out->population);
+  CUDA_TRY(fetch(o_fit, db + d_fit, 8 * size_t(n_out)));
+  CUDA_TRY(fetch(o_wr, db + d_wr, 4 * size_t(n_out)));
+  CUDA_TRY(fetch(o_nodes, db + d_nodes, 4 * size_t(n_out)));
+  CUDA_TRY(fetch(o_nc, db + d_nc, 4 * size_t(n_out)));
+  CUDA_TRY(fetch(o_cc, db + d_cc, 4 * size_t(n_out)));
+  CUDA_TRY(fetch(o_org, db + d_org, 4 * size_t(n_out) * W));
+  CUDA_TRY(fetch(o_con, db + d_con, 8 * size_t(n_out) * W));
   CUDA_TRY(fetch(o_cnt, d.counters, 8 * 4));
+  CUDA_TRY(cudaFreeAsync(db, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   const int64_t* sum = reinterpret_cast<const int64_t*>(hb + o_sum);
   const double* hf = reinterpret_cast<const double*>(hb + o_hf);
@@ -1605,12 +1622,6 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
   const uint64_t* hnode = reinterpret_cast<const uint64_t*>(hb + o_hnode);
   const int64_t* hc = reinterpret_cast<const int64_t*>(hb + o_hc);
   const int32_t* hl = reinterpret_cast<const int32_t*>(hb + o_hl);
-  const double* fit = reinterpret_cast<const double*>(hb + o_fit);
-  const uint32_t* wr = reinterpret_cast<const uint32_t*>(hb + o_wr);
-  const uint64_t* key = reinterpret_cast<const uint64_t*>(hb + o_key);
-  const uint64_t* node = reinterpret_cast<const uint64_t*>(hb + o_node);
-  const int64_t* cv = reinterpret_cast<const int64_t*>(hb + o_cv);
-  const int32_t* len = reinterpret_cast<const int32_t*>(hb + o_len);
   const uint64_t* counters = reinterpret_cast<const uint64_t*>(hb + o_cnt);
   auto put_row = [&](const gagp_rows& rows, int index, const uint64_t* node, const int64_t* cval, int32_t l) {
     const int n = l & 0xffff, nc = (l >> 16) & 0xffff;
@@ -1628,16 +1639,23 @@ gagp_status gagp_b200_search_result(gagp_engine* e, int32_t id, gagp_search_resu
     put_row(out->history_best, h, hnode + size_t(h) * S, hc + size_t(h) * S, hl[h]);
   }
   out->generations = H;
-  std::vector<int> order(P);
-  std::iota(order.begin(), order.end(), 0);
-  std::sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
-  const int n_out = std::min(P, out->population);
-  for (int r = 0; r < n_out; ++r) {
-    const int m = order[r];
-    out->final_fitness[r] = fit[m];
-    out->final_wrong[r] = s->has_wrong ? int32_t(wr[m]) : -1;
-    out->final_nodes[r] = s->fixed_nodes + (len[m] & 0xffff);
-    put_row(out->final_rows, r, node + size_t(m) * S, cv + size_t(m) * S, len[m]);
+  std::memcpy(out->final_fitness, hb + o_fit, 8 * size_t(n_out));
+  std::memcpy(out->final_wrong, hb + o_wr, 4 * size_t(n_out));
+  std::memcpy(out->final_nodes, hb + o_nodes, 4 * size_t(n_out));
+  const gagp_rows& fr = out->final_rows;
+  std::memcpy(fr.node_counts, hb + o_nc, 4 * size_t(n_out));
+  std::memcpy(fr.constant_counts, hb + o_cc, 4 * size_t(n_out));
+  const int32_t* org = reinterpret_cast<const int32_t*>(hb + o_org);
+  const int64_t* con = reinterpret_cast<const int64_t*>(hb + o_con);
+  if (fr.stride == W) {
+    std::memcpy(fr.origins, org, 4 * size_t(n_out) * W);
+    std::memcpy(fr.constants, con, 8 * size_t(n_out) * W);
+  } else {
+    const int w = std::min(W, fr.stride);
+    for (int r = 0; r < n_out; ++r) {
+      std::memcpy(fr.origins + size_t(r) * fr.stride, org + size_t(r) * W, 4 * size_t(w));
+      std::memcpy(fr.constants + size_t(r) * fr.stride, con + size_t(r) * W, 8 * size_t(w));
+    }
   }
   out->population = n_out;
   out->evaluated_programs = counters[0];

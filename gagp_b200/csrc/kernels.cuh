@@ -1221,6 +1221,59 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   }
 }
 
+// ------------------------------------------------------------ result export
+// The final population ranked as the reference ranks it (by ranking key,
+// ties by member index, selection.cpp:10-20): a member's rank is the number
+// of members before it, counted against shared-memory tiles of the keys.
+constexpr int kRankTile = 1024;
+__global__ void __launch_bounds__(128) k_rank_members(const SearchDesc* desc, int32_t* rank) {
+  __shared__ uint64_t tile[kRankTile];
+  const SearchDesc& s = *desc;
+  const int P = s.P;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t mk = m < P ? s.key[m] : 0;
+  int r = 0;
+  for (int base = 0; base < P; base += kRankTile) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRankTile; i += blockDim.x) tile[i] = base + i < P ? s.key[base + i] : ~0ULL;
+    __syncthreads();
+    const int lim = min(kRankTile, P - base);
+    if (m < P)
+      for (int j = 0; j < lim; ++j) {
+        const uint64_t k = tile[j];
+        r += k < mk || (k == mk && base + j < m);
+      }
+  }
+  if (m < P) rank[m] = r;
+}
+
+// Each member's statistics and transport row (construction expressions and
+// constants, `width` entries per row, zero past its counts) at its rank:
+// a warp per member.
+__global__ void k_export_members(const SearchDesc* desc, const int32_t* rank, int width, double* fitness,
+                                 int32_t* wrong, int32_t* nodes, int32_t* node_counts, int32_t* constant_counts,
+                                 int32_t* origins, int64_t* constants) {
+  const int m = int((size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  const SearchDesc& s = *desc;
+  if (m >= s.P) return;
+  const int r = rank[m];
+  const int32_t l = s.len[m];
+  const int n = len_nodes(l), nc = len_consts(l);
+  if (lane == 0) {
+    fitness[r] = s.fitness[m];
+    wrong[r] = s.has_wrong ? int32_t(s.wrong[m]) : -1;
+    nodes[r] = s.fixed_nodes + n;
+    node_counts[r] = n;
+    constant_counts[r] = nc;
+  }
+  const uint64_t* node = s.node + size_t(m) * s.stride;
+  const int64_t* cval = s.cval + size_t(m) * s.stride;
+  for (int i = lane; i < width; i += 32) {
+    origins[size_t(r) * width + i] = i < n && i < s.stride ? int32_t(node[i] & 0xffffu) : 0;
+    constants[size_t(r) * width + i] = i < nc && i < s.stride ? cval[i] : 0;
+  }
+}
+
 // commit_batch (phase_population_cpu.cpp:382-394): placed child rows replace
 // members.  Thread per member.
 __global__ void k_commit(const SearchDesc* descs, const int32_t* off, int n) {

@@ -340,7 +340,9 @@ gagp_status gagp_b200_server_result(gagp_server* server, int64_t ticket, gagp_se
 /* Drops a ticket in any state (a running search is stopped and freed). */
 gagp_status gagp_b200_server_cancel(gagp_server* server, int64_t ticket);
 
-/* Copies a finished search's history and final ranked population out. */
+/* Copies a finished search's history and final ranked population out (the
+ * population is ranked and put in transport form on the device; in
+ * final_rows, entries past a row's counts are set to 0). */
 gagp_status gagp_b200_search_result(gagp_engine* engine, int32_t search, gagp_search_result* out);
 
 #ifdef __cplusplus
