@@ -63,3 +63,36 @@ def test_search_matches_oracle_fresh_seeds(engine, seed, tmp_path):
     assert got["final"] == want["final"]
     assert got["evaluated_programs"] == want["evaluated_programs"]
     assert got["reused_programs"] == want["reused_programs"]
+
+
+def test_result_part_and_wider_rows(engine, tmp_path):
+    """Reading back only the best part of the ranked population, into rows
+    wider than the engine's, gives the first rows of the full read-back (the
+    population is ranked and put in transport form on the device)."""
+    from gagp_b200 import task as T
+    from gagp_b200.engine import _check, load_library
+    files = W.poly4(population=300, generations=4, seed=21, cases=40, max_nodes=40)
+    lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
+    s = engine.admit(lt)
+    try:
+        s.run()
+        full = s.result()
+        width = lt.tables.max_nodes - lt.tables.fixed_nodes
+        part = abi.ResultBuffer(lt.settings.generations, 100, width + 7)
+        _check(load_library().gagp_b200_search_result(engine.handle, s.id, part.ref()))
+        again = s.result()
+    finally:
+        s.close()
+    got = part.summary()
+    assert got["history"] == full["history"]
+    assert len(got["final"]) == 100
+    assert got["final"] == full["final"][:100]
+    assert again == full
+    # entries past a row's counts are zero up to the engine's row width (the
+    # node budget rounded up to 4 slots) and untouched beyond it
+    engine_width = (width + 3) // 4 * 4
+    rows = part.final_rows
+    for i in range(100):
+        n = int(rows.node_counts[i])
+        assert (rows.origins[i, n:engine_width] == 0).all()
+        assert (rows.origins[i, engine_width:] == -1).all()
