@@ -182,11 +182,13 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
   const uint32_t* __restrict__ prod_minimum = s.prod_minimum;
   const GenLevel* __restrict__ gen_level = s.gen_level;
   const GenEntry* __restrict__ gen_entry = s.gen_entry;
-  const int n_ex = s.n_ex, n_nts = s.n_nts, n_prods = s.n_prods, n_doms = s.n_doms, n_vals = s.n_vals;
+  const int n_ex = s.n_ex, n_nts = s.n_nts, n_prods = s.n_prods;
   const int depth_count = s.depth_count, logical_count = s.logical_count;
   const bool site_limited = s.site_depth > 0;
-  auto min_of = [&](int e, int d, int l) -> unsigned {
-    if (e < 0 || e >= n_ex || d < 0 || d >= depth_count || l < 0 || l >= logical_count) return kNoId;
+  // minimum cost of (expression, depth, site budget); admission has checked
+  // every expression id a table holds, and the generator keeps depth and site
+  // budget inside the table, so only the root's lookup is range-checked
+  auto min_at = [&](int e, int d, int l) -> unsigned {
     return __ldg(&minimum[(e * depth_count + d) * logical_count + l]);
   };
   int next_site = -1;  // entry expression of a pending site
@@ -196,20 +198,24 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       capacity <= 0 || capacity > kCapacity || n_ex > 131071)
     return result;
   if (capacity > s.stride) capacity = s.stride;  // callers pass at most the node budget
-  int count = 1;
   // a task: expression, depth, scope, site budget and its minimum cost (the
-  // reservation made when it was pushed)
+  // reservation made when it was pushed).  The task to run next is kept in a
+  // register (`next`, when have_next) rather than pushed and popped at once;
+  // `count` is what the reference's stack holds below it.
   auto pack = [](unsigned e, unsigned d, unsigned n, unsigned l, unsigned required) -> uint64_t {
     return uint64_t(e | (d << 17) | (n << 24) | (l << 28)) | (uint64_t(required) << 32);
   };
-  unsigned reserved = min_of(root_expression, depth, logical_depth);
-  pending[0] = pack(unsigned(root_expression), unsigned(depth), unsigned(scope_count), unsigned(logical_depth),
-                    reserved);
+  unsigned reserved = min_at(root_expression, depth, logical_depth);
+  uint64_t next = pack(unsigned(root_expression), unsigned(depth), unsigned(scope_count), unsigned(logical_depth),
+                       reserved);
+  bool have_next = true;
+  int count = 0;
   if (reserved > unsigned(capacity)) { result.status = ST_CAPACITY; return result; }
   Rng random(seed);
-  while (count) {
+  while (have_next || count) {
     if (++result.steps > 8192) { result.status = ST_CAPACITY; return result; }
-    const uint64_t task = pending[--count];
+    const uint64_t task = have_next ? next : pending[--count];
+    have_next = false;
     const int t_expr = int(task & 0x1ffffu), t_depth = int((task >> 17) & 0x7fu);
     const int t_scope = int((task >> 24) & 0xfu), t_logical = int((task >> 28) & 0xfu);
     const unsigned required = unsigned(task >> 32);
@@ -218,24 +224,21 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
     const int4 ra = __ldg(reinterpret_cast<const int4*>(gx + t_expr));      // children
     const int4 rb = __ldg(reinterpret_cast<const int4*>(gx + t_expr) + 1);  // target, class, kinds, scopes
     const int kind = int(int8_t(rb.z & 0xff)), arity = int(int8_t((rb.z >> 8) & 0xff));
-    const int e_scopes = int(int8_t((rb.z >> 16) & 0xff));
     const int target = rb.x;
     if (kind == EK_REFERENCE) {
-      if (target < 0 || target >= n_nts || e_scopes < 0 || e_scopes > 8) return result;
+      // admission: the target nonterminal exists, is unscoped (as is every
+      // reference) and its productions are in range
       if (next_site >= 0) return result;
       next_site = t_expr;
       next_class = uint32_t(rb.y);
       const int4 nt = __ldg(reinterpret_cast<const int4*>(gnt + target));
       const int nt_offset = nt.x, nt_count = nt.y;
       const bool normalized = nt.w != 0;
-      if (nt.z != e_scopes || nt_offset < 0 || nt_count <= 0 || nt_offset > n_prods || nt_count > n_prods - nt_offset)
-        return result;
       if (site_limited && t_logical == 0) { result.status = ST_CAPACITY; return result; }
       const int n_logical = t_logical - (site_limited ? 1 : 0);
-      unsigned next_expr = 131071u;  // unselected
       if (reserved > unsigned(capacity - result.nodes)) { result.status = ST_CAPACITY; return result; }
       const unsigned available = unsigned(capacity - result.nodes) - reserved;
-      const uint32_t* __restrict__ prow = prod_minimum + (t_depth * logical_count + n_logical) * n_prods + nt_offset;
+      unsigned next_expr, need;
       // the widest precomputed level whose productions all fit
       LevelView lv = load_level(gen_level + ((t_depth * logical_count + n_logical) * n_nts + target));
       while (lv.bound > available && lv.below >= 0) lv = load_level(gen_level + lv.below);
@@ -255,88 +258,71 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
             if (choice < __ldg(&en[i].threshold)) { pick = i; break; }
         }
         const int2 picked = __ldg(reinterpret_cast<const int2*>(en + pick) + 1);  // expression, need
-        const int pe = picked.x;
-        const unsigned need = unsigned(picked.y);
-        if (count >= 192) return result;
-        reserved += need;
-        pending[count++] = pack(unsigned(pe), unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical), need);
-        continue;
-      }
-      // feasibility of each production (a bit mask for the first 64)
-      uint64_t feasible_mask = 0;
-      for (int i = 0; i < nt_count && i < 64; ++i)
-        if (__ldg(&prow[i]) <= available) feasible_mask |= 1ULL << i;
-      auto feasible = [&](int i) -> bool { return i < 64 ? (feasible_mask >> i & 1) : __ldg(&prow[i]) <= available; };
-      double maximum = normalized ? 1.0 : 0.0, total = 0.0;
-      if (!normalized)
+        next_expr = unsigned(picked.x);
+        need = unsigned(picked.y);
+      } else {
+        // the reference's draw step by step (no precomputed level applies)
+        const uint32_t* __restrict__ prow = prod_minimum + (t_depth * logical_count + n_logical) * n_prods + nt_offset;
+        uint64_t feasible_mask = 0;  // a bit per production for the first 64
+        for (int i = 0; i < nt_count && i < 64; ++i)
+          if (__ldg(&prow[i]) <= available) feasible_mask |= 1ULL << i;
+        auto feasible = [&](int i) -> bool {
+          return i < 64 ? (feasible_mask >> i & 1) : __ldg(&prow[i]) <= available;
+        };
+        double maximum = normalized ? 1.0 : 0.0, total = 0.0;
+        if (!normalized)
+          for (int i = 0; i < nt_count; ++i) {
+            const double w = __ldg(&prods[nt_offset + i].weight);
+            if (feasible(i) && w > maximum) maximum = w;
+          }
+        if (!(maximum > 0)) { result.status = ST_CAPACITY; return result; }
+        for (int i = 0; i < nt_count; ++i)
+          if (feasible(i)) {
+            const double w = __ldg(&prods[nt_offset + i].weight);
+            total = __dadd_rn(total, normalized ? w : __ddiv_rn(w, maximum));
+          }
+        double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), total);
+        next_expr = 131071u;  // unselected
         for (int i = 0; i < nt_count; ++i) {
+          if (!feasible(i)) continue;
+          next_expr = unsigned(__ldg(&prods[nt_offset + i].expression));
           const double w = __ldg(&prods[nt_offset + i].weight);
-          if (feasible(i) && w > maximum) maximum = w;
+          choice = __dsub_rn(choice, normalized ? w : __ddiv_rn(w, maximum));
+          if (choice < 0) break;
         }
-      if (!(maximum > 0)) { result.status = ST_CAPACITY; return result; }
-      for (int i = 0; i < nt_count; ++i)
-        if (feasible(i)) {
-          const double w = __ldg(&prods[nt_offset + i].weight);
-          total = __dadd_rn(total, normalized ? w : __ddiv_rn(w, maximum));
-        }
-      double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), total);
-      for (int i = 0; i < nt_count; ++i) {
-        if (!feasible(i)) continue;
-        const int pe = __ldg(&prods[nt_offset + i].expression);
-        if (pe < 0 || pe >= n_ex) return result;
-        next_expr = unsigned(pe);
-        const double w = __ldg(&prods[nt_offset + i].weight);
-        choice = __dsub_rn(choice, normalized ? w : __ddiv_rn(w, maximum));
-        if (choice < 0) break;
+        if (next_expr == 131071u) return result;
+        need = min_at(int(next_expr), t_depth, n_logical);
       }
-      if (next_expr == 131071u || count >= 192) return result;
-      const unsigned need = min_of(int(next_expr), t_depth, n_logical);
+      if (count >= 192) return result;
       reserved += need;
-      pending[count++] = pack(next_expr, unsigned(t_depth), unsigned(e_scopes), unsigned(n_logical), need);
-      continue;
-    }
-    if (kind == EK_ALIAS) {
-      const int child = ra.x;
-      if (child < 0 || child >= n_ex || count >= 192) return result;
-      const int child_scope = int(int8_t(rb.w & 0xff));
-      const int scope = child_scope >= 0 ? child_scope : t_scope;
-      const unsigned need = min_of(child, t_depth, t_logical);
-      reserved += need;
-      pending[count++] = pack(unsigned(child), unsigned(t_depth), unsigned(scope), unsigned(t_logical), need);
+      next = pack(next_expr, unsigned(t_depth), 0u, unsigned(n_logical), need);
+      have_next = true;
       continue;
     }
     if (t_depth <= 0 || result.nodes >= capacity) { result.status = ST_CAPACITY; return result; }
-    if (arity < 0 || arity > 3) return result;  // admission bounds operation arity by 3
-    if (kind == EK_BOUND) {
-      const int operand = __ldg(&s.ex[t_expr].operand);
-      if (arity != 0 || operand < 0 || operand >= 16) return result;
-    } else if (kind == EK_CONSTANT) {
-      if (target < 0 || target >= n_doms || arity != 0) return result;
+    if (kind == EK_CONSTANT) {
+      // admission: the domain exists and is an Int range or a list of Ints
       const gagp_domain* domain = doms + target;
       int64_t value;
       if (__ldg(&domain->integer_range)) {
-        const int64_t lo = __ldg(&domain->minimum), hi = __ldg(&domain->maximum);
-        if (lo > hi) return result;
-        value = random.integer(lo, hi);
+        value = random.integer(__ldg(&domain->minimum), __ldg(&domain->maximum));
       } else {
         const int v_offset = __ldg(&domain->value_offset), v_count = __ldg(&domain->value_count);
-        if (v_offset < 0 || v_count <= 0 || v_offset > n_vals || v_count > n_vals - v_offset) return result;
-        const gagp_value* v = vals + v_offset + random.bounded(uint64_t(v_count));
-        if (__ldg(&v->tag) == GAGP_TAG_INVALID) return result;
-        value = __ldg(&v->i);
+        value = __ldg(&vals[v_offset + random.bounded(uint64_t(v_count))].i);
       }
       out_cval[result.constants++] = value;
     } else if (kind != EK_OPERATION && kind != EK_INPUT) {
-      return result;
+      return result;  // binders and aliases are declined at admission
     }
     out_node[result.nodes++] = w_make(t_expr, next_site, depth - t_depth + 1, logical_depth - t_logical, arity,
                                       kind == EK_CONSTANT, next_class);
     next_site = -1;
     next_class = kNoClass;
-    // the children's minimum costs, loaded together, then pushed last to first
-    const unsigned need0 = arity > 0 ? min_of(ra.x, t_depth - 1, t_logical) : 0;
-    const unsigned need1 = arity > 1 ? min_of(ra.y, t_depth - 1, t_logical) : 0;
-    const unsigned need2 = arity > 2 ? min_of(ra.z, t_depth - 1, t_logical) : 0;
+    // the children's minimum costs, loaded together, then pushed last to
+    // first (the first child straight into `next`)
+    const unsigned need0 = arity > 0 ? min_at(ra.x, t_depth - 1, t_logical) : 0;
+    const unsigned need1 = arity > 1 ? min_at(ra.y, t_depth - 1, t_logical) : 0;
+    const unsigned need2 = arity > 2 ? min_at(ra.z, t_depth - 1, t_logical) : 0;
     for (int i = arity - 1; i >= 0; --i) {
       if (count >= 192) { result.status = ST_CAPACITY; return result; }
       const int child = i == 0 ? ra.x : i == 1 ? ra.y : ra.z;
@@ -347,7 +333,13 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       }
       const int child_scope = int(int8_t((rb.w >> (8 * i)) & 0xff));
       const int scope = child_scope >= 0 ? child_scope : t_scope;
-      pending[count++] = pack(unsigned(child), unsigned(t_depth - 1), unsigned(scope), unsigned(t_logical), need);
+      const uint64_t t = pack(unsigned(child), unsigned(t_depth - 1), unsigned(scope), unsigned(t_logical), need);
+      if (i == 0) {
+        next = t;
+        have_next = true;
+      } else {
+        pending[count++] = t;
+      }
       reserved += need;
     }
   }

@@ -268,19 +268,50 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
   if (maxv < 1 || maxv > gb::kMaxLowerNodes) return fail(GAGP_DECLINED, "variable node budget outside 1..256");
   if (g->slot_max_depth < 1 || g->slot_max_depth >= g->depth_count || g->depth_count > 65)
     return fail(GAGP_DECLINED, "depth budget");
-  for (int i = 0; i < g->expression_count; ++i) {
+  // the subtree generator reads these tables without range checks: every id
+  // they hold must be in range
+  const int E = g->expression_count, NT = g->nonterminal_count, PR = g->production_count, ND = g->domain_count;
+  for (int i = 0; i < E; ++i) {
     const gagp_expression& e = g->expressions[i];
     if (e.kind == gb::EK_REFERENCE && e.scope_count != 0)
       return fail(GAGP_DECLINED, "scoped nonterminals are outside the resident scalar subset");
     if (e.kind == gb::EK_BOUND || e.kind == gb::EK_ALIAS)
       return fail(GAGP_DECLINED, "lexical binders/templates are outside the resident scalar subset");
+    if (e.kind != gb::EK_REFERENCE && e.kind != gb::EK_CONSTANT && e.kind != gb::EK_OPERATION &&
+        e.kind != gb::EK_INPUT)
+      return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": unknown kind");
     if (e.arity < 0 || e.arity > 3) return fail(GAGP_DECLINED, "arity capacity");
+    if (e.kind == gb::EK_REFERENCE) {
+      if (e.target < 0 || e.target >= NT) return fail(GAGP_INVALID_ARGUMENT, "reference to a missing nonterminal");
+      const gagp_nonterminal& n = g->nonterminals[e.target];
+      if (n.scope_count != 0) return fail(GAGP_DECLINED, "scoped nonterminals are outside the resident scalar subset");
+      if (n.production_count < 1 || n.production_offset < 0 || n.production_offset > PR ||
+          n.production_count > PR - n.production_offset)
+        return fail(GAGP_INVALID_ARGUMENT, "nonterminal " + std::to_string(e.target) + ": production range");
+      for (int k = 0; k < n.production_count; ++k) {
+        const int x = g->productions[n.production_offset + k].expression;
+        if (x < 0 || x >= E) return fail(GAGP_INVALID_ARGUMENT, "production of a missing expression");
+      }
+    } else if (e.kind == gb::EK_CONSTANT) {
+      if (e.arity != 0 || e.target < 0 || e.target >= ND) return fail(GAGP_INVALID_ARGUMENT, "constant domain");
+    } else {
+      for (int k = 0; k < e.arity; ++k)
+        if (e.children[k] < 0 || e.children[k] >= E) return fail(GAGP_INVALID_ARGUMENT, "child of a missing expression");
+    }
   }
-  for (int i = 0; i < g->domain_count; ++i)
-    if (!g->domains[i].integer_range)
-      for (int k = 0; k < g->domains[i].value_count; ++k)
-        if (g->values[g->domains[i].value_offset + k].tag != GAGP_TAG_INT)
+  for (int i = 0; i < ND; ++i) {
+    const gagp_domain& d = g->domains[i];
+    if (d.integer_range) {
+      if (d.minimum > d.maximum) return fail(GAGP_INVALID_ARGUMENT, "empty integer domain");
+    } else {
+      if (d.value_count < 1 || d.value_offset < 0 || d.value_offset > g->value_count ||
+          d.value_count > g->value_count - d.value_offset)
+        return fail(GAGP_INVALID_ARGUMENT, "domain value range");
+      for (int k = 0; k < d.value_count; ++k)
+        if (g->values[d.value_offset + k].tag != GAGP_TAG_INT)
           return fail(GAGP_DECLINED, "only Int constants are resident");
+    }
+  }
   return GAGP_OK;
 }
 
