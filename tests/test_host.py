@@ -1,0 +1,95 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports
+every function its header declares, and admission (gagp_b200_search_bytes,
+which runs on the host only) accepts the benchmark task and turns malformed
+tables into errors before any kernel could read them."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from gagp_b200 import abi, build, task as T, workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gagp_b200.h")
+
+
+def _declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gagp_b200_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    lib = C.CDLL(build.build())
+    names = _declared_functions()
+    assert len(names) > 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.fixture(scope="module")
+def poly_task(tmp_path_factory):
+    d = str(tmp_path_factory.mktemp("poly"))
+    files = W.poly4(population=256, generations=4, seed=3, cases=32, max_nodes=40)
+    return T.load(files.write(d), os.path.join(d, "search.json"))
+
+
+def _bytes(lt, edit=None, settings=None):
+    """Status and byte count of gagp_b200_search_bytes after `edit(blob)`."""
+    from gagp_b200.engine import load_library
+    blob = abi.GrammarBlob(lt.tables)
+    if edit:
+        edit(blob)
+    cfg = (settings or lt.settings).struct()
+    out = C.c_uint64(0)
+    st = load_library().gagp_b200_search_bytes(blob.ref(), lt.cases.ref(), C.byref(cfg), C.byref(out))
+    return st, out.value
+
+
+def test_admission_accepts_the_benchmark_task(poly_task):
+    st, n = _bytes(poly_task)
+    assert st == 0 and n > 0
+
+
+def _first(blob, kind):
+    return next(i for i in range(len(blob.tables.expressions)) if blob.expressions[i].kind == kind)
+
+
+@pytest.mark.parametrize("case", ["production", "reference", "child", "domain", "kind", "values"])
+def test_admission_rejects_malformed_tables(poly_task, case):
+    def edit(blob):
+        if case == "production":
+            blob.productions[0].expression = len(blob.tables.expressions) + 5
+        elif case == "reference":
+            blob.expressions[_first(blob, W_KINDS["reference"])].target = 999
+        elif case == "child":
+            e = next(i for i in range(len(blob.tables.expressions))
+                     if blob.expressions[i].kind == W_KINDS["operation"] and blob.expressions[i].arity > 0)
+            blob.expressions[e].children[0] = -3
+        elif case == "domain":
+            d = blob.domains[0]
+            d.integer_range, d.minimum, d.maximum = 1, 5, 2
+        elif case == "kind":
+            blob.expressions[0].kind = 9
+        elif case == "values":
+            d = blob.domains[0]
+            d.integer_range, d.value_offset, d.value_count = 0, 0, 0
+    st, _ = _bytes(poly_task, edit)
+    assert st == 2  # GAGP_INVALID_ARGUMENT
+
+
+def test_admission_declines_outside_the_resident_subset(poly_task):
+    def scoped(blob):
+        blob.nonterminals[0].scope_count = 1
+    assert _bytes(poly_task, scoped)[0] == 1  # GAGP_DECLINED
+    s = poly_task.settings
+    s_steady = s.steady_state
+    try:
+        s.steady_state = False
+        assert _bytes(poly_task)[0] == 1
+    finally:
+        s.steady_state = s_steady
+
+
+W_KINDS = {"operation": 0, "constant": 1, "reference": 3, "input": 4}
