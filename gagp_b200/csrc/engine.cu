@@ -139,11 +139,11 @@ namespace {
 
 enum KernelId {
   KN_INIT, KN_LOWER, KN_VM_FAST, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
-  KN_COMMIT, KN_STREAM, KN_COUNT
+  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_COUNT
 };
 const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast",
                                             "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
-                                            "k_place", "k_commit", "k_stream"};
+                                            "k_place", "k_commit", "k_stream", "k_place_levels"};
 
 cudaEvent_t take_event(gagp_engine* e) {
   if (e->event_next == e->event_pool.size()) {
@@ -453,7 +453,8 @@ struct Plan {
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
   size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_consts;
-  size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, round, hist_sum, hist_fitness,
+  size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, child_level, level_plan, round,
+      hist_sum, hist_fitness,
       hist_wrong,
       hist_nodes, hist_node, hist_cval, hist_len, counters;
   int stride, code_stride, bc_stride, stream_capacity, slots;
@@ -513,6 +514,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.stream_mod = L.take(4 * size_t(p.stream_capacity)); p.stream_head = L.take(16);
   p.round_seed = L.take(8); p.best = L.take(4); p.placed = L.take(4 * size_t(P)); p.round = L.take(16);
   p.place_state = L.take(4);
+  p.child_level = L.take(2 * size_t(B)); p.level_plan = L.take(8);
   const size_t H = size_t(cfg->generations);
   p.hist_sum = L.take(8 * H); p.hist_fitness = L.take(8 * H); p.hist_wrong = L.take(4 * H);
   p.hist_nodes = L.take(4 * H); p.hist_node = L.take(8 * S * H); p.hist_cval = L.take(8 * S * H);
@@ -765,6 +767,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.round_seed = at<uint64_t>(b, p.round_seed);
   d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
   d.place_state = at<int32_t>(b, p.place_state);
+  d.child_level = at<int16_t>(b, p.child_level); d.level_plan = at<int32_t>(b, p.level_plan);
   d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
   d.hist_wrong = at<uint32_t>(b, p.hist_wrong); d.hist_nodes = at<uint32_t>(b, p.hist_nodes);
   d.hist_node = at<uint64_t>(b, p.hist_node); d.hist_cval = at<int64_t>(b, p.hist_cval);
@@ -975,6 +978,14 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   CUDA_TRY(cudaEventRecord(e->fork, e->stream));
   CUDA_TRY(cudaStreamWaitEvent(e->side, e->fork, 0));
   { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
+  if (v.total_children >= gb::kClusterMinChildren) {
+    // the placement levels follow from the draws alone: found here, beside
+    // the variation, so the placement itself only compares and writes keys
+    Timed t(e, KN_LEVELS, e->side);
+    const int local_P = (v.max_P + gb::kPlaceCtas - 1) / gb::kPlaceCtas;
+    gb::k_place_levels<<<v.n * gb::kPlaceCtas, gb::kClusterThreads, 2 * size_t(local_P) * sizeof(int32_t) + 16,
+                         e->side>>>(v.d_desc, v.n);
+  }
   // the history entry reads only what the placement later rewrites
   { Timed t(e, KN_RECORD, e->side); gb::k_record<<<v.n, 1024, 0, e->side>>>(v.d_desc, v.n, 1); }
   CUDA_TRY(cudaEventRecord(e->join, e->side));

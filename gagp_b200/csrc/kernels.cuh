@@ -1008,83 +1008,83 @@ constexpr int kPlaceCtas = 8;
 constexpr int kClusterThreads = 1024;
 constexpr int kClusterPer = 2;
 constexpr int kClusterMinChildren = 4096;
+// Whether a round of search s is placed by the cluster (the same answer in
+// every block and in both cluster kernels of the round).
+__device__ __forceinline__ bool cluster_placement_applies(const SearchDesc& s, long long rp, long long wp) {
+  return s.replacement_size == 2 && s.B >= kClusterMinChildren && s.B <= kPlaceCtas * kClusterThreads * kClusterPer &&
+         wp - rp >= 2LL * s.B + 1;
+}
+
+// The children's two drawn members for this round, from the run generator's
+// residues (draws 2j and 2j + 1 after the read position).
+__device__ __forceinline__ uint32_t child_draws(const SearchDesc& s, int base, int j) {
+  const int cap = s.stream_capacity;
+  int p0 = base + 2 * j, p1 = p0 + 1;
+  if (p0 >= cap) p0 -= cap;
+  if (p1 >= cap) p1 -= cap;
+  return s.stream_mod[p0] | (s.stream_mod[p1] << 16);
+}
+
+// Placement levels of a round, found before the children's keys exist.  A
+// child can be placed once every earlier child that drew one of its members
+// is placed: its level is one more than the largest level among those, which
+// depends on the draws alone.  So this runs on the side stream, once the run
+// generator has topped up the stream, while the children are still being
+// varied and evaluated; k_place_cluster then only compares and writes keys,
+// level by level.  Levels are found as the placement would find them: each
+// level, every pending child claims both its members with a level-tagged
+// atomicMin on the owning block's owner word (member m lives in block
+// m % kPlaceCtas), and a child that owns both is at this level.  The owner
+// words alternate between two arrays by level parity: a thread that has
+// moved on to level L + 1 claims in the other array, so its claims never
+// disturb a slower thread still checking level L (and the array of level L
+// is claimed again only after barrier L + 1, which every check of level L
+// precedes).  The levels are therefore the exact longest-path levels,
+// whatever the timing.
+// level_plan: [0] the round + 1 the levels belong to, [1] their number.
 __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThreads, 1)
-    k_place_cluster(const SearchDesc* descs, int n) {
-  extern __shared__ __align__(16) uint64_t cl_keys[];
-  __shared__ uint64_t scan_key[32];
-  __shared__ int scan_idx[32];
-  __shared__ uint64_t cta_key[kPlaceCtas];  // block totals (read from block 0)
-  __shared__ int cta_idx[kPlaceCtas];
-  __shared__ int ready_count[3], redraw_at;
+    k_place_levels(const SearchDesc* descs, int n) {
+  extern __shared__ __align__(16) int32_t lv_owner[];
+  __shared__ int ready_count[3];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = int(cluster.block_rank());
   const SearchDesc& s = descs[blockIdx.x / kPlaceCtas];
   if (!search_live(s)) return;  // the same for every block of the cluster
-  const long long t0 = clock64();
-  const int P = s.P, B = s.B, cap = s.stream_capacity;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int P = s.P, B = s.B;
+  const int tid = threadIdx.x, lane = tid & 31;
   const long long rp = stream_ptrs(s)[0], wp = stream_ptrs(s)[1];
-  if (s.replacement_size != 2 || B < kClusterMinChildren || B > kPlaceCtas * kClusterThreads * kClusterPer ||
-      wp - rp < 2LL * B + 1) {
-    if (rank == 0 && tid == 0) *s.place_state = 0;
-    return;  // the same decision in every block
-  }
+  if (!cluster_placement_applies(s, rp, wp)) return;
   const int local_P = (P + kPlaceCtas - 1) / kPlaceCtas;
-  uint64_t* keys = cl_keys;
-  int32_t* owner = reinterpret_cast<int32_t*>(cl_keys + local_P + (local_P & 1));
-  for (int i = tid; i < local_P; i += blockDim.x) {
-    const int m = i * kPlaceCtas + rank;
-    keys[i] = m < P ? s.key[m] : ~0ULL;
-    owner[i] = 0x7fffffff;
-  }
-  int32_t* __restrict__ placed = s.placed;
-  for (int m = rank * kClusterThreads + tid; m < P; m += kPlaceCtas * kClusterThreads) placed[m] = -1;
-  if (tid == 0) {
-    ready_count[0] = ready_count[1] = ready_count[2] = 0;
-    redraw_at = 0x7fffffff;
-  }
+  for (int i = tid; i < 2 * local_P; i += blockDim.x) lv_owner[i] = 0x7fffffff;
+  if (tid == 0) ready_count[0] = ready_count[1] = ready_count[2] = 0;
   const int begin = (rank * kClusterThreads + tid) * kClusterPer;
-  const int base = int(rp % cap);
+  const int base = int(rp % s.stream_capacity);
   uint32_t cand[kClusterPer];
-  uint64_t kv[kClusterPer];  // the children's keys
   uint32_t pending = 0;
-  const uint64_t* __restrict__ ckey = s.c_key;
 #pragma unroll
   for (int t = 0; t < kClusterPer; ++t) {
-    const int j = begin + t;
     cand[t] = 0;
-    kv[t] = ~0ULL;
-    if (j < B) {
-      int p0 = base + 2 * j, p1 = p0 + 1;
-      if (p0 >= cap) p0 -= cap;
-      if (p1 >= cap) p1 -= cap;
-      cand[t] = s.stream_mod[p0] | (s.stream_mod[p1] << 16);
-      kv[t] = ckey[j];
+    if (begin + t < B) {
+      cand[t] = child_draws(s, base, begin + t);
       pending |= 1u << t;
     }
   }
-  auto owner_at = [&](int m) -> int* { return cluster.map_shared_rank(owner, m % kPlaceCtas) + m / kPlaceCtas; };
-  auto key_at = [&](int m) -> uint64_t* { return cluster.map_shared_rank(keys, m % kPlaceCtas) + m / kPlaceCtas; };
+  // owner word of member m for levels of parity `par`
+  auto owner_at = [&](int m, int par) -> int* {
+    return cluster.map_shared_rank(lv_owner, m % kPlaceCtas) + par * local_P + m / kPlaceCtas;
+  };
   int* counter0 = cluster.map_shared_rank(ready_count, 0);
+  int16_t* __restrict__ level_of = s.child_level;
   cluster.sync();
-  const long long level_start = clock64();
-  // One cluster barrier per level.  Level L claims members, passes barrier
-  // L, checks and places; a thread may then claim for level L + 1 while
-  // others still place for level L: its smaller tag never makes a level-L
-  // check succeed wrongly (it can only delay a child, which stays the
-  // earliest pending child of its members), and every level-L key write
-  // happens before barrier L + 1, ahead of every level-L+1 key read.  The
-  // level-L count is read after barrier L + 1 (slot L mod 3; the slot of
-  // level L - 1 is cleared for level L + 2 after barrier L + 1 too).
-  int left = B, levels_run = 0;
-  for (int level = 0; level <= B; ++level) {
-    ++levels_run;
-    const int tag = (0x7fff - level) << 16;
+  // one cluster barrier per level (count slots rotate as in k_place_cluster)
+  int left = B, level = 0;
+  for (; level <= B; ++level) {
+    const int tag = (0x7fff - level) << 16, par = level & 1;
 #pragma unroll
     for (int t = 0; t < kClusterPer; ++t)
       if (pending >> t & 1) {
-        atomicMin(owner_at(int(cand[t] & 0xffff)), tag | (begin + t));
-        atomicMin(owner_at(int(cand[t] >> 16)), tag | (begin + t));
+        atomicMin(owner_at(int(cand[t] & 0xffff), par), tag | (begin + t));
+        atomicMin(owner_at(int(cand[t] >> 16), par), tag | (begin + t));
       }
     cluster.sync();
     if (level > 0) {
@@ -1095,12 +1095,84 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
     uint32_t ready = 0;
 #pragma unroll
     for (int t = 0; t < kClusterPer; ++t)
-      if ((pending >> t & 1) && *owner_at(int(cand[t] & 0xffff)) == (tag | (begin + t)) &&
-          *owner_at(int(cand[t] >> 16)) == (tag | (begin + t)))
+      if ((pending >> t & 1) && *owner_at(int(cand[t] & 0xffff), par) == (tag | (begin + t)) &&
+          *owner_at(int(cand[t] >> 16), par) == (tag | (begin + t))) {
         ready |= 1u << t;
+        level_of[begin + t] = int16_t(level);
+      }
+    pending &= ~ready;
+    int placed_here = __popc(ready);
+    for (int o = 16; o; o >>= 1) placed_here += __shfl_xor_sync(kFull, placed_here, o);
+    if (lane == 0 && placed_here) atomicAdd(counter0 + level % 3, placed_here);
+  }
+  if (rank == 0 && tid == 0) {
+    s.level_plan[1] = level;  // levels 0 .. level - 1 hold every child
+    s.level_plan[0] = s.round[0] + 1;
+  }
+  cluster.sync();  // no block leaves while another may still read its shared memory
+}
+
+__global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThreads, 1)
+    k_place_cluster(const SearchDesc* descs, int n) {
+  extern __shared__ __align__(16) uint64_t cl_keys[];
+  __shared__ uint64_t scan_key[32];
+  __shared__ int scan_idx[32];
+  __shared__ uint64_t cta_key[kPlaceCtas];  // block totals (read from block 0)
+  __shared__ int cta_idx[kPlaceCtas];
+  __shared__ int redraw_at;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = int(cluster.block_rank());
+  const SearchDesc& s = descs[blockIdx.x / kPlaceCtas];
+  if (!search_live(s)) return;  // the same for every block of the cluster
+  const long long t0 = clock64();
+  const int P = s.P, B = s.B, cap = s.stream_capacity;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long long rp = stream_ptrs(s)[0], wp = stream_ptrs(s)[1];
+  // the levels come from k_place_levels, run earlier in this round
+  if (!cluster_placement_applies(s, rp, wp) || s.level_plan[0] != s.round[0] + 1) {
+    if (rank == 0 && tid == 0) *s.place_state = 0;
+    return;  // the same decision in every block
+  }
+  const int n_levels = s.level_plan[1];
+  const int local_P = (P + kPlaceCtas - 1) / kPlaceCtas;
+  uint64_t* keys = cl_keys;
+  for (int i = tid; i < local_P; i += blockDim.x) {
+    const int m = i * kPlaceCtas + rank;
+    keys[i] = m < P ? s.key[m] : ~0ULL;
+  }
+  int32_t* __restrict__ placed = s.placed;
+  for (int m = rank * kClusterThreads + tid; m < P; m += kPlaceCtas * kClusterThreads) placed[m] = -1;
+  if (tid == 0) redraw_at = 0x7fffffff;
+  const int begin = (rank * kClusterThreads + tid) * kClusterPer;
+  const int base = int(rp % cap);
+  uint32_t cand[kClusterPer];
+  uint64_t kv[kClusterPer];  // the children's keys
+  int lvl[kClusterPer];      // and placement levels
+  const uint64_t* __restrict__ ckey = s.c_key;
+#pragma unroll
+  for (int t = 0; t < kClusterPer; ++t) {
+    const int j = begin + t;
+    cand[t] = 0;
+    kv[t] = ~0ULL;
+    lvl[t] = -1;
+    if (j < B) {
+      cand[t] = child_draws(s, base, j);
+      kv[t] = ckey[j];
+      lvl[t] = s.child_level[j];
+    }
+  }
+  auto key_at = [&](int m) -> uint64_t* { return cluster.map_shared_rank(keys, m % kPlaceCtas) + m / kPlaceCtas; };
+  cluster.sync();
+  const long long level_start = clock64();
+  // Level by level: the children of level L read both members' keys, the
+  // worse member takes the child's key; a cluster barrier then makes the
+  // writes visible to level L + 1.  Children of one level draw disjoint
+  // members, so no two of them touch the same key.
+  const int levels_run = n_levels;
+  for (int level = 0; level < n_levels; ++level) {
 #pragma unroll
     for (int t = 0; t < kClusterPer; ++t)
-      if (ready >> t & 1) {
+      if (lvl[t] == level) {
         const int d0 = int(cand[t] & 0xffff), d1 = int(cand[t] >> 16);
         const uint64_t k0 = *key_at(d0), k1 = *key_at(d1);
         // worst of the pair: the second replaces the first when the first is better
@@ -1109,10 +1181,7 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
         placed[v] = begin + t;
         cand[t] = uint32_t(v);
       }
-    pending &= ~ready;
-    int placed_here = __popc(ready);
-    for (int o = 16; o; o >>= 1) placed_here += __shfl_xor_sync(kFull, placed_here, o);
-    if (lane == 0 && placed_here) atomicAdd(counter0 + level % 3, placed_here);
+    cluster.sync();
   }
   const long long level_end = clock64();
   // best member before each child: (key, victim) minimum of this thread's

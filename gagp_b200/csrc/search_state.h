@@ -148,6 +148,8 @@ struct SearchDesc {
   int32_t* best;                       // tracked best member
   int32_t* placed;                     // P: child placed into member, -1
   int32_t* place_state;                // 1: the cluster placement placed this round
+  int16_t* child_level;                // B: placement level of each child (k_place_levels)
+  int32_t* level_plan;                 // [0] round + 1 the levels belong to, [1] number of levels
   int32_t* round;                      // [0] rounds done, [1] history entries, [2] finished flag, [3] error
   int64_t* hist_sum;                   // per history entry: sum of member fitness (integral)
   double* hist_fitness; uint32_t* hist_wrong; uint32_t* hist_nodes;

@@ -96,3 +96,48 @@ def test_result_part_and_wider_rows(engine, tmp_path):
         n = int(rows.node_counts[i])
         assert (rows.origins[i, n:engine_width] == 0).all()
         assert (rows.origins[i, engine_width:] == -1).all()
+
+
+@pytest.mark.parametrize("population,seed", [(4096, 31), (8192, 32)])
+def test_cluster_placement_matches_oracle(engine, tmp_path, population, seed):
+    """Rounds of 4096 children or more are placed by the cluster kernels (the
+    placement levels found from the draws on the side stream, then applied
+    level by level): the search equals the oracle's."""
+    from gagp_b200 import task as T
+    files = W.poly4(population=population, generations=3, seed=seed, cases=24, max_nodes=40)
+    lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
+    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    s = engine.admit(lt)
+    try:
+        s.run()
+        got = s.result()
+        levels = engine.counters(s)["place_levels"]
+    finally:
+        s.close()
+    assert got["history"] == want["history"]
+    assert got["final"] == want["final"]
+    assert got["evaluated_programs"] == want["evaluated_programs"]
+    assert levels > 0
+
+
+def test_cluster_placement_batched_matches_oracle(engine, tmp_path):
+    """Two searches of 4096 children per round advanced as one batch (a level
+    cluster and a placement cluster each) equal the oracle's searches."""
+    from gagp_b200 import task as T
+    tasks, wants = [], []
+    for k, seed in enumerate((41, 42)):
+        d = tmp_path / str(k)
+        files = W.poly4(population=4096, generations=2, seed=seed, cases=20, max_nodes=40)
+        lt = T.load(files.write(str(d)), str(d / "search.json"))
+        tasks.append(lt)
+        wants.append(oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings))
+    searches = [engine.admit(t) for t in tasks]
+    try:
+        engine.run_batch(searches)
+        results = [s.result() for s in searches]
+    finally:
+        for s in searches:
+            s.close()
+    for got, want in zip(results, wants):
+        assert got["history"] == want["history"]
+        assert got["final"] == want["final"]
