@@ -824,6 +824,7 @@ struct BatchView {
   long long max_draws = 0;
   int max_code_stride = 2;
   int max_C = 1, max_inputs = 0;
+  int min_B = 1 << 30;               // the smallest round of the batch
 };
 
 gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
@@ -877,6 +878,7 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
     v->max_stride = std::max(v->max_stride, s->stride);
     v->max_code_stride = std::max(v->max_code_stride, s->desc.code_stride);
     v->max_draws = std::max(v->max_draws, (long long)s->B * s->desc.replacement_size + 1);
+    v->min_B = std::min(v->min_B, s->B);
   }
   return ensure_lists(e, size_t(std::max(v->total_members, v->total_children)));
 }
@@ -1023,7 +1025,12 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
       CUDA_TRY(cudaStreamWaitEvent(e->stream, e->chunk_done[c], 0));
     }
   }
-  { Timed t(e, KN_CHILD); gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n); }
+  // rounds of kClusterMinChildren or more children get their results from
+  // the cluster placement itself
+  if (v.min_B < gb::kClusterMinChildren) {
+    Timed t(e, KN_CHILD);
+    gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n);
+  }
   {
     Timed t(e, KN_PLACE);
     // member keys plus as many 16-bit staged draws as fit (B * replacement + slack)
@@ -1039,7 +1046,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     gb::k_place_cluster<<<v.n * gb::kPlaceCtas, gb::kClusterThreads, cluster_bytes, e->stream>>>(v.d_desc, v.n);
     gb::k_place<<<v.n, gb::kPlaceThreads, bytes, e->stream>>>(v.d_desc, v.n, int(bytes), 1);
   }
-  { Timed t(e, KN_COMMIT); gb::k_commit<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
+  { Timed t(e, KN_COMMIT); gb::k_commit<<<blocks_for(size_t(v.total_members) * gb::kCommitLanes, 256), 256, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
 }
 

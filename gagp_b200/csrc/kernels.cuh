@@ -480,22 +480,26 @@ __global__ void k_status(const SearchDesc* descs, int n, int32_t* out) {
   out[i] = (s.round[2] ? 1 : 0) | (s.round[3] ? 2 : 0);
 }
 
-// Results of all children before any placement (evolve.cpp:403-413).
-__global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int n) {
-  const int item = blockIdx.x * blockDim.x + threadIdx.x;
-  if (item >= off[n]) return;
-  const int si = find_search(off, n, item);
-  const SearchDesc& s = descs[si];
-  if (!search_live(s)) return;
-  const int b = item - off[si];
+// Cluster placement shape (k_place_levels, k_place_cluster): kPlaceCtas
+// blocks of kClusterThreads threads, kClusterPer children per thread, for
+// rounds of at least kClusterMinChildren children.
+constexpr int kPlaceCtas = 8;
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterPer = 2;
+constexpr int kClusterMinChildren = 4096;
+
+// A child's result and ranking key before any placement (evolve.cpp:403-413):
+// an unchanged genotype takes its parent's.  Returns the key; reports a
+// reuse through `reused`.
+__device__ inline uint64_t child_result_of(const SearchDesc& s, int b, bool* reused) {
   const int source = s.c_reuse[b];
   double f;
   uint32_t w, nodes;
+  *reused = source >= 0;
   if (source >= 0) {
     f = s.fitness[source];
     w = s.wrong[source];
     nodes = s.nodes[source];
-    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[1]), 1ULL);
   } else {
     f = s.c_fitness[b];
     w = s.c_wrong[b];
@@ -504,8 +508,29 @@ __global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int
   s.c_fitness[b] = f;
   s.c_wrong[b] = w;
   s.c_nodes[b] = nodes;
-  s.c_key[b] = pack_key(s, f, w, nodes);
+  const uint64_t key = pack_key(s, f, w, nodes);
+  s.c_key[b] = key;
+  return key;
 }
+__device__ inline void child_result(const SearchDesc& s, int b) {
+  bool reused;
+  child_result_of(s, b, &reused);
+  if (reused) atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[1]), 1ULL);
+}
+
+// Results of all children before any placement, thread per child, for
+// rounds that the single-block placement takes.
+__global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int n) {
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= off[n]) return;
+  const int si = find_search(off, n, item);
+  const SearchDesc& s = descs[si];
+  if (!search_live(s)) return;
+  if (s.B >= kClusterMinChildren) return;  // the cluster placement forms these
+  const int b = item - off[si];
+  child_result(s, b);
+}
+
 
 // Windowed placement step over lanes [seg_begin, seg_end) of a window whose
 // children's draws do not overlap (every lane's members differ from every
@@ -1004,10 +1029,6 @@ __global__ void __launch_bounds__(kPlaceThreads, 1) k_place(const SearchDesc* de
 // k_place (place_state 0), whose single block is then as fast.  On success
 // this kernel finishes the round as k_place does (statistics, best member,
 // stream position, next seed).
-constexpr int kPlaceCtas = 8;
-constexpr int kClusterThreads = 1024;
-constexpr int kClusterPer = 2;
-constexpr int kClusterMinChildren = 4096;
 // Whether a round of search s is placed by the cluster (the same answer in
 // every block and in both cluster kernels of the round).
 __device__ __forceinline__ bool cluster_placement_applies(const SearchDesc& s, long long rp, long long wp) {
@@ -1128,6 +1149,26 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   const int P = s.P, B = s.B, cap = s.stream_capacity;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long rp = stream_ptrs(s)[0], wp = stream_ptrs(s)[1];
+  // the children's results and keys (k_child_results leaves rounds of this
+  // size to this kernel), formed before any decision so that the single-block
+  // placement finds them too
+  const int begin = (rank * kClusterThreads + tid) * kClusterPer;
+  uint64_t kv[kClusterPer];  // the children's keys
+  if (B >= kClusterMinChildren) {
+    int reused_here = 0;
+#pragma unroll
+    for (int t = 0; t < kClusterPer; ++t) {
+      kv[t] = ~0ULL;
+      if (begin + t < B) {
+        bool reused;
+        kv[t] = child_result_of(s, begin + t, &reused);
+        reused_here += reused;
+      }
+    }
+    for (int o = 16; o; o >>= 1) reused_here += __shfl_xor_sync(kFull, reused_here, o);
+    if (lane == 0 && reused_here)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[1]), (unsigned long long)reused_here);
+  }
   // the levels come from k_place_levels, run earlier in this round
   if (!cluster_placement_applies(s, rp, wp) || s.level_plan[0] != s.round[0] + 1) {
     if (rank == 0 && tid == 0) *s.place_state = 0;
@@ -1143,21 +1184,16 @@ __global__ void __cluster_dims__(kPlaceCtas, 1, 1) __launch_bounds__(kClusterThr
   int32_t* __restrict__ placed = s.placed;
   for (int m = rank * kClusterThreads + tid; m < P; m += kPlaceCtas * kClusterThreads) placed[m] = -1;
   if (tid == 0) redraw_at = 0x7fffffff;
-  const int begin = (rank * kClusterThreads + tid) * kClusterPer;
   const int base = int(rp % cap);
   uint32_t cand[kClusterPer];
-  uint64_t kv[kClusterPer];  // the children's keys
-  int lvl[kClusterPer];      // and placement levels
-  const uint64_t* __restrict__ ckey = s.c_key;
+  int lvl[kClusterPer];  // the children's placement levels
 #pragma unroll
   for (int t = 0; t < kClusterPer; ++t) {
     const int j = begin + t;
     cand[t] = 0;
-    kv[t] = ~0ULL;
     lvl[t] = -1;
     if (j < B) {
       cand[t] = child_draws(s, base, j);
-      kv[t] = ckey[j];
       lvl[t] = s.child_level[j];
     }
   }
@@ -1345,8 +1381,10 @@ __global__ void k_export_members(const SearchDesc* desc, const int32_t* rank, in
 
 // commit_batch (phase_population_cpu.cpp:382-394): placed child rows replace
 // members.  Thread per member.
+constexpr int kCommitLanes = 16;  // threads per member row
 __global__ void k_commit(const SearchDesc* descs, const int32_t* off, int n) {
-  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t gid = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int item = int(gid / kCommitLanes), lane = int(gid % kCommitLanes);
   if (item >= off[n]) return;
   const int si = find_search(off, n, item);
   const SearchDesc& s = descs[si];
@@ -1354,14 +1392,15 @@ __global__ void k_commit(const SearchDesc* descs, const int32_t* off, int n) {
   const int m = item - off[si];
   const int b = s.placed[m];
   if (b < 0) return;
+  // the row's threads copy consecutive slots: coalesced reads and writes
   const int32_t l = s.clen[b];
   const uint64_t* from = s.cnode + size_t(b) * s.stride;
   const int64_t* cfrom = s.ccval + size_t(b) * s.stride;
   uint64_t* to = s.node + size_t(m) * s.stride;
   int64_t* cto = s.cval + size_t(m) * s.stride;
-  for (int i = 0; i < len_nodes(l); ++i) to[i] = from[i];
-  for (int i = 0; i < len_consts(l); ++i) cto[i] = cfrom[i];
-  s.len[m] = l;
+  for (int i = lane; i < len_nodes(l); i += kCommitLanes) to[i] = from[i];
+  for (int i = lane; i < len_consts(l); i += kCommitLanes) cto[i] = cfrom[i];
+  if (lane == 0) s.len[m] = l;
 }
 
 }  // namespace gb
