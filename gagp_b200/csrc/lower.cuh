@@ -155,8 +155,9 @@ struct LowerScratch {
   int16_t end[kMaxLowerNodes];    // one past the subtree
   int16_t size[kMaxLowerNodes];   // code words of the subtree
   int16_t start[kMaxLowerNodes];  // open slots before the node, then the subtree's first code word
-  int8_t temp_base[kMaxLowerNodes];
-  uint8_t depth[kMaxLowerNodes];  // non-leaf depth (root 1; 0: not yet placed)
+  int16_t temp_base[kMaxLowerNodes];
+  int16_t depth[kMaxLowerNodes];  // non-leaf depth (root 1)
+  int16_t anc[kMaxLowerNodes];    // pointer jumping: the ancestor the sums reach (-1: the root)
   uint32_t leaf[kMaxLowerNodes];  // leaves: operand kind << 16 | index
 };
 
@@ -212,7 +213,7 @@ __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code
   uint32_t pend = 0;  // bit k: node lane + 32 k not yet computed
   for (int k = 0; lane + 32 * k < n; ++k) {
     const int i = lane + 32 * k;
-    m.depth[i] = 0;
+    m.anc[i] = -2;  // no parent yet
     if (m.arity[i] == 0) { m.need[i] = 0; m.size[i] = 0; }
     else { m.need[i] = -1; pend |= 1u << k; }
   }
@@ -282,87 +283,130 @@ __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code
   }
   const int total = m.size[0];
   if (total > code_cap) return -1;
-  // ---- top-down: code positions, temporaries and depth; each node writes its words
-  pend = 0;
-  for (int k = 0; lane + 32 * k < n; ++k)
-    if (m.arity[lane + 32 * k]) pend |= 1u << k;
-  if (lane == 0) { m.start[0] = 0; m.temp_base[0] = 0; m.depth[0] = 1; }
-  __syncwarp();
-  while (__any_sync(kFull, pend != 0)) {
-    uint32_t ready = 0;
-    for (uint32_t b = pend; b; b &= b - 1) {
-      const int k = __ffs(b) - 1;
-      if (m.depth[lane + 32 * k]) ready |= 1u << k;
-    }
-    __syncwarp();
-    if (!__any_sync(kFull, ready != 0)) { fail = true; break; }
-    for (uint32_t b = ready; b; b &= b - 1) {
-      const int k = __ffs(b) - 1, i = lane + 32 * k, a = m.arity[i];
-      if (m.depth[i] >= 65) fail = true;  // the 65th nested frame overflows the 64-frame stack
-      const int ob = m.order[i], count = ob >> 6, tb = m.temp_base[i];
-      const int o0 = ob & 3, o1 = (ob >> 2) & 3, o2 = (ob >> 4) & 3;
-      const int c0 = i + 1, c1 = a > 1 ? m.end[c0] : 0, c2 = a > 2 ? m.end[c1] : 0;
-      auto child_at = [&](int x) { return x == 0 ? c0 : x == 1 ? c1 : c2; };
-      const int child_depth = min(int(m.depth[i]) + 1, 255);
-      int pos = m.start[i];
+  // ---- top-down: code positions, temporaries and depth.  Each is a sum
+  // along the path from the root (a child's code starts after its earlier
+  // evaluated siblings' code and spills, its temporaries after its
+  // position's, one level deeper), so every non-leaf node first records its
+  // children's offsets from itself, then pointer jumping adds up the paths
+  // in about log2(depth) rounds instead of one sweep per level.
+  if (lane == 0) { m.start[0] = 0; m.temp_base[0] = 0; m.depth[0] = 1; m.anc[0] = -1; }
+  for (int i = lane; i < n; i += 32) {
+    const int a = m.arity[i];
+    if (!a) continue;
+    const int ob = m.order[i], count = ob >> 6;
+    const int o0 = ob & 3, o1 = (ob >> 2) & 3, o2 = (ob >> 4) & 3;
+    const int c0 = i + 1, c1 = a > 1 ? m.end[c0] : 0, c2 = a > 2 ? m.end[c1] : 0;
+    int rel = 0;
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        if (q < count) {
-          const int c = child_at(q == 0 ? o0 : q == 1 ? o1 : o2);
-          if (q > 0) {
-            const int temp = tb + q - 1;
-            if (temp >= kMaxTemps) fail = true;
-            else code[pos] = a_instr(A_SPILL, false, K_TEMP, uint32_t(temp));
-            ++pos;
-          }
-          m.start[c] = int16_t(pos);
-          m.temp_base[c] = int8_t(tb + q);
-          m.depth[c] = uint8_t(child_depth);
-          pos += m.size[c];
-        }
-      }
-      const uint32_t op = m.aop[i];
-      const int last = count == 1 ? o0 : count == 2 ? o1 : count == 3 ? o2 : -1;
-      uint32_t kind0 = K_ACC, kind1 = K_ACC, kind2 = K_ACC, id0 = 0, id1 = 0, id2 = 0;
-#pragma unroll
-      for (int x = 0; x < 3; ++x) {
-        if (x < a) {
-          const int c = child_at(x);
-          uint32_t kind = K_ACC, id = 0;
-          if (m.end[c] - c == 1) {
-            const uint32_t leaf = m.leaf[c];
-            kind = leaf >> 16;
-            id = leaf & 0xffffu;
-          } else if (x != last) {
-            // a spilled non-leaf child: the temporary of its evaluation slot
-            kind = K_TEMP;
-            if (count > 1 && o0 == x) id = uint32_t(tb);
-            else if (count > 2 && o1 == x) id = uint32_t(tb + 1);
-          }
-          if (x == 0) { kind0 = kind; id0 = id; }
-          else if (x == 1) { kind1 = kind; id1 = id; }
-          else { kind2 = kind; id2 = id; }
-        }
-      }
-      if (a == 1) {
-        if (kind0 != K_ACC) code[pos++] = a_instr(A_MOV, false, kind0, id0);
-        code[pos] = a_instr(op, false, K_ACC, 0);
-      } else if (a == 2) {
-        if (kind0 != K_ACC && kind1 != K_ACC) {
-          code[pos++] = a_instr(A_MOV, false, kind0, id0);
-          code[pos] = a_instr(op, false, kind1, id1);
-        } else if (kind0 == K_ACC) {
-          code[pos] = a_instr(op, false, kind1, id1);
-        } else {
-          code[pos] = a_instr(op, true, kind0, id0);  // acc = op(first, acc)
-        }
-      } else {
-        code[pos] = a_instr(A_SELECT, false, kind0, id0, kind1, id1, kind2, id2);
+    for (int q = 0; q < 3; ++q) {
+      if (q < count) {
+        const int x = q == 0 ? o0 : q == 1 ? o1 : o2;
+        const int c = x == 0 ? c0 : x == 1 ? c1 : c2;
+        rel += q > 0;  // the spill before every child but the first
+        m.start[c] = int16_t(rel);
+        m.temp_base[c] = int16_t(q);
+        m.depth[c] = 1;
+        m.anc[c] = int16_t(i);
+        rel += m.size[c];
       }
     }
-    pend &= ~ready;
-    __syncwarp();
   }
+  __syncwarp();
+  for (int i = lane; i < n; i += 32)
+    if (m.arity[i] && m.anc[i] == -2) fail = true;  // unreachable from the root
+  if (__any_sync(kFull, fail)) return -1;
+  // pointer jumping: node += ancestor, ancestor = ancestor's ancestor; a read
+  // and a write step per node slot, so every read sees a consistent pair
+  for (int round = 0; round < 10; ++round) {
+    bool more = false;
+    for (int base = 0; base < n; base += 32) {
+      const int i = base + lane;
+      const bool live = i < n && m.arity[i] && m.anc[i] >= 0;
+      int s2 = 0, t2 = 0, d2 = 0, a2 = -1;
+      if (live) {
+        const int a = m.anc[i];
+        s2 = m.start[a];
+        t2 = m.temp_base[a];
+        d2 = m.depth[a];
+        a2 = m.anc[a];
+      }
+      __syncwarp();
+      if (live) {
+        m.start[i] = int16_t(m.start[i] + s2);
+        m.temp_base[i] = int16_t(min(m.temp_base[i] + t2, 32767));
+        m.depth[i] = int16_t(min(m.depth[i] + d2, 32767));
+        m.anc[i] = int16_t(a2);
+        more |= a2 >= 0;
+      }
+      __syncwarp();
+    }
+    if (!__any_sync(kFull, more)) break;
+  }
+  for (int i = lane; i < n; i += 32)
+    if (m.arity[i] && m.anc[i] >= 0) fail = true;  // deeper than 2^10 levels: impossible for admitted rows
+  // ---- every non-leaf node writes its spills and its own words
+  for (int i = lane; i < n; i += 32) {
+    const int a = m.arity[i];
+    if (!a) continue;
+    if (m.depth[i] >= 65) fail = true;  // the 65th nested frame overflows the 64-frame stack
+    const int ob = m.order[i], count = ob >> 6, tb = m.temp_base[i];
+    const int o0 = ob & 3, o1 = (ob >> 2) & 3, o2 = (ob >> 4) & 3;
+    const int c0 = i + 1, c1 = a > 1 ? m.end[c0] : 0, c2 = a > 2 ? m.end[c1] : 0;
+    auto child_at = [&](int x) { return x == 0 ? c0 : x == 1 ? c1 : c2; };
+    int pos = m.start[i];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      if (q < count) {
+        const int c = child_at(q == 0 ? o0 : q == 1 ? o1 : o2);
+        if (q > 0) {
+          const int temp = tb + q - 1;
+          if (temp >= kMaxTemps) fail = true;
+          else code[pos] = a_instr(A_SPILL, false, K_TEMP, uint32_t(temp));
+          ++pos;
+        }
+        pos += m.size[c];
+      }
+    }
+    const uint32_t op = m.aop[i];
+    const int last = count == 1 ? o0 : count == 2 ? o1 : count == 3 ? o2 : -1;
+    uint32_t kind0 = K_ACC, kind1 = K_ACC, kind2 = K_ACC, id0 = 0, id1 = 0, id2 = 0;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      if (x < a) {
+        const int c = child_at(x);
+        uint32_t kind = K_ACC, id = 0;
+        if (m.end[c] - c == 1) {
+          const uint32_t leaf = m.leaf[c];
+          kind = leaf >> 16;
+          id = leaf & 0xffffu;
+        } else if (x != last) {
+          // a spilled non-leaf child: the temporary of its evaluation slot
+          kind = K_TEMP;
+          if (count > 1 && o0 == x) id = uint32_t(tb);
+          else if (count > 2 && o1 == x) id = uint32_t(tb + 1);
+        }
+        if (x == 0) { kind0 = kind; id0 = id; }
+        else if (x == 1) { kind1 = kind; id1 = id; }
+        else { kind2 = kind; id2 = id; }
+      }
+    }
+    if (a == 1) {
+      if (kind0 != K_ACC) code[pos++] = a_instr(A_MOV, false, kind0, id0);
+      code[pos] = a_instr(op, false, K_ACC, 0);
+    } else if (a == 2) {
+      if (kind0 != K_ACC && kind1 != K_ACC) {
+        code[pos++] = a_instr(A_MOV, false, kind0, id0);
+        code[pos] = a_instr(op, false, kind1, id1);
+      } else if (kind0 == K_ACC) {
+        code[pos] = a_instr(op, false, kind1, id1);
+      } else {
+        code[pos] = a_instr(op, true, kind0, id0);  // acc = op(first, acc)
+      }
+    } else {
+      code[pos] = a_instr(A_SELECT, false, kind0, id0, kind1, id1, kind2, id2);
+    }
+  }
+  __syncwarp();
   if (__any_sync(kFull, fail)) return -1;
   return total;
 }
