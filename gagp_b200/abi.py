@@ -208,12 +208,16 @@ class SearchSettings:
 class RowsBuffer:
     """Caller-owned transport rows (``gagp_rows``)."""
 
-    def __init__(self, count: int, stride: int):
+    def __init__(self, count: int, stride: int, fill: bool = True):
+        """``fill`` False leaves the arrays uninitialised, for rows the
+        engine writes (a search result writes every slot of its width)."""
         self.count, self.stride = count, stride
-        self.node_counts = np.zeros(count, dtype=np.int32)
-        self.origins = np.full((count, stride), -1, dtype=np.int32)
-        self.constant_counts = np.zeros(count, dtype=np.int32)
-        self.constants = np.zeros((count, stride), dtype=np.int64)
+        make = (lambda shape, dtype, value: np.full(shape, value, dtype=dtype)) if fill else \
+            (lambda shape, dtype, value: np.empty(shape, dtype=dtype))
+        self.node_counts = make(count, np.int32, 0)
+        self.origins = make((count, stride), np.int32, -1)
+        self.constant_counts = make(count, np.int32, 0)
+        self.constants = make((count, stride), np.int64, 0)
         r = Rows()
         r.count, r.stride = count, stride
         r.node_counts = _ptr(self.node_counts, C.c_int32)
@@ -253,7 +257,7 @@ class ResultBuffer:
         self.final_fitness = np.zeros(population, dtype=np.float64)
         self.final_wrong = np.zeros(population, dtype=np.int32)
         self.final_nodes = np.zeros(population, dtype=np.int32)
-        self.final_rows = RowsBuffer(population, stride)
+        self.final_rows = RowsBuffer(population, stride, fill=False)
         r = SearchResult()
         r.generations = generations
         r.history_best_fitness = _ptr(self.history_best_fitness, C.c_double)

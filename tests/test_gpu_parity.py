@@ -79,6 +79,7 @@ def test_result_part_and_wider_rows(engine, tmp_path):
         full = s.result()
         width = lt.tables.max_nodes - lt.tables.fixed_nodes
         part = abi.ResultBuffer(lt.settings.generations, 100, width + 7)
+        part.final_rows.origins[:] = -1
         _check(load_library().gagp_b200_search_result(engine.handle, s.id, part.ref()))
         again = s.result()
     finally:
