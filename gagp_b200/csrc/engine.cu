@@ -244,6 +244,10 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
   if (!g || !c || !cfg) return fail(GAGP_INVALID_ARGUMENT, "null argument");
   if (!cfg->steady_state) return fail(GAGP_DECLINED, "the device-resident loop runs the steady-state schedule");
   if (cfg->population < 1 || cfg->population > 16384) return fail(GAGP_DECLINED, "population/grammar capacity");
+  // with one member every replacement draw is the best member, which the
+  // steady-state loop redraws without end (evolve.cpp:331-441)
+  if (cfg->steady_state && cfg->population < 2)
+    return fail(GAGP_INVALID_ARGUMENT, "steady-state replacement needs at least 2 members");
   const int B = cfg->batch > 0 ? cfg->batch : cfg->population;
   if (B > cfg->population || cfg->population % B) return fail(GAGP_INVALID_ARGUMENT, "steady-state batch must divide the population");
   if (cfg->generations < 1) return fail(GAGP_INVALID_ARGUMENT, "generations must be > 0");

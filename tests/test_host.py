@@ -93,3 +93,15 @@ def test_admission_declines_outside_the_resident_subset(poly_task):
 
 
 W_KINDS = {"operation": 0, "constant": 1, "reference": 3, "input": 4}
+
+
+def test_admission_rejects_a_single_member_steady_state(poly_task):
+    """One member: every replacement draw is the best member, which the
+    steady-state loop would redraw without end; admission refuses it."""
+    s = poly_task.settings
+    old = s.population, s.batch
+    try:
+        s.population, s.batch = 1, 0
+        assert _bytes(poly_task)[0] == 2  # GAGP_INVALID_ARGUMENT
+    finally:
+        s.population, s.batch = old
