@@ -225,15 +225,34 @@ __global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mo
     wrong = warp_sum(wrong);
     if (lane == 0) {
       unsigned long long* acc = s.vm_acc + 2 * size_t(p.slot);
-      atomicAdd(&acc[0], (unsigned long long)loss);
-      __threadfence();
-      const unsigned long long before = atomicAdd(&acc[1], (unsigned long long)wrong | (1ULL << 32));
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), (unsigned long long)ops);
       const unsigned tiles = unsigned((s.C + 32 * K - 1) / (32 * K));
-      if (unsigned(before >> 32) == tiles - 1) {  // the last tile of the program
+      const uint64_t worst = s.metric == GAGP_METRIC_EXACT ? 1 : uint64_t(s.penalty_int);
+      bool last;
+      int64_t total;
+      uint32_t total_wrong;
+      if (tiles < 256 && s.C < 65536 && uint64_t(s.C) * worst < (1ULL << 40)) {
+        // loss (40 bits), wrong count (16) and finished tiles (8) of the
+        // program in one word: one atomic per tile and no fence
+        const unsigned long long mine = (unsigned long long)loss | ((unsigned long long)wrong << 40) | (1ULL << 56);
+        const unsigned long long sum = atomicAdd(&acc[0], mine) + mine;
+        last = unsigned(sum >> 56) == tiles;
+        total = int64_t(sum & ((1ULL << 40) - 1));
+        total_wrong = uint32_t((sum >> 40) & 0xffffu);
+      } else {
+        atomicAdd(&acc[0], (unsigned long long)loss);
         __threadfence();
-        const int64_t total = int64_t(atomicAdd(&acc[0], 0ULL));
-        store_result(s, mode, p.slot, total, uint32_t(before) + wrong);
+        const unsigned long long before = atomicAdd(&acc[1], (unsigned long long)wrong | (1ULL << 32));
+        last = unsigned(before >> 32) == tiles - 1;
+        total_wrong = uint32_t(before) + wrong;
+        total = 0;
+        if (last) {
+          __threadfence();
+          total = int64_t(atomicAdd(&acc[0], 0ULL));
+        }
+      }
+      if (last) {  // the last tile of the program
+        store_result(s, mode, p.slot, total, total_wrong);
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
       }
