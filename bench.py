@@ -375,16 +375,18 @@ def run_own_arm(args, rank: int, world: int, local: int):
                          "place_cycles_per_step": {k: (after[k] - before[k]) / args.steps for k in
                                                    ("place_generate_cycles", "place_stage_cycles",
                                                     "place_serial_cycles", "place_levels", "place_level_cycles")},
-                         "vary_cycles_per_child": {k: (after[k] - before[k]) / max(1, args.steps * WORKLOAD["population"])
+                         # the variation kernel's per-child statistics are
+                         # collected in the profiled rounds only
+                         "vary_stats_rounds": PROFILE_ROUNDS,
+                         "vary_cycles_per_child": {k: pdelta[k] / max(1, PROFILE_ROUNDS * WORKLOAD["population"])
                                                    for k in ("vary_select_cycles", "vary_crossover_cycles",
                                                              "vary_generate_cycles", "vary_rest_cycles")},
-                         "vary_max_child_cycles": after["vary_max_child_cycles"],
-                         "vary_max_phase_cycles": after["vary_max_phase_cycles"],
-                         "vary_slow_children": after["vary_slow_children"] - before["vary_slow_children"],
-                         "generate_steps_per_generation": (after["generate_steps"] - before["generate_steps"]) /
-                         max(1, after["generations"] - before["generations"]),
-                         "generations_per_step": (after["generations"] - before["generations"]) / args.steps,
-                         "generate_max_steps": after["generate_max_steps"]}}
+                         "vary_max_child_cycles": profiled["vary_max_child_cycles"],
+                         "vary_max_phase_cycles": profiled["vary_max_phase_cycles"],
+                         "vary_slow_children_per_step": pdelta["vary_slow_children"] / PROFILE_ROUNDS,
+                         "generate_steps_per_generation": pdelta["generate_steps"] / max(1, pdelta["generations"]),
+                         "generations_per_step": pdelta["generations"] / PROFILE_ROUNDS,
+                         "generate_max_steps": profiled["generate_max_steps"]}}
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as d:
             make_task(seed, d)

@@ -1016,7 +1016,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
       const int share = std::max(1, std::max(1, per_sm) * e->sm_count / chunks);
       const int blocks = std::min(blocks_for(hi - lo, warps), share);
       gb::k_vary<<<blocks, warps * 32, vary_smem, st>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, counts + 2, lo,
-                                                        hi);
+                                                        hi, e->profiling ? 1 : 0);
     }
     {
       Timed t(e, KN_LOWER, st);

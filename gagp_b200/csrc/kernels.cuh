@@ -225,7 +225,6 @@ __global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mo
     wrong = warp_sum(wrong);
     if (lane == 0) {
       unsigned long long* acc = s.vm_acc + 2 * size_t(p.slot);
-      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), (unsigned long long)ops);
       const unsigned tiles = unsigned((s.C + 32 * K - 1) / (32 * K));
       const uint64_t worst = s.metric == GAGP_METRIC_EXACT ? 1 : uint64_t(s.penalty_int);
       bool last;
@@ -253,6 +252,9 @@ __global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mo
       }
       if (last) {  // the last tile of the program
         store_result(s, mode, p.slot, total, total_wrong);
+        // the program's instructions over all its cases, counted once
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]),
+                  (unsigned long long)s.code_len[p.slot] * (unsigned long long)s.C);
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
       }
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(1024) k_record(const SearchDesc* descs, int n,
 // varied, so warps that drew short children go on to the next one instead
 // of idling.
 __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max,
-                                                 int32_t* next_item, int lo, int hi) {
+                                                 int32_t* next_item, int lo, int hi, int collect_stats) {
   extern __shared__ __align__(16) char smem_rows[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   char* base = smem_rows + size_t(warp) * warp_rows_bytes(stride_max);
@@ -460,10 +462,10 @@ __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const 
     const int child = item - off[si];
     WarpRows rows = carve_rows(base, s.stride);
     int reuse = -1, parent = -1;
-    long long stamp[4] = {0, 0, 0, 0};
+    long long stamp[5] = {0, 0, 0, 0, 0};
     const long long started = clock64();
     const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent, stamp);
-    if (lane == 0) {
+    if (lane == 0 && collect_stats) {
       // per-phase SM cycles: selection, crossover, subtree generation, rest
       stamp[3] = clock64();
       long long prev = started;
@@ -475,16 +477,23 @@ __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const 
       }
       atomicMax(reinterpret_cast<unsigned long long*>(&s.counters[15]), (unsigned long long)(stamp[3] - started));
       if (stamp[3] - started > 200000) atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[20]), 1ULL);
-      s.c_parent[child] = parent;
-      s.c_reuse[child] = reuse;
-      s.c_error[child] = error;
-      s.c_eval[child] = error == 0 && reuse < 0;
-      if (error) raise_error(s, 100 + error);
+      if (stamp[4]) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[21]), (unsigned long long)(stamp[4] - 1));
+        atomicMax(reinterpret_cast<unsigned long long*>(&s.counters[22]), (unsigned long long)(stamp[4] - 1));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[23]), 1ULL);
+      }
       // rows read (parent, donor) and written (child) with their lengths,
       // 2 x pressure tournament keys, four per-child outputs
       const uint64_t bytes = 8ull * (rows.parent.n + rows.parent.nc + rows.donor.n + rows.donor.nc + rows.child.n +
                                      rows.child.nc + 2 * s.pressure) + 12 + 16;
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[8]), (unsigned long long)bytes);
+    }
+    if (lane == 0) {
+      s.c_parent[child] = parent;
+      s.c_reuse[child] = reuse;
+      s.c_error[child] = error;
+      s.c_eval[child] = error == 0 && reuse < 0;
+      if (error) raise_error(s, 100 + error);
     }
     __syncwarp();
   }

@@ -81,7 +81,8 @@ __device__ inline void load_members(const SearchDesc& s, int a, SRow& to_a, int 
 // source (the parent when the genotype is unchanged) and returns the
 // reference's OperatorStats error code (0: none).  stamp[0..2]: SM clock
 // after selection, after crossover, after the mutation's subtree generation
-// (left 0 for phases not reached).
+// (left 0 for phases not reached); stamp[4]: the generation's steps + 1 on
+// lane 0 (left 0 without a generation).
 __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t seed, WarpRows& w, int* reuse_out,
                                       int* parent_out, long long* stamp) {
   const int lane = lane_id();
@@ -143,9 +144,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
         if (lane == 0) {
           g = generate(s, entry, 0, s.slot_max_depth - depth + 1, bounded, gseed, w.gen.node, w.gen.cval, logical,
                        w.pending);
-          atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[21]), (unsigned long long)g.steps);
-          atomicMax(reinterpret_cast<unsigned long long*>(&s.counters[22]), (unsigned long long)g.steps);
-          atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[23]), 1ULL);
+          stamp[4] = (long long)g.steps + 1;
         }
         g.status = __shfl_sync(kFull, g.status, 0);
         g.nodes = __shfl_sync(kFull, g.nodes, 0);

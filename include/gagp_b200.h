@@ -237,9 +237,11 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
 
 /* Work counters of a search so far: [0] program evaluations, [1] children
  * that reused a member's result, [2] evaluated (program, case) pairs,
- * [3] VM instructions executed over all cases, [4..6] SM clock cycles of
+ * [3] VM instructions executed over all cases (accumulator VM: added when
+ * a program's last case tile finishes), [4..6] SM clock cycles of
  * the placement phases (stream generation, draw staging, placement),
- * [7] placement levels (+2^20 per sequential replay), [8] bytes the
+ * [7] placement levels (+2^20 per sequential replay), [8] and [10..23]
+ * only while kernel profiling is on (gagp_b200_engine_profile): [8] bytes the
  * variation kernel moved (parent, donor and child rows, tournament keys,
  * per-child outputs), [9] bytes the lowering kernel moved (rows read, code
  * and constants written), [10..13] SM clock cycles of the variation warps
