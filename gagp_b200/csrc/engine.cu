@@ -173,6 +173,9 @@ struct Timed {
 // Adds the elapsed times of completed launches (after a stream sync).
 // Fast-VM cases per lane, the autotuner's candidates.
 constexpr int kVmLanes[3] = {1, 2, 4};
+// rounds the VM autotuner times per candidate, in the order 1, 2, 4, 4, 2, 1
+// cases per lane (so that a drift over the first rounds favours none)
+constexpr int kTuneRounds = 2;
 
 void harvest(gagp_engine* e) {
   for (const auto& p : e->pending) {
@@ -193,7 +196,9 @@ void harvest(gagp_engine* e) {
   }
   for (const auto& m : e->tune_marks) {
     auto& t = e->vm_tune[m.key];
-    if (t.chosen >= 0 || t.pending > 0 || !t.rounds[0] || !t.rounds[1] || !t.rounds[2]) continue;
+    if (t.chosen >= 0 || t.pending > 0 || t.rounds[0] < kTuneRounds || t.rounds[1] < kTuneRounds ||
+        t.rounds[2] < kTuneRounds)
+      continue;
     int best = 0;
     for (int c = 1; c < 3; ++c)
       if (t.ms[c] / t.rounds[c] < t.ms[best] / t.rounds[best]) best = c;
@@ -918,14 +923,13 @@ VmPlan plan_vm(gagp_engine* e, const BatchView& v, bool may_measure) {
   if (t.chosen >= 0) { p.lanes = kVmLanes[t.chosen]; return p; }
   p.lanes = v.max_lanes;  // the heuristic until the candidates are timed
   if (!may_measure || e->profiling) return p;
-  for (int c = 0; c < 3; ++c)
-    if (!t.rounds[c]) {
-      p.lanes = kVmLanes[c];
-      p.cand = c;
-      p.measure_key = key;
-      ++t.rounds[c];
-      return p;
-    }
+  const int n = t.rounds[0] + t.rounds[1] + t.rounds[2];
+  if (n >= 3 * kTuneRounds) return p;
+  const int c = (n / 3) % 2 == 0 ? n % 3 : 2 - n % 3;
+  p.lanes = kVmLanes[c];
+  p.cand = c;
+  p.measure_key = key;
+  ++t.rounds[c];
   return p;
 }
 
@@ -1111,7 +1115,7 @@ gagp_status launch_rounds(gagp_engine* e, const BatchView& v, int rounds) {
   }
   // an untuned batch shape times its VM candidates on the first rounds
   int r = 0;
-  while (r < rounds && e->vm_tune[vm_key(v.max_C, v.max_inputs)].chosen < 0 && r < 3) {
+  while (r < rounds && e->vm_tune[vm_key(v.max_C, v.max_inputs)].chosen < 0 && r < 3 * kTuneRounds) {
     const gagp_status st = launch_round(e, v);
     if (st != GAGP_OK) return st;
     ++r;
