@@ -395,8 +395,17 @@ def run_own_arm(args, rank: int, world: int, local: int):
 
 
 def _mix_tasks(entries):
-    cache = {}
-    return [T.from_files(m["files"], cache) for m in entries if m["files"] is not None]
+    """The loaded tasks of the mix entries this engine admits, and how many
+    it declined at admission (the list programs: the grammar compiler raises
+    the reference's resident-admission decline for them)."""
+    from gagp_b200 import grammar as G
+    cache, tasks, declined = {}, [], 0
+    for m in entries:
+        try:
+            tasks.append(T.from_files(W.mix_files(m), cache))
+        except G.Declined:
+            declined += 1
+    return tasks, declined
 
 
 def run_batch_workload(args, rank: int, world: int):
@@ -409,8 +418,7 @@ def run_batch_workload(args, rank: int, world: int):
     dist = init_ranks(world, rank_info()[2])
     build.build()
     mix = W.batch_mix(64)
-    declined = sum(1 for m in mix if m["files"] is None)
-    tasks = _mix_tasks(shard(mix, rank, world))
+    tasks, declined = _mix_tasks(shard(mix, rank, world))
     with Engine(rank_info()[2] if world > 1 else 0) as eng:
         # warm-up: driver and modules (two searches run), and the engine's
         # memory pool grown to the batch's size (every search admitted and
@@ -451,8 +459,9 @@ def run_batch_workload(args, rank: int, world: int):
     line = {"metric": "searches/s", "value": n / batch_s, "unit": "searches/s", "n_gpus": world, "steps": 1,
             "warmup": 1, "ms_per_step": 1000.0 * (t2 - t1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": "batch of the scalar searches of a 64-search mix (populations log-uniform "
-                                   "256..8192, 16..1000 cases, 64 generations, seeds 0..63)",
+            "config": {"workload": "batch of the admitted (scalar) searches of a 64-search mix (populations "
+                                   "log-uniform 256..8192, 16..1000 cases, 64 generations, seeds 0..63; the list "
+                                   "programs are declined at admission)",
                        "searches": int(n), "declined_list_searches": declined,
                        "parallelism": "searches sharded round-robin over %d GPUs" % world if world > 1 else "single-gpu"},
             "e2e": {"value": n / e2e_s, "unit": "searches/s", "seconds": e2e_s},
@@ -474,8 +483,7 @@ def run_serve_workload(args, rank: int, world: int):
     from gagp_b200.engine import Engine, Server
     build.build()
     mix = W.serving_mix(args.requests, seed=0)
-    entries = [m for m in mix if m["files"] is not None]
-    tasks = _mix_tasks(entries)
+    tasks, declined = _mix_tasks(mix)
     rng = random.Random(12345)
     arrivals, t = [], 0.0
     for _ in tasks:
@@ -539,10 +547,11 @@ def run_serve_workload(args, rank: int, world: int):
     line = {"metric": "searches/s", "value": n / makespan, "unit": "searches/s", "n_gpus": 1, "steps": n,
             "warmup": 1, "ms_per_step": 1000.0 * makespan / n, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": "open-loop Poisson stream of the scalar requests of a %d-request serving mix "
-                                   "(populations log-uniform 256..16384, 16..2000 cases, 32..128 generations)"
+            "config": {"workload": "open-loop Poisson stream of the admitted (scalar) requests of a %d-request "
+                                   "serving mix (populations log-uniform 256..16384, 16..2000 cases, 32..128 "
+                                   "generations; the list-program requests are declined at admission)"
                                    % args.requests,
-                       "requests": n, "declined_list_requests": args.requests - n, "arrival_rate_per_s": args.rate,
+                       "requests": n, "declined_list_requests": declined, "arrival_rate_per_s": args.rate,
                        "parallelism": "single-gpu"},
             "latency_s": {"p50": pct(0.5), "p99": pct(0.99), "max": latencies[-1]},
             "program_cases_per_s": evals / makespan, "peak_running": peak_running,

@@ -16,6 +16,13 @@ Workloads:
   U{-5..5} from the seed; train x ~ U{-100..100}; grammar x, constants
   -2..3, add/sub/mul/idiv0/imod0 and if(lt(E,E),E,E); max 64 nodes, depth 16,
   fuel 1000.
+* ``list_threshold`` -- list programs with a loop: xs an IntList of length
+  U{0..50} with elements U[-1000, 1000] and a threshold t ~ U{-100..100};
+  the target is the sum of the elements above t, their count, or the
+  maximum (0 for an empty list); the grammar folds xs with a traversal
+  whose step (binders element, index, accumulator) adds, subtracts and
+  compares.  This engine declines these grammars at admission; the
+  reference runs them resident.
 
 Inputs are generated with ``random.Random(seed)``.
 """
@@ -143,26 +150,103 @@ def poly4(population: int = 16384, generations: int = 128, seed: int = 0, cases:
         search=search_config(population, generations, seed))
 
 
+LIST_TARGETS = ("threshold_sum", "threshold_count", "max")
+
+
+def list_threshold_grammar(max_nodes: int = 48, max_depth: int = 12, fuel: int = 4096) -> dict:
+    """The list grammar: a fold of xs whose step sees the element, its index
+    and the accumulator, plus the threshold input t."""
+    step = {"ref": "Step"}
+    cmp = lambda op: {"signature": "if(Bool,Int,Int)->Int",  # noqa: E731
+                      "args": [{"signature": f"{op}(Int,Int)->Bool", "args": [step, step]}, step, step]}
+    return {
+        "format_version": "grammar-definition-v2",
+        "entry": {"nonterminal": "Top", "type": "Int"},
+        "inputs": [{"name": "xs", "type": "IntList"}, {"name": "t", "type": "Int"}],
+        "search_limits": {"max_nodes": max_nodes, "max_depth": max_depth},
+        "execution_limits": {"fuel": fuel},
+        "nonterminals": [
+            {"id": "Top", "type": "Int", "scope": [], "alternatives": [
+                {"id": "fold", "weight": 3, "expression": {
+                    "signature": "traverse(IntList,Int,Int,Int)->Int",
+                    "args": [{"input": "xs"}, {"constant": {"type": "Int", "values": ["0"]}}, {"ref": "Leaf"}, step],
+                    "bind": {"3": ["element", "index", "acc"]}}}]},
+            {"id": "Leaf", "type": "Int", "scope": [], "alternatives": [
+                {"id": "t", "weight": 1, "expression": {"input": "t"}},
+                {"id": "k", "weight": 2, "expression": {"constant": {"type": "Int", "range": ["-1", "1"]}}},
+                {"id": "len", "weight": 1, "expression": {"signature": "len(IntList)->Int",
+                                                          "args": [{"input": "xs"}]}}]},
+            {"id": "Step", "type": "Int",
+             "scope": [{"name": "element", "type": "Int"}, {"name": "index", "type": "Int"},
+                       {"name": "acc", "type": "Int"}],
+             "alternatives": [
+                 {"id": "element", "weight": 2, "expression": {"bound": "element"}},
+                 {"id": "acc", "weight": 2, "expression": {"bound": "acc"}},
+                 {"id": "t", "weight": 1, "expression": {"input": "t"}},
+                 {"id": "one", "weight": 1, "expression": {"constant": {"type": "Int", "values": ["1"]}}},
+                 {"id": "add", "weight": 2, "expression": {"signature": "add(Int,Int)->Int", "args": [step, step]}},
+                 {"id": "sub", "weight": 1, "expression": {"signature": "sub(Int,Int)->Int", "args": [step, step]}},
+                 {"id": "if_gt", "weight": 1, "expression": cmp("gt")},
+                 {"id": "if_lt", "weight": 1, "expression": cmp("lt")}]},
+        ],
+    }
+
+
+def list_target(name: str, xs: List[int], t: int) -> int:
+    if name == "threshold_sum":
+        return sum(e for e in xs if e > t)
+    if name == "threshold_count":
+        return sum(1 for e in xs if e > t)
+    return max(xs) if xs else 0
+
+
+def list_threshold(population: int = 8192, generations: int = 96, seed: int = 0, cases: int = 200,
+                   target: str = "threshold_sum", max_nodes: int = 48) -> TaskFiles:
+    rng = random.Random(seed)
+    train = []
+    for _ in range(cases):
+        xs = [rng.randint(-1000, 1000) for _ in range(rng.randint(0, 50))]
+        t = rng.randint(-100, 100)
+        train.append({"inputs": {"xs": {"type": "int_list", "value": xs}, "t": {"type": "int", "value": t}},
+                      "expected": {"type": "int", "value": list_target(target, xs, t)}})
+    return TaskFiles(name=f"list-{target}-s{seed}", grammar=list_threshold_grammar(max_nodes=max_nodes),
+                     train=train, search=search_config(population, generations, seed))
+
+
 def _log_uniform_population(rng: random.Random, lo: int, hi: int) -> int:
     # floor(lo * (hi / lo) ** u), u ~ U[0, 1)
     return int(lo * (hi / lo) ** rng.random())
+
+
+def mix_files(entry: dict) -> TaskFiles:
+    """The task files of a mix entry: built with the mix for the scalar
+    entries, on demand for the list entries (their cases are the costly part
+    and this engine declines them at admission)."""
+    if entry["files"] is None:
+        entry["files"] = make(entry["workload"], **entry["args"])
+    return entry["files"]
 
 
 def batch_mix(count: int = 64, generations: int = 64, max_population: int = 8192) -> List[dict]:
     """The batching workload: `count` independent searches with seeds 0..count-1,
     populations log-uniform in 256..max_population, case counts uniform in
     16..1000.  Even indices are scalar regressions of a random integer
-    polynomial (the large scalar grammar); odd indices are list programs, which
-    this engine declines (entry ``files`` is None for them)."""
+    polynomial (the large scalar grammar); odd indices are list programs
+    (``list_threshold``, the target cycling through threshold sum, threshold
+    count and maximum), whose files ``mix_files`` builds on demand."""
     out = []
     for i in range(count):
         rng = random.Random(1000003 * i + 17)
         population = _log_uniform_population(rng, 256, max_population)
         cases = rng.randint(16, 1000)
+        args = dict(population=population, generations=generations, seed=i, cases=cases)
         entry = {"index": i, "seed": i, "population": population, "cases": cases, "generations": generations,
                  "kind": "scalar" if i % 2 == 0 else "list", "files": None}
         if i % 2 == 0:
-            entry["files"] = poly4(population=population, generations=generations, seed=i, cases=cases)
+            entry.update(workload="poly4", args=args)
+            entry["files"] = poly4(**args)
+        else:
+            entry.update(workload="list_threshold", args=dict(args, target=LIST_TARGETS[(i // 2) % 3]))
         out.append(entry)
     return out
 
@@ -171,7 +255,8 @@ def serving_mix(count: int = 2000, seed: int = 0) -> List[dict]:
     """The serving workload: `count` requests, populations log-uniform in
     256..16384, case counts uniform in 16..2000, generations uniform in
     32..128, half scalar regressions of a random integer polynomial and half
-    list programs (declined here: entry ``files`` is None)."""
+    list programs (``list_threshold``, files built on demand by
+    ``mix_files``)."""
     rng = random.Random(seed)
     out = []
     for i in range(count):
@@ -179,15 +264,19 @@ def serving_mix(count: int = 2000, seed: int = 0) -> List[dict]:
         cases = rng.randint(16, 2000)
         generations = rng.randint(32, 128)
         scalar = rng.random() < 0.5
-        entry = {"index": i, "seed": seed * 100003 + i, "population": population, "cases": cases,
+        args = dict(population=population, generations=generations, seed=seed * 100003 + i, cases=cases)
+        entry = {"index": i, "seed": args["seed"], "population": population, "cases": cases,
                  "generations": generations, "kind": "scalar" if scalar else "list", "files": None}
         if scalar:
-            entry["files"] = poly4(population=population, generations=generations, seed=entry["seed"], cases=cases)
+            entry.update(workload="poly4", args=args)
+            entry["files"] = poly4(**args)
+        else:
+            entry.update(workload="list_threshold", args=dict(args, target=LIST_TARGETS[i % 3]))
         out.append(entry)
     return out
 
 
-WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4}
+WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4, "list_threshold": list_threshold}
 
 
 def make(name: str, **kwargs) -> TaskFiles:

@@ -105,3 +105,49 @@ def test_admission_rejects_a_single_member_steady_state(poly_task):
         assert _bytes(poly_task)[0] == 2  # GAGP_INVALID_ARGUMENT
     finally:
         s.population, s.batch = old
+
+
+def test_list_programs_are_declined_at_admission():
+    """The list workload (a traversal with element/index/accumulator binders
+    over an IntList input) is outside the resident subset: loading it raises
+    the reference's resident-admission decline."""
+    from gagp_b200 import grammar as G
+    for target in W.LIST_TARGETS:
+        files = W.list_threshold(population=64, generations=2, seed=5, cases=12, target=target)
+        with pytest.raises(G.Declined):
+            T.from_files(files, {})
+
+
+def test_mixes_carry_list_programs():
+    """Half of the batching mix and about half of the serving mix are list
+    programs, built on demand with their targets' expected values."""
+    mix = W.batch_mix(8)
+    lists = [m for m in mix if m["kind"] == "list"]
+    assert len(lists) == 4 and all(m["files"] is None for m in lists)
+    files = W.mix_files(lists[0])
+    assert files.grammar["inputs"] == [{"name": "xs", "type": "IntList"}, {"name": "t", "type": "Int"}]
+    for case in files.train:
+        xs, t = case["inputs"]["xs"]["value"], case["inputs"]["t"]["value"]
+        assert 0 <= len(xs) <= 50 and -100 <= t <= 100
+        assert case["expected"]["value"] == W.list_target(lists[0]["args"]["target"], xs, t)
+    kinds = [m["kind"] for m in W.serving_mix(200, seed=0)]
+    assert 70 < kinds.count("list") < 130
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver")),
+                    reason="the reference CPU engine is not built (make -C oracle ref)")
+def test_reference_runs_list_programs_resident(tmp_path):
+    """The reference engine admits the same list task to its resident path
+    (no decline) and searches it, so the decline above is this engine's
+    subset, not a property of the task."""
+    import json
+    import subprocess
+    files = W.list_threshold(population=64, generations=2, seed=5, cases=12)
+    task = files.write(str(tmp_path))
+    out = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "ref_driver"), "run", task, "--search",
+                          str(tmp_path / "search.json"), "--generations", "2"],
+                         check=True, capture_output=True, text=True, timeout=120).stdout
+    run = json.loads(out)
+    assert run["declined"] == ""
+    assert len(run["history"]) == 2 and run["program_cases"] > 0
+    assert run["history"][0]["text"].startswith("(traverse xs")
