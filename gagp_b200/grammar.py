@@ -30,19 +30,22 @@ from typing import Dict, List, Optional, Tuple
 NO_ID = 0xFFFFFFFF
 
 # ValueTag (cpp/include/gagp/core/value.hpp:16-27)
-TAG_INT, TAG_FLOAT, TAG_BOOL, TAG_INVALID = 0, 1, 2, 9
+TAG_INT, TAG_FLOAT, TAG_BOOL, TAG_INTLIST, TAG_INVALID = 0, 1, 2, 5, 9
 TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL}
+# with the list subset (tables only: the engine declines these grammars)
+LIST_TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL, "IntList": TAG_INTLIST}
 
 # PhaseExpressionKind (device/phase_generate.cuh:25)
 EK_OPERATION, EK_CONSTANT, EK_BOUND, EK_REFERENCE, EK_INPUT, EK_ALIAS = range(6)
 # PhaseTreeKind (device/phase_compile.cuh:21)
 TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR = range(6)
+TK_BOUND, TK_TRAVERSE = 14, 16
 # Opcode (cpp/include/gagp/core/opcode.hpp:8-37)
 OP = {"push_const": 0, "load": 1, "store": 2, "neg": 3, "not": 4, "add": 5, "sub": 6, "mul": 7,
       "div": 8, "mod": 9, "lt": 10, "le": 11, "gt": 12, "ge": 13, "eq": 14, "ne": 15, "jmp": 16,
       "jmp_if_false": 17, "jmp_if_true": 18, "call_builtin": 19, "return": 20}
 # BuiltinId (cpp/include/gagp/core/builtin.hpp:13-45)
-BUILTIN = {"abs": 0, "min": 1, "max": 2, "clip": 3, "idiv0": 13, "imod0": 14,
+BUILTIN = {"abs": 0, "min": 1, "max": 2, "clip": 3, "len": 4, "idiv0": 13, "imod0": 14,
            "trunc_div0": 28, "trunc_mod0": 29}
 
 # Scalar primitives of the catalog (cpp/src/evolution/grammar/catalog.cpp:83-116):
@@ -70,6 +73,13 @@ def _scalar_catalog() -> Dict[str, tuple]:
 
 
 CATALOG = _scalar_catalog()
+# List primitives of the table builder's list subset: the forward traversal
+# (catalog.cpp:138-141; its body argument binds element, index and state) and
+# len.  Traversal entries carry the body argument's position.
+LIST_CATALOG = {
+    "len(IntList)->Int": (("IntList",), "Int", TK_OPERATION, OP["call_builtin"], BUILTIN["len"], "len"),
+    "traverse(IntList,Int,Int,Int)->Int": (("IntList", "Int", "Int", "Int"), "Int", TK_TRAVERSE, 0, 0, "traverse"),
+}
 
 
 class Declined(ValueError):
@@ -94,6 +104,7 @@ class Expression:
     child_scope: List[int] = field(default_factory=lambda: [-1] * 8)
     name: str = ""
     result: str = ""          # grammar result type name
+    scope_map: List[int] = field(default_factory=list)  # a reference's scope positions in its environment
 
 
 @dataclass
@@ -145,7 +156,9 @@ def load_definition(path: str) -> dict:
 
 
 class _Compiler:
-    def __init__(self, doc: dict):
+    def __init__(self, doc: dict, allow_lists: bool = False):
+        self.allow_lists = allow_lists
+        self.tags = LIST_TYPE_TAGS if allow_lists else TYPE_TAGS
         if doc.get("format_version") != "grammar-definition-v2":
             raise Declined("grammar-definition-v2 required")
         for key in ("imports", "templates", "locals"):
@@ -161,8 +174,11 @@ class _Compiler:
         self.productions: List[Tuple[int, int, float]] = []  # (nonterminal, expression, weight)
         self.nt_productions: List[List[int]] = [[] for _ in rules]
 
-    def expression(self, value: dict, nt_scope: int) -> int:
+    def expression(self, value: dict, scope: List[Tuple[str, str]]) -> int:
+        """Front-end expression of ``value`` under the visible names ``scope``
+        (the nonterminal's scope, then the binders of enclosing traversals)."""
         e = Expression()
+        nt_scope = len(scope)
         if "constant" in value:
             d = value["constant"]
             if d.get("type") != "Int":
@@ -185,36 +201,68 @@ class _Compiler:
                 raise Declined("unknown input")
             idx = names.index(value["input"])
             t = self.inputs[idx][1]
-            if t not in TYPE_TAGS:
+            if t not in self.tags:
                 raise Declined("only Int/Bool inputs are resident")
             e.kind, e.node_kind, e.target = EK_INPUT, TK_LOCAL, idx
-            e.type, e.result, e.name = TYPE_TAGS[t], t, value["input"]
+            e.type, e.result, e.name = self.tags[t], t, value["input"]
         elif "ref" in value:
             if value["ref"] not in self.nt_ids:
                 raise Declined("unknown nonterminal")
             target = self.nt_ids[value["ref"]]
             rule = self.rules[target]
             if rule.get("scope"):
-                raise Declined("scoped nonterminals are outside the scalar subset")
+                if not self.allow_lists:
+                    raise Declined("scoped nonterminals are outside the scalar subset")
+                # the target's scope names select from the visible names
+                # (innermost first)
+                names = [n for n, _ in scope]
+                for slot in rule["scope"]:
+                    if slot["name"] not in names:
+                        raise Declined("scope map outside its environment")
+                    e.scope_map.append(len(names) - 1 - names[::-1].index(slot["name"]))
+                e.scope_count = len(e.scope_map)
             e.kind, e.target, e.result = EK_REFERENCE, target, rule["type"]
-            e.type = TYPE_TAGS.get(rule["type"], TAG_INVALID)
+            e.type = self.tags.get(rule["type"], TAG_INVALID)
+        elif "bound" in value and self.allow_lists:
+            names = [n for n, _ in scope]
+            if value["bound"] not in names:
+                raise Declined("bound reference outside its environment")
+            position = len(names) - 1 - names[::-1].index(value["bound"])
+            t = scope[position][1]
+            e.kind, e.node_kind, e.target = EK_BOUND, TK_BOUND, position
+            e.type, e.result, e.name = self.tags.get(t, TAG_INVALID), t, value["bound"]
         elif "signature" in value:
             sig = value["signature"]
-            if sig not in CATALOG:
+            if sig in CATALOG:
+                entry = CATALOG[sig]
+            elif self.allow_lists and sig in LIST_CATALOG:
+                entry = LIST_CATALOG[sig]
+            else:
                 raise Declined(f"primitive {sig} is outside the resident scalar subset")
-            arg_types, result, tree_kind, opcode, operand, name = CATALOG[sig]
+            arg_types, result, tree_kind, opcode, operand, name = entry
             args = value.get("args", [])
             if len(args) != len(arg_types):
                 raise Declined("argument count mismatch")
-            children = [self.expression(a, nt_scope) for a in args]
+            binds = value.get("bind", {})
+            if binds and tree_kind != TK_TRAVERSE:
+                raise Declined("binders outside a traversal are outside the table builder's list subset")
+            child_scopes = [scope] * len(args)
+            if tree_kind == TK_TRAVERSE:
+                # the body (last argument) binds element, index and state
+                body = len(args) - 1
+                names = binds.get(str(body), [])
+                if set(binds) != {str(body)} or len(names) != 3:
+                    raise Declined("traversal capability")
+                child_scopes[body] = scope + [(names[0], "Int"), (names[1], "Int"), (names[2], arg_types[2])]
+            children = [self.expression(a, child_scopes[k]) for k, a in enumerate(args)]
             for c, t in zip(children, arg_types):
                 if self.exprs[c].result != t:
                     raise Declined("argument type mismatch")
             e.kind, e.node_kind, e.opcode, e.operand = EK_OPERATION, tree_kind, opcode, operand
-            e.arity, e.type, e.result, e.name = len(children), TYPE_TAGS[result], result, name
+            e.arity, e.type, e.result, e.name = len(children), self.tags[result], result, name
             for i, c in enumerate(children):
                 e.children[i] = c
-                e.child_scope[i] = nt_scope
+                e.child_scope[i] = len(child_scopes[i])
         else:
             raise Declined("expression form outside the resident scalar subset")
         if "fuel_events" in value:
@@ -228,20 +276,30 @@ class _Compiler:
                 raise Declined("statement grammars are outside the scalar subset")
             if rule["type"] not in TYPE_TAGS:
                 raise Declined("only Int/Bool nonterminals are resident")
+            scope = [(slot["name"], slot["type"]) for slot in rule.get("scope", [])]
+            if scope and (not self.allow_lists or any(t not in self.tags for _, t in scope) or len(scope) > 8):
+                raise Declined("scoped nonterminals are outside the scalar subset")
             for alt in sorted(rule["alternatives"], key=lambda a: a["id"]):
                 w = float(alt["weight"])
                 if not (w > 0) or w == float("inf"):
                     raise Declined("production weight")
-                x = self.expression(alt["expression"], 0)
+                x = self.expression(alt["expression"], scope)
                 if self.exprs[x].result != rule["type"]:
                     raise Declined("production result type mismatch")
                 self.nt_productions[i].append(len(self.productions))
                 self.productions.append((i, x, w))
 
 
-def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_depth: int = 7) -> PhaseTables:
-    """Admit ``doc`` and build the resident tables (one whole-program slot)."""
-    c = _Compiler(doc)
+def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_depth: int = 7,
+                   allow_lists: bool = False) -> PhaseTables:
+    """Admit ``doc`` and build the resident tables (one whole-program slot).
+
+    ``allow_lists`` builds the tables of the list subset too (IntList inputs,
+    len, forward traversals with their element/index/state binders, scoped
+    nonterminals and bound names), as compile_phase_grammar does
+    (``phase_grammar.hpp:94-300``); the engine still declines these grammars
+    at admission, so only the table builder's tests use it."""
+    c = _Compiler(doc, allow_lists)
     c.compile()
     entry = doc["entry"]
     if entry.get("category", "Expression") != "Expression":
@@ -265,32 +323,57 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
     out_domains = [Domain() for _ in c.domains]
     out_values: List[Tuple[int, int]] = []
     seen_nt, seen_expr, seen_dom = set(), set(), set()
+    # lexical environments: the binder numbers visible to a nonterminal or an
+    # expression (one per scope position); binders are numbered statically,
+    # a traversal's three above every visible one
+    nt_env: Dict[int, List[int]] = {}
+    expr_env: Dict[int, List[int]] = {}
+    regions = [0]
 
-    def visit_nt(i: int):
+    def visit_nt(i: int, env: List[int]):
         if i in seen_nt:
+            if nt_env[i] != env:
+                raise Declined("nonterminal entered under two lexical environments")
             return
         seen_nt.add(i)
+        nt_env[i] = env
         out_nts[i][0] = len(out_prods)
+        out_nts[i][2] = len(c.rules[i].get("scope", []))
         for p in c.nt_productions[i]:
             _, x, w = c.productions[p]
             out_prods.append((x, w))
             out_nts[i][1] += 1
         for p in c.nt_productions[i]:
-            visit_expr(c.productions[p][1])
+            visit_expr(c.productions[p][1], env)
 
-    def visit_expr(i: int):
+    def visit_expr(i: int, env: List[int]):
         if i in seen_expr:
+            if expr_env[i] != env:
+                raise Declined("expression entered under two lexical environments")
             return
         seen_expr.add(i)
+        expr_env[i] = env
         e = c.exprs[i]
         x = out_expr[i]
         x.kind, x.type, x.target, x.name, x.result = e.kind, e.type, e.target, e.name, e.result
         if e.kind == EK_REFERENCE:
-            x.scope_count = 0
-            visit_nt(e.target)
+            x.scope_count, x.scope_map = e.scope_count, list(e.scope_map)
+            visit_nt(e.target, [env[m] for m in e.scope_map])
             return
         x.node_kind, x.opcode, x.operand, x.arity = e.node_kind, e.opcode, e.operand, e.arity
         x.children, x.child_scope = list(e.children), list(e.child_scope)
+        child_env = [env] * e.arity
+        if e.kind == EK_BOUND:
+            x.operand = env[e.target]
+        elif e.node_kind == TK_TRAVERSE:
+            binder = max(env) + 1 if env else 0
+            if binder + 2 >= 16:
+                raise Declined("traversal capability")
+            child_env[e.arity - 1] = env + [binder, binder + 1, binder + 2]
+            x.operand = regions[0]
+            regions[0] += 1
+        if len(env) > 15:
+            raise Declined("lexical environment capacity")
         if e.kind == EK_CONSTANT and e.target not in seen_dom:
             seen_dom.add(e.target)
             d = c.domains[e.target]
@@ -305,10 +388,11 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
             position = names.index(grammar_inputs[e.target])
             x.target = position
             x.operand = position
-        for ch in e.children[: e.arity]:
-            visit_expr(ch)
+        for k in range(e.arity):
+            x.child_scope[k] = len(child_env[k])
+            visit_expr(e.children[k], child_env[k])
 
-    visit_nt(root_nt)
+    visit_nt(root_nt, list(range(len(c.rules[root_nt].get("scope", [])))))
     # Productions may not share a root node and must resolve to a node.
     resolved = set()
     for x, _ in out_prods:
@@ -337,7 +421,7 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         minimum=minimum, root_expression=root_expression, depth_count=depth_count,
         logical_depth_count=logical_count, site_depth=site_depth,
         slot_max_depth=slot_max_depth, slot_type=TYPE_TAGS[c.rules[root_nt]["type"]],
-        local_types=[TYPE_TAGS[dict(c.inputs)[n]] for n in names], input_names=names,
+        local_types=[c.tags[dict(c.inputs)[n]] for n in names], input_names=names,
         max_nodes=max_nodes, fixed_nodes=4, fuel=fuel,
         names=[e.name for e in out_expr])
     _normalize_static_weights(tables)

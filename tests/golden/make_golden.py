@@ -8,7 +8,7 @@ search (``ref_driver run``: per-generation history and the final ranked
 population with fitness, wrong counts, node counts, program text and rows).
 
 Run here (the container with the reference tree):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--list-only]
 """
 from __future__ import annotations
 
@@ -45,16 +45,50 @@ CASES = [
 ]
 
 
+# List programs (traversals over an IntList): the engine declines them, so
+# these fixtures pin the table builder's list subset and hold the reference's
+# runs for the list path.  They live in golden/list/.
+LIST_CASES = [
+    ("list_threshold_sum", dict(population=64, generations=3, seed=11, cases=12, target="threshold_sum"), False),
+    ("list_threshold_count", dict(population=64, generations=3, seed=12, cases=12, target="threshold_count"), False),
+    ("list_nested_traversal", dict(population=64, generations=3, seed=13, cases=12, target="max"), True),
+]
+
+
+def nested_traversal_grammar() -> dict:
+    """The list grammar with a second traversal inside the step, whose body
+    nonterminal maps the outer accumulator and the inner binders by name
+    (binder numbers 3..5, scope map [2, 3, 5])."""
+    g = W.list_threshold_grammar()
+    step = next(r for r in g["nonterminals"] if r["id"] == "Step")
+    step["alternatives"].append({"id": "inner", "weight": 1, "expression": {
+        "signature": "traverse(IntList,Int,Int,Int)->Int",
+        "args": [{"input": "xs"}, {"constant": {"type": "Int", "values": ["0"]}}, {"bound": "acc"}, {"ref": "Inner"}],
+        "bind": {"3": ["e2", "i2", "acc2"]}}})
+    g["nonterminals"].append({"id": "Inner", "type": "Int", "scope": [
+        {"name": "acc", "type": "Int"}, {"name": "e2", "type": "Int"}, {"name": "acc2", "type": "Int"}],
+        "alternatives": [
+            {"id": "acc", "weight": 1, "expression": {"bound": "acc"}},
+            {"id": "e2", "weight": 1, "expression": {"bound": "e2"}},
+            {"id": "sum", "weight": 2, "expression": {"signature": "add(Int,Int)->Int",
+                                                      "args": [{"bound": "acc2"}, {"bound": "e2"}]}}]})
+    return g
+
+
 def driver(*args) -> dict:
     out = subprocess.run([DRIVER, *args], check=True, capture_output=True, text=True).stdout
     return json.loads(out)
 
 
 def main() -> None:
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--list-only", action="store_true", help="regenerate golden/list/ only")
+    args = ap.parse_args()
     if not os.path.exists(DRIVER):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     here = os.path.dirname(os.path.abspath(__file__))
-    for name, workload, kwargs, extra in CASES:
+    for name, workload, kwargs, extra in ([] if args.list_only else CASES):
         task = W.make(workload, **kwargs)
         task.search.update(extra)
         if name.endswith("exact_metric"):
@@ -72,6 +106,27 @@ def main() -> None:
             "run": run,
         }
         with gzip.open(os.path.join(here, name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
+    os.makedirs(os.path.join(here, "list"), exist_ok=True)
+    for name, kwargs, nested in LIST_CASES:
+        task = W.list_threshold(**kwargs)
+        if nested:
+            task.grammar = nested_traversal_grammar()
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            tables = driver("tables", tp, "--search", sp)
+            run = driver("run", tp, "--search", sp)
+        assert run["declined"] == "", (name, run["declined"])
+        fixture = {
+            "name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+            "train": task.train, "test": task.test, "search": task.search,
+            "tables": {k: v for k, v in tables.items() if k != "initial"},
+            "initial": [rows[0] for rows in tables["initial"]],
+            "run": run,
+        }
+        with gzip.open(os.path.join(here, "list", name + ".json.gz"), "wt") as f:
             json.dump(fixture, f, separators=(",", ":"))
         print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
 

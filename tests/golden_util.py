@@ -23,6 +23,20 @@ def fixture(name: str) -> dict:
         return json.load(f)
 
 
+# list-program fixtures (golden/list/): the reference's tables and runs of
+# tasks this engine declines, which pin the table builder's list subset
+LIST_HERE = os.path.join(HERE, "list")
+
+
+def list_names():
+    return sorted(os.path.basename(p)[: -len(".json.gz")] for p in glob.glob(os.path.join(LIST_HERE, "*.json.gz")))
+
+
+def list_fixture(name: str) -> dict:
+    with gzip.open(os.path.join(LIST_HERE, name + ".json.gz"), "rt") as f:
+        return json.load(f)
+
+
 def load_task(fx: dict) -> T.LoadedTask:
     files = W.TaskFiles(name=fx["task"]["name"], grammar=fx["grammar"], train=fx["train"], test=fx["test"],
                         fitness=fx["task"]["fitness"], search=fx["search"])

@@ -1,0 +1,64 @@
+"""The table builder's list subset against the reference's tables (CPU).
+
+The list programs (a traversal of an IntList with element, index and
+accumulator binders, scoped nonterminals, bound names, len) are declined at
+admission by this engine.  Their phase tables are the first piece of that
+path: ``grammar.compile_tables(..., allow_lists=True)`` must equal the
+reference's compile_phase_grammar output (phase_grammar.hpp:94-300, weights
+normalised by normalize_static_phase_weights) for the fixtures that
+tests/golden/make_golden.py records from the reference engine, including a
+nested traversal whose body maps the outer accumulator and the inner binders
+by name.
+"""
+import pytest
+
+from gagp_b200 import grammar as G
+
+import golden_util as GU
+
+NAMES = GU.list_names()
+
+
+def test_list_fixtures_exist():
+    assert len(NAMES) >= 3
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_list_tables_match_reference(name):
+    fx = GU.list_fixture(name)
+    ref = fx["tables"]
+    t = G.compile_tables(fx["grammar"], ref["inputs"], allow_lists=True)
+    slot = ref["slots"][0]
+    p = slot["profile"]
+    assert p["root_expression"] == t.root_expression
+    assert (p["depth_count"], p["logical_depth_count"]) == (t.depth_count, t.logical_depth_count)
+    assert len(p["expressions"]) == len(t.expressions)
+    for i, (re, e) in enumerate(zip(p["expressions"], t.expressions)):
+        assert re["kind"] == e.kind, i
+        assert re["node"] == [e.node_kind, e.opcode, e.operand, e.arity, e.fuel, e.merge_fuel, e.type], i
+        assert re["target"] == e.target and re["children"] == e.children, i
+        assert re["scope_count"] == e.scope_count and re["child_scope"] == e.child_scope, i
+    assert [(x, float.fromhex(w)) for x, w in p["productions"]] == t.productions
+    assert [tuple(n) for n in p["nonterminals"]] == [(a, b, c, int(d), int(e)) for a, b, c, d, e in t.nonterminals]
+    assert [tuple(d) for d in p["domains"]] == [
+        (d.value_offset, d.value_count, int(d.integer_range), d.minimum, d.maximum) for d in t.domains]
+    assert [tuple(v[:2]) for v in p["values"]] == t.values
+    assert p["minimum"] == t.minimum
+    assert slot["max_depth"] == t.slot_max_depth and slot["type"] == t.slot_type
+    assert slot["locals"] == t.local_types
+    assert ref["layout"]["fixed_nodes"] == t.fixed_nodes and ref["layout"]["max_nodes"] == t.max_nodes
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_list_tasks_run_resident_in_the_reference(name):
+    """The recorded reference runs took the resident path (no decline)."""
+    run = GU.list_fixture(name)["run"]
+    assert run["declined"] == ""
+    assert len(run["history"]) == 3 and run["history"][0]["text"].startswith("(traverse xs")
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_list_tables_are_declined_without_the_list_subset(name):
+    fx = GU.list_fixture(name)
+    with pytest.raises(G.Declined):
+        G.compile_tables(fx["grammar"], fx["tables"]["inputs"])
