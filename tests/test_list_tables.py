@@ -62,3 +62,24 @@ def test_list_tables_are_declined_without_the_list_subset(name):
     fx = GU.list_fixture(name)
     with pytest.raises(G.Declined):
         G.compile_tables(fx["grammar"], fx["tables"]["inputs"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_list_initial_population_matches_reference(name):
+    """The oracle's generator (generate_phase_initial_population restated)
+    over the list tables reproduces the reference's initial rows: scoped
+    references, bound leaves and traversal bodies need nothing beyond the
+    tables."""
+    from gagp_b200 import abi, task as T
+    from oracle import oracle
+    fx = GU.list_fixture(name)
+    t = G.compile_tables(fx["grammar"], fx["tables"]["inputs"], allow_lists=True)
+    s = T.SearchSettings()
+    T.apply_search(s, T.DEFAULT_SEARCH)
+    T.apply_search(s, fx["search"])
+    rows = oracle.initial_population(abi.GrammarBlob(t), s)
+    assert len(fx["initial"]) == s.population
+    for i, ref in enumerate(fx["initial"]):
+        origins, constants = rows.row(i)
+        assert list(origins) == ref["origins"], i
+        assert list(constants) == [c[1] for c in ref["constants"]], i
