@@ -574,6 +574,52 @@ typedef struct {
   Instr* code; Val* consts; int code_cap, const_cap;
   int status, code_count, const_count, stack_bound, stack;
 } Emit;
+/* Exact-identity reuse of any current member's result (the CPU owner's
+ * member_hashes lookup, phase_population_cpu.cpp:318-320,341-344, with
+ * hash_program / equal_program of parent_fitness_cache.cuh:15-43): a child
+ * whose genotype equals some member's takes that member's completed result.
+ * The hash only chooses candidates; equality of every field decides. */
+static uint64_t fnv_mix(uint64_t h, uint64_t x) { return (h ^ x) * 0x100000001b3ULL; }
+static uint64_t row_hash(const View* t) {
+  uint64_t h = 0xcbf29ce484222325ULL;
+  h = fnv_mix(fnv_mix(h, (uint64_t)t->node_count), (uint64_t)t->constant_count);
+  for (int i = 0; i < t->node_count; ++i) {
+    const Node* n = &t->nodes[i];
+    h = fnv_mix(h, (unsigned)n->kind); h = fnv_mix(h, (unsigned)n->opcode); h = fnv_mix(h, (uint64_t)(int64_t)n->operand);
+    h = fnv_mix(h, (uint64_t)(int64_t)n->arity); h = fnv_mix(h, n->fuel); h = fnv_mix(h, n->merge_fuel);
+    h = fnv_mix(h, (uint64_t)(int64_t)t->origins[i]);
+  }
+  for (int i = 0; i < t->constant_count; ++i) {
+    const Val* v = &t->constants[i];
+    h = fnv_mix(h, (unsigned)v->tag); h = fnv_mix(h, (uint64_t)v->i); h = fnv_mix(h, (uint64_t)(int64_t)v->b);
+  }
+  return h;
+}
+static int rows_equal(const View* x, const View* y) {
+  if (x->node_count != y->node_count || x->constant_count != y->constant_count) return 0;
+  for (int i = 0; i < x->node_count; ++i) {
+    const Node* u = &x->nodes[i]; const Node* v = &y->nodes[i];
+    if (u->kind != v->kind || u->opcode != v->opcode || u->operand != v->operand || u->arity != v->arity ||
+        u->fuel != v->fuel || u->merge_fuel != v->merge_fuel || x->origins[i] != y->origins[i]) return 0;
+  }
+  for (int i = 0; i < x->constant_count; ++i) {
+    const Val* u = &x->constants[i]; const Val* v = &y->constants[i];
+    if (u->tag != v->tag || u->i != v->i || u->b != v->b) return 0;
+  }
+  return 1;
+}
+/* The lowest-indexed member equal to `child` of `children`, or -1. */
+static int find_member(const Trees* members, const uint64_t* member_hash, int population, const Trees* children, int child) {
+  const View c = view_of(children, child);
+  const uint64_t h = row_hash(&c);
+  for (int m = 0; m < population; ++m) {
+    if (member_hash[m] != h) continue;
+    const View v = view_of(members, m);
+    if (rows_equal(&v, &c)) return m;
+  }
+  return -1;
+}
+
 static int emit(Emit* o, int op, unsigned fuel, int a, int b, int flags) {
   if (o->code_count >= o->code_cap) { o->status = ST_CAPACITY; return 0; }
   if (fuel > 0x7fffffffU) { o->status = ST_INVALID; return 0; }
@@ -1130,6 +1176,11 @@ static int order_cmp(const void* x, const void* y) {
 
 int gagp_oracle_search(const gagp_grammar* g, const gagp_cases* cases, const gagp_search_config* cfg,
                        const gagp_rows* initial, gagp_search_result* out) {
+  return gagp_oracle_search_reuse(g, cases, cfg, initial, out, 0);
+}
+
+int gagp_oracle_search_reuse(const gagp_grammar* g, const gagp_cases* cases, const gagp_search_config* cfg,
+                             const gagp_rows* initial, gagp_search_result* out, int member_reuse) {
   Search s;
   if (search_init(&s, g) != 0) return -1;
   CaseSet cs;
@@ -1168,8 +1219,9 @@ int gagp_oracle_search(const gagp_grammar* g, const gagp_cases* cases, const gag
   unsigned* child_wrong = calloc((size_t)B, sizeof(unsigned));
   unsigned* child_count = calloc((size_t)B, sizeof(unsigned));
   Stat* stats = calloc((size_t)B, sizeof(Stat));
+  uint64_t* member_hash = calloc((size_t)P, sizeof(uint64_t));
   if (!fitness || !selection || !wrong || !nodes || !order || !placed || !reuse || !child_fitness || !child_wrong ||
-      !child_count || !stats) { snprintf(g_error, sizeof g_error, "out of memory"); goto done2; }
+      !child_count || !stats || !member_hash) { snprintf(g_error, sizeof g_error, "out of memory"); goto done2; }
   Policy policy = {cfg->counted_sites, cfg->uniform_phase, cfg->crossover_probability, cfg->crossover_attempts,
                    cfg->mutation_max_nodes};
   Mt rng;
@@ -1219,9 +1271,12 @@ int gagp_oracle_search(const gagp_grammar* g, const gagp_cases* cases, const gag
       mutate_child(child, &crossed, &next, &scratch, &s.slot, 1, s.maxv, cfg->mutation_probability, seed, &policy, &stats[child]);
       compare_child(child, &current, &crossed, P, 1, &stats[child]);
     }
+    if (member_reuse)
+      for (int m = 0; m < P; ++m) { const View v = view_of(&current, m); member_hash[m] = row_hash(&v); }
     for (int child = 0; child < B; ++child) {
       if (stats[child].error) { snprintf(g_error, sizeof g_error, "CPU genotype variation error %d", stats[child].error); goto done2; }
       reuse[child] = stats[child].reusable_parent;
+      if (member_reuse && reuse[child] < 0) reuse[child] = find_member(&current, member_hash, P, &crossed, child);
     }
     /* evaluate_batch + results of all children first (evolve.cpp:403-413) */
     for (int b = 0; b < B; ++b) {
@@ -1282,7 +1337,7 @@ int gagp_oracle_search(const gagp_grammar* g, const gagp_cases* cases, const gag
   rc = 0;
 done2:
   free(fitness); free(selection); free(wrong); free(nodes); free(order); free(placed); free(reuse);
-  free(child_fitness); free(child_wrong); free(child_count); free(stats);
+  free(child_fitness); free(child_wrong); free(child_count); free(stats); free(member_hash);
 done1:
   trees_free(&current); trees_free(&crossed); trees_free(&next); trees_free(&scratch);
 done0:
@@ -1302,6 +1357,60 @@ int gagp_oracle_initial_population(const gagp_grammar* g, const gagp_search_conf
     rc = 0;
   }
   trees_free(&rows);
+  free(s.expr_node);
+  return rc;
+}
+
+/* One make_batch (phase_population_cpu.cpp:322-353) over the generated
+ * initial population: every child of the first `batch` (cfg->batch, or the
+ * population) is varied with the given selection fitness and round seed;
+ * the children's rows go to `children` and the members whose results they
+ * reuse (their parent when unchanged, else an identical member; -1: none)
+ * to `reuse`.  Variation needs no cases, so this also runs on tables whose
+ * programs the oracle cannot evaluate. */
+int gagp_oracle_make_batch(const gagp_grammar* g, const gagp_search_config* cfg, const double* selection,
+                           uint64_t seed, gagp_rows* children, int32_t* reuse) {
+  Search s;
+  if (search_init(&s, g) != 0) return -1;
+  const int P = cfg->population, B = cfg->batch > 0 ? cfg->batch : cfg->population;
+  int rc = -1;
+  Trees current, crossed, next, scratch;
+  memset(&current, 0, sizeof current); memset(&crossed, 0, sizeof crossed);
+  memset(&next, 0, sizeof next); memset(&scratch, 0, sizeof scratch);
+  Stat* stats = calloc((size_t)(B > 0 ? B : 1), sizeof(Stat));
+  if (P <= 0 || B <= 0 || B > P || !stats) { snprintf(g_error, sizeof g_error, "batch contract"); goto done; }
+  if (trees_alloc(&current, P, s.maxv) || trees_alloc(&crossed, P, s.maxv) || trees_alloc(&next, P, s.maxv) ||
+      trees_alloc(&scratch, P, s.maxv)) { snprintf(g_error, sizeof g_error, "out of memory"); goto done; }
+  if (initial_rows(&s, P, cfg->seed, g->site_depth, &current)) goto done;
+  {
+    const int pressure = cfg->tournament_size < 1 ? 1 : cfg->tournament_size > P ? P : cfg->tournament_size;
+    Policy policy = {cfg->counted_sites, cfg->uniform_phase, cfg->crossover_probability, cfg->crossover_attempts,
+                     cfg->mutation_max_nodes};
+    for (int child = 0; child < B; ++child) {
+      crossover_child(child, &current, &crossed, &s.slot, 1, P, s.maxv, selection, pressure, seed, &policy, &stats[child]);
+      mutate_child(child, &crossed, &next, &scratch, &s.slot, 1, s.maxv, cfg->mutation_probability, seed, &policy,
+                   &stats[child]);
+      compare_child(child, &current, &crossed, P, 1, &stats[child]);
+    }
+    uint64_t* member_hash = calloc((size_t)P, sizeof(uint64_t));
+    if (!member_hash) { snprintf(g_error, sizeof g_error, "out of memory"); goto done; }
+    for (int m = 0; m < P; ++m) { const View v = view_of(&current, m); member_hash[m] = row_hash(&v); }
+    for (int child = 0; child < B; ++child) {
+      if (stats[child].error) {
+        snprintf(g_error, sizeof g_error, "CPU genotype variation error %d", stats[child].error);
+        free(member_hash);
+        goto done;
+      }
+      reuse[child] = stats[child].reusable_parent;
+      if (reuse[child] < 0) reuse[child] = find_member(&current, member_hash, P, &crossed, child);
+      if (child < children->count) export_row(&crossed, child, children, child);
+    }
+    free(member_hash);
+  }
+  rc = 0;
+done:
+  trees_free(&current); trees_free(&crossed); trees_free(&next); trees_free(&scratch);
+  free(stats);
   free(s.expr_node);
   return rc;
 }

@@ -27,6 +27,14 @@ int gagp_oracle_initial_population(const gagp_grammar* grammar, const gagp_searc
                                    gagp_rows* out);
 
 /* Fitness of rows (phase compiler + CPU VM + ordered reduction). */
+/* gagp_oracle_search with the reference's reuse of any identical member's
+ * result (member_reuse 1) or of the parent's only (0, as gagp_oracle_search). */
+int gagp_oracle_search_reuse(const gagp_grammar* grammar, const gagp_cases* cases,
+                             const gagp_search_config* config, const gagp_rows* initial,
+                             gagp_search_result* result, int member_reuse);
+/* One make_batch over the generated initial population (no cases needed). */
+int gagp_oracle_make_batch(const gagp_grammar* grammar, const gagp_search_config* config, const double* selection,
+                           uint64_t seed, gagp_rows* children, int32_t* reuse);
 int gagp_oracle_evaluate(const gagp_grammar* grammar, const gagp_cases* cases,
                          const gagp_search_config* config, const gagp_rows* rows,
                          double* fitness, uint32_t* wrong, uint64_t* instructions);

@@ -31,6 +31,7 @@ def load():
             build()
         lib = C.CDLL(LIB)
         lib.gagp_oracle_search.restype = C.c_int
+        lib.gagp_oracle_search_reuse.restype = C.c_int
         lib.gagp_oracle_initial_population.restype = C.c_int
         lib.gagp_oracle_evaluate.restype = C.c_int
         lib.gagp_oracle_compile.restype = C.c_int
@@ -45,13 +46,18 @@ def _check(rc: int):
 
 
 def search(grammar: abi.GrammarBlob, cases: abi.CasesBlob, settings: abi.SearchSettings,
-           initial: "abi.RowsBuffer | None" = None) -> dict:
+           initial: "abi.RowsBuffer | None" = None, member_reuse: bool = False) -> dict:
+    """A whole search.  `member_reuse` adds the reference's reuse of any
+    identical member's result; without it only a child equal to its parent
+    reuses (the rule the engine implements).  Results are the same either
+    way; the evaluation counters differ."""
     lib = load()
     stride = grammar.tables.max_nodes - grammar.tables.fixed_nodes
     res = abi.ResultBuffer(settings.generations, settings.population, stride)
     cfg = settings.struct()
-    _check(lib.gagp_oracle_search(grammar.ref(), cases.ref(), C.byref(cfg),
-                                  initial.ref() if initial is not None else None, res.ref()))
+    _check(lib.gagp_oracle_search_reuse(grammar.ref(), cases.ref(), C.byref(cfg),
+                                        initial.ref() if initial is not None else None, res.ref(),
+                                        C.c_int(1 if member_reuse else 0)))
     return res.summary()
 
 
@@ -62,6 +68,22 @@ def initial_population(grammar: abi.GrammarBlob, settings: abi.SearchSettings) -
     cfg = settings.struct()
     _check(lib.gagp_oracle_initial_population(grammar.ref(), C.byref(cfg), rows.ref()))
     return rows
+
+
+def make_batch(grammar: abi.GrammarBlob, settings: abi.SearchSettings, selection, seed: int):
+    """One make_batch over the generated initial population: the children's
+    rows and their reusable parents (-1: none)."""
+    lib = load()
+    stride = grammar.tables.max_nodes - grammar.tables.fixed_nodes
+    batch = settings.batch if settings.batch > 0 else settings.population
+    rows = abi.RowsBuffer(batch, stride)
+    reuse = np.full(batch, -2, dtype=np.int32)
+    sel = np.ascontiguousarray(np.asarray(selection, dtype=np.float64))
+    assert sel.size == settings.population
+    cfg = settings.struct()
+    _check(lib.gagp_oracle_make_batch(grammar.ref(), C.byref(cfg), sel.ctypes.data_as(C.POINTER(C.c_double)),
+                                      C.c_uint64(seed), rows.ref(), reuse.ctypes.data_as(C.POINTER(C.c_int32))))
+    return rows, reuse
 
 
 def evaluate(grammar: abi.GrammarBlob, cases: abi.CasesBlob, settings: abi.SearchSettings,

@@ -16,10 +16,19 @@
 //       per-generation history, and the final ranked population with fitness,
 //       wrong count, node count, program text and phase row.
 //
+//   ref_driver batch TASK.json [--search F] [--population N] [--seed S] --round-seed R
+//       one make_batch of the CPU resident owner (HostPhasePopulation,
+//       phase_population_cpu.cpp:322-353) over the generated initial population
+//       with the selection fitness sel[i] = (i * 7919) mod P + 1 and round seed
+//       R: every child's reusable parent and phase row (the children committed
+//       over members 0..B-1, then exported and imported back).
+//
 // These outputs are the golden vectors that pin the C restatement and the
 // table builder.
 #define __device__
 #define __host__
+#include <algorithm>
+#include <array>
 #include <cinttypes>
 #include <cstdio>
 #include <cstring>
@@ -57,6 +66,7 @@ struct Args {
   int population = 0, generations = 0;
   bool has_seed = false;
   std::uint64_t seed = 0;
+  std::uint64_t round_seed = 0;
 };
 
 std::string hex(double v) {
@@ -249,6 +259,43 @@ int run_tables(const Args& a) {
   return 0;
 }
 
+int run_batch(const Args& a) {
+  const auto task = cli_detail::load_task(a.task);
+  const auto grammar = std::make_shared<const gg::CompiledGrammar>(gg::compile_grammar(gg::load_definition(task.grammar_path)));
+  const auto cases = cli_detail::load_fitness_cases(task.train_path);
+  const auto cfg = make_config(a, task, grammar);
+  const auto case_set = evo::prepare_case_set(cases);
+  const auto& names = case_set.input_names;
+  const int site_depth = cfg.gpu_phase_site_depth;
+  const int P = cfg.population_size;
+  const auto population = rp::generate_phase_initial_population(*grammar, *cfg.generation_request, names, P, cfg.seed,
+                                                                 site_depth);
+  rp::HostPhasePopulation owner(grammar, population, names, site_depth,
+                                cfg.phase_variation ? *cfg.phase_variation : evo::PhaseVariationPolicy{});
+  int B = P;
+  if (cfg.phase_schedule && cfg.phase_schedule->batch > 0) B = cfg.phase_schedule->batch;
+  owner.begin_steady(B);
+  std::vector<double> selection(P);
+  for (int i = 0; i < P; ++i) selection[i] = double((std::uint64_t(i) * 7919u) % std::uint64_t(P) + 1);
+  const int pressure = std::clamp(cfg.selection_pressure, 1, P);
+  const auto reuse = owner.make_batch(selection, pressure, cfg.mutation_rate, a.round_seed, nullptr);
+  std::vector<std::array<int, 2>> placements;
+  for (int b = 0; b < B; ++b) placements.push_back({b, b});
+  owner.commit_batch(placements);
+  rp::NativePhaseGrammarProfiles profiles(grammar, names);
+  std::printf("{\"batch\":%d,\"round_seed\":\"%" PRIu64 "\",\"reuse\":[", B, a.round_seed);
+  for (std::size_t b = 0; b < reuse.size(); ++b) std::printf("%s%d", b ? "," : "", reuse[b]);
+  std::printf("],\"children\":[");
+  for (int b = 0; b < B; ++b) {
+    const auto imported = rp::import_native_phase_layout(*grammar, owner.export_member(std::size_t(b)), &profiles,
+                                                         &names, false);
+    std::printf("%s", b ? "," : "");
+    print_row(imported.genes.at(0), nullptr);
+  }
+  std::printf("]}\n");
+  return 0;
+}
+
 int run_search(const Args& a) {
   const auto task = cli_detail::load_task(a.task);
   const auto grammar = std::make_shared<const gg::CompiledGrammar>(gg::compile_grammar(gg::load_definition(task.grammar_path)));
@@ -294,7 +341,8 @@ int main(int argc, char** argv) {
     return 0;
   }
   if (argc < 3) {
-    std::fprintf(stderr, "usage: ref_driver tables|run TASK.json [--search F] [--population N] [--generations G] [--seed S]\n");
+    std::fprintf(stderr, "usage: ref_driver tables|run|batch TASK.json [--search F] [--population N] [--generations G] "
+                         "[--seed S] [--round-seed R]\n");
     return 2;
   }
   Args a;
@@ -306,11 +354,13 @@ int main(int argc, char** argv) {
     else if (k == "--population") a.population = std::stoi(v);
     else if (k == "--generations") a.generations = std::stoi(v);
     else if (k == "--seed") { a.has_seed = true; a.seed = std::stoull(v); }
+    else if (k == "--round-seed") a.round_seed = std::stoull(v);
     else { std::fprintf(stderr, "unknown option %s\n", k.c_str()); return 2; }
   }
   try {
     if (a.mode == "tables") return run_tables(a);
     if (a.mode == "run") return run_search(a);
+    if (a.mode == "batch") return run_batch(a);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "ref_driver: %s\n", e.what());
     return 1;

@@ -55,6 +55,10 @@ LIST_CASES = [
 ]
 
 
+# the round seed of the recorded make_batch (ref_driver batch)
+LIST_ROUND_SEED = 0x9E3779B97F4A7C15
+
+
 def nested_traversal_grammar() -> dict:
     """The list grammar with a second traversal inside the step, whose body
     nonterminal maps the outer accumulator and the inner binders by name
@@ -118,6 +122,7 @@ def main() -> None:
             tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
             tables = driver("tables", tp, "--search", sp)
             run = driver("run", tp, "--search", sp)
+            batch = driver("batch", tp, "--search", sp, "--round-seed", str(LIST_ROUND_SEED))
         assert run["declined"] == "", (name, run["declined"])
         fixture = {
             "name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
@@ -125,6 +130,7 @@ def main() -> None:
             "tables": {k: v for k, v in tables.items() if k != "initial"},
             "initial": [rows[0] for rows in tables["initial"]],
             "run": run,
+            "batch": batch,
         }
         with gzip.open(os.path.join(here, "list", name + ".json.gz"), "wt") as f:
             json.dump(fixture, f, separators=(",", ":"))

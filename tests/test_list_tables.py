@@ -83,3 +83,30 @@ def test_list_initial_population_matches_reference(name):
         origins, constants = rows.row(i)
         assert list(origins) == ref["origins"], i
         assert list(constants) == [c[1] for c in ref["constants"]], i
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_list_make_batch_matches_reference(name):
+    """One make_batch over the list tables (tournaments, typed subtree
+    crossover and mutation with scoped sites, traversal bodies included) gives
+    the reference owner's children row for row, and reuses a result exactly
+    for the children the reference does (its parent's when unchanged, else an
+    identical member's; which identical member is taken does not change the
+    result)."""
+    from gagp_b200 import abi, task as T
+    from oracle import oracle
+    fx = GU.list_fixture(name)
+    t = G.compile_tables(fx["grammar"], fx["tables"]["inputs"], allow_lists=True)
+    s = T.SearchSettings()
+    T.apply_search(s, T.DEFAULT_SEARCH)
+    T.apply_search(s, fx["search"])
+    P = s.population
+    selection = [float((i * 7919) % P + 1) for i in range(P)]
+    ref = fx["batch"]
+    rows, reuse = oracle.make_batch(abi.GrammarBlob(t), s, selection, int(ref["round_seed"]))
+    assert len(ref["children"]) == len(reuse)
+    for b, child in enumerate(ref["children"]):
+        origins, constants = rows.row(b)
+        assert list(origins) == child["origins"], b
+        assert list(constants) == [c[1] for c in child["constants"]], b
+        assert (reuse[b] >= 0) == (ref["reuse"][b] >= 0), b
