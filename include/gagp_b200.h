@@ -178,7 +178,9 @@ typedef struct gagp_search_result {
   int32_t* final_nodes;
   gagp_rows final_rows;
   uint64_t evaluated_programs;      /* program evaluations run */
-  uint64_t reused_programs;         /* children reusing a member's result */
+  uint64_t reused_programs;         /* children reusing their parent's result (a child equal to its
+                                       parent); the reference also counts children equal to any
+                                       other member, which this engine evaluates */
   uint64_t program_cases;           /* evaluated (program, case) pairs */
 } gagp_search_result;
 
@@ -236,7 +238,7 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
                                       int32_t* total_rounds, int32_t* finished);
 
 /* Work counters of a search so far: [0] program evaluations, [1] children
- * that reused a member's result, [2] evaluated (program, case) pairs,
+ * that reused their parent's result, [2] evaluated (program, case) pairs,
  * [3] VM instructions executed over all cases (accumulator VM: added when
  * a program's last case tile finishes), [4..6] SM clock cycles of
  * the placement phases (stream generation, draw staging, placement),
