@@ -151,3 +151,16 @@ def test_reference_runs_list_programs_resident(tmp_path):
     assert run["declined"] == ""
     assert len(run["history"]) == 2 and run["program_cases"] > 0
     assert run["history"][0]["text"].startswith("(traverse xs")
+
+
+def test_bench_mix_admission_counts():
+    """bench.py's batching and serving workloads admit the scalar entries of
+    their mixes and count the list entries the admission declines."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    mix = W.batch_mix(8)
+    tasks, declined = bench._mix_tasks(mix)
+    assert len(tasks) == 4 and declined == 4
+    assert all(t.settings.population == m["population"] for t, m in zip(tasks, [m for m in mix if m["kind"] == "scalar"]))
