@@ -139,11 +139,11 @@ namespace {
 
 enum KernelId {
   KN_INIT, KN_LOWER, KN_VM_FAST, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
-  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_MEMBERS, KN_COUNT
+  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_COUNT
 };
 const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast",
                                             "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
-                                            "k_place", "k_commit", "k_stream", "k_place_levels", "k_member_table"};
+                                            "k_place", "k_commit", "k_stream", "k_place_levels"};
 
 cudaEvent_t take_event(gagp_engine* e) {
   if (e->event_next == e->event_pool.size()) {
@@ -461,8 +461,6 @@ struct Plan {
       gen_nt, local_types, inputs, expected;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
-  size_t member_hash, member_table;
-  int table_slots;
   size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, child_level, level_plan, round,
       hist_sum, hist_fitness,
@@ -516,9 +514,6 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.c_parent = L.take(4 * size_t(B)); p.c_reuse = L.take(4 * size_t(B)); p.c_error = L.take(4 * size_t(B));
   p.c_fitness = L.take(8 * size_t(B)); p.c_wrong = L.take(4 * size_t(B)); p.c_nodes = L.take(4 * size_t(B));
   p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
-  p.table_slots = 1;
-  while (p.table_slots < 2 * P) p.table_slots <<= 1;
-  p.member_hash = L.take(8 * size_t(P)); p.member_table = L.take(8 * size_t(p.table_slots));
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
   p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots); p.vm_acc = L.take(16 * slots);
@@ -769,9 +764,6 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
   d.c_fitness = at<double>(b, p.c_fitness); d.c_wrong = at<uint32_t>(b, p.c_wrong);
   d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
-  d.member_hash = at<uint64_t>(b, p.member_hash);
-  d.member_table = at<unsigned long long>(b, p.member_table);
-  d.table_mask = p.table_slots - 1;
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
   d.vm_acc = at<unsigned long long>(b, p.vm_acc);
@@ -1010,12 +1002,6 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
   // next child of the variation warps; range c's lists start at item lo
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));
-  {
-    // the members' identity table of this round, read by the variation
-    Timed t(e, KN_MEMBERS);
-    gb::k_member_table<<<blocks_for(v.total_members, gb::kMemberTableWarps), gb::kMemberTableWarps * 32, 0,
-                         e->stream>>>(v.d_desc, v.d_member_off, v.n);
-  }
   CUDA_TRY(cudaEventRecord(e->chunk_fork, e->stream));
   const int chunks = v.total_children >= 4096 ? gagp_engine::kChunks : 1;
   const int warps = 4;

@@ -439,40 +439,6 @@ __global__ void __launch_bounds__(1024) k_record(const SearchDesc* descs, int n,
   }
 }
 
-// The members' identity table of a round (before the variation): a warp
-// per member hashes its row; lane 0 claims the first slot of its probe run
-// not yet tagged with this round.  The table needs no clearing between
-// rounds: a slot tagged with an earlier round is free.
-constexpr int kMemberTableWarps = 4;
-__global__ void __launch_bounds__(kMemberTableWarps * 32) k_member_table(const SearchDesc* descs, const int32_t* off,
-                                                                         int n) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int item = blockIdx.x * kMemberTableWarps + warp;
-  if (item >= off[n]) return;
-  const int si = find_search(off, n, item);
-  const SearchDesc& s = descs[si];
-  if (!search_live(s)) return;
-  const int m = item - off[si];
-  const int32_t l = s.len[m];
-  const uint64_t h = warp_row_hash(s.node + size_t(m) * s.stride, s.cval + size_t(m) * s.stride, len_nodes(l),
-                                   len_consts(l));
-  if (lane != 0) return;
-  s.member_hash[m] = h;
-  const unsigned long long tag = member_tag(s);
-  const unsigned mask = unsigned(s.table_mask);
-  unsigned slot = unsigned(h) & mask;
-  for (unsigned probe = 0; probe <= mask; ++probe, slot = (slot + 1) & mask) {
-    unsigned long long cur = s.member_table[slot];
-    // only this round's claims race for a slot, so a lost claim leaves it
-    // tagged with this round: at most one retry
-    for (int attempt = 0; attempt < 2 && (cur & 0xffffffff00000000ULL) != tag; ++attempt) {
-      const unsigned long long seen = atomicCAS(&s.member_table[slot], cur, tag | (unsigned long long)uint32_t(m));
-      if (seen == cur) return;
-      cur = seen;
-    }
-  }
-}
-
 // make_batch (phase_population_cpu.cpp:322-353): one warp per child, rows
 // staged in dynamic shared memory (warp_rows_bytes(stride) per warp).
 // Persistent warps over the batch items [lo, hi): each warp takes the next

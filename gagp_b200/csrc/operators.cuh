@@ -77,59 +77,6 @@ __device__ inline void load_members(const SearchDesc& s, int a, SRow& to_a, int 
   __syncwarp();
 }
 
-// ------------------------------------------------ identical-member lookup
-// The reference lets a child that is not its parent's copy reuse the result
-// of any current member with the same genotype (member_hashes,
-// phase_population_cpu.cpp:318-344; hash_program / equal_program,
-// parent_fitness_cache.cuh:15-43).  Here the hash is any function the warp
-// forms in parallel (a sum of mixed per-slot words): it only picks
-// candidates, and equality of every origin and constant decides.  Which
-// equal member is found does not matter, since equal programs score the
-// same.
-__device__ __forceinline__ uint64_t mix_word(uint64_t x) {
-  x ^= x >> 30;
-  x *= 0xbf58476d1ce4e5b9ULL;
-  x ^= x >> 27;
-  x *= 0x94d049bb133111ebULL;
-  return x ^ (x >> 31);
-}
-__device__ inline uint64_t warp_row_hash(const uint64_t* node, const int64_t* cval, int n, int nc) {
-  const int lane = lane_id();
-  uint64_t h = 0;
-  for (int i = lane; i < n; i += 32) h += mix_word((uint64_t(w_origin(node[i])) << 32) ^ uint64_t(i));
-  for (int j = lane; j < nc; j += 32) h += mix_word(uint64_t(cval[j]) ^ (uint64_t(j + 1) * 0x9e3779b97f4a7c15ULL));
-#pragma unroll
-  for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(kFull, h, o);
-  return mix_word(h ^ (uint64_t(n) << 48) ^ (uint64_t(nc) << 32));
-}
-// this round's tag in the member table: rounds done + 1 (0 never matches)
-__device__ __forceinline__ unsigned long long member_tag(const SearchDesc& s) {
-  return (unsigned long long)(uint32_t(s.round[0]) + 1u) << 32;
-}
-// The member whose row equals (node, cval, n, nc), or -1 (warp collective).
-__device__ inline int warp_find_member(const SearchDesc& s, const uint64_t* node, const int64_t* cval, int n, int nc) {
-  const int lane = lane_id();
-  const uint64_t h = warp_row_hash(node, cval, n, nc);
-  const unsigned long long tag = member_tag(s);
-  const unsigned mask = unsigned(s.table_mask);
-  unsigned slot = unsigned(h) & mask;
-  for (unsigned probe = 0; probe <= mask; ++probe, slot = (slot + 1) & mask) {
-    const unsigned long long e = s.member_table[slot];
-    if ((e & 0xffffffff00000000ULL) != tag) return -1;  // the end of this hash's run
-    const int m = int(uint32_t(e));
-    if (m < 0 || m >= s.P || s.member_hash[m] != h) continue;
-    const int32_t l = s.len[m];
-    if (len_nodes(l) != n || len_consts(l) != nc) continue;
-    const uint64_t* mn = s.node + size_t(m) * s.stride;
-    const int64_t* mc = s.cval + size_t(m) * s.stride;
-    bool same = true;
-    for (int i = lane; i < n; i += 32) same &= w_origin(mn[i]) == w_origin(node[i]);
-    for (int j = lane; j < nc; j += 32) same &= mc[j] == cval[j];
-    if (__all_sync(kFull, same)) return m;
-  }
-  return -1;
-}
-
 // One child, by one warp.  Writes the child row, its parent and reuse
 // source (the parent when the genotype is unchanged) and returns the
 // reference's OperatorStats error code (0: none).  stamp[0..2]: SM clock
@@ -230,7 +177,6 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
     equal = __all_sync(kFull, mine);
   }
   if (equal) *reuse_out = parent;
-  else *reuse_out = warp_find_member(s, w.child.node, w.child.cval, w.child.n, w.child.nc);
   // ---- publish the child row
   for (int i = lane; i < w.child.n; i += 32) s.cnode[size_t(child) * s.stride + i] = w.child.node[i];
   for (int i = lane; i < w.child.nc; i += 32) s.ccval[size_t(child) * s.stride + i] = w.child.cval[i];

@@ -124,11 +124,6 @@ struct SearchDesc {
   int32_t* c_parent; int32_t* c_reuse; int32_t* c_error;
   double* c_fitness; uint32_t* c_wrong; uint32_t* c_nodes; uint64_t* c_key;
   int32_t* c_eval;                     // 1: evaluate this child
-  // ---- identical-member lookup of one round: each member row's hash and an
-  // open-addressed table of (round tag << 32 | member), table_mask + 1 slots
-  uint64_t* member_hash;
-  unsigned long long* member_table;
-  int32_t table_mask;
   // ---- lowered programs (children, or members during the initial evaluation)
   uint2* code; int32_t* code_len; int64_t* kpool;
   int32_t code_stride;                 // accumulator instructions per program slot

@@ -51,7 +51,7 @@ def test_edge_shape_matches_oracle(engine, tmp_path, name, population, cases, ge
     if fitness is not None:
         files.fitness = fitness
     lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
-    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings, member_reuse=True)
+    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
     s = engine.admit(lt)
     try:
         s.run()
