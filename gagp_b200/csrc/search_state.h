@@ -128,8 +128,10 @@ struct SearchDesc {
   uint2* code; int32_t* code_len; int64_t* kpool;
   int32_t code_stride;                 // accumulator instructions per program slot
   int32_t* code_temps;                 // temporaries; <0: needs the general VM
-  // per program slot, the fast VM's tile accumulators: [2 slot] the loss
-  // sum, [2 slot + 1] wrong cases (low 32 bits) | tiles done (high 32 bits)
+  // per program slot, the fast VM's tile accumulators: [2 slot] loss (bits
+  // 0-39) | wrong cases (40-55) | tiles done (56-63) when the search's case
+  // count and penalty fit those fields; otherwise [2 slot] the loss sum and
+  // [2 slot + 1] wrong cases (low 32 bits) | tiles done (high 32 bits)
   unsigned long long* vm_acc;
   int32_t* bc;                         // reference bytecode (op,flags,a,b,fuel) per program
   int32_t* bc_len;
