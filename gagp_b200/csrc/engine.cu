@@ -213,6 +213,7 @@ gagp_status ensure_lists(gagp_engine* e, size_t items) {
   if (e->d_fast) cudaFree(e->d_fast);
   if (e->d_general) cudaFree(e->d_general);
   e->d_fast = e->d_general = nullptr;
+  e->list_capacity = 0;
   const size_t cap = std::max<size_t>({items, size_t(1024), 2 * e->list_capacity});
   CUDA_TRY(cudaMalloc(&e->d_fast, cap * sizeof(gb::ProgramRef)));
   CUDA_TRY(cudaMalloc(&e->d_general, cap * sizeof(gb::ProgramRef)));
@@ -844,15 +845,21 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
     v->d_member_off = list[0]->d_off;
     v->d_child_off = list[0]->d_off + 2;
   } else {
-    if (size_t(n) > e->batch_desc_capacity) {  // grown geometrically: batches change size while serving
+    // grown geometrically (batches change size while serving); a failed
+    // allocation leaves no stale pointer or capacity behind
+    if (size_t(n) > e->batch_desc_capacity) {
       const size_t cap = std::max<size_t>(size_t(n), 2 * e->batch_desc_capacity);
       cudaFree(e->d_batch_desc);
+      e->d_batch_desc = nullptr;
+      e->batch_desc_capacity = 0;
       CUDA_TRY(cudaMalloc(&e->d_batch_desc, sizeof(gb::SearchDesc) * cap));
       e->batch_desc_capacity = cap;
     }
     if (size_t(2 * (n + 1)) > e->batch_off_capacity) {
       const size_t cap = std::max<size_t>(size_t(2 * (n + 1)), 2 * e->batch_off_capacity);
       cudaFree(e->d_batch_off);
+      e->d_batch_off = nullptr;
+      e->batch_off_capacity = 0;
       CUDA_TRY(cudaMalloc(&e->d_batch_off, sizeof(int32_t) * cap));
       e->batch_off_capacity = cap;
     }
@@ -1058,7 +1065,13 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
 }
 
+// The searches of `ids`, each at most once: a repeated id would put one
+// search's device state into a batch twice, and both copies would write it.
 gagp_status collect(gagp_engine* e, const std::vector<int32_t>& ids, std::vector<Search*>* list) {
+  std::vector<int32_t> sorted(ids);
+  std::sort(sorted.begin(), sorted.end());
+  if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+    return fail(GAGP_INVALID_ARGUMENT, "a search id is listed more than once");
   for (int32_t id : ids) {
     auto it = e->searches.find(id);
     if (it == e->searches.end()) return fail(GAGP_INVALID_ARGUMENT, "unknown search " + std::to_string(id));
@@ -1431,8 +1444,7 @@ gagp_status gagp_b200_batch_run(gagp_engine* e, const int32_t* ids, int32_t coun
   return st;
 }
 
-gagp_status gagp_b200_batch_step(gagp_engine* e, const int32_t* ids, int32_t count, int32_t* finished) {
-  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+static gagp_status batch_step_body(gagp_engine* e, const int32_t* ids, int32_t count, int32_t* finished) {
   CUDA_TRY(cudaSetDevice(e->device));
   std::vector<Search*> list;
   gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
@@ -1457,8 +1469,7 @@ gagp_status gagp_b200_batch_step(gagp_engine* e, const int32_t* ids, int32_t cou
   return GAGP_OK;
 }
 
-gagp_status gagp_b200_batch_start(gagp_engine* e, const int32_t* ids, int32_t count) {
-  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+static gagp_status batch_start_body(gagp_engine* e, const int32_t* ids, int32_t count) {
   CUDA_TRY(cudaSetDevice(e->device));
   std::vector<Search*> list, fresh;
   gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
@@ -1472,9 +1483,19 @@ gagp_status gagp_b200_batch_start(gagp_engine* e, const int32_t* ids, int32_t co
   return check_errors(e, fresh);
 }
 
-gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t count, int32_t rounds,
-                                    int32_t flush_l2, double* device_ms) {
-  if (!e || (!ids && count) || rounds < 0) return fail(GAGP_INVALID_ARGUMENT, "bad argument");
+// Round timing events of one batch_advance call, destroyed on every return.
+struct RoundMarks {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks;
+  ~RoundMarks() {
+    for (auto& m : marks) {
+      if (m.first) cudaEventDestroy(m.first);
+      if (m.second) cudaEventDestroy(m.second);
+    }
+  }
+};
+
+static gagp_status batch_advance_body(gagp_engine* e, const int32_t* ids, int32_t count, int32_t rounds,
+                                      int32_t flush_l2, double* device_ms) {
   CUDA_TRY(cudaSetDevice(e->device));
   std::vector<Search*> list;
   gagp_status st = collect(e, std::vector<int32_t>(ids, ids + count), &list);
@@ -1487,32 +1508,56 @@ gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t 
     e->flush_bytes = size_t(256) << 20;  // twice the B200's 126 MB L2
     CUDA_TRY(cudaMalloc(&e->flush_buffer, e->flush_bytes));
   }
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks;
+  RoundMarks marks;
   RoundGraph graph;
   const bool replay = !e->profiling && rounds > 1 && e->vm_tune[vm_key(v.max_C, v.max_inputs)].chosen >= 0;
   if (replay && (st = capture_round(e, v, &graph)) != GAGP_OK) return st;
   for (int r = 0; r < rounds; ++r) {
     if (flush_l2) CUDA_TRY(cudaMemsetAsync(e->flush_buffer, r & 0xff, e->flush_bytes, e->stream));
-    cudaEvent_t a, b;
-    CUDA_TRY(cudaEventCreate(&a));
-    CUDA_TRY(cudaEventCreate(&b));
-    CUDA_TRY(cudaEventRecord(a, e->stream));
+    marks.marks.push_back({nullptr, nullptr});
+    auto& m = marks.marks.back();
+    CUDA_TRY(cudaEventCreate(&m.first));
+    CUDA_TRY(cudaEventCreate(&m.second));
+    CUDA_TRY(cudaEventRecord(m.first, e->stream));
     if (replay) CUDA_TRY(cudaGraphLaunch(graph.exec, e->stream));
     else if ((st = launch_round(e, v)) != GAGP_OK) return st;
-    CUDA_TRY(cudaEventRecord(b, e->stream));
-    marks.push_back({a, b});
+    CUDA_TRY(cudaEventRecord(m.second, e->stream));
   }
   st = check_errors(e, list);
   double total = 0;
-  for (auto& m : marks) {
+  for (auto& m : marks.marks) {
     float ms = 0;
     cudaEventElapsedTime(&ms, m.first, m.second);
     total += ms;
-    cudaEventDestroy(m.first);
-    cudaEventDestroy(m.second);
   }
   if (device_ms) *device_ms = total;
   return st;
+}
+
+// Entry points that launch work refuse a poisoned engine and poison it
+// after a device error that left a CUDA error pending, as search_run does.
+static gagp_status poison_after(gagp_engine* e, gagp_status st) {
+  if (st == GAGP_DEVICE_ERROR && cudaGetLastError() != cudaSuccess) e->poisoned = true;
+  return st;
+}
+
+gagp_status gagp_b200_batch_step(gagp_engine* e, const int32_t* ids, int32_t count, int32_t* finished) {
+  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  return poison_after(e, batch_step_body(e, ids, count, finished));
+}
+
+gagp_status gagp_b200_batch_start(gagp_engine* e, const int32_t* ids, int32_t count) {
+  if (!e || (!ids && count)) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  return poison_after(e, batch_start_body(e, ids, count));
+}
+
+gagp_status gagp_b200_batch_advance(gagp_engine* e, const int32_t* ids, int32_t count, int32_t rounds,
+                                    int32_t flush_l2, double* device_ms) {
+  if (!e || (!ids && count) || rounds < 0) return fail(GAGP_INVALID_ARGUMENT, "bad argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  return poison_after(e, batch_advance_body(e, ids, count, rounds, flush_l2, device_ms));
 }
 
 gagp_status gagp_b200_engine_transfers(gagp_engine* e, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {

@@ -193,11 +193,13 @@ class Engine:
 
 
 def evaluate_rows_static(task: LoadedTask, rows: abi.RowsBuffer, stream: int = 0):
-    """Row evaluation that allocates no device memory (for callers that may not
-    allocate: inside a stream capture, under a foreign allocator, or in a
-    latency-critical loop).  All device buffers live in the library's static
-    32 MiB scratch; larger requests raise EngineError(INVALID_ARGUMENT).  Calls
-    share that scratch, so concurrent calls must be serialized by the caller."""
+    """Row evaluation that allocates no device memory, for callers that may not
+    allocate: a host application whose own allocator owns all device memory,
+    or a latency-critical scoring loop that cannot pay for an allocation per
+    call.  All device buffers live in the library's static 32 MiB scratch;
+    larger requests raise EngineError(INVALID_ARGUMENT).  `stream` is a
+    cudaStream_t handle (0: the default stream).  Calls share that scratch,
+    so concurrent calls must be serialized by the caller."""
     g = abi.GrammarBlob(task.tables)
     cfg = task.settings.struct()
     fitness = np.zeros(rows.count, dtype=np.float64)

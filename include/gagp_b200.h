@@ -282,20 +282,22 @@ gagp_status gagp_b200_evaluate_rows(gagp_engine* engine, const gagp_grammar* gra
                                     uint32_t* wrong);
 
 /* gagp_b200_evaluate_rows without any device allocation -- no counterpart in
- * the reference.  For callers that must not call cudaMalloc: code running
- * while a stream is being captured into a CUDA graph, a host that leaves all
- * device memory to its own allocator, or a latency-critical loop that cannot
- * afford allocation.  Every device buffer of the call lives in one static
- * 32 MiB device array that each GPU loading this library holds until exit;
- * a call needing more (many rows, long rows or many cases) is rejected with
- * GAGP_INVALID_ARGUMENT and a message naming the bytes needed.  Runs on the
- * current device and `stream` (a cudaStream_t; NULL: the default stream) and
- * returns when the results are in the host arrays.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) and
- * sets kernel attributes; make that first call before any stream capture.
- * All calls share the one array, and it keeps the last call's contents
- * (the call clears what must start at zero): calls that overlap on the GPU,
- * from several host threads or streams, race and must be serialized. */
+ * the reference.  For callers that must not call cudaMalloc: a host
+ * application that hands all device memory to its own allocator (a framework
+ * caching allocator or a fixed arena), or a latency-critical scoring loop
+ * that cannot pay for an allocation and a free on every call.  Every device
+ * buffer of the call lives in one static 32 MiB device array that each GPU
+ * loading this library holds until exit; a call needing more (many rows,
+ * long rows or many cases) is rejected with GAGP_INVALID_ARGUMENT and a
+ * message naming the bytes needed.  Runs on the current device and `stream`
+ * (a cudaStream_t; NULL: the default stream); it copies its inputs from
+ * host memory, waits for the stream and returns when the results are in the
+ * host arrays.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and sets kernel attributes; make that first
+ * call before any stream capture.  All calls share the one array, and it
+ * keeps the last call's contents (the call clears what must start at zero):
+ * calls that overlap on the GPU, from several host threads or streams, race
+ * and must be serialized. */
 gagp_status gagp_b200_evaluate_rows_static(const gagp_grammar* grammar, const gagp_cases* cases,
                                            const gagp_search_config* config, const gagp_rows* rows,
                                            double* fitness, uint32_t* wrong, void* stream);

@@ -62,3 +62,24 @@ def test_edge_shape_matches_oracle(engine, tmp_path, name, population, cases, ge
     assert got["final"] == want["final"], name
     assert got["evaluated_programs"] == want["evaluated_programs"], name
     assert got["reused_programs"] == want["reused_programs"], name
+
+
+def test_batch_entry_points_reject_a_repeated_search(engine, tmp_path):
+    """A search listed twice in one batch would have two batch members write
+    its device state: every batch entry point refuses it before any launch,
+    and the search still runs alone afterwards."""
+    from gagp_b200.engine import EngineError
+    files = W.poly4(population=64, generations=2, seed=3, cases=16, max_nodes=40)
+    lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
+    s = engine.admit(lt)
+    try:
+        for call in (lambda: engine.run_batch([s, s]), lambda: engine.step([s, s]), lambda: engine.start([s, s]),
+                     lambda: engine.advance([s, s], 1)):
+            with pytest.raises(EngineError) as err:
+                call()
+            assert err.value.status == 2 and "more than once" in str(err.value)
+        s.run()
+        want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+        assert s.result()["final"] == want["final"]
+    finally:
+        s.close()

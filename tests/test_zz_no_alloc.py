@@ -1,9 +1,9 @@
 """The no-allocation row evaluator against the allocating one (GPU).
 
 gagp_b200_evaluate_rows_static serves callers that may not allocate device
-memory (inside a CUDA-graph stream capture, under a host application's own
-allocator, in latency-critical loops): its buffers live in one static device
-array.  Two calls in a row must each equal gagp_b200_evaluate_rows exactly
+memory (a host application whose own allocator owns the device memory, or a
+latency-critical scoring loop that cannot pay for an allocation per call):
+its buffers live in one static device array.  Two calls in a row must each equal gagp_b200_evaluate_rows exactly
 (fitness and wrong counts are integers here), which also shows the shared
 array carries nothing over from the previous call; an oversized request is
 rejected before any device work.  Collected last so that a failure here
@@ -36,6 +36,22 @@ def test_static_evaluation_matches_allocating_evaluation_twice(tmp_path):
             got_f, got_w = evaluate_rows_static(lt, rows)
             assert np.array_equal(got_f, want_f)
             assert np.array_equal(got_w, want_w)
+
+
+def test_static_evaluation_on_a_caller_stream(tmp_path):
+    """The stream argument: the call runs on a stream the caller created
+    (a non-default, non-blocking one), twice in a row, with the same
+    results as the allocating evaluator."""
+    import torch
+    from gagp_b200.engine import Engine, evaluate_rows_static
+    lt, rows = _rows_for(tmp_path, 24, 130, 700)
+    stream = torch.cuda.Stream(device=0)
+    with Engine(0) as engine:
+        want_f, want_w = engine.evaluate_rows(lt, rows)
+    for _ in range(2):
+        got_f, got_w = evaluate_rows_static(lt, rows, stream=stream.cuda_stream)
+        assert np.array_equal(got_f, want_f)
+        assert np.array_equal(got_w, want_w)
 
 
 def test_static_evaluation_rejects_oversized_requests(tmp_path):
