@@ -48,6 +48,12 @@ class Value(C.Structure):
     _fields_ = [("i", C.c_int64), ("tag", C.c_int32), ("reserved", C.c_int32)]
 
 
+class Region(C.Structure):
+    _fields_ = [("traversal", C.c_int32), ("ranged", C.c_int32), ("fuel_profile", C.c_int32),
+                ("binders", C.c_int32 * 3), ("operand_types", C.c_int32 * 6), ("binding_types", C.c_int32 * 3),
+                ("result_type", C.c_int32), ("event_cost", C.c_uint32 * 26)]
+
+
 class Grammar(C.Structure):
     _fields_ = [("expressions", C.POINTER(Expression)), ("expression_count", C.c_int32),
                 ("productions", C.POINTER(Production)), ("production_count", C.c_int32),
@@ -58,13 +64,15 @@ class Grammar(C.Structure):
                 ("depth_count", C.c_int32), ("logical_depth_count", C.c_int32), ("site_depth", C.c_int32),
                 ("root_expression", C.c_int32), ("slot_max_depth", C.c_int32), ("slot_type", C.c_int32),
                 ("local_count", C.c_int32), ("local_types", C.c_int32 * MAX_LOCALS),
-                ("max_nodes", C.c_int32), ("fixed_nodes", C.c_int32), ("return_fuel", C.c_uint32)]
+                ("max_nodes", C.c_int32), ("fixed_nodes", C.c_int32), ("return_fuel", C.c_uint32),
+                ("regions", C.POINTER(Region)), ("region_count", C.c_int32)]
 
 
 class Cases(C.Structure):
     _fields_ = [("case_count", C.c_int32), ("input_count", C.c_int32), ("inputs", C.POINTER(C.c_int64)),
                 ("input_tags", C.POINTER(C.c_int32)), ("expected", C.POINTER(C.c_int64)),
-                ("expected_tag", C.c_int32)]
+                ("expected_tag", C.c_int32), ("list_values", C.POINTER(C.c_int64)),
+                ("list_value_count", C.c_int64)]
 
 
 class SearchConfig(C.Structure):
@@ -141,6 +149,15 @@ class GrammarBlob:
         for j, tag in enumerate(t.local_types):
             g.local_types[j] = tag
         g.max_nodes, g.fixed_nodes, g.return_fuel = t.max_nodes, t.fixed_nodes, return_fuel
+        self.regions = (Region * max(1, len(t.regions)))()
+        for i, r in enumerate(t.regions):
+            x = self.regions[i]
+            x.traversal, x.ranged, x.fuel_profile, x.result_type = r.traversal, int(r.ranged), 0, r.result_type
+            for k in range(3):
+                x.binders[k], x.binding_types[k] = r.binders[k], r.binding_types[k]
+            for k, tag in enumerate(r.operand_types):
+                x.operand_types[k] = tag
+        g.regions, g.region_count = self.regions, len(t.regions)
         self.struct = g
 
     def ref(self):
@@ -148,19 +165,32 @@ class GrammarBlob:
 
 
 class CasesBlob:
-    """Scalar case set: ``inputs[case, input]`` payloads and expected values."""
+    """Case set: ``inputs[case, input]`` payloads and expected values.  An
+    IntList input's payload is the index in ``list_values`` of its length
+    word; its elements follow."""
 
-    def __init__(self, inputs: np.ndarray, input_tags: Sequence[int], expected: np.ndarray, expected_tag: int = 0):
+    def __init__(self, inputs: np.ndarray, input_tags: Sequence[int], expected: np.ndarray, expected_tag: int = 0,
+                 list_values: Optional[np.ndarray] = None):
         self.inputs = np.ascontiguousarray(np.asarray(inputs, dtype=np.int64).reshape(len(expected), -1))
         self.input_tags = np.ascontiguousarray(np.asarray(input_tags, dtype=np.int32))
         self.expected = np.ascontiguousarray(np.asarray(expected, dtype=np.int64))
+        self.list_values = None if list_values is None else np.ascontiguousarray(np.asarray(list_values, dtype=np.int64))
+        self.expected_tag = expected_tag
         c = Cases()
         c.case_count, c.input_count = len(self.expected), self.inputs.shape[1]
         c.inputs = _ptr(self.inputs, C.c_int64)
         c.input_tags = _ptr(self.input_tags, C.c_int32)
         c.expected = _ptr(self.expected, C.c_int64)
         c.expected_tag = expected_tag
+        if self.list_values is not None and len(self.list_values):
+            c.list_values, c.list_value_count = _ptr(self.list_values, C.c_int64), len(self.list_values)
         self.struct = c
+
+    def list_at(self, case: int, input_index: int) -> List[int]:
+        """The IntList value of one case input."""
+        at = int(self.inputs[case, input_index])
+        n = int(self.list_values[at])
+        return [int(x) for x in self.list_values[at + 1:at + 1 + n]]
 
     def ref(self):
         return C.byref(self.struct)

@@ -24,7 +24,8 @@ namespace gb {
 
 // PhaseExpressionKind / PhaseTreeKind / status codes (reference enums).
 enum { EK_OPERATION = 0, EK_CONSTANT = 1, EK_BOUND = 2, EK_REFERENCE = 3, EK_INPUT = 4, EK_ALIAS = 5 };
-enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5 };
+enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5, TK_BOUND = 14,
+       TK_TRAVERSE = 16 };
 enum { ST_OK = 0, ST_INVALID = 1, ST_UNSUPPORTED = 2, ST_CAPACITY = 3 };
 constexpr int kFixedSite = 1 << 30;
 constexpr uint32_t kNoClass = 0x7ffu;
@@ -103,33 +104,33 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
 }
 
 // ---------------------------------------------------------------- node words
-__device__ __forceinline__ int w_origin(uint64_t w) { return int(w & 0xffffu); }
-__device__ __forceinline__ int w_entry(uint64_t w) { return int((w >> 16) & 0xffffu) - 1; }
-__device__ __forceinline__ int w_depth(uint64_t w) { return int((w >> 32) & 0xffu); }
-__device__ __forceinline__ int w_sval(uint64_t w) { return int((w >> 40) & 0xffu); }
-__device__ __forceinline__ int w_arity(uint64_t w) { return int((w >> 48) & 0xfu); }
-__device__ __forceinline__ bool w_const(uint64_t w) { return (w >> 52) & 1u; }
-__device__ __forceinline__ uint32_t w_class(uint64_t w) { return uint32_t(w >> 53); }
-__device__ __forceinline__ bool w_site(uint64_t w) { return ((w >> 16) & 0xffffu) != 0; }
-__device__ __forceinline__ uint64_t w_make(int origin, int entry, int depth, int sval, int arity, bool constant,
+__host__ __device__ __forceinline__ int w_origin(uint64_t w) { return int(w & 0xffffu); }
+__host__ __device__ __forceinline__ int w_entry(uint64_t w) { return int((w >> 16) & 0xffffu) - 1; }
+__host__ __device__ __forceinline__ int w_depth(uint64_t w) { return int((w >> 32) & 0xffu); }
+__host__ __device__ __forceinline__ int w_sval(uint64_t w) { return int((w >> 40) & 0xffu); }
+__host__ __device__ __forceinline__ int w_arity(uint64_t w) { return int((w >> 48) & 0xfu); }
+__host__ __device__ __forceinline__ bool w_const(uint64_t w) { return (w >> 52) & 1u; }
+__host__ __device__ __forceinline__ uint32_t w_class(uint64_t w) { return uint32_t(w >> 53); }
+__host__ __device__ __forceinline__ bool w_site(uint64_t w) { return ((w >> 16) & 0xffffu) != 0; }
+__host__ __device__ __forceinline__ uint64_t w_make(int origin, int entry, int depth, int sval, int arity, bool constant,
                                            uint32_t cls) {
   return uint64_t(uint32_t(origin) & 0xffffu) | (uint64_t(uint32_t(entry + 1) & 0xffffu) << 16) |
          (uint64_t(uint32_t(depth) & 0xffu) << 32) | (uint64_t(uint32_t(sval) & 0xffu) << 40) |
          (uint64_t(uint32_t(arity) & 0xfu) << 48) | (uint64_t(constant) << 52) | (uint64_t(cls & 0x7ffu) << 53);
 }
 // Shifts depth and site depth (a donor subtree moved under another parent).
-__device__ __forceinline__ uint64_t w_shift(uint64_t w, int ddepth, int dsval) {
+__host__ __device__ __forceinline__ uint64_t w_shift(uint64_t w, int ddepth, int dsval) {
   const int d = w_depth(w) + ddepth, v = w_sval(w) + dsval;
   return (w & ~(0xffffULL << 32)) | (uint64_t(uint32_t(d) & 0xffu) << 32) | (uint64_t(uint32_t(v) & 0xffu) << 40);
 }
 // Replaces the site (entry and class) of a word by another word's site.
-__device__ __forceinline__ uint64_t w_with_site(uint64_t w, uint64_t site_from) {
+__host__ __device__ __forceinline__ uint64_t w_with_site(uint64_t w, uint64_t site_from) {
   const uint64_t mask = (0xffffULL << 16) | (0x7ffULL << 53);
   return (w & ~mask) | (site_from & mask);
 }
-__device__ __forceinline__ int len_nodes(int32_t l) { return l & 0xffff; }
-__device__ __forceinline__ int len_consts(int32_t l) { return (l >> 16) & 0xffff; }
-__device__ __forceinline__ int32_t make_len(int n, int c) { return n | (c << 16); }
+__host__ __device__ __forceinline__ int len_nodes(int32_t l) { return l & 0xffff; }
+__host__ __device__ __forceinline__ int len_consts(int32_t l) { return (l >> 16) & 0xffff; }
+__host__ __device__ __forceinline__ int32_t make_len(int n, int c) { return n | (c << 16); }
 
 // Crossover class of sites opened by reference expression `entry`.
 __device__ __forceinline__ uint32_t class_of_entry(const SearchDesc& s, int entry) {
@@ -311,22 +312,23 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
         value = __ldg(&vals[v_offset + random.bounded(uint64_t(v_count))].i);
       }
       out_cval[result.constants++] = value;
-    } else if (kind != EK_OPERATION && kind != EK_INPUT) {
-      return result;  // binders and aliases are declined at admission
+    } else if (kind != EK_OPERATION && kind != EK_INPUT && kind != EK_BOUND) {
+      return result;  // aliases are declined at admission
     }
     out_node[result.nodes++] = w_make(t_expr, next_site, depth - t_depth + 1, logical_depth - t_logical, arity,
                                       kind == EK_CONSTANT, next_class);
     next_site = -1;
     next_class = kNoClass;
     // the children's minimum costs, loaded together, then pushed last to
-    // first (the first child straight into `next`)
+    // first (the first child straight into `next`); a traversal has four
     const unsigned need0 = arity > 0 ? min_at(ra.x, t_depth - 1, t_logical) : 0;
     const unsigned need1 = arity > 1 ? min_at(ra.y, t_depth - 1, t_logical) : 0;
     const unsigned need2 = arity > 2 ? min_at(ra.z, t_depth - 1, t_logical) : 0;
+    const unsigned need3 = arity > 3 ? min_at(ra.w, t_depth - 1, t_logical) : 0;
     for (int i = arity - 1; i >= 0; --i) {
       if (count >= 192) { result.status = ST_CAPACITY; return result; }
-      const int child = i == 0 ? ra.x : i == 1 ? ra.y : ra.z;
-      const unsigned need = i == 0 ? need0 : i == 1 ? need1 : need2;
+      const int child = i == 0 ? ra.x : i == 1 ? ra.y : i == 2 ? ra.z : ra.w;
+      const unsigned need = i == 0 ? need0 : i == 1 ? need1 : i == 2 ? need2 : need3;
       if (need > unsigned(capacity - result.nodes) || reserved > unsigned(capacity - result.nodes) - need) {
         result.status = ST_CAPACITY;
         return result;

@@ -59,6 +59,10 @@ struct Search {
   int P = 0, B = 0, G = 0, total_rounds = 0, maxv = 0, stride = 0, fixed_nodes = 0;
   int has_wrong = 0;
   bool started = false;
+  // most of its programs need the exact VM (traversals, or operations that
+  // can fail); otherwise only the rare program past the accumulator VM's
+  // limits does
+  bool exact_heavy = false;
   gb::SearchDesc* d_desc = nullptr;   // single-search batch descriptor
   int32_t* d_off = nullptr;           // {0, P, 0, B}: member and child offsets
 };
@@ -139,11 +143,11 @@ namespace {
 
 enum KernelId {
   KN_INIT, KN_LOWER, KN_VM_FAST, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
-  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_COUNT
+  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_VM_GENERAL, KN_COUNT
 };
 const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast",
                                             "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
-                                            "k_place", "k_commit", "k_stream", "k_place_levels"};
+                                            "k_place", "k_commit", "k_stream", "k_place_levels", "k_vm_general"};
 
 cudaEvent_t take_event(gagp_engine* e) {
   if (e->event_next == e->event_pool.size()) {
@@ -244,6 +248,96 @@ int bits_for(uint64_t v) {
   return b;
 }
 
+// The phase tables, traversal table and cases as the device reads them:
+// every id the subtree generator and the lowering follow without a range
+// check is in range, and every IntList input lies inside list_values.
+// GAGP_DECLINED for constructs outside the resident subset.
+gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
+  // the subtree generator and the lowering read these tables without range
+  // checks: every id they hold must be in range
+  const int E = g->expression_count, NT = g->nonterminal_count, PR = g->production_count, ND = g->domain_count;
+  const int RG = g->region_count;
+  if (RG < 0 || RG > 1024 || (RG && !g->regions)) return fail(GAGP_INVALID_ARGUMENT, "traversal table");
+  auto value_tag = [](int t) { return t == GAGP_TAG_INT || t == GAGP_TAG_BOOL || t == GAGP_TAG_INTLIST; };
+  for (int r = 0; r < RG; ++r) {
+    const gagp_region& x = g->regions[r];
+    if (x.traversal != 1 && x.traversal != 2)
+      return fail(GAGP_DECLINED, "bounded regions other than traversals are outside the resident subset");
+    if (x.ranged) return fail(GAGP_DECLINED, "ranged traversals are outside the resident subset");
+    if (x.fuel_profile) return fail(GAGP_DECLINED, "traversal fuel profiles are outside the resident subset");
+    for (int k = 0; k < 3; ++k) {
+      if (x.binders[k] < 0 || x.binders[k] >= gb::kLowerBinders) return fail(GAGP_INVALID_ARGUMENT, "traversal binder");
+      if (!value_tag(x.binding_types[k])) return fail(GAGP_DECLINED, "traversal binding type");
+    }
+    for (int k = 0; k < 4; ++k)
+      if (!value_tag(x.operand_types[k])) return fail(GAGP_DECLINED, "traversal operand type");
+    if (!value_tag(x.result_type)) return fail(GAGP_DECLINED, "traversal result type");
+  }
+  for (int i = 0; i < E; ++i) {
+    const gagp_expression& e = g->expressions[i];
+    if (e.kind == gb::EK_ALIAS) return fail(GAGP_DECLINED, "templates are outside the resident subset");
+    if (e.kind != gb::EK_REFERENCE && e.kind != gb::EK_CONSTANT && e.kind != gb::EK_OPERATION &&
+        e.kind != gb::EK_INPUT && e.kind != gb::EK_BOUND)
+      return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": unknown kind");
+    if (e.kind == gb::EK_REFERENCE && (e.scope_count < 0 || e.scope_count > 15))
+      return fail(GAGP_INVALID_ARGUMENT, "reference scope");
+    if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_TRAVERSE) {
+      if (e.arity != 4 || e.operand < 0 || e.operand >= RG)
+        return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": traversal entry");
+    } else if (e.arity < 0 || e.arity > 3) {
+      return fail(GAGP_DECLINED, "arity capacity");
+    }
+    if (e.kind == gb::EK_OPERATION && e.node_kind != gb::TK_OPERATION && e.node_kind != gb::TK_IF &&
+        e.node_kind != gb::TK_AND && e.node_kind != gb::TK_OR && e.node_kind != gb::TK_TRAVERSE)
+      return fail(GAGP_DECLINED, "statements and lets are outside the resident subset");
+    if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_OPERATION && e.opcode == gb::OP_CALL_BUILTIN &&
+        e.operand != gb::B_ABS && e.operand != gb::B_MIN && e.operand != gb::B_MAX && e.operand != gb::B_LEN &&
+        e.operand != gb::B_INDEX && e.operand != gb::B_IDIV0 && e.operand != gb::B_IMOD0 &&
+        e.operand != gb::B_TRUNC_DIV0 && e.operand != gb::B_TRUNC_MOD0)
+      return fail(GAGP_DECLINED, "builtin outside the resident subset");
+    if (e.kind == gb::EK_BOUND && (e.arity != 0 || e.node_kind != gb::TK_BOUND || e.operand < 0 ||
+                                   e.operand >= gb::kLowerBinders))
+      return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": bound read");
+    if (e.kind == gb::EK_INPUT && (e.operand < 0 || e.operand >= g->local_count))
+      return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": input position");
+    if (e.kind == gb::EK_REFERENCE) {
+      if (e.target < 0 || e.target >= NT) return fail(GAGP_INVALID_ARGUMENT, "reference to a missing nonterminal");
+      const gagp_nonterminal& n = g->nonterminals[e.target];
+      if (n.production_count < 1 || n.production_offset < 0 || n.production_offset > PR ||
+          n.production_count > PR - n.production_offset)
+        return fail(GAGP_INVALID_ARGUMENT, "nonterminal " + std::to_string(e.target) + ": production range");
+      for (int k = 0; k < n.production_count; ++k) {
+        const int x = g->productions[n.production_offset + k].expression;
+        if (x < 0 || x >= E) return fail(GAGP_INVALID_ARGUMENT, "production of a missing expression");
+      }
+    } else if (e.kind == gb::EK_CONSTANT) {
+      if (e.arity != 0 || e.target < 0 || e.target >= ND) return fail(GAGP_INVALID_ARGUMENT, "constant domain");
+    } else {
+      for (int k = 0; k < e.arity; ++k)
+        if (e.children[k] < 0 || e.children[k] >= E) return fail(GAGP_INVALID_ARGUMENT, "child of a missing expression");
+    }
+  }
+  for (int j = 0; j < g->local_count; ++j)
+    if (!value_tag(g->local_types[j])) return fail(GAGP_DECLINED, "input type outside Int, Bool and IntList");
+  if (c->expected_tag != GAGP_TAG_INT && c->expected_tag != GAGP_TAG_BOOL)
+    return fail(GAGP_DECLINED, "expected outputs other than Int and Bool are outside the resident subset");
+  // every IntList input is a length word and its elements inside list_values
+  for (int j = 0; j < c->input_count; ++j) {
+    if (!c->input_tags || c->input_tags[j] != g->local_types[j])
+      return fail(GAGP_INVALID_ARGUMENT, "case input tags must equal the grammar's input types");
+    if (c->input_tags[j] != GAGP_TAG_INTLIST) continue;
+    if (!c->list_values || c->list_value_count < 1) return fail(GAGP_INVALID_ARGUMENT, "IntList inputs need list_values");
+    for (int k = 0; k < c->case_count; ++k) {
+      const int64_t at = c->inputs[size_t(k) * c->input_count + j];
+      if (at < 0 || at >= c->list_value_count) return fail(GAGP_INVALID_ARGUMENT, "IntList input outside list_values");
+      const int64_t len = c->list_values[at];
+      if (len < 0 || len > c->list_value_count - at - 1)
+        return fail(GAGP_INVALID_ARGUMENT, "IntList input overruns list_values");
+    }
+  }
+  return GAGP_OK;
+}
+
 // Admission checks of this engine (a decline reruns on the native path in
 // the reference).  Returns GAGP_OK or GAGP_DECLINED with a reason.
 gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg) {
@@ -278,37 +372,8 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
   if (maxv < 1 || maxv > gb::kMaxLowerNodes) return fail(GAGP_DECLINED, "variable node budget outside 1..256");
   if (g->slot_max_depth < 1 || g->slot_max_depth >= g->depth_count || g->depth_count > 65)
     return fail(GAGP_DECLINED, "depth budget");
-  // the subtree generator reads these tables without range checks: every id
-  // they hold must be in range
-  const int E = g->expression_count, NT = g->nonterminal_count, PR = g->production_count, ND = g->domain_count;
-  for (int i = 0; i < E; ++i) {
-    const gagp_expression& e = g->expressions[i];
-    if (e.kind == gb::EK_REFERENCE && e.scope_count != 0)
-      return fail(GAGP_DECLINED, "scoped nonterminals are outside the resident scalar subset");
-    if (e.kind == gb::EK_BOUND || e.kind == gb::EK_ALIAS)
-      return fail(GAGP_DECLINED, "lexical binders/templates are outside the resident scalar subset");
-    if (e.kind != gb::EK_REFERENCE && e.kind != gb::EK_CONSTANT && e.kind != gb::EK_OPERATION &&
-        e.kind != gb::EK_INPUT)
-      return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": unknown kind");
-    if (e.arity < 0 || e.arity > 3) return fail(GAGP_DECLINED, "arity capacity");
-    if (e.kind == gb::EK_REFERENCE) {
-      if (e.target < 0 || e.target >= NT) return fail(GAGP_INVALID_ARGUMENT, "reference to a missing nonterminal");
-      const gagp_nonterminal& n = g->nonterminals[e.target];
-      if (n.scope_count != 0) return fail(GAGP_DECLINED, "scoped nonterminals are outside the resident scalar subset");
-      if (n.production_count < 1 || n.production_offset < 0 || n.production_offset > PR ||
-          n.production_count > PR - n.production_offset)
-        return fail(GAGP_INVALID_ARGUMENT, "nonterminal " + std::to_string(e.target) + ": production range");
-      for (int k = 0; k < n.production_count; ++k) {
-        const int x = g->productions[n.production_offset + k].expression;
-        if (x < 0 || x >= E) return fail(GAGP_INVALID_ARGUMENT, "production of a missing expression");
-      }
-    } else if (e.kind == gb::EK_CONSTANT) {
-      if (e.arity != 0 || e.target < 0 || e.target >= ND) return fail(GAGP_INVALID_ARGUMENT, "constant domain");
-    } else {
-      for (int k = 0; k < e.arity; ++k)
-        if (e.children[k] < 0 || e.children[k] >= E) return fail(GAGP_INVALID_ARGUMENT, "child of a missing expression");
-    }
-  }
+  if (const gagp_status st = check_tables_and_cases(g, c); st != GAGP_OK) return st;
+  const int ND = g->domain_count;
   for (int i = 0; i < ND; ++i) {
     const gagp_domain& d = g->domains[i];
     if (d.integer_range) {
@@ -456,13 +521,64 @@ DrawTables draw_tables(const gagp_grammar* g, bool with_draws) {
   return t;
 }
 
+// Instructions (and constants) the lowering can emit for a row of at most
+// `maxv` nodes, the appended RETURN included: a leaf or operation emits 1, a
+// value if 2 (its jumps), and/or 5, and a traversal at most 36 of its own
+// beside its four children, so at most 8 per node of a row holding
+// traversals (36 + 4 children over 5 nodes).
+int bytecode_bound(const gagp_grammar* g, int maxv) {
+  int per_node = 1;
+  for (int i = 0; i < g->expression_count; ++i) {
+    const int nk = g->expressions[i].node_kind;
+    if (g->expressions[i].kind == gb::EK_OPERATION)
+      per_node = std::max(per_node, nk == gb::TK_TRAVERSE ? 8 : nk == gb::TK_IF ? 2
+                                    : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
+  }
+  return per_node * maxv + 2;
+}
+
+// Whether a grammar's programs mostly need the exact VM: it holds
+// traversals or bound reads, or operations that can raise a runtime error
+// (modulo and division by zero, list builtins).
+bool exact_heavy(const gagp_grammar* g) {
+  for (int i = 0; i < g->expression_count; ++i) {
+    const gagp_expression& e = g->expressions[i];
+    if (e.kind == gb::EK_BOUND) return true;
+    if (e.kind != gb::EK_OPERATION) continue;
+    if (e.node_kind == gb::TK_TRAVERSE) return true;
+    if (e.node_kind == gb::TK_OPERATION &&
+        gb::accumulator_op_of(e.node_kind, e.opcode, e.operand) == gb::A_COUNT)
+      return true;
+  }
+  return false;
+}
+
+// Device copy of the traversal table.
+std::vector<gb::RegionInfo> region_infos(const gagp_grammar* g) {
+  std::vector<gb::RegionInfo> out(std::max(1, g->region_count));
+  for (int r = 0; r < g->region_count; ++r) {
+    const gagp_region& x = g->regions[r];
+    gb::RegionInfo& y = out[r];
+    y.traversal = int8_t(x.traversal);
+    y.ranged = int8_t(x.ranged);
+    y.arity = int8_t(x.ranged ? 6 : 4);
+    y.result_type = int8_t(x.result_type);
+    for (int k = 0; k < 3; ++k) {
+      y.binders[k] = int8_t(x.binders[k]);
+      y.binding_types[k] = int8_t(x.binding_types[k]);
+    }
+    for (int k = 0; k < 6; ++k) y.operand_types[k] = int8_t(x.operand_types[k]);
+  }
+  return out;
+}
+
 struct Plan {
   Layout L;
   size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, gen_level, gen_entry, gen_expr,
-      gen_nt, local_types, inputs, expected;
+      gen_nt, local_types, regions, inputs, expected, lists;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
-  size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_consts;
+  size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, child_level, level_plan, round,
       hist_sum, hist_fitness,
       hist_wrong,
@@ -476,13 +592,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   const int maxv = g->max_nodes - g->fixed_nodes;
   p.stride = int(align_up(size_t(maxv), 4));
   p.code_stride = 2 * maxv + 8;
-  // bytecode bound: if -> 2 instructions, and/or -> 5, everything else 1
-  int per_node = 1;
-  for (int i = 0; i < g->expression_count; ++i) {
-    const int nk = g->expressions[i].node_kind;
-    if (g->expressions[i].kind == gb::EK_OPERATION) per_node = std::max(per_node, nk == gb::TK_IF ? 2 : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
-  }
-  p.bc_stride = per_node * maxv + 2;
+  p.bc_stride = bytecode_bound(g, maxv);
   p.slots = std::max(P, B);
   const long long draws = (long long)B * cfg->replacement_size + 1;
   p.stream_capacity = int(((draws + 311) / 312 + 2) * 312);
@@ -505,8 +615,10 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.gen_expr = L.take(sizeof(gb::GenExpr) * size_t(E));
   p.gen_nt = L.take(sizeof(gb::GenNt) * size_t(std::max(1, g->nonterminal_count)));
   p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
+  p.regions = L.take(sizeof(gb::RegionInfo) * size_t(std::max(1, g->region_count)));
   p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
   p.expected = L.take(sizeof(int64_t) * C);
+  p.lists = L.take(sizeof(int64_t) * size_t(std::max<int64_t>(1, c->list_values ? c->list_value_count : 0)));
   const size_t S = size_t(p.stride);
   p.node = L.take(8 * S * P); p.cval = L.take(8 * S * P); p.len = L.take(4 * size_t(P));
   p.cnode = L.take(8 * S * B); p.ccval = L.take(8 * S * B); p.clen = L.take(4 * size_t(B));
@@ -518,7 +630,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
   p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots); p.vm_acc = L.take(16 * slots);
-  p.bc = L.take(20 * slots * p.bc_stride); p.bc_len = L.take(4 * slots);
+  p.bc = L.take(20 * slots * p.bc_stride); p.bc_len = L.take(4 * slots); p.bc_locals = L.take(4 * slots);
   p.bc_consts = L.take(8 * slots * p.bc_stride);
   p.mt = L.take(8 * 312); p.stream = L.take(8 * size_t(p.stream_capacity));
   p.stream_mod = L.take(4 * size_t(p.stream_capacity)); p.stream_head = L.take(16);
@@ -581,6 +693,7 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   CUDA_TRY(cudaFuncSetAttribute(gb::k_vary, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
+  CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_general, cudaFuncAttributeMaxDynamicSharedMemorySize, int(e->max_smem) - 1024));
   *out = e.release();
   return GAGP_OK;
 }
@@ -644,6 +757,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   s->stride = p.stride;
   s->fixed_nodes = g->fixed_nodes;
   s->has_wrong = cfg->metric != GAGP_METRIC_LEGACY;
+  s->exact_heavy = exact_heavy(g);
   s->bytes = p.L.total;
   CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->block), s->bytes, e->pool, e->stream));
   CUDA_TRY(cudaMemsetAsync(s->block, 0, s->bytes, e->stream));
@@ -722,8 +836,12 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   }
   CUDA_TRY(up(p.gen_nt, gen_nt.data(), sizeof(gb::GenNt) * gen_nt.size()));
   CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
+  const std::vector<gb::RegionInfo> regions = region_infos(g);
+  CUDA_TRY(up(p.regions, regions.data(), sizeof(gb::RegionInfo) * regions.size()));
   CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
   CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
+  const int64_t n_lists = c->list_values ? c->list_value_count : 0;
+  if (n_lists) CUDA_TRY(up(p.lists, c->list_values, sizeof(int64_t) * size_t(n_lists)));
 
   gb::SearchDesc& d = s->desc;
   d.ex = at<gagp_expression>(b, p.ex);
@@ -739,6 +857,8 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.gen_expr = at<gb::GenExpr>(b, p.gen_expr);
   d.gen_nt = at<gb::GenNt>(b, p.gen_nt);
   d.local_types = at<int32_t>(b, p.local_types);
+  d.regions = at<gb::RegionInfo>(b, p.regions);
+  d.n_regions = g->region_count;
   d.n_ex = E; d.n_prods = g->production_count; d.n_nts = g->nonterminal_count;
   d.n_doms = g->domain_count; d.n_vals = g->value_count;
   d.depth_count = g->depth_count; d.logical_count = g->logical_depth_count; d.site_depth = g->site_depth;
@@ -757,6 +877,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.rounds_per_epoch = s->P / s->B;
   d.generations = s->G;
   d.inputs = at<int64_t>(b, p.inputs); d.expected = at<int64_t>(b, p.expected);
+  d.lists = at<int64_t>(b, p.lists); d.n_lists = n_lists;
   d.C = C; d.n_inputs = NI; d.expected_tag = c->expected_tag; d.vm_cases_per_lane = cases_per_lane(C);
   d.node = at<uint64_t>(b, p.node); d.cval = at<int64_t>(b, p.cval); d.len = at<int32_t>(b, p.len);
   d.cnode = at<uint64_t>(b, p.cnode); d.ccval = at<int64_t>(b, p.ccval); d.clen = at<int32_t>(b, p.clen);
@@ -768,7 +889,8 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
   d.vm_acc = at<unsigned long long>(b, p.vm_acc);
-  d.bc = at<int32_t>(b, p.bc); d.bc_len = at<int32_t>(b, p.bc_len); d.bc_consts = at<int64_t>(b, p.bc_consts);
+  d.bc = at<int32_t>(b, p.bc); d.bc_len = at<int32_t>(b, p.bc_len); d.bc_locals = at<int32_t>(b, p.bc_locals);
+  d.bc_consts = at<int64_t>(b, p.bc_consts);
   d.bc_stride = p.bc_stride;
   d.mt = at<uint64_t>(b, p.mt); d.stream = at<uint64_t>(b, p.stream); d.stream_mod = at<uint32_t>(b, p.stream_mod);
   d.stream_head = at<long long>(b, p.stream_head); d.stream_capacity = p.stream_capacity;
@@ -832,9 +954,10 @@ struct BatchView {
   int32_t* d_child_off = nullptr;    // n + 1
   int n = 0, total_members = 0, total_children = 0, max_P = 0, max_lanes = 1, max_rounds = 0, max_stride = 4;
   long long max_draws = 0;
-  int max_code_stride = 2;
+  int max_code_stride = 2, max_bc_stride = 2;
   int max_C = 1, max_inputs = 0;
   int min_B = 1 << 30;               // the smallest round of the batch
+  bool exact_heavy = false;          // some search's programs mostly need the exact VM
 };
 
 gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
@@ -880,10 +1003,13 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
   v->max_stride = 4;
   v->max_draws = 0;
   v->max_code_stride = 2;
+  v->max_bc_stride = 2;
   v->max_lanes = 1;
   v->max_C = 1;
   v->max_inputs = 0;
+  v->exact_heavy = false;
   for (Search* s : list) {
+    v->exact_heavy |= s->exact_heavy;
     v->max_C = std::max(v->max_C, s->desc.C);
     v->max_inputs = std::max(v->max_inputs, s->desc.n_inputs);
     v->total_members += s->P;
@@ -893,6 +1019,7 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
     v->max_rounds = std::max(v->max_rounds, s->total_rounds);
     v->max_stride = std::max(v->max_stride, s->stride);
     v->max_code_stride = std::max(v->max_code_stride, s->desc.code_stride);
+    v->max_bc_stride = std::max(v->max_bc_stride, s->desc.bc_stride);
     v->max_draws = std::max(v->max_draws, (long long)s->B * s->desc.replacement_size + 1);
     v->min_B = std::min(v->min_B, s->B);
   }
@@ -901,20 +1028,44 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
 
 int blocks_for(int items, int threads) { return std::max(1, (items + threads - 1) / threads); }
 
-// Evaluates lowered programs listed by k_lower (both VMs).
+// Evaluates lowered programs listed by k_lower: counts[0] programs on the
+// fast (accumulator) VM, counts[1] on the exact VM.
 // Fast-VM launch of one instantiation.
-// One VM launch over both lists: counts[0] fast programs, counts[1] programs
-// that need the exact VM.
 void vm_fast_launch(int lanes, int blocks, int threads, size_t smem, cudaStream_t stream, const gb::SearchDesc* descs,
-                    int mode, const gb::ProgramRef* list, const gb::ProgramRef* general, const int32_t* counts,
-                    int temp_stride, int code_stride, int const_stride, int max_C) {
+                    int mode, const gb::ProgramRef* list, const int32_t* counts, int temp_stride, int code_stride,
+                    int const_stride, int max_C) {
   const int tiles = (max_C + 32 * lanes - 1) / (32 * lanes);
   switch (lanes) {
-    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, general, counts + 1, temp_stride, code_stride, const_stride, tiles); break;
-    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, general, counts + 1, temp_stride, code_stride, const_stride, tiles); break;
-    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, general, counts + 1, temp_stride, code_stride, const_stride, tiles); break;
+    case 1: gb::k_vm_fast<1><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, temp_stride, code_stride, const_stride, tiles); break;
+    case 2: gb::k_vm_fast<2><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, temp_stride, code_stride, const_stride, tiles); break;
+    default: gb::k_vm_fast<4><<<blocks, threads, smem, stream>>>(descs, mode, list, counts, temp_stride, code_stride, const_stride, tiles); break;
   }
 }
+
+// Exact-VM launch over counts[1] programs: persistent blocks of 256 threads,
+// each program's bytecode (bc_stride_max instructions of 20 bytes) and
+// constants (8 bytes each) staged in dynamic shared memory.
+constexpr int kGeneralThreads = 256;
+size_t vm_general_smem(int bc_stride_max) { return size_t(bc_stride_max) * (20 + 8); }
+// `heavy`: most programs may be on the list, so the grid fills every SM;
+// otherwise the list is rarely more than a handful of programs and a
+// quarter of the SMs take them (an empty launch of a full grid costs a few
+// microseconds on every range's critical path).
+gagp_status vm_general_launch(int sm_count, cudaStream_t stream, const gb::SearchDesc* descs, int mode,
+                              const gb::ProgramRef* list, const int32_t* counts, int bc_stride_max, bool heavy) {
+  const size_t smem = vm_general_smem(bc_stride_max);
+  int blocks = std::max(1, sm_count / 4);
+  if (heavy) {
+    int per_sm = 0;
+    const cudaError_t occ = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vm_general, kGeneralThreads,
+                                                                          smem);
+    if (occ != cudaSuccess) return fail(GAGP_DEVICE_ERROR, std::string("exact VM occupancy: ") + cudaGetErrorString(occ));
+    blocks = sm_count * std::max(1, per_sm);
+  }
+  gb::k_vm_general<<<blocks, kGeneralThreads, smem, stream>>>(descs, mode, list, counts + 1, bc_stride_max);
+  return GAGP_OK;
+}
+
 
 // The VM configuration of one round: the tuned cases per lane, or the next
 // candidate to time (measure_key != 0) while the shape is being tuned.
@@ -962,7 +1113,7 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
   }
   {
     Timed t(e, KN_VM_FAST, stream);
-    vm_fast_launch(plan.lanes, blocks, warps * 32, smem, stream, v.d_desc, mode, fast, general, counts, temp_stride,
+    vm_fast_launch(plan.lanes, blocks, warps * 32, smem, stream, v.d_desc, mode, fast, counts, temp_stride,
                    code_stride, const_stride, v.max_C);
   }
   if (plan.measure_key) {
@@ -970,7 +1121,8 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
     e->tune_marks.push_back({plan.measure_key, plan.cand, mark_start, mark_stop});
     ++e->vm_tune[plan.measure_key].pending;
   }
-  return GAGP_OK;
+  Timed t(e, KN_VM_GENERAL, stream);
+  return vm_general_launch(e->sm_count, stream, v.d_desc, mode, general, counts, v.max_bc_stride, v.exact_heavy);
 }
 
 gagp_status launch_start(gagp_engine* e, const BatchView& v) {
@@ -1174,8 +1326,8 @@ namespace {
 // one caller-provided device region.
 struct EvalPlan {
   Layout L;
-  size_t desc, ex, info, minimum, local_types, inputs, expected, node, cval, len, code, code_len, kpool, code_temps, vm_acc,
-      bc, bc_len, bc_consts, fitness, wrong, counters, round, fast, general, counts, off;
+  size_t desc, ex, info, minimum, local_types, regions, inputs, expected, lists, node, cval, len, code, code_len, kpool,
+      code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts, fitness, wrong, counters, round, fast, general, counts, off;
   int stride, code_stride, bc_stride;
 };
 
@@ -1184,13 +1336,7 @@ EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   const int maxv = g->max_nodes - g->fixed_nodes;
   p.stride = int(align_up(size_t(std::max(1, maxv)), 4));
   p.code_stride = 2 * maxv + 8;
-  int per_node = 1;
-  for (int i = 0; i < g->expression_count; ++i) {
-    const int nk = g->expressions[i].node_kind;
-    if (g->expressions[i].kind == gb::EK_OPERATION)
-      per_node = std::max(per_node, nk == gb::TK_IF ? 2 : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
-  }
-  p.bc_stride = per_node * maxv + 2;
+  p.bc_stride = bytecode_bound(g, maxv);
   const int E = g->expression_count, C = c->case_count;
   const size_t R = size_t(std::max(1, rows)), S = size_t(p.stride);
   auto& L = p.L;
@@ -1199,12 +1345,15 @@ EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   p.info = L.take(sizeof(gb::ExprInfo) * E);
   p.minimum = L.take(sizeof(uint32_t));
   p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
+  p.regions = L.take(sizeof(gb::RegionInfo) * size_t(std::max(1, g->region_count)));
   p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
   p.expected = L.take(sizeof(int64_t) * C);
+  p.lists = L.take(sizeof(int64_t) * size_t(std::max<int64_t>(1, c->list_values ? c->list_value_count : 0)));
   p.node = L.take(8 * S * R); p.cval = L.take(8 * S * R); p.len = L.take(4 * R);
   p.code = L.take(8 * R * p.code_stride); p.code_len = L.take(4 * R); p.kpool = L.take(8 * R * S);
   p.code_temps = L.take(4 * R); p.vm_acc = L.take(16 * R);
-  p.bc = L.take(20 * R * p.bc_stride); p.bc_len = L.take(4 * R); p.bc_consts = L.take(8 * R * p.bc_stride);
+  p.bc = L.take(20 * R * p.bc_stride); p.bc_len = L.take(4 * R); p.bc_locals = L.take(4 * R);
+  p.bc_consts = L.take(8 * R * p.bc_stride);
   p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.counters = L.take(8 * GAGP_COUNTERS); p.round = L.take(16);
   p.fast = L.take(sizeof(gb::ProgramRef) * R); p.general = L.take(sizeof(gb::ProgramRef) * R);
   p.counts = L.take(16); p.off = L.take(8);
@@ -1226,6 +1375,7 @@ gagp_status eval_check(const gagp_grammar* g, const gagp_cases* c, const gagp_se
   if (g->expression_count < 1 || g->expression_count > 65534) return fail(GAGP_DECLINED, "expression table capacity");
   const int maxv = g->max_nodes - g->fixed_nodes;
   if (maxv < 1 || maxv > gb::kMaxLowerNodes) return fail(GAGP_DECLINED, "variable node budget outside 1..256");
+  if (const gagp_status st = check_tables_and_cases(g, c); st != GAGP_OK) return st;
   if (rows->count < 0 || (rows->count && (!rows->node_counts || !rows->origins || !rows->constant_counts)))
     return fail(GAGP_INVALID_ARGUMENT, "rows");
   for (int r = 0; r < rows->count; ++r) {
@@ -1290,6 +1440,8 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.minimum = at<uint32_t>(b, p.minimum);
   d.prod_minimum = d.minimum;  // no subtree generation in row evaluation
   d.local_types = at<int32_t>(b, p.local_types);
+  d.regions = at<gb::RegionInfo>(b, p.regions);
+  d.n_regions = g->region_count;
   d.n_ex = E;
   d.slot_type = g->slot_type;
   d.local_count = g->local_count;
@@ -1307,6 +1459,9 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.penalty_int = (int64_t)std::fabs(cfg->penalty);
   d.inputs = at<int64_t>(b, p.inputs);
   d.expected = at<int64_t>(b, p.expected);
+  const int64_t n_lists = c->list_values ? c->list_value_count : 0;
+  d.lists = at<int64_t>(b, p.lists);
+  d.n_lists = n_lists;
   d.C = C;
   d.n_inputs = NI;
   d.expected_tag = c->expected_tag;
@@ -1322,6 +1477,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.vm_acc = at<unsigned long long>(b, p.vm_acc);
   d.bc = at<int32_t>(b, p.bc);
   d.bc_len = at<int32_t>(b, p.bc_len);
+  d.bc_locals = at<int32_t>(b, p.bc_locals);
   d.bc_consts = at<int64_t>(b, p.bc_consts);
   d.bc_stride = p.bc_stride;
   d.fitness = at<double>(b, p.fitness);
@@ -1336,8 +1492,11 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   CUDA_TRY(up(p.ex, g->expressions, sizeof(gagp_expression) * E));
   CUDA_TRY(up(p.info, info.data(), sizeof(gb::ExprInfo) * E));
   CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
+  const std::vector<gb::RegionInfo> regions = region_infos(g);
+  CUDA_TRY(up(p.regions, regions.data(), sizeof(gb::RegionInfo) * regions.size()));
   CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
   CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
+  if (n_lists) CUDA_TRY(up(p.lists, c->list_values, sizeof(int64_t) * size_t(n_lists)));
   CUDA_TRY(up(p.node, node.data(), 8 * node.size()));
   CUDA_TRY(up(p.cval, cval.data(), 8 * cval.size()));
   CUDA_TRY(up(p.len, len.data(), 4 * len.size()));
@@ -1359,8 +1518,12 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   const size_t smem = size_t(warps) * (temp_stride + code_stride + p.stride) * sizeof(int64_t);
   if (smem > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the VM's shared memory");
   const int per_sm = std::max(1, std::min(4, int((max_smem - 1024) / smem)));
-  vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, general, counts, temp_stride,
-                 code_stride, p.stride, C);
+  vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, counts, temp_stride, code_stride,
+                 p.stride, C);
+  if (vm_general_smem(p.bc_stride) > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the exact VM");
+  if (const gagp_status st = vm_general_launch(sm_count, stream, dd, 0, general, counts, p.bc_stride, true);
+      st != GAGP_OK)
+    return st;
   CUDA_TRY(cudaGetLastError());
   int32_t round[4];
   CUDA_TRY(cudaMemcpyAsync(round, b + p.round, sizeof round, cudaMemcpyDeviceToHost, stream));
@@ -1407,6 +1570,7 @@ gagp_status static_scratch_on(int device, StaticDevice** out) {
     CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
     CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
     CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
+    CUDA_TRY(cudaFuncSetAttribute(gb::k_vm_general, cudaFuncAttributeMaxDynamicSharedMemorySize, smem - 1024));
     d.scratch = static_cast<char*>(ptr);
     d.sm_count = sms;
     d.max_smem = size_t(smem);

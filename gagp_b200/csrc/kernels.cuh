@@ -109,17 +109,18 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
       continue;
     }
     if (lane == 0) {
-      int nconst = 0, bound = 0;
-      const int bl = lower_reference(s, t, s.bc + size_t(slot) * 5 * s.bc_stride, s.bc_stride,
-                                     s.bc_consts + size_t(slot) * s.bc_stride, &nconst, &bound);
+      LowerResult r{};
+      const int bl = lower_program(lower_view(s), t.node, t.cval, t.n, t.nc, s.bc + size_t(slot) * 5 * s.bc_stride,
+                                   s.bc_stride, s.bc_consts + size_t(slot) * s.bc_stride, s.bc_stride, &r);
       if (bl < 0) {
         raise_error(s, 30);  // the phase compiler rejected a constructed program
       } else {
         s.bc_len[slot] = bl;
+        s.bc_locals[slot] = r.locals;
         s.code_temps[slot] = -1;
         general_list[atomicAdd(&list_count[1], 1)] = ProgramRef{si, slot};
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
-                  (unsigned long long)(row_bytes + 20ull * bl + 8ull * nconst + 16));
+                  (unsigned long long)(row_bytes + 20ull * bl + 8ull * r.constants + 16));
       }
     }
     __syncwarp();
@@ -137,24 +138,43 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
   }
 }
 
-// General VM: the block's threads run one program of the general list at a
-// time, thread per case (any block size that is a multiple of 32).
-__device__ inline void vm_general_programs(const SearchDesc* descs, int mode, const ProgramRef* list, int count) {
+// General VM: the programs the accumulator VM cannot run (list programs,
+// possible runtime errors or fuel exhaustion) on the exact interpreter.
+// Persistent blocks take one program of the list at a time: its bytecode
+// and constants are staged in shared memory (dynamic: bc_stride_max
+// instructions and constants), then the block's threads run its cases, a
+// case per thread, and the block reduces the losses in order-free integer
+// sums.  A separate kernel from the fast VM, so that the interpreter's
+// registers and local arrays do not lower the fast VM's occupancy.
+__global__ void __launch_bounds__(256) k_vm_general(const SearchDesc* descs, int mode, const ProgramRef* list,
+                                                    const int32_t* list_count, int bc_stride_max) {
+  extern __shared__ __align__(16) int64_t smem_general[];
   __shared__ int64_t red_loss[32];
   __shared__ uint32_t red_wrong[32];
+  __shared__ unsigned long long red_steps[32];
+  int64_t* consts = smem_general;
+  int32_t* code = reinterpret_cast<int32_t*>(smem_general + bc_stride_max);
+  const int count = *list_count;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = blockIdx.x; i < count; i += gridDim.x) {
     const ProgramRef p = list[i];
     const SearchDesc& s = descs[p.search];
-    const int32_t* code = s.bc + size_t(p.slot) * 5 * s.bc_stride;
-    const int64_t* consts = s.bc_consts + size_t(p.slot) * s.bc_stride;
-    const int n = s.bc_len[p.slot];
+    const int n = s.bc_len[p.slot], n_locals = s.bc_locals[p.slot];
+    {
+      const int32_t* gcode = s.bc + size_t(p.slot) * 5 * s.bc_stride;
+      const int64_t* gconsts = s.bc_consts + size_t(p.slot) * s.bc_stride;
+      for (int k = threadIdx.x; k < 5 * n; k += blockDim.x) code[k] = gcode[k];
+      for (int k = threadIdx.x; k < n; k += blockDim.x) consts[k] = gconsts[k];  // at most one constant per instruction
+    }
+    __syncthreads();
+    const VmView view = vm_view(s);
     int64_t loss = 0;
     uint32_t wrong = 0;
     uint64_t steps = 0;
     for (int c = threadIdx.x; c < s.C; c += blockDim.x) {
       int64_t value = 0;
       int tag = 0;
-      if (run_reference(s, code, n, consts, c, value, tag, steps)) {
+      if (run_program(view, code, n, consts, n_locals, c, value, tag, steps)) {
         loss += case_loss(s, tag, value, s.expected[c], wrong);
       } else {
         loss += error_loss(s);
@@ -164,15 +184,15 @@ __device__ inline void vm_general_programs(const SearchDesc* descs, int mode, co
     loss = warp_sum(loss);
     wrong = warp_sum(wrong);
     steps = warp_sum(steps);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) { red_loss[warp] = loss; red_wrong[warp] = wrong; }
-    if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), (unsigned long long)steps);
+    if (lane == 0) { red_loss[warp] = loss; red_wrong[warp] = wrong; red_steps[warp] = steps; }
     __syncthreads();
     if (threadIdx.x == 0) {
       int64_t tl = 0;
       uint32_t tw = 0;
-      for (int w = 0; w < (blockDim.x >> 5); ++w) { tl += red_loss[w]; tw += red_wrong[w]; }
+      unsigned long long ts = 0;
+      for (int w = 0; w < (blockDim.x >> 5); ++w) { tl += red_loss[w]; tw += red_wrong[w]; ts += red_steps[w]; }
       store_result(s, mode, p.slot, tl, tw);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), ts);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
     }
@@ -199,13 +219,10 @@ __device__ __forceinline__ void run_k(const SearchDesc& s, int slot, const VmWar
 // and wrong count to the program's accumulators and the last tile to finish
 // stores the program's result (integer sums: the order does not matter).
 template <int K>
-__global__ void __launch_bounds__(256) k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list,
-                                                 const int32_t* list_count, const ProgramRef* general,
-                                                 const int32_t* general_count, int temp_stride, int code_stride,
+__global__ void __launch_bounds__(256, K == 4 ? 2 : 4) k_vm_fast(const SearchDesc* descs, int mode, const ProgramRef* list,
+                                                 const int32_t* list_count, int temp_stride, int code_stride,
                                                  int const_stride, int tiles_max) {
   extern __shared__ __align__(16) int64_t smem_vm[];
-  // the programs that need the exact VM first, a block each (rarely any)
-  vm_general_programs(descs, mode, general, *general_count);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
   const size_t per_warp = size_t(temp_stride) + size_t(code_stride) + size_t(const_stride);  // int64 units

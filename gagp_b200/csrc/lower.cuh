@@ -17,12 +17,17 @@
 
 namespace gb {
 
+// Opcode (cpp/include/gagp/core/opcode.hpp:8-37) and BuiltinId
+// (cpp/include/gagp/core/builtin.hpp:13-45) numbers.
 enum {
-  OP_PUSH_CONST = 0, OP_LOAD = 1, OP_NEG = 3, OP_NOT = 4, OP_ADD = 5, OP_SUB = 6, OP_MUL = 7, OP_DIV = 8,
-  OP_MOD = 9, OP_LT = 10, OP_LE = 11, OP_GT = 12, OP_GE = 13, OP_EQ = 14, OP_NE = 15, OP_JMP = 16,
-  OP_JMP_IF_FALSE = 17, OP_JMP_IF_TRUE = 18, OP_CALL_BUILTIN = 19, OP_RETURN = 20
+  OP_PUSH_CONST = 0, OP_LOAD = 1, OP_STORE = 2, OP_NEG = 3, OP_NOT = 4, OP_ADD = 5, OP_SUB = 6, OP_MUL = 7,
+  OP_DIV = 8, OP_MOD = 9, OP_LT = 10, OP_LE = 11, OP_GT = 12, OP_GE = 13, OP_EQ = 14, OP_NE = 15, OP_JMP = 16,
+  OP_JMP_IF_FALSE = 17, OP_JMP_IF_TRUE = 18, OP_CALL_BUILTIN = 19, OP_RETURN = 20, OP_CHECK_INT = 22
 };
-enum { B_ABS = 0, B_MIN = 1, B_MAX = 2, B_IDIV0 = 13, B_IMOD0 = 14, B_TRUNC_DIV0 = 28, B_TRUNC_MOD0 = 29 };
+enum {
+  B_ABS = 0, B_MIN = 1, B_MAX = 2, B_LEN = 4, B_INDEX = 7, B_IDIV0 = 13, B_IMOD0 = 14, B_TRUNC_DIV0 = 28,
+  B_TRUNC_MOD0 = 29
+};
 
 // Accumulator VM operations.
 enum : uint32_t {
@@ -46,16 +51,78 @@ struct LRow {
   int n, nc;
 };
 
-// Reference bytecode of a value phase.  Returns the instruction count
-// (including the appended RETURN) or -1 when the compiler rejects the row.
-// Code: 5 ints per instruction (op, flags, a, b, fuel).
-__device__ inline int lower_reference(const SearchDesc& s, const LRow& t, int32_t* code, int code_cap,
-                                      int64_t* consts, int* n_consts, int* stack_bound_out) {
-  struct Frame { int node, base_stack, first_jump, second_jump, seen; int8_t args[3]; };
+// What lowering reads of an admitted search: the expression table, the
+// traversal table, the evaluator inputs (the preset locals), the phase's
+// result type and the fuel of the appended RETURN.
+struct LowerView {
+  const gagp_expression* ex;
+  const RegionInfo* regions;
+  int n_ex, n_regions;
+  int local_count;
+  const int32_t* local_types;
+  int slot_type;
+  uint32_t return_fuel;
+};
+__host__ __device__ inline LowerView lower_view(const SearchDesc& s) {
+  return LowerView{s.ex, s.regions, s.n_ex, s.n_regions, s.local_count, s.local_types, s.slot_type, s.return_fuel};
+}
+
+// Shape of a lowered program.
+struct LowerResult {
+  int code;         // instructions, the appended RETURN included
+  int constants;    // constant pool entries
+  int locals;       // inputs + temporaries
+  int stack_bound;  // deepest value stack
+};
+
+constexpr int kMaxStack = 64;     // MAX_STACK (cpp/include/gagp/runtime/gpu/constants_gpu.hpp:9)
+constexpr int kLowerLocals = 64;  // phase compiler local capacity
+constexpr int kLowerWalks = 8;    // open traversals on one lowering path (kPhaseWalks)
+constexpr int kLowerBinders = 16; // lexical binder numbers (kPhaseBinders)
+// instruction flags (DINSTR_HAS_A / DINSTR_HAS_B); bit 2 marks a Bool
+// constant, whose tag the reference keeps in its constant Value
+constexpr int kHasA = 1, kHasB = 2, kBoolConst = 4;
+
+// Reference bytecode of a whole-program value phase: compile_phase_tree
+// (cpp/src/evolution/repro/gpu/device/phase_compile.cuh:207-895) for the
+// node kinds this engine admits -- constants, inputs, operations, value
+// ifs, and/or, bound reads and forward or reverse traversals without a fuel
+// profile -- followed by the RETURN that patch_whole_program appends
+// (phase_layout.hpp:476-500).  Instructions are 5 ints (op, flags, a, b,
+// fuel) and the constants int64 payloads (flags bit 2: a Bool).  The
+// emitted code, constant numbering, temporaries and their LIFO reuse
+// follow the reference step by step, so the program consumes the same fuel
+// and fails the same way on every case.  Returns the instruction count, or
+// -1 when the compiler rejects the row (or it exceeds a capacity).
+//
+// Without a fuel profile none of the traversal's operands is aliased and no
+// event is uncharged, so the reference's binder facts and analysed ifs
+// (which only decide aliases and uncharged checks) never change the output
+// and are not kept here.
+__host__ __device__ inline int lower_program(const LowerView& v, const uint64_t* node, const int64_t* cval, int n,
+                                             int nc, int32_t* code, int code_cap, int64_t* consts, int const_cap,
+                                             LowerResult* result) {
+  struct Frame {
+    int node, base_stack, first_jump, second_jump, seen;
+    int8_t args[3];
+  };
+  // one open traversal: its table entry, the first live temporary it owns,
+  // its storage slots, the loop head and the exit jump to patch, and the
+  // binder slots its body shadows
+  struct Walk {
+    int info, live_begin, xs, start, begin, limit, length, counter, element, index, state, loop_head, done_jump;
+    int8_t saved_slot[3], saved_type[3];
+  };
   Frame frames[64];
-  int depth = 0, cursor = 0, count = 0, nconst = 0, stack = 0, stack_bound = 0, row_const = 0;
+  Walk walks[kLowerWalks];
+  int8_t env_slot[kLowerBinders], env_type[kLowerBinders];
+  int8_t live[kLowerLocals], freed[kLowerLocals] = {};
+  for (int i = 0; i < kLowerBinders; ++i) { env_slot[i] = -1; env_type[i] = GAGP_TAG_INVALID; }
+  int depth = 0, walk_depth = 0, cursor = 0, count = 0, nconst = 0, stack = 0, stack_bound = 0, row_const = 0;
+  int total_locals = v.local_count, live_count = 0, free_count = 0;
   int completed = GAGP_TAG_INVALID;
   bool have_value = false;
+  if (n <= 0 || n > kCapacity || v.local_count < 0 || v.local_count > kLowerLocals) return -1;
   auto emit = [&](int op, unsigned fuel, int a, int b, int flags) -> bool {
     if (count >= code_cap) return false;
     int32_t* x = code + 5 * count++;
@@ -63,78 +130,216 @@ __device__ inline int lower_reference(const SearchDesc& s, const LRow& t, int32_
     return true;
   };
   auto grow = [&](int by) { stack += by; if (stack > stack_bound) stack_bound = stack; };
-  if (t.n <= 0 || t.n > kCapacity) return -1;
+  auto add_const = [&](int64_t value) -> int {
+    if (nconst >= const_cap) return -1;
+    consts[nconst] = value;
+    return nconst++;
+  };
+  // a traversal's own instructions: unit fuel (no fuel profile)
+  auto put = [&](int op, int a, int b, int flags, int delta) -> bool {
+    if (!emit(op, 1u, a, b, flags)) return false;
+    if (delta > 0) grow(delta); else stack += delta;
+    return true;
+  };
+  auto put_load = [&](int slot) { return put(OP_LOAD, slot, 0, kHasA, 1); };
+  auto put_store = [&](int slot) { return put(OP_STORE, slot, 0, kHasA, -1); };
+  auto put_int = [&](int64_t value) {
+    const int index = add_const(value);
+    return index >= 0 && put(OP_PUSH_CONST, index, 0, kHasA, 1);
+  };
+  auto temporary = [&]() -> int {
+    int slot;
+    if (free_count) slot = freed[--free_count];
+    else if (total_locals >= kLowerLocals) return -1;
+    else slot = total_locals++;
+    live[live_count++] = int8_t(slot);
+    return slot;
+  };
+  auto subtree_end = [&](int i) -> int {
+    int pending = 1;
+    while (pending) {
+      if (i < 0 || i >= n) return -1;
+      pending += w_arity(node[i++]) - 1;
+    }
+    return i;
+  };
+  // compile_region_prefix of a traversal after its child `c` completed
+  // (phase_compile.cuh:409-516, every event charged and nothing aliased)
+  auto walk_after = [&](Walk& w, int c) -> bool {
+    const RegionInfo& info = v.regions[w.info];
+    const bool reverse = info.traversal == 2;
+    const int arity = info.arity;
+    if (c == 0 && !put_store(w.xs)) return false;                          // StoreSequence
+    if (c == 1) {
+      if (!put_store(w.start)) return false;                               // StoreStart
+      if (!put_load(w.start) || !put(OP_CHECK_INT, 0, 0, 0, 0) || !put_store(w.start)) return false;  // CheckStart
+      if (!put_load(w.xs) || !put(OP_CALL_BUILTIN, B_LEN, 1, kHasA | kHasB, 0) || !put_store(w.length))
+        return false;                                                      // ObserveSequence
+      if (!put_int(0) || !put_store(w.begin)) return false;                // SetBegin
+      if (!put_load(w.length) || !put_store(w.limit)) return false;        // SetEnd
+    }
+    if (c == arity - 2) {
+      if (!put_store(w.state)) return false;                               // InitializeState
+      if (!(reverse ? put_load(w.limit) : put_load(w.begin))) return false; // InitializeCursor
+      if (reverse && (!put_int(1) || !put(OP_SUB, 0, 0, 0, -1))) return false;
+      if (!put_store(w.counter)) return false;
+      w.loop_head = count;                                                 // TestCursor
+      if (!put_load(w.counter) || !(reverse ? put_load(w.begin) : put_load(w.limit)) ||
+          !put(reverse ? OP_GE : OP_LT, 0, 0, 0, -1))
+        return false;
+      w.done_jump = count;
+      if (!put(OP_JMP_IF_FALSE, 0, 0, kHasA, -1)) return false;
+      if (!put_load(w.xs) || !put_load(w.counter) || !put(OP_CALL_BUILTIN, B_INDEX, 2, kHasA | kHasB, -1))
+        return false;                                                      // ReadElement
+      if (!put_store(w.element)) return false;                             // BindElement
+      if (!put_load(w.start) || !put_load(w.counter) || !put(OP_ADD, 0, 0, 0, -1) || !put_store(w.index))
+        return false;                                                      // ComputeIndex
+      const int slots[3] = {w.element, w.index, w.state};
+      for (int k = 0; k < 3; ++k) {
+        const int b = info.binders[k];
+        w.saved_slot[k] = env_slot[b];
+        w.saved_type[k] = env_type[b];
+        env_slot[b] = int8_t(slots[k]);
+        env_type[b] = info.binding_types[k];
+      }
+    }
+    if (c == arity - 1) {
+      for (int k = 2; k >= 0; --k) {
+        const int b = info.binders[k];
+        env_slot[b] = w.saved_slot[k];
+        env_type[b] = w.saved_type[k];
+      }
+      if (!put_store(w.state)) return false;                               // UpdateState
+      if (!put_load(w.counter) || !put_int(1) || !put(reverse ? OP_SUB : OP_ADD, 0, 0, 0, -1) ||
+          !put_store(w.counter))
+        return false;                                                      // AdvanceCursor
+      if (!put(OP_JMP, w.loop_head, 0, kHasA, 0)) return false;            // Repeat
+      code[5 * w.done_jump + 2] = count;
+      if (!put_load(w.state)) return false;                                // Result
+    }
+    return true;
+  };
   for (;;) {
     if (!have_value) {
-      if (cursor >= t.n) return -1;
+      if (cursor >= n) return -1;
       const int index = cursor++;
-      const gagp_expression& e = s.ex[w_origin(t.node[index])];
+      const int origin = w_origin(node[index]);
+      if (origin < 0 || origin >= v.n_ex) return -1;
+      const gagp_expression& e = v.ex[origin];
       if (e.node_kind == TK_CONSTANT) {
-        // constants are Int payloads in prefix order
-        if (nconst >= kCapacity) return -1;
-        // the cursor visits nodes in prefix order, the order of row constants
-        if (row_const >= t.nc) return -1;
-        consts[nconst] = t.cval[row_const++];
-        if (!emit(OP_PUSH_CONST, e.fuel, nconst, 0, 1)) return -1;
-        ++nconst;
+        // constants are Int payloads in prefix order, the order the cursor
+        // visits the constant nodes in
+        if (row_const >= nc) return -1;
+        const int k = add_const(cval[row_const++]);
+        if (k < 0 || !emit(OP_PUSH_CONST, e.fuel, k, 0, kHasA)) return -1;
         grow(1);
         completed = GAGP_TAG_INT;
         have_value = true;
-      } else if (e.node_kind == TK_LOCAL) {
-        if (e.operand < 0 || e.operand >= s.local_count) return -1;
-        if (!emit(OP_LOAD, e.fuel, e.operand, 0, 1)) return -1;
+      } else if (e.node_kind == TK_BOUND && e.operand >= 0 && e.operand < kLowerBinders && env_slot[e.operand] >= 0) {
+        completed = env_type[e.operand];
+        if (e.type != GAGP_TAG_INVALID && e.type != completed) return -1;
+        if (!emit(OP_LOAD, e.fuel, env_slot[e.operand], 0, kHasA)) return -1;
         grow(1);
-        completed = e.type;
         have_value = true;
+      } else if (e.node_kind == TK_LOCAL || e.node_kind == TK_BOUND) {
+        if (e.operand < 0 || e.operand >= v.local_count) return -1;
+        if (!emit(OP_LOAD, e.fuel, e.operand, 0, kHasA)) return -1;
+        grow(1);
+        completed = v.local_types[e.operand];
+        have_value = true;
+      } else if (e.node_kind == TK_TRAVERSE) {
+        if (e.operand < 0 || e.operand >= v.n_regions) return -1;
+        const RegionInfo& info = v.regions[e.operand];
+        if ((info.traversal != 1 && info.traversal != 2) || info.ranged || e.arity != info.arity) return -1;
+        for (int k = 0; k < 3; ++k)
+          if (info.binders[k] < 0 || info.binders[k] >= kLowerBinders) return -1;
+        if (depth == 64 || walk_depth == kLowerWalks) return -1;
+        if (subtree_end(index) < 0) return -1;
+        Walk& w = walks[walk_depth++];
+        w.info = e.operand;
+        w.live_begin = live_count;
+        // the native temporary order
+        w.xs = temporary();
+        w.start = temporary();
+        w.begin = temporary();
+        w.limit = temporary();
+        w.length = temporary();
+        w.counter = temporary();
+        w.element = temporary();
+        w.index = temporary();
+        w.state = temporary();
+        if (w.xs < 0 || w.start < 0 || w.begin < 0 || w.limit < 0 || w.length < 0 || w.counter < 0 ||
+            w.element < 0 || w.index < 0 || w.state < 0)
+          return -1;
+        frames[depth++] = Frame{index, stack, -1, -1, 0, {0, 0, 0}};
+        continue;
       } else {
         if (e.arity < 1 || e.arity > 3 || depth == 64) return -1;
+        if (e.node_kind == TK_IF && e.arity != 3) return -1;
+        if ((e.node_kind == TK_AND || e.node_kind == TK_OR) && e.arity != 2) return -1;
+        if (e.node_kind != TK_OPERATION && e.node_kind != TK_IF && e.node_kind != TK_AND && e.node_kind != TK_OR)
+          return -1;
         frames[depth++] = Frame{index, stack, -1, -1, 0, {0, 0, 0}};
         continue;
       }
     }
     if (depth == 0) {
-      if (cursor != t.n || stack != 1 || completed != s.slot_type || stack_bound > 64) return -1;
-      if (!emit(OP_RETURN, s.return_fuel, 0, 0, 0)) return -1;
-      *n_consts = nconst;
-      *stack_bound_out = stack_bound;
+      if (cursor != n || stack != 1 || completed != v.slot_type || stack_bound > kMaxStack || stack_bound < 1) return -1;
+      if (!emit(OP_RETURN, v.return_fuel, 0, 0, 0)) return -1;
+      result->code = count;
+      result->constants = nconst;
+      result->locals = total_locals;
+      result->stack_bound = stack_bound;
       return count;
     }
     Frame& f = frames[depth - 1];
-    const gagp_expression& e = s.ex[w_origin(t.node[f.node])];
+    const gagp_expression& e = v.ex[w_origin(node[f.node])];
     if (f.seen < 3) f.args[f.seen] = int8_t(completed);
     ++f.seen;
+    if (e.node_kind == TK_TRAVERSE) {
+      Walk& w = walks[walk_depth - 1];
+      const RegionInfo& info = v.regions[w.info];
+      if (completed != info.operand_types[f.seen - 1] || !walk_after(w, f.seen - 1)) return -1;
+      if (f.seen < e.arity) { have_value = false; continue; }
+      while (live_count > w.live_begin) freed[free_count++] = live[--live_count];
+      --walk_depth;
+      completed = info.result_type;
+      --depth;
+      continue;
+    }
     const bool branch = e.node_kind == TK_IF || e.node_kind == TK_AND || e.node_kind == TK_OR;
     if (branch && f.seen == 1) {
+      if (completed != GAGP_TAG_BOOL) return -1;
       f.first_jump = count;
-      if (!emit(e.node_kind == TK_OR ? OP_JMP_IF_TRUE : OP_JMP_IF_FALSE, e.fuel, 0, 0, 1)) return -1;
+      if (!emit(e.node_kind == TK_OR ? OP_JMP_IF_TRUE : OP_JMP_IF_FALSE, e.fuel, 0, 0, kHasA)) return -1;
       --stack;
     } else if (e.node_kind == TK_IF && f.seen == 2) {
       f.second_jump = count;
-      if (!emit(OP_JMP, e.merge_fuel, 0, 0, 1)) return -1;
+      if (!emit(OP_JMP, e.merge_fuel, 0, 0, kHasA)) return -1;
       code[5 * f.first_jump + 2] = count;
       stack = f.base_stack;
     }
     if (f.seen < e.arity) { have_value = false; continue; }
     if (e.node_kind == TK_IF) {
+      if (f.args[1] != f.args[2]) return -1;
       code[5 * f.second_jump + 2] = count;
     } else if (e.node_kind == TK_AND || e.node_kind == TK_OR) {
+      if (completed != GAGP_TAG_BOOL) return -1;
       if (!emit(OP_NOT, e.fuel, 0, 0, 0) || !emit(OP_NOT, e.fuel, 0, 0, 0)) return -1;
       const int finish = count;
-      if (!emit(OP_JMP, e.fuel, 0, 0, 1)) return -1;
+      if (!emit(OP_JMP, e.fuel, 0, 0, kHasA)) return -1;
       code[5 * f.first_jump + 2] = count;
       stack = f.base_stack;
-      consts[nconst] = e.node_kind == TK_OR ? 1 : 0;
-      // flag 4 marks a Bool constant for the general VM (the reference keeps
-      // the tag in its constant Value); the low two bits are the reference's
-      if (!emit(OP_PUSH_CONST, e.fuel, nconst, 0, 5)) return -1;
-      ++nconst;
+      const int k = add_const(e.node_kind == TK_OR ? 1 : 0);
+      if (k < 0 || !emit(OP_PUSH_CONST, e.fuel, k, 0, kHasA | kBoolConst)) return -1;
       grow(1);
       code[5 * finish + 2] = count;
       completed = GAGP_TAG_BOOL;
     } else {
+      // the typed grammar fixes an operation's result type
       completed = e.type;
       if (e.opcode == OP_CALL_BUILTIN) {
-        if (!emit(e.opcode, e.fuel, e.operand, e.arity, 3)) return -1;
+        if (!emit(e.opcode, e.fuel, e.operand, e.arity, kHasA | kHasB)) return -1;
       } else if (!emit(e.opcode, e.fuel, 0, 0, 0)) {
         return -1;
       }
@@ -411,7 +616,7 @@ __device__ inline int lower_accumulator_emit(LowerScratch& m, int n, uint2* code
   return total;
 }
 
-__device__ __forceinline__ uint32_t accumulator_op_of(int node_kind, int opcode, int operand) {
+__host__ __device__ __forceinline__ uint32_t accumulator_op_of(int node_kind, int opcode, int operand) {
   if (node_kind == TK_AND) return A_AND;
   if (node_kind == TK_OR) return A_OR;
   if (node_kind == TK_IF) return A_SELECT;
@@ -467,6 +672,9 @@ __device__ inline int lower_accumulator_warp(const SearchDesc& s, const uint64_t
       m.arity[i] = uint8_t(arity);
       if (arity == 0) {
         m.aop[i] = kLeafOp;
+        // the accumulator VM reads constants and Int/Bool inputs; a bound
+        // read (a traversal binder) needs the general VM
+        total &= nk == TK_CONSTANT || nk == TK_LOCAL;
       } else {
         const uint32_t op = accumulator_op_of(nk, __ldg(&info[o].opcode), __ldg(&info[o].operand));
         m.aop[i] = uint8_t(op);

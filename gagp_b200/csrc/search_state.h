@@ -75,6 +75,20 @@ struct alignas(16) GenEntry {
   uint32_t need;
 };
 
+// A traversal table entry (the reference's PhaseRegionInfo for a traversal,
+// device/phase_compile.cuh:47-60) as lowering reads it: direction, the
+// binder numbers of element, index and state, the operand types the
+// children must complete with, the binding types and the result type.
+struct RegionInfo {
+  int8_t traversal;       // 1 forward, 2 reverse
+  int8_t ranged;          // 0: (source, start, initial state, body)
+  int8_t arity;           // 4, or 6 when ranged
+  int8_t result_type;     // ValueTag of the traversal's result
+  int8_t binders[3];
+  int8_t binding_types[3];
+  int8_t operand_types[6];
+};
+
 // Everything a kernel needs to work on one search (device pointers).
 struct SearchDesc {
   // ---- admitted grammar (phase tables)
@@ -96,6 +110,8 @@ struct SearchDesc {
   const GenLevel* gen_level;
   const GenEntry* gen_entry;
   const int32_t* local_types;          // ValueTag of each evaluator input
+  const RegionInfo* regions;           // traversal table entries (TK_TRAVERSE operands)
+  int32_t n_regions;
   int32_t n_ex, n_prods, n_nts, n_doms, n_vals;
   int32_t depth_count, logical_count, site_depth;
   int32_t root_expression, slot_max_depth, slot_type, local_count;
@@ -111,9 +127,12 @@ struct SearchDesc {
   uint64_t seed;
   int32_t rounds_per_epoch;            // P / B
   int32_t generations;
-  // ---- cases (input-major: inputs[j * C + c])
+  // ---- cases (input-major: inputs[j * C + c]); an IntList input's value is
+  // the offset in `lists` of its length word, its elements following
   const int64_t* inputs;
   const int64_t* expected;
+  const int64_t* lists;
+  int64_t n_lists;                     // words in `lists`
   int32_t C, n_inputs, expected_tag, vm_cases_per_lane;
   // ---- population rows (members) and children
   uint64_t* node;     int64_t* cval;     int32_t* len;        // P member rows (node words, constants)
@@ -135,6 +154,7 @@ struct SearchDesc {
   unsigned long long* vm_acc;
   int32_t* bc;                         // reference bytecode (op,flags,a,b,fuel) per program
   int32_t* bc_len;
+  int32_t* bc_locals;                  // locals of each lowered program (inputs + temporaries)
   int64_t* bc_consts;
   int32_t bc_stride;                   // instructions per program slot
   // ---- run generator (MT19937-64) and its output stream

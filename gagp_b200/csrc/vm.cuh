@@ -17,35 +17,35 @@
 
 namespace gb {
 
-__device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t b) { return int64_t(uint64_t(a) + uint64_t(b)); }
-__device__ __forceinline__ int64_t wrap_sub(int64_t a, int64_t b) { return int64_t(uint64_t(a) - uint64_t(b)); }
-__device__ __forceinline__ int64_t wrap_mul(int64_t a, int64_t b) { return int64_t(uint64_t(a) * uint64_t(b)); }
-__device__ __forceinline__ int64_t wrap_neg(int64_t a) { return int64_t(0ULL - uint64_t(a)); }
+__host__ __device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t b) { return int64_t(uint64_t(a) + uint64_t(b)); }
+__host__ __device__ __forceinline__ int64_t wrap_sub(int64_t a, int64_t b) { return int64_t(uint64_t(a) - uint64_t(b)); }
+__host__ __device__ __forceinline__ int64_t wrap_mul(int64_t a, int64_t b) { return int64_t(uint64_t(a) * uint64_t(b)); }
+__host__ __device__ __forceinline__ int64_t wrap_neg(int64_t a) { return int64_t(0ULL - uint64_t(a)); }
 // Truncating quotient and remainder of int64 operands (b != 0, and not
 // INT64_MIN / -1).  When both operands fit in 32 bits the 32-bit division
 // gives the same results at a fraction of the 64-bit division's cost
 // (program values are mostly small); b == -1 takes the 64-bit path, so the
 // 32-bit one never sees INT32_MIN / -1.
-__device__ __forceinline__ bool fits32(int64_t v) { return v == int64_t(int32_t(v)); }
-__device__ __forceinline__ int64_t tquot(int64_t a, int64_t b) {
+__host__ __device__ __forceinline__ bool fits32(int64_t v) { return v == int64_t(int32_t(v)); }
+__host__ __device__ __forceinline__ int64_t tquot(int64_t a, int64_t b) {
   return (fits32(a) && fits32(b) && b != -1) ? int64_t(int32_t(a) / int32_t(b)) : a / b;
 }
-__device__ __forceinline__ int64_t trem(int64_t a, int64_t b) {
+__host__ __device__ __forceinline__ int64_t trem(int64_t a, int64_t b) {
   return (fits32(a) && fits32(b) && b != -1) ? int64_t(int32_t(a) % int32_t(b)) : a % b;
 }
 // Python-sign modulo (vm_semantics::py_int_mod); b != 0.
-__device__ __forceinline__ int64_t py_mod(int64_t a, int64_t b) {
+__host__ __device__ __forceinline__ int64_t py_mod(int64_t a, int64_t b) {
   if (b == -1) return 0;
   int64_t r = trem(a, b);
   if (r != 0 && ((r < 0) != (b < 0))) r += b;
   return r;
 }
-__device__ __forceinline__ int64_t idiv0(int64_t a, int64_t b) { return b == 0 ? 0 : b == -1 ? wrap_neg(a) : tquot(a, b); }
-__device__ __forceinline__ int64_t imod0(int64_t a, int64_t b) { return b == 0 ? 0 : py_mod(a, b); }
-__device__ __forceinline__ int64_t tdiv0(int64_t a, int64_t b) {
+__host__ __device__ __forceinline__ int64_t idiv0(int64_t a, int64_t b) { return b == 0 ? 0 : b == -1 ? wrap_neg(a) : tquot(a, b); }
+__host__ __device__ __forceinline__ int64_t imod0(int64_t a, int64_t b) { return b == 0 ? 0 : py_mod(a, b); }
+__host__ __device__ __forceinline__ int64_t tdiv0(int64_t a, int64_t b) {
   return b == 0 || (a == INT64_MIN && b == -1) ? 0 : tquot(a, b);
 }
-__device__ __forceinline__ int64_t tmod0(int64_t a, int64_t b) {
+__host__ __device__ __forceinline__ int64_t tmod0(int64_t a, int64_t b) {
   return b == 0 || (a == INT64_MIN && b == -1) ? 0 : trem(a, b);
 }
 
@@ -278,37 +278,79 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
 }
 
 // ------------------------------------------------------------ general VM
-// Exact stack interpreter of the reference bytecode (unit fuel: the phase
-// compiler leaves all-unit charge tables empty, phase_layout.hpp:481-486).
-// One thread per case.  Returns false on a runtime error or timeout.
-__device__ inline bool run_reference(const SearchDesc& s, const int32_t* code, int n, const int64_t* consts, int c,
-                                     int64_t& value, int& tag, uint64_t& steps) {
-  int64_t sv[64];
-  int8_t st[64];
-  int sp = 0, ip = 0, fuel = s.fuel;
+// What the exact VM reads of a search: the case inputs (input-major), their
+// tags, the IntList arena and the fuel.
+struct VmView {
+  const int64_t* inputs;
+  const int32_t* local_types;
+  const int64_t* lists;
+  int64_t n_lists;
+  int C, n_inputs, fuel;
+};
+__host__ __device__ inline VmView vm_view(const SearchDesc& s) {
+  return VmView{s.inputs, s.local_types, s.lists, s.n_lists, s.C, s.n_inputs, s.fuel};
+}
+
+// Exact stack interpreter of the reference bytecode on case `c`: run_code_impl
+// (cpp/src/runtime/cpu/execute_bytecode_cpu.cpp:152-626) for the opcodes the
+// lowering emits, with the value semantics of value_semantics.hpp:91-190 and
+// the len/index builtins of builtins_cpu.cpp:220-370.  Every instruction
+// charges its fuel before it runs (Timeout when the fuel left is below the
+// charge; a chain of more uncharged instructions than the program has is an
+// error, as in the reference), so the loop is bounded by the fuel.  Values
+// are an int64 payload and a tag: an Int, a Bool (0/1) or an IntList (the
+// offset of its length word in the list arena).  `n_locals` is the
+// program's inputs plus temporaries; the inputs are preset.  Returns false
+// on any runtime error or timeout (every error scores the same), else the
+// returned value and its tag.  `steps` counts executed instructions.
+__host__ __device__ inline bool run_program(const VmView& v, const int32_t* code, int n, const int64_t* consts,
+                                            int n_locals, int c, int64_t& value, int& tag, uint64_t& steps) {
+  int64_t sv[kMaxStack], lv[kLowerLocals];
+  int8_t st[kMaxStack], lt[kLowerLocals];
+  if (n_locals < v.n_inputs || n_locals > kLowerLocals) return false;
+  uint64_t set = 0;  // bit k: local k holds a value
+  for (int j = 0; j < v.n_inputs; ++j) {
+    lv[j] = v.inputs[size_t(j) * v.C + c];
+    lt[j] = int8_t(v.local_types[j]);
+    set |= 1ull << j;
+  }
+  int sp = 0, ip = 0, fuel = v.fuel, uncharged = 0;
   while (ip < n) {
-    if (fuel <= 0) return false;  // Timeout
-    fuel -= 1;
-    ++steps;
     const int32_t* x = code + 5 * ip++;
     const int op = x[0], flags = x[1], a = x[2], b = x[3];
+    const int cost = x[4];
+    if (cost < 0 || fuel < cost) return false;  // Timeout (or a charge beyond the signed fuel range)
+    fuel -= cost;
+    if (cost) uncharged = 0;
+    else if (++uncharged > n) return false;     // zero-cost instruction cycle
+    ++steps;
     switch (op) {
       case OP_PUSH_CONST:
-        if (sp >= 64) return false;
+        if (sp >= kMaxStack) return false;
         sv[sp] = consts[a];
-        st[sp++] = int8_t((flags & 4) ? GAGP_TAG_BOOL : GAGP_TAG_INT);
+        st[sp++] = int8_t((flags & kBoolConst) ? GAGP_TAG_BOOL : GAGP_TAG_INT);
         break;
       case OP_LOAD:
-        if (sp >= 64 || a < 0 || a >= s.n_inputs) return false;
-        sv[sp] = s.inputs[size_t(a) * s.C + c];
-        st[sp++] = int8_t(s.local_types[a]);
+        if (sp >= kMaxStack || a < 0 || a >= n_locals || !((set >> a) & 1)) return false;  // Name error
+        sv[sp] = lv[a];
+        st[sp++] = lt[a];
+        break;
+      case OP_STORE:
+        if (!sp || a < 0 || a >= n_locals) return false;
+        --sp;
+        lv[a] = sv[sp];
+        lt[a] = st[sp];
+        set |= 1ull << a;
+        break;
+      case OP_CHECK_INT:
+        if (!sp || st[sp - 1] != GAGP_TAG_INT) return false;  // Type error
         break;
       case OP_NEG: case OP_NOT: {
         if (!sp) return false;
-        const int64_t v = sv[sp - 1];
+        const int64_t y = sv[sp - 1];
         const int t = st[sp - 1];
-        if (op == OP_NEG) { if (t != GAGP_TAG_INT) return false; sv[sp - 1] = wrap_neg(v); }
-        else { if (t != GAGP_TAG_BOOL) return false; sv[sp - 1] = v ^ 1; }
+        if (op == OP_NEG) { if (t != GAGP_TAG_INT) return false; sv[sp - 1] = wrap_neg(y); }
+        else { if (t != GAGP_TAG_BOOL) return false; sv[sp - 1] = y ^ 1; }
         break;
       }
       case OP_ADD: case OP_SUB: case OP_MUL: case OP_DIV: case OP_MOD: {
@@ -344,27 +386,44 @@ __device__ inline bool run_reference(const SearchDesc& s, const int32_t* code, i
         break;
       case OP_JMP_IF_FALSE: case OP_JMP_IF_TRUE: {
         if (!sp || a < 0 || a > n) return false;
-        const int64_t v = sv[--sp];
+        const int64_t y = sv[--sp];
         if (st[sp] != GAGP_TAG_BOOL) return false;
-        if ((op == OP_JMP_IF_FALSE && !v) || (op == OP_JMP_IF_TRUE && v)) ip = a;
+        if ((op == OP_JMP_IF_FALSE && !y) || (op == OP_JMP_IF_TRUE && y)) ip = a;
         break;
       }
       case OP_CALL_BUILTIN: {
         if (b < 0 || sp < b) return false;
-        for (int k = sp - b; k < sp; ++k) if (st[k] != GAGP_TAG_INT) return false;
         int64_t r;
-        if (a == B_ABS) { if (b != 1) return false; r = sv[sp - 1] < 0 ? wrap_neg(sv[sp - 1]) : sv[sp - 1]; }
-        else {
-          if (b != 2) return false;
-          const int64_t p = sv[sp - 2], q = sv[sp - 1];
-          switch (a) {
-            case B_MIN: r = p < q ? p : q; break;
-            case B_MAX: r = p > q ? p : q; break;
-            case B_IDIV0: r = idiv0(p, q); break;
-            case B_IMOD0: r = imod0(p, q); break;
-            case B_TRUNC_DIV0: r = tdiv0(p, q); break;
-            case B_TRUNC_MOD0: r = tmod0(p, q); break;
-            default: return false;
+        if (a == B_LEN || a == B_INDEX) {
+          // a read-only view of an input list: length word, then elements
+          if (b != (a == B_LEN ? 1 : 2) || st[sp - b] != GAGP_TAG_INTLIST) return false;
+          const int64_t at = sv[sp - b];
+          if (at < 0 || at >= v.n_lists) return false;
+          const int64_t len = v.lists[at];
+          if (a == B_LEN) {
+            r = len;
+          } else {
+            if (st[sp - 1] != GAGP_TAG_INT) return false;
+            int64_t j = sv[sp - 1];
+            if (j < 0) j += len;  // Python-style negative index
+            if (j < 0 || j >= len) return false;  // index out of range
+            r = v.lists[at + 1 + j];
+          }
+        } else {
+          for (int k = sp - b; k < sp; ++k) if (st[k] != GAGP_TAG_INT) return false;
+          if (a == B_ABS) { if (b != 1) return false; r = sv[sp - 1] < 0 ? wrap_neg(sv[sp - 1]) : sv[sp - 1]; }
+          else {
+            if (b != 2) return false;
+            const int64_t p = sv[sp - 2], q = sv[sp - 1];
+            switch (a) {
+              case B_MIN: r = p < q ? p : q; break;
+              case B_MAX: r = p > q ? p : q; break;
+              case B_IDIV0: r = idiv0(p, q); break;
+              case B_IMOD0: r = imod0(p, q); break;
+              case B_TRUNC_DIV0: r = tdiv0(p, q); break;
+              case B_TRUNC_MOD0: r = tmod0(p, q); break;
+              default: return false;
+            }
           }
         }
         sp -= b;

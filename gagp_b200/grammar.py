@@ -73,13 +73,18 @@ def _scalar_catalog() -> Dict[str, tuple]:
 
 
 CATALOG = _scalar_catalog()
-# List primitives of the table builder's list subset: the forward traversal
-# (catalog.cpp:138-141; its body argument binds element, index and state) and
-# len.  Traversal entries carry the body argument's position.
+# List primitives of the list subset: len and the forward and reverse
+# traversals of an IntList with an Int or Bool state (catalog.cpp:120-141;
+# the body argument binds element, index and state).  The operand of a
+# traversal entry here is its direction: 1 forward, 2 reverse.
 LIST_CATALOG = {
     "len(IntList)->Int": (("IntList",), "Int", TK_OPERATION, OP["call_builtin"], BUILTIN["len"], "len"),
-    "traverse(IntList,Int,Int,Int)->Int": (("IntList", "Int", "Int", "Int"), "Int", TK_TRAVERSE, 0, 0, "traverse"),
 }
+for _state in ("Int", "Bool"):
+    LIST_CATALOG[f"traverse(IntList,Int,{_state},{_state})->{_state}"] = (
+        ("IntList", "Int", _state, _state), _state, TK_TRAVERSE, 0, 1, "traverse")
+    LIST_CATALOG[f"traverse_reverse(IntList,Int,{_state},{_state})->{_state}"] = (
+        ("IntList", "Int", _state, _state), _state, TK_TRAVERSE, 0, 2, "traverse_reverse")
 
 
 class Declined(ValueError):
@@ -105,6 +110,7 @@ class Expression:
     name: str = ""
     result: str = ""          # grammar result type name
     scope_map: List[int] = field(default_factory=list)  # a reference's scope positions in its environment
+    binding_types: List[int] = field(default_factory=list)  # a traversal body's element/index/state tags
 
 
 @dataclass
@@ -139,6 +145,24 @@ class PhaseTables:
     fixed_nodes: int
     fuel: int
     names: List[str] = field(default_factory=list)  # printed name per expression
+    # traversal table (HostPhaseGrammar::regions): a Traverse node's operand
+    # indexes it; see Region
+    regions: List["Region"] = field(default_factory=list)
+
+
+@dataclass
+class Region:
+    """A traversal table entry (``PhaseRegionInfo``, device/phase_compile.cuh:47-60,
+    as ``compile_phase_grammar`` fills it, phase_grammar.hpp:263-285): direction
+    (1 forward, 2 reverse), the binder numbers of element, index and state, the
+    children's operand types, the binding types and the result type."""
+
+    traversal: int
+    binders: List[int]
+    operand_types: List[int]
+    binding_types: List[int]
+    result_type: int
+    ranged: bool = False
 
 
 def _parse_int(text) -> int:
@@ -260,6 +284,8 @@ class _Compiler:
                     raise Declined("argument type mismatch")
             e.kind, e.node_kind, e.opcode, e.operand = EK_OPERATION, tree_kind, opcode, operand
             e.arity, e.type, e.result, e.name = len(children), self.tags[result], result, name
+            if tree_kind == TK_TRAVERSE:
+                e.binding_types = [TAG_INT, TAG_INT, self.tags[arg_types[2]]]
             for i, c in enumerate(children):
                 e.children[i] = c
                 e.child_scope[i] = len(child_scopes[i])
@@ -328,7 +354,7 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
     # a traversal's three above every visible one
     nt_env: Dict[int, List[int]] = {}
     expr_env: Dict[int, List[int]] = {}
-    regions = [0]
+    regions: List[Region] = []
 
     def visit_nt(i: int, env: List[int]):
         if i in seen_nt:
@@ -370,8 +396,10 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
             if binder + 2 >= 16:
                 raise Declined("traversal capability")
             child_env[e.arity - 1] = env + [binder, binder + 1, binder + 2]
-            x.operand = regions[0]
-            regions[0] += 1
+            x.operand = len(regions)
+            regions.append(Region(traversal=e.operand, binders=[binder, binder + 1, binder + 2],
+                                  operand_types=[c.exprs[k].type for k in e.children[:e.arity]],
+                                  binding_types=list(e.binding_types), result_type=e.type))
         if len(env) > 15:
             raise Declined("lexical environment capacity")
         if e.kind == EK_CONSTANT and e.target not in seen_dom:
@@ -423,7 +451,7 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         slot_max_depth=slot_max_depth, slot_type=TYPE_TAGS[c.rules[root_nt]["type"]],
         local_types=[c.tags[dict(c.inputs)[n]] for n in names], input_names=names,
         max_nodes=max_nodes, fixed_nodes=4, fuel=fuel,
-        names=[e.name for e in out_expr])
+        names=[e.name for e in out_expr], regions=regions)
     _normalize_static_weights(tables)
     return tables
 

@@ -28,7 +28,7 @@ DEFAULT_SEARCH = {
     "ranking": {"tie_break": "ast_nodes"}, "schedule": {"mode": "steady_state", "replacement_size": 2},
 }
 
-_TYPE_TAGS = {"int": G.TAG_INT, "bool": G.TAG_BOOL}
+_TYPE_TAGS = {"int": G.TAG_INT, "bool": G.TAG_BOOL, "int_list": G.TAG_INTLIST}
 
 
 @dataclass
@@ -41,28 +41,37 @@ class LoadedTask:
 
 
 def _case_values(doc: dict, names):
+    """Inputs in evaluator order, their tags, expected values and tag, and the
+    IntList arena: an int_list input becomes the offset of its length word in
+    the arena, its elements following."""
     rows, expected, tags, etag = [], [], None, None
+    lists: list = []
     for case in doc["cases"]:
         row, row_tags = [], []
         for n in names:
             v = case["inputs"][n]
             if v["type"] not in _TYPE_TAGS:
-                raise G.Declined(f"input type {v['type']} is outside the resident scalar subset")
+                raise G.Declined(f"input type {v['type']} is outside the resident subset")
             row_tags.append(_TYPE_TAGS[v["type"]])
-            row.append(int(v["value"]))
+            if v["type"] == "int_list":
+                row.append(len(lists))
+                lists.append(len(v["value"]))
+                lists.extend(int(x) for x in v["value"])
+            else:
+                row.append(int(v["value"]))
         if tags is None:
             tags = row_tags
         elif tags != row_tags:
             raise G.Declined("mixed input types")
         e = case["expected"]
-        if e["type"] not in _TYPE_TAGS:
-            raise G.Declined(f"expected type {e['type']} is outside the resident scalar subset")
+        if e["type"] not in ("int", "bool"):
+            raise G.Declined(f"expected type {e['type']} is outside the resident subset")
         if etag is None:
             etag = _TYPE_TAGS[e["type"]]
         rows.append(row)
         expected.append(int(e["value"]))
     return np.array(rows, dtype=np.int64).reshape(len(expected), len(names)), tags or [], \
-        np.array(expected, dtype=np.int64), etag or 0
+        np.array(expected, dtype=np.int64), etag or 0, (np.array(lists, dtype=np.int64) if lists else None)
 
 
 def apply_search(settings: SearchSettings, doc: dict) -> None:
@@ -159,15 +168,15 @@ def assemble(name: str, grammar_doc: dict, train: dict, fitness: dict, search: O
     key = (json.dumps(grammar_doc, sort_keys=True), tuple(names), settings.site_depth)
     tables = table_cache.get(key) if table_cache is not None else None
     if tables is None:
-        tables = G.compile_tables(grammar_doc, names, settings.site_depth)
+        tables = G.compile_tables(grammar_doc, names, settings.site_depth, allow_lists=True)
         if table_cache is not None:
             table_cache[key] = tables
-    inputs, tags, expected, etag = _case_values(train, names)
+    inputs, tags, expected, etag, lists = _case_values(train, names)
     test_blob = None
     if test:
-        ti, tt, te, tet = _case_values(test, names)
-        test_blob = CasesBlob(ti, tt, te, tet)
-    return LoadedTask(name, tables, CasesBlob(inputs, tags, expected, etag), settings, test_blob)
+        ti, tt, te, tet, tl = _case_values(test, names)
+        test_blob = CasesBlob(ti, tt, te, tet, tl)
+    return LoadedTask(name, tables, CasesBlob(inputs, tags, expected, etag, lists), settings, test_blob)
 
 
 def from_files(files, table_cache: Optional[dict] = None) -> LoadedTask:
@@ -178,12 +187,18 @@ def from_files(files, table_cache: Optional[dict] = None) -> LoadedTask:
                     table_cache=table_cache)
 
 
-def program_text(tables: G.PhaseTables, origins, constants) -> str:
+def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 0) -> str:
     """Prefix program text of a phase row (``cli_detail::program_text``,
-    ``cpp/src/cli/program_json.cpp:876-946``)."""
+    ``cpp/src/cli/program_json.cpp:876-946``).  A traversal shows its body's
+    bound variables before the body, ``[vA vB vC] body``, numbered in prefix
+    order from ``first_binder`` as the reference's export numbers them
+    (``export_native_phase_layout``, phase_layout.hpp:388-396); a bound read
+    prints its variable."""
     out = []
     pos = [0]
     k = [0]
+    env = {}
+    next_id = [first_binder]
 
     def node():
         e = tables.expressions[origins[pos[0]]]
@@ -195,10 +210,25 @@ def program_text(tables: G.PhaseTables, origins, constants) -> str:
         if e.kind == G.EK_INPUT:
             out.append(e.name)
             return
+        if e.kind == G.EK_BOUND:
+            out.append("v%d" % env[e.operand])
+            return
+        ids, binders = None, None
+        if e.node_kind == G.TK_TRAVERSE:
+            binders = tables.regions[e.operand].binders
+            ids = [next_id[0] + j for j in range(3)]
+            next_id[0] += 3
         out.append("(" + e.name)
-        for _ in range(e.arity):
+        for i in range(e.arity):
             out.append(" ")
-            node()
+            if ids is not None and i == e.arity - 1:
+                out.append("[" + " ".join("v%d" % x for x in ids) + "] ")
+                saved = {b: env.get(b) for b in binders}
+                env.update(zip(binders, ids))
+                node()
+                env.update(saved)
+            else:
+                node()
         out.append(")")
 
     node()

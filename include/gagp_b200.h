@@ -42,7 +42,7 @@ enum {
 #define GAGP_PHASE_CAPACITY 1024  /* physical phase row capacity of the reference */
 
 /* ValueTag (cpp/include/gagp/core/value.hpp:16-27) */
-enum { GAGP_TAG_INT = 0, GAGP_TAG_FLOAT = 1, GAGP_TAG_BOOL = 2, GAGP_TAG_INVALID = 9 };
+enum { GAGP_TAG_INT = 0, GAGP_TAG_FLOAT = 1, GAGP_TAG_BOOL = 2, GAGP_TAG_INTLIST = 5, GAGP_TAG_INVALID = 9 };
 
 /* One generation record (PhaseExpression, device/phase_generate.cuh:79-92).
  * kind: PhaseExpressionKind; node_*: the PhaseTreeNode it emits
@@ -91,6 +91,23 @@ typedef struct gagp_value {        /* scalar Value: tag + payload */
   int32_t reserved;
 } gagp_value;
 
+/* A traversal table entry: the reference's PhaseRegionInfo for a traversal
+ * (cpp/src/evolution/repro/gpu/device/phase_compile.cuh:47-60), filled by
+ * compile_phase_grammar (cpp/src/evolution/repro/gpu/phase_grammar.hpp:263-285).
+ * A Traverse node's operand indexes this table.  Its children are source,
+ * start, [begin, end,] initial state and body; the body binds element, index
+ * and state as binder numbers binders[0..2]. */
+typedef struct gagp_region {
+  int32_t traversal;                /* 1: forward, 2: reverse (0: a bounded region, declined) */
+  int32_t ranged;                   /* 1: traverse_range (begin and end operands) */
+  int32_t fuel_profile;             /* 1: per-event fuel charges (event_cost), else every instruction costs 1 */
+  int32_t binders[3];               /* binder numbers of element, index, state */
+  int32_t operand_types[6];         /* ValueTag each child must complete with */
+  int32_t binding_types[3];         /* ValueTag of element, index, state */
+  int32_t result_type;              /* ValueTag of the traversal's value (phase_type[0]) */
+  uint32_t event_cost[26];          /* PhaseFuelEvent charges when fuel_profile */
+} gagp_region;
+
 /* The admitted grammar of one search: phase tables plus its single
  * whole-program slot (expression entry: program(block(return phase))). */
 typedef struct gagp_grammar {
@@ -111,10 +128,16 @@ typedef struct gagp_grammar {
   int32_t max_nodes;                /* grammar search_limits.max_nodes */
   int32_t fixed_nodes;              /* AST nodes outside the phase */
   uint32_t return_fuel;             /* fuel of the appended RETURN */
+  const gagp_region* regions;       /* traversal table (HostPhaseGrammar::regions) */
+  int32_t region_count;
 } gagp_grammar;
 
-/* Scalar fitness cases: inputs[case * input_count + j] is the payload of
- * evaluator input j (an Int, or 0/1 for a Bool); tags per input. */
+/* Fitness cases: inputs[case * input_count + j] is the payload of evaluator
+ * input j (an Int, 0/1 for a Bool, or for an IntList the index in
+ * list_values of the list's length word, its elements following); tags per
+ * input.  The reference keeps list inputs as payload handles into its
+ * payload registry (cpp/src/runtime/payload/payload.cpp); here they are
+ * read-only views into one flat array. */
 typedef struct gagp_cases {
   int32_t case_count;
   int32_t input_count;
@@ -122,6 +145,8 @@ typedef struct gagp_cases {
   const int32_t* input_tags;
   const int64_t* expected;
   int32_t expected_tag;
+  const int64_t* list_values;       /* IntList inputs: length words and elements (NULL: none) */
+  int64_t list_value_count;
 } gagp_cases;
 
 /* FitnessMetric (cpp/include/gagp/core/fitness_policy.hpp:4) */

@@ -16,6 +16,12 @@
 //       per-generation history, and the final ranked population with fitness,
 //       wrong count, node count, program text and phase row.
 //
+//   ref_driver lower TASK.json [--search F] [--population N] [--seed S] [--case-detail K]
+//       the initial population lowered by the resident owner's phase compiler
+//       (reference bytecode: op, flags, a, b, fuel; constants; locals; stack
+//       bound), each program's fitness and wrong count from the CPU
+//       evaluator, and the outcome of its first K cases.
+//
 //   ref_driver batch TASK.json [--search F] [--population N] [--seed S] --round-seed R
 //       one make_batch of the CPU resident owner (HostPhasePopulation,
 //       phase_population_cpu.cpp:322-353) over the generated initial population
@@ -47,6 +53,9 @@
 #include "gagp/evolution/grammar/request.hpp"
 #include "repro/gpu/phase_layout.hpp"
 #include "repro/gpu/phase_population_cpu.hpp"
+#include "repro/gpu/phase_operators.cuh"
+#include "gagp/runtime/cpu/execute_bytecode_cpu.hpp"
+#include "gagp/runtime/cpu/fitness_cpu.hpp"
 
 using namespace gagp;
 namespace gg = gagp::evo::grammar;
@@ -67,6 +76,7 @@ struct Args {
   bool has_seed = false;
   std::uint64_t seed = 0;
   std::uint64_t round_seed = 0;
+  int case_detail = 8;
 };
 
 std::string hex(double v) {
@@ -296,6 +306,80 @@ int run_batch(const Args& a) {
   return 0;
 }
 
+// The initial population lowered by the resident owner's phase compiler, as
+// HostPhasePopulation::lower_member does for a batch child
+// (phase_population_cpu.cpp:144-159: compile_phase_tree<true,true>, then
+// patch_whole_program), and each program scored by the CPU evaluator
+// (eval_fitness_cpu, cpp/src/runtime/cpu/fitness_cpu.cpp:57-176) with the
+// first `case_detail` cases run one by one (execute_bytecode_cpu).
+int run_lower(const Args& a) {
+  const auto task = cli_detail::load_task(a.task);
+  const auto grammar = std::make_shared<const gg::CompiledGrammar>(gg::compile_grammar(gg::load_definition(task.grammar_path)));
+  const auto cases = cli_detail::load_fitness_cases(task.train_path);
+  const auto cfg = make_config(a, task, grammar);
+  const auto case_set = evo::prepare_case_set(cases);
+  const auto& names = case_set.input_names;
+  const int site_depth = cfg.gpu_phase_site_depth;
+  const auto population = rp::generate_phase_initial_population(*grammar, *cfg.generation_request, names,
+                                                                 cfg.population_size, cfg.seed, site_depth);
+  rp::NativePhaseGrammarProfiles profiles(grammar, names);
+  auto layout = rp::import_native_phase_layout(*grammar, population.front(), &profiles, &names, true);
+  for (std::size_t k = 0; k < layout.slots.size(); ++k)
+    layout.profiles[k] = rp::compile_phase_variation_grammar(*grammar, layout.slots[k].nonterminal,
+                                                             grammar->search_limits().max_depth, site_depth, &names);
+  if (!layout.whole_program || layout.slots.size() != 1) throw std::runtime_error("lower: one whole-program phase only");
+  const auto& g = layout.profiles[0];
+  const auto& nt = grammar->nonterminals()[layout.slots[0].nonterminal];
+  const auto type = layout.program_terminator ? rp::phase_value_tag(nt.type) : rp::kPhaseStatement;
+  std::vector<ValueTag> locals(names.size(), ValueTag::Invalid);
+  for (std::size_t j = 0; j < names.size(); ++j)
+    for (const auto& binding : grammar->inputs())
+      if (binding.name == names[j]) locals[j] = rp::phase_value_tag(binding.type);
+  std::vector<gagp::gpu_detail::DInstr> code(4 * 1024);
+  std::vector<Value> values(1024);
+  std::vector<std::vector<std::pair<int, Value>>> inputs(case_set.bindings.size());
+  for (std::size_t c = 0; c < case_set.bindings.size(); ++c)
+    for (const auto& b : case_set.bindings[c]) inputs[c].emplace_back(b.idx, b.value);
+  const int detail = std::min<int>(a.case_detail, int(inputs.size()));
+  std::printf("{\"fuel\":%d,\"rows\":[", cfg.fuel);
+  for (std::size_t p = 0; p < population.size(); ++p) {
+    const auto imported = rp::import_native_phase_layout(*grammar, population[p], &profiles, &names, false);
+    const auto& gene = imported.genes.at(0);
+    const auto r = rp::compile_phase_tree<true, true>(gene.nodes.data(), int(gene.nodes.size()), gene.constants.data(),
+        int(gene.constants.size()), locals.data(), int(locals.size()), type, code.data(), int(code.size()),
+        values.data(), int(values.size()), g.regions.data(), int(g.regions.size()));
+    std::printf("%s{\"origins\":[", p ? "," : "");
+    for (std::size_t j = 0; j < gene.origins.size(); ++j) std::printf("%s%d", j ? "," : "", gene.origins[j]);
+    std::printf("],\"constants\":[");
+    for (std::size_t j = 0; j < gene.constants.size(); ++j) std::printf("%s%" PRId64, j ? "," : "", gene.constants[j].i);
+    std::printf("],\"status\":%d", int(r.status));
+    if (r.status != rp::PhaseCompileStatus::Ok) { std::printf("}"); continue; }
+    BytecodeProgram program = imported.executable;
+    rp::patch_whole_program(program, layout, code.data(), r.code_count, values.data(), r.constant_count, r);
+    std::printf(",\"stack_bound\":%d,\"n_locals\":%d,\"fuel_table\":%d,\"code\":[", r.stack_bound, program.n_locals,
+                int(!program.instruction_fuel.empty()));
+    for (int i = 0; i < r.code_count; ++i)
+      std::printf("%s[%d,%d,%d,%d,%u]", i ? "," : "", int(code[i].op), int(code[i].flags), code[i].a, code[i].b,
+                  code[i].fuel);
+    std::printf("],\"consts\":[");
+    for (int i = 0; i < r.constant_count; ++i) std::printf("%s%s", i ? "," : "", value_json(values[i]).c_str());
+    std::vector<unsigned> wrong;
+    const auto fitness = eval_fitness_cpu({program}, case_set.bindings, case_set.expected_values, cfg.fuel,
+                                          cfg.penalty, cfg.gpu_blocksize, cfg.fitness_policy, &wrong, nullptr);
+    std::printf("],\"fitness\":%s,\"wrong\":%u,\"cases\":[", num(fitness.at(0)).c_str(), wrong.at(0));
+    for (int c = 0; c < detail; ++c) {
+      int fuel = cfg.fuel;
+      const auto out = execute_bytecode_cpu(program, inputs[c], fuel);
+      // [error code or -1, result tag, result payload, fuel left]
+      std::printf("%s[%d,%d,%" PRId64 ",%d]", c ? "," : "", out.is_error ? int(out.err.code) : -1,
+                  out.is_error ? -1 : int(out.value.tag), out.is_error ? 0 : out.value.i, fuel);
+    }
+    std::printf("]}");
+  }
+  std::printf("]}\n");
+  return 0;
+}
+
 int run_search(const Args& a) {
   const auto task = cli_detail::load_task(a.task);
   const auto grammar = std::make_shared<const gg::CompiledGrammar>(gg::compile_grammar(gg::load_definition(task.grammar_path)));
@@ -355,12 +439,14 @@ int main(int argc, char** argv) {
     else if (k == "--generations") a.generations = std::stoi(v);
     else if (k == "--seed") { a.has_seed = true; a.seed = std::stoull(v); }
     else if (k == "--round-seed") a.round_seed = std::stoull(v);
+    else if (k == "--case-detail") a.case_detail = std::stoi(v);
     else { std::fprintf(stderr, "unknown option %s\n", k.c_str()); return 2; }
   }
   try {
     if (a.mode == "tables") return run_tables(a);
     if (a.mode == "run") return run_search(a);
     if (a.mode == "batch") return run_batch(a);
+    if (a.mode == "lower") return run_lower(a);
   } catch (const std::exception& e) {
     std::fprintf(stderr, "ref_driver: %s\n", e.what());
     return 1;

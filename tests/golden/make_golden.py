@@ -58,6 +58,24 @@ LIST_CASES = [
 # the round seed of the recorded make_batch (ref_driver batch)
 LIST_ROUND_SEED = 0x9E3779B97F4A7C15
 
+# Whole list searches recorded without a make_batch: a reverse traversal,
+# and the list-program benchmark's shape (200 cases, lists of 0..50
+# elements, P = 1024) over 16 generations.
+LIST_RUNS = [
+    ("list_reverse_traversal", dict(population=96, generations=4, seed=14, cases=16, target="max"), "reverse"),
+    ("list_config3_p1024_g16", dict(population=1024, generations=16, seed=0, cases=200, target="threshold_sum"),
+     None),
+]
+
+# Lowering pins (golden/lower/): the reference's phase compiler output and
+# CPU fitness of every member of a generated population (ref_driver lower).
+LOWER_CASES = [
+    ("lower_list_threshold", "list", dict(population=256, generations=1, seed=21, cases=24), None),
+    ("lower_list_nested", "list", dict(population=256, generations=1, seed=22, cases=24, target="max"), "nested"),
+    ("lower_list_reverse", "list", dict(population=256, generations=1, seed=23, cases=24, target="max"), "reverse"),
+    ("lower_poly4", "poly4", dict(population=256, generations=1, seed=24, cases=32), None),
+]
+
 
 def nested_traversal_grammar() -> dict:
     """The list grammar with a second traversal inside the step, whose body
@@ -79,6 +97,25 @@ def nested_traversal_grammar() -> dict:
     return g
 
 
+def reverse_traversal_grammar() -> dict:
+    """The list grammar with the fold as a reverse traversal beside the
+    forward one."""
+    g = W.list_threshold_grammar()
+    top = next(r for r in g["nonterminals"] if r["id"] == "Top")
+    fold = top["alternatives"][0]["expression"]
+    top["alternatives"].append({"id": "rfold", "weight": 2, "expression": dict(
+        fold, signature="traverse_reverse(IntList,Int,Int,Int)->Int")})
+    return g
+
+
+def variant_grammar(variant):
+    if variant == "nested":
+        return nested_traversal_grammar()
+    if variant == "reverse":
+        return reverse_traversal_grammar()
+    return None
+
+
 def driver(*args) -> dict:
     out = subprocess.run([DRIVER, *args], check=True, capture_output=True, text=True).stdout
     return json.loads(out)
@@ -88,7 +125,11 @@ def main() -> None:
     import argparse
     ap = argparse.ArgumentParser()
     ap.add_argument("--list-only", action="store_true", help="regenerate golden/list/ only")
+    ap.add_argument("--lower-only", action="store_true", help="regenerate golden/lower/ only")
     args = ap.parse_args()
+    if args.lower_only:
+        lower_fixtures()
+        return
     if not os.path.exists(DRIVER):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     here = os.path.dirname(os.path.abspath(__file__))
@@ -135,6 +176,39 @@ def main() -> None:
         with gzip.open(os.path.join(here, "list", name + ".json.gz"), "wt") as f:
             json.dump(fixture, f, separators=(",", ":"))
         print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
+    for name, kwargs, variant in LIST_RUNS:
+        task = W.list_threshold(**kwargs)
+        if variant:
+            task.grammar = variant_grammar(variant)
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            run = driver("run", tp, "--search", sp)
+        assert run["declined"] == "", (name, run["declined"])
+        fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+                   "train": task.train, "test": task.test, "search": task.search, "run": run}
+        with gzip.open(os.path.join(here, "list", name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
+    lower_fixtures()
+
+
+def lower_fixtures() -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "lower"), exist_ok=True)
+    for name, workload, kwargs, variant in LOWER_CASES:
+        task = W.list_threshold(**kwargs) if workload == "list" else W.make(workload, **kwargs)
+        if variant:
+            task.grammar = variant_grammar(variant)
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            lowered = driver("lower", tp, "--search", sp, "--case-detail", "4")
+        fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+                   "train": task.train, "test": task.test, "search": task.search, "lower": lowered}
+        with gzip.open(os.path.join(here, "lower", name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(lowered["rows"]), "rows")
 
 
 if __name__ == "__main__":

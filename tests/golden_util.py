@@ -5,6 +5,7 @@ import glob
 import gzip
 import json
 import os
+import re
 import tempfile
 
 from gagp_b200 import abi
@@ -49,12 +50,21 @@ def reference_rows(rows, stride: int) -> abi.RowsBuffer:
     return abi.RowsBuffer.from_rows([(r["origins"], [c[1] for c in r["constants"]]) for r in rows], stride)
 
 
+def binder_names_in_order(text: str) -> str:
+    """Program text with its bound variables renamed v0, v1, ... in order of
+    first appearance: the reference's export numbers them from the largest
+    binder id of its prototype program, which only that numbering depends on."""
+    names = {}
+    return re.sub(r"\bv\d+\b", lambda m: names.setdefault(m.group(0), "v%d" % len(names)), text)
+
+
 def compare_result(lt: T.LoadedTask, got: dict, run: dict, label: str = "") -> None:
     """Asserts a search result equals the reference run bit for bit."""
     ref_hist, ref_final = run["history"], run["final"]
     assert len(got["history"]) == len(ref_hist), label
     for i, (a, b) in enumerate(zip(got["history"], ref_hist)):
-        text = T.program_text(lt.tables, *a["row"])
+        text = binder_names_in_order(T.program_text(lt.tables, *a["row"]))
+        b = dict(b, text=binder_names_in_order(b["text"]))
         assert a["best_fitness"] == b["best_fitness"], (label, "history", i, a["best_fitness"], b["best_fitness"])
         assert a["mean_fitness"] == float.fromhex(b["mean_fitness"]), (label, "mean", i)
         assert a["best_wrong"] == b["best_wrong"], (label, "wrong", i)

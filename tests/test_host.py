@@ -80,9 +80,15 @@ def test_admission_rejects_malformed_tables(poly_task, case):
 
 
 def test_admission_declines_outside_the_resident_subset(poly_task):
-    def scoped(blob):
-        blob.nonterminals[0].scope_count = 1
-    assert _bytes(poly_task, scoped)[0] == 1  # GAGP_DECLINED
+    def template(blob):
+        blob.expressions[_first(blob, W_KINDS["input"])].kind = 5  # an alias (template instance)
+    assert _bytes(poly_task, template)[0] == 1  # GAGP_DECLINED
+
+    def statement(blob):
+        e = next(i for i in range(len(blob.tables.expressions))
+                 if blob.expressions[i].kind == W_KINDS["operation"] and blob.expressions[i].arity > 0)
+        blob.expressions[e].node_kind = 9  # Assign
+    assert _bytes(poly_task, statement)[0] == 1
     s = poly_task.settings
     s_steady = s.steady_state
     try:
@@ -107,15 +113,17 @@ def test_admission_rejects_a_single_member_steady_state(poly_task):
         s.population, s.batch = old
 
 
-def test_list_programs_are_declined_at_admission():
+def test_list_programs_load_with_their_traversal_table():
     """The list workload (a traversal with element/index/accumulator binders
-    over an IntList input) is outside the resident subset: loading it raises
-    the reference's resident-admission decline."""
-    from gagp_b200 import grammar as G
+    over an IntList input) loads into resident tables: one traversal entry,
+    the IntList input as a view into the list arena."""
     for target in W.LIST_TARGETS:
         files = W.list_threshold(population=64, generations=2, seed=5, cases=12, target=target)
-        with pytest.raises(G.Declined):
-            T.from_files(files, {})
+        lt = T.from_files(files, {})
+        assert [r.binders for r in lt.tables.regions] == [[0, 1, 2]]
+        xs = lt.tables.input_names.index("xs")
+        for c, case in enumerate(files.train):
+            assert lt.cases.list_at(c, xs) == case["inputs"]["xs"]["value"]
 
 
 def test_mixes_carry_list_programs():
@@ -138,8 +146,7 @@ def test_mixes_carry_list_programs():
                     reason="the reference CPU engine is not built (make -C oracle ref)")
 def test_reference_runs_list_programs_resident(tmp_path):
     """The reference engine admits the same list task to its resident path
-    (no decline) and searches it, so the decline above is this engine's
-    subset, not a property of the task."""
+    (no decline) and searches it."""
     import json
     import subprocess
     files = W.list_threshold(population=64, generations=2, seed=5, cases=12)
@@ -154,13 +161,54 @@ def test_reference_runs_list_programs_resident(tmp_path):
 
 
 def test_bench_mix_admission_counts():
-    """bench.py's batching and serving workloads admit the scalar entries of
-    their mixes and count the list entries the admission declines."""
+    """bench.py's batching and serving workloads admit every entry of their
+    mixes, scalar and list programs alike."""
     import importlib.util
     spec = importlib.util.spec_from_file_location("bench_module", os.path.join(ROOT, "bench.py"))
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
     mix = W.batch_mix(8)
     tasks, declined = bench._mix_tasks(mix)
-    assert len(tasks) == 4 and declined == 4
-    assert all(t.settings.population == m["population"] for t, m in zip(tasks, [m for m in mix if m["kind"] == "scalar"]))
+    assert len(tasks) == 8 and declined == 0
+    assert [t.settings.population for t in tasks] == [m["population"] for m in mix]
+    assert sum(1 for t in tasks if t.tables.regions) == 4
+
+
+@pytest.fixture
+def list_task(tmp_path):
+    files = W.list_threshold(population=64, generations=2, seed=3, cases=20)
+    return T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
+
+
+def test_admission_accepts_list_programs(list_task):
+    """Traversals, bound reads, scoped nonterminals and IntList inputs are
+    admitted; the traversal table is uploaded with the grammar."""
+    st, n = _bytes(list_task)
+    assert st == 0 and n > 0
+    assert len(list_task.tables.regions) == 1 and list_task.tables.regions[0].traversal == 1
+
+
+@pytest.mark.parametrize("case", ["ranged", "fuel_profile", "binder", "overrun", "tags"])
+def test_admission_checks_list_tables_and_cases(list_task, case):
+    cases = list_task.cases
+
+    def edit(blob):
+        r = blob.regions[0]
+        if case == "ranged":
+            r.ranged = 1
+        elif case == "fuel_profile":
+            r.fuel_profile = 1
+        elif case == "binder":
+            r.binders[1] = 16
+    saved = cases.inputs.copy(), cases.input_tags.copy()
+    try:
+        xs = list_task.tables.input_names.index("xs")
+        if case == "overrun":
+            cases.inputs[0, xs] = len(cases.list_values) - 1  # a length word with no room for its elements
+            cases.list_values[-1] = 5
+        if case == "tags":
+            cases.input_tags[xs] = 0
+        st, _ = _bytes(list_task, edit)
+    finally:
+        cases.inputs[:], cases.input_tags[:] = saved
+    assert st == (1 if case in ("ranged", "fuel_profile") else 2), case

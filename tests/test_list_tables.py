@@ -1,9 +1,9 @@
 """The table builder's list subset against the reference's tables (CPU).
 
 The list programs (a traversal of an IntList with element, index and
-accumulator binders, scoped nonterminals, bound names, len) are declined at
-admission by this engine.  Their phase tables are the first piece of that
-path: ``grammar.compile_tables(..., allow_lists=True)`` must equal the
+accumulator binders, scoped nonterminals, bound names, len) run on the
+device.  Their phase tables: ``grammar.compile_tables(..., allow_lists=True)``
+must equal the
 reference's compile_phase_grammar output (phase_grammar.hpp:94-300, weights
 normalised by normalize_static_phase_weights) for the fixtures that
 tests/golden/make_golden.py records from the reference engine, including a
@@ -16,7 +16,9 @@ from gagp_b200 import grammar as G
 
 import golden_util as GU
 
-NAMES = GU.list_names()
+# the list fixtures that also hold the reference's tables, initial rows and
+# one make_batch (the others hold whole runs only)
+NAMES = [n for n in GU.list_names() if "tables" in GU.list_fixture(n)]
 
 
 def test_list_fixtures_exist():
@@ -55,6 +57,13 @@ def test_list_tasks_run_resident_in_the_reference(name):
     run = GU.list_fixture(name)["run"]
     assert run["declined"] == ""
     assert len(run["history"]) == 3 and run["history"][0]["text"].startswith("(traverse xs")
+
+
+def test_every_list_run_took_the_resident_path():
+    for name in GU.list_names():
+        run = GU.list_fixture(name)["run"]
+        assert run["declined"] == "", name
+        assert any(h["text"].startswith("(traverse") for h in run["history"]), name
 
 
 @pytest.mark.parametrize("name", NAMES)
