@@ -1,24 +1,38 @@
 #!/usr/bin/env python
 """Benchmark of the resident GAGP search path on B200.
 
-Metric: VM program-case evaluations per second (whole job), on the
-large scalar-regression search: a random degree<=4 integer polynomial, 256
-train cases x ~ U{-100..100}, grammar x, constants -2..3, add/sub/mul/idiv0/
-imod0 and if(lt(E,E),E,E), max 64 nodes, population 16384, 128 generations,
-absolute error (cap 1000), gagp's default resident search (steady state,
-batch = population).  A step is one steady-state round: one batch of 16384
-children varied, lowered, evaluated on all cases and placed.
+Workloads (``--workload``):
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+* ``poly4`` (default): the large scalar-regression search -- a random
+  degree<=4 integer polynomial, 256 train cases x ~ U{-100..100}, grammar x,
+  constants -2..3, add/sub/mul/idiv0/imod0 and if(lt(E,E),E,E), max 64 nodes,
+  population 16384, 128 generations, absolute error (cap 1000), gagp's
+  default resident search (steady state, batch = population).
+* ``list``: list programs with a loop -- IntLists of 0..50 elements in
+  [-1000, 1000] and a threshold t in [-100, 100], target the sum of the
+  elements above t, a traversal grammar (element/index/accumulator binders,
+  comparisons, add/sub), 200 cases, population 8192, 96 generations.
+* ``batch``: 64 independent searches (half scalar, half list programs) run
+  as one batch, against each run alone.
+* ``serve``: an open-loop Poisson stream of scalar and list search requests
+  through the continuous-batching server.
+
+For ``poly4`` and ``list`` a step is one steady-state round: one batch of
+children varied, lowered, evaluated on all cases and placed.  Metric: VM
+program-case evaluations per second (whole job).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload W]
 
 Own arm: `value` is program-case evaluations per second of device time over K
 rounds (CUDA events on the engine stream, L2 flushed before every round,
 outside the timed region); `e2e` runs a whole search through the C ABI from
 host buffers (admission upload, device loop, result download).  Reference arm
 (--impl reference): the reference's own CPU engine compiled from its sources
-(oracle/_ref/ref_driver), one process per host core, each step a bounded
-sample search.  Several GPUs run independent replica searches (one per rank,
-seed + rank): the path has no data-path collective.
+(oracle/_ref/ref_driver) on the same task, one process per host core (as many
+as host memory holds), each step the initial evaluation and the first
+generation of the search, timed by the reference's own clock.  Several GPUs
+run independent replica searches (one per rank, seed + rank): the path has no
+data-path collective.
 """
 from __future__ import annotations
 
@@ -39,9 +53,23 @@ from gagp_b200 import task as T  # noqa: E402
 
 METRIC = "VM program-case evals/s"
 UNIT = "program-case evals/s"
-WORKLOAD = dict(population=16384, generations=128, cases=256, max_nodes=64)
 PROFILE_ROUNDS = 3
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+# The single-search workloads: task files from the seed, their shape and label.
+SEARCH_WORKLOADS = {
+    "poly4": dict(population=16384, generations=128, cases=256, max_nodes=64,
+                  make=lambda seed: W.poly4(population=16384, generations=128, seed=seed, cases=256, max_nodes=64),
+                  label="poly4 scalar regression (large): P=16384, G=128, C=256, max_nodes=64, seed=%d",
+                  cpu_generations=4, profile="poly4_p16384"),
+    "list": dict(population=8192, generations=96, cases=200, max_nodes=48,
+                 make=lambda seed: W.list_threshold(population=8192, generations=96, seed=seed, cases=200,
+                                                    target="threshold_sum"),
+                 label="list programs (threshold sum over IntLists of 0..50 elements, traversal grammar): "
+                       "P=8192, G=96, C=200, max_nodes=48, seed=%d",
+                 cpu_generations=1, profile="list_p8192"),
+}
+WORKLOAD = SEARCH_WORKLOADS["poly4"]
 
 
 def combine_ranks(dist, seconds: float, units: float, device: str = "cuda"):
@@ -78,16 +106,12 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-def make_task(seed: int, directory: str, **overrides) -> str:
-    cfg = dict(WORKLOAD)
-    cfg.update(overrides)
-    files = W.poly4(population=cfg["population"], generations=cfg["generations"], seed=seed, cases=cfg["cases"],
-                    max_nodes=cfg["max_nodes"])
-    return files.write(directory)
+def make_task(seed: int, directory: str) -> str:
+    return WORKLOAD["make"](seed).write(directory)
 
 
 def config_block(world: int, seed: int) -> dict:
-    return {"workload": "poly4 scalar regression (large): P=16384, G=128, C=256, max_nodes=64, seed=%d" % seed,
+    return {"workload": WORKLOAD["label"] % seed,
             "population": WORKLOAD["population"], "generations": WORKLOAD["generations"],
             "cases": WORKLOAD["cases"], "max_nodes": WORKLOAD["max_nodes"], "batch": WORKLOAD["population"],
             "parallelism": "replicas%d" % world if world > 1 else "single-gpu",
@@ -160,11 +184,13 @@ def peaks() -> dict:
         return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def reference_sample(task_path: str, search_path: str, generations: int) -> dict:
+def reference_sample(task_path: str, search_path: str, generations: int, seed=None) -> dict:
     """One reference CPU-engine search (single thread), timed by its own clock."""
     driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
-    out = subprocess.run([driver, "run", task_path, "--search", search_path, "--generations", str(generations)],
-                         check=True, capture_output=True, text=True).stdout
+    cmd = [driver, "run", task_path, "--search", search_path, "--generations", str(generations)]
+    if seed is not None:
+        cmd += ["--seed", str(seed)]
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
     d = json.loads(out)
     return {"program_cases": d["program_cases"], "ms": d["time_ms"]}
 
@@ -172,12 +198,13 @@ def reference_sample(task_path: str, search_path: str, generations: int) -> dict
 def cpu_baseline(directory: str) -> dict:
     """The reference CPU engine on a bounded sample of the workload (1 thread)."""
     driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    g = WORKLOAD["cpu_generations"]
     if os.path.exists(driver):
-        r = reference_sample(os.path.join(directory, "task.json"), os.path.join(directory, "search.json"), 4)
+        r = reference_sample(os.path.join(directory, "task.json"), os.path.join(directory, "search.json"), g)
         return {"value": r["program_cases"] / (r["ms"] / 1000.0), "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": "reference CPU engine (HostPhasePopulation, single-threaded), same task and seed, "
-                          "population 16384, 4 generations + initial evaluation (%d program-cases in %.1f s)" % (
-                              r["program_cases"], r["ms"] / 1000.0)}
+                          "population %d, %d generation(s) + initial evaluation (%d program-cases in %.1f s)" % (
+                              WORKLOAD["population"], g, r["program_cases"], r["ms"] / 1000.0)}
     sys.path.insert(0, ROOT)
     from oracle import oracle  # noqa: WPS433 (checker only)
     from gagp_b200 import abi
@@ -186,11 +213,37 @@ def cpu_baseline(directory: str) -> dict:
     res = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
     dt = time.perf_counter() - t0
     return {"value": res["program_cases"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "C oracle restatement, population 16384, 2 generations + initial evaluation"}
+            "sample": "C oracle restatement, population %d, 2 generations + initial evaluation" % WORKLOAD["population"]}
+
+
+def host_memory_bytes() -> int:
+    """Memory this process may use on the host: MemAvailable, capped by the
+    cgroup limit when there is one."""
+    avail = None
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    for path in ("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory/memory.limit_in_bytes"):
+        try:
+            text = open(path).read().strip()
+            if text.isdigit():
+                avail = min(avail or int(text), int(text))
+        except OSError:
+            pass
+    return avail or (8 << 30)
+
+
+# resident memory of one reference CPU-engine process on each workload (its
+# fixed 1024-node rows: about 4.2 GB at population 16384, 2.2 GB at 8192)
+REFERENCE_PROCESS_BYTES = {"poly4": 5 << 30, "list": 3 << 30}
 
 
 def run_reference_arm(args, rank: int, world: int):
-    """--impl reference: the reference CPU engine on all host cores."""
+    """--impl reference: the reference CPU engine on the host cores, same task
+    and configuration as the own arm."""
     if rank != 0:
         return
     driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
@@ -199,24 +252,30 @@ def run_reference_arm(args, rank: int, world: int):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver was not built"}))
         return
     cores = os.cpu_count() or 1
+    # concurrent processes: every core, as far as host memory holds them
+    procs_n = max(1, min(cores, int(0.7 * host_memory_bytes()) // REFERENCE_PROCESS_BYTES[args.workload]))
     with tempfile.TemporaryDirectory() as d:
         make_task(seed, d)
         tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
-        sample_generations = 2
-        make_task(seed, d, population=2048)
+        sample_generations = 1
 
         def step():
-            t0 = time.perf_counter()
+            # each process: the same task with its own seed, initial
+            # population, its evaluation and one generation; the step's time
+            # is the slowest process's own search clock (start-up, grammar
+            # load and the final JSON dump are outside it)
             procs = [subprocess.Popen([driver, "run", tp, "--search", sp, "--generations", str(sample_generations),
                                        "--seed", str(seed + i)], stdout=subprocess.PIPE, text=True)
-                     for i in range(cores)]
-            total = 0
+                     for i in range(procs_n)]
+            total, slowest = 0, 0.0
             for p in procs:
                 out, _ = p.communicate()
                 if p.returncode:
                     raise RuntimeError("reference run failed")
-                total += json.loads(out)["program_cases"]
-            return total, time.perf_counter() - t0
+                r = json.loads(out)
+                total += r["program_cases"]
+                slowest = max(slowest, r["time_ms"] / 1000.0)
+            return total, slowest
 
         for _ in range(args.warmup):
             step()
@@ -226,14 +285,16 @@ def run_reference_arm(args, rank: int, world: int):
             cases += c
             secs += s
     value = cases / secs
+    sample = ("per step: %d concurrent single-threaded reference CPU-engine searches of this task (population %d, "
+              "%d cases; initial population, its evaluation and generation 1 of %d; seeds 0..%d), timed by the "
+              "reference's own search clock (max over processes)" % (
+                  procs_n, WORKLOAD["population"], WORKLOAD["cases"], WORKLOAD["generations"], procs_n - 1))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / max(1, args.steps),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": config_block(1, seed),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": "per step: %d concurrent single-threaded reference CPU-engine searches "
-                                       "(population 2048, initial evaluation + %d generations, seeds 0..%d)" % (
-                                           cores, sample_generations, cores - 1)},
+            "data": "synthetic", "config": dict(config_block(1, seed), generation_window="initial + 1 of %d"
+                                                % WORKLOAD["generations"]),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs_n, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -254,7 +315,7 @@ def algorithmic_bytes(kernel: str, delta: dict, steps: int, population: int, bat
 
 def profiled_traffic(kernel: str):
     """dram bytes per launch of `kernel` from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "%s_poly4_p16384.txt" % kernel)
+    path = os.path.join(ROOT, "profiles", "%s_%s.txt" % (kernel, WORKLOAD["profile"]))
     try:
         for line in open(path):
             f = line.split()
@@ -280,14 +341,57 @@ def roofline_entry(stats: dict, delta: dict, steps: int, peak: dict) -> dict:
             "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak["source"]}
 
 
-def vm_entry(stats: dict, delta: dict) -> dict:
-    """VM bytecode instructions and program-case evaluations per second of VM kernel time."""
-    ms = sum(stats[k]["ms"] for k in ("k_vm_fast", "k_vm_general") if k in stats)
-    if ms <= 0:
-        return {}
-    return {"kernel_ms": ms, "bytecode_ops_per_s": delta["vm_ops"] / (ms / 1000.0),
-            "program_cases_per_s": delta["program_cases"] / (ms / 1000.0),
-            "ops_per_program_case": delta["vm_ops"] / max(1, delta["program_cases"])}
+def vm_issue_summary(workload: str):
+    """Integer-issue figures of the VM kernels from the committed ncu summary
+    (profiles/vm_issue_<workload>.txt): per kernel, warp instructions issued
+    on the integer pipes (ALU + FMA) and in all, per launch, and the
+    fraction of the SM sub-partitions' issue slots they filled."""
+    path = os.path.join(ROOT, "profiles", "vm_issue_%s.txt" % workload)
+    out = {}
+    try:
+        for line in open(path):
+            f = line.split()
+            if len(f) == 6 and f[0] == "vm_issue:":
+                out[f[1]] = {"int_inst_per_launch": float(f[2]), "inst_per_launch": float(f[3]),
+                             "int_issue_frac": float(f[4]), "issue_frac": float(f[5])}
+    except OSError:
+        pass
+    return out
+
+
+def vm_entry(stats: dict, delta: dict, clock_mhz, sm_count: int = 148) -> dict:
+    """The VMs' work per second of their kernel time, and the integer-issue
+    roofline: integer-pipe warp instructions per launch (ncu, committed
+    summary) over the live CUDA-event launch time, against the issue peak
+    (one warp instruction per cycle on each of the SMs' 4 sub-partitions)."""
+    out = {}
+    fast = stats.get("k_vm_fast", {"ms": 0, "launches": 0})
+    exact = stats.get("k_vm_general", {"ms": 0, "launches": 0})
+    if fast["ms"] > 0:
+        out["fast"] = {"kernel_ms": fast["ms"], "launches": fast["launches"],
+                       "accumulator_ops_per_s": delta["accumulator_ops"] / (fast["ms"] / 1000.0)}
+    if exact["ms"] > 0:
+        out["exact"] = {"kernel_ms": exact["ms"], "launches": exact["launches"],
+                        "bytecode_instructions_per_s": delta["exact_vm_instructions"] / (exact["ms"] / 1000.0)}
+    ms = fast["ms"] + exact["ms"]
+    if ms > 0:
+        out["program_cases_per_s"] = delta["program_cases"] / (ms / 1000.0)
+    issue = vm_issue_summary(ARGS_WORKLOAD[0])
+    clock = (clock_mhz or 1965.0) * 1e6
+    for name, st, key in (("k_vm_fast", fast, "fast"), ("k_vm_general", exact, "exact")):
+        if name in issue and st["launches"] and key in out:
+            per_launch_s = st["ms"] / st["launches"] / 1000.0
+            slots = sm_count * 4 * clock * per_launch_s
+            out[key]["roofline"] = {
+                "bound": "integer issue", "achieved_int_issue_frac": issue[name]["int_inst_per_launch"] / slots,
+                "achieved_issue_frac": issue[name]["inst_per_launch"] / slots,
+                "ncu_int_issue_frac": issue[name]["int_issue_frac"], "ncu_issue_frac": issue[name]["issue_frac"],
+                "source": "profiles/vm_issue_%s.txt instruction counts over the live launch time at %.0f MHz"
+                          % (ARGS_WORKLOAD[0], clock / 1e6)}
+    return out
+
+
+ARGS_WORKLOAD = ["poly4"]
 
 
 def run_own_arm(args, rank: int, world: int, local: int):
@@ -358,6 +462,7 @@ def run_own_arm(args, rank: int, world: int, local: int):
     if rank != 0:
         return
     launches = sum(v["launches"] for v in stats.values()) * args.steps // PROFILE_ROUNDS
+    clock_summary = clocks.summary()
     delta = {k: after[k] - before[k] for k in after if isinstance(after[k], int)}
     pdelta = {k: profiled[k] - after[k] for k in after if isinstance(after[k], int)}
     line = {"metric": METRIC, "value": cases / secs, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -367,11 +472,11 @@ def run_own_arm(args, rank: int, world: int, local: int):
             "kernels": {k: {"ms_per_step": v["ms"] / PROFILE_ROUNDS, "launches_per_step": v["launches"] / PROFILE_ROUNDS}
                         for k, v in stats.items()},
             "kernel_timing": "CUDA events per launch over %d profiled rounds right after the timed region" % PROFILE_ROUNDS,
-            "vm": vm_entry(stats, pdelta),
-            "roofline": roofline_entry(stats, pdelta, PROFILE_ROUNDS, peaks()), "clocks": clocks.summary(),
+            "roofline": roofline_entry(stats, pdelta, PROFILE_ROUNDS, peaks()), "clocks": clock_summary,
             "counters": {"program_cases": cases, "evaluated_programs": after["evaluated_programs"] - before["evaluated_programs"],
                          "reused_programs": after["reused_programs"] - before["reused_programs"],
-                         "vm_ops": after["vm_ops"] - before["vm_ops"],
+                         "accumulator_ops": after["accumulator_ops"] - before["accumulator_ops"],
+                         "exact_vm_instructions": after["exact_vm_instructions"] - before["exact_vm_instructions"],
                          "place_cycles_per_step": {k: (after[k] - before[k]) / args.steps for k in
                                                    ("place_generate_cycles", "place_stage_cycles",
                                                     "place_serial_cycles", "place_levels", "place_level_cycles")},
@@ -387,6 +492,7 @@ def run_own_arm(args, rank: int, world: int, local: int):
                          "generate_steps_per_generation": pdelta["generate_steps"] / max(1, pdelta["generations"]),
                          "generations_per_step": pdelta["generations"] / PROFILE_ROUNDS,
                          "generate_max_steps": profiled["generate_max_steps"]}}
+    line["vm"] = vm_entry(stats, pdelta, clock_summary.get("sm_mhz"))
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as d:
             make_task(seed, d)
@@ -396,8 +502,8 @@ def run_own_arm(args, rank: int, world: int, local: int):
 
 def _mix_tasks(entries):
     """The loaded tasks of the mix entries this engine admits, and how many
-    it declined at admission (the list programs: the grammar compiler raises
-    the reference's resident-admission decline for them)."""
+    it declined at admission (none of the scalar and list tasks of the
+    mixes is outside the resident subset)."""
     from gagp_b200 import grammar as G
     cache, tasks, declined = {}, [], 0
     for m in entries:
@@ -409,10 +515,11 @@ def _mix_tasks(entries):
 
 
 def run_batch_workload(args, rank: int, world: int):
-    """Batching: the scalar half of 64 independent searches (populations
-    log-uniform 256..8192, 16..1000 cases, 64 generations, seeds 0..63) run
-    as one batch (one launch sequence per round, rounds replayed from a CUDA
-    graph) against the plain path (each search alone, one after another)."""
+    """Batching: 64 independent searches, half scalar regressions and half
+    list programs (populations log-uniform 256..8192, 16..1000 cases, 64
+    generations, seeds 0..63) run as one batch (one launch sequence per
+    round, rounds replayed from a CUDA graph) against the plain path (each
+    search alone, one after another)."""
     from gagp_b200 import build
     from gagp_b200.engine import Engine
     dist = init_ranks(world, rank_info()[2])
@@ -459,9 +566,8 @@ def run_batch_workload(args, rank: int, world: int):
     line = {"metric": "searches/s", "value": n / batch_s, "unit": "searches/s", "n_gpus": world, "steps": 1,
             "warmup": 1, "ms_per_step": 1000.0 * (t2 - t1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": "batch of the admitted (scalar) searches of a 64-search mix (populations "
-                                   "log-uniform 256..8192, 16..1000 cases, 64 generations, seeds 0..63; the list "
-                                   "programs are declined at admission)",
+            "config": {"workload": "batch of a 64-search mix, half scalar regressions and half list programs "
+                                   "(populations log-uniform 256..8192, 16..1000 cases, 64 generations, seeds 0..63)",
                        "searches": int(n), "declined_list_searches": declined,
                        "parallelism": "searches sharded round-robin over %d GPUs" % world if world > 1 else "single-gpu"},
             "e2e": {"value": n / e2e_s, "unit": "searches/s", "seconds": e2e_s},
@@ -474,10 +580,11 @@ def run_batch_workload(args, rank: int, world: int):
 
 
 def run_serve_workload(args, rank: int, world: int):
-    """Serving: an open-loop Poisson stream of the scalar requests of a
-    config-5 mix (populations log-uniform 256..16384, 16..2000 cases, 32..128
-    generations) through the continuous-batching server; searches/s and
-    p50/p99 time-to-result against the plain path."""
+    """Serving: an open-loop Poisson stream of the requests of a serving mix
+    (half scalar regressions, half list programs; populations log-uniform
+    256..16384, 16..2000 cases, 32..128 generations) through the
+    continuous-batching server; searches/s and p50/p99 time-to-result against
+    the plain path."""
     import random
     from gagp_b200 import build
     from gagp_b200.engine import Engine, Server
@@ -547,10 +654,9 @@ def run_serve_workload(args, rank: int, world: int):
     line = {"metric": "searches/s", "value": n / makespan, "unit": "searches/s", "n_gpus": 1, "steps": n,
             "warmup": 1, "ms_per_step": 1000.0 * makespan / n, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": "open-loop Poisson stream of the admitted (scalar) requests of a %d-request "
-                                   "serving mix (populations log-uniform 256..16384, 16..2000 cases, 32..128 "
-                                   "generations; the list-program requests are declined at admission)"
-                                   % args.requests,
+            "config": {"workload": "open-loop Poisson stream of a %d-request serving mix, scalar regressions and "
+                                   "list programs (populations log-uniform 256..16384, 16..2000 cases, 32..128 "
+                                   "generations)" % args.requests,
                        "requests": n, "declined_list_requests": declined, "arrival_rate_per_s": args.rate,
                        "parallelism": "single-gpu"},
             "latency_s": {"p50": pct(0.5), "p99": pct(0.99), "max": latencies[-1]},
@@ -570,13 +676,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="poly4", choices=["poly4", "batch", "serve"],
-                    help="poly4: the large scalar search (default); batch: 64-search batching mix; "
-                         "serve: open-loop serving stream")
+    ap.add_argument("--workload", default="poly4", choices=["poly4", "list", "batch", "serve"],
+                    help="poly4: the large scalar search (default); list: the list-program search; "
+                         "batch: 64-search batching mix; serve: open-loop serving stream")
     ap.add_argument("--requests", type=int, default=500, help="serve: requests in the mix")
     ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrival rate (requests/s)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global WORKLOAD
+    if args.workload in SEARCH_WORKLOADS:
+        WORKLOAD = SEARCH_WORKLOADS[args.workload]
+        ARGS_WORKLOAD[0] = args.workload
     if args.steps + args.warmup + PROFILE_ROUNDS > WORKLOAD["generations"]:
         raise SystemExit("steps + warmup + %d profiled rounds must not exceed the search's %d rounds"
                          % (PROFILE_ROUNDS, WORKLOAD["generations"]))
@@ -588,6 +698,11 @@ def main():
         run_serve_workload(args, rank, world)
         return
     if args.impl == "reference":
+        if args.workload not in SEARCH_WORKLOADS:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference arm runs the single-search "
+                                  "workloads (poly4, list); the batch and serve mixes compare against the plain path"}))
+            return
         run_reference_arm(args, rank, world)
     else:
         run_own_arm(args, rank, world, local)

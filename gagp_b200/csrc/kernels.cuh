@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256) k_vm_general(const SearchDesc* descs, int
       unsigned long long ts = 0;
       for (int w = 0; w < (blockDim.x >> 5); ++w) { tl += red_loss[w]; tw += red_wrong[w]; ts += red_steps[w]; }
       store_result(s, mode, p.slot, tl, tw);
-      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]), ts);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[24]), ts);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
     }

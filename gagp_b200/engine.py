@@ -143,9 +143,10 @@ class Engine:
         return ms.value
 
     def counters(self, search: Search) -> dict:
-        out = (C.c_uint64 * 24)()
-        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out, C.c_int32(24)))
-        return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2], "vm_ops": out[3],
+        out = (C.c_uint64 * 25)()
+        _check(load_library().gagp_b200_search_counters(self.handle, C.c_int32(search.id), out, C.c_int32(25)))
+        return {"evaluated_programs": out[0], "reused_programs": out[1], "program_cases": out[2],
+                "accumulator_ops": out[3], "exact_vm_instructions": out[24],
                 "place_generate_cycles": out[4], "place_stage_cycles": out[5], "place_serial_cycles": out[6],
                 "place_levels": out[7], "vary_bytes": out[8], "lower_bytes": out[9],
                 "vary_select_cycles": out[10], "vary_crossover_cycles": out[11], "vary_generate_cycles": out[12],

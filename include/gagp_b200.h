@@ -264,8 +264,10 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
 
 /* Work counters of a search so far: [0] program evaluations, [1] children
  * that reused their parent's result, [2] evaluated (program, case) pairs,
- * [3] VM instructions executed over all cases (accumulator VM: added when
- * a program's last case tile finishes), [4..6] SM clock cycles of
+ * [3] accumulator-VM instructions executed over all cases (added when a
+ * program's last case tile finishes), [24] bytecode instructions the exact
+ * VM executed (the reference's fuel consumed by those programs), [4..6] SM
+ * clock cycles of
  * the placement phases (stream generation, draw staging, placement),
  * [7] placement levels (+2^20 per sequential replay), [8] and [10..23]
  * only while kernel profiling is on (gagp_b200_engine_profile): [8] bytes the
@@ -285,7 +287,7 @@ gagp_status gagp_b200_search_progress(gagp_engine* engine, int32_t search, int32
  * result reads). */
 gagp_status gagp_b200_engine_transfers(gagp_engine* engine, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
 
-#define GAGP_COUNTERS 24
+#define GAGP_COUNTERS 25
 gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint64_t* out, int32_t count);
 
 /* Per-kernel CUDA-event timing: enable (resets) or disable, then read the
