@@ -781,11 +781,25 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
         !g->nonterminals[x.target].fixed)
       f.site_class = x.target * 16 + x.scope_count;
   }
-  // cases, input-major
+  // cases, input-major.  With IntList inputs the cases are ordered by their
+  // lists' total length, so that the 32 cases of a VM warp loop about as
+  // many times (a program's loss and wrong count are integer sums, which
+  // the case order does not change)
   const int C = c->case_count, NI = c->input_count;
-  std::vector<int64_t> inputs(size_t(std::max(1, NI)) * C, 0);
-  for (int j = 0; j < NI; ++j)
-    for (int k = 0; k < C; ++k) inputs[size_t(j) * C + k] = c->inputs[size_t(k) * NI + j];
+  std::vector<int> order(C);
+  std::iota(order.begin(), order.end(), 0);
+  if (c->list_values) {
+    std::vector<int64_t> length(C, 0);
+    for (int k = 0; k < C; ++k)
+      for (int j = 0; j < NI; ++j)
+        if (c->input_tags[j] == GAGP_TAG_INTLIST) length[k] += c->list_values[c->inputs[size_t(k) * NI + j]];
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return length[x] < length[y]; });
+  }
+  std::vector<int64_t> inputs(size_t(std::max(1, NI)) * C, 0), expected(C);
+  for (int k = 0; k < C; ++k) {
+    for (int j = 0; j < NI; ++j) inputs[size_t(j) * C + k] = c->inputs[size_t(order[k]) * NI + j];
+    expected[k] = c->expected[order[k]];
+  }
   std::vector<int32_t> local_types(GAGP_MAX_LOCALS, GAGP_TAG_INVALID);
   for (int j = 0; j < g->local_count; ++j) local_types[j] = g->local_types[j];
   auto up = [&](size_t off, const void* src, size_t bytes) {
@@ -839,7 +853,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   const std::vector<gb::RegionInfo> regions = region_infos(g);
   CUDA_TRY(up(p.regions, regions.data(), sizeof(gb::RegionInfo) * regions.size()));
   CUDA_TRY(up(p.inputs, inputs.data(), sizeof(int64_t) * inputs.size()));
-  CUDA_TRY(up(p.expected, c->expected, sizeof(int64_t) * C));
+  CUDA_TRY(up(p.expected, expected.data(), sizeof(int64_t) * C));
   const int64_t n_lists = c->list_values ? c->list_value_count : 0;
   if (n_lists) CUDA_TRY(up(p.lists, c->list_values, sizeof(int64_t) * size_t(n_lists)));
 
@@ -1042,11 +1056,11 @@ void vm_fast_launch(int lanes, int blocks, int threads, size_t smem, cudaStream_
   }
 }
 
-// Exact-VM launch over counts[1] programs: persistent blocks of 256 threads,
-// each program's bytecode (bc_stride_max instructions of 20 bytes) and
-// constants (8 bytes each) staged in dynamic shared memory.
-constexpr int kGeneralThreads = 256;
-size_t vm_general_smem(int bc_stride_max) { return size_t(bc_stride_max) * (20 + 8); }
+// Exact-VM launch over counts[1] programs: persistent blocks of 8 warps,
+// each program's bytecode staged in dynamic shared memory with the warp-SIMD
+// VM's slots (gb::general_smem_bytes).
+constexpr int kGeneralThreads = gb::kGeneralWarps * 32;
+size_t vm_general_smem(int bc_stride_max) { return gb::general_smem_bytes(bc_stride_max); }
 // `heavy`: most programs may be on the list, so the grid fills every SM;
 // otherwise the list is rarely more than a handful of programs and a
 // quarter of the SMs take them (an empty launch of a full grid costs a few

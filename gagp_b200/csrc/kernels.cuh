@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
         raise_error(s, 30);  // the phase compiler rejected a constructed program
       } else {
         s.bc_len[slot] = bl;
-        s.bc_locals[slot] = r.locals;
+        s.bc_locals[slot] = r.locals | (r.stack_bound << 8);
         s.code_temps[slot] = -1;
         general_list[atomicAdd(&list_count[1], 1)] = ProgramRef{si, slot};
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
@@ -140,45 +140,82 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
 
 // General VM: the programs the accumulator VM cannot run (list programs,
 // possible runtime errors or fuel exhaustion) on the exact interpreter.
-// Persistent blocks take one program of the list at a time: its bytecode
-// and constants are staged in shared memory (dynamic: bc_stride_max
-// instructions and constants), then the block's threads run its cases, a
-// case per thread, and the block reduces the losses in order-free integer
-// sums.  A separate kernel from the fast VM, so that the interpreter's
-// registers and local arrays do not lower the fast VM's occupancy.
-__global__ void __launch_bounds__(256) k_vm_general(const SearchDesc* descs, int mode, const ProgramRef* list,
-                                                    const int32_t* list_count, int bc_stride_max) {
+// Persistent blocks of 8 warps take one program of the list at a time and
+// stage its bytecode and constants in shared memory.  A program whose costs
+// are all 1..255 and whose locals and stack fit kSimdSlots runs on the
+// warp-SIMD VM (run_program_simd): the block's warps take its tiles of 32
+// cases; any other runs on run_program, a case per thread.  The block
+// reduces the losses in order-free integer sums.  A separate kernel from the
+// fast VM, so that the interpreters' registers and local arrays do not
+// lower the fast VM's occupancy.
+//
+// Dynamic shared memory: constants (bc_stride_max int64), the 5-int code
+// (bc_stride_max instructions), the staged SIMD words (bc_stride_max uint2)
+// and per warp kSimdSlots x 32 int64 slots.
+constexpr int kGeneralWarps = 8;
+__host__ __device__ __forceinline__ size_t general_smem_bytes(int bc_stride_max) {
+  return size_t(bc_stride_max) * (8 + 20 + 8) + 16 + size_t(kGeneralWarps) * kSimdSlots * 32 * 8;
+}
+__global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchDesc* descs, int mode,
+                                                                   const ProgramRef* list, const int32_t* list_count,
+                                                                   int bc_stride_max) {
   extern __shared__ __align__(16) int64_t smem_general[];
-  __shared__ int64_t red_loss[32];
-  __shared__ uint32_t red_wrong[32];
-  __shared__ unsigned long long red_steps[32];
+  __shared__ int64_t red_loss[kGeneralWarps];
+  __shared__ uint32_t red_wrong[kGeneralWarps];
+  __shared__ unsigned long long red_steps[kGeneralWarps];
   int64_t* consts = smem_general;
-  int32_t* code = reinterpret_cast<int32_t*>(smem_general + bc_stride_max);
+  uint2* words = reinterpret_cast<uint2*>(smem_general + bc_stride_max);
+  int32_t* code = reinterpret_cast<int32_t*>(smem_general + 2 * size_t(bc_stride_max));
+  int64_t* slots_all = smem_general + 2 * size_t(bc_stride_max) + (5 * size_t(bc_stride_max) + 1) / 2;
   const int count = *list_count;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t* slots = slots_all + size_t(warp) * kSimdSlots * 32;
   for (int i = blockIdx.x; i < count; i += gridDim.x) {
     const ProgramRef p = list[i];
     const SearchDesc& s = descs[p.search];
-    const int n = s.bc_len[p.slot], n_locals = s.bc_locals[p.slot];
+    const int n = s.bc_len[p.slot], shape = s.bc_locals[p.slot];
+    const int n_locals = shape & 0xff, stack_bound = (shape >> 8) & 0xff;
+    bool simd_ok = n_locals + stack_bound <= kSimdSlots;
     {
       const int32_t* gcode = s.bc + size_t(p.slot) * 5 * s.bc_stride;
       const int64_t* gconsts = s.bc_consts + size_t(p.slot) * s.bc_stride;
       for (int k = threadIdx.x; k < 5 * n; k += blockDim.x) code[k] = gcode[k];
-      for (int k = threadIdx.x; k < n; k += blockDim.x) consts[k] = gconsts[k];  // at most one constant per instruction
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        consts[k] = gconsts[k];  // at most one constant per instruction
+        const int32_t* x = gcode + 5 * k;
+        const int cost = x[4];
+        simd_ok &= cost >= 1 && cost <= 255 && x[3] >= 0 && x[3] <= 255;
+        words[k] = make_uint2(uint32_t(x[0] & 0xff) | (uint32_t(x[1] & 0xff) << 8) | (uint32_t(x[3] & 0xff) << 16) |
+                                  (uint32_t(cost & 0xff) << 24),
+                              uint32_t(x[2]));
+      }
     }
-    __syncthreads();
+    simd_ok = __syncthreads_and(simd_ok);
     const VmView view = vm_view(s);
     int64_t loss = 0;
     uint32_t wrong = 0;
     uint64_t steps = 0;
-    for (int c = threadIdx.x; c < s.C; c += blockDim.x) {
-      int64_t value = 0;
-      int tag = 0;
-      if (run_program(view, code, n, consts, n_locals, c, value, tag, steps)) {
-        loss += case_loss(s, tag, value, s.expected[c], wrong);
-      } else {
-        loss += error_loss(s);
-        ++wrong;
+    if (simd_ok) {
+      for (int c0 = warp * 32; c0 < s.C; c0 += kGeneralWarps * 32) {
+        const int c = c0 + lane;
+        const bool live = c < s.C;
+        const SimdCase r = run_program_simd(view, words, n, consts, n_locals, c, live, slots);
+        if (live) {
+          if (r.ok) loss += case_loss(s, s.slot_type, r.value, s.expected[c], wrong);
+          else { loss += error_loss(s); ++wrong; }
+        }
+        steps += r.steps;
+      }
+    } else {
+      for (int c = threadIdx.x; c < s.C; c += blockDim.x) {
+        int64_t value = 0;
+        int tag = 0;
+        if (run_program(view, code, n, consts, n_locals, c, value, tag, steps)) {
+          loss += case_loss(s, tag, value, s.expected[c], wrong);
+        } else {
+          loss += error_loss(s);
+          ++wrong;
+        }
       }
     }
     loss = warp_sum(loss);
@@ -190,7 +227,7 @@ __global__ void __launch_bounds__(256) k_vm_general(const SearchDesc* descs, int
       int64_t tl = 0;
       uint32_t tw = 0;
       unsigned long long ts = 0;
-      for (int w = 0; w < (blockDim.x >> 5); ++w) { tl += red_loss[w]; tw += red_wrong[w]; ts += red_steps[w]; }
+      for (int w = 0; w < kGeneralWarps; ++w) { tl += red_loss[w]; tw += red_wrong[w]; ts += red_steps[w]; }
       store_result(s, mode, p.slot, tl, tw);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[24]), ts);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);

@@ -154,7 +154,7 @@ struct SearchDesc {
   unsigned long long* vm_acc;
   int32_t* bc;                         // reference bytecode (op,flags,a,b,fuel) per program
   int32_t* bc_len;
-  int32_t* bc_locals;                  // locals of each lowered program (inputs + temporaries)
+  int32_t* bc_locals;                  // per lowered program: locals (inputs + temporaries) | stack bound << 8
   int64_t* bc_consts;
   int32_t bc_stride;                   // instructions per program slot
   // ---- run generator (MT19937-64) and its output stream

@@ -443,4 +443,118 @@ __host__ __device__ inline bool run_program(const VmView& v, const int32_t* code
   return false;  // finished without return
 }
 
+// ------------------------------------------------------------ warp-SIMD exact VM
+// The exact VM for the 32 cases of one tile, executed by one warp with one
+// decoded instruction at a time: every lane keeps its own instruction
+// pointer, fuel and result, and at each step the lanes whose pointer is the
+// smallest among the running lanes execute the instruction there together
+// (a warp-uniform opcode, so no divergence inside the step).  Lanes that
+// are ahead -- past a branch the others did not take, or out of a loop the
+// others are still in -- wait until the others reach them, so branch joins
+// and loop exits re-merge the warp.  The thread-per-case VM instead lets the
+// lanes drift apart, after which every distinct opcode of a step runs
+// serially.
+//
+// The stack and the locals live in shared memory as [slot][lane] columns of
+// int64 payloads: locals first (inputs preset), then the stack.  Tags are
+// not kept: the lowering's output is well typed (each operation's operands
+// have the grammar's types, the stack depth and the definedness of every
+// local are fixed per instruction), so none of the reference VM's type,
+// underflow or uninitialised-local checks can fail on it and the result's
+// tag is the phase's type; the checks that can fail on some case -- fuel,
+// modulo by zero, index range -- are kept.  Results equal run_program's.
+//
+// Staged instruction word: x = op | flags << 8 | b << 16 | cost << 24,
+// y = a.  The kernel stages a program this way only when every cost is in
+// 1..255 and its locals and stack fit kSimdSlots; otherwise it runs it on
+// run_program.
+constexpr int kSimdSlots = 24;
+constexpr int kSimdDone = 0x7fffffff;
+
+struct SimdCase {
+  int64_t value;
+  bool ok;
+  uint32_t steps;
+};
+
+__device__ inline SimdCase run_program_simd(const VmView& v, const uint2* code, int n, const int64_t* consts,
+                                            int n_locals, int c, bool live, int64_t* slots) {
+  const int lane = threadIdx.x & 31;
+  SimdCase out{0, false, 0};
+  // locals [0, n_locals): inputs preset; the stack follows
+  for (int j = 0; j < v.n_inputs; ++j)
+    if (live) slots[j * 32 + lane] = __ldg(&v.inputs[size_t(j) * v.C + c]);
+  int ip = live ? 0 : kSimdDone, sp = n_locals, fuel = v.fuel;
+  auto at = [&](int k) -> int64_t& { return slots[k * 32 + lane]; };
+  for (;;) {
+    const int ipm = __reduce_min_sync(kFull, ip);
+    if (ipm == kSimdDone) break;
+    if (ip != ipm) continue;
+    const uint2 w = code[ipm];
+    const int op = int(w.x & 0xffu), flags = int((w.x >> 8) & 0xffu), b = int((w.x >> 16) & 0xffu);
+    const int cost = int(w.x >> 24), a = int(w.y);
+    if (fuel < cost) { ip = kSimdDone; continue; }  // Timeout
+    fuel -= cost;
+    ++out.steps;
+    ++ip;
+    switch (op) {
+      case OP_PUSH_CONST: at(sp++) = consts[a]; break;
+      case OP_LOAD: { const int64_t x = at(a); at(sp++) = x; break; }
+      case OP_STORE: at(a) = at(--sp); break;
+      case OP_CHECK_INT: break;
+      case OP_NEG: at(sp - 1) = wrap_neg(at(sp - 1)); break;
+      case OP_NOT: at(sp - 1) ^= 1; break;
+      case OP_ADD: case OP_SUB: case OP_MUL: case OP_MOD: {
+        const int64_t y = at(--sp), x = at(sp - 1);
+        if (op == OP_MOD && y == 0) { ip = kSimdDone; break; }  // ZeroDiv
+        at(sp - 1) = op == OP_ADD ? wrap_add(x, y) : op == OP_SUB ? wrap_sub(x, y) : op == OP_MUL ? wrap_mul(x, y)
+                                                                                              : py_mod(x, y);
+        break;
+      }
+      case OP_LT: case OP_LE: case OP_GT: case OP_GE: case OP_EQ: case OP_NE: {
+        const int64_t y = at(--sp), x = at(sp - 1);
+        at(sp - 1) = op == OP_LT ? x < y : op == OP_LE ? x <= y : op == OP_GT ? x > y : op == OP_GE ? x >= y
+                   : op == OP_EQ ? x == y : x != y;
+        break;
+      }
+      case OP_JMP: ip = a; break;
+      case OP_JMP_IF_FALSE: case OP_JMP_IF_TRUE: {
+        const int64_t y = at(--sp);
+        if ((op == OP_JMP_IF_FALSE) == (y == 0)) ip = a;
+        break;
+      }
+      case OP_CALL_BUILTIN: {
+        int64_t r = 0;
+        if (a == B_LEN) {
+          r = __ldg(&v.lists[at(sp - 1)]);
+        } else if (a == B_INDEX) {
+          const int64_t j0 = at(--sp), h = at(sp - 1), len = __ldg(&v.lists[h]);
+          const int64_t j = j0 < 0 ? j0 + len : j0;
+          if (j < 0 || j >= len) { ip = kSimdDone; break; }  // index out of range
+          r = __ldg(&v.lists[h + 1 + j]);
+        } else if (a == B_ABS) {
+          const int64_t x = at(sp - 1);
+          r = x < 0 ? wrap_neg(x) : x;
+        } else {
+          const int64_t q = at(--sp), p = at(sp - 1);
+          r = a == B_MIN ? (p < q ? p : q) : a == B_MAX ? (p > q ? p : q) : a == B_IDIV0 ? idiv0(p, q)
+            : a == B_IMOD0 ? imod0(p, q) : a == B_TRUNC_DIV0 ? tdiv0(p, q) : tmod0(p, q);
+        }
+        at(sp - 1) = r;
+        break;
+      }
+      case OP_RETURN:
+        out.value = at(sp - 1);
+        out.ok = true;
+        ip = kSimdDone;
+        break;
+      default:
+        ip = kSimdDone;  // not emitted by the lowering
+    }
+    (void)flags;
+    (void)b;
+  }
+  return out;
+}
+
 }  // namespace gb

@@ -74,6 +74,7 @@ LOWER_CASES = [
     ("lower_list_nested", "list", dict(population=256, generations=1, seed=22, cases=24, target="max"), "nested"),
     ("lower_list_reverse", "list", dict(population=256, generations=1, seed=23, cases=24, target="max"), "reverse"),
     ("lower_poly4", "poly4", dict(population=256, generations=1, seed=24, cases=32), None),
+    ("lower_list_deep", "list", dict(population=384, generations=1, seed=25, cases=40, target="max"), "deep"),
 ]
 
 
@@ -97,6 +98,29 @@ def nested_traversal_grammar() -> dict:
     return g
 
 
+def deep_traversal_grammar() -> dict:
+    """The nested-traversal grammar with a third traversal inside the inner
+    body (binder numbers 6..8): a program with all three open needs 29
+    locals (2 inputs + 3 x 9 temporaries)."""
+    g = nested_traversal_grammar()
+    inner = next(r for r in g["nonterminals"] if r["id"] == "Inner")
+    inner["alternatives"].append({"id": "inner2", "weight": 2, "expression": {
+        "signature": "traverse(IntList,Int,Int,Int)->Int",
+        "args": [{"input": "xs"}, {"constant": {"type": "Int", "values": ["1"]}}, {"bound": "acc2"}, {"ref": "Inner2"}],
+        "bind": {"3": ["e3", "i3", "acc3"]}}})
+    g["nonterminals"].append({"id": "Inner2", "type": "Int", "scope": [
+        {"name": "e2", "type": "Int"}, {"name": "e3", "type": "Int"}, {"name": "i3", "type": "Int"},
+        {"name": "acc3", "type": "Int"}],
+        "alternatives": [
+            {"id": "acc3", "weight": 1, "expression": {"bound": "acc3"}},
+            {"id": "max", "weight": 2, "expression": {"signature": "if(Bool,Int,Int)->Int", "args": [
+                {"signature": "gt(Int,Int)->Bool", "args": [{"bound": "e3"}, {"bound": "acc3"}]},
+                {"bound": "e3"}, {"bound": "acc3"}]}},
+            {"id": "idx", "weight": 1, "expression": {"signature": "add(Int,Int)->Int",
+                                                      "args": [{"bound": "i3"}, {"bound": "e2"}]}}]})
+    return g
+
+
 def reverse_traversal_grammar() -> dict:
     """The list grammar with the fold as a reverse traversal beside the
     forward one."""
@@ -113,6 +137,8 @@ def variant_grammar(variant):
         return nested_traversal_grammar()
     if variant == "reverse":
         return reverse_traversal_grammar()
+    if variant == "deep":
+        return deep_traversal_grammar()
     return None
 
 
