@@ -143,11 +143,12 @@ namespace {
 
 enum KernelId {
   KN_INIT, KN_LOWER, KN_VM_FAST, KN_KEYS, KN_START, KN_RECORD, KN_VARY, KN_CHILD, KN_PLACE,
-  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_VM_GENERAL, KN_COUNT
+  KN_COMMIT, KN_STREAM, KN_LEVELS, KN_VM_GENERAL, KN_INDEX, KN_COUNT
 };
 const char* const kKernelNames[KN_COUNT] = {"k_init_population", "k_lower", "k_vm_fast",
                                             "k_member_keys", "k_start", "k_record", "k_vary", "k_child_results",
-                                            "k_place", "k_commit", "k_stream", "k_place_levels", "k_vm_general"};
+                                            "k_place", "k_commit", "k_stream", "k_place_levels", "k_vm_general",
+                                            "k_member_index"};
 
 cudaEvent_t take_event(gagp_engine* e) {
   if (e->event_next == e->event_pool.size()) {
@@ -578,6 +579,8 @@ struct Plan {
       gen_nt, local_types, regions, inputs, expected, lists;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
+  size_t mtab, mhash;
+  int mtab_slots = 0;
   size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, child_level, level_plan, round,
       hist_sum, hist_fitness,
@@ -627,6 +630,9 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.c_parent = L.take(4 * size_t(B)); p.c_reuse = L.take(4 * size_t(B)); p.c_error = L.take(4 * size_t(B));
   p.c_fitness = L.take(8 * size_t(B)); p.c_wrong = L.take(4 * size_t(B)); p.c_nodes = L.take(4 * size_t(B));
   p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
+  p.mtab_slots = 2;
+  while (p.mtab_slots < 2 * P) p.mtab_slots *= 2;
+  p.mtab = L.take(4 * size_t(p.mtab_slots)); p.mhash = L.take(8 * size_t(P));
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
   p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots); p.vm_acc = L.take(16 * slots);
@@ -761,6 +767,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   s->bytes = p.L.total;
   CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->block), s->bytes, e->pool, e->stream));
   CUDA_TRY(cudaMemsetAsync(s->block, 0, s->bytes, e->stream));
+  CUDA_TRY(cudaMemsetAsync(s->block + p.mtab, 0xff, 4 * size_t(p.mtab_slots), e->stream));  // an empty member index
   char* b = s->block;
   const int E = g->expression_count;
   // derived per-expression facts
@@ -900,6 +907,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
   d.c_fitness = at<double>(b, p.c_fitness); d.c_wrong = at<uint32_t>(b, p.c_wrong);
   d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
+  d.mtab = at<int32_t>(b, p.mtab); d.mhash = at<uint64_t>(b, p.mhash); d.mtab_mask = p.mtab_slots - 1;
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
   d.vm_acc = at<unsigned long long>(b, p.vm_acc);
@@ -1172,6 +1180,12 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   // the history entry reads only what the placement later rewrites
   { Timed t(e, KN_RECORD, e->side); gb::k_record<<<v.n, 1024, 0, e->side>>>(v.d_desc, v.n, 1); }
   CUDA_TRY(cudaEventRecord(e->join, e->side));
+  // the round's member index (one member per distinct row), which the
+  // variation kernels probe for children their parents do not cover
+  {
+    Timed t(e, KN_INDEX);
+    gb::k_member_index<<<blocks_for(v.total_members, 8), 256, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+  }
   // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
   // next child of the variation warps; range c's lists start at item lo
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));

@@ -77,8 +77,60 @@ __device__ inline void load_members(const SearchDesc& s, int a, SRow& to_a, int 
   __syncwarp();
 }
 
+// Hash of a row's genotype (construction expressions and constants): a
+// wrap-around sum over positions of a mixed (value, position) word, so that
+// the lanes hash their strided elements independently.  Equality of rows
+// decides a reuse; the hash only picks candidates, as the reference's
+// serial FNV-style fold does (parent_cache::hash_program,
+// parent_fitness_cache.cuh:15-31).  Every lane returns the same hash.
+__device__ inline uint64_t warp_row_hash(const uint64_t* node, const int64_t* cval, int n, int nc) {
+  const int lane = lane_id();
+  uint64_t acc = 0;
+  for (int i = lane; i < n; i += 32) acc += mix64(uint64_t(w_origin(node[i])) | (uint64_t(i) << 32));
+  for (int i = lane; i < nc; i += 32) acc += mix64(uint64_t(cval[i]) ^ mix64(0x5bd1e995ULL + uint64_t(i)));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+  return mix64(acc ^ (uint64_t(n) << 40) ^ (uint64_t(nc) << 20));
+}
+
+// Genotype equality of two rows (parent_cache::equal_program,
+// parent_fitness_cache.cuh:33-48): lengths, construction expressions (every
+// other node field is a function of them) and constants.
+__device__ inline bool warp_rows_equal(const uint64_t* an, const int64_t* ac, int a_n, int a_nc, const uint64_t* bn,
+                                       const int64_t* bc, int b_n, int b_nc) {
+  if (a_n != b_n || a_nc != b_nc) return false;
+  bool same = true;
+  for (int i = lane_id(); i < a_n; i += 32) same &= w_origin(an[i]) == w_origin(bn[i]);
+  for (int i = lane_id(); i < a_nc; i += 32) same &= ac[i] == bc[i];
+  return __all_sync(kFull, same);
+}
+
+// A current member identical to `row` (the member_hashes lookup of
+// HostPhasePopulation::make_batch, phase_population_cpu.cpp:336-339): the
+// round's member index holds one member per distinct row, probed linearly
+// from the row's hash up to an empty slot.  Which identical member is found
+// does not matter: identical programs score the same.  -1: none.
+__device__ inline int warp_find_member(const SearchDesc& s, const SRow& row) {
+  const uint64_t h = warp_row_hash(row.node, row.cval, row.n, row.nc);
+  const uint32_t mask = uint32_t(s.mtab_mask);
+  uint32_t slot = uint32_t(h) & mask;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const int m = s.mtab[slot];
+    if (m < 0) return -1;
+    if (s.mhash[m] == h) {
+      const int32_t l = s.len[m];
+      if (warp_rows_equal(s.node + size_t(m) * s.stride, s.cval + size_t(m) * s.stride, len_nodes(l), len_consts(l),
+                          row.node, row.cval, row.n, row.nc))
+        return m;
+    }
+    slot = (slot + 1) & mask;
+  }
+  return -1;
+}
+
 // One child, by one warp.  Writes the child row, its parent and reuse
-// source (the parent when the genotype is unchanged) and returns the
+// source (the parent when the genotype is unchanged, else an identical
+// current member) and returns the
 // reference's OperatorStats error code (0: none).  stamp[0..2]: SM clock
 // after selection, after crossover, after the mutation's subtree generation
 // (left 0 for phases not reached); stamp[4]: the generation's steps + 1 on
@@ -177,6 +229,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
     equal = __all_sync(kFull, mine);
   }
   if (equal) *reuse_out = parent;
+  else if (s.mtab) *reuse_out = warp_find_member(s, w.child);
   // ---- publish the child row
   for (int i = lane; i < w.child.n; i += 32) s.cnode[size_t(child) * s.stride + i] = w.child.node[i];
   for (int i = lane; i < w.child.nc; i += 32) s.ccval[size_t(child) * s.stride + i] = w.child.cval[i];

@@ -203,9 +203,8 @@ typedef struct gagp_search_result {
   int32_t* final_nodes;
   gagp_rows final_rows;
   uint64_t evaluated_programs;      /* program evaluations run */
-  uint64_t reused_programs;         /* children reusing their parent's result (a child equal to its
-                                       parent); the reference also counts children equal to any
-                                       other member, which this engine evaluates */
+  uint64_t reused_programs;         /* children reusing a completed result: their parent's when
+                                       unchanged, else an identical current member's */
   uint64_t program_cases;           /* evaluated (program, case) pairs */
 } gagp_search_result;
 

@@ -59,8 +59,14 @@ def binder_names_in_order(text: str) -> str:
 
 
 def compare_result(lt: T.LoadedTask, got: dict, run: dict, label: str = "") -> None:
-    """Asserts a search result equals the reference run bit for bit."""
+    """Asserts a search result equals the reference run bit for bit: history,
+    final ranked population and the evaluation counters (program-case pairs
+    evaluated, children that reused a completed result)."""
     ref_hist, ref_final = run["history"], run["final"]
+    assert got["program_cases"] == run["program_cases"], (label, "program_cases", got["program_cases"],
+                                                          run["program_cases"])
+    assert got["reused_programs"] == run["reused_programs"], (label, "reused", got["reused_programs"],
+                                                              run["reused_programs"])
     assert len(got["history"]) == len(ref_hist), label
     for i, (a, b) in enumerate(zip(got["history"], ref_hist)):
         text = binder_names_in_order(T.program_text(lt.tables, *a["row"]))

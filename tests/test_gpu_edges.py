@@ -51,7 +51,7 @@ def test_edge_shape_matches_oracle(engine, tmp_path, name, population, cases, ge
     if fitness is not None:
         files.fitness = fitness
     lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
-    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings, member_reuse=True)
     s = engine.admit(lt)
     try:
         s.run()
@@ -79,7 +79,7 @@ def test_batch_entry_points_reject_a_repeated_search(engine, tmp_path):
                 call()
             assert err.value.status == 2 and "more than once" in str(err.value)
         s.run()
-        want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+        want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings, member_reuse=True)
         assert s.result()["final"] == want["final"]
     finally:
         s.close()

@@ -54,7 +54,7 @@ def test_search_matches_oracle_fresh_seeds(engine, seed, tmp_path):
     files = W.poly4(population=384, generations=6, seed=seed, cases=300)
     from gagp_b200 import task as T
     lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
-    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings, member_reuse=True)
     s = engine.admit(lt)
     s.run()
     got = s.result()
@@ -107,7 +107,7 @@ def test_cluster_placement_matches_oracle(engine, tmp_path, population, seed):
     from gagp_b200 import task as T
     files = W.poly4(population=population, generations=3, seed=seed, cases=24, max_nodes=40)
     lt = T.load(files.write(str(tmp_path)), str(tmp_path / "search.json"))
-    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    want = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings, member_reuse=True)
     s = engine.admit(lt)
     try:
         s.run()

@@ -61,7 +61,7 @@ def test_oracle_initial_population_matches_reference(name):
 def test_oracle_search_matches_reference(name):
     fx = GU.fixture(name)
     lt = GU.load_task(fx)
-    got = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings)
+    got = oracle.search(abi.GrammarBlob(lt.tables), lt.cases, lt.settings, member_reuse=True)
     GU.compare_result(lt, got, fx["run"], name)
 
 
@@ -71,7 +71,7 @@ def test_oracle_imported_population_reproduces_generated_one():
     lt = GU.load_task(fx)
     gb = abi.GrammarBlob(lt.tables)
     rows = GU.reference_rows(fx["initial"], lt.tables.max_nodes - lt.tables.fixed_nodes)
-    got = oracle.search(gb, lt.cases, lt.settings, initial=rows)
+    got = oracle.search(gb, lt.cases, lt.settings, initial=rows, member_reuse=True)
     GU.compare_result(lt, got, fx["run"], "imported")
 
 
