@@ -74,7 +74,7 @@ struct gagp_engine {
   cudaStream_t stream = nullptr;
   // side stream of the run-generator top-up, forked from and joined to `stream`
   cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, indexed = nullptr;
   // the children of a round in kChunks ranges, each varied, lowered and
   // evaluated on its own stream so that one range's slowest children
   // overlap the other ranges' work
@@ -675,6 +675,7 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&e->indexed, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->chunk_fork, cudaEventDisableTiming));
   for (int c = 0; c < gagp_engine::kChunks; ++c) {
     CUDA_TRY(cudaStreamCreateWithFlags(&e->chunk_stream[c], cudaStreamNonBlocking));
@@ -727,6 +728,7 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   if (e->side) cudaStreamDestroy(e->side);
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->join) cudaEventDestroy(e->join);
+  if (e->indexed) cudaEventDestroy(e->indexed);
   if (e->chunk_fork) cudaEventDestroy(e->chunk_fork);
   for (int c = 0; c < gagp_engine::kChunks; ++c) {
     if (e->chunk_stream[c]) cudaStreamDestroy(e->chunk_stream[c]);
@@ -1168,6 +1170,14 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   // the run-generator top-up overlaps everything up to the placement
   CUDA_TRY(cudaEventRecord(e->fork, e->stream));
   CUDA_TRY(cudaStreamWaitEvent(e->side, e->fork, 0));
+  // the round's member index (one member per distinct row), built beside
+  // the variation: the lowering probes it for the children their parents
+  // do not cover, so every range's lowering waits for it
+  {
+    Timed t(e, KN_INDEX, e->side);
+    gb::k_member_index<<<blocks_for(v.total_members, 8), 256, 0, e->side>>>(v.d_desc, v.d_member_off, v.n);
+  }
+  CUDA_TRY(cudaEventRecord(e->indexed, e->side));
   { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
   if (v.total_children >= gb::kClusterMinChildren) {
     // the placement levels follow from the draws alone: found here, beside
@@ -1180,12 +1190,6 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   // the history entry reads only what the placement later rewrites
   { Timed t(e, KN_RECORD, e->side); gb::k_record<<<v.n, 1024, 0, e->side>>>(v.d_desc, v.n, 1); }
   CUDA_TRY(cudaEventRecord(e->join, e->side));
-  // the round's member index (one member per distinct row), which the
-  // variation kernels probe for children their parents do not cover
-  {
-    Timed t(e, KN_INDEX);
-    gb::k_member_index<<<blocks_for(v.total_members, 8), 256, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
-  }
   // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
   // next child of the variation warps; range c's lists start at item lo
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));
@@ -1209,6 +1213,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
       gb::k_vary<<<blocks, warps * 32, vary_smem, st>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, counts + 2, lo,
                                                         hi, e->profiling ? 1 : 0);
     }
+    CUDA_TRY(cudaStreamWaitEvent(st, e->indexed, 0));
     {
       Timed t(e, KN_LOWER, st);
       gb::k_lower<<<blocks_for(hi - lo, gb::kLowerWarps), gb::kLowerWarps * 32, 0, st>>>(

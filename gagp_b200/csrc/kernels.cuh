@@ -90,6 +90,20 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
       if (!s.c_eval[slot]) continue;
       const int32_t l = s.clen[slot];
       t = LRow{s.cnode + size_t(slot) * s.stride, s.ccval + size_t(slot) * s.stride, len_nodes(l), len_consts(l)};
+      // a child its parent does not cover reuses an identical current
+      // member's result when there is one (make_batch's member_hashes
+      // lookup, phase_population_cpu.cpp:336-339) and is neither lowered
+      // nor evaluated
+      if (s.mtab) {
+        const int m = warp_find_member(s, SRow{const_cast<uint64_t*>(t.node), const_cast<int64_t*>(t.cval), t.n, t.nc});
+        if (m >= 0) {
+          if (lane == 0) {
+            s.c_reuse[slot] = m;
+            s.c_eval[slot] = 0;
+          }
+          continue;
+        }
+      }
     }
     int temps = 0;
     const int len = lower_accumulator_warp(s, t.node, t.n, t.cval, t.nc, s.code + size_t(slot) * s.code_stride,

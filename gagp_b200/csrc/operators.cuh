@@ -129,8 +129,8 @@ __device__ inline int warp_find_member(const SearchDesc& s, const SRow& row) {
 }
 
 // One child, by one warp.  Writes the child row, its parent and reuse
-// source (the parent when the genotype is unchanged, else an identical
-// current member) and returns the
+// source (the parent when the genotype is unchanged; k_lower looks for an
+// identical current member otherwise) and returns the
 // reference's OperatorStats error code (0: none).  stamp[0..2]: SM clock
 // after selection, after crossover, after the mutation's subtree generation
 // (left 0 for phases not reached); stamp[4]: the generation's steps + 1 on
@@ -229,7 +229,6 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
     equal = __all_sync(kFull, mine);
   }
   if (equal) *reuse_out = parent;
-  else if (s.mtab) *reuse_out = warp_find_member(s, w.child);
   // ---- publish the child row
   for (int i = lane; i < w.child.n; i += 32) s.cnode[size_t(child) * s.stride + i] = w.child.node[i];
   for (int i = lane; i < w.child.nc; i += 32) s.ccval[size_t(child) * s.stride + i] = w.child.cval[i];
