@@ -61,13 +61,13 @@ SEARCH_WORKLOADS = {
     "poly4": dict(population=16384, generations=128, cases=256, max_nodes=64,
                   make=lambda seed: W.poly4(population=16384, generations=128, seed=seed, cases=256, max_nodes=64),
                   label="poly4 scalar regression (large): P=16384, G=128, C=256, max_nodes=64, seed=%d",
-                  cpu_generations=4, profile="poly4_p16384"),
+                  cpu_generations=4, gpu_generations=8, profile="poly4_p16384"),
     "list": dict(population=8192, generations=96, cases=200, max_nodes=48,
                  make=lambda seed: W.list_threshold(population=8192, generations=96, seed=seed, cases=200,
                                                     target="threshold_sum"),
                  label="list programs (threshold sum over IntLists of 0..50 elements, traversal grammar): "
                        "P=8192, G=96, C=200, max_nodes=48, seed=%d",
-                 cpu_generations=1, profile="list_p8192"),
+                 cpu_generations=1, gpu_generations=2, profile="list_p8192"),
 }
 WORKLOAD = SEARCH_WORKLOADS["poly4"]
 
@@ -239,6 +239,93 @@ def host_memory_bytes() -> int:
 # resident memory of one reference CPU-engine process on each workload (its
 # fixed 1024-node rows: about 4.2 GB at population 16384, 2.2 GB at 8192)
 REFERENCE_PROCESS_BYTES = {"poly4": 5 << 30, "list": 3 << 30}
+
+
+REF_GPU = os.path.join(ROOT, "oracle", "_ref", "gpu", "gagp")
+
+
+def reference_gpu_search(directory: str, generations=None, timeout: float = 600.0) -> dict:
+    """One search of the task in `directory` by the reference's own CUDA
+    engine (`gagp run --engine gpu`, the plain one-search-per-launch path),
+    timed by the reference's own clock: time_ms.total is the whole
+    evolve_population call (initial population, its evaluation and every
+    generation), time_ms.search the part after the initial population."""
+    out = os.path.join(directory, "ref_gpu_out")
+    cmd = [REF_GPU, "run", os.path.join(directory, "task.json"), "--engine", "gpu", "--search",
+           os.path.join(directory, "search.json"), "--out", out, "--quiet"]
+    if generations:
+        cmd += ["--generations", str(generations)]
+    subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
+    with open(os.path.join(out, "result.json")) as f:
+        r = json.load(f)
+    return {"total_s": r["time_ms"]["total"] / 1000.0, "search_s": r["time_ms"]["search"] / 1000.0,
+            "init_s": r["time_ms"]["initialization"] / 1000.0, "best_fitness": r["best"]["fitness"],
+            "declined": r.get("resident_declined", "")}
+
+
+def run_reference_gpu_arm(args, rank: int, world: int):
+    """--impl reference --reference-engine gpu: the reference's own CUDA engine
+    (plain path: one search per process, a host round trip per round) on the
+    same single-search task, one search per step over a bounded window of
+    generations.  The program-case count of that window is the reference CPU
+    engine's for the identical search (same task, seed and generations),
+    counted once outside the timed region."""
+    if rank != 0:
+        return
+    if not os.path.exists(REF_GPU):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/gpu/gagp was not built (make -C oracle ref-gpu)"}))
+        return
+    seed, gens = 0, WORKLOAD["gpu_generations"]
+    with tempfile.TemporaryDirectory() as d:
+        make_task(seed, d)
+        cases = reference_sample(os.path.join(d, "task.json"), os.path.join(d, "search.json"), gens)["program_cases"]
+        for _ in range(args.warmup):
+            reference_gpu_search(d, gens)
+        runs = [reference_gpu_search(d, gens) for _ in range(args.steps)]
+    secs = sum(r["total_s"] for r in runs)
+    value = cases * len(runs) / secs
+    line = {"impl": "reference", "engine": "reference CUDA engine (gagp run --engine gpu, sm_100a build)",
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * secs / len(runs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": dict(config_block(1, seed), generation_window="initial + %d of %d" % (gens, WORKLOAD["generations"])),
+            "program_cases_per_step": cases, "best_fitness": runs[0]["best_fitness"],
+            "declined": runs[0]["declined"],
+            "search_s": [r["search_s"] for r in runs], "total_s": [r["total_s"] for r in runs]}
+    print(json.dumps(line))
+
+
+def run_reference_batch_arm(args, rank: int, world: int, serving: bool = False):
+    """--impl reference --workload batch|serve: the reference's plain GPU path
+    on the mix, each search alone (one `gagp run --engine gpu` process after
+    another), as far as a time budget allows; searches/s from the
+    reference's own clock."""
+    if rank != 0:
+        return
+    if not os.path.exists(REF_GPU):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/gpu/gagp was not built (make -C oracle ref-gpu)"}))
+        return
+    mix = W.serving_mix(args.requests, seed=0) if serving else W.batch_mix(64)
+    budget = args.reference_budget
+    done, total_s, search_s, started = [], 0.0, 0.0, time.perf_counter()
+    for m in mix:
+        if time.perf_counter() - started > budget:
+            break
+        with tempfile.TemporaryDirectory() as d:
+            W.mix_files(m).write(d)
+            r = reference_gpu_search(d)
+        done.append({"index": m["index"], "kind": m["kind"], "population": m["population"], "cases": m["cases"],
+                     "generations": m["generations"], "total_s": r["total_s"], "declined": r["declined"]})
+        total_s += r["total_s"]
+        search_s += r["search_s"]
+    line = {"impl": "reference", "engine": "reference CUDA engine (gagp run --engine gpu, sm_100a build), each search alone",
+            "metric": "searches/s", "value": len(done) / total_s, "unit": "searches/s", "n_gpus": 1,
+            "steps": len(done), "warmup": 0, "ms_per_step": 1000.0 * total_s / len(done), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": ("serving" if serving else "batching") + " mix, the first %d searches in mix order "
+                                   "within a %.0f s budget" % (len(done), budget)},
+            "searches": done, "kinds": {k: sum(1 for x in done if x["kind"] == k) for k in ("scalar", "list")}}
+    print(json.dumps(line))
 
 
 def run_reference_arm(args, rank: int, world: int):
@@ -681,6 +768,10 @@ def main():
                          "batch: 64-search batching mix; serve: open-loop serving stream")
     ap.add_argument("--requests", type=int, default=500, help="serve: requests in the mix")
     ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--reference-engine", default="cpu", choices=["cpu", "gpu"],
+                    help="--impl reference on poly4/list: the reference CPU engine (default) or its CUDA engine")
+    ap.add_argument("--reference-budget", type=float, default=240.0,
+                    help="--impl reference on batch/serve: seconds of reference searches to run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global WORKLOAD
@@ -698,12 +789,12 @@ def main():
         run_serve_workload(args, rank, world)
         return
     if args.impl == "reference":
-        if args.workload not in SEARCH_WORKLOADS:
-            if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable": "the reference arm runs the single-search "
-                                  "workloads (poly4, list); the batch and serve mixes compare against the plain path"}))
-            return
-        run_reference_arm(args, rank, world)
+        if args.workload in ("batch", "serve"):
+            run_reference_batch_arm(args, rank, world, serving=args.workload == "serve")
+        elif args.reference_engine == "gpu":
+            run_reference_gpu_arm(args, rank, world)
+        else:
+            run_reference_arm(args, rank, world)
     else:
         run_own_arm(args, rank, world, local)
 

@@ -579,7 +579,7 @@ struct Plan {
       gen_nt, local_types, regions, inputs, expected, lists;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
-  size_t mtab, mhash;
+  size_t mtab;
   int mtab_slots = 0;
   size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts;
   size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, child_level, level_plan, round,
@@ -632,7 +632,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.c_key = L.take(8 * size_t(B)); p.c_eval = L.take(4 * size_t(B));
   p.mtab_slots = 2;
   while (p.mtab_slots < 2 * P) p.mtab_slots *= 2;
-  p.mtab = L.take(4 * size_t(p.mtab_slots)); p.mhash = L.take(8 * size_t(P));
+  p.mtab = L.take(8 * size_t(p.mtab_slots));
   const size_t slots = size_t(p.slots);
   p.code = L.take(8 * slots * p.code_stride); p.code_len = L.take(4 * slots);
   p.kpool = L.take(8 * slots * S); p.code_temps = L.take(4 * slots); p.vm_acc = L.take(16 * slots);
@@ -671,14 +671,19 @@ gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_e
   CUDA_TRY(cudaSetDevice(device));
   auto e = std::make_unique<gagp_engine>();
   e->device = device;
+  // the variation ranges take the SMs first; the side stream's run
+  // generator, placement levels, history entry and member index, needed
+  // later in the round, fill what is left
+  int least = 0, greatest = 0;
+  CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-  CUDA_TRY(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, least));
   CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->indexed, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->chunk_fork, cudaEventDisableTiming));
   for (int c = 0; c < gagp_engine::kChunks; ++c) {
-    CUDA_TRY(cudaStreamCreateWithFlags(&e->chunk_stream[c], cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithPriority(&e->chunk_stream[c], cudaStreamNonBlocking, greatest));
     CUDA_TRY(cudaEventCreateWithFlags(&e->chunk_done[c], cudaEventDisableTiming));
   }
   cudaDeviceProp prop;
@@ -769,7 +774,6 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   s->bytes = p.L.total;
   CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->block), s->bytes, e->pool, e->stream));
   CUDA_TRY(cudaMemsetAsync(s->block, 0, s->bytes, e->stream));
-  CUDA_TRY(cudaMemsetAsync(s->block + p.mtab, 0xff, 4 * size_t(p.mtab_slots), e->stream));  // an empty member index
   char* b = s->block;
   const int E = g->expression_count;
   // derived per-expression facts
@@ -909,7 +913,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.c_parent = at<int32_t>(b, p.c_parent); d.c_reuse = at<int32_t>(b, p.c_reuse); d.c_error = at<int32_t>(b, p.c_error);
   d.c_fitness = at<double>(b, p.c_fitness); d.c_wrong = at<uint32_t>(b, p.c_wrong);
   d.c_nodes = at<uint32_t>(b, p.c_nodes); d.c_key = at<uint64_t>(b, p.c_key); d.c_eval = at<int32_t>(b, p.c_eval);
-  d.mtab = at<int32_t>(b, p.mtab); d.mhash = at<uint64_t>(b, p.mhash); d.mtab_mask = p.mtab_slots - 1;
+  d.mtab = at<unsigned long long>(b, p.mtab); d.mtab_mask = p.mtab_slots - 1;
   d.code = at<uint2>(b, p.code); d.code_len = at<int32_t>(b, p.code_len); d.kpool = at<int64_t>(b, p.kpool);
   d.code_stride = p.code_stride; d.code_temps = at<int32_t>(b, p.code_temps);
   d.vm_acc = at<unsigned long long>(b, p.vm_acc);

@@ -512,10 +512,11 @@ __global__ void __launch_bounds__(1024) k_record(const SearchDesc* descs, int n,
 // per member hashes its row and inserts it by linear probing unless an
 // identical row is indexed already, so every distinct row has one entry and
 // the probe runs stay short however many copies the population holds.  A
-// warp that loses a slot to another reads the winner's hash after a fence
-// (the winner stored it before its fence and insertion) and compares the
-// rows.  At most P entries in at least 2P slots: every probe sequence meets
-// an empty slot.  k_commit clears the table for the next round.
+// slot word carries the hash's top bits with the member, so a warp that
+// loses a slot to another compares tags and then rows (stable in memory
+// all round) without waiting for any other write.  At most P entries in at
+// least 2P slots: every probe sequence meets an empty slot.  k_commit clears
+// the table for the next round.
 __global__ void __launch_bounds__(256) k_member_index(const SearchDesc* descs, const int32_t* off, int n) {
   const int item = int((size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (item >= off[n]) return;
@@ -527,21 +528,18 @@ __global__ void __launch_bounds__(256) k_member_index(const SearchDesc* descs, c
   const uint64_t* node = s.node + size_t(m) * s.stride;
   const int64_t* cval = s.cval + size_t(m) * s.stride;
   const uint64_t h = warp_row_hash(node, cval, len_nodes(l), len_consts(l));
-  if (lane == 0) s.mhash[m] = h;
-  __threadfence();
-  __syncwarp();
+  const unsigned long long mine = index_word(h, m);
   const uint32_t mask = uint32_t(s.mtab_mask);
   uint32_t slot = uint32_t(h) & mask;
   for (uint32_t probe = 0; probe <= mask; ++probe) {
-    int cur = -1;
-    if (lane == 0) cur = atomicCAS(&s.mtab[slot], -1, m);
+    unsigned long long cur = 0;
+    if (lane == 0) cur = atomicCAS(&s.mtab[slot], 0ULL, mine);
     cur = __shfl_sync(kFull, cur, 0);
-    if (cur < 0) return;  // indexed
-    __threadfence();
-    const uint64_t hc = *reinterpret_cast<const volatile uint64_t*>(&s.mhash[cur]);
-    if (hc == h) {
-      const int32_t lc = s.len[cur];
-      if (warp_rows_equal(s.node + size_t(cur) * s.stride, s.cval + size_t(cur) * s.stride, len_nodes(lc),
+    if (!cur) return;  // indexed
+    if (index_tag_matches(cur, h)) {
+      const int other = index_member(cur);
+      const int32_t lc = s.len[other];
+      if (warp_rows_equal(s.node + size_t(other) * s.stride, s.cval + size_t(other) * s.stride, len_nodes(lc),
                           len_consts(lc), node, cval, len_nodes(l), len_consts(l)))
         return;  // an identical row is indexed already
     }
@@ -1531,7 +1529,7 @@ __global__ void k_commit(const SearchDesc* descs, const int32_t* off, int n) {
   // this round's member index is spent: its slots start the next round empty
   if (s.mtab) {
     const int e = m * kCommitLanes + lane;
-    if (e <= s.mtab_mask) s.mtab[e] = -1;
+    if (e <= s.mtab_mask) s.mtab[e] = 0;
   }
   const int b = s.placed[m];
   if (b < 0) return;

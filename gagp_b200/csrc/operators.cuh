@@ -105,6 +105,14 @@ __device__ inline bool warp_rows_equal(const uint64_t* an, const int64_t* ac, in
   return __all_sync(kFull, same);
 }
 
+// Member index slot words: the row hash's top 44 bits and member + 1
+// (members below 2^20; 0 marks an empty slot).
+__device__ __forceinline__ unsigned long long index_word(uint64_t h, int m) {
+  return ((h >> 20) << 20) | (unsigned long long)(m + 1);
+}
+__device__ __forceinline__ int index_member(unsigned long long w) { return int(w & 0xfffffu) - 1; }
+__device__ __forceinline__ bool index_tag_matches(unsigned long long w, uint64_t h) { return (w >> 20) == (h >> 20); }
+
 // A current member identical to `row` (the member_hashes lookup of
 // HostPhasePopulation::make_batch, phase_population_cpu.cpp:336-339): the
 // round's member index holds one member per distinct row, probed linearly
@@ -115,9 +123,10 @@ __device__ inline int warp_find_member(const SearchDesc& s, const SRow& row) {
   const uint32_t mask = uint32_t(s.mtab_mask);
   uint32_t slot = uint32_t(h) & mask;
   for (uint32_t probe = 0; probe <= mask; ++probe) {
-    const int m = s.mtab[slot];
-    if (m < 0) return -1;
-    if (s.mhash[m] == h) {
+    const unsigned long long w = s.mtab[slot];
+    if (!w) return -1;
+    if (index_tag_matches(w, h)) {
+      const int m = index_member(w);
       const int32_t l = s.len[m];
       if (warp_rows_equal(s.node + size_t(m) * s.stride, s.cval + size_t(m) * s.stride, len_nodes(l), len_consts(l),
                           row.node, row.cval, row.n, row.nc))

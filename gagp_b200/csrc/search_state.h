@@ -144,9 +144,9 @@ struct SearchDesc {
   double* c_fitness; uint32_t* c_wrong; uint32_t* c_nodes; uint64_t* c_key;
   int32_t* c_eval;                     // 1: evaluate this child
   // ---- member index of one round: open addressing over mtab_mask + 1
-  // slots (at least 2P) holding one member per distinct row (-1: empty),
-  // and each member's row hash
-  int32_t* mtab; uint64_t* mhash; int32_t mtab_mask;
+  // slots (at least 2P) holding one member per distinct row, each slot
+  // word the row hash's top 44 bits << 20 | member + 1 (0: empty)
+  unsigned long long* mtab; int32_t mtab_mask;
   // ---- lowered programs (children, or members during the initial evaluation)
   uint2* code; int32_t* code_len; int64_t* kpool;
   int32_t code_stride;                 // accumulator instructions per program slot
