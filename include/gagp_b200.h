@@ -191,13 +191,13 @@ typedef struct gagp_rows {
 /* Result of one search (history per generation-equivalent, final ranked
  * population), in caller-allocated arrays. */
 typedef struct gagp_search_result {
-  int32_t generations;              /* history entries written */
+  int32_t generations;              /* in: capacity of the history arrays; out: entries written */
   double* history_best_fitness;
   double* history_mean_fitness;
   int32_t* history_best_wrong;
   int32_t* history_best_nodes;
   gagp_rows history_best;           /* champion row per history entry */
-  int32_t population;
+  int32_t population;               /* capacity of the final arrays (the best `population` members) */
   double* final_fitness;            /* ranked: best first */
   int32_t* final_wrong;
   int32_t* final_nodes;

@@ -42,6 +42,7 @@ CASES = [
     ("polynomial_grammar_sites", "polynomial", dict(population=200, generations=20, seed=9),
      {"ranking": {"tie_break": "grammar_sites"}}),
     ("poly4_exact_metric", "poly4", dict(population=256, generations=6, seed=7, cases=64), {}),
+    ("int64_edges", "int64_edges", dict(population=256, generations=8, seed=8), {}),
 ]
 
 
@@ -75,7 +76,35 @@ LOWER_CASES = [
     ("lower_list_reverse", "list", dict(population=256, generations=1, seed=23, cases=24, target="max"), "reverse"),
     ("lower_poly4", "poly4", dict(population=256, generations=1, seed=24, cases=32), None),
     ("lower_list_deep", "list", dict(population=384, generations=1, seed=25, cases=40, target="max"), "deep"),
+    ("lower_int64_edges", "int64_edges", dict(population=512, generations=1, seed=26), None),
 ]
+
+
+# int64 edge values: the extremes, the 32-bit boundaries the fast VM's
+# division shortcut tests, and a pair whose squares do and do not wrap.  The
+# reference reads case integers through a double (cpp/src/cli/codec.cpp:70-78),
+# so every value here is one a double holds exactly: INT64_MIN, INT64_MIN +
+# 2048 and INT64_MAX - 2047 (2^63 - 2048) are the extremes it accepts.
+INT64_EDGE_X = [-2 ** 63, -2 ** 63 + 2048, 2 ** 63 - 2048, -2 ** 62, 2 ** 62, 2 ** 62 + 4096, -2 ** 31 - 1, -2 ** 31,
+                2 ** 31 - 1, 2 ** 31, 3037000499, -3037000500, -1, 0, 1, 7, -7, 100, -100]
+
+
+def int64_edge_target(x: int) -> int:
+    """x*x - 3 where it is exact in a double, else x itself."""
+    return x * x - 3 if abs(x) < 2 ** 26 else x
+
+
+def int64_edge_task(population: int, generations: int, seed: int) -> "W.TaskFiles":
+    """The large scalar grammar plus Python-sign `mod` (ZeroDiv on 0) and
+    `neg`, on cases at int64 edge values, where programs wrap."""
+    g = W.poly4_grammar(max_nodes=40)
+    alts = g["nonterminals"][0]["alternatives"]
+    ref = {"ref": "Expr"}
+    alts.append({"id": "mod", "weight": 1, "expression": {"signature": "mod(Int,Int)->Int", "args": [ref, ref]}})
+    alts.append({"id": "neg", "weight": 1, "expression": {"signature": "neg(Int)->Int", "args": [ref]}})
+    train = [W._int_case(x, int64_edge_target(x)) for x in INT64_EDGE_X]
+    return W.TaskFiles(name="int64-edges-s%d" % seed, grammar=g, train=train,
+                       search=W.search_config(population, generations, seed))
 
 
 def nested_traversal_grammar() -> dict:
@@ -152,7 +181,12 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--list-only", action="store_true", help="regenerate golden/list/ only")
     ap.add_argument("--lower-only", action="store_true", help="regenerate golden/lower/ only")
+    ap.add_argument("--headline", action="store_true",
+                    help="regenerate golden/headline/ only (the benchmark's search, several minutes)")
     args = ap.parse_args()
+    if args.headline:
+        headline_fixture()
+        return
     if args.lower_only:
         lower_fixtures()
         return
@@ -160,7 +194,7 @@ def main() -> None:
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     here = os.path.dirname(os.path.abspath(__file__))
     for name, workload, kwargs, extra in ([] if args.list_only else CASES):
-        task = W.make(workload, **kwargs)
+        task = int64_edge_task(**kwargs) if workload == "int64_edges" else W.make(workload, **kwargs)
         task.search.update(extra)
         if name.endswith("exact_metric"):
             task.fitness = {"metric": "exact"}
@@ -219,11 +253,52 @@ def main() -> None:
     lower_fixtures()
 
 
+def row_digest(rows) -> str:
+    """SHA-256 over the ranked rows' construction expressions and constants."""
+    import hashlib
+    h = hashlib.sha256()
+    for r in rows:
+        h.update(json.dumps([r["origins"], [c[1] for c in r["constants"]]], separators=(",", ":")).encode())
+    return h.hexdigest()
+
+
+def headline_fixture() -> None:
+    """The benchmark's own search (large scalar regression: P = 16384, 128
+    generations, 256 cases, max 64 nodes, seed 0) run whole by the reference
+    CPU engine: the full history, the final ranked fitness, wrong and node
+    vectors, the best 256 rows and a digest of all 16384 ranked rows."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "headline"), exist_ok=True)
+    task = W.poly4(population=16384, generations=128, seed=0, cases=256, max_nodes=64)
+    with tempfile.TemporaryDirectory() as d:
+        task.write(d)
+        tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+        run = driver("run", tp, "--search", sp)
+    final = run["final"]
+    fixture = {"name": "poly4_p16384_g128_s0", "task": {"name": task.name, "fitness": task.fitness},
+               "grammar": task.grammar, "train": task.train, "test": task.test, "search": task.search,
+               "run": {"declined": run["declined"], "time_ms": run["time_ms"], "program_cases": run["program_cases"],
+                       "reused_programs": run["reused_programs"], "history": run["history"],
+                       "final_fitness": [m["fitness"] for m in final], "final_wrong": [m["wrong"] for m in final],
+                       "final_nodes": [m["nodes"] for m in final],
+                       "top": [dict(m, rows=m["rows"]) for m in final[:256]],
+                       "row_digest": row_digest([m["rows"][0] for m in final])}}
+    with gzip.open(os.path.join(here, "headline", "poly4_p16384_g128_s0.json.gz"), "wt") as f:
+        json.dump(fixture, f, separators=(",", ":"))
+    print("headline", len(run["history"]), "history entries,", len(final), "final members",
+          "%.1f s" % (run["time_ms"] / 1000.0))
+
+
 def lower_fixtures() -> None:
     here = os.path.dirname(os.path.abspath(__file__))
     os.makedirs(os.path.join(here, "lower"), exist_ok=True)
     for name, workload, kwargs, variant in LOWER_CASES:
-        task = W.list_threshold(**kwargs) if workload == "list" else W.make(workload, **kwargs)
+        if workload == "list":
+            task = W.list_threshold(**kwargs)
+        elif workload == "int64_edges":
+            task = int64_edge_task(**kwargs)
+        else:
+            task = W.make(workload, **kwargs)
         if variant:
             task.grammar = variant_grammar(variant)
         with tempfile.TemporaryDirectory() as d:
