@@ -428,6 +428,19 @@ def roofline_entry(stats: dict, delta: dict, steps: int, peak: dict) -> dict:
             "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak["source"]}
 
 
+def round_timeline(spans):
+    """The launches of the last profiled round (each round opens with its
+    member index build), as [kernel, start ms, end ms] after the round's
+    first launch started, and the round's span."""
+    starts = [i for i, (name, _, _) in enumerate(spans) if name == "k_member_index"]
+    if not starts:
+        return None
+    last = spans[starts[-1]:]
+    t0 = min(a for _, a, _ in last)
+    return {"span_ms": max(b for _, _, b in last) - t0,
+            "launches": [[name, round(a - t0, 4), round(b - t0, 4)] for name, a, b in last]}
+
+
 def vm_issue_summary(workload: str):
     """Integer-issue figures of the VM kernels from the committed ncu summary
     (profiles/vm_issue_<workload>.txt): per kernel, warp instructions issued
@@ -537,6 +550,7 @@ def run_own_arm(args, rank: int, world: int, local: int):
             eng.profile(True)
             eng.advance([s], PROFILE_ROUNDS, flush_l2=True)
             stats = eng.kernel_stats()
+            timeline = round_timeline(eng.timeline())
             eng.profile(False)
             profiled = eng.counters(s)
             s.close()
@@ -559,6 +573,7 @@ def run_own_arm(args, rank: int, world: int, local: int):
             "kernels": {k: {"ms_per_step": v["ms"] / PROFILE_ROUNDS, "launches_per_step": v["launches"] / PROFILE_ROUNDS}
                         for k, v in stats.items()},
             "kernel_timing": "CUDA events per launch over %d profiled rounds right after the timed region" % PROFILE_ROUNDS,
+            "round_timeline": timeline,
             "roofline": roofline_entry(stats, pdelta, PROFILE_ROUNDS, peaks()), "clocks": clock_summary,
             "counters": {"program_cases": cases, "evaluated_programs": after["evaluated_programs"] - before["evaluated_programs"],
                          "reused_programs": after["reused_programs"] - before["reused_programs"],

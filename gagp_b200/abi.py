@@ -91,6 +91,19 @@ class Rows(C.Structure):
                 ("constants", C.POINTER(C.c_int64))]
 
 
+class Verdict(C.Structure):
+    """``gagp_verdict``: one program's judgement on a case set."""
+    _fields_ = [("cases", C.c_int32), ("correct", C.c_int32), ("runtime_errors", C.c_int32), ("reserved", C.c_int32),
+                ("loss", C.c_double)]
+
+    def summary(self) -> dict:
+        """The reference's judge object (cpp/src/cli/run.cpp:232-237)."""
+        n = float(self.cases)
+        return {"cases": n, "correct": float(self.correct), "wrong": n - self.correct,
+                "runtime_errors": float(self.runtime_errors), "mean_loss": self.loss / n,
+                "solved": self.correct == self.cases}
+
+
 class SearchResult(C.Structure):
     _fields_ = [("generations", C.c_int32), ("history_best_fitness", C.POINTER(C.c_double)),
                 ("history_mean_fitness", C.POINTER(C.c_double)), ("history_best_wrong", C.POINTER(C.c_int32)),

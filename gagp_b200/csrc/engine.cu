@@ -102,6 +102,10 @@ struct gagp_engine {
   size_t event_next = 0;
   struct Pending { int kernel; cudaEvent_t start, stop; };
   std::vector<Pending> pending;
+  // the launches of the last harvested batch of rounds: kernel, start and
+  // end (ms after the batch's first timed launch started)
+  struct Span { int kernel; float start, end; };
+  std::vector<Span> timeline;
   double kernel_ms[16] = {};
   long long kernel_launches[16] = {};
   void* flush_buffer = nullptr;
@@ -183,11 +187,14 @@ constexpr int kVmLanes[3] = {1, 2, 4};
 constexpr int kTuneRounds = 2;
 
 void harvest(gagp_engine* e) {
+  if (!e->pending.empty()) e->timeline.clear();
   for (const auto& p : e->pending) {
-    float ms = 0;
+    float ms = 0, at = 0;
     if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
       e->kernel_ms[p.kernel] += ms;
       e->kernel_launches[p.kernel] += 1;
+      if (cudaEventElapsedTime(&at, e->pending[0].start, p.start) == cudaSuccess)
+        e->timeline.push_back({p.kernel, at, at + ms});
     }
   }
   e->pending.clear();
@@ -343,16 +350,22 @@ gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
 // the reference).  Returns GAGP_OK or GAGP_DECLINED with a reason.
 gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg) {
   if (!g || !c || !cfg) return fail(GAGP_INVALID_ARGUMENT, "null argument");
-  if (!cfg->steady_state) return fail(GAGP_DECLINED, "the device-resident loop runs the steady-state schedule");
   if (cfg->population < 1 || cfg->population > 16384) return fail(GAGP_DECLINED, "population/grammar capacity");
-  // with one member every replacement draw is the best member, which the
-  // steady-state loop redraws without end (evolve.cpp:331-441)
-  if (cfg->steady_state && cfg->population < 2)
-    return fail(GAGP_INVALID_ARGUMENT, "steady-state replacement needs at least 2 members");
-  const int B = cfg->batch > 0 ? cfg->batch : cfg->population;
-  if (B > cfg->population || cfg->population % B) return fail(GAGP_INVALID_ARGUMENT, "steady-state batch must divide the population");
+  if (cfg->steady_state) {
+    // with one member every replacement draw is the best member, which the
+    // steady-state loop redraws without end (evolve.cpp:331-441)
+    if (cfg->population < 2) return fail(GAGP_INVALID_ARGUMENT, "steady-state replacement needs at least 2 members");
+    const int B = cfg->batch > 0 ? cfg->batch : cfg->population;
+    if (B > cfg->population || cfg->population % B)
+      return fail(GAGP_INVALID_ARGUMENT, "steady-state batch must divide the population");
+    if (cfg->replacement_size < 1 || cfg->replacement_size > 64) return fail(GAGP_INVALID_ARGUMENT, "replacement_size");
+  } else {
+    // reproduce's elite contract (phase_population_cpu.cpp:271)
+    if (cfg->elite_count < 0 || cfg->elite_count >= cfg->population)
+      return fail(GAGP_INVALID_ARGUMENT, "elite count must be in [0, population)");
+    if (cfg->elite_count > gb::kMaxElites) return fail(GAGP_DECLINED, "more elites than the device keeps");
+  }
   if (cfg->generations < 1) return fail(GAGP_INVALID_ARGUMENT, "generations must be > 0");
-  if (cfg->replacement_size < 1 || cfg->replacement_size > 64) return fail(GAGP_INVALID_ARGUMENT, "replacement_size");
   if (cfg->tournament_size < 1 || cfg->crossover_attempts < 1 || cfg->crossover_attempts > 64)
     return fail(GAGP_INVALID_ARGUMENT, "selection/crossover contract");
   if (!(cfg->mutation_probability >= 0 && cfg->mutation_probability <= 1) ||
@@ -582,16 +595,24 @@ struct Plan {
   size_t mtab;
   int mtab_slots = 0;
   size_t code, code_len, kpool, code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts;
-  size_t mt, stream, stream_mod, stream_head, round_seed, best, placed, place_state, child_level, level_plan, round,
+  size_t mt, stream, stream_mod, stream_head, round_seed, best, elites, placed, place_state, child_level, level_plan,
+      round,
       hist_sum, hist_fitness,
       hist_wrong,
       hist_nodes, hist_node, hist_cval, hist_len, counters;
   int stride, code_stride, bc_stride, stream_capacity, slots;
 };
 
+// Children per round: the steady-state batch, or the whole population under
+// the generational schedule.
+int children_per_round(const gagp_search_config* cfg) {
+  if (!cfg->steady_state) return cfg->population;
+  return cfg->batch > 0 ? cfg->batch : cfg->population;
+}
+
 Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_config* cfg) {
   Plan p{};
-  const int P = cfg->population, B = cfg->batch > 0 ? cfg->batch : P, C = c->case_count;
+  const int P = cfg->population, B = children_per_round(cfg), C = c->case_count;
   const int maxv = g->max_nodes - g->fixed_nodes;
   p.stride = int(align_up(size_t(maxv), 4));
   p.code_stride = 2 * maxv + 8;
@@ -641,6 +662,7 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
   p.mt = L.take(8 * 312); p.stream = L.take(8 * size_t(p.stream_capacity));
   p.stream_mod = L.take(4 * size_t(p.stream_capacity)); p.stream_head = L.take(16);
   p.round_seed = L.take(8); p.best = L.take(4); p.placed = L.take(4 * size_t(P)); p.round = L.take(16);
+  p.elites = L.take(4 * size_t(gb::kMaxElites));
   p.place_state = L.take(4);
   p.child_level = L.take(2 * size_t(B)); p.level_plan = L.take(8);
   const size_t H = size_t(cfg->generations);
@@ -763,7 +785,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
     return fail(GAGP_OUT_OF_MEMORY, "search does not fit the engine's device-memory budget");
   auto s = std::make_unique<Search>();
   s->P = cfg->population;
-  s->B = cfg->batch > 0 ? cfg->batch : cfg->population;
+  s->B = children_per_round(cfg);
   s->G = cfg->generations;
   s->total_rounds = int((long long)s->P * s->G / s->B);
   s->maxv = g->max_nodes - g->fixed_nodes;
@@ -902,6 +924,8 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.penalty = cfg->penalty; d.penalty_int = (int64_t)std::fabs(cfg->penalty);
   d.seed = cfg->seed;
   d.rounds_per_epoch = s->P / s->B;
+  d.generational = !cfg->steady_state;
+  d.elite_count = cfg->steady_state ? 0 : cfg->elite_count;
   d.generations = s->G;
   d.inputs = at<int64_t>(b, p.inputs); d.expected = at<int64_t>(b, p.expected);
   d.lists = at<int64_t>(b, p.lists); d.n_lists = n_lists;
@@ -926,6 +950,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.bounded_threshold = (0 - uint64_t(s->P)) % uint64_t(s->P);
   d.round_seed = at<uint64_t>(b, p.round_seed);
   d.best = at<int32_t>(b, p.best); d.placed = at<int32_t>(b, p.placed); d.round = at<int32_t>(b, p.round);
+  d.elites = at<int32_t>(b, p.elites);
   d.place_state = at<int32_t>(b, p.place_state);
   d.child_level = at<int16_t>(b, p.child_level); d.level_plan = at<int32_t>(b, p.level_plan);
   d.hist_sum = at<int64_t>(b, p.hist_sum); d.hist_fitness = at<double>(b, p.hist_fitness);
@@ -986,11 +1011,16 @@ struct BatchView {
   int max_C = 1, max_inputs = 0;
   int min_B = 1 << 30;               // the smallest round of the batch
   bool exact_heavy = false;          // some search's programs mostly need the exact VM
+  bool generational = false;         // the batch's schedule (one per batch)
 };
 
 gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
   const int n = int(list.size());
   v->n = n;
+  v->generational = n > 0 && list[0]->desc.generational;
+  for (Search* s : list)
+    if (bool(s->desc.generational) != v->generational)
+      return fail(GAGP_INVALID_ARGUMENT, "a batch holds searches of one schedule (steady-state or generational)");
   if (n == 1) {
     v->d_desc = list[0]->d_desc;
     v->d_member_off = list[0]->d_off;
@@ -1182,8 +1212,9 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     gb::k_member_index<<<blocks_for(v.total_members, 8), 256, 0, e->side>>>(v.d_desc, v.d_member_off, v.n);
   }
   CUDA_TRY(cudaEventRecord(e->indexed, e->side));
-  { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
-  if (v.total_children >= gb::kClusterMinChildren) {
+  // the generational round draws one run-generator output (k_gen_finish)
+  if (!v.generational) { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
+  if (v.total_children >= gb::kClusterMinChildren && !v.generational) {
     // the placement levels follow from the draws alone: found here, beside
     // the variation, so the placement itself only compares and writes keys
     Timed t(e, KN_LEVELS, e->side);
@@ -1228,6 +1259,27 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
       CUDA_TRY(cudaEventRecord(e->chunk_done[c], st));
       CUDA_TRY(cudaStreamWaitEvent(e->stream, e->chunk_done[c], 0));
     }
+  }
+  if (v.generational) {
+    // every child becomes the member of its index (reproduce's swap), after
+    // the reused children have read their sources' results and the history
+    // entry has read the members
+    {
+      Timed t(e, KN_CHILD);
+      gb::k_child_results<<<blocks_for(v.total_children, 128), 128, 0, e->stream>>>(v.d_desc, v.d_child_off, v.n);
+    }
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join, 0));
+    {
+      Timed t(e, KN_PLACE);
+      gb::k_gen_place<<<blocks_for(v.total_members, 256), 256, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n);
+    }
+    {
+      Timed t(e, KN_COMMIT);
+      gb::k_commit<<<blocks_for(size_t(v.total_members) * gb::kCommitLanes, 256), 256, 0, e->stream>>>(
+          v.d_desc, v.d_member_off, v.n);
+    }
+    { Timed t(e, KN_STREAM); gb::k_gen_finish<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n); }
+    return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
   }
   // rounds of kClusterMinChildren or more children get their results from
   // the cluster placement itself
@@ -1364,7 +1416,8 @@ namespace {
 struct EvalPlan {
   Layout L;
   size_t desc, ex, info, minimum, local_types, regions, inputs, expected, lists, node, cval, len, code, code_len, kpool,
-      code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts, fitness, wrong, counters, round, fast, general, counts, off;
+      code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts, fitness, wrong, errors, counters, round, fast, general,
+      counts, off;
   int stride, code_stride, bc_stride;
 };
 
@@ -1391,7 +1444,8 @@ EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   p.code_temps = L.take(4 * R); p.vm_acc = L.take(16 * R);
   p.bc = L.take(20 * R * p.bc_stride); p.bc_len = L.take(4 * R); p.bc_locals = L.take(4 * R);
   p.bc_consts = L.take(8 * R * p.bc_stride);
-  p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.counters = L.take(8 * GAGP_COUNTERS); p.round = L.take(16);
+  p.fitness = L.take(8 * R); p.wrong = L.take(4 * R); p.errors = L.take(4 * R);
+  p.counters = L.take(8 * GAGP_COUNTERS); p.round = L.take(16);
   p.fast = L.take(sizeof(gb::ProgramRef) * R); p.general = L.take(sizeof(gb::ProgramRef) * R);
   p.counts = L.take(16); p.off = L.take(8);
   return p;
@@ -1428,10 +1482,11 @@ gagp_status eval_check(const gagp_grammar* g, const gagp_cases* c, const gagp_se
 }
 
 // Fills `region` (device, plan.L.total bytes) and evaluates every row on
-// `stream`; results are copied to the host arrays.  No device allocation.
+// `stream`; results are copied to the host arrays (`wrong` and `errors`, the
+// cases that ended in a runtime error, may be null).  No device allocation.
 gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g, const gagp_cases* c,
                          const gagp_search_config* cfg, const gagp_rows* rows, double* fitness, uint32_t* wrong,
-                         cudaStream_t stream, int sm_count, size_t max_smem) {
+                         uint32_t* errors, cudaStream_t stream, int sm_count, size_t max_smem) {
   const int E = g->expression_count, C = c->case_count, NI = c->input_count, R = rows->count;
   if (R == 0) return GAGP_OK;
   char* b = region;
@@ -1519,6 +1574,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.bc_stride = p.bc_stride;
   d.fitness = at<double>(b, p.fitness);
   d.wrong = at<uint32_t>(b, p.wrong);
+  d.errors = at<uint32_t>(b, p.errors);
   d.counters = at<uint64_t>(b, p.counters);
   d.round = at<int32_t>(b, p.round);
   const int32_t off[2] = {0, R};
@@ -1566,6 +1622,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   CUDA_TRY(cudaMemcpyAsync(round, b + p.round, sizeof round, cudaMemcpyDeviceToHost, stream));
   CUDA_TRY(cudaMemcpyAsync(fitness, b + p.fitness, 8 * size_t(R), cudaMemcpyDeviceToHost, stream));
   if (wrong) CUDA_TRY(cudaMemcpyAsync(wrong, b + p.wrong, 4 * size_t(R), cudaMemcpyDeviceToHost, stream));
+  if (errors) CUDA_TRY(cudaMemcpyAsync(errors, b + p.errors, 4 * size_t(R), cudaMemcpyDeviceToHost, stream));
   CUDA_TRY(cudaStreamSynchronize(stream));
   if (round[3]) return fail(GAGP_DEVICE_ERROR, "row evaluation failed on the device (code " + std::to_string(round[3]) + ")");
   return GAGP_OK;
@@ -1798,6 +1855,20 @@ gagp_status gagp_b200_engine_kernel_stats(gagp_engine* e, int32_t kernel, const 
   return GAGP_OK;
 }
 
+gagp_status gagp_b200_engine_timeline(gagp_engine* e, int32_t capacity, int32_t* kernel, float* start_ms,
+                                      float* end_ms, int32_t* count) {
+  if (!e || !count || capacity < 0 || (capacity && (!kernel || !start_ms || !end_ms)))
+    return fail(GAGP_INVALID_ARGUMENT, "null argument or negative capacity");
+  *count = int32_t(e->timeline.size());
+  const int32_t n = std::min(capacity, *count);
+  for (int32_t i = 0; i < n; ++i) {
+    kernel[i] = e->timeline[i].kernel;
+    start_ms[i] = e->timeline[i].start;
+    end_ms[i] = e->timeline[i].end;
+  }
+  return GAGP_OK;
+}
+
 gagp_status gagp_b200_search_progress(gagp_engine* e, int32_t id, int32_t* rounds_done, int32_t* total_rounds,
                                       int32_t* finished) {
   if (!e) return fail(GAGP_INVALID_ARGUMENT, "null engine");
@@ -1825,9 +1896,46 @@ gagp_status gagp_b200_evaluate_rows(gagp_engine* e, const gagp_grammar* grammar,
   const EvalPlan p = plan_eval(grammar, cases, rows->count);
   char* region = nullptr;
   CUDA_TRY(cudaMalloc(&region, p.L.total));
-  st = eval_rows_in(region, p, grammar, cases, config, rows, fitness, wrong, e->stream, e->sm_count, e->max_smem);
+  st = eval_rows_in(region, p, grammar, cases, config, rows, fitness, wrong, nullptr, e->stream, e->sm_count,
+                    e->max_smem);
   cudaFree(region);
   return st;
+}
+
+gagp_status gagp_b200_judge_rows(gagp_engine* e, const gagp_grammar* grammar, const gagp_cases* cases,
+                                 const gagp_search_config* config, const gagp_rows* rows, gagp_verdict* out) {
+  if (!e || !out) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
+  gagp_status st = eval_check(grammar, cases, config, rows);
+  if (st != GAGP_OK) return st;
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int R = rows->count, C = cases->case_count;
+  std::vector<double> fitness(size_t(std::max(1, R)));
+  std::vector<uint32_t> wrong(size_t(std::max(1, R))), errors(size_t(std::max(1, R)));
+  const EvalPlan p = plan_eval(grammar, cases, R);
+  char* region = nullptr;
+  CUDA_TRY(cudaMalloc(&region, p.L.total));
+  st = eval_rows_in(region, p, grammar, cases, config, rows, fitness.data(), wrong.data(), errors.data(), e->stream,
+                    e->sm_count, e->max_smem);
+  cudaFree(region);
+  if (st != GAGP_OK) return st;
+  // run.cpp's judge_case from the fitness terms: a case is correct exactly
+  // when it is not wrong; an Int-expected case whose value is not an Int is
+  // an error as a runtime failure is; a correct case loses 0, so with Bool
+  // expectations under the absolute metric (whose case score is the ceiling
+  // whatever the value) the correct cases' ceilings come off the loss
+  const bool type_errors = cases->expected_tag == GAGP_TAG_INT && grammar->slot_type != GAGP_TAG_INT;
+  const int64_t cap = int64_t(std::fabs(config->penalty));
+  for (int r = 0; r < R; ++r) {
+    gagp_verdict& v = out[r];
+    v.cases = C;
+    v.correct = C - int32_t(wrong[r]);
+    v.runtime_errors = type_errors ? C : int32_t(errors[r]);
+    int64_t loss = int64_t(-fitness[r]);
+    if (config->metric == GAGP_METRIC_ABSOLUTE && cases->expected_tag != GAGP_TAG_INT) loss -= int64_t(v.correct) * cap;
+    v.loss = double(loss);
+  }
+  return GAGP_OK;
 }
 
 // Row evaluation for callers that may not allocate device memory: it runs the
@@ -1849,7 +1957,7 @@ gagp_status gagp_b200_evaluate_rows_static(const gagp_grammar* grammar, const ga
   CUDA_TRY(cudaGetDevice(&device));
   StaticDevice* d = nullptr;
   if ((st = static_scratch_on(device, &d)) != GAGP_OK) return st;
-  return eval_rows_in(d->scratch, p, grammar, cases, config, rows, fitness, wrong,
+  return eval_rows_in(d->scratch, p, grammar, cases, config, rows, fitness, wrong, nullptr,
                       static_cast<cudaStream_t>(stream), d->sm_count, d->max_smem);
 }
 
@@ -2098,6 +2206,7 @@ void gagp_b200_server_destroy(gagp_server* sv) {
 gagp_status gagp_b200_server_submit(gagp_server* sv, const gagp_grammar* g, const gagp_cases* c,
                                     const gagp_search_config* cfg, int64_t* ticket) {
   if (!sv || !g || !c || !cfg || !ticket) return fail(GAGP_INVALID_ARGUMENT, "null argument");
+  if (!cfg->steady_state) return fail(GAGP_DECLINED, "the server batches steady-state searches");
   gagp_status st = admit(g, c, cfg);
   if (st != GAGP_OK) return st;
   const Plan p = plan_search(g, c, cfg);

@@ -141,11 +141,13 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
   }
 }
 
-__device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int slot, int64_t loss, uint32_t wrong) {
+__device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int slot, int64_t loss, uint32_t wrong,
+                                             uint32_t errors) {
   const double f = -double(loss);
   if (mode == 0) {
     s.fitness[slot] = f;
     s.wrong[slot] = s.has_wrong ? wrong : 0;
+    if (s.errors) s.errors[slot] = errors;
   } else {
     s.c_fitness[slot] = f;
     s.c_wrong[slot] = s.has_wrong ? wrong : 0;
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
                                                                    int bc_stride_max) {
   extern __shared__ __align__(16) int64_t smem_general[];
   __shared__ int64_t red_loss[kGeneralWarps];
-  __shared__ uint32_t red_wrong[kGeneralWarps];
+  __shared__ uint32_t red_wrong[kGeneralWarps], red_errors[kGeneralWarps];
   __shared__ unsigned long long red_steps[kGeneralWarps];
   int64_t* consts = smem_general;
   uint2* words = reinterpret_cast<uint2*>(smem_general + bc_stride_max);
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
     simd_ok = __syncthreads_and(simd_ok);
     const VmView view = vm_view(s);
     int64_t loss = 0;
-    uint32_t wrong = 0;
+    uint32_t wrong = 0, errors = 0;
     uint64_t steps = 0;
     if (simd_ok) {
       for (int c0 = warp * 32; c0 < s.C; c0 += kGeneralWarps * 32) {
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
         const SimdCase r = run_program_simd(view, words, n, consts, n_locals, c, live, slots);
         if (live) {
           if (r.ok) loss += case_loss(s, s.slot_type, r.value, s.expected[c], wrong);
-          else { loss += error_loss(s); ++wrong; }
+          else { loss += error_loss(s); ++wrong; ++errors; }
         }
         steps += r.steps;
       }
@@ -229,20 +231,32 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
         } else {
           loss += error_loss(s);
           ++wrong;
+          ++errors;
         }
       }
     }
     loss = warp_sum(loss);
     wrong = warp_sum(wrong);
+    errors = warp_sum(errors);
     steps = warp_sum(steps);
-    if (lane == 0) { red_loss[warp] = loss; red_wrong[warp] = wrong; red_steps[warp] = steps; }
+    if (lane == 0) {
+      red_loss[warp] = loss;
+      red_wrong[warp] = wrong;
+      red_errors[warp] = errors;
+      red_steps[warp] = steps;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
       int64_t tl = 0;
-      uint32_t tw = 0;
+      uint32_t tw = 0, te = 0;
       unsigned long long ts = 0;
-      for (int w = 0; w < kGeneralWarps; ++w) { tl += red_loss[w]; tw += red_wrong[w]; ts += red_steps[w]; }
-      store_result(s, mode, p.slot, tl, tw);
+      for (int w = 0; w < kGeneralWarps; ++w) {
+        tl += red_loss[w];
+        tw += red_wrong[w];
+        te += red_errors[w];
+        ts += red_steps[w];
+      }
+      store_result(s, mode, p.slot, tl, tw, te);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[24]), ts);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
       atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
@@ -319,7 +333,7 @@ __global__ void __launch_bounds__(256, K == 4 ? 2 : 4) k_vm_fast(const SearchDes
         }
       }
       if (last) {  // the last tile of the program
-        store_result(s, mode, p.slot, total, total_wrong);
+        store_result(s, mode, p.slot, total, total_wrong, 0);  // accumulator programs never fail
         // the program's instructions over all its cases, counted once
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[3]),
                   (unsigned long long)s.code_len[p.slot] * (unsigned long long)s.C);
@@ -430,6 +444,45 @@ __global__ void k_stream(const SearchDesc* descs, int n) {
   if (threadIdx.x == 0) stream_ptrs(s)[1] = wp;
 }
 
+// The `count` best members in ranking order (smallest (key, member) first),
+// written to out[0..count): pass j takes the smallest (key, member) above
+// pass j-1's.  For the generational schedule's elites this is the order of
+// reproduce's stable sort by completed fitness (phase_population_cpu.cpp:
+// 283-288): rank values when wrong counts are kept, fitness with ties to the
+// lower index otherwise.  The whole block calls it; out[0] is the best.
+__device__ inline void block_best_members(const SearchDesc& s, int count, int32_t* out) {
+  __shared__ uint64_t top_key[32];
+  __shared__ int top_idx[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = (blockDim.x + 31) >> 5;
+  uint64_t prev_key = 0;
+  int prev_idx = -1;
+  for (int j = 0; j < count; ++j) {
+    uint64_t bk = ~0ULL;
+    int bi = 0x7fffffff;
+    for (int m = threadIdx.x; m < s.P; m += blockDim.x) {
+      const uint64_t k = s.key[m];
+      const bool above = k > prev_key || (k == prev_key && m > prev_idx);
+      if (above && (k < bk || (k == bk && m < bi))) { bk = k; bi = m; }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const uint64_t k2 = __shfl_xor_sync(kFull, bk, o);
+      const int i2 = __shfl_xor_sync(kFull, bi, o);
+      if (k2 < bk || (k2 == bk && i2 < bi)) { bk = k2; bi = i2; }
+    }
+    if (lane == 0) { top_key[warp] = bk; top_idx[warp] = bi; }
+    __syncthreads();
+    bk = top_key[0];
+    bi = top_idx[0];
+    for (int w = 1; w < warps; ++w)
+      if (top_key[w] < bk || (top_key[w] == bk && top_idx[w] < bi)) { bk = top_key[w]; bi = top_idx[w]; }
+    __syncthreads();
+    if (threadIdx.x == 0) out[j] = bi;
+    prev_key = bk;
+    prev_idx = bi;
+  }
+}
+
 // Seeds the generator, tops up the stream, finds the best member and draws
 // the first round's variation seed.  One block per search.
 __global__ void k_start(const SearchDesc* descs, int n) {
@@ -468,6 +521,7 @@ __global__ void k_start(const SearchDesc* descs, int n) {
     s.round[2] = s.total_rounds == 0;
   }
   for (int i = threadIdx.x; i < 312; i += blockDim.x) s.mt[i] = mt[i];
+  if (s.generational && s.elite_count > 0) block_best_members(s, s.elite_count, s.elites);
 }
 
 // ----------------------------------------------------------- one round
@@ -651,7 +705,13 @@ __device__ inline uint64_t child_result_of(const SearchDesc& s, int b, bool* reu
 __device__ inline void child_result(const SearchDesc& s, int b) {
   bool reused;
   child_result_of(s, b, &reused);
-  if (reused) atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[1]), 1ULL);
+  if (reused) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[1]), 1ULL);
+    // the generational evaluate copies a reused member's case counts too
+    // (HostPhasePopulation::evaluate, phase_population_cpu.cpp:252-253), so
+    // its program-case total covers every member
+    if (s.generational) atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
+  }
 }
 
 // Results of all children before any placement, thread per child, for
@@ -662,7 +722,7 @@ __global__ void k_child_results(const SearchDesc* descs, const int32_t* off, int
   const int si = find_search(off, n, item);
   const SearchDesc& s = descs[si];
   if (!search_live(s)) return;
-  if (s.B >= kClusterMinChildren) return;  // the cluster placement forms these
+  if (s.B >= kClusterMinChildren && !s.generational) return;  // the cluster placement forms these
   const int b = item - off[si];
   child_result(s, b);
 }
@@ -1542,6 +1602,60 @@ __global__ void k_commit(const SearchDesc* descs, const int32_t* off, int n) {
   for (int i = lane; i < len_nodes(l); i += kCommitLanes) to[i] = from[i];
   for (int i = lane; i < len_consts(l); i += kCommitLanes) cto[i] = cfrom[i];
   if (lane == 0) s.len[m] = l;
+}
+
+// ----------------------------------------------------------- generational
+// The generational schedule's placement (reproduce, phase_population_cpu.cpp:
+// 269-312, then the next evaluate's reuse, :243-265): child i becomes member
+// i with its result.  Runs after k_child_results, which read the members'
+// results for the reused children; k_commit then copies the rows.
+__global__ void k_gen_place(const SearchDesc* descs, const int32_t* off, int n) {
+  const int item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= off[n]) return;
+  const int si = find_search(off, n, item);
+  const SearchDesc& s = descs[si];
+  if (!search_live(s)) return;
+  const int m = item - off[si];
+  s.fitness[m] = s.c_fitness[m];
+  s.wrong[m] = s.c_wrong[m];
+  s.nodes[m] = s.c_nodes[m];
+  s.key[m] = s.c_key[m];
+  s.placed[m] = m;
+}
+
+// End of a generational round, one block per search: the next round's
+// elites and best member, its variation seed (the next run-generator output,
+// one per generation as run_phase_population draws rng() per reproduce,
+// evolve.cpp:300-301) and the round count.
+__global__ void k_gen_finish(const SearchDesc* descs, int n) {
+  __shared__ uint64_t mt[312], nw[312];
+  __shared__ int32_t best_one[1];
+  const SearchDesc& s = descs[blockIdx.x];
+  if (!search_live(s)) return;
+  if (s.elite_count > 0) {
+    block_best_members(s, s.elite_count, s.elites);
+  } else {
+    block_best_members(s, 1, best_one);
+  }
+  __syncthreads();
+  long long* head = stream_ptrs(s);
+  const long long rp = head[0], wp = head[1];
+  if (rp >= wp) {  // the run generator's next block (every 312 generations)
+    for (int i = threadIdx.x; i < 312; i += blockDim.x) mt[i] = s.mt[i];
+    __syncthreads();
+    mt_block(s, mt, nw, wp);
+    for (int i = threadIdx.x; i < 312; i += blockDim.x) s.mt[i] = mt[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s.best[0] = s.elite_count > 0 ? s.elites[0] : best_one[0];
+    s.round_seed[0] = s.stream[rp % s.stream_capacity];
+    head[0] = rp + 1;
+    if (rp >= wp) head[1] = wp + 312;
+    const int done = s.round[0] + 1;
+    s.round[0] = done;
+    if (done >= s.total_rounds) s.round[2] = 1;
+  }
 }
 
 }  // namespace gb

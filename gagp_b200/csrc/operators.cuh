@@ -10,23 +10,64 @@
 
 namespace gb {
 
-// Selection-value comparison of two members.  For metrics with wrong counts
-// the reference's selection values are ranks (evolve.cpp:285,361), so a
-// larger selection value is exactly a better rank; otherwise they are the
-// fitness values.  Keys pack (-fitness, wrong, nodes) so smaller is better.
-__device__ __forceinline__ bool selection_greater(const SearchDesc& s, const uint64_t* key, int c, int b) {
-  const uint64_t kc = key[c], kb = key[b];
-  return kc < kb || (s.has_wrong && kc == kb && c < b);
+// A tournament entrant: its key, tie-break and member; `live` false for a
+// lane that holds no draw.  Keys pack (-fitness, wrong, nodes), smaller is
+// better.  For metrics with wrong counts the reference's selection values are
+// ranks (evolve.cpp:285,361), and of two members with equal keys the one of
+// smaller index holds the better rank; otherwise they are the fitness values,
+// and equal keys are equal selection values.
+struct Entrant {
+  uint64_t key;
+  uint32_t tie;
+  int member;
+  bool live;
+};
+__device__ __forceinline__ bool entrant_better(const Entrant& a, const Entrant& b) {
+  return a.live && (!b.live || a.key < b.key || (a.key == b.key && a.tie < b.tie));
+}
+__device__ __forceinline__ Entrant warp_best_entrant(Entrant e) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    Entrant f;
+    f.key = __shfl_xor_sync(kFull, e.key, o);
+    f.tie = __shfl_xor_sync(kFull, e.tie, o);
+    f.member = __shfl_xor_sync(kFull, e.member, o);
+    f.live = __shfl_xor_sync(kFull, int(e.live), o) != 0;
+    if (entrant_better(f, e)) e = f;
+  }
+  return e;
 }
 
-// tournament (phase_operators.cuh:46-50)
-__device__ inline int tournament(const SearchDesc& s, Rng& random) {
-  int best = int(random.bounded_fixed(uint64_t(s.P), s.bounded_threshold, s.mod_magic));
-  for (int i = 1; i < s.pressure; ++i) {
-    const int c = int(random.bounded_fixed(uint64_t(s.P), s.bounded_threshold, s.mod_magic));
-    if (selection_greater(s, s.key, c, best)) best = c;
+// The parent's and the donor's tournaments, one after the other on `random`
+// (crossover_child's two tournament calls, phase_operators.cuh:46-50,
+// 135-136), with their key loads in flight together.  Every lane draws the
+// same 2 x pressure members in order and lane j keeps draw j of each chunk
+// of 32.  The sequential tournament replaces its best only by a strictly
+// better selection value or, for rank values, an equal one of smaller member
+// index, so its winner is the entrant of the smallest (key, tie): tie = the
+// member index for rank values, the draw position otherwise.
+__device__ inline void warp_tournaments(const SearchDesc& s, Rng& random, int* parent, int* donor) {
+  const int lane = lane_id();
+  const int p = s.pressure, total = 2 * p;
+  Entrant best[2] = {{0, 0, 0, false}, {0, 0, 0, false}};
+  for (int base = 0; base < total; base += 32) {
+    const int n = min(32, total - base);
+    int mine = 0;
+    for (int j = 0; j < n; ++j) {
+      const int d = int(random.bounded_fixed(uint64_t(s.P), s.bounded_threshold, s.mod_magic));
+      if (j == lane) mine = d;
+    }
+    const int position = base + lane;
+    const int which = position < p ? 0 : 1;
+    const uint64_t key = lane < n ? s.key[mine] : 0;
+    for (int t = 0; t < 2; ++t) {
+      const Entrant e{key, s.has_wrong ? uint32_t(mine) : uint32_t(position - t * p), mine, lane < n && which == t};
+      const Entrant w = warp_best_entrant(e);
+      if (entrant_better(w, best[t])) best[t] = w;
+    }
   }
-  return best;
+  *parent = best[0].member;
+  *donor = best[1].member;
 }
 
 // Shared-memory rows of one warp: parent, donor, child, splice output,
@@ -52,28 +93,27 @@ __device__ inline WarpRows carve_rows(char* base, int stride) {
   return r;
 }
 
-// The parent's and the donor's rows into shared memory, their loads in
-// flight together.
+// The parent's and the donor's rows into shared memory.  Every member row
+// holds `stride` words, so the whole stride is copied without waiting for
+// the lengths: the row loads and the length loads are in flight together.
 __device__ inline void load_members(const SearchDesc& s, int a, SRow& to_a, int b, SRow& to_b) {
   const int32_t la = s.len[a], lb = s.len[b];
-  to_a.n = len_nodes(la);
-  to_a.nc = len_consts(la);
-  to_b.n = len_nodes(lb);
-  to_b.nc = len_consts(lb);
   const uint64_t* na = s.node + size_t(a) * s.stride;
   const uint64_t* nb = s.node + size_t(b) * s.stride;
   const int64_t* ca = s.cval + size_t(a) * s.stride;
   const int64_t* cb = s.cval + size_t(b) * s.stride;
-  const int n = max(max(to_a.n, to_b.n), max(to_a.nc, to_b.nc));
-  for (int i = lane_id(); i < n; i += 32) {
-    const bool na_ok = i < to_a.n, nb_ok = i < to_b.n, ca_ok = i < to_a.nc, cb_ok = i < to_b.nc;
-    const uint64_t x = na_ok ? na[i] : 0, y = nb_ok ? nb[i] : 0;
-    const int64_t u = ca_ok ? ca[i] : 0, v = cb_ok ? cb[i] : 0;
-    if (na_ok) to_a.node[i] = x;
-    if (nb_ok) to_b.node[i] = y;
-    if (ca_ok) to_a.cval[i] = u;
-    if (cb_ok) to_b.cval[i] = v;
+  for (int i = lane_id(); i < s.stride; i += 32) {
+    const uint64_t x = na[i], y = nb[i];
+    const int64_t u = ca[i], v = cb[i];
+    to_a.node[i] = x;
+    to_b.node[i] = y;
+    to_a.cval[i] = u;
+    to_b.cval[i] = v;
   }
+  to_a.n = len_nodes(la);
+  to_a.nc = len_consts(la);
+  to_b.n = len_nodes(lb);
+  to_b.nc = len_consts(lb);
   __syncwarp();
 }
 
@@ -150,7 +190,8 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
   *reuse_out = -1;
   // ---- crossover_child
   Rng random(seed ^ (0x617089e168ULL + uint64_t(child)));
-  const int parent = tournament(s, random), donor = tournament(s, random);
+  int parent, donor;
+  warp_tournaments(s, random, &parent, &donor);
   *parent_out = parent;
   load_members(s, parent, w.parent, donor, w.donor);
   stamp[0] = clock64();
@@ -228,6 +269,21 @@ __device__ inline int warp_vary_child(const SearchDesc& s, int child, uint64_t s
         }
       }
     }
+  }
+  // ---- the generational schedule's elites (reproduce,
+  // phase_population_cpu.cpp:283-290): the first elite_count children are
+  // the best members, each reusing its own completed result (an identical
+  // program: the same result as the parent or member the reference finds)
+  if (s.generational && child < s.elite_count) {
+    const int src = s.elites[child];
+    const int32_t l = s.len[src];
+    for (int i = lane; i < len_nodes(l); i += 32)
+      s.cnode[size_t(child) * s.stride + i] = s.node[size_t(src) * s.stride + i];
+    for (int i = lane; i < len_consts(l); i += 32)
+      s.ccval[size_t(child) * s.stride + i] = s.cval[size_t(src) * s.stride + i];
+    if (lane == 0) s.clen[child] = l;
+    *reuse_out = src;
+    return 0;
   }
   // ---- compare_child: identical construction records and constants
   bool equal = w.child.n == w.parent.n && w.child.nc == w.parent.nc;

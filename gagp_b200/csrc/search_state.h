@@ -18,6 +18,9 @@
 
 namespace gb {
 
+// Elites the generational schedule keeps on the device.
+constexpr int kMaxElites = 64;
+
 constexpr int kCapacity = 1024;        // semantic phase capacity (phase_operators.cuh:13)
 constexpr unsigned kNoId = 0xffffffffu;
 constexpr int kMaxTemps = 6;           // accumulator VM temporaries
@@ -125,8 +128,12 @@ struct SearchDesc {
   double crossover_probability, mutation_probability, penalty;
   int64_t penalty_int;                 // |penalty| when integral
   uint64_t seed;
-  int32_t rounds_per_epoch;            // P / B
+  int32_t rounds_per_epoch;            // P / B (1 for the generational schedule)
   int32_t generations;
+  // generational schedule (run_phase_population, evolve.cpp:253-322): every
+  // round replaces the whole population (B = P), its first elite_count
+  // children by the elites of the ranking
+  int32_t generational, elite_count;
   // ---- cases (input-major: inputs[j * C + c]); an IntList input's value is
   // the offset in `lists` of its length word, its elements following
   const int64_t* inputs;
@@ -139,6 +146,7 @@ struct SearchDesc {
   uint64_t* cnode;    int64_t* ccval;    int32_t* clen;       // B child rows
   // ---- member statistics; key: packed ranking key (smaller is better)
   double* fitness; uint32_t* wrong; uint32_t* nodes; uint64_t* key;
+  uint32_t* errors;  // row evaluation only (null otherwise): cases that ended in a runtime error
   // ---- per-child results of one round
   int32_t* c_parent; int32_t* c_reuse; int32_t* c_error;
   double* c_fitness; uint32_t* c_wrong; uint32_t* c_nodes; uint64_t* c_key;
@@ -172,6 +180,7 @@ struct SearchDesc {
   uint64_t* round_seed;                // seed of the next round's variation
   // ---- search progress and history
   int32_t* best;                       // tracked best member
+  int32_t* elites;                     // generational: the elite_count best members, best first
   int32_t* placed;                     // P: child placed into member, -1
   int32_t* place_state;                // 1: the cluster placement placed this round
   int16_t* child_level;                // B: placement level of each child (k_place_levels)

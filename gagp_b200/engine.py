@@ -39,7 +39,8 @@ def load_library():
                      "gagp_b200_search_destroy", "gagp_b200_search_run", "gagp_b200_batch_run",
                      "gagp_b200_batch_step", "gagp_b200_search_result", "gagp_b200_batch_start",
                      "gagp_b200_batch_advance", "gagp_b200_search_progress", "gagp_b200_search_counters", "gagp_b200_engine_transfers",
-                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_evaluate_rows",
+                     "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_engine_timeline",
+                     "gagp_b200_evaluate_rows", "gagp_b200_judge_rows",
                      "gagp_b200_evaluate_rows_static", "gagp_b200_server_create", "gagp_b200_server_submit",
                      "gagp_b200_server_step", "gagp_b200_server_poll", "gagp_b200_server_times",
                      "gagp_b200_server_result", "gagp_b200_server_cancel"):
@@ -181,6 +182,19 @@ class Engine:
             i += 1
         return out
 
+    def timeline(self) -> List[tuple]:
+        """(kernel name, start ms, end ms) of the timed launches of the last
+        batch of rounds read back, in launch order."""
+        lib = load_library()
+        count = C.c_int32()
+        _check(lib.gagp_b200_engine_timeline(self.handle, C.c_int32(0), None, None, None, C.byref(count)))
+        n = count.value
+        kernel = (C.c_int32 * max(1, n))()
+        start, end = (C.c_float * max(1, n))(), (C.c_float * max(1, n))()
+        _check(lib.gagp_b200_engine_timeline(self.handle, C.c_int32(n), kernel, start, end, C.byref(count)))
+        names = list(self.kernel_stats())
+        return [(names[kernel[i]], start[i], end[i]) for i in range(min(n, count.value))]
+
     def evaluate_rows(self, task: LoadedTask, rows: abi.RowsBuffer):
         """Fitness and wrong counts of transport rows on the task's cases."""
         g = abi.GrammarBlob(task.tables)
@@ -191,6 +205,25 @@ class Engine:
                                                       fitness.ctypes.data_as(C.POINTER(C.c_double)),
                                                       wrong.ctypes.data_as(C.POINTER(C.c_uint32))))
         return fitness, wrong
+
+    def judge_rows(self, task: LoadedTask, rows: abi.RowsBuffer, cases: Optional[abi.CasesBlob] = None) -> List[dict]:
+        """The reference's judgement (cases, correct, wrong, runtime_errors,
+        mean_loss, solved) of each row on `cases`, by default the task's test
+        split."""
+        cases = cases if cases is not None else task.test_cases
+        if cases is None:
+            raise ValueError("the task has no test split")
+        g = abi.GrammarBlob(task.tables)
+        cfg = task.settings.struct()
+        out = (abi.Verdict * max(1, rows.count))()
+        _check(load_library().gagp_b200_judge_rows(self.handle, g.ref(), cases.ref(), C.byref(cfg), rows.ref(), out))
+        return [out[i].summary() for i in range(rows.count)]
+
+    def judge_best(self, task: LoadedTask, result: dict) -> dict:
+        """The judgement of a search result's best program on the task's test
+        split, as `gagp run` reports it under "test"."""
+        stride = task.tables.max_nodes - task.tables.fixed_nodes
+        return self.judge_rows(task, abi.RowsBuffer.from_rows([result["final"][0]["row"]], stride))[0]
 
 
 def evaluate_rows_static(task: LoadedTask, rows: abi.RowsBuffer, stream: int = 0):

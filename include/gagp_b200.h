@@ -295,6 +295,12 @@ gagp_status gagp_b200_search_counters(gagp_engine* engine, int32_t search, uint6
 gagp_status gagp_b200_engine_profile(gagp_engine* engine, int32_t enable);
 gagp_status gagp_b200_engine_kernel_stats(gagp_engine* engine, int32_t kernel, const char** name,
                                           double* total_ms, int64_t* launches);
+/* The timed launches of the last batch of rounds read back (profiling on),
+ * in launch order: kernel index, start and end in ms after the batch's first
+ * timed launch started.  *count is the number held; at most `capacity` are
+ * written. */
+gagp_status gagp_b200_engine_timeline(gagp_engine* engine, int32_t capacity, int32_t* kernel, float* start_ms,
+                                      float* end_ms, int32_t* count);
 
 /* Fitness and wrong-case counts of phase rows (host `rows`) on a case set:
  * each row is lowered on the device and run on every case, with the case
@@ -306,6 +312,24 @@ gagp_status gagp_b200_engine_kernel_stats(gagp_engine* engine, int32_t kernel, c
 gagp_status gagp_b200_evaluate_rows(gagp_engine* engine, const gagp_grammar* grammar, const gagp_cases* cases,
                                     const gagp_search_config* config, const gagp_rows* rows, double* fitness,
                                     uint32_t* wrong);
+
+/* The verdict of one program on a case set, as the reference judges a run's
+ * best program on the task's test split (judge / judge_case,
+ * cpp/src/cli/run.cpp:176-238): cases, correct cases, runtime errors (a
+ * failed execution, or a value that is not an Int where an Int is expected)
+ * and the summed case loss (absolute metric: the integer gap capped at the
+ * penalty, the penalty for an error or a wrong non-Int value; exact metric:
+ * 1 per case that is not correct; 0 for a correct case).  The reference
+ * reports mean_loss = loss / cases and solved = (correct == cases). */
+typedef struct gagp_verdict {
+  int32_t cases, correct, runtime_errors, reserved;
+  double loss;
+} gagp_verdict;
+/* Verdicts of phase rows (host `rows`, e.g. a result's best row) on a case
+ * set (e.g. the test split), lowered and run on the device like
+ * gagp_b200_evaluate_rows; out[rows->count]. */
+gagp_status gagp_b200_judge_rows(gagp_engine* engine, const gagp_grammar* grammar, const gagp_cases* cases,
+                                 const gagp_search_config* config, const gagp_rows* rows, gagp_verdict* out);
 
 /* gagp_b200_evaluate_rows without any device allocation -- no counterpart in
  * the reference.  For callers that must not call cudaMalloc: a host

@@ -20,7 +20,8 @@
 //       the initial population lowered by the resident owner's phase compiler
 //       (reference bytecode: op, flags, a, b, fuel; constants; locals; stack
 //       bound), each program's fitness and wrong count from the CPU
-//       evaluator, and the outcome of its first K cases.
+//       evaluator, the outcome of its first K cases, and the program as
+//       ast-prefix-v2 JSON (encode_ast_json, for `gagp eval`).
 //
 //   ref_driver batch TASK.json [--search F] [--population N] [--seed S] --round-seed R
 //       one make_batch of the CPU resident owner (HostPhasePopulation,
@@ -352,7 +353,7 @@ int run_lower(const Args& a) {
     for (std::size_t j = 0; j < gene.origins.size(); ++j) std::printf("%s%d", j ? "," : "", gene.origins[j]);
     std::printf("],\"constants\":[");
     for (std::size_t j = 0; j < gene.constants.size(); ++j) std::printf("%s%" PRId64, j ? "," : "", gene.constants[j].i);
-    std::printf("],\"status\":%d", int(r.status));
+    std::printf("],\"status\":%d,\"program\":%s", int(r.status), cli_detail::encode_ast_json(population[p].ast).c_str());
     if (r.status != rp::PhaseCompileStatus::Ok) { std::printf("}"); continue; }
     BytecodeProgram program = imported.executable;
     rp::patch_whole_program(program, layout, code.data(), r.code_count, values.data(), r.constant_count, r);

@@ -171,6 +171,161 @@ def variant_grammar(variant):
     return None
 
 
+# Generational schedule (golden/generational/): whole reference CPU-engine
+# searches under schedule.mode generational with elites
+# (run_phase_population, cpp/src/evolution/evolve.cpp:253-322).
+GEN_CASES = [
+    ("gen_poly4_e1", "poly4", dict(population=256, generations=8, seed=41, cases=48), {"elitism": 1}),
+    ("gen_poly4_e4_t3", "poly4", dict(population=300, generations=8, seed=42, cases=40),
+     {"elitism": 4, "selection": {"method": "tournament", "size": 3}}),
+    ("gen_polynomial_e0", "polynomial", dict(population=200, generations=10, seed=43), {"elitism": 0}),
+    ("gen_poly4_exact_e2", "poly4_exact", dict(population=256, generations=6, seed=44, cases=40), {"elitism": 2}),
+    ("gen_list_e2", "list", dict(population=128, generations=5, seed=45, cases=20), {"elitism": 2}),
+    ("gen_poly4_p4096", "poly4", dict(population=4096, generations=4, seed=46, cases=64), {"elitism": 3}),
+]
+
+
+def gen_fixtures() -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "generational"), exist_ok=True)
+    for name, workload, kwargs, extra in GEN_CASES:
+        if workload == "list":
+            task = W.list_threshold(**kwargs)
+        elif workload == "poly4_exact":
+            task = W.poly4(**kwargs)
+            task.fitness = {"metric": "exact"}
+        else:
+            task = W.make(workload, **kwargs)
+        task.search.update(extra)
+        task.search["schedule"] = {"mode": "generational"}
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            run = driver("run", tp, "--search", sp)
+        assert run["declined"] == "", (name, run["declined"])
+        fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+                   "train": task.train, "test": task.test, "search": task.search, "run": run}
+        with gzip.open(os.path.join(here, "generational", name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(run["history"]), "history entries,", len(run["final"]), "final members",
+              run["program_cases"], "program-cases,", run["reused_programs"], "reused")
+
+
+# Judgement pins (golden/judge/): the reference's `gagp eval --split test`
+# verdict (cpp/src/cli/run.cpp:176-238) of generated programs on a test split,
+# and one `gagp run` whose result carries the best program's test verdict.
+JUDGE_CASES = [
+    ("judge_int64_edges", "int64_edges", dict(population=160, generations=1, seed=31)),
+    ("judge_polynomial", "polynomial", dict(population=96, generations=1, seed=32)),
+    ("judge_list", "list", dict(population=96, generations=1, seed=33, cases=24)),
+    ("judge_bool_absolute", "bool", dict(population=96, generations=1, seed=34)),
+    ("judge_bool_exact", "bool_exact", dict(population=96, generations=1, seed=35)),
+    ("judge_poly4_exact", "poly4_exact", dict(population=96, generations=1, seed=36, cases=40)),
+]
+JUDGE_RUN = ("judge_run_polynomial", dict(population=512, generations=24, seed=37))
+REF_CLI = os.path.join(ROOT, "oracle", "_ref", "gagp")
+
+
+def bool_task(population: int, generations: int, seed: int, metric: str = "absolute") -> "W.TaskFiles":
+    """A Bool-valued program grammar (comparisons of Int terms, not/and, and a
+    Python-sign `mod` that fails on 0) with target x mod 3 == 1 read as x > 2
+    and x < 9; the absolute metric scores a Bool case at the penalty ceiling
+    whatever its value, the judge counts it correct when it equals."""
+    e, c = {"ref": "E"}, {"ref": "Cond"}
+    g = {"format_version": "grammar-definition-v2", "entry": {"nonterminal": "Cond", "type": "Bool"},
+         "inputs": [{"name": "x", "type": "Int"}], "search_limits": {"max_nodes": 24, "max_depth": 6},
+         "execution_limits": {"fuel": 1000},
+         "nonterminals": [
+             {"id": "Cond", "type": "Bool", "scope": [], "alternatives": [
+                 {"id": "lt", "weight": 2, "expression": {"signature": "lt(Int,Int)->Bool", "args": [e, e]}},
+                 {"id": "gt", "weight": 2, "expression": {"signature": "gt(Int,Int)->Bool", "args": [e, e]}},
+                 {"id": "not", "weight": 1, "expression": {"signature": "not(Bool)->Bool", "args": [c]}},
+                 {"id": "and", "weight": 1, "expression": {"signature": "and(Bool,Bool)->Bool", "args": [c, c]}}]},
+             {"id": "E", "type": "Int", "scope": [], "alternatives": [
+                 {"id": "x", "weight": 3, "expression": {"input": "x"}},
+                 {"id": "k", "weight": 2, "expression": {"constant": {"type": "Int", "range": ["-3", "9"]}}},
+                 {"id": "add", "weight": 1, "expression": {"signature": "add(Int,Int)->Int", "args": [e, e]}},
+                 {"id": "mod", "weight": 1, "expression": {"signature": "mod(Int,Int)->Int", "args": [e, e]}}]}]}
+
+    def case(x):
+        return {"inputs": {"x": {"type": "int", "value": x}}, "expected": {"type": "bool", "value": 2 < x < 9}}
+    fitness = {"metric": metric, "case_cap": 7} if metric == "absolute" else {"metric": "exact"}
+    return W.TaskFiles(name="bool-%s-s%d" % (metric, seed), grammar=g, train=[case(x) for x in range(-6, 14)],
+                       test=[case(x) for x in range(-10, 20, 3)] + [case(0)], fitness=fitness,
+                       search=W.search_config(population, generations, seed))
+
+
+def judge_task(workload: str, kwargs: dict) -> "W.TaskFiles":
+    """A task with a test split for the judgement pins."""
+    if workload == "int64_edges":
+        task = int64_edge_task(**kwargs)
+        task.test = [W._int_case(x, int64_edge_target(x) + (x & 1)) for x in reversed(INT64_EDGE_X)]
+    elif workload == "polynomial":
+        task = W.polynomial(**kwargs)
+    elif workload == "list":
+        task = W.list_threshold(**kwargs)
+        task.test = W.list_threshold(population=8, generations=1, seed=kwargs["seed"] + 1000, cases=30).train
+    elif workload == "bool":
+        task = bool_task(**kwargs)
+    elif workload == "bool_exact":
+        task = bool_task(**kwargs, metric="exact")
+    else:
+        task = W.poly4(**kwargs)
+        task.fitness = {"metric": "exact"}
+        task.test = W.poly4(population=8, generations=1, seed=kwargs["seed"] + 1000, cases=25).train
+    assert task.test, workload
+    return task
+
+
+def judge_fixtures() -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "judge"), exist_ok=True)
+    for name, workload, kwargs in JUDGE_CASES:
+        task = judge_task(workload, kwargs)
+        rows = []
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            lowered = driver("lower", tp, "--search", sp)
+            for r in lowered["rows"]:
+                if r["status"] != 0:
+                    continue
+                pp = os.path.join(d, "program.json")
+                with open(pp, "w") as f:
+                    json.dump(r["program"], f)
+                out = subprocess.run([REF_CLI, "eval", tp, pp, "--split", "test"], check=True, capture_output=True,
+                                     text=True).stdout
+                verdict = json.loads(out)
+                rows.append({"origins": r["origins"], "constants": r["constants"],
+                             "verdict": {k: verdict[k] for k in ("cases", "correct", "wrong", "runtime_errors",
+                                                                 "mean_loss", "solved")}})
+        fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+                   "train": task.train, "test": task.test, "search": task.search, "rows": rows}
+        with gzip.open(os.path.join(here, "judge", name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        errors = sum(1 for r in rows if r["verdict"]["runtime_errors"])
+        print(name, len(rows), "programs,", errors, "with runtime errors")
+    name, kwargs = JUDGE_RUN
+    task = W.polynomial(**kwargs)
+    with tempfile.TemporaryDirectory() as d:
+        task.write(d)
+        tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+        subprocess.run([REF_CLI, "run", tp, "--engine", "cpu", "--search", sp, "--out", os.path.join(d, "out"),
+                        "--quiet"], check=True, capture_output=True)
+        with open(os.path.join(d, "out", "result.json")) as f:
+            result = json.load(f)
+        run = driver("run", tp, "--search", sp)
+    assert result["best"]["text"] == run["final"][0]["text"], "the CLI and the driver ran different searches"
+    fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+               "train": task.train, "test": task.test, "search": task.search,
+               "best": {k: result["best"][k] for k in ("fitness", "wrong", "nodes", "text")}, "test_verdict": result["test"],
+               "run": {"history": run["history"], "final": run["final"][:4], "program_cases": run["program_cases"],
+                       "reused_programs": run["reused_programs"]}}
+    with gzip.open(os.path.join(here, "judge", name + ".json.gz"), "wt") as f:
+        json.dump(fixture, f, separators=(",", ":"))
+    print(name, "best", result["best"]["text"], "test", result["test"])
+
+
 def driver(*args) -> dict:
     out = subprocess.run([DRIVER, *args], check=True, capture_output=True, text=True).stdout
     return json.loads(out)
@@ -181,6 +336,8 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--list-only", action="store_true", help="regenerate golden/list/ only")
     ap.add_argument("--lower-only", action="store_true", help="regenerate golden/lower/ only")
+    ap.add_argument("--judge-only", action="store_true", help="regenerate golden/judge/ only")
+    ap.add_argument("--generational-only", action="store_true", help="regenerate golden/generational/ only")
     ap.add_argument("--headline", action="store_true",
                     help="regenerate golden/headline/ only (the benchmark's search, several minutes)")
     args = ap.parse_args()
@@ -189,6 +346,12 @@ def main() -> None:
         return
     if args.lower_only:
         lower_fixtures()
+        return
+    if args.judge_only:
+        judge_fixtures()
+        return
+    if args.generational_only:
+        gen_fixtures()
         return
     if not os.path.exists(DRIVER):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
@@ -251,6 +414,8 @@ def main() -> None:
             json.dump(fixture, f, separators=(",", ":"))
         print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
     lower_fixtures()
+    judge_fixtures()
+    gen_fixtures()
 
 
 def row_digest(rows) -> str:

@@ -1,7 +1,7 @@
 // Test harness: the reference-side binding of gagp_b200, compiled against the
 // reference's own sources (oracle/Makefile, target `boundary`) and linked with
 // the reference's CPU engine and libgagp_b200.so.  It is the adapter a
-// maintainer adds to the reference (INTEGRATION.md shows it): the engine's
+// maintainer adds to the reference: the engine's
 // tables come from the reference's own phase compiler, the search runs through
 // the C ABI, and the result comes back through the reference's own phase-row
 // export.  `main` runs one task both through this adapter and through the

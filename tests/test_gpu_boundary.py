@@ -1,7 +1,7 @@
 """The C-ABI boundary driven from the reference's own code (GPU).
 
 oracle/_ref/reference_adapter is tests/native/reference_adapter.cpp -- the
-reference-side binding a maintainer adds (INTEGRATION.md) -- compiled
+reference-side binding a maintainer adds -- compiled
 against the reference's sources and linked with its CPU engine and
 libgagp_b200.so.  For each task it builds the engine's tables with the
 reference's own phase compiler (compile_phase_grammar), runs the search

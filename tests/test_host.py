@@ -89,13 +89,21 @@ def test_admission_declines_outside_the_resident_subset(poly_task):
                  if blob.expressions[i].kind == W_KINDS["operation"] and blob.expressions[i].arity > 0)
         blob.expressions[e].node_kind = 9  # Assign
     assert _bytes(poly_task, statement)[0] == 1
+
+
+def test_admission_of_the_generational_schedule(poly_task):
+    """The generational schedule is admitted with reproduce's elite contract
+    (0 <= elites < population, phase_population_cpu.cpp:271); more elites
+    than the device keeps are declined."""
     s = poly_task.settings
-    s_steady = s.steady_state
+    old = s.steady_state, s.elite_count
     try:
         s.steady_state = False
-        assert _bytes(poly_task)[0] == 1
+        for elites, status in ((0, 0), (1, 0), (64, 0), (65, 1), (-1, 2), (s.population, 2)):
+            s.elite_count = elites
+            assert _bytes(poly_task)[0] == status, elites
     finally:
-        s.steady_state = s_steady
+        s.steady_state, s.elite_count = old
 
 
 W_KINDS = {"operation": 0, "constant": 1, "reference": 3, "input": 4}
