@@ -39,6 +39,11 @@ from __future__ import annotations
 import argparse
 import json
 import os
+
+# the engine's rounds run on 11 CUDA streams; more hardware work queues than
+# the default 8 keep them from waiting on each other (read when the CUDA
+# context is created, so before anything touches the GPU)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 import statistics
 import subprocess
 import sys
@@ -705,7 +710,7 @@ def run_serve_workload(args, rank: int, world: int):
         for s in warm:
             s.close()
         latencies, evals = [], 0
-        with Server(eng) as server:
+        with Server(eng, rounds_per_step=args.rounds_per_step) as server:
             outstanding = {}
             nxt, done = 0, 0
             t0 = time.perf_counter()
@@ -760,6 +765,7 @@ def run_serve_workload(args, rank: int, world: int):
                                    "list programs (populations log-uniform 256..16384, 16..2000 cases, 32..128 "
                                    "generations)" % args.requests,
                        "requests": n, "declined_list_requests": declined, "arrival_rate_per_s": args.rate,
+                       "rounds_per_step": args.rounds_per_step,
                        "parallelism": "single-gpu"},
             "latency_s": {"p50": pct(0.5), "p99": pct(0.99), "max": latencies[-1]},
             "program_cases_per_s": evals / makespan, "peak_running": peak_running,
@@ -783,6 +789,8 @@ def main():
                          "batch: 64-search batching mix; serve: open-loop serving stream")
     ap.add_argument("--requests", type=int, default=500, help="serve: requests in the mix")
     ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--rounds-per-step", type=int, default=8,
+                    help="serve: rounds each server step runs before reading the searches' states")
     ap.add_argument("--reference-engine", default="cpu", choices=["cpu", "gpu"],
                     help="--impl reference on poly4/list: the reference CPU engine (default) or its CUDA engine")
     ap.add_argument("--reference-budget", type=float, default=240.0,

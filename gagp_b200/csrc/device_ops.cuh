@@ -32,23 +32,9 @@ constexpr uint32_t kNoClass = 0x7ffu;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---------------------------------------------------------------- RNG
-// Rejection bound ((2^64 - u) mod u) and reciprocal floor((2^64 - 1) / u) of
-// every range u <= kBoundTable, fixed at compile time: site counts, value
-// lists and small integer domains draw without a 64-bit division.
-constexpr int kBoundTable = 1024;
-struct BoundTable {
-  uint64_t threshold[kBoundTable + 1];
-  uint64_t magic[kBoundTable + 1];
-};
-constexpr BoundTable make_bound_table() {
-  BoundTable t{};
-  for (int u = 1; u <= kBoundTable; ++u) {
-    t.threshold[u] = (0 - uint64_t(u)) % uint64_t(u);
-    t.magic[u] = ~uint64_t(0) / uint64_t(u);
-  }
-  return t;
-}
-__device__ const BoundTable g_bounds = make_bound_table();
+// Ranges up to kSmallBound (site counts, value lists, small integer
+// domains) draw with 32-bit arithmetic only (Rng::bounded).
+constexpr uint64_t kSmallBound = uint64_t(1) << 16;
 
 // SplitMix64 stream with rejection-sampled bounds
 // (DGrammarRandom, cpp/src/evolution/repro/gpu/device/grammar_random.cuh:10-51).
@@ -62,8 +48,20 @@ struct Rng {
     return v ^ (v >> 31);
   }
   __device__ __forceinline__ uint64_t bounded(uint64_t upper) {
-    if (upper - 1 < uint64_t(kBoundTable))
-      return bounded_fixed(upper, __ldg(&g_bounds.threshold[upper]), __ldg(&g_bounds.magic[upper]));
+    if (upper - 1 < uint64_t(kSmallBound)) {
+      // the same rejection bound and residue from 32-bit arithmetic, with no
+      // table load on the generator's dependent chain: m = 2^32 mod u, so
+      // the bound (2^64 - u) mod u = 2^64 mod u = m^2 mod u, and a draw
+      // v = hi * 2^32 + lo has v mod u = ((hi mod u) * m + lo mod u) mod u
+      // (every intermediate below 2^32 for u <= 2^16)
+      const uint32_t u = uint32_t(upper);
+      const uint32_t m = (0u - u) % u;
+      const uint32_t threshold = (m * m) % u;
+      for (;;) {
+        const uint64_t v = next();
+        if (v >= threshold) return ((uint32_t(v >> 32) % u) * m + uint32_t(v) % u) % u;
+      }
+    }
     const uint64_t threshold = (0 - upper) % upper;
     for (;;) {
       const uint64_t v = next();

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <deque>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -73,8 +74,9 @@ struct gagp_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
   // side stream of the run-generator top-up, forked from and joined to `stream`
-  cudaStream_t side = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr, indexed = nullptr;
+  cudaStream_t side = nullptr;   // member index and history entry
+  cudaStream_t draws = nullptr;  // run generator and placement levels
+  cudaEvent_t fork = nullptr, join = nullptr, indexed = nullptr, drawn = nullptr;
   // the children of a round in kChunks ranges, each varied, lowered and
   // evaluated on its own stream so that one range's slowest children
   // overlap the other ranges' work
@@ -482,6 +484,8 @@ DrawTables draw_tables(const gagp_grammar* g, bool with_draws) {
     }
     return memo.emplace(std::make_pair(nt, feasible), std::move(dr)).first->second;
   };
+  std::map<std::tuple<int, uint32_t, std::vector<uint32_t>>, std::pair<uint32_t, std::pair<double, int>>> entry_memo;
+  std::map<std::tuple<uint32_t, uint32_t, int32_t>, int32_t> level_memo;
   for (int nt = 0; nt < NT; ++nt) {
     const gagp_nonterminal& n = g->nonterminals[nt];
     const int off = n.production_offset, cnt = n.production_count;
@@ -501,32 +505,50 @@ DrawTables draw_tables(const gagp_grammar* g, bool with_draws) {
         std::sort(bounds.begin(), bounds.end());
         bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
         if (bounds.empty() || t.entry.size() + bounds.size() * size_t(cnt) > kMaxDrawEntries) continue;
-        // widest level at the head, narrower ones appended and chained
-        int32_t slot = int32_t((size_t(d) * LC + l) * NT + nt);
-        for (int k = int(bounds.size()) - 1; k >= 0; --k) {
+        // the chain from the narrowest level up: the widest is the head, the
+        // narrower ones are shared by every head whose chain holds them.  A
+        // level's entries depend only on (nonterminal, bound, costs), and a
+        // narrower level on the same plus the levels below it, so equal keys
+        // are equal records: the tables hold each once, which keeps the
+        // generator's working set small
+        int32_t below = -1;
+        for (int k = 0; k < int(bounds.size()); ++k) {
+          const std::vector<uint32_t> key_costs(cost.begin(), cost.end());
+          const auto ekey = std::make_tuple(nt, bounds[k], key_costs);
+          auto eit = entry_memo.find(ekey);
+          if (eit == entry_memo.end()) {
+            std::vector<uint8_t> feasible(cnt);
+            for (int i = 0; i < cnt; ++i) feasible[i] = cost[i] <= bounds[k];
+            const Draw* dr = with_draws ? &draw_of(nt, feasible) : nullptr;
+            const uint32_t at = uint32_t(t.entry.size());
+            for (int i = 0; i < cnt; ++i) {
+              gb::GenEntry en{};
+              en.threshold = dr ? dr->threshold[i] : 0.0;
+              en.expression = g->productions[off + i].expression;
+              en.need = cost[i];
+              t.entry.push_back(en);
+            }
+            eit = entry_memo.emplace(ekey, std::make_pair(at, dr ? std::make_pair(dr->total, dr->last)
+                                                                  : std::make_pair(0.0, -1))).first;
+          }
           gb::GenLevel lv = none;
           lv.bound = bounds[k];
-          lv.entry = uint32_t(t.entry.size());
-          std::vector<uint8_t> feasible(cnt);
-          for (int i = 0; i < cnt; ++i) feasible[i] = cost[i] <= bounds[k];
-          const Draw* dr = with_draws ? &draw_of(nt, feasible) : nullptr;
-          if (dr) {
-            lv.total = dr->total;
-            lv.last = dr->last;
+          lv.entry = eit->second.first;
+          if (with_draws) {
+            lv.total = eit->second.second.first;
+            lv.last = eit->second.second.second;
           }
-          for (int i = 0; i < cnt; ++i) {
-            gb::GenEntry en{};
-            en.threshold = dr ? dr->threshold[i] : 0.0;
-            en.expression = g->productions[off + i].expression;
-            en.need = cost[i];
-            t.entry.push_back(en);
-          }
+          lv.below = below;
           if (k == int(bounds.size()) - 1) {
-            t.level[size_t(slot)] = lv;
+            t.level[size_t((size_t(d) * LC + l) * NT + nt)] = lv;
           } else {
-            t.level[size_t(slot)].below = int32_t(t.level.size());
-            slot = int32_t(t.level.size());
-            t.level.push_back(lv);
+            const auto lkey = std::make_tuple(lv.entry, lv.bound, lv.below);
+            auto lit = level_memo.find(lkey);
+            if (lit == level_memo.end()) {
+              lit = level_memo.emplace(lkey, int32_t(t.level.size())).first;
+              t.level.push_back(lv);
+            }
+            below = lit->second;
           }
         }
       }
@@ -687,19 +709,27 @@ const char* gagp_b200_version(void) { return "gagp_b200 1.0 (sm_100a)"; }
 gagp_status gagp_b200_engine_create(int32_t device, uint64_t arena_bytes, gagp_engine** out) {
   if (!out) return fail(GAGP_INVALID_ARGUMENT, "null engine pointer");
   *out = nullptr;
+  // a round runs on 11 streams (the engine stream, 8 variation ranges and 2
+  // side streams); with the default 8 hardware work queues some of them
+  // would share a queue and wait on each other's kernels.  The setting only
+  // takes effect when this call creates the process's CUDA context.
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(GAGP_DEVICE_ERROR, "no CUDA device");
   if (device < 0 || device >= count) return fail(GAGP_INVALID_ARGUMENT, "device index");
   CUDA_TRY(cudaSetDevice(device));
   auto e = std::make_unique<gagp_engine>();
   e->device = device;
-  // the variation ranges take the SMs first; the side stream's run
-  // generator, placement levels, history entry and member index, needed
-  // later in the round, fill what is left
+  // the variation ranges take the SMs first and the member index and
+  // history entry (needed by the lowering and the placement) fill what is
+  // left; the run generator and the placement levels, a chain of few blocks
+  // that the placement waits for, go first
   int least = 0, greatest = 0;
   CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   CUDA_TRY(cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, least));
+  CUDA_TRY(cudaStreamCreateWithPriority(&e->draws, cudaStreamNonBlocking, greatest));
+  CUDA_TRY(cudaEventCreateWithFlags(&e->drawn, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming));
   CUDA_TRY(cudaEventCreateWithFlags(&e->indexed, cudaEventDisableTiming));
@@ -753,6 +783,8 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
   cudaStreamDestroy(e->stream);
   if (e->side) cudaStreamDestroy(e->side);
+  if (e->draws) cudaStreamDestroy(e->draws);
+  if (e->drawn) cudaEventDestroy(e->drawn);
   if (e->fork) cudaEventDestroy(e->fork);
   if (e->join) cudaEventDestroy(e->join);
   if (e->indexed) cudaEventDestroy(e->indexed);
@@ -1212,19 +1244,25 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     gb::k_member_index<<<blocks_for(v.total_members, 8), 256, 0, e->side>>>(v.d_desc, v.d_member_off, v.n);
   }
   CUDA_TRY(cudaEventRecord(e->indexed, e->side));
-  // the generational round draws one run-generator output (k_gen_finish)
-  if (!v.generational) { Timed t(e, KN_STREAM, e->side); gb::k_stream<<<v.n, 256, 0, e->side>>>(v.d_desc, v.n); }
-  if (v.total_children >= gb::kClusterMinChildren && !v.generational) {
-    // the placement levels follow from the draws alone: found here, beside
-    // the variation, so the placement itself only compares and writes keys
-    Timed t(e, KN_LEVELS, e->side);
-    const int local_P = (v.max_P + gb::kPlaceCtas - 1) / gb::kPlaceCtas;
-    gb::k_place_levels<<<v.n * gb::kPlaceCtas, gb::kClusterThreads, 2 * size_t(local_P) * sizeof(int32_t) + 16,
-                         e->side>>>(v.d_desc, v.n);
-  }
   // the history entry reads only what the placement later rewrites
   { Timed t(e, KN_RECORD, e->side); gb::k_record<<<v.n, 1024, 0, e->side>>>(v.d_desc, v.n, 1); }
   CUDA_TRY(cudaEventRecord(e->join, e->side));
+  // the run generator's top-up and the placement levels, on their own
+  // stream beside the variation; the generational round draws one
+  // run-generator output at its end instead (k_gen_finish)
+  if (!v.generational) {
+    CUDA_TRY(cudaStreamWaitEvent(e->draws, e->fork, 0));
+    { Timed t(e, KN_STREAM, e->draws); gb::k_stream<<<v.n, 256, 0, e->draws>>>(v.d_desc, v.n); }
+    if (v.total_children >= gb::kClusterMinChildren) {
+      // the placement levels follow from the draws alone: found here, beside
+      // the variation, so the placement itself only compares and writes keys
+      Timed t(e, KN_LEVELS, e->draws);
+      const int local_P = (v.max_P + gb::kPlaceCtas - 1) / gb::kPlaceCtas;
+      gb::k_place_levels<<<v.n * gb::kPlaceCtas, gb::kClusterThreads, 2 * size_t(local_P) * sizeof(int32_t) + 16,
+                           e->draws>>>(v.d_desc, v.n);
+    }
+    CUDA_TRY(cudaEventRecord(e->drawn, e->draws));
+  }
   // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
   // next child of the variation warps; range c's lists start at item lo
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));
@@ -1296,6 +1334,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
                    std::max(size_t(v.max_P) * sizeof(int32_t) + 64, size_t(v.max_draws + 64) * sizeof(uint16_t));
     bytes = std::min(bytes, limit);
     CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join, 0));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->drawn, 0));
     // the cluster placement first; the single-block kernel replays what it could not place
     const int local_P = (v.max_P + gb::kPlaceCtas - 1) / gb::kPlaceCtas;
     const size_t cluster_bytes = size_t(local_P + 2) * (sizeof(uint64_t) + sizeof(int32_t)) + 16;
@@ -2099,6 +2138,7 @@ struct Request {
   gagp_search_config config{};
   uint64_t bytes = 0;
   int32_t search = -1;
+  int32_t rounds_done = 0;  // rounds the server has run for this search
   double submitted = -1, admitted = -1, finished = -1;
   // result (gagp_search_result layout)
   int32_t generations = 0, population = 0, stride = 0;
@@ -2126,6 +2166,8 @@ struct gagp_server {
   std::map<int64_t, std::unique_ptr<Request>> requests;
   int32_t* d_status = nullptr;
   size_t status_capacity = 0;
+  // rounds each step runs before the server reads the searches' states
+  int32_t rounds_per_step = 1;
   std::chrono::steady_clock::time_point epoch = std::chrono::steady_clock::now();
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - epoch).count();
@@ -2179,6 +2221,12 @@ gagp_status retire(gagp_server* sv, Request& r) {
 }  // namespace
 
 extern "C" {
+
+gagp_status gagp_b200_server_set_rounds_per_step(gagp_server* sv, int32_t rounds) {
+  if (!sv || rounds < 1 || rounds > 4096) return fail(GAGP_INVALID_ARGUMENT, "rounds per step must be in 1..4096");
+  sv->rounds_per_step = rounds;
+  return GAGP_OK;
+}
 
 gagp_status gagp_b200_server_create(gagp_engine* e, uint64_t memory_budget, int32_t max_active, gagp_server** out) {
   if (!e || !out || max_active < 0) return fail(GAGP_INVALID_ARGUMENT, "bad argument");
@@ -2280,7 +2328,18 @@ gagp_status gagp_b200_server_step(gagp_server* sv, int32_t* running, int32_t* qu
       for (Search* s : fresh) s->started = true;
     }
     if ((st = make_batch_view(e, list, &v)) != GAGP_OK) return st;
-    if ((st = launch_round(e, v)) != GAGP_OK) return st;
+    // up to rounds_per_step rounds (graph replays after the first), no more
+    // than the longest remaining search needs; a search that finishes within
+    // them idles (its kernels skip finished searches) until the states are
+    // read after the last
+    int rounds = 1;
+    for (int64_t t : sv->active) {
+      const Request& r = *sv->requests.at(t);
+      rounds = std::max(rounds, e->searches.at(r.search)->total_rounds - r.rounds_done);
+    }
+    rounds = std::max(1, std::min(rounds, sv->rounds_per_step));
+    if ((st = launch_rounds(e, v, rounds)) != GAGP_OK) return st;
+    for (int64_t t : sv->active) sv->requests.at(t)->rounds_done += rounds;
     const size_t n = list.size();
     if (n > sv->status_capacity) {
       const size_t cap = std::max(n, 2 * sv->status_capacity);

@@ -83,6 +83,61 @@ struct VmWarpSmem {
   int64_t* consts;
 };
 
+// Staged form of an accumulator instruction: one handler per (operation,
+// operand class), chosen once when a warp stages a program, so that running
+// an instruction costs one dispatch.  Swapped operands are normalised away
+// (a swapped comparison is the mirrored one; subtraction and the divisions
+// have reversed handlers).  Staged word: x = handler | kinds << 8 | i3 << 16
+// (kinds: the three 2-bit operand kinds, read by SELECT), y = i1 | i2 << 16.
+enum : uint32_t {
+  H_MOV_T = 0, H_MOV_I, H_MOV_C, H_SPILL, H_NEG, H_NOT, H_ABS, H_SELECT,
+  H_BINARY  // first binary handler: H_BINARY + 3 * binary op + class (T, I, C)
+};
+enum : uint32_t {
+  HB_ADD = 0, HB_SUB, HB_RSUB, HB_MUL, HB_LT, HB_LE, HB_GT, HB_GE, HB_EQ, HB_NE, HB_AND, HB_OR, HB_MIN, HB_MAX,
+  HB_IDIV0, HB_RIDIV0, HB_IMOD0, HB_RIMOD0, HB_TDIV0, HB_RTDIV0, HB_TMOD0, HB_RTMOD0, HB_COUNT
+};
+__device__ __forceinline__ uint2 stage_accumulator(uint2 w) {
+  const uint32_t op = w.x & 0xffu;
+  const bool swap = (w.x >> 8) & 1u;
+  const uint32_t k1 = (w.x >> 9) & 3u;
+  const uint32_t kinds = (w.x >> 9) & 0x3fu;
+  const uint32_t cls = k1 == K_TEMP ? 0u : k1 == K_INPUT ? 1u : 2u;  // binary and MOV operands are never the accumulator
+  uint32_t h;
+  switch (op) {
+    case A_MOV: h = H_MOV_T + cls; break;
+    case A_SPILL: h = H_SPILL; break;
+    case A_NEG: h = H_NEG; break;
+    case A_NOT: h = H_NOT; break;
+    case A_ABS: h = H_ABS; break;
+    case A_SELECT: h = H_SELECT; break;
+    default: {
+      uint32_t b;
+      switch (op) {
+        case A_ADD: b = HB_ADD; break;
+        case A_SUB: b = swap ? HB_RSUB : HB_SUB; break;
+        case A_MUL: b = HB_MUL; break;
+        case A_LT: b = swap ? HB_GT : HB_LT; break;
+        case A_LE: b = swap ? HB_GE : HB_LE; break;
+        case A_GT: b = swap ? HB_LT : HB_GT; break;
+        case A_GE: b = swap ? HB_LE : HB_GE; break;
+        case A_EQ: b = HB_EQ; break;
+        case A_NE: b = HB_NE; break;
+        case A_AND: b = HB_AND; break;
+        case A_OR: b = HB_OR; break;
+        case A_MIN: b = HB_MIN; break;
+        case A_MAX: b = HB_MAX; break;
+        case A_IDIV0: b = swap ? HB_RIDIV0 : HB_IDIV0; break;
+        case A_IMOD0: b = swap ? HB_RIMOD0 : HB_IMOD0; break;
+        case A_TDIV0: b = swap ? HB_RTDIV0 : HB_TDIV0; break;
+        default: b = swap ? HB_RTMOD0 : HB_TMOD0; break;
+      }
+      h = H_BINARY + 3 * b + cls;
+    }
+  }
+  return make_uint2(h | (kinds << 8) | (w.x & 0xffff0000u), w.y);
+}
+
 // Runs cases [case_begin, case_end) (tiles of 32 K from case_begin).
 template <int K, int NIN>
 __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWarpSmem& w, int case_begin,
@@ -110,11 +165,12 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
   {
     const uint2* code = s.code + size_t(slot) * s.code_stride;
     const int64_t* kpool = s.kpool + size_t(slot) * s.stride;
-    for (int i = lane; i < len; i += 32) w.code[i] = code[i];
+    for (int i = lane; i < len; i += 32) w.code[i] = stage_accumulator(code[i]);
     for (int i = lane; i < s.stride; i += 32) w.consts[i] = kpool[i];
     __syncwarp();
   }
   int64_t* __restrict__ temps = w.temps;
+  const int64_t* __restrict__ consts = w.consts;
   int64_t loss = 0;
   uint32_t wrong = 0;
   for (int tile = case_begin; tile < case_end; tile += 32 * K) {
@@ -130,8 +186,7 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
       cur_want[k] = want[k];
     }
     if (tile + 32 * K < case_end) fetch(tile + 32 * K);
-    // operand vector of one instruction: the kind switch is warp-uniform and
-    // taken once per instruction, not once per case
+    // operand vector of kind `kind` (SELECT's operands)
     auto load = [&](uint32_t kind, uint32_t index, int64_t* v) {
       switch (kind) {
         case K_ACC:
@@ -143,128 +198,131 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
           for (int k = 0; k < K; ++k) v[k] = temps[(index * K + k) * 32 + lane];
           break;
         case K_INPUT:
-          if (NIN == 1 || (NIN == 2 && index == 0)) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) v[k] = cur0[k];
-          } else if (NIN == 2) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) v[k] = cur1[k];
-          } else {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
+          for (int k = 0; k < K; ++k) {
+            if (NIN == 1 || (NIN == 2 && index == 0)) v[k] = cur0[k];
+            else if (NIN == 2) v[k] = cur1[k];
+            else {
               const int c = tile + k * 32 + lane;
               v[k] = c < case_end ? __ldg(&inputs[size_t(index) * C + c]) : 0;
             }
           }
           break;
         default: {
-          const int64_t x = w.consts[index];
+          const int64_t x = consts[index];
 #pragma unroll
           for (int k = 0; k < K; ++k) v[k] = x;
         }
       }
     };
+    // the input operand of case k (I-class handlers)
+    auto input = [&](uint32_t index, int k) -> int64_t {
+      if (NIN == 1) return cur0[k];
+      if (NIN == 2) return index == 0 ? cur0[k] : cur1[k];
+      const int c = tile + k * 32 + lane;
+      return c < case_end ? __ldg(&inputs[size_t(index) * C + c]) : 0;
+    };
+// One binary handler per operand class: a = the accumulator, b = the operand.
+#define GB_ACC_BINARY(NAME, EXPR)                                        \
+  case H_BINARY + 3 * NAME: {                                            \
+    const int64_t* t = temps + i1 * (K * 32) + lane;                     \
+    _Pragma("unroll") for (int k = 0; k < K; ++k) {                      \
+      const int64_t a = acc[k], b = t[k * 32];                           \
+      acc[k] = (EXPR);                                                   \
+    }                                                                    \
+    break;                                                               \
+  }                                                                      \
+  case H_BINARY + 3 * NAME + 1: {                                        \
+    _Pragma("unroll") for (int k = 0; k < K; ++k) {                      \
+      const int64_t a = acc[k], b = input(i1, k);                        \
+      acc[k] = (EXPR);                                                   \
+    }                                                                    \
+    break;                                                               \
+  }                                                                      \
+  case H_BINARY + 3 * NAME + 2: {                                        \
+    const int64_t b = consts[i1];                                        \
+    _Pragma("unroll") for (int k = 0; k < K; ++k) {                      \
+      const int64_t a = acc[k];                                          \
+      acc[k] = (EXPR);                                                   \
+    }                                                                    \
+    break;                                                               \
+  }
     uint2 ins = len ? w.code[0] : make_uint2(0, 0);
     for (int ip = 0; ip < len; ++ip) {
       const uint2 cur = ins;
       if (ip + 1 < len) ins = w.code[ip + 1];
-      const uint32_t op = cur.x & 0xffu;
-      const bool swap = (cur.x >> 8) & 1u;
-      const uint32_t k1 = (cur.x >> 9) & 3u, k2 = (cur.x >> 11) & 3u, k3 = (cur.x >> 13) & 3u;
-      const uint32_t i1 = cur.y & 0xffffu, i2 = cur.y >> 16, i3 = cur.x >> 16;
-      if (op == A_SPILL) {
+      const uint32_t i1 = cur.y & 0xffffu;
+      switch (cur.x & 0xffu) {
+        case H_MOV_T: {
+          const int64_t* t = temps + i1 * (K * 32) + lane;
 #pragma unroll
-        for (int k = 0; k < K; ++k) temps[(i1 * K + k) * 32 + lane] = acc[k];
-        continue;
-      }
-      int64_t b[K];
-      if (op != A_NEG && op != A_NOT && op != A_ABS) load(k1, i1, b);
-      switch (op) {
-        case A_MOV:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = b[k];
+          for (int k = 0; k < K; ++k) acc[k] = t[k * 32];
           break;
-        case A_NEG:
+        }
+        case H_MOV_I:
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = input(i1, k);
+          break;
+        case H_MOV_C: {
+          const int64_t x = consts[i1];
+#pragma unroll
+          for (int k = 0; k < K; ++k) acc[k] = x;
+          break;
+        }
+        case H_SPILL: {
+          int64_t* t = temps + i1 * (K * 32) + lane;
+#pragma unroll
+          for (int k = 0; k < K; ++k) t[k * 32] = acc[k];
+          break;
+        }
+        case H_NEG:
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] = wrap_neg(acc[k]);
           break;
-        case A_NOT:
+        case H_NOT:
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] ^= 1;
           break;
-        case A_ABS:
+        case H_ABS:
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] = acc[k] < 0 ? wrap_neg(acc[k]) : acc[k];
           break;
-        case A_SELECT: {
-          int64_t t[K], e[K];
-          load(k2, i2, t);
-          load(k3, i3, e);
+        case H_SELECT: {
+          const uint32_t kinds = (cur.x >> 8) & 0x3fu;
+          int64_t b[K], t[K], e[K];
+          load(kinds & 3u, i1, b);
+          load((kinds >> 2) & 3u, cur.y >> 16, t);
+          load((kinds >> 4) & 3u, cur.x >> 16, e);
 #pragma unroll
           for (int k = 0; k < K; ++k) acc[k] = b[k] ? t[k] : e[k];
           break;
         }
-        case A_ADD:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = wrap_add(acc[k], b[k]);
-          break;
-        case A_SUB:
-          if (swap) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) acc[k] = wrap_sub(b[k], acc[k]);
-          } else {
-#pragma unroll
-            for (int k = 0; k < K; ++k) acc[k] = wrap_sub(acc[k], b[k]);
-          }
-          break;
-        case A_MUL:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = wrap_mul(acc[k], b[k]);
-          break;
-        case A_LT: case A_LE: case A_GT: case A_GE: {
-          // ordered comparison of (x, y) = swap ? (b, acc) : (acc, b)
-          const bool gt = op == A_GT || op == A_GE, eq = op == A_LE || op == A_GE;
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int64_t x = swap ? b[k] : acc[k], y = swap ? acc[k] : b[k];
-            acc[k] = gt ? (eq ? x >= y : x > y) : (eq ? x <= y : x < y);
-          }
-          break;
-        }
-        case A_EQ:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = acc[k] == b[k];
-          break;
-        case A_NE:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = acc[k] != b[k];
-          break;
-        case A_AND:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] &= b[k];
-          break;
-        case A_OR:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] |= b[k];
-          break;
-        case A_MIN:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = acc[k] < b[k] ? acc[k] : b[k];
-          break;
-        case A_MAX:
-#pragma unroll
-          for (int k = 0; k < K; ++k) acc[k] = acc[k] > b[k] ? acc[k] : b[k];
-          break;
-        default: {
-#pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const int64_t x = swap ? b[k] : acc[k], y = swap ? acc[k] : b[k];
-            acc[k] = op == A_IDIV0 ? idiv0(x, y) : op == A_IMOD0 ? imod0(x, y) : op == A_TDIV0 ? tdiv0(x, y)
-                                                                                               : tmod0(x, y);
-          }
-        }
+        GB_ACC_BINARY(HB_ADD, wrap_add(a, b))
+        GB_ACC_BINARY(HB_SUB, wrap_sub(a, b))
+        GB_ACC_BINARY(HB_RSUB, wrap_sub(b, a))
+        GB_ACC_BINARY(HB_MUL, wrap_mul(a, b))
+        GB_ACC_BINARY(HB_LT, int64_t(a < b))
+        GB_ACC_BINARY(HB_LE, int64_t(a <= b))
+        GB_ACC_BINARY(HB_GT, int64_t(a > b))
+        GB_ACC_BINARY(HB_GE, int64_t(a >= b))
+        GB_ACC_BINARY(HB_EQ, int64_t(a == b))
+        GB_ACC_BINARY(HB_NE, int64_t(a != b))
+        GB_ACC_BINARY(HB_AND, a & b)
+        GB_ACC_BINARY(HB_OR, a | b)
+        GB_ACC_BINARY(HB_MIN, a < b ? a : b)
+        GB_ACC_BINARY(HB_MAX, a > b ? a : b)
+        GB_ACC_BINARY(HB_IDIV0, idiv0(a, b))
+        GB_ACC_BINARY(HB_RIDIV0, idiv0(b, a))
+        GB_ACC_BINARY(HB_IMOD0, imod0(a, b))
+        GB_ACC_BINARY(HB_RIMOD0, imod0(b, a))
+        GB_ACC_BINARY(HB_TDIV0, tdiv0(a, b))
+        GB_ACC_BINARY(HB_RTDIV0, tdiv0(b, a))
+        GB_ACC_BINARY(HB_TMOD0, tmod0(a, b))
+        GB_ACC_BINARY(HB_RTMOD0, tmod0(b, a))
+        default: break;
       }
     }
+#undef GB_ACC_BINARY
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int c = tile + k * 32 + lane;

@@ -42,7 +42,7 @@ def load_library():
                      "gagp_b200_engine_profile", "gagp_b200_engine_kernel_stats", "gagp_b200_engine_timeline",
                      "gagp_b200_evaluate_rows", "gagp_b200_judge_rows",
                      "gagp_b200_evaluate_rows_static", "gagp_b200_server_create", "gagp_b200_server_submit",
-                     "gagp_b200_server_step", "gagp_b200_server_poll", "gagp_b200_server_times",
+                     "gagp_b200_server_step", "gagp_b200_server_poll", "gagp_b200_server_set_rounds_per_step", "gagp_b200_server_times",
                      "gagp_b200_server_result", "gagp_b200_server_cancel"):
             getattr(lib, name).restype = C.c_int32
         lib.gagp_b200_engine_destroy.restype = None
@@ -251,16 +251,19 @@ class Server:
     """Continuous-batching request loop over one engine (gagp_b200_server_*).
 
     submit() queues a search; every step() admits queued requests in arrival
-    order while their device bytes fit `memory_budget`, runs one round of
-    every running search in one batched launch sequence and retires the
+    order while their device bytes fit `memory_budget`, runs up to
+    `rounds_per_step` rounds of every running search in one batched launch
+    sequence (a captured round replayed) and retires the
     finished ones; result() returns a finished request's history and final
     population exactly as Search.result() does for the search run alone."""
 
-    def __init__(self, engine: Engine, memory_budget: int = 0, max_active: int = 0):
+    def __init__(self, engine: Engine, memory_budget: int = 0, max_active: int = 0, rounds_per_step: int = 1):
         h = C.c_void_p()
         _check(load_library().gagp_b200_server_create(engine.handle, C.c_uint64(memory_budget),
                                                       C.c_int32(max_active), C.byref(h)))
         self.engine, self.handle, self.tasks = engine, h, {}
+        if rounds_per_step != 1:
+            _check(load_library().gagp_b200_server_set_rounds_per_step(h, C.c_int32(rounds_per_step)))
 
     def close(self):
         if self.handle:

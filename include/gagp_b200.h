@@ -357,9 +357,10 @@ gagp_status gagp_b200_evaluate_rows_static(const gagp_grammar* grammar, const ga
  * in the reference, which runs one search per process.  Requests are queued
  * on submit; every gagp_b200_server_step admits queued requests in arrival
  * order while their device bytes fit the server's memory budget (a request
- * waits, it is not reordered), starts the newly admitted searches, runs one
- * steady-state round of every running search in one batched launch
- * sequence, and retires the searches that finished: their history and final
+ * waits, it is not reordered), starts the newly admitted searches, runs
+ * steady-state rounds of every running search in one batched launch
+ * sequence (gagp_b200_server_set_rounds_per_step), and retires the searches
+ * that finished: their history and final
  * population are copied to host memory and their device memory is released
  * at once for the next admissions.  A request's result is the same as that
  * search run alone (every kernel works per search; the batch only shares
@@ -377,6 +378,11 @@ enum {
 gagp_status gagp_b200_server_create(gagp_engine* engine, uint64_t memory_budget, int32_t max_active,
                                     gagp_server** out);
 void gagp_b200_server_destroy(gagp_server* server);
+/* Rounds each step runs (1..4096, default 1) before it reads the searches'
+ * states: the batch's round is captured once and replayed, and the host
+ * reads states and retires searches once per step.  A search that finishes
+ * within a step waits for the step's end; results do not depend on it. */
+gagp_status gagp_b200_server_set_rounds_per_step(gagp_server* server, int32_t rounds);
 /* Queues a search request (the blobs are copied).  Declines at once what
  * the engine would decline at admission (GAGP_DECLINED) and what can never
  * fit the budget (GAGP_OUT_OF_MEMORY). */

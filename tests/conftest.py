@@ -1,6 +1,9 @@
 import os
 import sys
 
+# as bench.py: the engine's 11 streams each get a hardware work queue
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)

@@ -51,10 +51,11 @@ def _drain(server, tickets, limit=500):
     return finished
 
 
-def test_results_in_the_mix_equal_alone(alone):
+@pytest.mark.parametrize("rounds_per_step", [1, 5])
+def test_results_in_the_mix_equal_alone(alone, rounds_per_step):
     from gagp_b200.engine import Engine, Server
     tasks = _tasks()
-    with Engine(0) as engine, Server(engine) as server:
+    with Engine(0) as engine, Server(engine, rounds_per_step=rounds_per_step) as server:
         tickets = {}
         # arrivals spread over the first steps: later requests join running ones
         arrivals = {0: [0, 1], 1: [2], 3: [3, 4], 4: [5]}
