@@ -787,7 +787,7 @@ def main():
     ap.add_argument("--workload", default="poly4", choices=["poly4", "list", "batch", "serve"],
                     help="poly4: the large scalar search (default); list: the list-program search; "
                          "batch: 64-search batching mix; serve: open-loop serving stream")
-    ap.add_argument("--requests", type=int, default=500, help="serve: requests in the mix")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the mix")
     ap.add_argument("--rate", type=float, default=100.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--rounds-per-step", type=int, default=8,
                     help="serve: rounds each server step runs before reading the searches' states")

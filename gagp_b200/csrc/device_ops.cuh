@@ -140,10 +140,27 @@ struct GenResult {
   int steps;  // tasks processed
 };
 
-// Minimum node cost of (expression, depth, site budget); kNoId when infeasible.
-__device__ __forceinline__ unsigned minimum_of(const SearchDesc& s, int e, int d, int l) {
-  if (e < 0 || e >= s.n_ex || d < 0 || d >= s.depth_count || l < 0 || l >= s.logical_count) return kNoId;
-  return __ldg(&s.minimum[(size_t(e) * s.depth_count + d) * s.logical_count + l]);
+// The subtree generator's tables: the sections of a search's GenImage, in
+// shared memory (the variation kernel's staged copy) or in global memory.
+// Read with plain loads, which serve either.
+struct GenTables {
+  const GenExpr* gx;
+  const GenNt* gnt;
+  const uint32_t* head;
+  const GenLevel* level;
+  const GenEntry* entry;
+  const gagp_domain* doms;
+  const gagp_value* vals;
+  const uint16_t* minimum;
+};
+__device__ __forceinline__ GenTables gen_tables(const SearchDesc& s, const char* image) {
+  return GenTables{reinterpret_cast<const GenExpr*>(image), reinterpret_cast<const GenNt*>(image + s.gi.nt),
+                   reinterpret_cast<const uint32_t*>(image + s.gi.head),
+                   reinterpret_cast<const GenLevel*>(image + s.gi.level),
+                   reinterpret_cast<const GenEntry*>(image + s.gi.entry),
+                   reinterpret_cast<const gagp_domain*>(image + s.gi.doms),
+                   reinterpret_cast<const gagp_value*>(image + s.gi.vals),
+                   reinterpret_cast<const uint16_t*>(image + s.gi.minimum)};
 }
 
 // A precomputed draw level (GenLevel) in registers.
@@ -153,8 +170,8 @@ struct LevelView {
   int last, below;
 };
 __device__ __forceinline__ LevelView load_level(const GenLevel* p) {
-  const int4 a = __ldg(reinterpret_cast<const int4*>(p));
-  const int2 b = __ldg(reinterpret_cast<const int2*>(p) + 2);
+  const int4 a = *reinterpret_cast<const int4*>(p);
+  const int2 b = *(reinterpret_cast<const int2*>(p) + 2);
   return LevelView{__hiloint2double(a.y, a.x), unsigned(a.z), unsigned(a.w), b.x, b.y};
 }
 
@@ -166,21 +183,22 @@ __device__ __forceinline__ LevelView load_level(const GenLevel* p) {
 // Tasks pack (expression:17, depth:7, scope_count:4, logical:4) in `pending`
 // (192 entries).  Emitted words carry depth relative to the generated root
 // (root = 1) and site depth relative to the budget `logical_depth`.
-__device__ inline GenResult generate(const SearchDesc& s, int root_expression, int scope_count, int depth,
-                                     int capacity, uint64_t seed, uint64_t* out_node, int64_t* out_cval,
+__device__ inline GenResult generate(const SearchDesc& s, const GenTables& tables, int root_expression, int scope_count,
+                                     int depth, int capacity, uint64_t seed, uint64_t* out_node, int64_t* out_cval,
                                      int logical_depth, uint64_t* pending) {
   GenResult result{ST_INVALID, 0, 0, 0};
-  // the tables, read once into registers: every table load below is a
-  // read-only load through these
-  const GenExpr* __restrict__ gx = s.gen_expr;
-  const GenNt* __restrict__ gnt = s.gen_nt;
+  // the tables (staged in shared memory by the variation kernel), read once
+  // into registers; the sequential draw's production tables stay global
+  const GenExpr* __restrict__ gx = tables.gx;
+  const GenNt* __restrict__ gnt = tables.gnt;
+  const uint32_t* __restrict__ head = tables.head;
+  const GenLevel* __restrict__ gen_level = tables.level;
+  const GenEntry* __restrict__ gen_entry = tables.entry;
+  const gagp_domain* __restrict__ doms = tables.doms;
+  const gagp_value* __restrict__ vals = tables.vals;
+  const uint16_t* __restrict__ minimum = tables.minimum;
   const gagp_production* __restrict__ prods = s.prods;
-  const gagp_domain* __restrict__ doms = s.doms;
-  const gagp_value* __restrict__ vals = s.vals;
-  const uint32_t* __restrict__ minimum = s.minimum;
   const uint32_t* __restrict__ prod_minimum = s.prod_minimum;
-  const GenLevel* __restrict__ gen_level = s.gen_level;
-  const GenEntry* __restrict__ gen_entry = s.gen_entry;
   const int n_ex = s.n_ex, n_nts = s.n_nts, n_prods = s.n_prods;
   const int depth_count = s.depth_count, logical_count = s.logical_count;
   const bool site_limited = s.site_depth > 0;
@@ -188,7 +206,8 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
   // every expression id a table holds, and the generator keeps depth and site
   // budget inside the table, so only the root's lookup is range-checked
   auto min_at = [&](int e, int d, int l) -> unsigned {
-    return __ldg(&minimum[(e * depth_count + d) * logical_count + l]);
+    const unsigned v = minimum[(e * depth_count + d) * logical_count + l];
+    return v == kNoMinimum16 ? kNoId : v;
   };
   int next_site = -1;  // entry expression of a pending site
   uint32_t next_class = kNoClass;
@@ -220,8 +239,8 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
     const unsigned required = unsigned(task >> 32);
     if (required > reserved) return result;
     reserved -= required;
-    const int4 ra = __ldg(reinterpret_cast<const int4*>(gx + t_expr));      // children
-    const int4 rb = __ldg(reinterpret_cast<const int4*>(gx + t_expr) + 1);  // target, class, kinds, scopes
+    const int4 ra = *reinterpret_cast<const int4*>(gx + t_expr);      // children
+    const int4 rb = *(reinterpret_cast<const int4*>(gx + t_expr) + 1);  // target, class, kinds, scopes
     const int kind = int(int8_t(rb.z & 0xff)), arity = int(int8_t((rb.z >> 8) & 0xff));
     const int target = rb.x;
     if (kind == EK_REFERENCE) {
@@ -230,7 +249,7 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       if (next_site >= 0) return result;
       next_site = t_expr;
       next_class = uint32_t(rb.y);
-      const int4 nt = __ldg(reinterpret_cast<const int4*>(gnt + target));
+      const int4 nt = *reinterpret_cast<const int4*>(gnt + target);
       const int nt_offset = nt.x, nt_count = nt.y;
       const bool normalized = nt.w != 0;
       if (site_limited && t_logical == 0) { result.status = ST_CAPACITY; return result; }
@@ -239,7 +258,7 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       const unsigned available = unsigned(capacity - result.nodes) - reserved;
       unsigned next_expr, need;
       // the widest precomputed level whose productions all fit
-      LevelView lv = load_level(gen_level + ((t_depth * logical_count + n_logical) * n_nts + target));
+      LevelView lv = load_level(gen_level + head[(t_depth * logical_count + n_logical) * n_nts + target]);
       while (lv.bound > available && lv.below >= 0) lv = load_level(gen_level + lv.below);
       if (lv.bound <= available && lv.total == lv.total) {
         const double choice = __dmul_rn(__dmul_rn(double(random.next() >> 11), 0x1.0p-53), lv.total);
@@ -248,15 +267,15 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
         if (nt_count <= 8) {
           double th[8];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) th[k] = k < nt_count ? __ldg(&en[k].threshold) : 0.0;
+          for (int k = 0; k < 8; ++k) th[k] = k < nt_count ? en[k].threshold : 0.0;
 #pragma unroll
           for (int k = 7; k >= 0; --k)
             if (k < nt_count && choice < th[k]) pick = k;
         } else {
           for (int i = 0; i < nt_count; ++i)
-            if (choice < __ldg(&en[i].threshold)) { pick = i; break; }
+            if (choice < en[i].threshold) { pick = i; break; }
         }
-        const int2 picked = __ldg(reinterpret_cast<const int2*>(en + pick) + 1);  // expression, need
+        const int2 picked = *(reinterpret_cast<const int2*>(en + pick) + 1);  // expression, need
         next_expr = unsigned(picked.x);
         need = unsigned(picked.y);
       } else {
@@ -303,11 +322,11 @@ __device__ inline GenResult generate(const SearchDesc& s, int root_expression, i
       // admission: the domain exists and is an Int range or a list of Ints
       const gagp_domain* domain = doms + target;
       int64_t value;
-      if (__ldg(&domain->integer_range)) {
-        value = random.integer(__ldg(&domain->minimum), __ldg(&domain->maximum));
+      if (domain->integer_range) {
+        value = random.integer(domain->minimum, domain->maximum);
       } else {
-        const int v_offset = __ldg(&domain->value_offset), v_count = __ldg(&domain->value_count);
-        value = __ldg(&vals[v_offset + random.bounded(uint64_t(v_count))].i);
+        const int v_offset = domain->value_offset, v_count = domain->value_count;
+        value = vals[v_offset + random.bounded(uint64_t(v_count))].i;
       }
       out_cval[result.constants++] = value;
     } else if (kind != EK_OPERATION && kind != EK_INPUT && kind != EK_BOUND) {

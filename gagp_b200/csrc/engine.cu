@@ -425,6 +425,7 @@ gagp_status admit(const gagp_grammar* g, const gagp_cases* c, const gagp_search_
 constexpr size_t kMaxDrawEntries = size_t(1) << 16;
 
 struct DrawTables {
+  std::vector<uint32_t> head;  // per (depth, site budget, nonterminal): its widest level (0: none)
   std::vector<gb::GenLevel> level;
   std::vector<gb::GenEntry> entry;
 };
@@ -441,7 +442,8 @@ DrawTables draw_tables(const gagp_grammar* g, bool with_draws) {
   none.entry = 0;
   none.last = -1;
   none.below = -1;
-  t.level.assign(heads, none);
+  t.level.assign(1, none);  // level 0: no precomputed draw
+  t.head.assign(heads, 0);
   struct Draw { double total; int last; std::vector<double> threshold; };
   std::map<std::pair<int, std::vector<uint8_t>>, Draw> memo;
   auto from_bits = [](uint64_t b) { double d; std::memcpy(&d, &b, sizeof d); return d; };
@@ -539,22 +541,85 @@ DrawTables draw_tables(const gagp_grammar* g, bool with_draws) {
             lv.last = eit->second.second.second;
           }
           lv.below = below;
-          if (k == int(bounds.size()) - 1) {
-            t.level[size_t((size_t(d) * LC + l) * NT + nt)] = lv;
-          } else {
-            const auto lkey = std::make_tuple(lv.entry, lv.bound, lv.below);
-            auto lit = level_memo.find(lkey);
-            if (lit == level_memo.end()) {
-              lit = level_memo.emplace(lkey, int32_t(t.level.size())).first;
-              t.level.push_back(lv);
-            }
-            below = lit->second;
+          const auto lkey = std::make_tuple(lv.entry, lv.bound, lv.below);
+          auto lit = level_memo.find(lkey);
+          if (lit == level_memo.end()) {
+            lit = level_memo.emplace(lkey, int32_t(t.level.size())).first;
+            t.level.push_back(lv);
           }
+          below = lit->second;
         }
+        t.head[(size_t(d) * LC + l) * NT + nt] = uint32_t(below);  // the widest
       }
   }
   if (t.entry.empty()) t.entry.push_back(gb::GenEntry{});
   return t;
+}
+
+// The subtree generator's tables as one image (gb::GenImage sections, each
+// 16-byte aligned), which the variation kernel copies into shared memory.
+// `with_draws` false: the layout only.
+struct GenImageLayout {
+  gb::GenImage at;
+  size_t bytes = 0;
+};
+GenImageLayout gen_image_layout(const gagp_grammar* g, const DrawTables& t) {
+  GenImageLayout out;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t here = off;
+    off = align_up(off + bytes, 16);
+    return int32_t(here);
+  };
+  const int E = g->expression_count, NT = std::max(1, g->nonterminal_count);
+  take(sizeof(gb::GenExpr) * size_t(E));  // expressions first: offset 0
+  out.at.nt = take(sizeof(gb::GenNt) * size_t(NT));
+  out.at.head = take(sizeof(uint32_t) * t.head.size());
+  out.at.level = take(sizeof(gb::GenLevel) * t.level.size());
+  out.at.entry = take(sizeof(gb::GenEntry) * t.entry.size());
+  out.at.doms = take(sizeof(gagp_domain) * size_t(std::max(1, g->domain_count)));
+  out.at.vals = take(sizeof(gagp_value) * size_t(std::max(1, g->value_count)));
+  out.at.minimum = take(sizeof(uint16_t) * size_t(E) * g->depth_count * g->logical_depth_count);
+  out.bytes = off;
+  return out;
+}
+std::vector<char> gen_image(const gagp_grammar* g, const std::vector<gb::ExprInfo>& info, const DrawTables& t,
+                            const GenImageLayout& lay) {
+  std::vector<char> img(lay.bytes, 0);
+  const int E = g->expression_count;
+  auto* gx = reinterpret_cast<gb::GenExpr*>(img.data());
+  for (int i = 0; i < E; ++i) {
+    const gagp_expression& x = g->expressions[i];
+    gb::GenExpr& r = gx[i];
+    for (int k = 0; k < 4; ++k) {
+      r.child[k] = k < GAGP_MAX_ARITY ? x.children[k] : -1;
+      r.child_scope[k] = k < GAGP_MAX_ARITY ? x.child_scope[k] : -1;
+    }
+    r.target = x.target;
+    r.site_class = info[i].site_class;
+    r.kind = int8_t(x.kind);
+    r.arity = info[i].arity;
+    // out-of-range counts keep their validity (admission bounds them anyway)
+    r.scope_count = int8_t(std::min(std::max(x.scope_count, -1), 100));
+    r.reserved = 0;
+  }
+  auto* nt = reinterpret_cast<gb::GenNt*>(img.data() + lay.at.nt);
+  for (int i = 0; i < g->nonterminal_count; ++i) {
+    const gagp_nonterminal& n = g->nonterminals[i];
+    nt[i] = gb::GenNt{n.production_offset, n.production_count, n.scope_count, n.normalized_weights};
+  }
+  std::memcpy(img.data() + lay.at.head, t.head.data(), sizeof(uint32_t) * t.head.size());
+  std::memcpy(img.data() + lay.at.level, t.level.data(), sizeof(gb::GenLevel) * t.level.size());
+  std::memcpy(img.data() + lay.at.entry, t.entry.data(), sizeof(gb::GenEntry) * t.entry.size());
+  if (g->domain_count) std::memcpy(img.data() + lay.at.doms, g->domains, sizeof(gagp_domain) * g->domain_count);
+  if (g->value_count) std::memcpy(img.data() + lay.at.vals, g->values, sizeof(gagp_value) * g->value_count);
+  auto* minimum = reinterpret_cast<uint16_t*>(img.data() + lay.at.minimum);
+  const size_t cells = size_t(E) * g->depth_count * g->logical_depth_count;
+  for (size_t i = 0; i < cells; ++i) {
+    const uint32_t v = g->minimum[i];
+    minimum[i] = v >= gb::kNoMinimum16 ? gb::kNoMinimum16 : uint16_t(v);
+  }
+  return img;
 }
 
 // Instructions (and constants) the lowering can emit for a row of at most
@@ -610,8 +675,8 @@ std::vector<gb::RegionInfo> region_infos(const gagp_grammar* g) {
 
 struct Plan {
   Layout L;
-  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, gen_level, gen_entry, gen_expr,
-      gen_nt, local_types, regions, inputs, expected, lists;
+  size_t ex, info, prods, nts, doms, vals, minimum, prod_minimum, gen_image, gen_image_bytes, local_types, regions,
+      inputs, expected, lists;
   size_t node, cval, len, cnode, ccval, clen;
   size_t fitness, wrong, nodes, key, c_parent, c_reuse, c_error, c_fitness, c_wrong, c_nodes, c_key, c_eval;
   size_t mtab;
@@ -655,11 +720,9 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
                           g->logical_depth_count);
   {
     const DrawTables shape = draw_tables(g, false);
-    p.gen_level = L.take(sizeof(gb::GenLevel) * shape.level.size());
-    p.gen_entry = L.take(sizeof(gb::GenEntry) * shape.entry.size());
+    p.gen_image_bytes = gen_image_layout(g, shape).bytes;
+    p.gen_image = L.take(p.gen_image_bytes);
   }
-  p.gen_expr = L.take(sizeof(gb::GenExpr) * size_t(E));
-  p.gen_nt = L.take(sizeof(gb::GenNt) * size_t(std::max(1, g->nonterminal_count)));
   p.local_types = L.take(sizeof(int32_t) * GAGP_MAX_LOCALS);
   p.regions = L.take(sizeof(gb::RegionInfo) * size_t(std::max(1, g->region_count)));
   p.inputs = L.take(sizeof(int64_t) * size_t(std::max(1, c->input_count)) * C);
@@ -891,31 +954,10 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
       }
   CUDA_TRY(up(p.prod_minimum, prod_minimum.data(), sizeof(uint32_t) * prod_minimum.size()));
   const DrawTables draw = draw_tables(g, true);
-  CUDA_TRY(up(p.gen_level, draw.level.data(), sizeof(gb::GenLevel) * draw.level.size()));
-  CUDA_TRY(up(p.gen_entry, draw.entry.data(), sizeof(gb::GenEntry) * draw.entry.size()));
-  std::vector<gb::GenExpr> gen_expr(E);
-  for (int i = 0; i < E; ++i) {
-    const gagp_expression& x = g->expressions[i];
-    gb::GenExpr& r = gen_expr[i];
-    for (int k = 0; k < 4; ++k) {
-      r.child[k] = k < GAGP_MAX_ARITY ? x.children[k] : -1;
-      r.child_scope[k] = k < GAGP_MAX_ARITY ? x.child_scope[k] : -1;
-    }
-    r.target = x.target;
-    r.site_class = info[i].site_class;
-    r.kind = int8_t(x.kind);
-    r.arity = info[i].arity;
-    // out-of-range counts keep their validity (admission bounds them anyway)
-    r.scope_count = int8_t(std::min(std::max(x.scope_count, -1), 100));
-    r.reserved = 0;
-  }
-  CUDA_TRY(up(p.gen_expr, gen_expr.data(), sizeof(gb::GenExpr) * gen_expr.size()));
-  std::vector<gb::GenNt> gen_nt(std::max(1, g->nonterminal_count));
-  for (int i = 0; i < g->nonterminal_count; ++i) {
-    const gagp_nonterminal& n = g->nonterminals[i];
-    gen_nt[i] = gb::GenNt{n.production_offset, n.production_count, n.scope_count, n.normalized_weights};
-  }
-  CUDA_TRY(up(p.gen_nt, gen_nt.data(), sizeof(gb::GenNt) * gen_nt.size()));
+  const GenImageLayout lay = gen_image_layout(g, draw);
+  if (lay.bytes != p.gen_image_bytes) return fail(GAGP_DEVICE_ERROR, "generator table plan mismatch");
+  const std::vector<char> image = gen_image(g, info, draw, lay);
+  CUDA_TRY(up(p.gen_image, image.data(), image.size()));
   CUDA_TRY(up(p.local_types, local_types.data(), sizeof(int32_t) * GAGP_MAX_LOCALS));
   const std::vector<gb::RegionInfo> regions = region_infos(g);
   CUDA_TRY(up(p.regions, regions.data(), sizeof(gb::RegionInfo) * regions.size()));
@@ -933,10 +975,9 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.vals = at<gagp_value>(b, p.vals);
   d.minimum = at<uint32_t>(b, p.minimum);
   d.prod_minimum = at<uint32_t>(b, p.prod_minimum);
-  d.gen_level = at<gb::GenLevel>(b, p.gen_level);
-  d.gen_entry = at<gb::GenEntry>(b, p.gen_entry);
-  d.gen_expr = at<gb::GenExpr>(b, p.gen_expr);
-  d.gen_nt = at<gb::GenNt>(b, p.gen_nt);
+  d.gen_image = at<char>(b, p.gen_image);
+  d.gen_image_bytes = int32_t(lay.bytes);
+  d.gi = lay.at;
   d.local_types = at<int32_t>(b, p.local_types);
   d.regions = at<gb::RegionInfo>(b, p.regions);
   d.n_regions = g->region_count;
@@ -1044,7 +1085,13 @@ struct BatchView {
   int min_B = 1 << 30;               // the smallest round of the batch
   bool exact_heavy = false;          // some search's programs mostly need the exact VM
   bool generational = false;         // the batch's schedule (one per batch)
+  std::vector<int> child_off;        // host copy of the child offsets (n + 1)
+  std::vector<size_t> image_bytes;   // each search's generator image
 };
+
+// Generator images up to this size are staged in the variation kernel's
+// shared memory (beside 4 warps' rows, 6 blocks still fit an SM).
+constexpr size_t kMaxStagedImage = size_t(12) << 10;
 
 gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, BatchView* v) {
   const int n = int(list.size());
@@ -1098,7 +1145,11 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
   v->max_C = 1;
   v->max_inputs = 0;
   v->exact_heavy = false;
+  v->child_off.assign(1, 0);
+  v->image_bytes.clear();
   for (Search* s : list) {
+    v->child_off.push_back(v->child_off.back() + s->B);
+    v->image_bytes.push_back(size_t(s->desc.gen_image_bytes));
     v->exact_heavy |= s->exact_heavy;
     v->max_C = std::max(v->max_C, s->desc.C);
     v->max_inputs = std::max(v->max_inputs, s->desc.n_inputs);
@@ -1269,11 +1320,29 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   CUDA_TRY(cudaEventRecord(e->chunk_fork, e->stream));
   const int chunks = v.total_children >= 4096 ? gagp_engine::kChunks : 1;
   const int warps = 4;
-  const size_t vary_smem = warps * gb::warp_rows_bytes(v.max_stride);
+  // a range whose children all belong to one search stages that search's
+  // generator image in shared memory (when it is small enough to keep the
+  // variation kernel's occupancy)
+  auto range_of = [&](int c) {
+    return std::make_pair(int(int64_t(v.total_children) * c / chunks),
+                          int(int64_t(v.total_children) * (c + 1) / chunks));
+  };
+  int staged[gagp_engine::kChunks];
+  size_t image_max = 0;
+  for (int c = 0; c < chunks; ++c) {
+    const auto [lo, hi] = range_of(c);
+    staged[c] = -1;
+    const int si = int(std::upper_bound(v.child_off.begin(), v.child_off.end(), lo) - v.child_off.begin()) - 1;
+    if (si >= 0 && si < v.n && hi <= v.child_off[si + 1] && v.image_bytes[si] <= kMaxStagedImage) {
+      staged[c] = si;
+      image_max = std::max(image_max, v.image_bytes[si]);
+    }
+  }
+  const size_t vary_smem = warps * gb::warp_rows_bytes(v.max_stride) + image_max;
   int per_sm = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vary, warps * 32, vary_smem));
   for (int c = 0; c < chunks; ++c) {
-    const int lo = int(int64_t(v.total_children) * c / chunks), hi = int(int64_t(v.total_children) * (c + 1) / chunks);
+    const auto [lo, hi] = range_of(c);
     cudaStream_t st = chunks == 1 ? e->stream : e->chunk_stream[c];
     if (chunks > 1) CUDA_TRY(cudaStreamWaitEvent(st, e->chunk_fork, 0));
     int32_t* counts = e->d_counts + 4 * c;
@@ -1284,7 +1353,8 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
       const int share = std::max(1, std::max(1, per_sm) * e->sm_count / chunks);
       const int blocks = std::min(blocks_for(hi - lo, warps), share);
       gb::k_vary<<<blocks, warps * 32, vary_smem, st>>>(v.d_desc, v.d_child_off, v.n, v.max_stride, counts + 2, lo,
-                                                        hi, e->profiling ? 1 : 0);
+                                                        hi, e->profiling ? 1 : 0, staged[c],
+                                                        staged[c] >= 0 ? int(v.image_bytes[staged[c]]) : 0);
     }
     CUDA_TRY(cudaStreamWaitEvent(st, e->indexed, 0));
     {

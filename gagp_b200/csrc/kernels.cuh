@@ -51,7 +51,7 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
   GenResult g{ST_INVALID, 0, 0, 0};
   for (int logical = ramp, attempt = 0; g.status != ST_OK; ++attempt) {
     const int room = s.maxv < kCapacity ? s.maxv : kCapacity;
-    g = generate(s, s.root_expression, 0, s.slot_max_depth, room,
+    g = generate(s, gen_tables(s, s.gen_image), s.root_expression, 0, s.slot_max_depth, room,
                  mix64(s.seed ^ mix64((uint64_t(i) * 8 + 0) * 64 + uint64_t(attempt))), node, cval, logical, pending);
     if (g.status != ST_OK && attempt % 4 == 3 && logical < site_limit) ++logical;
     if (attempt >= 256 && g.status != ST_OK) {
@@ -606,12 +606,23 @@ __global__ void __launch_bounds__(256) k_member_index(const SearchDesc* descs, c
 // Persistent warps over the batch items [lo, hi): each warp takes the next
 // child from `next_item` (zeroed before the launch) until the range is
 // varied, so warps that drew short children go on to the next one instead
-// of idling.
+// of idling.  When the range's children all belong to search `staged`, the
+// block first copies that search's generator image (image_bytes) into
+// shared memory after the rows: a generation step is a chain of dependent
+// table lookups, each a shared-memory load instead of a global one.
 __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const int32_t* off, int n, int stride_max,
-                                                 int32_t* next_item, int lo, int hi, int collect_stats) {
+                                                 int32_t* next_item, int lo, int hi, int collect_stats, int staged,
+                                                 int image_bytes) {
   extern __shared__ __align__(16) char smem_rows[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   char* base = smem_rows + size_t(warp) * warp_rows_bytes(stride_max);
+  char* image = smem_rows + size_t(blockDim.x >> 5) * warp_rows_bytes(stride_max);
+  if (staged >= 0) {
+    const uint4* from = reinterpret_cast<const uint4*>(descs[staged].gen_image);
+    uint4* to = reinterpret_cast<uint4*>(image);
+    for (int i = threadIdx.x; i < image_bytes / 16; i += blockDim.x) to[i] = from[i];
+    __syncthreads();
+  }
   const int total = min(off[n], hi);
   for (;;) {
     int item = 0;
@@ -626,7 +637,8 @@ __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const 
     int reuse = -1, parent = -1;
     long long stamp[5] = {0, 0, 0, 0, 0};
     const long long started = clock64();
-    const int error = warp_vary_child(s, child, s.round_seed[0], rows, &reuse, &parent, stamp);
+    const GenTables tables = gen_tables(s, si == staged ? image : s.gen_image);
+    const int error = warp_vary_child(s, tables, child, s.round_seed[0], rows, &reuse, &parent, stamp);
     if (lane == 0 && collect_stats) {
       // per-phase SM cycles: selection, crossover, subtree generation, rest
       stamp[3] = clock64();

@@ -78,6 +78,18 @@ struct alignas(16) GenEntry {
   uint32_t need;
 };
 
+// Byte offsets of the subtree generator's image sections (GenExpr[n_ex] at
+// offset 0, each section 16-byte aligned): GenNt[n_nts]; head[depth_count *
+// logical_count * n_nts], the widest GenLevel of each nonterminal at each
+// (depth, site budget) (0: no precomputed draw); the GenLevel table (level 0
+// is the empty one) and GenEntry table, each record held once however many
+// heads share it; gagp_domain[n_doms]; gagp_value[n_vals]; the minimum cost
+// table as uint16 (kNoMinimum16: infeasible).
+struct GenImage {
+  int32_t nt, head, level, entry, doms, vals, minimum, reserved;
+};
+constexpr uint16_t kNoMinimum16 = 0xffff;
+
 // A traversal table entry (the reference's PhaseRegionInfo for a traversal,
 // device/phase_compile.cuh:47-60) as lowering reads it: direction, the
 // binder numbers of element, index and state, the operand types the
@@ -105,13 +117,10 @@ struct SearchDesc {
   // minimum of each production's expression, production-major per (depth,
   // site budget): prod_minimum[(d * logical_count + l) * n_prods + p]
   const uint32_t* prod_minimum;
-  const GenExpr* gen_expr;
-  const GenNt* gen_nt;
-  // precomputed production draws: gen_level[(d * logical_count + l) * n_nts
-  // + nt] is the widest level of nonterminal nt at (depth d, site budget l);
-  // narrower levels follow the first depth_count * logical_count * n_nts
-  const GenLevel* gen_level;
-  const GenEntry* gen_entry;
+  // the subtree generator's tables (GenImage layout), gen_image_bytes long
+  const char* gen_image;
+  int32_t gen_image_bytes;
+  GenImage gi;
   const int32_t* local_types;          // ValueTag of each evaluator input
   const RegionInfo* regions;           // traversal table entries (TK_TRAVERSE operands)
   int32_t n_regions;
