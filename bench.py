@@ -511,9 +511,10 @@ def run_own_arm(args, rank: int, world: int, local: int):
         make_task(seed, d)
         tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
         with Engine(local if world > 1 else 0) as eng:
-            # e2e: whole searches through the C ABI from host buffers (median of 3)
+            # e2e: whole searches through the C ABI from host buffers (median of
+            # 3; --no-e2e, for profiler captures of the timed rounds, skips it)
             runs = []
-            for _ in range(3):
+            for _ in range(0 if args.no_e2e else 3):
                 lt = T.load(tp, sp)
                 moved0 = eng.transfers()
                 t0 = time.perf_counter()
@@ -530,8 +531,8 @@ def run_own_arm(args, rank: int, world: int, local: int):
                              "place_levels": eng.counters(s).get("place_levels")})
                 s.close()
             runs.sort(key=lambda r: r["seconds"])
-            mid = runs[1]
-            e2e = {"value": mid["program_cases"] / mid["seconds"], "unit": UNIT,
+            mid = runs[1] if runs else None
+            e2e = None if mid is None else {"value": mid["program_cases"] / mid["seconds"], "unit": UNIT,
                    "h2d_bytes_per_step": mid["h2d"], "d2h_bytes_per_step": mid["d2h"], "seconds": mid["seconds"],
                    "step": "one whole search (admission + %d rounds + result); median of 3" % WORKLOAD["generations"],
                    "all_seconds": [r["seconds"] for r in runs], "parts": mid["parts"],
@@ -784,6 +785,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the whole-search e2e leg (profiler captures)")
     ap.add_argument("--workload", default="poly4", choices=["poly4", "list", "batch", "serve"],
                     help="poly4: the large scalar search (default); list: the list-program search; "
                          "batch: 64-search batching mix; serve: open-loop serving stream")

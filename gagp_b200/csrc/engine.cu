@@ -222,6 +222,12 @@ void harvest(gagp_engine* e) {
   e->event_next = 0;
 }
 
+// Device counters of a round: per variation range c, [4c] and [4c+1] its
+// lowered-program list sizes (fast, exact) and [4c+2] its next child; then
+// [4 kChunks + 1] the size of the shared exact-VM list of a round whose
+// ranges hand their exact-VM programs to one launch.
+constexpr int kCountWords = 4 * gagp_engine::kChunks + 4;
+
 gagp_status ensure_lists(gagp_engine* e, size_t items) {
   if (items <= e->list_capacity) return GAGP_OK;
   if (e->d_fast) cudaFree(e->d_fast);
@@ -231,7 +237,7 @@ gagp_status ensure_lists(gagp_engine* e, size_t items) {
   const size_t cap = std::max<size_t>({items, size_t(1024), 2 * e->list_capacity});
   CUDA_TRY(cudaMalloc(&e->d_fast, cap * sizeof(gb::ProgramRef)));
   CUDA_TRY(cudaMalloc(&e->d_general, cap * sizeof(gb::ProgramRef)));
-  if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, 4 * gagp_engine::kChunks * sizeof(int32_t)));
+  if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, kCountWords * sizeof(int32_t)));
   e->list_capacity = cap;
   return GAGP_OK;
 }
@@ -1232,8 +1238,8 @@ VmPlan plan_vm(gagp_engine* e, const BatchView& v, bool may_measure) {
   return p;
 }
 
-gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t stream, const gb::ProgramRef* fast,
-                      const gb::ProgramRef* general, const int32_t* counts, const VmPlan& plan) {
+gagp_status launch_vm_fast(gagp_engine* e, const BatchView& v, int mode, cudaStream_t stream, const gb::ProgramRef* fast,
+                           const int32_t* counts, const VmPlan& plan) {
   const int warps = 8;
   const int temp_stride = gb::kMaxTemps * plan.lanes * 32;
   const int code_stride = (v.max_code_stride + 1) & ~1;  // uint2 slots, in int64 units
@@ -1262,6 +1268,13 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
     e->tune_marks.push_back({plan.measure_key, plan.cand, mark_start, mark_stop});
     ++e->vm_tune[plan.measure_key].pending;
   }
+  return GAGP_OK;
+}
+
+// Both VMs over one range's lists: counts[0] fast programs, counts[1] exact.
+gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t stream, const gb::ProgramRef* fast,
+                      const gb::ProgramRef* general, const int32_t* counts, const VmPlan& plan) {
+  if (const gagp_status st = launch_vm_fast(e, v, mode, stream, fast, counts, plan); st != GAGP_OK) return st;
   Timed t(e, KN_VM_GENERAL, stream);
   return vm_general_launch(e->sm_count, stream, v.d_desc, mode, general, counts, v.max_bc_stride, v.exact_heavy);
 }
@@ -1272,11 +1285,13 @@ gagp_status launch_start(gagp_engine* e, const BatchView& v) {
   {
     Timed t(e, KN_LOWER);
     gb::k_lower<<<blocks_for(v.total_members, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(
-        v.d_desc, v.d_member_off, v.n, 0, e->d_fast, e->d_general, e->d_counts, 0, v.total_members);
+        v.d_desc, v.d_member_off, v.n, 0, e->d_fast, e->d_general, e->d_counts, e->d_counts + 1, 0, v.total_members);
   }
   VmPlan start_plan;
   start_plan.lanes = v.max_lanes;
-  launch_vm(e, v, 0, e->stream, e->d_fast, e->d_general, e->d_counts, start_plan);
+  if (const gagp_status st = launch_vm(e, v, 0, e->stream, e->d_fast, e->d_general, e->d_counts, start_plan);
+      st != GAGP_OK)
+    return st;
   { Timed t(e, KN_KEYS); gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   { Timed t(e, KN_START); gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
@@ -1316,7 +1331,7 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
   }
   // per range c: counts[4c] / [4c+1] lowered-program list sizes, [4c+2] the
   // next child of the variation warps; range c's lists start at item lo
-  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 4 * gagp_engine::kChunks * sizeof(int32_t), e->stream));
+  CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, kCountWords * sizeof(int32_t), e->stream));
   CUDA_TRY(cudaEventRecord(e->chunk_fork, e->stream));
   const int chunks = v.total_children >= 4096 ? gagp_engine::kChunks : 1;
   const int warps = 4;
@@ -1339,6 +1354,12 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     }
   }
   const size_t vary_smem = warps * gb::warp_rows_bytes(v.max_stride) + image_max;
+  // rounds whose programs rarely need the exact VM list them in one shared
+  // list, run by one launch once the ranges have joined: a per-range launch,
+  // mostly empty, would still wait for an SM with room for its shared memory
+  // on every range's critical path
+  const bool shared_exact = chunks > 1 && !v.exact_heavy;
+  int32_t* shared_count = e->d_counts + 4 * gagp_engine::kChunks;
   int per_sm = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vary, warps * 32, vary_smem));
   for (int c = 0; c < chunks; ++c) {
@@ -1360,13 +1381,28 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     {
       Timed t(e, KN_LOWER, st);
       gb::k_lower<<<blocks_for(hi - lo, gb::kLowerWarps), gb::kLowerWarps * 32, 0, st>>>(
-          v.d_desc, v.d_child_off, v.n, 1, e->d_fast + lo, e->d_general + lo, counts, lo, hi);
+          v.d_desc, v.d_child_off, v.n, 1, e->d_fast + lo, shared_exact ? e->d_general : e->d_general + lo, counts,
+          shared_exact ? shared_count + 1 : counts + 1, lo, hi);
     }
-    launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts, vm);
+    if (shared_exact) {
+      if (const gagp_status st2 = launch_vm_fast(e, v, 1, st, e->d_fast + lo, counts, vm); st2 != GAGP_OK) return st2;
+    } else {
+      if (const gagp_status st2 = launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts, vm);
+          st2 != GAGP_OK)
+        return st2;
+    }
     if (chunks > 1) {
       CUDA_TRY(cudaEventRecord(e->chunk_done[c], st));
       CUDA_TRY(cudaStreamWaitEvent(e->stream, e->chunk_done[c], 0));
     }
+  }
+  if (shared_exact) {
+    // the few programs past the accumulator VM, all ranges' at once
+    Timed t(e, KN_VM_GENERAL);
+    if (const gagp_status st2 = vm_general_launch(e->sm_count, e->stream, v.d_desc, 1, e->d_general, shared_count,
+                                                  v.max_bc_stride, false);
+        st2 != GAGP_OK)
+      return st2;
   }
   if (v.generational) {
     // every child becomes the member of its index (reproduce's swap), after
@@ -1712,7 +1748,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   gb::ProgramRef* general = at<gb::ProgramRef>(b, p.general);
   int32_t* counts = at<int32_t>(b, p.counts);
   gb::k_lower<<<blocks_for(R, gb::kLowerWarps), gb::kLowerWarps * 32, 0, stream>>>(dd, doff, 1, 0, fast, general, counts,
-                                                                                  0, R);
+                                                                                  counts + 1, 0, R);
   const int warps = 8;
   const int lanes = d.vm_cases_per_lane;
   const int temp_stride = gb::kMaxTemps * lanes * 32;
@@ -2201,7 +2237,8 @@ struct Request {
   std::vector<gagp_domain> doms;
   std::vector<gagp_value> vals;
   std::vector<uint32_t> minimum;
-  std::vector<int64_t> inputs, expected;
+  std::vector<gagp_region> regions;
+  std::vector<int64_t> inputs, expected, lists;
   std::vector<int32_t> tags;
   gagp_grammar grammar{};
   gagp_cases cases{};
@@ -2337,6 +2374,7 @@ gagp_status gagp_b200_server_submit(gagp_server* sv, const gagp_grammar* g, cons
   r->doms = copy_of(g->domains, g->domain_count);
   r->vals = copy_of(g->values, g->value_count);
   r->minimum = copy_of(g->minimum, g->expression_count * g->depth_count * g->logical_depth_count);
+  r->regions = copy_of(g->regions, g->region_count);
   r->grammar = *g;
   r->grammar.expressions = r->ex.data();
   r->grammar.productions = r->prods.data();
@@ -2344,13 +2382,16 @@ gagp_status gagp_b200_server_submit(gagp_server* sv, const gagp_grammar* g, cons
   r->grammar.domains = r->doms.data();
   r->grammar.values = r->vals.data();
   r->grammar.minimum = r->minimum.data();
+  r->grammar.regions = r->regions.empty() ? nullptr : r->regions.data();
   r->inputs = copy_of(c->inputs, c->case_count * c->input_count);
+  r->lists = copy_of(c->list_values, c->list_values ? int(c->list_value_count) : 0);
   r->expected = copy_of(c->expected, c->case_count);
   r->tags = copy_of(c->input_tags, c->input_count);
   r->cases = *c;
   r->cases.inputs = r->inputs.data();
   r->cases.expected = r->expected.data();
   r->cases.input_tags = r->tags.empty() ? nullptr : r->tags.data();
+  r->cases.list_values = r->lists.empty() ? nullptr : r->lists.data();
   r->config = *cfg;
   r->bytes = p.L.total;
   r->submitted = sv->now();

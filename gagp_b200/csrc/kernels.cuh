@@ -68,12 +68,14 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
 // ----------------------------------------------------------- lowering
 // mode 0: the members (initial evaluation); mode 1: this round's children
 // that reuse no member's result; batch items [lo, hi).  One warp per row:
-// the accumulator program when the row is total and fits the fuel, else the
-// reference bytecode for the general VM (lane 0).
+// the accumulator program when the row is total and fits the fuel (listed in
+// fast_list, counted in list_count[0]), else the reference bytecode for the
+// general VM (lane 0; listed in general_list, counted in *general_count).
 constexpr int kLowerWarps = 4;
 __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* descs, const int32_t* off, int n,
                                                             int mode, ProgramRef* fast_list, ProgramRef* general_list,
-                                                            int32_t* list_count, int lo, int hi) {
+                                                            int32_t* list_count, int32_t* general_count, int lo,
+                                                            int hi) {
   __shared__ LowerScratch scratch[kLowerWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int total_items = min(off[n], hi);
@@ -132,7 +134,7 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
         s.bc_len[slot] = bl;
         s.bc_locals[slot] = r.locals | (r.stack_bound << 8);
         s.code_temps[slot] = -1;
-        general_list[atomicAdd(&list_count[1], 1)] = ProgramRef{si, slot};
+        general_list[atomicAdd(general_count, 1)] = ProgramRef{si, slot};
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
                   (unsigned long long)(row_bytes + 20ull * bl + 8ull * r.constants + 16));
       }

@@ -49,6 +49,37 @@ __device__ __forceinline__ Entrant warp_best_entrant(Entrant e) {
 __device__ inline void warp_tournaments(const SearchDesc& s, Rng& random, int* parent, int* donor) {
   const int lane = lane_id();
   const int p = s.pressure, total = 2 * p;
+  if (p <= 16) {
+    // both tournaments in aligned power-of-two lane segments (the parent's
+    // entrants from lane 0, the donor's from lane `seg`): log2(seg) steps of
+    // a segmented shuffle reduction, then each winner from its lane
+    int seg = 1;
+    while (seg < p) seg <<= 1;
+    int mine = 0;
+    for (int j = 0; j < total; ++j) {
+      const int d = int(random.bounded_fixed(uint64_t(s.P), s.bounded_threshold, s.mod_magic));
+      if ((j < p ? j : seg + j - p) == lane) mine = d;
+    }
+    const int position = lane < seg ? lane : lane - seg;
+    const bool live = lane < 2 * seg && position < p;
+    uint64_t key = live ? s.key[mine] : ~0ULL;
+    uint32_t tie = live ? (s.has_wrong ? uint32_t(mine) : uint32_t(position)) : ~0u;
+    int from = lane;
+    for (int o = 1; o < seg; o <<= 1) {
+      const uint64_t k2 = __shfl_xor_sync(kFull, key, o);
+      const uint32_t t2 = __shfl_xor_sync(kFull, tie, o);
+      const int f2 = __shfl_xor_sync(kFull, from, o);
+      if (k2 < key || (k2 == key && t2 < tie)) {
+        key = k2;
+        tie = t2;
+        from = f2;
+      }
+    }
+    const int parent_lane = __shfl_sync(kFull, from, 0), donor_lane = __shfl_sync(kFull, from, seg);
+    *parent = __shfl_sync(kFull, mine, parent_lane);
+    *donor = __shfl_sync(kFull, mine, donor_lane);
+    return;
+  }
   Entrant best[2] = {{0, 0, 0, false}, {0, 0, 0, false}};
   for (int base = 0; base < total; base += 32) {
     const int n = min(32, total - base);

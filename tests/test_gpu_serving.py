@@ -110,3 +110,30 @@ def test_cancel_and_decline():
         with pytest.raises(EngineError) as err:
             server.submit(generational)
         assert err.value.status == 1  # GAGP_DECLINED
+
+
+def test_list_requests_equal_alone():
+    """List programs through the server: a request owns copies of every
+    table and case array it was submitted with (the traversal table and the
+    IntList values included), so it runs the same search whenever the server
+    admits it."""
+    from gagp_b200 import build
+    from gagp_b200.engine import Engine, Server
+    build.build()
+    shapes = [(128, 12, 3, 21), (200, 20, 4, 22), (96, 16, 3, 23)]
+    make = lambda p, c, g, s: T.from_files(W.list_threshold(population=p, generations=g, seed=s, cases=c))  # noqa: E731
+    with Engine(0) as engine:
+        alone = []
+        for shape in shapes:
+            s = engine.admit(make(*shape))
+            s.run()
+            alone.append(s.result())
+            s.close()
+        with Server(engine, max_active=1, rounds_per_step=3) as server:
+            # the tasks' own buffers go away after submit; later admissions
+            # read the server's copies
+            tickets = {i: server.submit(make(*shape)) for i, shape in enumerate(shapes)}
+            finished = _drain(server, tickets)
+    assert sorted(finished) == list(range(len(shapes)))
+    for i, result in finished.items():
+        assert result == alone[i], i
