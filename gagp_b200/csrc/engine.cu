@@ -1354,11 +1354,16 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     }
   }
   const size_t vary_smem = warps * gb::warp_rows_bytes(v.max_stride) + image_max;
-  // rounds whose programs rarely need the exact VM list them in one shared
-  // list, run by one launch once the ranges have joined: a per-range launch,
-  // mostly empty, would still wait for an SM with room for its shared memory
-  // on every range's critical path
-  const bool shared_exact = chunks > 1 && !v.exact_heavy;
+  // With ranges, the VM that a round rarely needs gets one launch for all
+  // ranges once they have joined: the exact VM in rounds of mostly
+  // accumulator programs, and in rounds of mostly exact-VM programs (list
+  // programs) both, so that the exact VM's persistent blocks see every
+  // program at once.  A per-range launch, mostly empty, still waits for SM
+  // room (shared memory) behind the other ranges' VM blocks, on its range's
+  // critical path.  The lowering then lists those programs in one shared
+  // list (counts at shared_count: [0] fast, [1] exact).
+  const bool shared_exact = chunks > 1;
+  const bool shared_fast = chunks > 1 && v.exact_heavy;
   int32_t* shared_count = e->d_counts + 4 * gagp_engine::kChunks;
   int per_sm = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gb::k_vary, warps * 32, vary_smem));
@@ -1381,10 +1386,13 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     {
       Timed t(e, KN_LOWER, st);
       gb::k_lower<<<blocks_for(hi - lo, gb::kLowerWarps), gb::kLowerWarps * 32, 0, st>>>(
-          v.d_desc, v.d_child_off, v.n, 1, e->d_fast + lo, shared_exact ? e->d_general : e->d_general + lo, counts,
+          v.d_desc, v.d_child_off, v.n, 1, shared_fast ? e->d_fast : e->d_fast + lo,
+          shared_exact ? e->d_general : e->d_general + lo, shared_fast ? shared_count : counts,
           shared_exact ? shared_count + 1 : counts + 1, lo, hi);
     }
-    if (shared_exact) {
+    if (shared_fast) {
+      // both VMs after the join
+    } else if (shared_exact) {
       if (const gagp_status st2 = launch_vm_fast(e, v, 1, st, e->d_fast + lo, counts, vm); st2 != GAGP_OK) return st2;
     } else {
       if (const gagp_status st2 = launch_vm(e, v, 1, st, e->d_fast + lo, e->d_general + lo, counts, vm);
@@ -1397,10 +1405,14 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
     }
   }
   if (shared_exact) {
-    // the few programs past the accumulator VM, all ranges' at once
+    // all ranges' exact-VM programs (and, in exact-heavy rounds, their
+    // accumulator programs) at once
+    if (shared_fast)
+      if (const gagp_status st2 = launch_vm_fast(e, v, 1, e->stream, e->d_fast, shared_count, vm); st2 != GAGP_OK)
+        return st2;
     Timed t(e, KN_VM_GENERAL);
     if (const gagp_status st2 = vm_general_launch(e->sm_count, e->stream, v.d_desc, 1, e->d_general, shared_count,
-                                                  v.max_bc_stride, false);
+                                                  v.max_bc_stride, v.exact_heavy);
         st2 != GAGP_OK)
       return st2;
   }
