@@ -183,10 +183,11 @@ __device__ __forceinline__ LevelView load_level(const GenLevel* p) {
 // Tasks pack (expression:17, depth:7, scope_count:4, logical:4) in `pending`
 // (192 entries).  Emitted words carry depth relative to the generated root
 // (root = 1) and site depth relative to the budget `logical_depth`.
-__device__ inline GenResult generate(const SearchDesc& s, const GenTables& tables, int root_expression, int scope_count,
+__device__ inline GenResult generate(const SearchDesc& s, const char* image, int root_expression, int scope_count,
                                      int depth, int capacity, uint64_t seed, uint64_t* out_node, int64_t* out_cval,
                                      int logical_depth, uint64_t* pending) {
   GenResult result{ST_INVALID, 0, 0, 0};
+  const GenTables tables = gen_tables(s, image);
   // the tables (staged in shared memory by the variation kernel), read once
   // into registers; the sequential draw's production tables stay global
   const GenExpr* __restrict__ gx = tables.gx;

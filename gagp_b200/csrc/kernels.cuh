@@ -51,7 +51,7 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
   GenResult g{ST_INVALID, 0, 0, 0};
   for (int logical = ramp, attempt = 0; g.status != ST_OK; ++attempt) {
     const int room = s.maxv < kCapacity ? s.maxv : kCapacity;
-    g = generate(s, gen_tables(s, s.gen_image), s.root_expression, 0, s.slot_max_depth, room,
+    g = generate(s, s.gen_image, s.root_expression, 0, s.slot_max_depth, room,
                  mix64(s.seed ^ mix64((uint64_t(i) * 8 + 0) * 64 + uint64_t(attempt))), node, cval, logical, pending);
     if (g.status != ST_OK && attempt % 4 == 3 && logical < site_limit) ++logical;
     if (attempt >= 256 && g.status != ST_OK) {
@@ -167,12 +167,13 @@ __device__ __forceinline__ void store_result(const SearchDesc& s, int mode, int 
 // fast VM, so that the interpreters' registers and local arrays do not
 // lower the fast VM's occupancy.
 //
-// Dynamic shared memory: constants (bc_stride_max int64), the 5-int code
-// (bc_stride_max instructions), the staged SIMD words (bc_stride_max uint2)
-// and per warp kSimdSlots x 32 int64 slots.
+// Dynamic shared memory: constants (bc_stride_max int64), the staged SIMD
+// words (bc_stride_max uint4), the 5-int code (bc_stride_max instructions),
+// a jump-target bit per instruction and per warp kSimdSlots x 32 int64 slots.
 constexpr int kGeneralWarps = 8;
 __host__ __device__ __forceinline__ size_t general_smem_bytes(int bc_stride_max) {
-  return size_t(bc_stride_max) * (8 + 20 + 8) + 16 + size_t(kGeneralWarps) * kSimdSlots * 32 * 8;
+  return size_t(bc_stride_max) * (8 + 16 + 20) + 8 * ((size_t(bc_stride_max) + 63) / 64) + 16 +
+         size_t(kGeneralWarps) * kSimdSlots * 32 * 8;
 }
 __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchDesc* descs, int mode,
                                                                    const ProgramRef* list, const int32_t* list_count,
@@ -182,9 +183,11 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
   __shared__ uint32_t red_wrong[kGeneralWarps], red_errors[kGeneralWarps];
   __shared__ unsigned long long red_steps[kGeneralWarps];
   int64_t* consts = smem_general;
-  uint2* words = reinterpret_cast<uint2*>(smem_general + bc_stride_max);
-  int32_t* code = reinterpret_cast<int32_t*>(smem_general + 2 * size_t(bc_stride_max));
-  int64_t* slots_all = smem_general + 2 * size_t(bc_stride_max) + (5 * size_t(bc_stride_max) + 1) / 2;
+  uint4* words = reinterpret_cast<uint4*>(smem_general + bc_stride_max);
+  int32_t* code = reinterpret_cast<int32_t*>(smem_general + 3 * size_t(bc_stride_max));
+  unsigned long long* targets =
+      reinterpret_cast<unsigned long long*>(smem_general + 3 * size_t(bc_stride_max) + (5 * size_t(bc_stride_max) + 1) / 2);
+  int64_t* slots_all = reinterpret_cast<int64_t*>(targets + (size_t(bc_stride_max) + 63) / 64);
   const int count = *list_count;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t* slots = slots_all + size_t(warp) * kSimdSlots * 32;
@@ -202,13 +205,14 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
         consts[k] = gconsts[k];  // at most one constant per instruction
         const int32_t* x = gcode + 5 * k;
         const int cost = x[4];
-        simd_ok &= cost >= 1 && cost <= 255 && x[3] >= 0 && x[3] <= 255;
-        words[k] = make_uint2(uint32_t(x[0] & 0xff) | (uint32_t(x[1] & 0xff) << 8) | (uint32_t(x[3] & 0xff) << 16) |
-                                  (uint32_t(cost & 0xff) << 24),
-                              uint32_t(x[2]));
+        simd_ok &= cost >= 1 && cost <= 255 && x[0] >= 0 && x[0] < 64;
+        words[k] = simd_plain(x[0], x[2], cost);
       }
+      for (int k = threadIdx.x; k < (n + 63) / 64; k += blockDim.x) targets[k] = 0;
     }
     simd_ok = __syncthreads_and(simd_ok);
+    if (simd_ok && threadIdx.x == 0) simd_fuse(code, n, words, targets);
+    __syncthreads();
     const VmView view = vm_view(s);
     int64_t loss = 0;
     uint32_t wrong = 0, errors = 0;
@@ -639,8 +643,8 @@ __global__ void __launch_bounds__(128, 6) k_vary(const SearchDesc* descs, const 
     int reuse = -1, parent = -1;
     long long stamp[5] = {0, 0, 0, 0, 0};
     const long long started = clock64();
-    const GenTables tables = gen_tables(s, si == staged ? image : s.gen_image);
-    const int error = warp_vary_child(s, tables, child, s.round_seed[0], rows, &reuse, &parent, stamp);
+    const int error = warp_vary_child(s, si == staged ? image : s.gen_image, child, s.round_seed[0], rows, &reuse,
+                                      &parent, stamp);
     if (lane == 0 && collect_stats) {
       // per-phase SM cycles: selection, crossover, subtree generation, rest
       stamp[3] = clock64();

@@ -215,7 +215,7 @@ __device__ inline int warp_find_member(const SearchDesc& s, const SRow& row) {
 // after selection, after crossover, after the mutation's subtree generation
 // (left 0 for phases not reached); stamp[4]: the generation's steps + 1 on
 // lane 0 (left 0 without a generation).
-__device__ inline int warp_vary_child(const SearchDesc& s, const GenTables& tables, int child, uint64_t seed, WarpRows& w,
+__device__ inline int warp_vary_child(const SearchDesc& s, const char* image, int child, uint64_t seed, WarpRows& w,
                                       int* reuse_out, int* parent_out, long long* stamp) {
   const int lane = lane_id();
   *reuse_out = -1;
@@ -275,7 +275,7 @@ __device__ inline int warp_vary_child(const SearchDesc& s, const GenTables& tabl
         const uint64_t gseed = m.next();
         GenResult g{ST_INVALID, 0, 0, 0};
         if (lane == 0) {
-          g = generate(s, tables, entry, 0, s.slot_max_depth - depth + 1, bounded, gseed, w.gen.node, w.gen.cval,
+          g = generate(s, image, entry, 0, s.slot_max_depth - depth + 1, bounded, gseed, w.gen.node, w.gen.cval,
                        logical, w.pending);
           stamp[4] = (long long)g.steps + 1;
         }

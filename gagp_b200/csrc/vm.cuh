@@ -522,12 +522,111 @@ __host__ __device__ inline bool run_program(const VmView& v, const int32_t* code
 // tag is the phase's type; the checks that can fail on some case -- fuel,
 // modulo by zero, index range -- are kept.  Results equal run_program's.
 //
-// Staged instruction word: x = op | flags << 8 | b << 16 | cost << 24,
-// y = a.  The kernel stages a program this way only when every cost is in
-// 1..255 and its locals and stack fit kSimdSlots; otherwise it runs it on
-// run_program.
+// Staged instruction (uint4): x = op (bits 0-6) | jump when true (bit 7) |
+// instructions it stands for (bits 8-11) | binary operation (bits 12-15) |
+// their summed fuel (bits 16-31); y, z, w: operands.  The kernel stages a
+// program this way only when every cost is in 1..255 and its locals and
+// stack fit kSimdSlots; otherwise it runs it on run_program.
+//
+// Superinstructions.  One thread of the block fuses, left to right, short
+// straight-line runs that start anywhere but hold no jump target past their
+// first instruction: LOAD a; LOAD b; op; STORE c (S_BIN_LL_ST), the same
+// with PUSH_CONST k for the second load (S_BIN_LC_ST), LOAD a; LOAD b / PUSH
+// k; comparison; JMP_IF_FALSE/TRUE t (S_JCMP_LL / S_JCMP_LC), LOAD a; LOAD b;
+// CALL index; STORE c (S_INDEX_LL_ST), the three-instruction prefixes of the
+// binary forms (S_BIN_LL, S_BIN_LC), op; STORE c (S_BIN_ST) and LOAD a;
+// STORE c (S_MOVE).  A fused instruction charges the summed fuel before it
+// runs (a timeout anywhere inside the run, or an error of one of its
+// instructions, ends the case with an error in both forms, and otherwise
+// every instruction runs) and counts as the instructions it stands for.  The
+// skipped slots are never reached: jumps land only on run starts.
+enum : int {
+  S_MOVE = 64, S_BIN_LL, S_BIN_LC, S_BIN_LL_ST, S_BIN_LC_ST, S_JCMP_LL, S_JCMP_LC, S_INDEX_LL_ST, S_BIN_ST
+};
 constexpr int kSimdSlots = 24;
 constexpr int kSimdDone = 0x7fffffff;
+
+__device__ __forceinline__ uint4 simd_plain(int op, int a, int cost) {
+  return make_uint4(uint32_t(op & 0x7f) | (1u << 8) | (uint32_t(cost) << 16), uint32_t(a), 0u, 0u);
+}
+__device__ __forceinline__ bool simd_binary_op(int op) {
+  return op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_MOD || (op >= OP_LT && op <= OP_NE);
+}
+__device__ __forceinline__ bool simd_compare_op(int op) { return op >= OP_LT && op <= OP_NE; }
+// One binary operation of the reference VM on Int payloads (comparisons give
+// 0/1); false on a modulo by zero (ZeroDiv).
+__device__ __forceinline__ bool simd_binary(int op, int64_t x, int64_t y, int64_t& r) {
+  switch (op) {
+    case OP_ADD: r = wrap_add(x, y); return true;
+    case OP_SUB: r = wrap_sub(x, y); return true;
+    case OP_MUL: r = wrap_mul(x, y); return true;
+    case OP_MOD:
+      if (y == 0) return false;
+      r = py_mod(x, y);
+      return true;
+    case OP_LT: r = x < y; return true;
+    case OP_LE: r = x <= y; return true;
+    case OP_GT: r = x > y; return true;
+    case OP_GE: r = x >= y; return true;
+    case OP_EQ: r = x == y; return true;
+    default: r = x != y; return true;
+  }
+}
+
+// The fusion pass over a staged program (code: 5 ints per instruction; words
+// hold the plain staging; targets: n bits, zeroed).  One thread.
+__device__ inline void simd_fuse(const int32_t* code, int n, uint4* words, unsigned long long* targets) {
+  auto op_at = [&](int k) { return code[5 * k]; };
+  auto a_at = [&](int k) { return code[5 * k + 2]; };
+  auto cost_at = [&](int k) { return uint32_t(code[5 * k + 4]); };
+  for (int k = 0; k < n; ++k) {
+    const int op = op_at(k), t = a_at(k);
+    if ((op == OP_JMP || op == OP_JMP_IF_FALSE || op == OP_JMP_IF_TRUE) && t >= 0 && t < n)
+      targets[t >> 6] |= 1ull << (t & 63);
+  }
+  // instructions k+1 .. k+len-1 exist and none is a jump target
+  auto free_run = [&](int k, int len) {
+    if (k + len > n) return false;
+    for (int j = 1; j < len; ++j)
+      if (targets[(k + j) >> 6] >> ((k + j) & 63) & 1) return false;
+    return true;
+  };
+  auto fused = [&](int k, int len, int op, int bop, bool jt, uint32_t y, uint32_t z, uint32_t w) {
+    uint32_t cost = 0;
+    for (int j = 0; j < len; ++j) cost += cost_at(k + j);
+    words[k] = make_uint4(uint32_t(op) | (uint32_t(jt) << 7) | (uint32_t(len) << 8) | (uint32_t(bop - OP_ADD) << 12) |
+                              (cost << 16),
+                          y, z, w);
+  };
+  for (int k = 0; k < n;) {
+    const int o0 = op_at(k), o1 = k + 1 < n ? op_at(k + 1) : -1, o2 = k + 2 < n ? op_at(k + 2) : -1,
+              o3 = k + 3 < n ? op_at(k + 3) : -1;
+    const bool second = o1 == OP_LOAD || o1 == OP_PUSH_CONST;
+    int len = 1;
+    if (o0 == OP_LOAD && second && simd_binary_op(o2) && o3 == OP_STORE && free_run(k, 4)) {
+      fused(k, 4, o1 == OP_LOAD ? S_BIN_LL_ST : S_BIN_LC_ST, o2, false, a_at(k), a_at(k + 1), a_at(k + 3));
+      len = 4;
+    } else if (o0 == OP_LOAD && second && simd_compare_op(o2) && (o3 == OP_JMP_IF_FALSE || o3 == OP_JMP_IF_TRUE) &&
+               free_run(k, 4)) {
+      fused(k, 4, o1 == OP_LOAD ? S_JCMP_LL : S_JCMP_LC, o2, o3 == OP_JMP_IF_TRUE, a_at(k), a_at(k + 1), a_at(k + 3));
+      len = 4;
+    } else if (o0 == OP_LOAD && o1 == OP_LOAD && o2 == OP_CALL_BUILTIN && a_at(k + 2) == B_INDEX && o3 == OP_STORE &&
+               free_run(k, 4)) {
+      fused(k, 4, S_INDEX_LL_ST, OP_ADD, false, a_at(k), a_at(k + 1), a_at(k + 3));
+      len = 4;
+    } else if (o0 == OP_LOAD && second && simd_binary_op(o2) && free_run(k, 3)) {
+      fused(k, 3, o1 == OP_LOAD ? S_BIN_LL : S_BIN_LC, o2, false, a_at(k), a_at(k + 1), 0);
+      len = 3;
+    } else if (simd_binary_op(o0) && o1 == OP_STORE && free_run(k, 2)) {
+      fused(k, 2, S_BIN_ST, o0, false, a_at(k + 1), 0, 0);
+      len = 2;
+    } else if (o0 == OP_LOAD && o1 == OP_STORE && free_run(k, 2)) {
+      fused(k, 2, S_MOVE, OP_ADD, false, a_at(k), a_at(k + 1), 0);
+      len = 2;
+    }
+    k += len;
+  }
+}
 
 struct SimdCase {
   int64_t value;
@@ -535,7 +634,7 @@ struct SimdCase {
   uint32_t steps;
 };
 
-__device__ inline SimdCase run_program_simd(const VmView& v, const uint2* code, int n, const int64_t* consts,
+__device__ inline SimdCase run_program_simd(const VmView& v, const uint4* code, int n, const int64_t* consts,
                                             int n_locals, int c, bool live, int64_t* slots) {
   const int lane = threadIdx.x & 31;
   SimdCase out{0, false, 0};
@@ -548,13 +647,13 @@ __device__ inline SimdCase run_program_simd(const VmView& v, const uint2* code, 
     const int ipm = __reduce_min_sync(kFull, ip);
     if (ipm == kSimdDone) break;
     if (ip != ipm) continue;
-    const uint2 w = code[ipm];
-    const int op = int(w.x & 0xffu), flags = int((w.x >> 8) & 0xffu), b = int((w.x >> 16) & 0xffu);
-    const int cost = int(w.x >> 24), a = int(w.y);
+    const uint4 w = code[ipm];
+    const int op = int(w.x & 0x7fu), len = int((w.x >> 8) & 0xfu), bop = OP_ADD + int((w.x >> 12) & 0xfu);
+    const int cost = int(w.x >> 16), a = int(w.y);
     if (fuel < cost) { ip = kSimdDone; continue; }  // Timeout
     fuel -= cost;
-    ++out.steps;
-    ++ip;
+    out.steps += len;
+    ip += len;
     switch (op) {
       case OP_PUSH_CONST: at(sp++) = consts[a]; break;
       case OP_LOAD: { const int64_t x = at(a); at(sp++) = x; break; }
@@ -562,17 +661,12 @@ __device__ inline SimdCase run_program_simd(const VmView& v, const uint2* code, 
       case OP_CHECK_INT: break;
       case OP_NEG: at(sp - 1) = wrap_neg(at(sp - 1)); break;
       case OP_NOT: at(sp - 1) ^= 1; break;
-      case OP_ADD: case OP_SUB: case OP_MUL: case OP_MOD: {
-        const int64_t y = at(--sp), x = at(sp - 1);
-        if (op == OP_MOD && y == 0) { ip = kSimdDone; break; }  // ZeroDiv
-        at(sp - 1) = op == OP_ADD ? wrap_add(x, y) : op == OP_SUB ? wrap_sub(x, y) : op == OP_MUL ? wrap_mul(x, y)
-                                                                                              : py_mod(x, y);
-        break;
-      }
+      case OP_ADD: case OP_SUB: case OP_MUL: case OP_MOD:
       case OP_LT: case OP_LE: case OP_GT: case OP_GE: case OP_EQ: case OP_NE: {
         const int64_t y = at(--sp), x = at(sp - 1);
-        at(sp - 1) = op == OP_LT ? x < y : op == OP_LE ? x <= y : op == OP_GT ? x > y : op == OP_GE ? x >= y
-                   : op == OP_EQ ? x == y : x != y;
+        int64_t r;
+        if (!simd_binary(op, x, y, r)) { ip = kSimdDone; break; }  // ZeroDiv
+        at(sp - 1) = r;
         break;
       }
       case OP_JMP: ip = a; break;
@@ -586,9 +680,9 @@ __device__ inline SimdCase run_program_simd(const VmView& v, const uint2* code, 
         if (a == B_LEN) {
           r = __ldg(&v.lists[at(sp - 1)]);
         } else if (a == B_INDEX) {
-          const int64_t j0 = at(--sp), h = at(sp - 1), len = __ldg(&v.lists[h]);
-          const int64_t j = j0 < 0 ? j0 + len : j0;
-          if (j < 0 || j >= len) { ip = kSimdDone; break; }  // index out of range
+          const int64_t j0 = at(--sp), h = at(sp - 1), len_h = __ldg(&v.lists[h]);
+          const int64_t j = j0 < 0 ? j0 + len_h : j0;
+          if (j < 0 || j >= len_h) { ip = kSimdDone; break; }  // index out of range
           r = __ldg(&v.lists[h + 1 + j]);
         } else if (a == B_ABS) {
           const int64_t x = at(sp - 1);
@@ -606,11 +700,39 @@ __device__ inline SimdCase run_program_simd(const VmView& v, const uint2* code, 
         out.ok = true;
         ip = kSimdDone;
         break;
+      case S_MOVE: at(int(w.z)) = at(a); break;
+      case S_BIN_LL: case S_BIN_LC: case S_BIN_LL_ST: case S_BIN_LC_ST: {
+        const int64_t x = at(a), y = (op == S_BIN_LL || op == S_BIN_LL_ST) ? at(int(w.z)) : consts[w.z];
+        int64_t r;
+        if (!simd_binary(bop, x, y, r)) { ip = kSimdDone; break; }  // ZeroDiv
+        if (op == S_BIN_LL || op == S_BIN_LC) at(sp++) = r;
+        else at(int(w.w)) = r;
+        break;
+      }
+      case S_JCMP_LL: case S_JCMP_LC: {
+        const int64_t x = at(a), y = op == S_JCMP_LL ? at(int(w.z)) : consts[w.z];
+        int64_t r;
+        simd_binary(bop, x, y, r);  // a comparison: never fails
+        if ((r != 0) == bool(w.x & 0x80u)) ip = int(w.w);
+        break;
+      }
+      case S_INDEX_LL_ST: {
+        const int64_t h = at(a), j0 = at(int(w.z)), len_h = __ldg(&v.lists[h]);
+        const int64_t j = j0 < 0 ? j0 + len_h : j0;
+        if (j < 0 || j >= len_h) { ip = kSimdDone; break; }  // index out of range
+        at(int(w.w)) = __ldg(&v.lists[h + 1 + j]);
+        break;
+      }
+      case S_BIN_ST: {
+        const int64_t y = at(--sp), x = at(--sp);
+        int64_t r;
+        if (!simd_binary(bop, x, y, r)) { ip = kSimdDone; break; }  // ZeroDiv
+        at(a) = r;
+        break;
+      }
       default:
         ip = kSimdDone;  // not emitted by the lowering
     }
-    (void)flags;
-    (void)b;
   }
   return out;
 }
