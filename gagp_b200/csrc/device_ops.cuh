@@ -24,8 +24,8 @@ namespace gb {
 
 // PhaseExpressionKind / PhaseTreeKind / status codes (reference enums).
 enum { EK_OPERATION = 0, EK_CONSTANT = 1, EK_BOUND = 2, EK_REFERENCE = 3, EK_INPUT = 4, EK_ALIAS = 5 };
-enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5, TK_BOUND = 14,
-       TK_TRAVERSE = 16 };
+enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5, TK_LET = 13,
+       TK_BOUND = 14, TK_TRAVERSE = 16 };
 enum { ST_OK = 0, ST_INVALID = 1, ST_UNSUPPORTED = 2, ST_CAPACITY = 3 };
 constexpr int kFixedSite = 1 << 30;
 constexpr uint32_t kNoClass = 0x7ffu;

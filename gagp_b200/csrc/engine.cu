@@ -304,8 +304,12 @@ gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
       return fail(GAGP_DECLINED, "arity capacity");
     }
     if (e.kind == gb::EK_OPERATION && e.node_kind != gb::TK_OPERATION && e.node_kind != gb::TK_IF &&
-        e.node_kind != gb::TK_AND && e.node_kind != gb::TK_OR && e.node_kind != gb::TK_TRAVERSE)
-      return fail(GAGP_DECLINED, "statements and lets are outside the resident subset");
+        e.node_kind != gb::TK_AND && e.node_kind != gb::TK_OR && e.node_kind != gb::TK_TRAVERSE &&
+        e.node_kind != gb::TK_LET)
+      return fail(GAGP_DECLINED, "statements are outside the resident subset");
+    if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_LET &&
+        (e.arity != 2 || e.operand < 0 || e.operand >= gb::kLowerBinders))
+      return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": let binder");
     if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_OPERATION && e.opcode == gb::OP_CALL_BUILTIN &&
         e.operand != gb::B_ABS && e.operand != gb::B_MIN && e.operand != gb::B_MAX && e.operand != gb::B_LEN &&
         e.operand != gb::B_INDEX && e.operand != gb::B_IDIV0 && e.operand != gb::B_IMOD0 &&

@@ -79,6 +79,7 @@ constexpr int kMaxStack = 64;     // MAX_STACK (cpp/include/gagp/runtime/gpu/con
 constexpr int kLowerLocals = 64;  // phase compiler local capacity
 constexpr int kLowerWalks = 8;    // open traversals on one lowering path (kPhaseWalks)
 constexpr int kLowerBinders = 16; // lexical binder numbers (kPhaseBinders)
+constexpr int kLowerLets = 16;     // open lets (kPhaseLets)
 // instruction flags (DINSTR_HAS_A / DINSTR_HAS_B); bit 2 marks a Bool
 // constant, whose tag the reference keeps in its constant Value
 constexpr int kHasA = 1, kHasB = 2, kBoolConst = 4;
@@ -86,8 +87,8 @@ constexpr int kHasA = 1, kHasB = 2, kBoolConst = 4;
 // Reference bytecode of a whole-program value phase: compile_phase_tree
 // (cpp/src/evolution/repro/gpu/device/phase_compile.cuh:207-895) for the
 // node kinds this engine admits -- constants, inputs, operations, value
-// ifs, and/or, bound reads and forward or reverse traversals without a fuel
-// profile -- followed by the RETURN that patch_whole_program appends
+// ifs, and/or, lets, bound reads and forward or reverse traversals without a
+// fuel profile -- followed by the RETURN that patch_whole_program appends
 // (phase_layout.hpp:476-500).  Instructions are 5 ints (op, flags, a, b,
 // fuel) and the constants int64 payloads (flags bit 2: a Bool).  The
 // emitted code, constant numbering, temporaries and their LIFO reuse
@@ -113,8 +114,16 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
     int info, live_begin, xs, start, begin, limit, length, counter, element, index, state, loop_head, done_jump;
     int8_t saved_slot[3], saved_type[3];
   };
+  // one open let (phase_compile.cuh:263): its binder, its slot, the first
+  // live temporary it owns and the binder slot its body shadows
+  struct Let {
+    int binder, slot, live_begin;
+    int8_t saved_slot, saved_type;
+  };
   Frame frames[64];
   Walk walks[kLowerWalks];
+  Let lets[kLowerLets];
+  int let_depth = 0;
   int8_t env_slot[kLowerBinders], env_type[kLowerBinders];
   int8_t live[kLowerLocals], freed[kLowerLocals] = {};
   for (int i = 0; i < kLowerBinders; ++i) { env_slot[i] = -1; env_type[i] = GAGP_TAG_INVALID; }
@@ -273,6 +282,17 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
           return -1;
         frames[depth++] = Frame{index, stack, -1, -1, 0, {0, 0, 0}};
         continue;
+      } else if (e.node_kind == TK_LET) {
+        // the value's slot is taken before the value's own temporaries
+        if (e.arity != 2 || depth == 64 || e.operand < 0 || e.operand >= kLowerBinders) return -1;
+        if (let_depth == kLowerLets) return -1;
+        Let& l = lets[let_depth++];
+        l.binder = e.operand;
+        l.live_begin = live_count;
+        l.slot = temporary();
+        if (l.slot < 0) return -1;
+        frames[depth++] = Frame{index, stack, -1, -1, 0, {0, 0, 0}};
+        continue;
       } else {
         if (e.arity < 1 || e.arity > 3 || depth == 64) return -1;
         if (e.node_kind == TK_IF && e.arity != 3) return -1;
@@ -304,6 +324,28 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
       while (live_count > w.live_begin) freed[free_count++] = live[--live_count];
       --walk_depth;
       completed = info.result_type;
+      --depth;
+      continue;
+    }
+    if (e.node_kind == TK_LET) {
+      Let& l = lets[let_depth - 1];
+      if (f.seen == 1) {
+        // store the value and bind it for the body
+        if (!emit(OP_STORE, e.fuel, l.slot, 0, kHasA)) return -1;
+        stack = f.base_stack;
+        l.saved_slot = env_slot[l.binder];
+        l.saved_type = env_type[l.binder];
+        env_slot[l.binder] = int8_t(l.slot);
+        env_type[l.binder] = int8_t(completed);
+        have_value = false;
+        continue;
+      }
+      // the body's value is the let's
+      if (e.type != GAGP_TAG_INVALID && e.type != completed) return -1;
+      env_slot[l.binder] = l.saved_slot;
+      env_type[l.binder] = l.saved_type;
+      while (live_count > l.live_begin) freed[free_count++] = live[--live_count];
+      --let_depth;
       --depth;
       continue;
     }

@@ -39,7 +39,7 @@ LIST_TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL, "IntList": TAG_INTLIST}
 EK_OPERATION, EK_CONSTANT, EK_BOUND, EK_REFERENCE, EK_INPUT, EK_ALIAS = range(6)
 # PhaseTreeKind (device/phase_compile.cuh:21)
 TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR = range(6)
-TK_BOUND, TK_TRAVERSE = 14, 16
+TK_LET, TK_BOUND, TK_TRAVERSE = 13, 14, 16
 # Opcode (cpp/include/gagp/core/opcode.hpp:8-37)
 OP = {"push_const": 0, "load": 1, "store": 2, "neg": 3, "not": 4, "add": 5, "sub": 6, "mul": 7,
       "div": 8, "mod": 9, "lt": 10, "le": 11, "gt": 12, "ge": 13, "eq": 14, "ne": 15, "jmp": 16,
@@ -80,6 +80,11 @@ CATALOG = _scalar_catalog()
 LIST_CATALOG = {
     "len(IntList)->Int": (("IntList",), "Int", TK_OPERATION, OP["call_builtin"], BUILTIN["len"], "len"),
 }
+# let(value, body) binds one name for its body (catalog.cpp:89-92, a
+# LET_REGION whose region argument is the body)
+for _bound in ("Int", "Bool"):
+    for _t in ("Int", "Bool"):
+        LIST_CATALOG[f"let({_bound},{_t})->{_t}"] = ((_bound, _t), _t, TK_LET, 0, 0, "let_region")
 for _state in ("Int", "Bool"):
     LIST_CATALOG[f"traverse(IntList,Int,{_state},{_state})->{_state}"] = (
         ("IntList", "Int", _state, _state), _state, TK_TRAVERSE, 0, 1, "traverse")
@@ -268,9 +273,15 @@ class _Compiler:
             if len(args) != len(arg_types):
                 raise Declined("argument count mismatch")
             binds = value.get("bind", {})
-            if binds and tree_kind != TK_TRAVERSE:
-                raise Declined("binders outside a traversal are outside the table builder's list subset")
+            if binds and tree_kind not in (TK_TRAVERSE, TK_LET):
+                raise Declined("binders outside a traversal or let are outside the table builder's list subset")
             child_scopes = [scope] * len(args)
+            if tree_kind == TK_LET:
+                # the body (argument 1) binds the value
+                names = binds.get("1", [])
+                if set(binds) != {"1"} or len(names) != 1:
+                    raise Declined("let capability")
+                child_scopes[1] = scope + [(names[0], arg_types[0])]
             if tree_kind == TK_TRAVERSE:
                 # the body (last argument) binds element, index and state
                 body = len(args) - 1
@@ -391,6 +402,13 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         child_env = [env] * e.arity
         if e.kind == EK_BOUND:
             x.operand = env[e.target]
+        elif e.node_kind == TK_LET:
+            # one binder, numbered above every visible one (phase_grammar.hpp:255-261)
+            binder = max(env) + 1 if env else 0
+            if binder >= 16:
+                raise Declined("let capability")
+            child_env[1] = env + [binder]
+            x.operand = binder
         elif e.node_kind == TK_TRAVERSE:
             binder = max(env) + 1 if env else 0
             if binder + 2 >= 16:

@@ -189,8 +189,8 @@ def from_files(files, table_cache: Optional[dict] = None) -> LoadedTask:
 
 def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 0) -> str:
     """Prefix program text of a phase row (``cli_detail::program_text``,
-    ``cpp/src/cli/program_json.cpp:876-946``).  A traversal shows its body's
-    bound variables before the body, ``[vA vB vC] body``, numbered in prefix
+    ``cpp/src/cli/program_json.cpp:876-946``).  A traversal (or a let) shows
+    its body's bound variables before the body, ``[vA vB vC] body``, numbered in prefix
     order from ``first_binder`` as the reference's export numbers them
     (``export_native_phase_layout``, phase_layout.hpp:388-396); a bound read
     prints its variable."""
@@ -218,6 +218,11 @@ def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 
             binders = tables.regions[e.operand].binders
             ids = [next_id[0] + j for j in range(3)]
             next_id[0] += 3
+        elif e.node_kind == G.TK_LET:
+            # a let binds one variable for its body (the last argument)
+            binders = [e.operand]
+            ids = [next_id[0]]
+            next_id[0] += 1
         out.append("(" + e.name)
         for i in range(e.arity):
             out.append(" ")

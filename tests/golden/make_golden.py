@@ -66,6 +66,7 @@ LIST_RUNS = [
     ("list_reverse_traversal", dict(population=96, generations=4, seed=14, cases=16, target="max"), "reverse"),
     ("list_config3_p1024_g16", dict(population=1024, generations=16, seed=0, cases=200, target="threshold_sum"),
      None),
+    ("list_let_p256_g8", dict(population=256, generations=8, seed=15, cases=30, target="threshold_sum"), "let"),
 ]
 
 # Lowering pins (golden/lower/): the reference's phase compiler output and
@@ -77,6 +78,8 @@ LOWER_CASES = [
     ("lower_poly4", "poly4", dict(population=256, generations=1, seed=24, cases=32), None),
     ("lower_list_deep", "list", dict(population=384, generations=1, seed=25, cases=40, target="max"), "deep"),
     ("lower_int64_edges", "int64_edges", dict(population=512, generations=1, seed=26), None),
+    ("lower_list_let", "list", dict(population=384, generations=1, seed=27, cases=24, target="threshold_sum"), "let"),
+    ("lower_scalar_let", "scalar_let", dict(population=384, generations=1, seed=28, cases=32), None),
 ]
 
 
@@ -161,7 +164,54 @@ def reverse_traversal_grammar() -> dict:
     return g
 
 
+def let_grammar() -> dict:
+    """The list grammar with lets: the step may bind a value (an Int or a
+    comparison) for a body that reads it, and lets nest inside traversal
+    bodies and inside each other."""
+    g = W.list_threshold_grammar()
+    step = {"ref": "Step"}
+    steps = next(r for r in g["nonterminals"] if r["id"] == "Step")
+    steps["alternatives"].append({"id": "let_int", "weight": 1, "expression": {
+        "signature": "let(Int,Int)->Int", "args": [step, {"ref": "LetBody"}], "bind": {"1": ["v"]}}})
+    g["nonterminals"].append({
+        "id": "LetBody", "type": "Int",
+        "scope": [{"name": "element", "type": "Int"}, {"name": "acc", "type": "Int"}, {"name": "v", "type": "Int"}],
+        "alternatives": [
+            {"id": "v", "weight": 3, "expression": {"bound": "v"}},
+            {"id": "element", "weight": 1, "expression": {"bound": "element"}},
+            {"id": "acc", "weight": 1, "expression": {"bound": "acc"}},
+            {"id": "add", "weight": 2, "expression": {"signature": "add(Int,Int)->Int",
+                                                      "args": [{"ref": "LetBody"}, {"ref": "LetBody"}]}},
+            {"id": "sub", "weight": 1, "expression": {"signature": "sub(Int,Int)->Int",
+                                                      "args": [{"ref": "LetBody"}, {"ref": "LetBody"}]}},
+            {"id": "pick", "weight": 1, "expression": {"signature": "if(Bool,Int,Int)->Int", "args": [
+                {"signature": "gt(Int,Int)->Bool", "args": [{"ref": "LetBody"}, {"ref": "LetBody"}]},
+                {"ref": "LetBody"}, {"ref": "LetBody"}]}}]})
+    return g
+
+
+def scalar_let_grammar() -> dict:
+    """The large scalar grammar with a let whose body sees the bound value."""
+    g = W.poly4_grammar(max_nodes=40)
+    expr = next(r for r in g["nonterminals"] if r["id"] == "Expr")
+    expr["alternatives"].append({"id": "let", "weight": 1, "expression": {
+        "signature": "let(Int,Int)->Int", "args": [{"ref": "Expr"}, {"ref": "Body"}], "bind": {"1": ["y"]}}})
+    g["nonterminals"].append({
+        "id": "Body", "type": "Int", "scope": [{"name": "y", "type": "Int"}],
+        "alternatives": [
+            {"id": "y", "weight": 3, "expression": {"bound": "y"}},
+            {"id": "x", "weight": 1, "expression": {"input": "x"}},
+            {"id": "k", "weight": 1, "expression": {"constant": {"type": "Int", "range": ["-2", "3"]}}},
+            {"id": "add", "weight": 1, "expression": {"signature": "add(Int,Int)->Int",
+                                                      "args": [{"ref": "Body"}, {"ref": "Body"}]}},
+            {"id": "mul", "weight": 1, "expression": {"signature": "mul(Int,Int)->Int",
+                                                      "args": [{"ref": "Body"}, {"ref": "Body"}]}}]})
+    return g
+
+
 def variant_grammar(variant):
+    if variant == "let":
+        return let_grammar()
     if variant == "nested":
         return nested_traversal_grammar()
     if variant == "reverse":
@@ -462,6 +512,9 @@ def lower_fixtures() -> None:
             task = W.list_threshold(**kwargs)
         elif workload == "int64_edges":
             task = int64_edge_task(**kwargs)
+        elif workload == "scalar_let":
+            task = W.poly4(**kwargs)
+            task.grammar = scalar_let_grammar()
         else:
             task = W.make(workload, **kwargs)
         if variant:
