@@ -29,6 +29,9 @@ TASKS = [
     ("list_max_reservoir", lambda: _with_search(W.list_threshold(population=96, generations=3, seed=7, cases=20,
                                                                  target="max"),
                                                 {"sites": {"scope": "genome", "draw": "reservoir"}})),
+    ("poly4_generational", lambda: _with_search(W.poly4(population=200, generations=5, seed=8, cases=32,
+                                                        max_nodes=40),
+                                                {"schedule": {"mode": "generational"}, "elitism": 2})),
 ]
 
 
