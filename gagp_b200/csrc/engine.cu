@@ -770,6 +770,76 @@ Plan plan_search(const gagp_grammar* g, const gagp_cases* c, const gagp_search_c
 template <class T>
 T* at(char* block, size_t off) { return reinterpret_cast<T*>(block + off); }
 
+// The member rows of an imported initial population (`gagp run --init`,
+// run.cpp:146-174, imported by import_native_phase_layout): each row's node
+// words from its construction expressions, annotated as annotate_phase_tree
+// (device/phase_variation.cuh:23-79) annotates a tree -- a node a reference
+// expands is a variation site of that reference (its entry and crossover
+// class), depth counts tree levels from the root (1) and the site depth the
+// sites on the path from the root, the node's own included (0 without a site
+// depth limit).  False when a row does not derive from the slot's root, does
+// not fit the node budget or exceeds the site depth limit.
+bool import_rows(const gagp_grammar* g, const std::vector<gb::ExprInfo>& info, const gagp_rows* rows, int P, int stride,
+                 std::vector<uint64_t>* node, std::vector<int64_t>* cval, std::vector<int32_t>* len,
+                 std::string* why) {
+  const int E = g->expression_count, maxv = g->max_nodes - g->fixed_nodes;
+  const bool site_limited = g->site_depth > 0;
+  node->assign(size_t(stride) * P, 0);
+  cval->assign(size_t(stride) * P, 0);
+  len->assign(P, 0);
+  struct Task { int expr, entry, depth, sites; uint32_t cls; };
+  std::vector<Task> pending;
+  for (int r = 0; r < P; ++r) {
+    const int n = rows->node_counts[r], nc = rows->constant_counts[r];
+    if (n < 1 || n > maxv || n > rows->stride || nc < 0 || nc > n) {
+      *why = "row " + std::to_string(r) + " outside the node budget";
+      return false;
+    }
+    const int32_t* origins = rows->origins + size_t(r) * rows->stride;
+    pending.assign(1, Task{g->root_expression, -1, 1, 0, gb::kNoClass});
+    int cursor = 0, constants = 0, steps = 0;
+    while (!pending.empty()) {
+      const Task t = pending.back();
+      pending.pop_back();
+      if (++steps > 8192 || t.expr < 0 || t.expr >= E) break;
+      const gagp_expression& e = g->expressions[t.expr];
+      if (e.kind == gb::EK_REFERENCE) {
+        // one site per node; the node's origin names the production
+        if (t.entry >= 0 || cursor >= n || e.target < 0 || e.target >= g->nonterminal_count) break;
+        const gagp_nonterminal& nt = g->nonterminals[e.target];
+        int production = -1;
+        for (int i = 0; i < nt.production_count && production < 0; ++i)
+          if (g->productions[nt.production_offset + i].expression == origins[cursor])
+            production = origins[cursor];
+        if (production < 0) break;
+        pending.push_back(Task{production, t.expr, t.depth, t.sites + (site_limited ? 1 : 0),
+                               uint32_t(info[t.expr].site_class)});
+        continue;
+      }
+      if (cursor >= n || origins[cursor] != t.expr || t.depth > 255 || t.sites > 255) {
+        cursor = -1;
+        break;
+      }
+      if (site_limited && t.sites > g->site_depth) {
+        *why = "row " + std::to_string(r) + " exceeds the site depth limit";
+        return false;
+      }
+      const bool constant = e.kind == gb::EK_CONSTANT;
+      constants += constant;
+      (*node)[size_t(r) * stride + cursor++] =
+          gb::w_make(t.expr, t.entry, t.depth, t.sites, info[t.expr].arity, constant, t.cls);
+      for (int i = info[t.expr].arity - 1; i >= 0; --i)
+        pending.push_back(Task{e.children[i], -1, t.depth + 1, t.sites, gb::kNoClass});
+    }
+    if (cursor != n || !pending.empty() || constants != nc) {
+      *why = "row " + std::to_string(r) + " does not derive from the grammar's root";
+      return false;
+    }
+    for (int k = 0; k < nc; ++k) (*cval)[size_t(r) * stride + k] = rows->constants[size_t(r) * rows->stride + k];
+    (*len)[r] = gb::make_len(n, nc);
+  }
+  return true;
+}
 
 }  // namespace
 
@@ -881,9 +951,11 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
                                     const gagp_search_config* cfg, const gagp_rows* initial, int32_t* out_search) {
   if (!e || !out_search) return fail(GAGP_INVALID_ARGUMENT, "null argument");
   if (e->poisoned) return fail(GAGP_DEVICE_ERROR, "engine is poisoned by an earlier device error");
-  if (initial) return fail(GAGP_DECLINED, "imported initial populations are not supported by this engine yet");
   const gagp_status st = admit(g, c, cfg);
   if (st != GAGP_OK) return st;
+  if (initial && (initial->count < cfg->population || initial->stride < 1 || !initial->node_counts ||
+                  !initial->origins || !initial->constant_counts || (!initial->constants && initial->count)))
+    return fail(GAGP_INVALID_ARGUMENT, "an imported population needs population rows");
   CUDA_TRY(cudaSetDevice(e->device));
   Plan p = plan_search(g, c, cfg);
   if (e->arena_used + p.L.total > e->arena_limit)
@@ -1051,6 +1123,22 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.key_shift_nodes = node_bits;
   d.key_shift_wrong = node_bits + wrong_bits;
   d.total_rounds = s->total_rounds;
+  if (initial) {
+    // the caller's population replaces the generated one (its first
+    // population rows, in order)
+    std::vector<uint64_t> node;
+    std::vector<int64_t> cval;
+    std::vector<int32_t> len;
+    std::string why;
+    if (!import_rows(g, info, initial, s->P, p.stride, &node, &cval, &len, &why)) {
+      cudaFreeAsync(s->block, e->stream);
+      return fail(GAGP_INVALID_ARGUMENT, "imported population: " + why);
+    }
+    CUDA_TRY(up(p.node, node.data(), 8 * node.size()));
+    CUDA_TRY(up(p.cval, cval.data(), 8 * cval.size()));
+    CUDA_TRY(up(p.len, len.data(), 4 * len.size()));
+    d.imported = 1;
+  }
   CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->d_desc), sizeof(gb::SearchDesc), e->pool, e->stream));
   CUDA_TRY(copy_h2d(e, s->d_desc, &d, sizeof(gb::SearchDesc)));
   const int32_t off[4] = {0, s->P, 0, s->B};

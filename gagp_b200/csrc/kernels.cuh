@@ -42,6 +42,7 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
   if (item >= off[n]) return;
   const int si = find_search(off, n, item);
   const SearchDesc& s = descs[si];
+  if (s.imported) return;  // the caller's rows are the initial population
   const int i = item - off[si];
   const int site_limit = s.site_depth;
   const int ramp = site_limit < 2 ? site_limit : 2 + i % (site_limit - 1);

@@ -143,6 +143,7 @@ struct SearchDesc {
   // round replaces the whole population (B = P), its first elite_count
   // children by the elites of the ranking
   int32_t generational, elite_count;
+  int32_t imported;  // the members were imported (no initial generation)
   // ---- cases (input-major: inputs[j * C + c]); an IntList input's value is
   // the offset in `lists` of its length word, its elements following
   const int64_t* inputs;

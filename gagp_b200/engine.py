@@ -110,12 +110,14 @@ class Engine:
         _check(load_library().gagp_b200_search_bytes(g.ref(), task.cases.ref(), C.byref(cfg), C.byref(out)))
         return int(out.value)
 
-    def admit(self, task: LoadedTask) -> Search:
+    def admit(self, task: LoadedTask, initial: Optional[abi.RowsBuffer] = None) -> Search:
+        """Admits a search; `initial`: rows of an imported initial population
+        (its first `population` rows), else the population is generated."""
         g = abi.GrammarBlob(task.tables)
         cfg = task.settings.struct()
         sid = C.c_int32(0)
-        _check(load_library().gagp_b200_search_create(self.handle, g.ref(), task.cases.ref(), C.byref(cfg), None,
-                                                     C.byref(sid)))
+        _check(load_library().gagp_b200_search_create(self.handle, g.ref(), task.cases.ref(), C.byref(cfg),
+                                                     initial.ref() if initial is not None else None, C.byref(sid)))
         return Search(self, sid.value, task, g)
 
     def run(self, search: Search):

@@ -226,8 +226,12 @@ gagp_status gagp_b200_search_bytes(const gagp_grammar* grammar, const gagp_cases
 /* Admits one search (NativePhasePopulation ctor, phase_population.cu:489-629):
  * uploads its tables and cases and builds its initial population on the
  * device, generated from the seed as generate_phase_initial_population does
- * (phase_population_cpu.cpp:54-113).  `initial` must be NULL: an imported
- * population is declined (GAGP_DECLINED), so the caller keeps its own path. */
+ * (phase_population_cpu.cpp:54-113).  With `initial` (not NULL) the first
+ * `population` of its rows are the initial population instead, in order, as
+ * `gagp run --init` imports one (run.cpp:146-174, rows as the reference's
+ * import_native_phase_layout gives them): each row must derive from the
+ * grammar's root, fit the node budget and the site depth limit
+ * (GAGP_INVALID_ARGUMENT otherwise). */
 gagp_status gagp_b200_search_create(gagp_engine* engine, const gagp_grammar* grammar,
                                     const gagp_cases* cases, const gagp_search_config* config,
                                     const gagp_rows* initial, int32_t* out_search);

@@ -10,11 +10,13 @@
 //       phase rows (generate_phase_initial_population, then the owner's import
 //       and site annotation, phase_population_cpu.cpp:54-113,220-238).
 //
-//   ref_driver run TASK.json [--search F] [--population N] [--generations G] [--seed S]
+//   ref_driver run TASK.json [--search F] [--population N] [--generations G] [--seed S] [--init POP.json]
 //       one CPU-engine search (evolve_population, cpp/src/evolution/evolve.cpp:839)
-//       with the gagp run defaults (cpp/src/cli/run.cpp:275-300): the
-//       per-generation history, and the final ranked population with fitness,
-//       wrong count, node count, program text and phase row.
+//       with the gagp run defaults (cpp/src/cli/run.cpp:275-300), from the
+//       generated population or, with --init, from the first programs of a
+//       population document (as `gagp run --init`): the per-generation
+//       history, and the final ranked population with fitness, wrong count,
+//       node count, program text, program as ast-prefix-v2 JSON and phase row.
 //
 //   ref_driver lower TASK.json [--search F] [--population N] [--seed S] [--case-detail K]
 //       the initial population lowered by the resident owner's phase compiler
@@ -72,7 +74,7 @@ constexpr const char* kDefaultSearch = R"({
   "ranking": {"tie_break": "ast_nodes"}, "schedule": {"mode": "steady_state", "replacement_size": 2}})";
 
 struct Args {
-  std::string mode, task, search;
+  std::string mode, task, search, init;
   int population = 0, generations = 0;
   bool has_seed = false;
   std::uint64_t seed = 0;
@@ -387,7 +389,28 @@ int run_search(const Args& a) {
   const auto cases = cli_detail::load_fitness_cases(task.train_path);
   const auto cfg = make_config(a, task, grammar);
   const auto case_set = evo::prepare_case_set(cases);
-  const auto result = evo::evolve_population(cases, cfg, nullptr);
+  // an imported initial population (`gagp run --init`, run.cpp:146-174): the
+  // first population_size programs of a population document, in order
+  std::vector<evo::ProgramGenome> initial;
+  if (!a.init.empty()) {
+    std::FILE* f = std::fopen(a.init.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open " + a.init);
+    std::string text;
+    char buf[65536];
+    for (std::size_t got; (got = std::fread(buf, 1, sizeof buf, f)) > 0;) text.append(buf, got);
+    std::fclose(f);
+    const auto doc = cli_detail::JsonParser(text, {true, 512}).parse();
+    for (const auto& program : doc.object_v.at("programs").array_v) {
+      if (initial.size() == std::size_t(cfg.population_size)) break;
+      evo::ProgramGenome g;
+      g.ast = cli_detail::decode_ast_json(program);
+      g.meta = evo::build_genome_meta(g.ast);
+      g.derivation = std::make_shared<gg::DerivationMetadata>(gg::reconstruct_derivation(*grammar, g));
+      initial.push_back(std::move(g));
+    }
+    if (initial.size() != std::size_t(cfg.population_size)) throw std::runtime_error("--init: too few programs");
+  }
+  const auto result = evo::evolve_population(cases, cfg, initial.empty() ? nullptr : &initial);
   rp::NativePhaseGrammarProfiles profiles(grammar, case_set.input_names);
   const auto& totals = result.timing.evaluation_totals;
   std::printf("{\"declined\":%s,\"time_ms\":%s,\"init_ms\":%s,\"program_cases\":%llu,\"reused_programs\":%llu,\"history\":[",
@@ -403,9 +426,9 @@ int run_search(const Args& a) {
   std::printf("],\"final\":[");
   for (std::size_t i = 0; i < result.final_population.size(); ++i) {
     const auto& m = result.final_population[i];
-    std::printf("%s{\"fitness\":%s,\"wrong\":%d,\"nodes\":%zu,\"text\":%s,\"rows\":[", i ? "," : "",
+    std::printf("%s{\"fitness\":%s,\"wrong\":%d,\"nodes\":%zu,\"text\":%s,\"program\":%s,\"rows\":[", i ? "," : "",
                 num(m.fitness).c_str(), m.wrong, m.genome.ast.nodes.size(),
-                quote(cli_detail::program_text(m.genome.ast)).c_str());
+                quote(cli_detail::program_text(m.genome.ast)).c_str(), cli_detail::encode_ast_json(m.genome.ast).c_str());
     if (result.resident_declined.empty()) {
       const auto imported = rp::import_native_phase_layout(*grammar, m.genome, &profiles, &case_set.input_names, false);
       for (std::size_t k = 0; k < imported.genes.size(); ++k) {
@@ -441,6 +464,7 @@ int main(int argc, char** argv) {
     else if (k == "--seed") { a.has_seed = true; a.seed = std::stoull(v); }
     else if (k == "--round-seed") a.round_seed = std::stoull(v);
     else if (k == "--case-detail") a.case_detail = std::stoi(v);
+    else if (k == "--init") a.init = v;
     else { std::fprintf(stderr, "unknown option %s\n", k.c_str()); return 2; }
   }
   try {

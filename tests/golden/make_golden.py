@@ -261,6 +261,42 @@ def gen_fixtures() -> None:
               run["program_cases"], "program-cases,", run["reused_programs"], "reused")
 
 
+# Imported initial populations (golden/init/): a short reference search A,
+# then a search B of the same task started from A's final population
+# (`ref_driver run --init`, as `gagp run --init`, run.cpp:146-174).
+INIT_CASES = [
+    ("init_poly4", "poly4", dict(population=128, generations=3, seed=51, cases=40, max_nodes=40), 6, {}),
+    ("init_list", "list", dict(population=96, generations=2, seed=52, cases=20), 4, {}),
+    ("init_generational", "poly4", dict(population=120, generations=3, seed=53, cases=32, max_nodes=40), 5,
+     {"schedule": {"mode": "generational"}, "elitism": 2}),
+]
+
+
+def init_fixtures() -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "init"), exist_ok=True)
+    for name, workload, kwargs, generations_b, extra in INIT_CASES:
+        task = W.list_threshold(**kwargs) if workload == "list" else W.make(workload, **kwargs)
+        task.search.update(extra)
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            first = driver("run", tp, "--search", sp)
+            pp = os.path.join(d, "population.json")
+            with open(pp, "w") as f:
+                json.dump({"format": "gagp-population-v1", "programs": [m["program"] for m in first["final"]]}, f)
+            run = driver("run", tp, "--search", sp, "--init", pp, "--generations", str(generations_b))
+        assert run["declined"] == "", (name, run["declined"])
+        task.search["generations"] = generations_b
+        initial = [{"origins": m["rows"][0]["origins"], "constants": [c[1] for c in m["rows"][0]["constants"]]}
+                   for m in first["final"]]
+        fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+                   "train": task.train, "test": task.test, "search": task.search, "initial": initial, "run": run}
+        with gzip.open(os.path.join(here, "init", name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(initial), "imported members,", len(run["history"]), "history entries")
+
+
 # Judgement pins (golden/judge/): the reference's `gagp eval --split test`
 # verdict (cpp/src/cli/run.cpp:176-238) of generated programs on a test split,
 # and one `gagp run` whose result carries the best program's test verdict.
@@ -388,6 +424,7 @@ def main() -> None:
     ap.add_argument("--lower-only", action="store_true", help="regenerate golden/lower/ only")
     ap.add_argument("--judge-only", action="store_true", help="regenerate golden/judge/ only")
     ap.add_argument("--generational-only", action="store_true", help="regenerate golden/generational/ only")
+    ap.add_argument("--init-only", action="store_true", help="regenerate golden/init/ only")
     ap.add_argument("--headline", action="store_true",
                     help="regenerate golden/headline/ only (the benchmark's search, several minutes)")
     args = ap.parse_args()
@@ -402,6 +439,9 @@ def main() -> None:
         return
     if args.generational_only:
         gen_fixtures()
+        return
+    if args.init_only:
+        init_fixtures()
         return
     if not os.path.exists(DRIVER):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
@@ -466,6 +506,7 @@ def main() -> None:
     lower_fixtures()
     judge_fixtures()
     gen_fixtures()
+    init_fixtures()
 
 
 def row_digest(rows) -> str:
