@@ -24,8 +24,15 @@ namespace gb {
 
 // PhaseExpressionKind / PhaseTreeKind / status codes (reference enums).
 enum { EK_OPERATION = 0, EK_CONSTANT = 1, EK_BOUND = 2, EK_REFERENCE = 3, EK_INPUT = 4, EK_ALIAS = 5 };
-enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5, TK_LET = 13,
+enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5, TK_PROGRAM = 6,
+       TK_BLOCK = 7, TK_NIL = 8, TK_ASSIGN = 9, TK_RETURN = 10, TK_FOR_RANGE = 11, TK_VAR = 12, TK_LET = 13,
        TK_BOUND = 14, TK_TRAVERSE = 16 };
+// Completion tag of a statement (kPhaseStatement,
+// cpp/src/evolution/repro/gpu/device/phase_compile.cuh:23): a node or phase
+// type, never a runtime value.  Tables narrowed to int8_t keep it as -16.
+constexpr int kStatementTag = 0xF0;
+__host__ __device__ __forceinline__ bool is_statement_tag(int t) { return (t & 0xff) == kStatementTag; }
+constexpr int kNamedLocals = 16;  // grammar locals a phase can name (kPhaseNamedLocals)
 enum { ST_OK = 0, ST_INVALID = 1, ST_UNSUPPORTED = 2, ST_CAPACITY = 3 };
 constexpr int kFixedSite = 1 << 30;
 constexpr uint32_t kNoClass = 0x7ffu;
@@ -133,6 +140,63 @@ __host__ __device__ __forceinline__ int32_t make_len(int n, int c) { return n | 
 // Crossover class of sites opened by reference expression `entry`.
 __device__ __forceinline__ uint32_t class_of_entry(const SearchDesc& s, int entry) {
   return entry < 0 ? kNoClass : uint32_t(s.info[entry].site_class);
+}
+
+// Definite assignment of grammar locals in a statement program
+// (phase_locals_defined, cpp/src/evolution/repro/gpu/device/phase_compile.cuh:170-200):
+// a grammar local may be read after an assignment to it, inside a for_range
+// body that names it, and after a statement if only when both branches
+// assigned it; a loop body's assignments do not outlive the loop, and inputs
+// are always defined.  `at(i)` gives node i's tree kind, operand, arity and
+// type.  False also for a tree deeper than 64 open nodes or one that ends
+// early.
+struct StatementNode {
+  int kind, operand, arity, type;
+};
+// (`at` may be host-only: the engine's host code checks imported rows with it)
+#pragma nv_exec_check_disable
+template <class At>
+__host__ __device__ inline bool locals_defined(int n, At at) {
+  struct Frame {
+    int16_t index, seen;
+    uint16_t saved, branch;
+  };
+  Frame frames[64];
+  int depth = 0;
+  unsigned mask = 0;
+  auto bit = [](int operand) -> unsigned { return operand >= 0 && operand < kNamedLocals ? 1u << operand : 0u; };
+  for (int i = 0; i < n; ++i) {
+    const StatementNode x = at(i);
+    if (x.kind == TK_VAR && !(mask & bit(x.operand))) return false;
+    if (x.arity > 0) {
+      if (depth == 64) return false;
+      frames[depth++] = Frame{int16_t(i), 0, uint16_t(mask), 0};
+      continue;
+    }
+    while (depth) {
+      Frame& f = frames[depth - 1];
+      const StatementNode owner = at(f.index);
+      ++f.seen;
+      if (owner.kind == TK_FOR_RANGE && f.seen == 1) {
+        f.saved = uint16_t(mask);
+        mask |= bit(owner.operand);
+      } else if (owner.kind == TK_IF && is_statement_tag(owner.type)) {
+        if (f.seen == 1) {
+          f.saved = uint16_t(mask);
+        } else if (f.seen == 2) {
+          f.branch = uint16_t(mask);
+          mask = f.saved;
+        } else {
+          mask &= f.branch;
+        }
+      }
+      if (f.seen < owner.arity) break;
+      if (owner.kind == TK_ASSIGN) mask |= bit(owner.operand);
+      else if (owner.kind == TK_FOR_RANGE) mask = f.saved;
+      --depth;
+    }
+  }
+  return depth == 0;
 }
 
 struct GenResult {

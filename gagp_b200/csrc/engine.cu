@@ -264,6 +264,19 @@ int bits_for(uint64_t v) {
   return b;
 }
 
+// The value type a program of `g` returns: the phase type of an expression
+// entry; for a statement program (a Program entry, whose phase completes as
+// a statement) the type its returns carry, which the grammar makes the
+// entry's result contract (compiled.cpp:512-513).
+int result_type_of(const gagp_grammar* g) {
+  if (!gb::is_statement_tag(g->slot_type)) return g->slot_type;
+  for (int i = 0; i < g->expression_count; ++i) {
+    const gagp_expression& e = g->expressions[i];
+    if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_RETURN) return e.type;
+  }
+  return GAGP_TAG_INVALID;
+}
+
 // The phase tables, traversal table and cases as the device reads them:
 // every id the subtree generator and the lowering follow without a range
 // check is in range, and every IntList input lies inside list_values.
@@ -305,8 +318,23 @@ gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
     }
     if (e.kind == gb::EK_OPERATION && e.node_kind != gb::TK_OPERATION && e.node_kind != gb::TK_IF &&
         e.node_kind != gb::TK_AND && e.node_kind != gb::TK_OR && e.node_kind != gb::TK_TRAVERSE &&
-        e.node_kind != gb::TK_LET)
-      return fail(GAGP_DECLINED, "statements are outside the resident subset");
+        e.node_kind != gb::TK_LET && !(e.node_kind >= gb::TK_PROGRAM && e.node_kind <= gb::TK_VAR))
+      return fail(GAGP_DECLINED, "tree kind outside the resident subset");
+    if (e.kind == gb::EK_OPERATION && e.node_kind >= gb::TK_PROGRAM && e.node_kind <= gb::TK_VAR) {
+      // statements belong to a Program entry's whole-program phase; a named
+      // target is a grammar local or an input (-1 - its position)
+      if (!gb::is_statement_tag(g->slot_type)) return fail(GAGP_INVALID_ARGUMENT, "a statement in a value phase");
+      const int nk = e.node_kind;
+      const int want = nk == gb::TK_NIL || nk == gb::TK_VAR ? 0 : nk == gb::TK_BLOCK || nk == gb::TK_FOR_RANGE ? 2 : 1;
+      if (e.arity != want) return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": statement arity");
+      const bool named = nk == gb::TK_ASSIGN || nk == gb::TK_FOR_RANGE || nk == gb::TK_VAR;
+      if (named && (e.operand >= gb::kNamedLocals || e.operand < -g->local_count || (nk == gb::TK_VAR && e.operand < 0)))
+        return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": statement target");
+      if ((nk == gb::TK_RETURN || nk == gb::TK_VAR) && !value_tag(e.type))
+        return fail(GAGP_DECLINED, "statement value type outside Int, Bool and IntList");
+      if (nk == gb::TK_RETURN && result_type_of(g) != e.type)
+        return fail(GAGP_INVALID_ARGUMENT, "returns of one program disagree on its result type");
+    }
     if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_LET &&
         (e.arity != 2 || e.operand < 0 || e.operand >= gb::kLowerBinders))
       return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": let binder");
@@ -636,13 +664,17 @@ std::vector<char> gen_image(const gagp_grammar* g, const std::vector<gb::ExprInf
 // `maxv` nodes, the appended RETURN included: a leaf or operation emits 1, a
 // value if 2 (its jumps), and/or 5, and a traversal at most 36 of its own
 // beside its four children, so at most 8 per node of a row holding
-// traversals (36 + 4 children over 5 nodes).
+// traversals (36 + 4 children over 5 nodes).  A for_range emits 23 of its
+// own; its body's root is a block node that emits none and is no other
+// loop's body root, so at most 12 per node of a row holding loops.
+// Program, block and nil nodes emit nothing, an if_stmt 2 and an assign,
+// a return or a local read 1.
 int bytecode_bound(const gagp_grammar* g, int maxv) {
   int per_node = 1;
   for (int i = 0; i < g->expression_count; ++i) {
     const int nk = g->expressions[i].node_kind;
     if (g->expressions[i].kind == gb::EK_OPERATION)
-      per_node = std::max(per_node, nk == gb::TK_TRAVERSE ? 8 : nk == gb::TK_IF ? 2
+      per_node = std::max(per_node, nk == gb::TK_FOR_RANGE ? 12 : nk == gb::TK_TRAVERSE ? 8 : nk == gb::TK_IF ? 2
                                     : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
   }
   return per_node * maxv + 2;
@@ -652,6 +684,7 @@ int bytecode_bound(const gagp_grammar* g, int maxv) {
 // traversals or bound reads, or operations that can raise a runtime error
 // (modulo and division by zero, list builtins).
 bool exact_heavy(const gagp_grammar* g) {
+  if (gb::is_statement_tag(g->slot_type)) return true;  // statement programs run on the exact VM only
   for (int i = 0; i < g->expression_count; ++i) {
     const gagp_expression& e = g->expressions[i];
     if (e.kind == gb::EK_BOUND) return true;
@@ -833,6 +866,16 @@ bool import_rows(const gagp_grammar* g, const std::vector<gb::ExprInfo>& info, c
     }
     if (cursor != n || !pending.empty() || constants != nc) {
       *why = "row " + std::to_string(r) + " does not derive from the grammar's root";
+      return false;
+    }
+    // a statement program reads only definitely assigned grammar locals
+    // (the native verifier's definite assignment, ast_type_verify)
+    if (gb::is_statement_tag(g->slot_type) && !gb::locals_defined(n, [&](int i) {
+          const gagp_expression& x = g->expressions[origins[i]];
+          return gb::StatementNode{x.kind == gb::EK_OPERATION ? x.node_kind : -1, x.operand,
+                                   info[origins[i]].arity, x.type};
+        })) {
+      *why = "row " + std::to_string(r) + " reads a grammar local before assigning it";
       return false;
     }
     for (int k = 0; k < nc; ++k) (*cval)[size_t(r) * stride + k] = rows->constants[size_t(r) * rows->stride + k];
@@ -1067,6 +1110,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.n_doms = g->domain_count; d.n_vals = g->value_count;
   d.depth_count = g->depth_count; d.logical_count = g->logical_depth_count; d.site_depth = g->site_depth;
   d.root_expression = g->root_expression; d.slot_max_depth = g->slot_max_depth; d.slot_type = g->slot_type;
+  d.result_type = result_type_of(g);
   d.local_count = g->local_count; d.max_nodes = g->max_nodes; d.fixed_nodes = g->fixed_nodes;
   d.return_fuel = g->return_fuel;
   d.P = s->P; d.B = s->B; d.maxv = s->maxv; d.stride = p.stride;
@@ -1785,6 +1829,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.n_regions = g->region_count;
   d.n_ex = E;
   d.slot_type = g->slot_type;
+  d.result_type = result_type_of(g);
   d.local_count = g->local_count;
   d.max_nodes = g->max_nodes;
   d.fixed_nodes = g->fixed_nodes;
@@ -2173,7 +2218,7 @@ gagp_status gagp_b200_judge_rows(gagp_engine* e, const gagp_grammar* grammar, co
   // an error as a runtime failure is; a correct case loses 0, so with Bool
   // expectations under the absolute metric (whose case score is the ceiling
   // whatever the value) the correct cases' ceilings come off the loss
-  const bool type_errors = cases->expected_tag == GAGP_TAG_INT && grammar->slot_type != GAGP_TAG_INT;
+  const bool type_errors = cases->expected_tag == GAGP_TAG_INT && result_type_of(grammar) != GAGP_TAG_INT;
   const int64_t cap = int64_t(std::fabs(config->penalty));
   for (int r = 0; r < R; ++r) {
     gagp_verdict& v = out[r];

@@ -54,6 +54,10 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
     const int room = s.maxv < kCapacity ? s.maxv : kCapacity;
     g = generate(s, s.gen_image, s.root_expression, 0, s.slot_max_depth, room,
                  mix64(s.seed ^ mix64((uint64_t(i) * 8 + 0) * 64 + uint64_t(attempt))), node, cval, logical, pending);
+    // a statement program that reads a grammar local before assigning it
+    // is retried with the next seed (phase_population_cpu.cpp:95-96)
+    if (g.status == ST_OK && is_statement_tag(s.slot_type) && !row_locals_defined(s, node, g.nodes))
+      g.status = ST_INVALID;
     if (g.status != ST_OK && attempt % 4 == 3 && logical < site_limit) ++logical;
     if (attempt >= 256 && g.status != ST_OK) {
       raise_error(s, 20);
@@ -207,7 +211,7 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
         const int32_t* x = gcode + 5 * k;
         const int cost = x[4];
         simd_ok &= cost >= 1 && cost <= 255 && x[0] >= 0 && x[0] < 64;
-        words[k] = simd_plain(x[0], x[2], cost);
+        words[k] = simd_stage(gcode, k);
       }
       for (int k = threadIdx.x; k < (n + 63) / 64; k += blockDim.x) targets[k] = 0;
     }
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
         const bool live = c < s.C;
         const SimdCase r = run_program_simd(view, words, n, consts, n_locals, c, live, slots);
         if (live) {
-          if (r.ok) loss += case_loss(s, s.slot_type, r.value, s.expected[c], wrong);
+          if (r.ok) loss += case_loss(s, s.result_type, r.value, s.expected[c], wrong);
           else { loss += error_loss(s); ++wrong; ++errors; }
         }
         steps += r.steps;

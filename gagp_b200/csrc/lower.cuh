@@ -25,7 +25,7 @@ enum {
   OP_JMP_IF_FALSE = 17, OP_JMP_IF_TRUE = 18, OP_CALL_BUILTIN = 19, OP_RETURN = 20, OP_CHECK_INT = 22
 };
 enum {
-  B_ABS = 0, B_MIN = 1, B_MAX = 2, B_LEN = 4, B_INDEX = 7, B_IDIV0 = 13, B_IMOD0 = 14, B_TRUNC_DIV0 = 28,
+  B_ABS = 0, B_MIN = 1, B_MAX = 2, B_LEN = 4, B_INDEX = 7, B_IS_INT = 12, B_IDIV0 = 13, B_IMOD0 = 14, B_TRUNC_DIV0 = 28,
   B_TRUNC_MOD0 = 29
 };
 
@@ -80,6 +80,7 @@ constexpr int kLowerLocals = 64;  // phase compiler local capacity
 constexpr int kLowerWalks = 8;    // open traversals on one lowering path (kPhaseWalks)
 constexpr int kLowerBinders = 16; // lexical binder numbers (kPhaseBinders)
 constexpr int kLowerLets = 16;     // open lets (kPhaseLets)
+constexpr int kLowerLoops = 16;    // open for_range loops (kPhaseLoops)
 // instruction flags (DINSTR_HAS_A / DINSTR_HAS_B); bit 2 marks a Bool
 // constant, whose tag the reference keeps in its constant Value
 constexpr int kHasA = 1, kHasB = 2, kBoolConst = 4;
@@ -124,6 +125,17 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
   Walk walks[kLowerWalks];
   Let lets[kLowerLets];
   int let_depth = 0;
+  // one open for_range (phase_compile.cuh:251-252): its bound and counter
+  // slots, the loop head, the exit jump to patch, the constant 1's index
+  // and the first live temporary it owns
+  struct Loop {
+    int bound, counter, head, end_jump, one, live_begin;
+  };
+  Loop loops[kLowerLoops];
+  int loop_depth = 0;
+  // grammar locals get a slot on first use, after the inputs, and keep it
+  unsigned named_mask = 0;
+  int8_t named[kNamedLocals];
   int8_t env_slot[kLowerBinders], env_type[kLowerBinders];
   int8_t live[kLowerLocals], freed[kLowerLocals] = {};
   for (int i = 0; i < kLowerBinders; ++i) { env_slot[i] = -1; env_type[i] = GAGP_TAG_INVALID; }
@@ -131,7 +143,16 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
   int total_locals = v.local_count, live_count = 0, free_count = 0;
   int completed = GAGP_TAG_INVALID;
   bool have_value = false;
+  const bool statements = is_statement_tag(v.slot_type);
   if (n <= 0 || n > kCapacity || v.local_count < 0 || v.local_count > kLowerLocals) return -1;
+  // a statement program reads only definitely assigned grammar locals
+  if (statements && !locals_defined(n, [&](int i) {
+        const int o = w_origin(node[i]);
+        if (o < 0 || o >= v.n_ex) return StatementNode{-1, 0, w_arity(node[i]), 0};
+        const gagp_expression& x = v.ex[o];
+        return StatementNode{x.kind == EK_OPERATION ? x.node_kind : -1, x.operand, w_arity(node[i]), x.type};
+      }))
+    return -1;
   auto emit = [&](int op, unsigned fuel, int a, int b, int flags) -> bool {
     if (count >= code_cap) return false;
     int32_t* x = code + 5 * count++;
@@ -163,6 +184,18 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
     else slot = total_locals++;
     live[live_count++] = int8_t(slot);
     return slot;
+  };
+  // the slot of an assignment target or local read: an input (-1 - its
+  // evaluator position) or a grammar local, numbered on first use
+  auto variable_slot = [&](int operand) -> int {
+    if (operand < 0) return -1 - operand < v.local_count ? -1 - operand : -1;
+    if (operand >= kNamedLocals) return -1;
+    if (!((named_mask >> operand) & 1u)) {
+      if (total_locals >= kLowerLocals) return -1;
+      named[operand] = int8_t(total_locals++);
+      named_mask |= 1u << operand;
+    }
+    return named[operand];
   };
   auto subtree_end = [&](int i) -> int {
     int pending = 1;
@@ -256,6 +289,18 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
         grow(1);
         completed = v.local_types[e.operand];
         have_value = true;
+      } else if (e.node_kind == TK_NIL) {
+        if (e.arity != 0) return -1;
+        completed = kStatementTag;
+        have_value = true;
+      } else if (e.node_kind == TK_VAR) {
+        // a grammar local's read
+        if (e.arity != 0 || e.operand < 0 || e.type == GAGP_TAG_INVALID || is_statement_tag(e.type)) return -1;
+        const int slot = variable_slot(e.operand);
+        if (slot < 0 || !emit(OP_LOAD, e.fuel, slot, 0, kHasA)) return -1;
+        grow(1);
+        completed = e.type;
+        have_value = true;
       } else if (e.node_kind == TK_TRAVERSE) {
         if (e.operand < 0 || e.operand >= v.n_regions) return -1;
         const RegionInfo& info = v.regions[e.operand];
@@ -297,15 +342,32 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
         if (e.arity < 1 || e.arity > 3 || depth == 64) return -1;
         if (e.node_kind == TK_IF && e.arity != 3) return -1;
         if ((e.node_kind == TK_AND || e.node_kind == TK_OR) && e.arity != 2) return -1;
-        if (e.node_kind != TK_OPERATION && e.node_kind != TK_IF && e.node_kind != TK_AND && e.node_kind != TK_OR)
+        if ((e.node_kind == TK_PROGRAM || e.node_kind == TK_ASSIGN || e.node_kind == TK_RETURN) && e.arity != 1)
           return -1;
+        if ((e.node_kind == TK_BLOCK || e.node_kind == TK_FOR_RANGE) && e.arity != 2) return -1;
+        if (e.node_kind != TK_OPERATION && e.node_kind != TK_IF && e.node_kind != TK_AND && e.node_kind != TK_OR &&
+            e.node_kind != TK_PROGRAM && e.node_kind != TK_BLOCK && e.node_kind != TK_ASSIGN &&
+            e.node_kind != TK_RETURN && e.node_kind != TK_FOR_RANGE)
+          return -1;
+        if (e.node_kind == TK_FOR_RANGE) {
+          // the bound's slot precedes the bound expression's own temporaries
+          if (loop_depth == kLowerLoops) return -1;
+          Loop& l = loops[loop_depth++];
+          l.live_begin = live_count;
+          l.bound = temporary();
+          if (l.bound < 0) return -1;
+        }
         frames[depth++] = Frame{index, stack, -1, -1, 0, {0, 0, 0}};
         continue;
       }
     }
     if (depth == 0) {
-      if (cursor != n || stack != 1 || completed != v.slot_type || stack_bound > kMaxStack || stack_bound < 1) return -1;
-      if (!emit(OP_RETURN, v.return_fuel, 0, 0, 0)) return -1;
+      // a value phase leaves its value for the appended RETURN; a statement
+      // program returns by its own RETURNs and has no terminator
+      // (patch_whole_program, phase_layout.hpp:494-496)
+      if (cursor != n || stack != (statements ? 0 : 1) || completed != v.slot_type || stack_bound > kMaxStack)
+        return -1;
+      if (!statements && (stack_bound < 1 || !emit(OP_RETURN, v.return_fuel, 0, 0, 0))) return -1;
       result->code = count;
       result->constants = nconst;
       result->locals = total_locals;
@@ -361,10 +423,89 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
       code[5 * f.first_jump + 2] = count;
       stack = f.base_stack;
     }
+    if (e.node_kind == TK_FOR_RANGE && f.seen == 1) {
+      // for_range (phase_compile.cuh:767-807): store the bound, fail on a
+      // bound that is not an Int or is negative (NEG of true, a type
+      // error), then count from zero, copying the counter into the named
+      // target at the top of every pass
+      Loop& l = loops[loop_depth - 1];
+      if (is_statement_tag(completed)) return -1;
+      if (!emit(OP_STORE, 1, l.bound, 0, kHasA)) return -1;
+      stack = f.base_stack;
+      if (!emit(OP_LOAD, 1, l.bound, 0, kHasA)) return -1;
+      grow(1);
+      if (!emit(OP_CALL_BUILTIN, 1, B_IS_INT, 1, kHasA | kHasB)) return -1;
+      const int bad = count;
+      if (!emit(OP_JMP_IF_FALSE, 1, 0, 0, kHasA)) return -1;
+      stack = f.base_stack;
+      if (!emit(OP_LOAD, 1, l.bound, 0, kHasA)) return -1;
+      grow(1);
+      const int zero_test = add_const(0);
+      if (zero_test < 0 || !emit(OP_PUSH_CONST, 1, zero_test, 0, kHasA)) return -1;
+      grow(1);
+      if (!emit(OP_LT, 1, 0, 0, 0)) return -1;
+      const int valid = count;
+      if (!emit(OP_JMP_IF_FALSE, 1, 0, 0, kHasA)) return -1;
+      stack = f.base_stack;
+      code[5 * bad + 2] = count;
+      const int truth = add_const(1);
+      if (truth < 0 || !emit(OP_PUSH_CONST, 1, truth, 0, kHasA | kBoolConst)) return -1;
+      grow(1);
+      if (!emit(OP_NEG, 1, 0, 0, 0)) return -1;
+      code[5 * valid + 2] = count;
+      stack = f.base_stack;
+      const int zero = add_const(0);
+      l.one = add_const(1);
+      if (zero < 0 || l.one < 0) return -1;
+      l.counter = temporary();
+      const int user = variable_slot(e.operand);
+      if (l.counter < 0 || user < 0) return -1;
+      if (!emit(OP_PUSH_CONST, 1, zero, 0, kHasA)) return -1;
+      grow(1);
+      if (!emit(OP_STORE, 1, l.counter, 0, kHasA)) return -1;
+      stack = f.base_stack;
+      l.head = count;
+      if (!emit(OP_LOAD, 1, l.counter, 0, kHasA) || !emit(OP_LOAD, 1, l.bound, 0, kHasA)) return -1;
+      grow(2);
+      if (!emit(OP_LT, 1, 0, 0, 0)) return -1;
+      l.end_jump = count;
+      if (!emit(OP_JMP_IF_FALSE, 1, 0, 0, kHasA)) return -1;
+      stack = f.base_stack;
+      if (!emit(OP_LOAD, 1, l.counter, 0, kHasA)) return -1;
+      grow(1);
+      if (!emit(OP_STORE, 1, user, 0, kHasA)) return -1;
+      stack = f.base_stack;
+    }
     if (f.seen < e.arity) { have_value = false; continue; }
     if (e.node_kind == TK_IF) {
       if (f.args[1] != f.args[2]) return -1;
       code[5 * f.second_jump + 2] = count;
+    } else if (e.node_kind == TK_PROGRAM) {
+      if (!is_statement_tag(completed)) return -1;
+    } else if (e.node_kind == TK_BLOCK) {
+      if (!is_statement_tag(f.args[0]) || !is_statement_tag(f.args[1])) return -1;
+    } else if (e.node_kind == TK_ASSIGN || e.node_kind == TK_RETURN) {
+      // the grammar fixes the stored or returned type; an assigned grammar
+      // local gets its slot after its value's temporaries
+      if (completed != e.type || is_statement_tag(completed)) return -1;
+      if (e.node_kind == TK_ASSIGN) {
+        const int slot = variable_slot(e.operand);
+        if (slot < 0 || !emit(OP_STORE, e.fuel, slot, 0, kHasA)) return -1;
+      } else if (!emit(OP_RETURN, e.fuel, 0, 0, 0)) {
+        return -1;
+      }
+      stack = f.base_stack;
+      completed = kStatementTag;
+    } else if (e.node_kind == TK_FOR_RANGE) {
+      if (!is_statement_tag(completed)) return -1;
+      const Loop l = loops[--loop_depth];
+      if (!emit(OP_LOAD, 1, l.counter, 0, kHasA) || !emit(OP_PUSH_CONST, 1, l.one, 0, kHasA)) return -1;
+      grow(2);
+      if (!emit(OP_ADD, 1, 0, 0, 0) || !emit(OP_STORE, 1, l.counter, 0, kHasA) || !emit(OP_JMP, 1, l.head, 0, kHasA))
+        return -1;
+      code[5 * l.end_jump + 2] = count;
+      stack = f.base_stack;
+      while (live_count > l.live_begin) freed[free_count++] = live[--live_count];
     } else if (e.node_kind == TK_AND || e.node_kind == TK_OR) {
       if (completed != GAGP_TAG_BOOL) return -1;
       if (!emit(OP_NOT, e.fuel, 0, 0, 0) || !emit(OP_NOT, e.fuel, 0, 0, 0)) return -1;

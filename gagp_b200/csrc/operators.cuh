@@ -208,6 +208,26 @@ __device__ inline int warp_find_member(const SearchDesc& s, const SRow& row) {
   return -1;
 }
 
+// locals_defined of a row of node words, for a statement program (true for
+// a value phase, whose reads are inputs and binders only).  Out of line: the
+// walk's frame stack stays out of the variation kernel's own frame.
+__device__ __noinline__ bool row_locals_defined(const SearchDesc& s, const uint64_t* node, int n) {
+  return locals_defined(n, [&](int i) {
+    const uint64_t w = node[i];
+    const ExprInfo& x = s.info[w_origin(w)];
+    return StatementNode{x.kind == EK_OPERATION ? int(x.node_kind) : -1, x.operand, w_arity(w), int(x.type)};
+  });
+}
+// The same for a row in a warp's shared memory: lane 0 walks it and every
+// lane returns its answer.
+__device__ inline bool warp_locals_defined(const SearchDesc& s, const uint64_t* node, int n) {
+  if (!is_statement_tag(s.slot_type)) return true;
+  __syncwarp();
+  bool ok = false;
+  if (lane_id() == 0) ok = row_locals_defined(s, node, n);
+  return __shfl_sync(kFull, ok, 0);
+}
+
 // One child, by one warp.  Writes the child row, its parent and reuse
 // source (the parent when the genotype is unchanged; k_lower looks for an
 // identical current member otherwise) and returns the
@@ -244,7 +264,9 @@ __device__ inline int warp_vary_child(const SearchDesc& s, const char* image, in
       if (total - (ae - dest) + (be - src) > s.maxv) continue;
       const GenResult r = warp_splice(w.parent, dest, ae, w.donor, src, be, w.out, s.stride, s.slot_max_depth,
                                       s.site_depth);
-      if (r.status == ST_OK) {
+      // a splice that reads a grammar local before assigning it is a
+      // rejected attempt (crossover_child, phase_operators.cuh:185)
+      if (r.status == ST_OK && warp_locals_defined(s, w.out.node, r.nodes)) {
         warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
         w.child.n = r.nodes;
         w.child.nc = r.constants;
@@ -294,9 +316,14 @@ __device__ inline int warp_vary_child(const SearchDesc& s, const char* image, in
           const GenResult r = warp_splice(w.child, dest, end, w.gen, 0, w.gen.n, w.out, s.stride, s.slot_max_depth,
                                           s.site_depth);
           if (r.status != ST_OK) return 8;
-          warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
-          w.child.n = r.nodes;
-          w.child.nc = r.constants;
+          // a mutation that reads a grammar local before assigning it is
+          // dropped and the crossed child stands (mutate_child,
+          // phase_operators.cuh:240-241)
+          if (warp_locals_defined(s, w.out.node, r.nodes)) {
+            warp_copy(w.out.node, w.out.cval, r.nodes, r.constants, w.child.node, w.child.cval);
+            w.child.n = r.nodes;
+            w.child.nc = r.constants;
+          }
         }
       }
     }

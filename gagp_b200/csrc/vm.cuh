@@ -326,7 +326,7 @@ __device__ inline void run_accumulator(const SearchDesc& s, int slot, const VmWa
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       const int c = tile + k * 32 + lane;
-      if (c < case_end) loss += case_loss(s, s.slot_type, acc[k], cur_want[k], wrong);
+      if (c < case_end) loss += case_loss(s, s.result_type, acc[k], cur_want[k], wrong);
     }
   }
   __syncwarp();
@@ -452,6 +452,13 @@ __host__ __device__ inline bool run_program(const VmView& v, const int32_t* code
       case OP_CALL_BUILTIN: {
         if (b < 0 || sp < b) return false;
         int64_t r;
+        if (a == B_IS_INT) {
+          // whether the value is an Int (builtins_cpu.cpp:493-499): a for_range's bound check
+          if (b != 1) return false;
+          sv[sp - 1] = st[sp - 1] == GAGP_TAG_INT;
+          st[sp - 1] = int8_t(GAGP_TAG_BOOL);
+          break;
+        }
         if (a == B_LEN || a == B_INDEX) {
           // a read-only view of an input list: length word, then elements
           if (b != (a == B_LEN ? 1 : 2) || st[sp - b] != GAGP_TAG_INTLIST) return false;
@@ -541,13 +548,24 @@ __host__ __device__ inline bool run_program(const VmView& v, const int32_t* code
 // every instruction runs) and counts as the instructions it stands for.  The
 // skipped slots are never reached: jumps land only on run starts.
 enum : int {
-  S_MOVE = 64, S_BIN_LL, S_BIN_LC, S_BIN_LL_ST, S_BIN_LC_ST, S_JCMP_LL, S_JCMP_LC, S_INDEX_LL_ST, S_BIN_ST
+  S_MOVE = 64, S_BIN_LL, S_BIN_LC, S_BIN_LL_ST, S_BIN_LC_ST, S_JCMP_LL, S_JCMP_LC, S_INDEX_LL_ST, S_BIN_ST, S_FAIL
 };
 constexpr int kSimdSlots = 24;
 constexpr int kSimdDone = 0x7fffffff;
 
 __device__ __forceinline__ uint4 simd_plain(int op, int a, int cost) {
   return make_uint4(uint32_t(op & 0x7f) | (1u << 8) | (uint32_t(cost) << 16), uint32_t(a), 0u, 0u);
+}
+// The staged word of instruction k of `code` (5 ints per instruction).  The
+// one type error the lowering emits on purpose -- NEG of the Bool constant
+// that a for_range pushes for a bound that is not a non-negative Int --
+// stages as S_FAIL, which charges the NEG's fuel and fails the case as the
+// reference's NEG does; every other NEG has an Int operand.
+__device__ __forceinline__ uint4 simd_stage(const int32_t* code, int k) {
+  const int32_t* x = code + 5 * k;
+  const bool bool_neg = x[0] == OP_NEG && k > 0 && code[5 * (k - 1)] == OP_PUSH_CONST &&
+                        (code[5 * (k - 1) + 1] & kBoolConst);
+  return simd_plain(bool_neg ? S_FAIL : x[0], x[2], x[4]);
 }
 __device__ __forceinline__ bool simd_binary_op(int op) {
   return op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_MOD || (op >= OP_LT && op <= OP_NE);
@@ -677,7 +695,9 @@ __device__ inline SimdCase run_program_simd(const VmView& v, const uint4* code, 
       }
       case OP_CALL_BUILTIN: {
         int64_t r = 0;
-        if (a == B_LEN) {
+        if (a == B_IS_INT) {
+          r = 1;  // a for_range bound: an Int in a well-typed program
+        } else if (a == B_LEN) {
           r = __ldg(&v.lists[at(sp - 1)]);
         } else if (a == B_INDEX) {
           const int64_t j0 = at(--sp), h = at(sp - 1), len_h = __ldg(&v.lists[h]);
@@ -730,6 +750,7 @@ __device__ inline SimdCase run_program_simd(const VmView& v, const uint4* code, 
         at(a) = r;
         break;
       }
+      case S_FAIL: ip = kSimdDone; break;  // NEG of a Bool: a type error
       default:
         ip = kSimdDone;  // not emitted by the lowering
     }

@@ -31,6 +31,9 @@ NO_ID = 0xFFFFFFFF
 
 # ValueTag (cpp/include/gagp/core/value.hpp:16-27)
 TAG_INT, TAG_FLOAT, TAG_BOOL, TAG_INTLIST, TAG_INVALID = 0, 1, 2, 5, 9
+# completion tag of a statement, never a runtime value (kPhaseStatement,
+# device/phase_compile.cuh:23)
+TAG_STATEMENT = 0xF0
 TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL}
 # with the list subset (tables only: the engine declines these grammars)
 LIST_TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL, "IntList": TAG_INTLIST}
@@ -39,14 +42,19 @@ LIST_TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL, "IntList": TAG_INTLIST}
 EK_OPERATION, EK_CONSTANT, EK_BOUND, EK_REFERENCE, EK_INPUT, EK_ALIAS = range(6)
 # PhaseTreeKind (device/phase_compile.cuh:21)
 TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR = range(6)
+TK_PROGRAM, TK_BLOCK, TK_NIL, TK_ASSIGN, TK_RETURN, TK_FOR_RANGE, TK_VAR = range(6, 13)
 TK_LET, TK_BOUND, TK_TRAVERSE = 13, 14, 16
+# grammar locals a phase can name (kPhaseNamedLocals), open lets and loops on
+# one lowering path (kPhaseLets, kPhaseLoops, kPhaseWalks) and the
+# evaluator's locals (MAX_LOCALS)
+NAMED_LOCALS, LOWER_LETS, LOWER_LOOPS, LOWER_WALKS, MAX_LOCALS = 16, 16, 16, 8, 64
 # Opcode (cpp/include/gagp/core/opcode.hpp:8-37)
 OP = {"push_const": 0, "load": 1, "store": 2, "neg": 3, "not": 4, "add": 5, "sub": 6, "mul": 7,
       "div": 8, "mod": 9, "lt": 10, "le": 11, "gt": 12, "ge": 13, "eq": 14, "ne": 15, "jmp": 16,
       "jmp_if_false": 17, "jmp_if_true": 18, "call_builtin": 19, "return": 20}
 # BuiltinId (cpp/include/gagp/core/builtin.hpp:13-45)
-BUILTIN = {"abs": 0, "min": 1, "max": 2, "clip": 3, "len": 4, "idiv0": 13, "imod0": 14,
-           "trunc_div0": 28, "trunc_mod0": 29}
+BUILTIN = {"abs": 0, "min": 1, "max": 2, "clip": 3, "len": 4, "index": 7, "is_int": 12, "idiv0": 13,
+           "imod0": 14, "trunc_div0": 28, "trunc_mod0": 29}
 
 # Scalar primitives of the catalog (cpp/src/evolution/grammar/catalog.cpp:83-116):
 # name -> (argument types, result type, tree kind, opcode, builtin operand, printed name).
@@ -90,6 +98,34 @@ for _state in ("Int", "Bool"):
         ("IntList", "Int", _state, _state), _state, TK_TRAVERSE, 0, 1, "traverse")
     LIST_CATALOG[f"traverse_reverse(IntList,Int,{_state},{_state})->{_state}"] = (
         ("IntList", "Int", _state, _state), _state, TK_TRAVERSE, 0, 2, "traverse_reverse")
+# index(xs, i): Python-style indexing, an error out of range (catalog.cpp:128)
+LIST_CATALOG["index(IntList,Int)->Int"] = (("IntList", "Int"), "Int", TK_OPERATION, OP["call_builtin"],
+                                          BUILTIN["index"], "index")
+
+
+def _controls() -> Dict[str, tuple]:
+    """Statement controls of the catalog (catalog.cpp:53-68): key ->
+    (argument slots as (category, value type or None for the control's own
+    result contract), result category, tree kind, printed name, whether it
+    names a local or input target)."""
+    out = {
+        "program(Block)->Program": ((("Block", None),), "Program", TK_PROGRAM, "program", False),
+        "block_nil()->Block": ((), "Block", TK_NIL, "block_nil", False),
+        "block_cons(Statement,Block)->Block": ((("Statement", None), ("Block", None)), "Block", TK_BLOCK,
+                                               "block_cons", False),
+        "if_stmt(Bool,Block,Block)->Statement": ((("Expression", "Bool"), ("Block", None), ("Block", None)),
+                                                 "Statement", TK_IF, "if_stmt", False),
+        "for_range(Int,Block)->Statement": ((("Expression", "Int"), ("Block", None)), "Statement", TK_FOR_RANGE,
+                                            "for_range", True),
+    }
+    for t in ("Int", "Bool", "IntList"):
+        out[f"assign({t})->Statement"] = ((("Expression", t),), "Statement", TK_ASSIGN, "assign", True)
+        out[f"return({t})->Statement"] = ((("Expression", t),), "Statement", TK_RETURN, "return", False)
+    return out
+
+
+CONTROLS = _controls()
+STATEMENT_CATEGORIES = ("Program", "Block", "Statement")
 
 
 class Declined(ValueError):
@@ -116,6 +152,8 @@ class Expression:
     result: str = ""          # grammar result type name
     scope_map: List[int] = field(default_factory=list)  # a reference's scope positions in its environment
     binding_types: List[int] = field(default_factory=list)  # a traversal body's element/index/state tags
+    category: str = "Expression"  # syntax category: Expression, or Program/Block/Statement
+    label: str = ""               # the local or input an assign, a for_range or a local read names
 
 
 @dataclass
@@ -150,6 +188,12 @@ class PhaseTables:
     fixed_nodes: int
     fuel: int
     names: List[str] = field(default_factory=list)  # printed name per expression
+    labels: List[str] = field(default_factory=list)  # named target per expression ("" for none)
+    # the value type a program returns: slot_type for an expression entry,
+    # the entry's result contract for a Program entry (slot_type is then the
+    # statement completion tag)
+    result_type: int = TAG_INVALID
+    local_names: List[str] = field(default_factory=list)  # grammar locals in declaration order
     # traversal table (HostPhaseGrammar::regions): a Traverse node's operand
     # indexes it; see Region
     regions: List["Region"] = field(default_factory=list)
@@ -190,11 +234,20 @@ class _Compiler:
         self.tags = LIST_TYPE_TAGS if allow_lists else TYPE_TAGS
         if doc.get("format_version") != "grammar-definition-v2":
             raise Declined("grammar-definition-v2 required")
-        for key in ("imports", "templates", "locals"):
+        for key in ("imports", "templates"):
             if doc.get(key):
                 raise Declined(f"grammar {key} are outside the resident scalar subset")
+        if doc.get("locals") and not allow_lists:
+            raise Declined("grammar locals are outside the resident scalar subset")
         self.doc = doc
         self.inputs = [(b["name"], b["type"]) for b in doc.get("inputs", [])]
+        # grammar locals in declaration order: a local's number is its
+        # position (compiled.cpp:155, binding())
+        self.locals = [(b["name"], b["type"]) for b in doc.get("locals", [])]
+        if any(t not in self.tags for _, t in self.locals):
+            raise Declined("only Int/Bool/IntList grammar locals are resident")
+        if {n for n, _ in self.locals} & {n for n, _ in self.inputs}:
+            raise Declined("local declaration conflicts with input name")
         rules = sorted(doc["nonterminals"], key=lambda r: r["id"])
         self.rules = rules
         self.nt_ids = {r["id"]: i for i, r in enumerate(rules)}
@@ -251,7 +304,8 @@ class _Compiler:
                     e.scope_map.append(len(names) - 1 - names[::-1].index(slot["name"]))
                 e.scope_count = len(e.scope_map)
             e.kind, e.target, e.result = EK_REFERENCE, target, rule["type"]
-            e.type = self.tags.get(rule["type"], TAG_INVALID)
+            e.category = rule.get("category", "Expression")
+            e.type = TAG_STATEMENT if e.category in STATEMENT_CATEGORIES else self.tags.get(rule["type"], TAG_INVALID)
         elif "bound" in value and self.allow_lists:
             names = [n for n, _ in scope]
             if value["bound"] not in names:
@@ -260,6 +314,65 @@ class _Compiler:
             t = scope[position][1]
             e.kind, e.node_kind, e.target = EK_BOUND, TK_BOUND, position
             e.type, e.result, e.name = self.tags.get(t, TAG_INVALID), t, value["bound"]
+        elif "local" in value and self.allow_lists:
+            # a read of a grammar local (a Var node naming the local)
+            names = [n for n, _ in self.locals]
+            if value["local"] not in names:
+                raise Declined("unknown grammar local")
+            idx = names.index(value["local"])
+            if idx >= NAMED_LOCALS:
+                raise Declined("grammar local capacity")
+            t = self.locals[idx][1]
+            e.kind, e.node_kind, e.operand = EK_OPERATION, TK_VAR, idx
+            e.type, e.result, e.name, e.label = self.tags[t], t, "var", value["local"]
+        elif "control" in value and self.allow_lists:
+            # a statement control (compiled.cpp:498-526): its argument slots
+            # are typed expressions or statement categories carrying the
+            # control's own result contract ("type")
+            if value["control"] not in CONTROLS:
+                raise Declined(f"control {value['control']} is outside the resident subset")
+            slots, category, tree_kind, name, named = CONTROLS[value["control"]]
+            contract = value.get("type")
+            if contract not in self.tags:
+                raise Declined("statement result contract outside Int, Bool and IntList")
+            if tree_kind == TK_RETURN and slots[0][1] != contract:
+                raise Declined("return type disagrees with enclosing result contract")
+            e.operand = 0
+            if named:
+                if ("name" in value) + ("input_name" in value) != 1:
+                    raise Declined("control requires exactly one name or input_name target")
+                targets = self.inputs if "input_name" in value else self.locals
+                target = value["input_name"] if "input_name" in value else value["name"]
+                tnames = [n for n, _ in targets]
+                if target not in tnames:
+                    raise Declined("control target is not visible")
+                idx = tnames.index(target)
+                if targets[idx][1] != slots[0][1]:
+                    raise Declined("control target local type mismatch")
+                if "input_name" in value:
+                    e.operand = ("input", idx)  # resolved to -1 - evaluator position by the table builder
+                else:
+                    if idx >= NAMED_LOCALS:
+                        raise Declined("grammar local capacity")
+                    e.operand = idx
+                e.label = target
+            elif "name" in value or "input_name" in value:
+                raise Declined("control does not accept a target name")
+            args = value.get("args", [])
+            if len(args) != len(slots):
+                raise Declined("control argument count mismatch")
+            children = [self.expression(a, scope) for a in args]
+            for c, (cat, t) in zip(children, slots):
+                if self.exprs[c].category != cat or self.exprs[c].result != (t if cat == "Expression" else contract):
+                    raise Declined("control argument category or type mismatch")
+            e.kind, e.node_kind, e.arity, e.category = EK_OPERATION, tree_kind, len(children), category
+            e.result, e.name = contract, name
+            # a statement completes without a value; an assign or a return
+            # carries its value's type (phase_grammar.hpp:177,327-329)
+            e.type = self.tags[slots[0][1]] if tree_kind in (TK_ASSIGN, TK_RETURN) else TAG_STATEMENT
+            for i, c in enumerate(children):
+                e.children[i] = c
+                e.child_scope[i] = len(scope)
         elif "signature" in value:
             sig = value["signature"]
             if sig in CATALOG:
@@ -309,9 +422,10 @@ class _Compiler:
 
     def compile(self):
         for i, rule in enumerate(self.rules):
-            if rule.get("category", "Expression") != "Expression":
+            category = rule.get("category", "Expression")
+            if category != "Expression" and (not self.allow_lists or category not in STATEMENT_CATEGORIES):
                 raise Declined("statement grammars are outside the scalar subset")
-            if rule["type"] not in TYPE_TAGS:
+            if rule["type"] not in (self.tags if category != "Expression" else TYPE_TAGS):
                 raise Declined("only Int/Bool nonterminals are resident")
             scope = [(slot["name"], slot["type"]) for slot in rule.get("scope", [])]
             if scope and (not self.allow_lists or any(t not in self.tags for _, t in scope) or len(scope) > 8):
@@ -321,7 +435,7 @@ class _Compiler:
                 if not (w > 0) or w == float("inf"):
                     raise Declined("production weight")
                 x = self.expression(alt["expression"], scope)
-                if self.exprs[x].result != rule["type"]:
+                if self.exprs[x].result != rule["type"] or self.exprs[x].category != category:
                     raise Declined("production result type mismatch")
                 self.nt_productions[i].append(len(self.productions))
                 self.productions.append((i, x, w))
@@ -339,9 +453,12 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
     c = _Compiler(doc, allow_lists)
     c.compile()
     entry = doc["entry"]
-    if entry.get("category", "Expression") != "Expression":
-        raise Declined("Program-entry grammars are outside the scalar subset")
     root_nt = c.nt_ids[entry["nonterminal"]]
+    # a Program entry is its own whole-program phase, without the expression
+    # entry's terminator (phase_layout.hpp:118-130)
+    program_entry = c.rules[root_nt].get("category", "Expression") == "Program"
+    if c.rules[root_nt].get("category", "Expression") not in ("Expression", "Program"):
+        raise Declined("whole-program phase requires an expression or program entry")
     limits = doc["search_limits"]
     max_depth, max_nodes = int(limits["max_depth"]), int(limits["max_nodes"])
     fuel = int(doc["execution_limits"]["fuel"])
@@ -376,6 +493,9 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         nt_env[i] = env
         out_nts[i][0] = len(out_prods)
         out_nts[i][2] = len(c.rules[i].get("scope", []))
+        # a nonterminal with variation disabled opens no variation site
+        # (phase_variation.hpp:13)
+        out_nts[i][4] = not c.rules[i].get("variation", True)
         for p in c.nt_productions[i]:
             _, x, w = c.productions[p]
             out_prods.append((x, w))
@@ -393,6 +513,7 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         e = c.exprs[i]
         x = out_expr[i]
         x.kind, x.type, x.target, x.name, x.result = e.kind, e.type, e.target, e.name, e.result
+        x.category, x.label = e.category, e.label
         if e.kind == EK_REFERENCE:
             x.scope_count, x.scope_map = e.scope_count, list(e.scope_map)
             visit_nt(e.target, [env[m] for m in e.scope_map])
@@ -400,6 +521,10 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         x.node_kind, x.opcode, x.operand, x.arity = e.node_kind, e.opcode, e.operand, e.arity
         x.children, x.child_scope = list(e.children), list(e.child_scope)
         child_env = [env] * e.arity
+        if isinstance(e.operand, tuple):
+            # an input target is the preset evaluator slot -1 - position
+            # (phase_grammar.hpp:310-320)
+            x.operand = -1 - names.index(grammar_inputs[e.operand[1]])
         if e.kind == EK_BOUND:
             x.operand = env[e.target]
         elif e.node_kind == TK_LET:
@@ -452,12 +577,17 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
     # An expression entry runs as program(block(return e)): the phase starts at
     # AST depth 4 and keeps max_depth - 3 levels (phase_layout.hpp:131-134),
     # and the four wrapper nodes are the layout's fixed nodes.
-    slot_max_depth = max_depth - 3
+    # A Program entry's phase is the whole tree: it starts at depth 1 and has
+    # no fixed nodes.
+    slot_max_depth = max_depth if program_entry else max_depth - 3
     if slot_max_depth < 1:
         raise Declined("max_depth leaves no room for the entry phase")
-    entry_expr = Expression(kind=EK_REFERENCE, target=root_nt, name="", result=c.rules[root_nt]["type"])
+    entry_expr = Expression(kind=EK_REFERENCE, target=root_nt, name="", result=c.rules[root_nt]["type"],
+                            category=c.rules[root_nt].get("category", "Expression"))
     root_expression = n_expr
     out_expr.append(entry_expr)
+    _check_lowering_capacity(out_expr, out_nts, out_prods, seen_expr | {root_expression}, root_expression,
+                             depth_count, max_depth, len(names), len(c.locals))
     logical_count = site_depth + 1 if site_depth else 1
     minimum = _minimum_table(out_expr, out_nts, out_prods, seen_expr | {root_expression}, depth_count,
                              logical_count, site_depth > 0)
@@ -466,12 +596,71 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         nonterminals=[tuple(n) for n in out_nts], domains=out_domains, values=out_values,
         minimum=minimum, root_expression=root_expression, depth_count=depth_count,
         logical_depth_count=logical_count, site_depth=site_depth,
-        slot_max_depth=slot_max_depth, slot_type=TYPE_TAGS[c.rules[root_nt]["type"]],
+        slot_max_depth=slot_max_depth,
+        slot_type=TAG_STATEMENT if program_entry else TYPE_TAGS[c.rules[root_nt]["type"]],
         local_types=[c.tags[dict(c.inputs)[n]] for n in names], input_names=names,
-        max_nodes=max_nodes, fixed_nodes=4, fuel=fuel,
-        names=[e.name for e in out_expr], regions=regions)
+        max_nodes=max_nodes, fixed_nodes=0 if program_entry else 4, fuel=fuel,
+        names=[e.name for e in out_expr], regions=regions, labels=[e.label for e in out_expr],
+        result_type=c.tags[c.rules[root_nt]["type"]] if program_entry else TYPE_TAGS[c.rules[root_nt]["type"]],
+        local_names=[n for n, _ in c.locals])
     _normalize_static_weights(tables)
     return tables
+
+
+def _check_lowering_capacity(exprs, nts, prods, reachable, root, depth_count, max_depth, inputs, named_locals):
+    """Decline a grammar whose trees within the depth budget could run the
+    lowering out of its fixed tables (phase_grammar.hpp:455-498): over every
+    derivation, the open traversals, lets, loops and value ifs on one path and
+    the temporaries they hold (nine for a traversal, one for a let or a
+    loop), next to the inputs and the grammar locals."""
+    plain = _minimum_table(exprs, nts, prods, reachable, depth_count, 1, False)
+    TEMPS, WALKS, LETS, LOOPS, IFS = range(5)
+    memo = {}
+
+    def feasible(i, d):
+        return plain[i * depth_count + d] != NO_ID
+
+    def need(i, d):
+        key = (i, d)
+        if key in memo:
+            return memo[key]
+        e = exprs[i]
+        h = [0] * 5
+        if e.kind == EK_REFERENCE:
+            off, count = nts[e.target][0], nts[e.target][1]
+            for p in range(off, off + count):
+                x = prods[p][0]
+                if feasible(x, d):
+                    h = [max(a, b) for a, b in zip(h, need(x, d))]
+        elif d > 0:
+            for k in range(e.arity):
+                if feasible(e.children[k], d - 1):
+                    h = [max(a, b) for a, b in zip(h, need(e.children[k], d - 1))]
+            if e.node_kind == TK_TRAVERSE:
+                h[TEMPS] += 9
+                h[WALKS] += 1
+            elif e.node_kind == TK_LET:
+                h[TEMPS] += 1
+                h[LETS] += 1
+            elif e.node_kind == TK_FOR_RANGE:
+                h[TEMPS] += 1
+                h[LOOPS] += 1
+            elif e.node_kind == TK_IF and e.type != TAG_STATEMENT:
+                h[IFS] += 1
+        memo[key] = h
+        return h
+
+    import sys
+    old = sys.getrecursionlimit()
+    sys.setrecursionlimit(max(old, 100000))
+    try:
+        h = need(root, max_depth)
+    finally:
+        sys.setrecursionlimit(old)
+    named = min(named_locals, NAMED_LOCALS)
+    if (inputs + named + h[TEMPS] > MAX_LOCALS or h[WALKS] > LOWER_WALKS or h[LETS] > LOWER_LETS
+            or h[LOOPS] > LOWER_LOOPS or (h[WALKS] and h[IFS] > 16)):
+        raise Declined("lowering capacity within the depth budget requires native fallback")
 
 
 def _minimum_table(exprs, nts, prods, reachable, depth_count, logical_count, site_depth):

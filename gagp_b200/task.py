@@ -203,6 +203,29 @@ def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 
     def node():
         e = tables.expressions[origins[pos[0]]]
         pos[0] += 1
+        # statements (ProgramPrinter::node): a program prints its block, a
+        # block chain prints as one (block s1 s2 ...), a named control shows
+        # its target and a local read its name
+        if e.node_kind == G.TK_PROGRAM and e.kind == G.EK_OPERATION:
+            node()
+            return
+        if e.node_kind == G.TK_NIL and e.kind == G.EK_OPERATION:
+            out.append("(block)")
+            return
+        if e.node_kind == G.TK_BLOCK and e.kind == G.EK_OPERATION:
+            out.append("(block")
+            while True:
+                out.append(" ")
+                node()
+                tail = tables.expressions[origins[pos[0]]]
+                pos[0] += 1
+                if tail.node_kind != G.TK_BLOCK:
+                    break
+            out.append(")")
+            return
+        if e.node_kind == G.TK_VAR and e.kind == G.EK_OPERATION:
+            out.append(e.label)
+            return
         if e.kind == G.EK_CONSTANT:
             out.append(str(constants[k[0]]))
             k[0] += 1
@@ -224,6 +247,8 @@ def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 
             ids = [next_id[0]]
             next_id[0] += 1
         out.append("(" + e.name)
+        if e.node_kind in (G.TK_ASSIGN, G.TK_FOR_RANGE) and e.kind == G.EK_OPERATION:
+            out.append(" " + e.label)
         for i in range(e.arity):
             out.append(" ")
             if ids is not None and i == e.arity - 1:
@@ -236,5 +261,17 @@ def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 
                 node()
         out.append(")")
 
+    n = len(origins)
+    kinds = [tables.expressions[o].node_kind if tables.expressions[o].kind == G.EK_OPERATION else -1
+             for o in origins]
+    if n >= 4 and kinds[0] == G.TK_PROGRAM and kinds[1] == G.TK_BLOCK and kinds[2] == G.TK_RETURN \
+            and kinds[-1] == G.TK_NIL:
+        # a program that is a single `return e` reads as just `e`
+        pos[0] = 3
+        node()
+        if pos[0] == n - 1:
+            return "".join(out)
+        out.clear()
+        pos[0], k[0], next_id[0] = 0, 0, first_binder
     node()
     return "".join(out)

@@ -21,8 +21,11 @@ Workloads:
   the target is the sum of the elements above t, their count, or the
   maximum (0 for an empty list); the grammar folds xs with a traversal
   whose step (binders element, index, accumulator) adds, subtracts and
-  compares.  This engine declines these grammars at admission; the
-  reference runs them resident.
+  compares.
+* ``list_statements`` -- the same list cases searched by a statement
+  program: a Program entry whose blocks assign grammar locals, loop with
+  for_range, branch with if_stmt and return, reading xs through len and
+  index.
 
 Inputs are generated with ``random.Random(seed)``.
 """
@@ -213,6 +216,81 @@ def list_threshold(population: int = 8192, generations: int = 96, seed: int = 0,
                      train=train, search=search_config(population, generations, seed))
 
 
+def list_statements_grammar(max_nodes: int = 64, max_depth: int = 12, fuel: int = 4096) -> dict:
+    """A statement grammar over the list cases: the program assigns the
+    local acc, then runs statements (assignments to acc, k or the input t,
+    for_range loops counting i, if_stmt branches, returns) and ends with a
+    return; expressions read t, small constants, the locals, len(xs) and
+    index(xs, e)."""
+    def control(key, args, **extra):
+        return dict({"control": key, "type": "Int", "args": args}, **extra)
+
+    ref = lambda n: {"ref": n}  # noqa: E731
+    binary = lambda op, a, b: {"signature": f"{op}(Int,Int)->Int", "args": [ref(a), ref(b)]}  # noqa: E731
+    compare = lambda op: {"signature": f"{op}(Int,Int)->Bool", "args": [ref("Value"), ref("Value")]}  # noqa: E731
+    return {
+        "format_version": "grammar-definition-v2",
+        "entry": {"category": "Program", "nonterminal": "Main", "type": "Int"},
+        "inputs": [{"name": "xs", "type": "IntList"}, {"name": "t", "type": "Int"}],
+        "locals": [{"name": "acc", "type": "Int"}, {"name": "i", "type": "Int"}, {"name": "k", "type": "Int"}],
+        "search_limits": {"max_nodes": max_nodes, "max_depth": max_depth},
+        "execution_limits": {"fuel": fuel},
+        "nonterminals": [
+            {"id": "Main", "category": "Program", "type": "Int", "scope": [], "variation": False, "alternatives": [
+                {"id": "main", "weight": 1, "expression": control("program(Block)->Program", [
+                    control("block_cons(Statement,Block)->Block", [
+                        control("assign(Int)->Statement", [ref("Value")], name="acc"), ref("Rest")])])}]},
+            {"id": "Rest", "category": "Block", "type": "Int", "scope": [], "alternatives": [
+                {"id": "more", "weight": 3, "expression": control("block_cons(Statement,Block)->Block",
+                                                                  [ref("Stmt"), ref("Rest")])},
+                {"id": "last", "weight": 1, "expression": control("block_cons(Statement,Block)->Block", [
+                    control("return(Int)->Statement", [ref("Value")]),
+                    control("block_nil()->Block", [])])}]},
+            {"id": "Body", "category": "Block", "type": "Int", "scope": [], "alternatives": [
+                {"id": "empty", "weight": 2, "expression": control("block_nil()->Block", [])},
+                {"id": "cons", "weight": 2, "expression": control("block_cons(Statement,Block)->Block",
+                                                                  [ref("Stmt"), ref("Body")])}]},
+            {"id": "Stmt", "category": "Statement", "type": "Int", "scope": [], "alternatives": [
+                {"id": "acc", "weight": 3, "expression": control("assign(Int)->Statement", [ref("Value")],
+                                                                 name="acc")},
+                {"id": "k", "weight": 1, "expression": control("assign(Int)->Statement", [ref("Value")], name="k")},
+                {"id": "t", "weight": 1, "expression": control("assign(Int)->Statement", [ref("Value")],
+                                                               input_name="t")},
+                {"id": "loop", "weight": 2, "expression": control("for_range(Int,Block)->Statement",
+                                                                  [ref("Bound"), ref("Body")], name="i")},
+                {"id": "when", "weight": 2, "expression": control("if_stmt(Bool,Block,Block)->Statement",
+                                                                  [ref("Test"), ref("Body"), ref("Body")])},
+                {"id": "ret", "weight": 1, "expression": control("return(Int)->Statement", [ref("Value")])}]},
+            {"id": "Bound", "type": "Int", "scope": [], "alternatives": [
+                {"id": "len", "weight": 3, "expression": {"signature": "len(IntList)->Int", "args": [{"input": "xs"}]}},
+                {"id": "small", "weight": 1, "expression": {"constant": {"type": "Int", "range": ["0", "3"]}}}]},
+            {"id": "Value", "type": "Int", "scope": [], "alternatives": [
+                {"id": "t", "weight": 2, "expression": {"input": "t"}},
+                {"id": "c", "weight": 2, "expression": {"constant": {"type": "Int", "range": ["-1", "2"]}}},
+                {"id": "acc", "weight": 3, "expression": {"local": "acc"}},
+                {"id": "i", "weight": 1, "expression": {"local": "i"}},
+                {"id": "k", "weight": 1, "expression": {"local": "k"}},
+                {"id": "at", "weight": 3, "expression": {"signature": "index(IntList,Int)->Int",
+                                                         "args": [{"input": "xs"}, ref("Value")]}},
+                {"id": "add", "weight": 2, "expression": binary("add", "Value", "Value")},
+                {"id": "sub", "weight": 1, "expression": binary("sub", "Value", "Value")}]},
+            {"id": "Test", "type": "Bool", "scope": [], "alternatives": [
+                {"id": "gt", "weight": 2, "expression": compare("gt")},
+                {"id": "lt", "weight": 1, "expression": compare("lt")},
+                {"id": "eq", "weight": 1, "expression": compare("eq")}]},
+        ],
+    }
+
+
+def list_statements(population: int = 8192, generations: int = 96, seed: int = 0, cases: int = 200,
+                    target: str = "threshold_sum", max_nodes: int = 64) -> "TaskFiles":
+    """The list cases of ``list_threshold`` searched with ``list_statements_grammar``."""
+    task = list_threshold(population=population, generations=generations, seed=seed, cases=cases, target=target)
+    task.name = f"list-statements-{target}-s{seed}"
+    task.grammar = list_statements_grammar(max_nodes=max_nodes)
+    return task
+
+
 def _log_uniform_population(rng: random.Random, lo: int, hi: int) -> int:
     # floor(lo * (hi / lo) ** u), u ~ U[0, 1)
     return int(lo * (hi / lo) ** rng.random())
@@ -276,7 +354,8 @@ def serving_mix(count: int = 2000, seed: int = 0) -> List[dict]:
     return out
 
 
-WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4, "list_threshold": list_threshold}
+WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4, "list_threshold": list_threshold,
+                                "list_statements": list_statements}
 
 
 def make(name: str, **kwargs) -> TaskFiles:

@@ -20,7 +20,10 @@ const char* gagp_oracle_last_error(void) { return g_error; }
 
 /* ----------------------------------------------------------------- types */
 enum { EK_OPERATION, EK_CONSTANT, EK_BOUND, EK_REFERENCE, EK_INPUT, EK_ALIAS };
-enum { TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR };
+enum { TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR, TK_PROGRAM, TK_BLOCK, TK_NIL, TK_ASSIGN,
+       TK_RETURN, TK_FOR_RANGE, TK_VAR };
+#define STATEMENT_TAG 0xF0     /* kPhaseStatement, device/phase_compile.cuh:23 */
+#define NAMED_LOCALS 16        /* kPhaseNamedLocals */
 enum { ST_OK, ST_INVALID, ST_UNSUPPORTED, ST_CAPACITY };
 enum {
   OP_PUSH_CONST = 0, OP_LOAD = 1, OP_STORE = 2, OP_NEG = 3, OP_NOT = 4, OP_ADD = 5, OP_SUB = 6,
@@ -84,6 +87,45 @@ typedef struct {
 static Node expression_node(const gagp_expression* e) {
   Node n = {e->node_kind, e->opcode, e->operand, e->arity, e->fuel, e->merge_fuel, e->type};
   return n;
+}
+
+/* Definite assignment of grammar locals in a statement program
+ * (phase_locals_defined, device/phase_compile.cuh:170-200): a local is
+ * readable after an assign, inside a for_range body naming it, and after a
+ * statement if only when both branches assigned it; a loop body's
+ * assignments end with the loop; inputs are always defined. */
+static int locals_defined(const Node* nodes, int count) {
+  struct { int index, seen; unsigned saved, branch; } frames[64];
+  int depth = 0;
+  unsigned mask = 0;
+#define LOCAL_BIT(operand) ((operand) >= 0 && (operand) < NAMED_LOCALS ? 1u << (operand) : 0u)
+  for (int i = 0; i < count; ++i) {
+    const Node node = nodes[i];
+    if (node.kind == TK_VAR && !(mask & LOCAL_BIT(node.operand))) return 0;
+    if (node.arity > 0) {
+      if (depth == 64) return 0;
+      frames[depth].index = i; frames[depth].seen = 0; frames[depth].saved = mask; frames[depth].branch = 0;
+      ++depth;
+      continue;
+    }
+    while (depth) {
+      const Node owner = nodes[frames[depth - 1].index];
+      const int seen = ++frames[depth - 1].seen;
+      if (owner.kind == TK_FOR_RANGE && seen == 1) {
+        frames[depth - 1].saved = mask; mask |= LOCAL_BIT(owner.operand);
+      } else if (owner.kind == TK_IF && owner.type == STATEMENT_TAG) {
+        if (seen == 1) frames[depth - 1].saved = mask;
+        else if (seen == 2) { frames[depth - 1].branch = mask; mask = frames[depth - 1].saved; }
+        else mask &= frames[depth - 1].branch;
+      }
+      if (seen < owner.arity) break;
+      if (owner.kind == TK_ASSIGN) mask |= LOCAL_BIT(owner.operand);
+      else if (owner.kind == TK_FOR_RANGE) mask = frames[depth - 1].saved;
+      --depth;
+    }
+  }
+#undef LOCAL_BIT
+  return depth == 0;
 }
 
 /* ------------------------------------------------ grammar random (SplitMix64)
@@ -491,7 +533,9 @@ static void crossover_child(int child, const Trees* input, Trees* output, const 
     const int slot = destination.row % slot_count, target = child * slot_count + slot;
     const Slot* s = &slots[slot];
     const Gen r = splice(&a, destination.node, &b, source.node, out_of(output, target), s->max_depth, s->logical_depth);
-    if (r.status == ST_OK) {
+    /* a statement program must read only definitely assigned locals
+     * (locals_defined, phase_operators.cuh:148-154,185) */
+    if (r.status == ST_OK && (s->type != STATEMENT_TAG || locals_defined(out_of(output, target).nodes, r.nodes))) {
       output->lengths[target] = r;
       stat->crossover = 1;
       return;
@@ -537,6 +581,8 @@ static void mutate_child(int child, Trees* input, Trees* output, Trees* scratch,
   const View donor = view_of(scratch, child);
   const Gen r = splice(&a, destination.node, &donor, 0, out_of(output, child), slot->max_depth, slot->logical_depth);
   if (r.status != ST_OK) { stat->error = 8; return; }
+  /* an undefined local read drops the mutation; the crossed child stands */
+  if (slot->type == STATEMENT_TAG && !locals_defined(out_of(output, child).nodes, r.nodes)) return;
   output->lengths[child] = r;
   copy_tree(output, child, input, destination.row);
   stat->mutation = 1;
@@ -1063,6 +1109,10 @@ static int initial_rows(const Search* s, int population, uint64_t seed, int site
       generated = generate_phase(&s->slot.G, g->root_expression, 0, g->slot_max_depth, (int)room,
                                  mix64(seed ^ mix64(((uint64_t)i * 8 + 0) * 64 + (uint64_t)attempt)),
                                  o.nodes, o.origins, o.constants, o.sites, logical);
+      /* a statement program that reads an unassigned local is retried
+       * (phase_population_cpu.cpp:95-96) */
+      if (generated.status == ST_OK && g->slot_type == STATEMENT_TAG && !locals_defined(o.nodes, generated.nodes))
+        generated.status = ST_INVALID;
       if (generated.status != ST_OK && attempt % 4 == 3 && logical < site_limit) ++logical;
       if (attempt >= 256) FAIL("initial phase generation failed");
     }

@@ -84,11 +84,19 @@ def test_admission_declines_outside_the_resident_subset(poly_task):
         blob.expressions[_first(blob, W_KINDS["input"])].kind = 5  # an alias (template instance)
     assert _bytes(poly_task, template)[0] == 1  # GAGP_DECLINED
 
+    def region(blob):
+        e = next(i for i in range(len(blob.tables.expressions))
+                 if blob.expressions[i].kind == W_KINDS["operation"] and blob.expressions[i].arity > 0)
+        blob.expressions[e].node_kind = 15  # a bounded region
+    assert _bytes(poly_task, region)[0] == 1
+
+    # a statement belongs to a Program entry's phase: in a value phase the
+    # tables are malformed
     def statement(blob):
         e = next(i for i in range(len(blob.tables.expressions))
                  if blob.expressions[i].kind == W_KINDS["operation"] and blob.expressions[i].arity > 0)
         blob.expressions[e].node_kind = 9  # Assign
-    assert _bytes(poly_task, statement)[0] == 1
+    assert _bytes(poly_task, statement)[0] == 2
 
 
 def test_admission_of_the_generational_schedule(poly_task):

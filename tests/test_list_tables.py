@@ -8,7 +8,8 @@ reference's compile_phase_grammar output (phase_grammar.hpp:94-300, weights
 normalised by normalize_static_phase_weights) for the fixtures that
 tests/golden/make_golden.py records from the reference engine, including a
 nested traversal whose body maps the outer accumulator and the inner binders
-by name.
+by name, and a statement program (Program entry, grammar locals, assign,
+for_range, if_stmt and return controls, a variation-disabled entry).
 """
 import pytest
 
@@ -54,16 +55,27 @@ def test_list_tables_match_reference(name):
 @pytest.mark.parametrize("name", NAMES)
 def test_list_tasks_run_resident_in_the_reference(name):
     """The recorded reference runs took the resident path (no decline)."""
-    run = GU.list_fixture(name)["run"]
+    fx = GU.list_fixture(name)
+    run = fx["run"]
     assert run["declined"] == ""
-    assert len(run["history"]) == 3 and run["history"][0]["text"].startswith("(traverse xs")
+    assert len(run["history"]) == 3
+    if fx["grammar"]["entry"].get("category") == "Program":
+        # a statement program: the reference's tables hold its controls and
+        # the slot is the whole program, without a terminator
+        assert fx["tables"]["layout"]["program_terminator"] == 0 and fx["tables"]["layout"]["fixed_nodes"] == 0
+    else:
+        assert run["history"][0]["text"].startswith("(traverse xs")
 
 
 def test_every_list_run_took_the_resident_path():
     for name in GU.list_names():
-        run = GU.list_fixture(name)["run"]
+        fx = GU.list_fixture(name)
+        run = fx["run"]
         assert run["declined"] == "", name
-        assert any(h["text"].startswith("(traverse") for h in run["history"]), name
+        if fx["grammar"]["entry"].get("category") == "Program":
+            assert any("for_range" in h["text"] or "(block" in h["text"] for h in run["history"]), name
+        else:
+            assert any(h["text"].startswith("(traverse") for h in run["history"]), name
 
 
 @pytest.mark.parametrize("name", NAMES)
