@@ -109,7 +109,9 @@ typedef struct gagp_region {
 } gagp_region;
 
 /* The admitted grammar of one search: phase tables plus its single
- * whole-program slot (expression entry: program(block(return phase))). */
+ * whole-program slot (expression entry: program(block(return phase)), four
+ * fixed nodes; Program entry: the whole statement program, no fixed nodes
+ * and no terminator). */
 typedef struct gagp_grammar {
   const gagp_expression* expressions; int32_t expression_count;
   const gagp_production* productions; int32_t production_count;
@@ -122,7 +124,8 @@ typedef struct gagp_grammar {
   int32_t site_depth;               /* 0: no site-depth limit */
   int32_t root_expression;
   int32_t slot_max_depth;
-  int32_t slot_type;                /* ValueTag of the phase result */
+  int32_t slot_type;                /* ValueTag of the phase result, or 0xF0 (kPhaseStatement) for a
+                                       Program entry's statement program, whose returns carry its type */
   int32_t local_count;              /* evaluator inputs, sorted by name */
   int32_t local_types[GAGP_MAX_LOCALS];
   int32_t max_nodes;                /* grammar search_limits.max_nodes */

@@ -232,6 +232,7 @@ GEN_CASES = [
     ("gen_poly4_exact_e2", "poly4_exact", dict(population=256, generations=6, seed=44, cases=40), {"elitism": 2}),
     ("gen_list_e2", "list", dict(population=128, generations=5, seed=45, cases=20), {"elitism": 2}),
     ("gen_poly4_p4096", "poly4", dict(population=4096, generations=4, seed=46, cases=64), {"elitism": 3}),
+    ("gen_statements_e2", "list_statements", dict(population=128, generations=5, seed=47, cases=20), {"elitism": 2}),
 ]
 
 
@@ -269,6 +270,7 @@ INIT_CASES = [
     ("init_list", "list", dict(population=96, generations=2, seed=52, cases=20), 4, {}),
     ("init_generational", "poly4", dict(population=120, generations=3, seed=53, cases=32, max_nodes=40), 5,
      {"schedule": {"mode": "generational"}, "elitism": 2}),
+    ("init_statements", "list_statements", dict(population=96, generations=2, seed=54, cases=20), 4, {}),
 ]
 
 
@@ -307,6 +309,7 @@ JUDGE_CASES = [
     ("judge_bool_absolute", "bool", dict(population=96, generations=1, seed=34)),
     ("judge_bool_exact", "bool_exact", dict(population=96, generations=1, seed=35)),
     ("judge_poly4_exact", "poly4_exact", dict(population=96, generations=1, seed=36, cases=40)),
+    ("judge_statements", "statements", dict(population=96, generations=1, seed=38, cases=24)),
 ]
 JUDGE_RUN = ("judge_run_polynomial", dict(population=512, generations=24, seed=37))
 REF_CLI = os.path.join(ROOT, "oracle", "_ref", "gagp")
@@ -350,6 +353,9 @@ def judge_task(workload: str, kwargs: dict) -> "W.TaskFiles":
         task = W.polynomial(**kwargs)
     elif workload == "list":
         task = W.list_threshold(**kwargs)
+        task.test = W.list_threshold(population=8, generations=1, seed=kwargs["seed"] + 1000, cases=30).train
+    elif workload == "statements":
+        task = W.list_statements(**kwargs)
         task.test = W.list_threshold(population=8, generations=1, seed=kwargs["seed"] + 1000, cases=30).train
     elif workload == "bool":
         task = bool_task(**kwargs)

@@ -68,3 +68,29 @@ def test_rows_outside_the_grammar_are_refused(engine):
     with pytest.raises(EngineError) as err:  # the root's origin is a reference, not a production
         engine.admit(lt, initial=_rows(lt, [bad] + members[1:]))
     assert err.value.status == 2
+
+
+def test_statement_rows_reading_an_unassigned_local_are_refused(engine):
+    """A statement program whose first assignment reads the local it
+    assigns (acc = acc) fails the definite-assignment check and is refused,
+    as the reference's verifier refuses it."""
+    from gagp_b200 import grammar as G
+    from gagp_b200.engine import EngineError
+    fx = _fixture("init_statements")
+    lt = GU.load_task(fx)
+    ex = lt.tables.expressions
+    read_acc = next(i for i, e in enumerate(ex) if e.kind == G.EK_OPERATION and e.node_kind == G.TK_VAR
+                    and e.label == "acc")
+    member = fx["initial"][0]
+    origins, constants = list(member["origins"]), list(member["constants"])
+    # program, block_cons, assign acc, then the assigned value's subtree
+    assert [ex[o].node_kind for o in origins[:3]] == [G.TK_PROGRAM, G.TK_BLOCK, G.TK_ASSIGN]
+    end, pending = 3, 1
+    while pending:
+        pending += ex[origins[end]].arity - 1
+        end += 1
+    dropped = sum(1 for o in origins[3:end] if ex[o].kind == G.EK_CONSTANT)
+    bad = dict(member, origins=origins[:3] + [read_acc] + origins[end:], constants=constants[dropped:])
+    with pytest.raises(EngineError) as err:
+        engine.admit(lt, initial=_rows(lt, [bad] + fx["initial"][1:]))
+    assert err.value.status == 2 and "local" in str(err.value)
