@@ -51,7 +51,19 @@ class Value(C.Structure):
 class Region(C.Structure):
     _fields_ = [("traversal", C.c_int32), ("ranged", C.c_int32), ("fuel_profile", C.c_int32),
                 ("binders", C.c_int32 * 3), ("operand_types", C.c_int32 * 6), ("binding_types", C.c_int32 * 3),
-                ("result_type", C.c_int32), ("event_cost", C.c_uint32 * 26)]
+                ("result_type", C.c_int32), ("event_cost", C.c_uint32 * 26),
+                # a bounded region (traversal 0)
+                ("operands", C.c_int32), ("phases", C.c_int32), ("captures", C.c_int32),
+                ("capture_kind", C.c_int32 * 8), ("capture_target", C.c_int32 * 8), ("phase_type", C.c_int32 * 8),
+                ("phase_bindings", C.c_int32 * 8), ("binding_bank", (C.c_int32 * 8) * 8),
+                ("binding_slot", (C.c_int32 * 8) * 8), ("phase_binding_types", (C.c_int32 * 8) * 8),
+                ("state_count", C.c_int32), ("request_count", C.c_int32), ("axis_count", C.c_int32),
+                ("inclusive", C.c_int32), ("memoized", C.c_int32), ("frames", C.c_uint32), ("cells", C.c_uint32),
+                ("entry_fuel", C.c_uint32), ("parameter_types", C.c_int32 * 8),
+                ("transition_kind", (C.c_int32 * 4) * 8), ("transition_source", (C.c_int32 * 4) * 8),
+                ("axis_slot", C.c_int32 * 4), ("lower_kind", C.c_int32 * 4), ("upper_kind", C.c_int32 * 4),
+                ("reserved", C.c_int32), ("transition_offset", (C.c_int64 * 4) * 8),
+                ("lower", C.c_int64 * 4), ("upper", C.c_int64 * 4)]
 
 
 class Grammar(C.Structure):
@@ -118,6 +130,35 @@ def _ptr(array: np.ndarray, ctype):
     return array.ctypes.data_as(C.POINTER(ctype))
 
 
+def fill_bounded_region(x: Region, r) -> None:
+    """The bounded-region fields of a region table entry from the table
+    builder's plan (grammar.BoundedPlan)."""
+    p = r.plan
+    x.operands = len(p.state_types) + p.bound_count
+    x.phases = 4
+    x.captures = len(p.captures)
+    for c, (kind, target) in enumerate(p.captures):
+        x.capture_kind[c], x.capture_target[c] = kind, target
+    for ph in range(4):
+        x.phase_type[ph] = p.phase_types[ph]
+        x.phase_bindings[ph] = len(p.phase_bindings[ph])
+        for b, (bank, slot, tag) in enumerate(p.phase_bindings[ph]):
+            x.binding_bank[ph][b], x.binding_slot[ph][b], x.phase_binding_types[ph][b] = bank, slot, tag
+    x.state_count, x.request_count, x.axis_count = len(p.state_types), len(p.requests), len(p.axes)
+    x.inclusive, x.memoized = int(p.inclusive), int(p.memoized)
+    x.frames, x.cells, x.entry_fuel = p.frames, p.cells, p.entry_fuel
+    for k, tag in enumerate(p.parameter_types):
+        x.parameter_types[k] = tag
+    for q, row in enumerate(p.requests):
+        for st, (kind, source, offset) in enumerate(row):
+            x.transition_kind[q][st], x.transition_source[q][st], x.transition_offset[q][st] = kind, source, offset
+    for a, (slot, (lk, lv), (uk, uv)) in enumerate(p.axes):
+        x.axis_slot[a], x.lower_kind[a], x.lower[a], x.upper_kind[a], x.upper[a] = slot, lk, lv, uk, uv
+    for k, tag in enumerate(r.operand_types[:8]):
+        if k < 6:
+            x.operand_types[k] = tag
+
+
 class GrammarBlob:
     """Keeps the ctypes arrays of one ``gagp_grammar`` alive."""
 
@@ -168,8 +209,10 @@ class GrammarBlob:
             x.traversal, x.ranged, x.fuel_profile, x.result_type = r.traversal, int(r.ranged), 0, r.result_type
             for k in range(3):
                 x.binders[k], x.binding_types[k] = r.binders[k], r.binding_types[k]
-            for k, tag in enumerate(r.operand_types):
+            for k, tag in enumerate(r.operand_types[:6]):
                 x.operand_types[k] = tag
+            if r.plan is not None:
+                fill_bounded_region(x, r)
         g.regions, g.region_count = self.regions, len(t.regions)
         self.struct = g
 

@@ -26,7 +26,7 @@ namespace gb {
 enum { EK_OPERATION = 0, EK_CONSTANT = 1, EK_BOUND = 2, EK_REFERENCE = 3, EK_INPUT = 4, EK_ALIAS = 5 };
 enum { TK_CONSTANT = 0, TK_LOCAL = 1, TK_OPERATION = 2, TK_IF = 3, TK_AND = 4, TK_OR = 5, TK_PROGRAM = 6,
        TK_BLOCK = 7, TK_NIL = 8, TK_ASSIGN = 9, TK_RETURN = 10, TK_FOR_RANGE = 11, TK_VAR = 12, TK_LET = 13,
-       TK_BOUND = 14, TK_TRAVERSE = 16 };
+       TK_BOUND = 14, TK_REGION = 15, TK_TRAVERSE = 16 };
 // Completion tag of a statement (kPhaseStatement,
 // cpp/src/evolution/repro/gpu/device/phase_compile.cuh:23): a node or phase
 // type, never a runtime value.  Tables narrowed to int8_t keep it as -16.
@@ -216,6 +216,7 @@ struct GenTables {
   const gagp_domain* doms;
   const gagp_value* vals;
   const uint16_t* minimum;
+  const int4* extra;  // children 4..7 and their scopes, two int4 per expression (arity above 4 only)
 };
 __device__ __forceinline__ GenTables gen_tables(const SearchDesc& s, const char* image) {
   return GenTables{reinterpret_cast<const GenExpr*>(image), reinterpret_cast<const GenNt*>(image + s.gi.nt),
@@ -224,7 +225,8 @@ __device__ __forceinline__ GenTables gen_tables(const SearchDesc& s, const char*
                    reinterpret_cast<const GenEntry*>(image + s.gi.entry),
                    reinterpret_cast<const gagp_domain*>(image + s.gi.doms),
                    reinterpret_cast<const gagp_value*>(image + s.gi.vals),
-                   reinterpret_cast<const uint16_t*>(image + s.gi.minimum)};
+                   reinterpret_cast<const uint16_t*>(image + s.gi.minimum),
+                   reinterpret_cast<const int4*>(image + s.gi.extra)};
 }
 
 // A precomputed draw level (GenLevel) in registers.
@@ -403,6 +405,32 @@ __device__ inline GenResult generate(const SearchDesc& s, const char* image, int
     next_class = kNoClass;
     // the children's minimum costs, loaded together, then pushed last to
     // first (the first child straight into `next`); a traversal has four
+    if (arity > 4) {
+      // a bounded region: children 4..7 from the image's extra section,
+      // pushed last to first as below
+      const int4 xa = tables.extra[2 * t_expr], xb = tables.extra[2 * t_expr + 1];
+      for (int i = arity - 1; i >= 0; --i) {
+        if (count >= 192) { result.status = ST_CAPACITY; return result; }
+        const int child = i == 0 ? ra.x : i == 1 ? ra.y : i == 2 ? ra.z : i == 3 ? ra.w : i == 4 ? xa.x
+                          : i == 5 ? xa.y : i == 6 ? xa.z : xa.w;
+        const unsigned need = min_at(child, t_depth - 1, t_logical);
+        if (need > unsigned(capacity - result.nodes) || reserved > unsigned(capacity - result.nodes) - need) {
+          result.status = ST_CAPACITY;
+          return result;
+        }
+        const int child_scope = i < 4 ? int(int8_t((rb.w >> (8 * i)) & 0xff)) : int(int8_t((xb.x >> (8 * (i - 4))) & 0xff));
+        const int scope = child_scope >= 0 ? child_scope : t_scope;
+        const uint64_t t = pack(unsigned(child), unsigned(t_depth - 1), unsigned(scope), unsigned(t_logical), need);
+        if (i == 0) {
+          next = t;
+          have_next = true;
+        } else {
+          pending[count++] = t;
+        }
+        reserved += need;
+      }
+      continue;
+    }
     const unsigned need0 = arity > 0 ? min_at(ra.x, t_depth - 1, t_logical) : 0;
     const unsigned need1 = arity > 1 ? min_at(ra.y, t_depth - 1, t_logical) : 0;
     const unsigned need2 = arity > 2 ? min_at(ra.z, t_depth - 1, t_logical) : 0;

@@ -64,6 +64,7 @@ struct Search {
   // can fail); otherwise only the rare program past the accumulator VM's
   // limits does
   bool exact_heavy = false;
+  size_t region_words = 0;  // the largest bounded-region plan's workspace per lane (0: none)
   gb::SearchDesc* d_desc = nullptr;   // single-search batch descriptor
   int32_t* d_off = nullptr;           // {0, P, 0, B}: member and child offsets
 };
@@ -91,7 +92,13 @@ struct gagp_engine {
   // batch scratch
   gb::ProgramRef* d_fast = nullptr;
   gb::ProgramRef* d_general = nullptr;
+  gb::ProgramRef* d_region = nullptr;  // programs with bounded regions, deferred by the exact VM
   int32_t* d_counts = nullptr;
+  // the bounded-region kernel's frame and memo workspace: region_ws_words
+  // int64 words per lane, region_lanes lanes (sized by the largest plan admitted)
+  int64_t* region_ws = nullptr;
+  size_t region_ws_words = 0;
+  int region_lanes = 0;
   size_t list_capacity = 0;
   gb::SearchDesc* d_batch_desc = nullptr;
   size_t batch_desc_capacity = 0;
@@ -227,16 +234,21 @@ void harvest(gagp_engine* e) {
 // [4 kChunks + 1] the size of the shared exact-VM list of a round whose
 // ranges hand their exact-VM programs to one launch.
 constexpr int kCountWords = 4 * gagp_engine::kChunks + 4;
+// [4 kChunks + 2]: the size of the deferred bounded-region program list
+constexpr int kRegionCount = 4 * gagp_engine::kChunks + 2;
+gagp_status ensure_region_workspace(gagp_engine* e, size_t words);
 
 gagp_status ensure_lists(gagp_engine* e, size_t items) {
   if (items <= e->list_capacity) return GAGP_OK;
   if (e->d_fast) cudaFree(e->d_fast);
   if (e->d_general) cudaFree(e->d_general);
-  e->d_fast = e->d_general = nullptr;
+  if (e->d_region) cudaFree(e->d_region);
+  e->d_fast = e->d_general = e->d_region = nullptr;
   e->list_capacity = 0;
   const size_t cap = std::max<size_t>({items, size_t(1024), 2 * e->list_capacity});
   CUDA_TRY(cudaMalloc(&e->d_fast, cap * sizeof(gb::ProgramRef)));
   CUDA_TRY(cudaMalloc(&e->d_general, cap * sizeof(gb::ProgramRef)));
+  CUDA_TRY(cudaMalloc(&e->d_region, cap * sizeof(gb::ProgramRef)));
   if (!e->d_counts) CUDA_TRY(cudaMalloc(&e->d_counts, kCountWords * sizeof(int32_t)));
   e->list_capacity = cap;
   return GAGP_OK;
@@ -262,6 +274,59 @@ int bits_for(uint64_t v) {
   int b = 0;
   while (b < 64 && (v >> b)) ++b;
   return b;
+}
+
+// A bounded region's table entry, in the subset the device runs: a
+// coordinate recurrence of 1..4 Int states with at most 4 operands and the
+// four phases, requests that copy or offset states, literal or operand
+// coordinate bounds, at most 128 frames and 256 memo cells, phase bindings
+// from the state, parameter and (in the combine phase) request-result
+// banks.  The reference's grammar compiler and plan validation
+// (region_plan.cpp) have checked the plan itself.
+gagp_status check_bounded_region(const gagp_grammar* g, const gagp_region& x) {
+  auto value_tag = [](int t) { return t == GAGP_TAG_INT || t == GAGP_TAG_BOOL || t == GAGP_TAG_INTLIST; };
+  if (x.state_count < 1 || x.state_count > 4 || x.operands < x.state_count || x.operands > 4 || x.phases != 4)
+    return fail(GAGP_DECLINED, "bounded regions other than coordinate recurrences of at most 4 operands");
+  if (x.request_count < 1 || x.request_count > 8 || x.axis_count < 1 || x.axis_count > 4)
+    return fail(GAGP_DECLINED, "bounded region request or axis count");
+  if (x.frames > 128 || x.cells > 256 || x.entry_fuel > 0x7fffffffu)
+    return fail(GAGP_DECLINED, "bounded region limits beyond 128 frames and 256 memo cells");
+  if ((x.result_type != GAGP_TAG_INT && x.result_type != GAGP_TAG_BOOL) || x.phase_type[0] != GAGP_TAG_BOOL ||
+      x.phase_type[1] != x.result_type || x.phase_type[2] != x.result_type || x.phase_type[3] != x.result_type)
+    return fail(GAGP_DECLINED, "bounded region phase types");
+  for (int k = 0; k < x.operands; ++k)
+    if (x.operand_types[k] != GAGP_TAG_INT) return fail(GAGP_DECLINED, "bounded region operands other than Int");
+  if (x.captures < 0 || x.captures > 8) return fail(GAGP_INVALID_ARGUMENT, "bounded region captures");
+  for (int c = 0; c < x.captures; ++c) {
+    const int kind = x.capture_kind[c], t = x.capture_target[c];
+    if (!value_tag(x.parameter_types[c])) return fail(GAGP_DECLINED, "bounded region parameter type");
+    if ((kind == 0 && (t < 0 || t >= g->local_count)) || (kind == 1 && (t < 0 || t >= gb::kNamedLocals)) ||
+        (kind == 2 && (t < 0 || t >= gb::kLowerBinders)) || kind < 0 || kind > 2)
+      return fail(GAGP_INVALID_ARGUMENT, "bounded region capture");
+  }
+  for (int p = 0; p < 4; ++p) {
+    if (x.phase_bindings[p] < 0 || x.phase_bindings[p] > 7) return fail(GAGP_DECLINED, "bounded region phase bindings");
+    for (int b = 0; b < x.phase_bindings[p]; ++b) {
+      const int bank = x.binding_bank[p][b], slot = x.binding_slot[p][b], t = x.phase_binding_types[p][b];
+      const bool ok = (bank == 0 && slot >= 0 && slot < x.state_count && t == GAGP_TAG_INT) ||
+                      (bank == 1 && slot >= 0 && slot < x.captures && t == x.parameter_types[slot]) ||
+                      (bank == 3 && p == 2 && slot >= 0 && slot < x.request_count && t == x.result_type);
+      if (!ok) return fail(GAGP_DECLINED, "bounded region binding outside the state, parameter and result banks");
+    }
+  }
+  for (int q = 0; q < x.request_count; ++q)
+    for (int k = 0; k < x.state_count; ++k)
+      if ((x.transition_kind[q][k] != 0 && x.transition_kind[q][k] != 1) || x.transition_source[q][k] < 0 ||
+          x.transition_source[q][k] >= x.state_count)
+        return fail(GAGP_DECLINED, "bounded region transitions other than state copies and coordinate offsets");
+  for (int a = 0; a < x.axis_count; ++a) {
+    if (x.axis_slot[a] < 0 || x.axis_slot[a] >= x.state_count) return fail(GAGP_INVALID_ARGUMENT, "bounded region axis");
+    if ((x.lower_kind[a] == 1 && (x.lower[a] < 0 || x.lower[a] >= x.operands)) ||
+        (x.upper_kind[a] == 1 && (x.upper[a] < 0 || x.upper[a] >= x.operands)) || x.lower_kind[a] < 0 ||
+        x.lower_kind[a] > 1 || x.upper_kind[a] < 0 || x.upper_kind[a] > 1)
+      return fail(GAGP_INVALID_ARGUMENT, "bounded region coordinate bound");
+  }
+  return GAGP_OK;
 }
 
 // The value type a program of `g` returns: the phase type of an expression
@@ -290,8 +355,12 @@ gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
   auto value_tag = [](int t) { return t == GAGP_TAG_INT || t == GAGP_TAG_BOOL || t == GAGP_TAG_INTLIST; };
   for (int r = 0; r < RG; ++r) {
     const gagp_region& x = g->regions[r];
+    if (x.traversal == 0) {
+      if (const gagp_status st = check_bounded_region(g, x); st != GAGP_OK) return st;
+      continue;
+    }
     if (x.traversal != 1 && x.traversal != 2)
-      return fail(GAGP_DECLINED, "bounded regions other than traversals are outside the resident subset");
+      return fail(GAGP_INVALID_ARGUMENT, "region table entry kind");
     if (x.ranged) return fail(GAGP_DECLINED, "ranged traversals are outside the resident subset");
     if (x.fuel_profile) return fail(GAGP_DECLINED, "traversal fuel profiles are outside the resident subset");
     for (int k = 0; k < 3; ++k) {
@@ -311,14 +380,18 @@ gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
     if (e.kind == gb::EK_REFERENCE && (e.scope_count < 0 || e.scope_count > 15))
       return fail(GAGP_INVALID_ARGUMENT, "reference scope");
     if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_TRAVERSE) {
-      if (e.arity != 4 || e.operand < 0 || e.operand >= RG)
+      if (e.arity != 4 || e.operand < 0 || e.operand >= RG || g->regions[e.operand].traversal == 0)
         return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": traversal entry");
+    } else if (e.kind == gb::EK_OPERATION && e.node_kind == gb::TK_REGION) {
+      if (e.operand < 0 || e.operand >= RG || g->regions[e.operand].traversal != 0 ||
+          e.arity != g->regions[e.operand].operands + g->regions[e.operand].phases || e.arity > GAGP_MAX_ARITY)
+        return fail(GAGP_INVALID_ARGUMENT, "expression " + std::to_string(i) + ": bounded region entry");
     } else if (e.arity < 0 || e.arity > 3) {
       return fail(GAGP_DECLINED, "arity capacity");
     }
     if (e.kind == gb::EK_OPERATION && e.node_kind != gb::TK_OPERATION && e.node_kind != gb::TK_IF &&
         e.node_kind != gb::TK_AND && e.node_kind != gb::TK_OR && e.node_kind != gb::TK_TRAVERSE &&
-        e.node_kind != gb::TK_LET && !(e.node_kind >= gb::TK_PROGRAM && e.node_kind <= gb::TK_VAR))
+        e.node_kind != gb::TK_LET && e.node_kind != gb::TK_REGION && !(e.node_kind >= gb::TK_PROGRAM && e.node_kind <= gb::TK_VAR))
       return fail(GAGP_DECLINED, "tree kind outside the resident subset");
     if (e.kind == gb::EK_OPERATION && e.node_kind >= gb::TK_PROGRAM && e.node_kind <= gb::TK_VAR) {
       // statements belong to a Program entry's whole-program phase; a named
@@ -618,6 +691,11 @@ GenImageLayout gen_image_layout(const gagp_grammar* g, const DrawTables& t) {
   out.at.doms = take(sizeof(gagp_domain) * size_t(std::max(1, g->domain_count)));
   out.at.vals = take(sizeof(gagp_value) * size_t(std::max(1, g->value_count)));
   out.at.minimum = take(sizeof(uint16_t) * size_t(E) * g->depth_count * g->logical_depth_count);
+  // children 4..7 (a bounded region's phases) only when an arity needs them
+  int widest = 0;
+  for (int i = 0; i < E; ++i)
+    if (g->expressions[i].kind != gb::EK_REFERENCE) widest = std::max(widest, g->expressions[i].arity);
+  out.at.extra = widest > 4 ? take(2 * sizeof(int4) * size_t(E)) : 0;
   out.bytes = off;
   return out;
 }
@@ -637,6 +715,13 @@ std::vector<char> gen_image(const gagp_grammar* g, const std::vector<gb::ExprInf
     r.site_class = info[i].site_class;
     r.kind = int8_t(x.kind);
     r.arity = info[i].arity;
+    if (lay.at.extra && r.arity > 4) {
+      auto* extra = reinterpret_cast<int32_t*>(img.data() + lay.at.extra) + 8 * size_t(i);
+      for (int k = 4; k < 8; ++k) {
+        extra[k - 4] = x.children[k];
+        extra[4] |= int32_t(uint32_t(uint8_t(x.child_scope[k])) << (8 * (k - 4)));
+      }
+    }
     // out-of-range counts keep their validity (admission bounds them anyway)
     r.scope_count = int8_t(std::min(std::max(x.scope_count, -1), 100));
     r.reserved = 0;
@@ -666,7 +751,9 @@ std::vector<char> gen_image(const gagp_grammar* g, const std::vector<gb::ExprInf
 // beside its four children, so at most 8 per node of a row holding
 // traversals (36 + 4 children over 5 nodes).  A for_range emits 23 of its
 // own; its body's root is a block node that emits none and is no other
-// loop's body root, so at most 12 per node of a row holding loops.
+// loop's body root, so at most 12 per node of a row holding loops.  A
+// bounded region emits its BOUNDED_REGION and at most 13 record
+// instructions beside at least five children: at most 3 per node.
 // Program, block and nil nodes emit nothing, an if_stmt 2 and an assign,
 // a return or a local read 1.
 int bytecode_bound(const gagp_grammar* g, int maxv) {
@@ -674,7 +761,8 @@ int bytecode_bound(const gagp_grammar* g, int maxv) {
   for (int i = 0; i < g->expression_count; ++i) {
     const int nk = g->expressions[i].node_kind;
     if (g->expressions[i].kind == gb::EK_OPERATION)
-      per_node = std::max(per_node, nk == gb::TK_FOR_RANGE ? 12 : nk == gb::TK_TRAVERSE ? 8 : nk == gb::TK_IF ? 2
+      per_node = std::max(per_node, nk == gb::TK_FOR_RANGE ? 12 : nk == gb::TK_TRAVERSE ? 8 : nk == gb::TK_REGION ? 3
+                                    : nk == gb::TK_IF ? 2
                                     : (nk == gb::TK_AND || nk == gb::TK_OR) ? 5 : 1);
   }
   return per_node * maxv + 2;
@@ -700,19 +788,7 @@ bool exact_heavy(const gagp_grammar* g) {
 // Device copy of the traversal table.
 std::vector<gb::RegionInfo> region_infos(const gagp_grammar* g) {
   std::vector<gb::RegionInfo> out(std::max(1, g->region_count));
-  for (int r = 0; r < g->region_count; ++r) {
-    const gagp_region& x = g->regions[r];
-    gb::RegionInfo& y = out[r];
-    y.traversal = int8_t(x.traversal);
-    y.ranged = int8_t(x.ranged);
-    y.arity = int8_t(x.ranged ? 6 : 4);
-    y.result_type = int8_t(x.result_type);
-    for (int k = 0; k < 3; ++k) {
-      y.binders[k] = int8_t(x.binders[k]);
-      y.binding_types[k] = int8_t(x.binding_types[k]);
-    }
-    for (int k = 0; k < 6; ++k) y.operand_types[k] = int8_t(x.operand_types[k]);
-  }
+  for (int r = 0; r < g->region_count; ++r) out[r] = gb::region_info_of(g->regions[r]);
   return out;
 }
 
@@ -962,6 +1038,8 @@ void gagp_b200_engine_destroy(gagp_engine* e) {
   if (e->pinned) cudaFreeHost(e->pinned);
   cudaFree(e->d_fast);
   cudaFree(e->d_general);
+  cudaFree(e->d_region);
+  cudaFree(e->region_ws);
   cudaFree(e->d_counts);
   cudaFree(e->d_batch_desc);
   cudaFree(e->d_batch_off);
@@ -1013,6 +1091,12 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   s->fixed_nodes = g->fixed_nodes;
   s->has_wrong = cfg->metric != GAGP_METRIC_LEGACY;
   s->exact_heavy = exact_heavy(g);
+  s->region_words = 0;
+  for (int r = 0; r < g->region_count; ++r)
+    if (g->regions[r].traversal == 0)
+      s->region_words = std::max(s->region_words, gb::region_lane_words(gb::region_info_of(g->regions[r])));
+  if (s->region_words)
+    if (const gagp_status st = ensure_region_workspace(e, s->region_words); st != GAGP_OK) return st;
   s->bytes = p.L.total;
   CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->block), s->bytes, e->pool, e->stream));
   CUDA_TRY(cudaMemsetAsync(s->block, 0, s->bytes, e->stream));
@@ -1226,6 +1310,7 @@ struct BatchView {
   int max_C = 1, max_inputs = 0;
   int min_B = 1 << 30;               // the smallest round of the batch
   bool exact_heavy = false;          // some search's programs mostly need the exact VM
+  bool regions = false;              // some search's grammar has bounded regions
   bool generational = false;         // the batch's schedule (one per batch)
   std::vector<int> child_off;        // host copy of the child offsets (n + 1)
   std::vector<size_t> image_bytes;   // each search's generator image
@@ -1287,12 +1372,14 @@ gagp_status make_batch_view(gagp_engine* e, const std::vector<Search*>& list, Ba
   v->max_C = 1;
   v->max_inputs = 0;
   v->exact_heavy = false;
+  v->regions = false;
   v->child_off.assign(1, 0);
   v->image_bytes.clear();
   for (Search* s : list) {
     v->child_off.push_back(v->child_off.back() + s->B);
     v->image_bytes.push_back(size_t(s->desc.gen_image_bytes));
     v->exact_heavy |= s->exact_heavy;
+    v->regions |= s->region_words > 0;
     v->max_C = std::max(v->max_C, s->desc.C);
     v->max_inputs = std::max(v->max_inputs, s->desc.n_inputs);
     v->total_members += s->P;
@@ -1335,7 +1422,8 @@ size_t vm_general_smem(int bc_stride_max) { return gb::general_smem_bytes(bc_str
 // quarter of the SMs take them (an empty launch of a full grid costs a few
 // microseconds on every range's critical path).
 gagp_status vm_general_launch(int sm_count, cudaStream_t stream, const gb::SearchDesc* descs, int mode,
-                              const gb::ProgramRef* list, const int32_t* counts, int bc_stride_max, bool heavy) {
+                              const gb::ProgramRef* list, const int32_t* counts, int bc_stride_max, bool heavy,
+                              gb::ProgramRef* deferred, int32_t* deferred_count) {
   const size_t smem = vm_general_smem(bc_stride_max);
   int blocks = std::max(1, sm_count / 4);
   if (heavy) {
@@ -1345,7 +1433,37 @@ gagp_status vm_general_launch(int sm_count, cudaStream_t stream, const gb::Searc
     if (occ != cudaSuccess) return fail(GAGP_DEVICE_ERROR, std::string("exact VM occupancy: ") + cudaGetErrorString(occ));
     blocks = sm_count * std::max(1, per_sm);
   }
-  gb::k_vm_general<<<blocks, kGeneralThreads, smem, stream>>>(descs, mode, list, counts + 1, bc_stride_max);
+  gb::k_vm_general<<<blocks, kGeneralThreads, smem, stream>>>(descs, mode, list, counts + 1, bc_stride_max, deferred,
+                                                              deferred_count);
+  return GAGP_OK;
+}
+
+// The bounded-region workspace for plans of up to `words` int64 words per
+// lane (grown, never shrunk; the device is idle between API calls).
+gagp_status ensure_region_workspace(gagp_engine* e, size_t words) {
+  const int lanes = 2 * e->sm_count * gb::kRegionThreads;
+  if (e->region_ws && words <= e->region_ws_words && lanes <= e->region_lanes) return GAGP_OK;
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (e->region_ws) cudaFree(e->region_ws);
+  e->region_ws = nullptr;
+  e->region_ws_words = 0;
+  const size_t w = std::max(words, e->region_ws_words);
+  if (cudaMalloc(&e->region_ws, w * size_t(lanes) * sizeof(int64_t)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GAGP_OUT_OF_MEMORY, "bounded-region workspace");
+  }
+  e->region_ws_words = w;
+  e->region_lanes = lanes;
+  return GAGP_OK;
+}
+
+// The deferred programs with bounded regions: a fixed grid of the region
+// workspace's lanes, after every exact-VM launch that deferred to it.
+gagp_status vm_region_launch(gagp_engine* e, cudaStream_t stream, const gb::SearchDesc* descs, int mode,
+                             const gb::ProgramRef* list, const int32_t* count) {
+  if (!e->region_ws) return fail(GAGP_DEVICE_ERROR, "bounded regions without a workspace");
+  gb::k_vm_region<<<e->region_lanes / gb::kRegionThreads, gb::kRegionThreads, 0, stream>>>(
+      descs, mode, list, count, e->region_ws, e->region_ws_words);
   return GAGP_OK;
 }
 
@@ -1412,12 +1530,14 @@ gagp_status launch_vm(gagp_engine* e, const BatchView& v, int mode, cudaStream_t
                       const gb::ProgramRef* general, const int32_t* counts, const VmPlan& plan) {
   if (const gagp_status st = launch_vm_fast(e, v, mode, stream, fast, counts, plan); st != GAGP_OK) return st;
   Timed t(e, KN_VM_GENERAL, stream);
-  return vm_general_launch(e->sm_count, stream, v.d_desc, mode, general, counts, v.max_bc_stride, v.exact_heavy);
+  return vm_general_launch(e->sm_count, stream, v.d_desc, mode, general, counts, v.max_bc_stride, v.exact_heavy,
+                           e->d_region, e->d_counts + kRegionCount);
 }
 
 gagp_status launch_start(gagp_engine* e, const BatchView& v) {
   { Timed t(e, KN_INIT); gb::k_init_population<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   CUDA_TRY(cudaMemsetAsync(e->d_counts, 0, 2 * sizeof(int32_t), e->stream));
+  CUDA_TRY(cudaMemsetAsync(e->d_counts + kRegionCount, 0, sizeof(int32_t), e->stream));
   {
     Timed t(e, KN_LOWER);
     gb::k_lower<<<blocks_for(v.total_members, gb::kLowerWarps), gb::kLowerWarps * 32, 0, e->stream>>>(
@@ -1428,6 +1548,10 @@ gagp_status launch_start(gagp_engine* e, const BatchView& v) {
   if (const gagp_status st = launch_vm(e, v, 0, e->stream, e->d_fast, e->d_general, e->d_counts, start_plan);
       st != GAGP_OK)
     return st;
+  if (v.regions)
+    if (const gagp_status st = vm_region_launch(e, e->stream, v.d_desc, 0, e->d_region, e->d_counts + kRegionCount);
+        st != GAGP_OK)
+      return st;
   { Timed t(e, KN_KEYS); gb::k_member_keys<<<blocks_for(v.total_members, 128), 128, 0, e->stream>>>(v.d_desc, v.d_member_off, v.n); }
   { Timed t(e, KN_START); gb::k_start<<<v.n, 256, 0, e->stream>>>(v.d_desc, v.n); }
   return cudaPeekAtLastError() == cudaSuccess ? GAGP_OK : fail(GAGP_DEVICE_ERROR, cudaGetErrorString(cudaGetLastError()));
@@ -1548,10 +1672,15 @@ gagp_status launch_round(gagp_engine* e, const BatchView& v, bool may_measure = 
         return st2;
     Timed t(e, KN_VM_GENERAL);
     if (const gagp_status st2 = vm_general_launch(e->sm_count, e->stream, v.d_desc, 1, e->d_general, shared_count,
-                                                  v.max_bc_stride, v.exact_heavy);
+                                                  v.max_bc_stride, v.exact_heavy, e->d_region,
+                                                  e->d_counts + kRegionCount);
         st2 != GAGP_OK)
       return st2;
   }
+  if (v.regions)
+    if (const gagp_status st2 = vm_region_launch(e, e->stream, v.d_desc, 1, e->d_region, e->d_counts + kRegionCount);
+        st2 != GAGP_OK)
+      return st2;
   if (v.generational) {
     // every child becomes the member of its index (reproduce's swap), after
     // the reused children have read their sources' results and the history
@@ -1710,9 +1839,12 @@ struct EvalPlan {
   Layout L;
   size_t desc, ex, info, minimum, local_types, regions, inputs, expected, lists, node, cval, len, code, code_len, kpool,
       code_temps, vm_acc, bc, bc_len, bc_locals, bc_consts, fitness, wrong, errors, counters, round, fast, general,
-      counts, off;
+      counts, off, region_list, region_ws;
   int stride, code_stride, bc_stride;
+  size_t region_words;  // bounded-region workspace per lane (0: the grammar has none)
 };
+// Lanes of a row evaluation's bounded-region kernel.
+constexpr int kRowRegionBlocks = 64;
 
 EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   EvalPlan p{};
@@ -1741,6 +1873,12 @@ EvalPlan plan_eval(const gagp_grammar* g, const gagp_cases* c, int rows) {
   p.counters = L.take(8 * GAGP_COUNTERS); p.round = L.take(16);
   p.fast = L.take(sizeof(gb::ProgramRef) * R); p.general = L.take(sizeof(gb::ProgramRef) * R);
   p.counts = L.take(16); p.off = L.take(8);
+  p.region_words = 0;
+  for (int r = 0; r < g->region_count; ++r)
+    if (g->regions[r].traversal == 0)
+      p.region_words = std::max(p.region_words, gb::region_lane_words(gb::region_info_of(g->regions[r])));
+  p.region_list = L.take(sizeof(gb::ProgramRef) * R);
+  p.region_ws = L.take(8 * std::max<size_t>(1, p.region_words * kRowRegionBlocks * gb::kRegionThreads));
   return p;
 }
 
@@ -1908,9 +2046,14 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   vm_fast_launch(lanes, sm_count * per_sm, warps * 32, smem, stream, dd, 0, fast, counts, temp_stride, code_stride,
                  p.stride, C);
   if (vm_general_smem(p.bc_stride) > max_smem - 1024) return fail(GAGP_DECLINED, "program too long for the exact VM");
-  if (const gagp_status st = vm_general_launch(sm_count, stream, dd, 0, general, counts, p.bc_stride, true);
+  gb::ProgramRef* region_list = at<gb::ProgramRef>(b, p.region_list);
+  if (const gagp_status st = vm_general_launch(sm_count, stream, dd, 0, general, counts, p.bc_stride, true,
+                                               region_list, counts + 2);
       st != GAGP_OK)
     return st;
+  if (p.region_words)
+    gb::k_vm_region<<<kRowRegionBlocks, gb::kRegionThreads, 0, stream>>>(dd, 0, region_list, counts + 2,
+                                                                          at<int64_t>(b, p.region_ws), p.region_words);
   CUDA_TRY(cudaGetLastError());
   int32_t round[4];
   CUDA_TRY(cudaMemcpyAsync(round, b + p.round, sizeof round, cudaMemcpyDeviceToHost, stream));

@@ -77,7 +77,7 @@ __global__ void k_init_population(const SearchDesc* descs, const int32_t* off, i
 // fast_list, counted in list_count[0]), else the reference bytecode for the
 // general VM (lane 0; listed in general_list, counted in *general_count).
 constexpr int kLowerWarps = 4;
-__global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* descs, const int32_t* off, int n,
+__global__ void __launch_bounds__(kLowerWarps * 32, 8) k_lower(const SearchDesc* descs, const int32_t* off, int n,
                                                             int mode, ProgramRef* fast_list, ProgramRef* general_list,
                                                             int32_t* list_count, int32_t* general_count, int lo,
                                                             int hi) {
@@ -137,8 +137,12 @@ __global__ void __launch_bounds__(kLowerWarps * 32) k_lower(const SearchDesc* de
         raise_error(s, 30);  // the phase compiler rejected a constructed program
       } else {
         s.bc_len[slot] = bl;
-        s.bc_locals[slot] = r.locals | (r.stack_bound << 8);
-        s.code_temps[slot] = -1;
+        // the main code's length marks a program with bounded regions (its
+        // records and phase code follow); an exact-VM program keeps its
+        // main constant count where an accumulator program keeps its
+        // temporaries
+        s.bc_locals[slot] = r.locals | (r.stack_bound << 8) | (r.main << 16);
+        s.code_temps[slot] = r.main_constants;
         general_list[atomicAdd(general_count, 1)] = ProgramRef{si, slot};
         atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[9]),
                   (unsigned long long)(row_bytes + 20ull * bl + 8ull * r.constants + 16));
@@ -182,7 +186,8 @@ __host__ __device__ __forceinline__ size_t general_smem_bytes(int bc_stride_max)
 }
 __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchDesc* descs, int mode,
                                                                    const ProgramRef* list, const int32_t* list_count,
-                                                                   int bc_stride_max) {
+                                                                   int bc_stride_max, ProgramRef* deferred,
+                                                                   int32_t* deferred_count) {
   extern __shared__ __align__(16) int64_t smem_general[];
   __shared__ int64_t red_loss[kGeneralWarps];
   __shared__ uint32_t red_wrong[kGeneralWarps], red_errors[kGeneralWarps];
@@ -201,6 +206,12 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
     const SearchDesc& s = descs[p.search];
     const int n = s.bc_len[p.slot], shape = s.bc_locals[p.slot];
     const int n_locals = shape & 0xff, stack_bound = (shape >> 8) & 0xff;
+    if (((shape >> 16) & 0xffff) < n) {
+      // a program with bounded regions: k_vm_region runs it with a frame
+      // and memo workspace per lane
+      if (threadIdx.x == 0) deferred[atomicAdd(deferred_count, 1)] = p;
+      continue;
+    }
     bool simd_ok = n_locals + stack_bound <= kSimdSlots;
     {
       const int32_t* gcode = s.bc + size_t(p.slot) * 5 * s.bc_stride;
@@ -262,6 +273,75 @@ __global__ void __launch_bounds__(kGeneralWarps * 32) k_vm_general(const SearchD
       uint32_t tw = 0, te = 0;
       unsigned long long ts = 0;
       for (int w = 0; w < kGeneralWarps; ++w) {
+        tl += red_loss[w];
+        tw += red_wrong[w];
+        te += red_errors[w];
+        ts += red_steps[w];
+      }
+      store_result(s, mode, p.slot, tl, tw, te);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[24]), ts);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[0]), 1ULL);
+      atomicAdd(reinterpret_cast<unsigned long long*>(&s.counters[2]), (unsigned long long)s.C);
+    }
+    __syncthreads();
+  }
+}
+
+// Programs with bounded regions (deferred by k_vm_general): a fixed grid of
+// blocks of kRegionThreads, one program per block at a time and one case
+// per thread at a time on the per-thread interpreter
+// (run_program_regions), each thread with its own `ws_words` words of
+// frames and memo cells in `ws` (gridDim x kRegionThreads lanes).
+constexpr int kRegionThreads = 128;
+__global__ void __launch_bounds__(kRegionThreads) k_vm_region(const SearchDesc* descs, int mode, const ProgramRef* list,
+                                                              const int32_t* list_count, int64_t* ws,
+                                                              size_t ws_words) {
+  __shared__ int64_t red_loss[kRegionThreads / 32];
+  __shared__ uint32_t red_wrong[kRegionThreads / 32], red_errors[kRegionThreads / 32];
+  __shared__ unsigned long long red_steps[kRegionThreads / 32];
+  const int count = *list_count;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t* mine = ws + (size_t(blockIdx.x) * kRegionThreads + threadIdx.x) * ws_words;
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const ProgramRef p = list[i];
+    const SearchDesc& s = descs[p.search];
+    const int n = s.bc_len[p.slot], shape = s.bc_locals[p.slot];
+    const int n_locals = shape & 0xff, n_main = (shape >> 16) & 0xffff;
+    const int32_t* code = s.bc + size_t(p.slot) * 5 * s.bc_stride;
+    const int64_t* consts = s.bc_consts + size_t(p.slot) * s.bc_stride;
+    const int main_consts = s.code_temps[p.slot];
+    const VmView view = vm_view(s);
+    int64_t loss = 0;
+    uint32_t wrong = 0, errors = 0;
+    uint64_t steps = 0;
+    for (int c = threadIdx.x; c < s.C; c += kRegionThreads) {
+      int64_t value = 0;
+      int tag = 0;
+      if (run_program_regions(view, s.regions, s.n_regions, code, n, n_main, consts, main_consts, n_locals, c, mine,
+                              ws_words, value, tag, steps)) {
+        loss += case_loss(s, tag, value, s.expected[c], wrong);
+      } else {
+        loss += error_loss(s);
+        ++wrong;
+        ++errors;
+      }
+    }
+    loss = warp_sum(loss);
+    wrong = warp_sum(wrong);
+    errors = warp_sum(errors);
+    steps = warp_sum(steps);
+    if (lane == 0) {
+      red_loss[warp] = loss;
+      red_wrong[warp] = wrong;
+      red_errors[warp] = errors;
+      red_steps[warp] = steps;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t tl = 0;
+      uint32_t tw = 0, te = 0;
+      unsigned long long ts = 0;
+      for (int w = 0; w < kRegionThreads / 32; ++w) {
         tl += red_loss[w];
         tw += red_wrong[w];
         te += red_errors[w];

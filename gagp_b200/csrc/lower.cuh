@@ -22,7 +22,8 @@ namespace gb {
 enum {
   OP_PUSH_CONST = 0, OP_LOAD = 1, OP_STORE = 2, OP_NEG = 3, OP_NOT = 4, OP_ADD = 5, OP_SUB = 6, OP_MUL = 7,
   OP_DIV = 8, OP_MOD = 9, OP_LT = 10, OP_LE = 11, OP_GT = 12, OP_GE = 13, OP_EQ = 14, OP_NE = 15, OP_JMP = 16,
-  OP_JMP_IF_FALSE = 17, OP_JMP_IF_TRUE = 18, OP_CALL_BUILTIN = 19, OP_RETURN = 20, OP_CHECK_INT = 22
+  OP_JMP_IF_FALSE = 17, OP_JMP_IF_TRUE = 18, OP_CALL_BUILTIN = 19, OP_RETURN = 20, OP_CHECK_INT = 22,
+  OP_BOUNDED_REGION = 28
 };
 enum {
   B_ABS = 0, B_MIN = 1, B_MAX = 2, B_LEN = 4, B_INDEX = 7, B_IS_INT = 12, B_IDIV0 = 13, B_IMOD0 = 14, B_TRUNC_DIV0 = 28,
@@ -69,10 +70,25 @@ __host__ __device__ inline LowerView lower_view(const SearchDesc& s) {
 
 // Shape of a lowered program.
 struct LowerResult {
-  int code;         // instructions, the appended RETURN included
+  int code;         // instructions: the main code, its appended RETURN, then any region records and phase code
   int constants;    // constant pool entries
   int locals;       // inputs + temporaries
   int stack_bound;  // deepest value stack
+  int main;         // instructions of the main code with its RETURN (the records start here)
+  int main_constants;  // constants of the main code (the phases' follow)
+};
+
+// Bounded regions of one program, in completion order (the reference's
+// RegionRecord, phase_compile.cuh:236-238): the table entry, the caller
+// slot of each capture, the node range of each phase subtree and the row
+// constant index where each phase's constants start.
+constexpr int kMaxRegions = 4;   // kPhaseMaxRegions
+constexpr int kRegionRecord = 0xFF;
+struct RegionRecords {
+  int count;
+  struct {
+    int info, captures[8], bounds[5], consts[4];
+  } r[kMaxRegions];
 };
 
 constexpr int kMaxStack = 64;     // MAX_STACK (cpp/include/gagp/runtime/gpu/constants_gpu.hpp:9)
@@ -101,9 +117,14 @@ constexpr int kHasA = 1, kHasB = 2, kBoolConst = 4;
 // event is uncharged, so the reference's binder facts and analysed ifs
 // (which only decide aliases and uncharged checks) never change the output
 // and are not kept here.
-__host__ __device__ inline int lower_program(const LowerView& v, const uint64_t* node, const int64_t* cval, int n,
-                                             int nc, int32_t* code, int code_cap, int64_t* consts, int const_cap,
-                                             LowerResult* result) {
+//
+// `regions` null: a bounded region's phase (Regions=false in the
+// reference): the value is left on the stack with no RETURN, and no region
+// may occur.  Otherwise the main code, whose bounded regions are recorded
+// there (the operands lowered in place, the phase subtrees set aside).
+__host__ __device__ __noinline__ int lower_code(const LowerView& v, const uint64_t* node, const int64_t* cval, int n, int nc,
+                                          int32_t* code, int code_cap, int64_t* consts, int const_cap,
+                                          LowerResult* result, RegionRecords* regions) {
   struct Frame {
     int node, base_stack, first_jump, second_jump, seen;
     int8_t args[3];
@@ -196,6 +217,42 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
       named_mask |= 1u << operand;
     }
     return named[operand];
+  };
+  // the operands are on the stack: resolve the captures, set the phase
+  // subtrees aside and emit BOUNDED_REGION (finish_region,
+  // phase_compile.cuh:289-319)
+  auto finish_region = [&](const gagp_expression& e) -> bool {
+    if (!regions || regions->count == kMaxRegions) return false;
+    const RegionInfo& info = v.regions[e.operand];
+    auto& rec = regions->r[regions->count];
+    rec.info = e.operand;
+    for (int c = 0; c < info.captures; ++c) {
+      const int target = info.capture_target[c];
+      int slot = -1;
+      if (info.capture_kind[c] == 0) slot = target >= 0 ? variable_slot(-1 - target) : -1;
+      else if (info.capture_kind[c] == 1) slot = variable_slot(target);
+      else if (target >= 0 && target < kLowerBinders) slot = env_slot[target];
+      if (slot < 0) return false;
+      rec.captures[c] = slot;
+    }
+    for (int p = 0; p < info.phases; ++p) {
+      rec.bounds[p] = cursor;
+      rec.consts[p] = row_const;
+      int pending = 1;
+      while (pending) {
+        if (cursor >= n) return false;
+        const uint64_t w = node[cursor++];
+        row_const += w_const(w);
+        pending += w_arity(w) - 1;
+      }
+    }
+    rec.bounds[info.phases] = cursor;
+    if (!emit(OP_BOUNDED_REGION, e.fuel, regions->count, 0, kHasA)) return false;
+    stack -= info.operands;
+    grow(1);
+    ++regions->count;
+    completed = e.type;
+    return true;
   };
   auto subtree_end = [&](int i) -> int {
     int pending = 1;
@@ -301,6 +358,20 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
         grow(1);
         completed = e.type;
         have_value = true;
+      } else if (e.node_kind == TK_REGION) {
+        // a bounded region (phase_compile.cuh:652-666): operands first, its
+        // phases set aside when the last operand completes
+        if (!regions || e.operand < 0 || e.operand >= v.n_regions) return -1;
+        const RegionInfo& info = v.regions[e.operand];
+        if (info.traversal != 0 || info.phases < 1 || e.arity != info.operands + info.phases || e.arity > 8) return -1;
+        if (info.operands == 0) {
+          if (!finish_region(e)) return -1;
+          have_value = true;
+        } else {
+          if (depth == 64) return -1;
+          frames[depth++] = Frame{index, stack, -1, -1, 0, {0, 0, 0}};
+          continue;
+        }
       } else if (e.node_kind == TK_TRAVERSE) {
         if (e.operand < 0 || e.operand >= v.n_regions) return -1;
         const RegionInfo& info = v.regions[e.operand];
@@ -367,8 +438,9 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
       // (patch_whole_program, phase_layout.hpp:494-496)
       if (cursor != n || stack != (statements ? 0 : 1) || completed != v.slot_type || stack_bound > kMaxStack)
         return -1;
-      if (!statements && (stack_bound < 1 || !emit(OP_RETURN, v.return_fuel, 0, 0, 0))) return -1;
+      if (regions && !statements && (stack_bound < 1 || !emit(OP_RETURN, v.return_fuel, 0, 0, 0))) return -1;
       result->code = count;
+      result->main = count;
       result->constants = nconst;
       result->locals = total_locals;
       result->stack_bound = stack_bound;
@@ -408,6 +480,14 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
       env_type[l.binder] = l.saved_type;
       while (live_count > l.live_begin) freed[free_count++] = live[--live_count];
       --let_depth;
+      --depth;
+      continue;
+    }
+    if (e.node_kind == TK_REGION) {
+      const RegionInfo& info = v.regions[e.operand];
+      if (completed != info.operand_types[f.seen - 1]) return -1;
+      if (f.seen < info.operands) { have_value = false; continue; }
+      if (!finish_region(e)) return -1;
       --depth;
       continue;
     }
@@ -530,6 +610,68 @@ __host__ __device__ inline int lower_program(const LowerView& v, const uint64_t*
     }
     --depth;
   }
+}
+
+// Reference bytecode of a whole program: the main code (lower_code) with
+// its RETURN, then, for each bounded region in completion order, the
+// reference's records (phase_compile.cuh:889-912): a header (fuel: the
+// capture count, a: the table entry, b: the phase count), one record per
+// capture (a: its caller slot), and per phase a header (a: its
+// instructions, b: its constants, fuel: its locals, bit 16 when it reads a
+// binder or a let) followed by the phase's own code, lowered with its
+// bindings as its first locals.  Phase constants follow the main ones in
+// the pool.  Returns the instruction count or -1.
+__host__ __device__ inline int lower_program(const LowerView& v, const uint64_t* node, const int64_t* cval, int n,
+                                             int nc, int32_t* code, int code_cap, int64_t* consts, int const_cap,
+                                             LowerResult* result) {
+  RegionRecords rec;
+  rec.count = 0;
+  int count = lower_code(v, node, cval, n, nc, code, code_cap, consts, const_cap, result, &rec);
+  if (count >= 0) result->main_constants = result->constants;
+  if (count < 0 || !rec.count) return count;
+  int nconst = result->constants;
+  auto emit = [&](int fuel, int a, int b) -> bool {
+    if (count >= code_cap) return false;
+    int32_t* x = code + 5 * count++;
+    x[0] = kRegionRecord; x[1] = 0; x[2] = a; x[3] = b; x[4] = fuel;
+    return true;
+  };
+  for (int r = 0; r < rec.count; ++r) {
+    const RegionInfo& info = v.regions[rec.r[r].info];
+    if (!emit(info.captures, rec.r[r].info, info.phases)) return -1;
+    for (int c = 0; c < info.captures; ++c)
+      if (!emit(0, rec.r[r].captures[c], 0)) return -1;
+    for (int p = 0; p < info.phases; ++p) {
+      const int header = count;
+      if (!emit(0, 0, 0)) return -1;
+      int32_t types[8];
+      for (int b = 0; b < info.phase_bindings[p]; ++b) types[b] = info.phase_binding_types[p][b];
+      LowerView pv = v;
+      pv.local_count = info.phase_bindings[p];
+      pv.local_types = types;
+      pv.slot_type = info.phase_type[p];
+      const int begin = rec.r[r].bounds[p], end = rec.r[r].bounds[p + 1];
+      LowerResult pr{};
+      const int pc = lower_code(pv, node + begin, cval + rec.r[r].consts[p], end - begin, nc - rec.r[r].consts[p],
+                                code + 5 * count, code_cap - count, consts + nconst, const_cap - nconst, &pr, nullptr);
+      if (pc < 0) return -1;
+      // a phase that reads a binding or binds a let keeps its fuel table
+      bool general = false;
+      for (int i = begin; i < end; ++i) {
+        const int nk = v.ex[w_origin(node[i])].node_kind;
+        general |= nk == TK_BOUND || nk == TK_LET;
+      }
+      code[5 * header + 2] = pc;
+      code[5 * header + 3] = pr.constants;
+      code[5 * header + 4] = pr.locals | (general ? 1 << 16 : 0);
+      count += pc;
+      nconst += pr.constants;
+      if (pr.stack_bound > result->stack_bound) result->stack_bound = pr.stack_bound;
+    }
+  }
+  result->code = count;
+  result->constants = nconst;
+  return count;
 }
 
 // Per-warp shared memory of the accumulator lowering: per-node tables

@@ -86,7 +86,8 @@ struct alignas(16) GenEntry {
 // heads share it; gagp_domain[n_doms]; gagp_value[n_vals]; the minimum cost
 // table as uint16 (kNoMinimum16: infeasible).
 struct GenImage {
-  int32_t nt, head, level, entry, doms, vals, minimum, reserved;
+  int32_t nt, head, level, entry, doms, vals, minimum;
+  int32_t extra;  // children 4..7 of each expression and their scopes (two int4), when an arity exceeds 4
 };
 constexpr uint16_t kNoMinimum16 = 0xffff;
 
@@ -95,14 +96,76 @@ constexpr uint16_t kNoMinimum16 = 0xffff;
 // binder numbers of element, index and state, the operand types the
 // children must complete with, the binding types and the result type.
 struct RegionInfo {
-  int8_t traversal;       // 1 forward, 2 reverse
+  int8_t traversal;       // 1 forward, 2 reverse; 0 a bounded region
   int8_t ranged;          // 0: (source, start, initial state, body)
-  int8_t arity;           // 4, or 6 when ranged
-  int8_t result_type;     // ValueTag of the traversal's result
+  int8_t arity;           // 4, or 6 when ranged; a bounded region: operands + phases
+  int8_t result_type;     // ValueTag of the traversal's (or the bounded region's) result
   int8_t binders[3];
   int8_t binding_types[3];
   int8_t operand_types[6];
+  // a bounded region: a coordinate recurrence (gagp_region's bounded fields)
+  int8_t operands, phases, captures, state_count, request_count, axis_count, inclusive, memoized;
+  int8_t capture_kind[8], capture_target[8];
+  int8_t phase_type[4], phase_bindings[4];
+  int8_t binding_bank[4][8], binding_slot[4][8], phase_binding_types[4][8];
+  int8_t transition_kind[8][4], transition_source[8][4];
+  int8_t axis_slot[4], lower_kind[4], upper_kind[4];
+  uint32_t frames, cells, entry_fuel;
+  int64_t transition_offset[8][4];
+  int64_t lower[4], upper[4];
 };
+// The device view of a region table entry (gagp_region), traversal or
+// bounded region (a bounded one checked by the engine's admission).
+inline RegionInfo region_info_of(const gagp_region& x) {
+  RegionInfo y{};
+  y.traversal = int8_t(x.traversal);
+  y.ranged = int8_t(x.ranged);
+  y.arity = int8_t(x.ranged ? 6 : 4);
+  y.result_type = int8_t(x.result_type);
+  for (int k = 0; k < 3; ++k) {
+    y.binders[k] = int8_t(x.binders[k]);
+    y.binding_types[k] = int8_t(x.binding_types[k]);
+  }
+  if (x.traversal == 0) {
+    // a bounded region (checked by check_tables_and_cases)
+    y.arity = int8_t(x.operands + x.phases);
+    y.operands = int8_t(x.operands); y.phases = int8_t(x.phases); y.captures = int8_t(x.captures);
+    y.state_count = int8_t(x.state_count); y.request_count = int8_t(x.request_count);
+    y.axis_count = int8_t(x.axis_count); y.inclusive = int8_t(x.inclusive != 0); y.memoized = int8_t(x.memoized != 0);
+    for (int c = 0; c < 8; ++c) { y.capture_kind[c] = int8_t(x.capture_kind[c]); y.capture_target[c] = int8_t(x.capture_target[c]); }
+    for (int p = 0; p < 4; ++p) {
+      y.phase_type[p] = int8_t(x.phase_type[p]);
+      y.phase_bindings[p] = int8_t(x.phase_bindings[p]);
+      for (int b = 0; b < 8; ++b) {
+        y.binding_bank[p][b] = int8_t(x.binding_bank[p][b]);
+        y.binding_slot[p][b] = int8_t(x.binding_slot[p][b]);
+        y.phase_binding_types[p][b] = int8_t(x.phase_binding_types[p][b]);
+      }
+    }
+    for (int q = 0; q < 8; ++q)
+      for (int k = 0; k < 4; ++k) {
+        y.transition_kind[q][k] = int8_t(x.transition_kind[q][k]);
+        y.transition_source[q][k] = int8_t(x.transition_source[q][k]);
+        y.transition_offset[q][k] = x.transition_offset[q][k];
+      }
+    for (int a = 0; a < 4; ++a) {
+      y.axis_slot[a] = int8_t(x.axis_slot[a]);
+      y.lower_kind[a] = int8_t(x.lower_kind[a]); y.upper_kind[a] = int8_t(x.upper_kind[a]);
+      y.lower[a] = x.lower[a]; y.upper[a] = x.upper[a];
+    }
+    y.frames = x.frames; y.cells = x.cells; y.entry_fuel = x.entry_fuel;
+    for (int k = 0; k < 4; ++k) y.operand_types[k] = int8_t(k < x.operands ? x.operand_types[k] : 0);
+  }
+  for (int k = 0; k < 6; ++k) y.operand_types[k] = int8_t(x.operand_types[k]);
+  return y;
+}
+
+// Frames, memo cells and their int64 words in one lane's bounded-region
+// workspace: a frame holds the states, the request results and the next
+// request; a cell the states and the value.
+__host__ __device__ inline size_t region_lane_words(const RegionInfo& r) {
+  return size_t(r.frames) * (r.state_count + r.request_count + 1) + size_t(r.cells) * (r.state_count + 1);
+}
 
 // Everything a kernel needs to work on one search (device pointers).
 struct SearchDesc {

@@ -361,18 +361,27 @@ __host__ __device__ inline VmView vm_view(const SearchDesc& s) {
 // program's inputs plus temporaries; the inputs are preset.  Returns false
 // on any runtime error or timeout (every error scores the same), else the
 // returned value and its tag.  `steps` counts executed instructions.
-__host__ __device__ inline bool run_program(const VmView& v, const int32_t* code, int n, const int64_t* consts,
-                                            int n_locals, int c, int64_t& value, int& tag, uint64_t& steps) {
-  int64_t sv[kMaxStack], lv[kLowerLocals];
-  int8_t st[kMaxStack], lt[kLowerLocals];
-  if (n_locals < v.n_inputs || n_locals > kLowerLocals) return false;
-  uint64_t set = 0;  // bit k: local k holds a value
-  for (int j = 0; j < v.n_inputs; ++j) {
-    lv[j] = v.inputs[size_t(j) * v.C + c];
-    lt[j] = int8_t(v.local_types[j]);
-    set |= 1ull << j;
-  }
-  int sp = 0, ip = 0, fuel = v.fuel, uncharged = 0;
+//
+// A program with bounded regions runs through run_program_regions: its
+// BOUNDED_REGION instructions execute the region (run_region) from the
+// records and phase code that follow its main code.
+struct RegionRun;
+__host__ __device__ inline int region_operands(const RegionRun& rr, int ordinal);
+__host__ __device__ inline bool run_region(const VmView& v, const RegionRun& rr, int ordinal, const int64_t* opv,
+                                           const int8_t* opt, const int64_t* caller_lv, const int8_t* caller_lt,
+                                           uint64_t caller_set, int& fuel, int64_t& value, int& tag, uint64_t& steps);
+
+// The interpreter loop shared by a main program (Phase false: RETURN ends
+// it, falling off the end is an error) and a bounded region's phase (Phase
+// true: an expression segment whose value is the stack top at its end,
+// run_code with require_return false).  lv/lt/set: the preset locals.
+template <bool Phase>
+__host__ __device__ inline bool run_code(const VmView& v, const int32_t* code, int n, const int64_t* consts,
+                                         int n_locals, int64_t* lv, int8_t* lt, uint64_t set, int& fuel,
+                                         const RegionRun* rr, int64_t& value, int& tag, uint64_t& steps) {
+  int64_t sv[kMaxStack];
+  int8_t st[kMaxStack];
+  int sp = 0, ip = 0, uncharged = 0;
   while (ip < n) {
     const int32_t* x = code + 5 * ip++;
     const int op = x[0], flags = x[1], a = x[2], b = x[3];
@@ -501,11 +510,289 @@ __host__ __device__ inline bool run_program(const VmView& v, const int32_t* code
         value = sv[sp - 1];
         tag = st[sp - 1];
         return true;
+      case OP_BOUNDED_REGION: {
+        // the region's operands (initial states, bound operands) are popped
+        // and its value pushed (execute_bytecode_cpu.cpp:482-570); a phase
+        // holds no region
+        if constexpr (Phase) {
+          return false;
+        } else {
+          if (!rr || (flags & kHasA) == 0) return false;
+          const int operands = region_operands(*rr, a);
+          if (operands < 0 || sp < operands) return false;
+          sp -= operands;
+          int64_t r;
+          int rt;
+          if (!run_region(v, *rr, a, sv + sp, st + sp, lv, lt, set, fuel, r, rt, steps)) return false;
+          sv[sp] = r;
+          st[sp++] = int8_t(rt);
+          break;
+        }
+      }
       default:
         return false;
     }
   }
+  if (Phase && sp) {
+    // an expression segment's value
+    value = sv[sp - 1];
+    tag = st[sp - 1];
+    return true;
+  }
   return false;  // finished without return
+}
+
+__host__ __device__ inline bool run_program(const VmView& v, const int32_t* code, int n, const int64_t* consts,
+                                            int n_locals, int c, int64_t& value, int& tag, uint64_t& steps) {
+  int64_t lv[kLowerLocals];
+  int8_t lt[kLowerLocals];
+  if (n_locals < v.n_inputs || n_locals > kLowerLocals) return false;
+  uint64_t set = 0;  // bit k: local k holds a value
+  for (int j = 0; j < v.n_inputs; ++j) {
+    lv[j] = v.inputs[size_t(j) * v.C + c];
+    lt[j] = int8_t(v.local_types[j]);
+    set |= 1ull << j;
+  }
+  int fuel = v.fuel;
+  return run_code<false>(v, code, n, consts, n_locals, lv, lt, set, fuel, nullptr, value, tag, steps);
+}
+
+// ------------------------------------------------------------ bounded regions
+// A program's bounded regions at run time: the region table, the records
+// and phase code after the main code (lower_program's layout), the phase
+// constants after the main ones, and this lane's frame and memo workspace
+// (region_lane_words int64 words).
+struct RegionRun {
+  const RegionInfo* regions;
+  int n_regions;
+  const int32_t* records;   // code + 5 * (main instructions)
+  int n_records;            // instructions after the main code
+  const int64_t* phase_consts;
+  int64_t* ws;
+  size_t ws_words;
+};
+
+// The records of region `ordinal`: its header's position, and its table
+// entry; -1 when the records do not hold it.
+__host__ __device__ inline int region_header(const RegionRun& rr, int ordinal, int* const_offset) {
+  int at = 0, co = 0;
+  for (int r = 0;; ++r) {
+    if (at < 0 || at >= rr.n_records || rr.records[5 * at] != kRegionRecord) return -1;
+    const int captures = rr.records[5 * at + 4], phases = rr.records[5 * at + 3];
+    if (r == ordinal) {
+      *const_offset = co;
+      return at;
+    }
+    at += 1 + captures;
+    for (int p = 0; p < phases; ++p) {
+      if (at >= rr.n_records) return -1;
+      co += rr.records[5 * at + 3];
+      at += 1 + rr.records[5 * at + 2];
+    }
+  }
+}
+__host__ __device__ inline int region_operands(const RegionRun& rr, int ordinal) {
+  int co = 0;
+  const int at = region_header(rr, ordinal, &co);
+  if (at < 0) return -1;
+  const int info = rr.records[5 * at + 2];
+  return info >= 0 && info < rr.n_regions ? rr.regions[info].operands : -1;
+}
+
+__host__ __device__ inline bool region_addable(int64_t a, int64_t b) {
+  return b > 0 ? a <= INT64_MAX - b : b < 0 ? a >= INT64_MIN - b : true;
+}
+
+// One bounded region: the frame stack of d_run_bounded_region_impl
+// (cpp/src/runtime/gpu/device/region_execution_device.cuh:328-510), whose
+// results equal the reference CPU engine's execute_bounded_region with its
+// region adapter (cpu/bounded_region.hpp:112-189, cpu/region_adapter.hpp:171-269).
+// The coordinate bounds are resolved once and checked (lower <= upper;
+// every request's offsets representable over a non-empty domain).  A frame
+// entered is charged entry_fuel; a state outside the domain takes the
+// boundary phase, else the base predicate decides between the base body
+// and, after a memo miss, the requests in order -- each child state built
+// by its transitions, a push past the frame limit a timeout -- and then
+// the combine phase, whose value a memoized region stores (a store past
+// the cell limit a timeout).  Phases run on the shared fuel with their
+// bindings preset.  Coordinates are Int by the region's admission, so
+// frames keep payloads only.
+__host__ __device__ inline bool run_region(const VmView& v, const RegionRun& rr, int ordinal, const int64_t* opv,
+                                           const int8_t* opt, const int64_t* caller_lv, const int8_t* caller_lt,
+                                           uint64_t caller_set, int& fuel, int64_t& value, int& tag, uint64_t& steps) {
+  int co = 0;
+  const int at = region_header(rr, ordinal, &co);
+  if (at < 0) return false;
+  const int info_index = rr.records[5 * at + 2];
+  if (info_index < 0 || info_index >= rr.n_regions) return false;
+  const RegionInfo& R = rr.regions[info_index];
+  const int S = R.state_count, Q = R.request_count;
+  // phase code, constants and locals
+  const int32_t* pcode[4];
+  const int64_t* pconst[4];
+  int plen[4], plocals[4];
+  {
+    int k = at + 1 + R.captures;
+    for (int p = 0; p < 4; ++p) {
+      if (k >= rr.n_records) return false;
+      plen[p] = rr.records[5 * k + 2];
+      plocals[p] = rr.records[5 * k + 4] & 0xffff;
+      pcode[p] = rr.records + 5 * (k + 1);
+      pconst[p] = rr.phase_consts + co;
+      co += rr.records[5 * k + 3];
+      k += 1 + plen[p];
+      if (k > rr.n_records || plocals[p] > kLowerLocals) return false;
+    }
+  }
+  int capture_slot[8];
+  for (int c = 0; c < R.captures; ++c) capture_slot[c] = rr.records[5 * (at + 1 + c) + 2];
+  for (int i = 0; i < R.operands; ++i)
+    if (opt[i] != GAGP_TAG_INT) return false;  // states and bound operands are Int
+  // the coordinate domain
+  int64_t lower[4], upper[4];
+  bool empty = false;
+  for (int x = 0; x < R.axis_count; ++x) {
+    lower[x] = R.lower_kind[x] ? opv[R.lower[x]] : R.lower[x];
+    upper[x] = R.upper_kind[x] ? opv[R.upper[x]] : R.upper[x];
+    if (lower[x] > upper[x]) return false;
+    empty |= !R.inclusive && lower[x] == upper[x];
+  }
+  if (!empty)
+    for (int x = 0; x < R.axis_count; ++x) {
+      const int64_t top = R.inclusive ? upper[x] : upper[x] - 1;
+      for (int q = 0; q < Q; ++q) {
+        const int64_t off = R.transition_offset[q][R.axis_slot[x]];
+        if (!region_addable(lower[x], off) || !region_addable(top, off)) return false;
+      }
+    }
+  if (R.frames == 0) return false;  // Timeout
+  if (!rr.ws || rr.ws_words < region_lane_words(R)) return false;
+  // workspace: frames of (states, results, next request), then memo cells
+  // of (states, value)
+  const int fw = S + Q + 1;
+  int64_t* frames = rr.ws;
+  int64_t* memo = rr.ws + size_t(R.frames) * fw;
+  uint32_t memo_count = 0;
+  int depth = 1;
+  for (int i = 0; i < S; ++i) frames[i] = opv[i];
+  frames[S + Q] = -1;
+  // one phase on frame f: bindings preset as its first locals
+  auto phase = [&](int p, const int64_t* f, int64_t& out) -> bool {
+    int64_t lv[kLowerLocals];
+    int8_t lt[kLowerLocals];
+    uint64_t set = 0;
+    for (int b = 0; b < R.phase_bindings[p]; ++b) {
+      const int bank = R.binding_bank[p][b], slot = R.binding_slot[p][b];
+      if (bank == 0) {
+        lv[b] = f[slot];
+        lt[b] = int8_t(GAGP_TAG_INT);
+      } else if (bank == 3) {
+        lv[b] = f[S + slot];
+        lt[b] = int8_t(R.result_type);
+      } else {
+        const int local = capture_slot[slot];
+        if (local < 0 || local >= 64 || !((caller_set >> local) & 1)) continue;  // unset: not preset
+        lv[b] = caller_lv[local];
+        lt[b] = caller_lt[local];
+      }
+      set |= 1ull << b;
+    }
+    int t = 0;
+    if (!run_code<true>(v, pcode[p], plen[p], pconst[p], plocals[p], lv, lt, set, fuel, nullptr, out, t, steps))
+      return false;
+    return t == R.phase_type[p];
+  };
+  int64_t result = 0;
+  for (;;) {
+    int64_t* f = frames + size_t(depth - 1) * fw;
+    bool completed = false;
+    if (f[S + Q] < 0) {
+      if (fuel < 0 || R.entry_fuel > uint32_t(fuel)) return false;  // Timeout
+      fuel -= int(R.entry_fuel);
+      bool boundary = false, base = false;
+      for (int x = 0; x < R.axis_count; ++x) {
+        const int64_t c = f[R.axis_slot[x]];
+        boundary |= c < lower[x] || (R.inclusive ? c > upper[x] : c >= upper[x]);
+      }
+      if (!boundary) {
+        int64_t b;
+        if (!phase(0, f, b)) return false;
+        base = b != 0;
+      }
+      if (boundary || base) {
+        if (!phase(boundary ? 3 : 1, f, result)) return false;
+        completed = true;
+      } else {
+        if (R.memoized)
+          for (uint32_t cell = 0; cell < memo_count; ++cell) {
+            bool match = true;
+            for (int i = 0; i < S; ++i) match &= memo[size_t(cell) * (S + 1) + i] == f[i];
+            if (match) {
+              result = memo[size_t(cell) * (S + 1) + S];
+              completed = true;
+              break;
+            }
+          }
+        if (!completed) f[S + Q] = 0;
+      }
+    }
+    if (!completed && f[S + Q] < Q) {
+      const int q = int(f[S + Q]);
+      int64_t next[4];
+      for (int i = 0; i < S; ++i) {
+        const int64_t src = f[R.transition_source[q][i]];
+        if (R.transition_kind[q][i] == 0) {
+          next[i] = src;
+        } else {
+          if (!region_addable(src, R.transition_offset[q][i])) return false;
+          next[i] = src + R.transition_offset[q][i];
+        }
+      }
+      if (uint32_t(depth) >= R.frames) return false;  // Timeout: frame capacity
+      ++f[S + Q];
+      int64_t* g = frames + size_t(depth) * fw;
+      for (int i = 0; i < S; ++i) g[i] = next[i];
+      g[S + Q] = -1;
+      ++depth;
+      continue;
+    }
+    if (!completed) {
+      if (!phase(2, f, result)) return false;
+      if (R.memoized) {
+        if (memo_count >= R.cells) return false;  // Timeout: memo capacity
+        for (int i = 0; i < S; ++i) memo[size_t(memo_count) * (S + 1) + i] = f[i];
+        memo[size_t(memo_count) * (S + 1) + S] = result;
+        ++memo_count;
+      }
+    }
+    if (--depth == 0) break;
+    int64_t* parent = frames + size_t(depth - 1) * fw;
+    parent[S + parent[S + Q] - 1] = result;
+  }
+  value = result;
+  tag = R.result_type;
+  return true;
+}
+
+// A program with bounded regions on case `c`: n_main instructions of main
+// code followed by n - n_main of records and phase code; the phase
+// constants follow main_consts main constants.
+__host__ __device__ inline bool run_program_regions(const VmView& v, const RegionInfo* regions, int n_regions,
+                                                    const int32_t* code, int n, int n_main, const int64_t* consts,
+                                                    int main_consts, int n_locals, int c, int64_t* ws,
+                                                    size_t ws_words, int64_t& value, int& tag, uint64_t& steps) {
+  int64_t lv[kLowerLocals];
+  int8_t lt[kLowerLocals];
+  if (n_locals < v.n_inputs || n_locals > kLowerLocals || n_main > n) return false;
+  uint64_t set = 0;
+  for (int j = 0; j < v.n_inputs; ++j) {
+    lv[j] = v.inputs[size_t(j) * v.C + c];
+    lt[j] = int8_t(v.local_types[j]);
+    set |= 1ull << j;
+  }
+  const RegionRun rr{regions, n_regions, code + 5 * n_main, n - n_main, consts + main_consts, ws, ws_words};
+  int fuel = v.fuel;
+  return run_code<false>(v, code, n_main, consts, n_locals, lv, lt, set, fuel, &rr, value, tag, steps);
 }
 
 // ------------------------------------------------------------ warp-SIMD exact VM

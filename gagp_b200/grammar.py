@@ -43,7 +43,7 @@ EK_OPERATION, EK_CONSTANT, EK_BOUND, EK_REFERENCE, EK_INPUT, EK_ALIAS = range(6)
 # PhaseTreeKind (device/phase_compile.cuh:21)
 TK_CONSTANT, TK_LOCAL, TK_OPERATION, TK_IF, TK_AND, TK_OR = range(6)
 TK_PROGRAM, TK_BLOCK, TK_NIL, TK_ASSIGN, TK_RETURN, TK_FOR_RANGE, TK_VAR = range(6, 13)
-TK_LET, TK_BOUND, TK_TRAVERSE = 13, 14, 16
+TK_LET, TK_BOUND, TK_REGION, TK_TRAVERSE = 13, 14, 15, 16
 # grammar locals a phase can name (kPhaseNamedLocals), open lets and loops on
 # one lowering path (kPhaseLets, kPhaseLoops, kPhaseWalks) and the
 # evaluator's locals (MAX_LOCALS)
@@ -154,6 +154,7 @@ class Expression:
     binding_types: List[int] = field(default_factory=list)  # a traversal body's element/index/state tags
     category: str = "Expression"  # syntax category: Expression, or Program/Block/Statement
     label: str = ""               # the local or input an assign, a for_range or a local read names
+    plan: Optional["BoundedPlan"] = None  # a bounded region's plan (front end only)
 
 
 @dataclass
@@ -212,6 +213,39 @@ class Region:
     binding_types: List[int]
     result_type: int
     ranged: bool = False
+    # a bounded region (traversal 0): its plan and phases (BoundedPlan)
+    plan: Optional["BoundedPlan"] = None
+
+
+# region slot banks (RegionSlotBank, cpp/include/gagp/core/region_plan.hpp:96)
+BANKS = {"state": 0, "parameter": 1, "prepared": 2, "result": 3, "measure": 4}
+# capture kinds (PhaseCaptureKind, device/phase_compile.cuh:42)
+CAPTURE_INPUT, CAPTURE_LOCAL, CAPTURE_BOUND = 0, 1, 2
+
+
+@dataclass
+class BoundedPlan:
+    """A bounded region with coordinate progress (``RegionPlan``,
+    cpp/include/gagp/core/region_plan.hpp:64-91, and the phase layout of
+    ``compile_phase_grammar``, phase_grammar.hpp:331-385): initial states and
+    bound operands, four phases (base predicate, base body, combine,
+    boundary), requests that copy or offset states, coordinate axes with
+    literal or operand bounds, and the frame, memo-cell and entry-fuel
+    limits."""
+
+    state_types: List[int]
+    bound_count: int
+    parameter_types: List[int]
+    requests: List[List[Tuple[int, int, int]]]       # per request, per state: (kind 0 copy/1 offset, source, offset)
+    axes: List[Tuple[int, Tuple[int, int], Tuple[int, int]]]  # (state slot, (lower kind, value), (upper kind, value))
+    inclusive: bool
+    memoized: bool
+    frames: int
+    cells: int
+    entry_fuel: int
+    captures: List[Tuple[int, int]]                  # (kind, target)
+    phase_bindings: List[List[Tuple[int, int, int]]]  # per phase: (bank, slot, type)
+    phase_types: List[int]
 
 
 def _parse_int(text) -> int:
@@ -373,6 +407,8 @@ class _Compiler:
             for i, c in enumerate(children):
                 e.children[i] = c
                 e.child_scope[i] = len(scope)
+        elif "structured" in value and self.allow_lists:
+            return self.bounded_region(value, scope)
         elif "signature" in value:
             sig = value["signature"]
             if sig in CATALOG:
@@ -417,6 +453,150 @@ class _Compiler:
             raise Declined("expression form outside the resident scalar subset")
         if "fuel_events" in value:
             raise Declined("fuel profiles are outside the resident scalar subset")
+        self.exprs.append(e)
+        return len(self.exprs) - 1
+
+    def bounded_region(self, value: dict, scope: List[Tuple[str, str]]) -> int:
+        """A bounded structured expression (compiled.cpp:538-640) in the
+        subset this engine runs: coordinate progress, requests that copy or
+        offset states, no preparations and no request expressions."""
+        st = value["structured"]
+        if st.get("family") != "bounded":
+            raise Declined("structured family outside bounded regions")
+        plan = st["plan"]
+        if plan.get("version", 1) != 1 or plan.get("progress") != "coordinates":
+            raise Declined("bounded regions other than coordinate recurrences")
+        if plan.get("preparations") or plan.get("request_expression_types"):
+            raise Declined("bounded region preparations and request expressions")
+        state_types = [self.tags.get(t, TAG_INVALID) for t in plan["state_types"]]
+        if not state_types or len(state_types) > 4 or any(t != TAG_INT for t in state_types):
+            raise Declined("bounded region states other than 1..4 Int coordinates")
+        bound_count = int(plan.get("bound_operand_count", 0))
+        if not 0 <= bound_count <= 8:
+            raise Declined("bounded region bound operands")
+        result = plan["result_type"]
+        if result not in ("Int", "Bool"):
+            raise Declined("bounded region result type")
+        parameters = plan.get("parameter_types", [])
+        if len(parameters) > 8 or any(t not in self.tags for t in parameters):
+            raise Declined("bounded region parameters")
+        requests = []
+        for r in plan["requests"]:
+            row = []
+            for tr in r["states"]:
+                kind = {"copy_state": 0, "coordinate_offset": 1}.get(tr["kind"])
+                if kind is None:
+                    raise Declined("bounded region transition outside copy and coordinate offset")
+                source = int(tr["source_state"])
+                if not 0 <= source < len(state_types):
+                    raise Declined("bounded region transition source")
+                row.append((kind, source, _parse_int(tr.get("offset", "0")) if kind == 1 else 0))
+            if len(row) != len(state_types):
+                raise Declined("bounded region request shape")
+            requests.append(row)
+        if not 1 <= len(requests) <= 8:
+            raise Declined("bounded region request count")
+        slots = [int(x) for x in plan["coordinate_slots"]]
+        domains = plan["coordinate_domains"]
+        if not slots or len(slots) != len(domains) or any(not 0 <= x < len(state_types) for x in slots):
+            raise Declined("bounded region coordinate axes")
+
+        def bound(b):
+            if b["kind"] == "literal":
+                return (0, _parse_int(b["literal"]))
+            if b["kind"] == "operand":
+                k = int(b["operand"])
+                if not 0 <= k < len(state_types) + bound_count:
+                    raise Declined("bounded region bound operand")
+                return (1, k)
+            raise Declined("bounded region bound kind")
+        axes = [(x, bound(d["lower"]), bound(d["upper"])) for x, d in zip(slots, domains)]
+        limits = plan.get("limits", {})
+        frames, cells, entry_fuel = int(limits.get("frames", 64)), int(limits.get("cells", 0)), \
+            int(limits.get("entry_fuel", 1))
+        if not 0 <= frames <= 128 or not 0 <= cells <= 256 or not 0 <= entry_fuel < 2 ** 31:
+            raise Declined("bounded region limits")
+        # captures: the caller's inputs, grammar locals or binders the
+        # phases read as parameters
+        captures = []
+        for cap, ptype in zip(value.get("captures", []), parameters):
+            if "input" in cap:
+                names = [n for n, _ in self.inputs]
+                if cap["input"] not in names:
+                    raise Declined("bounded region capture")
+                k = names.index(cap["input"])
+                captures.append((CAPTURE_INPUT, k, self.inputs[k][1]))
+            elif "local" in cap:
+                names = [n for n, _ in self.locals]
+                if cap["local"] not in names:
+                    raise Declined("bounded region capture")
+                k = names.index(cap["local"])
+                captures.append((CAPTURE_LOCAL, k, self.locals[k][1]))
+            elif "bound" in cap:
+                names = [n for n, _ in scope]
+                if cap["bound"] not in names:
+                    raise Declined("bounded region capture")
+                k = len(names) - 1 - names[::-1].index(cap["bound"])
+                captures.append((CAPTURE_BOUND, k, scope[k][1]))
+            else:
+                raise Declined("bounded region capture")
+            if captures[-1][2] != ptype:
+                raise Declined("bounded region capture type mismatch")
+        if len(captures) != len(parameters):
+            raise Declined("bounded region capture count must match plan parameters")
+        operands = len(state_types) + bound_count
+        phases = value["phases"]
+        if len(phases) != 4:
+            raise Declined("bounded region phases")
+        # phase kinds in argument order: base predicate, base body, combine,
+        # boundary (bounded_region_phase_kind, region_plan.cpp:511-527)
+        phase_types = [TAG_BOOL, self.tags[result], self.tags[result], self.tags[result]]
+        phase_scopes, phase_bindings = [], []
+        for p, ph in enumerate(phases):
+            if int(ph["argument"]) != operands + p:
+                raise Declined("bounded region phase argument is not canonical")
+            names, bindings = [], []
+            for b in ph["bindings"]:
+                bank = BANKS.get(b["bank"])
+                slot = int(b["slot"])
+                if bank == BANKS["state"] and 0 <= slot < len(state_types):
+                    t = "Int"
+                elif bank == BANKS["parameter"] and 0 <= slot < len(parameters):
+                    t = parameters[slot]
+                elif bank == BANKS["result"] and p == 2 and 0 <= slot < len(requests):
+                    t = result
+                else:
+                    raise Declined("bounded region binding outside the subset")
+                names.append((b["name"], t))
+                bindings.append((bank, slot, self.tags[t]))
+            if len(bindings) > 7:
+                raise Declined("bounded region phase binding capacity")
+            phase_scopes.append(names)
+            phase_bindings.append(bindings)
+        args = value.get("args", [])
+        if len(args) != operands + 4:
+            raise Declined("bounded region argument count")
+        arg_types = ["Int"] * operands + ["Bool", result, result, result]
+        children = []
+        for k, a in enumerate(args):
+            children.append(self.expression(a, scope if k < operands else phase_scopes[k - operands]))
+            if self.exprs[children[-1]].result != arg_types[k] or self.exprs[children[-1]].category != "Expression":
+                raise Declined("bounded region argument type mismatch")
+        e = Expression(kind=EK_OPERATION, node_kind=TK_REGION, arity=len(children), type=self.tags[result],
+                       result=result, name="bounded_region")
+        for k, ch in enumerate(children):
+            e.children[k] = ch
+            e.child_scope[k] = len(scope) if k < operands else len(phase_scopes[k - operands])
+        fuel = value.get("fuel_events", {})
+        if set(fuel) - {"operation"}:
+            raise Declined("bounded region fuel profile capability")
+        e.fuel = int(fuel.get("operation", 1))
+        e.plan = BoundedPlan(state_types=state_types, bound_count=bound_count,
+                             parameter_types=[self.tags[t] for t in parameters], requests=requests, axes=axes,
+                             inclusive=plan.get("coordinate_endpoint", "exclusive") == "inclusive",
+                             memoized=bool(plan.get("memoized", False)), frames=frames, cells=cells,
+                             entry_fuel=entry_fuel, captures=[(k, t) for k, t, _ in captures],
+                             phase_bindings=phase_bindings, phase_types=phase_types)
         self.exprs.append(e)
         return len(self.exprs) - 1
 
@@ -519,6 +699,7 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
             visit_nt(e.target, [env[m] for m in e.scope_map])
             return
         x.node_kind, x.opcode, x.operand, x.arity = e.node_kind, e.opcode, e.operand, e.arity
+        x.fuel, x.merge_fuel = e.fuel, e.merge_fuel
         x.children, x.child_scope = list(e.children), list(e.child_scope)
         child_env = [env] * e.arity
         if isinstance(e.operand, tuple):
@@ -534,6 +715,29 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
                 raise Declined("let capability")
             child_env[1] = env + [binder]
             x.operand = binder
+        elif e.node_kind == TK_REGION:
+            # a bounded region (phase_grammar.hpp:331-385): operands see the
+            # surrounding environment; phase p sees only its own bindings,
+            # numbered from zero
+            plan = e.plan
+            operands = len(plan.state_types) + plan.bound_count
+            for p in range(4):
+                child_env[operands + p] = list(range(len(plan.phase_bindings[p])))
+                _check_phase_closed(c, e.children[operands + p])
+            captures = []
+            for kind, target in plan.captures:
+                if kind == CAPTURE_INPUT:
+                    target = names.index(grammar_inputs[target])
+                elif kind == CAPTURE_BOUND:
+                    target = env[target]
+                elif target >= NAMED_LOCALS:
+                    raise Declined("grammar local capacity")
+                captures.append((kind, target))
+            x.operand = len(regions)
+            regions.append(Region(traversal=0, binders=[0, 0, 0],
+                                  operand_types=[c.exprs[k].type for k in e.children[:operands]],
+                                  binding_types=[TAG_INVALID] * 3, result_type=e.type,
+                                  plan=BoundedPlan(**dict(plan.__dict__, captures=captures))))
         elif e.node_kind == TK_TRAVERSE:
             binder = max(env) + 1 if env else 0
             if binder + 2 >= 16:
@@ -605,6 +809,27 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
         local_names=[n for n, _ in c.locals])
     _normalize_static_weights(tables)
     return tables
+
+
+def _check_phase_closed(c: "_Compiler", root: int) -> None:
+    """A region phase reads only its bindings: no input, grammar local,
+    statement, traversal or nested region is reachable from it
+    (phase_grammar.hpp:413-431)."""
+    seen = set()
+    stack = [root]
+    while stack:
+        i = stack.pop()
+        if i in seen:
+            continue
+        seen.add(i)
+        e = c.exprs[i]
+        if e.kind == EK_INPUT or e.node_kind in (TK_VAR, TK_REGION, TK_TRAVERSE) and e.kind == EK_OPERATION \
+                or e.category != "Expression":
+            raise Declined("region phase reaches a program variable, statement, traversal or nested region")
+        if e.kind == EK_REFERENCE:
+            stack.extend(c.productions[p][1] for p in c.nt_productions[e.target])
+        else:
+            stack.extend(e.children[:e.arity])
 
 
 def _check_lowering_capacity(exprs, nts, prods, reachable, root, depth_count, max_depth, inputs, named_locals):

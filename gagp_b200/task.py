@@ -237,6 +237,28 @@ def program_text(tables: G.PhaseTables, origins, constants, first_binder: int = 
             out.append("v%d" % env[e.operand])
             return
         ids, binders = None, None
+        if e.node_kind == G.TK_REGION and e.kind == G.EK_OPERATION:
+            # a bounded region: operands, then each phase, whose bindings
+            # (binders 0.. of the phase) read as fresh variables
+            plan = tables.regions[e.operand].plan
+            operands = len(plan.state_types) + plan.bound_count
+            out.append("(" + e.name)
+            for i in range(e.arity):
+                out.append(" ")
+                if i < operands:
+                    node()
+                    continue
+                bound = len(plan.phase_bindings[i - operands])
+                ids = [next_id[0] + j for j in range(bound)]
+                next_id[0] += bound
+                saved = dict(env)
+                env.clear()
+                env.update(zip(range(bound), ids))
+                node()
+                env.clear()
+                env.update(saved)
+            out.append(")")
+            return
         if e.node_kind == G.TK_TRAVERSE:
             binders = tables.regions[e.operand].binders
             ids = [next_id[0] + j for j in range(3)]

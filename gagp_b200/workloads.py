@@ -32,6 +32,7 @@ Inputs are generated with ``random.Random(seed)``.
 from __future__ import annotations
 
 import json
+import math
 import os
 import random
 from dataclasses import dataclass, field
@@ -291,6 +292,111 @@ def list_statements(population: int = 8192, generations: int = 96, seed: int = 0
     return task
 
 
+def _transition(kind: str, source: int, offset: int = 0) -> dict:
+    return {"kind": kind, "source_state": source, "offset": str(offset),
+            "window": {"begin": {"kind": "begin", "cut": 0}, "end": {"kind": "begin", "cut": 0}}, "expression": 0}
+
+
+def grid_paths_grammar(max_nodes: int = 48, max_depth: int = 12, fuel: int = 20000, frames: int = 16,
+                       cells: int = 64) -> dict:
+    """A grammar with a bounded region: a memoized coordinate recurrence
+    over (r, c) in [0, rows) x [0, columns) whose requests step to (r - 1, c)
+    and (r, c - 1), and whose four phases are evolved: the base predicate
+    (reads r and c), the base body (reads the captured input `columns`),
+    the combine (reads both request results) and the boundary value.  No
+    program has two derivations: the reference re-derives its generated
+    initial programs from their syntax trees, which picks one derivation of
+    an ambiguous program, while the device keeps the generated one."""
+    ref = lambda n: {"ref": n}  # noqa: E731
+    plan = {
+        "version": 1, "state_types": ["Int", "Int"], "result_type": "Int", "parameter_types": ["Int"],
+        "preparations": [], "request_expression_types": [], "bound_operand_count": 2,
+        "requests": [{"states": [_transition("coordinate_offset", 0, -1), _transition("coordinate_offset", 1, 0)]},
+                     {"states": [_transition("coordinate_offset", 0, 0), _transition("coordinate_offset", 1, -1)]}],
+        "limits": {"frames": frames, "cells": cells, "entry_fuel": 1}, "memoized": True,
+        "duplicate_policy": "reject", "progress": "coordinates", "coordinate_slots": [0, 1],
+        "coordinate_rank": [{"coordinate": 0, "direction": 1}, {"coordinate": 1, "direction": 1}],
+        "coordinate_domains": [
+            {"lower": {"kind": "literal", "literal": "0", "operand": 0},
+             "upper": {"kind": "operand", "literal": "0", "operand": 2}},
+            {"lower": {"kind": "literal", "literal": "0", "operand": 0},
+             "upper": {"kind": "operand", "literal": "0", "operand": 3}}],
+        "coordinate_endpoint": "exclusive", "sequence_state": 0}
+    region = {"structured": {"family": "bounded", "plan": plan}, "captures": [{"input": "columns"}],
+              "phases": [{"argument": 4, "bindings": [{"bank": "state", "slot": 0, "name": "r"},
+                                                      {"bank": "state", "slot": 1, "name": "c"}]},
+                         {"argument": 5, "bindings": [{"bank": "parameter", "slot": 0, "name": "p"}]},
+                         {"argument": 6, "bindings": [{"bank": "result", "slot": 0, "name": "up"},
+                                                      {"bank": "result", "slot": 1, "name": "left"}]},
+                         {"argument": 7, "bindings": []}],
+              "args": [ref("Coord"), ref("Coord"), {"input": "rows"}, {"input": "columns"}, ref("Test"),
+                       ref("Base"), ref("Join"), ref("Edge")]}
+    small = lambda *v: {"constant": {"type": "Int", "values": [str(x) for x in v]}}  # noqa: E731
+    return {
+        "format_version": "grammar-definition-v2",
+        "entry": {"nonterminal": "Top", "type": "Int"},
+        "inputs": [{"name": "row", "type": "Int"}, {"name": "column", "type": "Int"},
+                   {"name": "rows", "type": "Int"}, {"name": "columns", "type": "Int"}],
+        "search_limits": {"max_nodes": max_nodes, "max_depth": max_depth},
+        "execution_limits": {"fuel": fuel},
+        "nonterminals": [
+            {"id": "Top", "type": "Int", "scope": [], "alternatives": [
+                {"id": "paths", "weight": 3, "expression": region},
+                {"id": "shift", "weight": 1, "expression": {"signature": "add(Int,Int)->Int",
+                                                            "args": [ref("Top"), ref("Coord")]}},
+                {"id": "one", "weight": 1, "expression": small(1)}]},
+            {"id": "Coord", "type": "Int", "scope": [], "alternatives": [
+                {"id": "row", "weight": 2, "expression": {"input": "row"}},
+                {"id": "column", "weight": 2, "expression": {"input": "column"}},
+                {"id": "k", "weight": 1, "expression": small(0, 1)},
+                {"id": "add", "weight": 1, "expression": {"signature": "add(Int,Int)->Int",
+                                                          "args": [ref("Coord"), ref("Coord")]}}]},
+            {"id": "Test", "type": "Bool", "scope": [{"name": "r", "type": "Int"}, {"name": "c", "type": "Int"}],
+             "alternatives": [
+                 {"id": "r0", "weight": 2, "expression": {"signature": "eq(Int,Int)->Bool",
+                                                          "args": [{"bound": "r"}, small(0, 1)]}},
+                 {"id": "c0", "weight": 2, "expression": {"signature": "eq(Int,Int)->Bool",
+                                                          "args": [{"bound": "c"}, small(0, 1)]}},
+                 {"id": "lt", "weight": 1, "expression": {"signature": "lt(Int,Int)->Bool",
+                                                          "args": [{"bound": "r"}, {"bound": "c"}]}},
+                 {"id": "or", "weight": 1, "expression": {"signature": "or(Bool,Bool)->Bool",
+                                                          "args": [ref("Test"), ref("Test")]}}]},
+            {"id": "Base", "type": "Int", "scope": [{"name": "p", "type": "Int"}], "alternatives": [
+                {"id": "one", "weight": 2, "expression": small(1, 2)},
+                {"id": "p", "weight": 1, "expression": {"bound": "p"}},
+                {"id": "sub", "weight": 1, "expression": {"signature": "sub(Int,Int)->Int",
+                                                          "args": [ref("Base"), ref("Base")]}}]},
+            {"id": "Join", "type": "Int", "scope": [{"name": "up", "type": "Int"}, {"name": "left", "type": "Int"}],
+             "alternatives": [
+                 {"id": "add", "weight": 2, "expression": {"signature": "add(Int,Int)->Int",
+                                                           "args": [{"bound": "up"}, {"bound": "left"}]}},
+                 {"id": "up", "weight": 1, "expression": {"bound": "up"}},
+                 {"id": "left", "weight": 1, "expression": {"bound": "left"}},
+                 {"id": "max", "weight": 1, "expression": {"signature": "max(Int,Int)->Int",
+                                                           "args": [ref("Join"), ref("Join")]}},
+                 {"id": "sub", "weight": 1, "expression": {"signature": "sub(Int,Int)->Int",
+                                                           "args": [ref("Join"), ref("Join")]}}]},
+            {"id": "Edge", "type": "Int", "scope": [], "alternatives": [
+                {"id": "k", "weight": 1, "expression": small(0, 1)}]},
+        ],
+    }
+
+
+def grid_paths(population: int = 1024, generations: int = 32, seed: int = 0, cases: int = 40,
+               size: int = 7) -> "TaskFiles":
+    """Lattice paths: C(row + column, row) for row, column in [0, size) on a
+    size x size grid, searched with ``grid_paths_grammar``."""
+    rng = random.Random(seed)
+    train = []
+    for _ in range(cases):
+        r, c = rng.randrange(size), rng.randrange(size)
+        train.append({"inputs": {"row": {"type": "int", "value": r}, "column": {"type": "int", "value": c},
+                                 "rows": {"type": "int", "value": size}, "columns": {"type": "int", "value": size}},
+                      "expected": {"type": "int", "value": math.comb(r + c, r)}})
+    return TaskFiles(name=f"grid-paths-s{seed}", grammar=grid_paths_grammar(), train=train,
+                     search=search_config(population, generations, seed))
+
+
 def _log_uniform_population(rng: random.Random, lo: int, hi: int) -> int:
     # floor(lo * (hi / lo) ** u), u ~ U[0, 1)
     return int(lo * (hi / lo) ** rng.random())
@@ -355,7 +461,7 @@ def serving_mix(count: int = 2000, seed: int = 0) -> List[dict]:
 
 
 WORKLOADS: Dict[str, object] = {"polynomial": polynomial, "poly4": poly4, "list_threshold": list_threshold,
-                                "list_statements": list_statements}
+                                "list_statements": list_statements, "grid_paths": grid_paths}
 
 
 def make(name: str, **kwargs) -> TaskFiles:

@@ -104,8 +104,43 @@ typedef struct gagp_region {
   int32_t binders[3];               /* binder numbers of element, index, state */
   int32_t operand_types[6];         /* ValueTag each child must complete with */
   int32_t binding_types[3];         /* ValueTag of element, index, state */
-  int32_t result_type;              /* ValueTag of the traversal's value (phase_type[0]) */
+  int32_t result_type;              /* ValueTag of the traversal's (or the bounded region's) value */
   uint32_t event_cost[26];          /* PhaseFuelEvent charges when fuel_profile */
+  /* A bounded region (traversal 0): a coordinate recurrence (RegionPlan,
+   * cpp/include/gagp/core/region_plan.hpp:64-91, laid out as compile_phase_grammar
+   * lays it out, phase_grammar.hpp:331-385).  Its children are `operands`
+   * values -- the state_count initial states, then the bound operands --
+   * and its `phases` phase subtrees: base predicate (Bool), base body,
+   * combine and boundary.  Phase p sees phase_bindings[p] values as its
+   * first locals, each from a bank of the current frame. */
+  int32_t operands;
+  int32_t phases;                   /* 4 */
+  int32_t captures;                 /* parameters the phases may read from the caller */
+  int32_t capture_kind[8];          /* 0 evaluator input, 1 grammar local, 2 binder */
+  int32_t capture_target[8];        /* evaluator input position, grammar local or binder number */
+  int32_t phase_type[8];            /* ValueTag phase p yields */
+  int32_t phase_bindings[8];
+  int32_t binding_bank[8][8];       /* 0 state, 1 parameter, 3 request result (RegionSlotBank) */
+  int32_t binding_slot[8][8];
+  int32_t phase_binding_types[8][8];
+  int32_t state_count;              /* Int coordinates, 1..4 */
+  int32_t request_count;            /* 1..8 */
+  int32_t axis_count;               /* 1..4 */
+  int32_t inclusive;                /* coordinate endpoint: 1 inclusive upper bound, 0 exclusive */
+  int32_t memoized;
+  uint32_t frames;                  /* frame limit, <= 128 */
+  uint32_t cells;                   /* memo cell limit, <= 256 */
+  uint32_t entry_fuel;              /* charged when a frame is entered */
+  int32_t parameter_types[8];
+  int32_t transition_kind[8][4];    /* request r, state s: 0 copy a state, 1 offset a coordinate */
+  int32_t transition_source[8][4];
+  int32_t axis_slot[4];             /* the state each coordinate axis reads */
+  int32_t lower_kind[4];            /* 0 literal, 1 operand */
+  int32_t upper_kind[4];
+  int32_t reserved;
+  int64_t transition_offset[8][4];
+  int64_t lower[4];                 /* the literal, or the operand index */
+  int64_t upper[4];
 } gagp_region;
 
 /* The admitted grammar of one search: phase tables plus its single

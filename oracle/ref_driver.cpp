@@ -164,6 +164,26 @@ void print_profile(const rp::HostPhaseGrammar& g) {
   for (std::size_t i = 0; i < g.values.size(); ++i) std::printf("%s%s", i ? "," : "", value_json(g.values[i]).c_str());
   std::printf("],\"minimum\":[");
   for (std::size_t i = 0; i < g.minimum.size(); ++i) std::printf("%s%u", i ? "," : "", g.minimum[i]);
+  // the region table: traversals and bounded regions (PhaseRegionInfo)
+  std::printf("],\"regions\":[");
+  for (std::size_t i = 0; i < g.regions.size(); ++i) {
+    const auto& r = g.regions[i];
+    std::printf("%s{\"traversal\":%d,\"operands\":%d,\"phases\":%d,\"captures\":[", i ? "," : "", r.traversal,
+                r.operands, r.phases);
+    for (int c = 0; c < r.captures; ++c)
+      std::printf("%s[%d,%d]", c ? "," : "", int(r.capture_kind[c]), r.capture_target[c]);
+    std::printf("],\"operand_types\":[");
+    for (int c = 0; c < r.operands; ++c) std::printf("%s%d", c ? "," : "", int(r.operand_types[c]));
+    std::printf("],\"phase_types\":[");
+    for (int p = 0; p < r.phases; ++p) std::printf("%s%d", p ? "," : "", int(r.phase_type[p]));
+    std::printf("],\"binding_types\":[");
+    for (int p = 0; p < r.phases; ++p) {
+      std::printf("%s[", p ? "," : "");
+      for (int b = 0; b < r.phase_bindings[p]; ++b) std::printf("%s%d", b ? "," : "", int(r.binding_types[p][b]));
+      std::printf("]");
+    }
+    std::printf("]}");
+  }
   std::printf("]}");
 }
 

@@ -50,9 +50,11 @@ CASES = [
 # these fixtures pin the table builder's list subset and hold the reference's
 # runs for the list path.  They live in golden/list/.
 LIST_CASES = [
-    ("list_threshold_sum", dict(population=64, generations=3, seed=11, cases=12, target="threshold_sum"), False),
-    ("list_threshold_count", dict(population=64, generations=3, seed=12, cases=12, target="threshold_count"), False),
-    ("list_nested_traversal", dict(population=64, generations=3, seed=13, cases=12, target="max"), True),
+    ("list_threshold_sum", dict(population=64, generations=3, seed=11, cases=12, target="threshold_sum"), None),
+    ("list_threshold_count", dict(population=64, generations=3, seed=12, cases=12, target="threshold_count"), None),
+    ("list_nested_traversal", dict(population=64, generations=3, seed=13, cases=12, target="max"), "nested"),
+    ("list_statements_sum", dict(population=64, generations=3, seed=16, cases=12, target="threshold_sum"),
+     "statements"),
 ]
 
 
@@ -67,6 +69,10 @@ LIST_RUNS = [
     ("list_config3_p1024_g16", dict(population=1024, generations=16, seed=0, cases=200, target="threshold_sum"),
      None),
     ("list_let_p256_g8", dict(population=256, generations=8, seed=15, cases=30, target="threshold_sum"), "let"),
+    ("list_statements_p512_g8", dict(population=512, generations=8, seed=17, cases=40, target="threshold_sum"),
+     "statements"),
+    ("list_statements_p2048_g12", dict(population=2048, generations=12, seed=18, cases=100, target="max"),
+     "statements"),
 ]
 
 # Lowering pins (golden/lower/): the reference's phase compiler output and
@@ -80,7 +86,41 @@ LOWER_CASES = [
     ("lower_int64_edges", "int64_edges", dict(population=512, generations=1, seed=26), None),
     ("lower_list_let", "list", dict(population=384, generations=1, seed=27, cases=24, target="threshold_sum"), "let"),
     ("lower_scalar_let", "scalar_let", dict(population=384, generations=1, seed=28, cases=32), None),
+    ("lower_list_statements", "list_statements", dict(population=512, generations=1, seed=29, cases=24), None),
+    ("lower_grid_paths", "grid_paths", dict(population=512, generations=1, seed=63, cases=30), None),
 ]
+
+# Bounded regions (golden/region/): the lattice-path workload, whose
+# grammar holds a memoized coordinate recurrence with evolved phases.  The
+# first fixture also holds the reference's tables, initial rows and one
+# make_batch.
+REGION_CASES = [
+    ("region_grid_paths_p256", dict(population=256, generations=6, seed=61, cases=30), True),
+    ("region_grid_paths_p1024_g16", dict(population=1024, generations=16, seed=62, cases=49), False),
+]
+
+
+def region_fixtures() -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "region"), exist_ok=True)
+    for name, kwargs, full in REGION_CASES:
+        task = W.grid_paths(**kwargs)
+        with tempfile.TemporaryDirectory() as d:
+            task.write(d)
+            tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
+            run = driver("run", tp, "--search", sp)
+            if full:
+                tables = driver("tables", tp, "--search", sp)
+                batch = driver("batch", tp, "--search", sp, "--round-seed", str(LIST_ROUND_SEED))
+        assert run["declined"] == "", (name, run["declined"])
+        fixture = {"name": name, "task": {"name": task.name, "fitness": task.fitness}, "grammar": task.grammar,
+                   "train": task.train, "test": task.test, "search": task.search, "run": run}
+        if full:
+            fixture.update(tables={k: v for k, v in tables.items() if k != "initial"},
+                           initial=[rows[0] for rows in tables["initial"]], batch=batch)
+        with gzip.open(os.path.join(here, "region", name + ".json.gz"), "wt") as f:
+            json.dump(fixture, f, separators=(",", ":"))
+        print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
 
 
 # int64 edge values: the extremes, the 32-bit boundaries the fast VM's
@@ -218,6 +258,8 @@ def variant_grammar(variant):
         return reverse_traversal_grammar()
     if variant == "deep":
         return deep_traversal_grammar()
+    if variant == "statements":
+        return W.list_statements_grammar()
     return None
 
 
@@ -431,6 +473,7 @@ def main() -> None:
     ap.add_argument("--judge-only", action="store_true", help="regenerate golden/judge/ only")
     ap.add_argument("--generational-only", action="store_true", help="regenerate golden/generational/ only")
     ap.add_argument("--init-only", action="store_true", help="regenerate golden/init/ only")
+    ap.add_argument("--region-only", action="store_true", help="regenerate golden/region/ only")
     ap.add_argument("--headline", action="store_true",
                     help="regenerate golden/headline/ only (the benchmark's search, several minutes)")
     args = ap.parse_args()
@@ -445,6 +488,9 @@ def main() -> None:
         return
     if args.generational_only:
         gen_fixtures()
+        return
+    if args.region_only:
+        region_fixtures()
         return
     if args.init_only:
         init_fixtures()
@@ -473,10 +519,10 @@ def main() -> None:
             json.dump(fixture, f, separators=(",", ":"))
         print(name, len(run["history"]), "history entries,", len(run["final"]), "final members")
     os.makedirs(os.path.join(here, "list"), exist_ok=True)
-    for name, kwargs, nested in LIST_CASES:
+    for name, kwargs, variant in LIST_CASES:
         task = W.list_threshold(**kwargs)
-        if nested:
-            task.grammar = nested_traversal_grammar()
+        if variant:
+            task.grammar = variant_grammar(variant)
         with tempfile.TemporaryDirectory() as d:
             task.write(d)
             tp, sp = os.path.join(d, "task.json"), os.path.join(d, "search.json")
@@ -513,6 +559,7 @@ def main() -> None:
     judge_fixtures()
     gen_fixtures()
     init_fixtures()
+    region_fixtures()
 
 
 def row_digest(rows) -> str:

@@ -44,15 +44,17 @@ def _i32(a):
     return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
 
 
-def lower(grammar_blob, origins, constants, code_cap=4096):
+def lower(grammar_blob, origins, constants, code_cap=4096, shape=False):
     """(code as an (n, 5) array, constants, locals, stack bound), or None when
-    the lowering rejects the row."""
+    the lowering rejects the row; with `shape` also the main code's
+    instructions and constants (a program with bounded regions has records
+    and phase code after them)."""
     lib = library()
     o = _i32(origins)
     k = np.ascontiguousarray(np.asarray(constants, dtype=np.int64))
     code = np.zeros((code_cap, 5), dtype=np.int32)
     consts = np.zeros(code_cap, dtype=np.int64)
-    out = np.zeros(4, dtype=np.int32)
+    out = np.zeros(6, dtype=np.int32)
     n = lib.host_lower(grammar_blob.ref(), o.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int(len(o)),
                        k.ctypes.data_as(C.POINTER(C.c_int64)), C.c_int(len(k)),
                        code.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int(code_cap),
@@ -60,6 +62,8 @@ def lower(grammar_blob, origins, constants, code_cap=4096):
                        out.ctypes.data_as(C.POINTER(C.c_int32)))
     if n < 0:
         return None
+    if shape:
+        return code[:n].copy(), consts[:out[1]].copy(), int(out[2]), int(out[3]), int(out[4]), int(out[5])
     return code[:n].copy(), consts[:out[1]].copy(), int(out[2]), int(out[3])
 
 
@@ -74,4 +78,18 @@ def run(cases_blob, local_types, fuel, code, consts, n_locals, case):
                       code.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int(len(code)),
                       consts.ctypes.data_as(C.POINTER(C.c_int64)), C.c_int(n_locals), C.c_int(case),
                       C.byref(value), C.byref(tag), C.byref(steps))
+    return bool(ok), value.value, tag.value, steps.value
+
+
+def run_regions(grammar_blob, cases_blob, fuel, code, n_main, consts, main_consts, n_locals, case):
+    """(ok, value, tag, steps) of one case of a program with bounded regions."""
+    lib = library()
+    lib.host_run_regions.restype = C.c_int
+    code = np.ascontiguousarray(code, dtype=np.int32)
+    consts = np.ascontiguousarray(consts, dtype=np.int64)
+    value, tag, steps = C.c_int64(), C.c_int32(), C.c_uint64()
+    ok = lib.host_run_regions(grammar_blob.ref(), cases_blob.ref(), C.c_int(fuel),
+                              code.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int(len(code)), C.c_int(n_main),
+                              consts.ctypes.data_as(C.POINTER(C.c_int64)), C.c_int(main_consts), C.c_int(n_locals),
+                              C.c_int(case), C.byref(value), C.byref(tag), C.byref(steps))
     return bool(ok), value.value, tag.value, steps.value

@@ -3,6 +3,7 @@
 // with the reference's own compiler output and CPU evaluator without a GPU.
 // The product never loads this library; its kernels run the same functions
 // on the device.
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -11,19 +12,7 @@
 namespace {
 std::vector<gb::RegionInfo> regions_of(const gagp_region* regions, int count) {
   std::vector<gb::RegionInfo> out(count > 0 ? count : 1);
-  for (int r = 0; r < count; ++r) {
-    const gagp_region& x = regions[r];
-    gb::RegionInfo& y = out[r];
-    y.traversal = int8_t(x.traversal);
-    y.ranged = int8_t(x.ranged);
-    y.arity = int8_t(x.ranged ? 6 : 4);
-    y.result_type = int8_t(x.result_type);
-    for (int k = 0; k < 3; ++k) {
-      y.binders[k] = int8_t(x.binders[k]);
-      y.binding_types[k] = int8_t(x.binding_types[k]);
-    }
-    for (int k = 0; k < 6; ++k) y.operand_types[k] = int8_t(x.operand_types[k]);
-  }
+  for (int r = 0; r < count; ++r) out[r] = gb::region_info_of(regions[r]);
   return out;
 }
 }  // namespace
@@ -49,6 +38,8 @@ int host_lower(const gagp_grammar* g, const int32_t* origins, int n, const int64
   out[1] = r.constants;
   out[2] = r.locals;
   out[3] = r.stack_bound;
+  out[4] = r.main;
+  out[5] = r.main_constants;
   return len;
 }
 
@@ -66,6 +57,31 @@ int host_run(const gagp_cases* cases, const int32_t* local_types, int fuel, cons
   int t = 0;
   uint64_t s = 0;
   const bool ok = gb::run_program(v, code, n, consts, n_locals, c, *value, t, s);
+  *tag = t;
+  *steps = s;
+  return ok ? 1 : 0;
+}
+
+// Runs a lowered program with bounded regions (its main code the first
+// n_main instructions, its main constants the first main_consts) on case
+// `c`, with a host frame and memo workspace.
+int host_run_regions(const gagp_grammar* g, const gagp_cases* cases, int fuel, const int32_t* code, int n, int n_main,
+                     const int64_t* consts, int main_consts, int n_locals, int c, int64_t* value, int32_t* tag,
+                     uint64_t* steps) {
+  const int C = cases->case_count, NI = cases->input_count;
+  std::vector<int64_t> inputs(size_t(NI > 0 ? NI : 1) * C);
+  for (int j = 0; j < NI; ++j)
+    for (int k = 0; k < C; ++k) inputs[size_t(j) * C + k] = cases->inputs[size_t(k) * NI + j];
+  const gb::VmView v{inputs.data(), g->local_types, cases->list_values,
+                     cases->list_values ? cases->list_value_count : 0, C, NI, fuel};
+  const std::vector<gb::RegionInfo> regions = regions_of(g->regions, g->region_count);
+  size_t words = 0;
+  for (int r = 0; r < g->region_count; ++r) words = std::max(words, gb::region_lane_words(regions[r]));
+  std::vector<int64_t> ws(words + 1);
+  int t = 0;
+  uint64_t s = 0;
+  const bool ok = gb::run_program_regions(v, regions.data(), g->region_count, code, n, n_main, consts, main_consts,
+                                          n_locals, c, ws.data(), words, *value, t, s);
   *tag = t;
   *steps = s;
   return ok ? 1 : 0;

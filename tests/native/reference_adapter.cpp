@@ -115,6 +115,50 @@ bool evolve_b200_phase_population(gagp_engine* engine, const EvolutionConfig& cf
     for (int k = 0; k < 6; ++k) y.operand_types[k] = int32_t(r.operand_types[k]);
     y.result_type = int32_t(r.phase_type[0]);
     for (int k = 0; k < 26; ++k) y.event_cost[k] = r.event_cost[k];
+    if (r.traversal == 0) {
+      // a bounded region: its table entry, the phase bindings' sources and
+      // the plan (HostPhaseGrammar::region_sources)
+      const auto& source = g.region_sources.at(i);
+      const auto& plan = source.plan;
+      y.operands = r.operands; y.phases = r.phases; y.captures = r.captures;
+      for (int c = 0; c < r.captures && c < 8; ++c) {
+        y.capture_kind[c] = int32_t(r.capture_kind[c]);
+        y.capture_target[c] = r.capture_target[c];
+      }
+      for (int p = 0; p < r.phases && p < 8; ++p) {
+        y.phase_type[p] = int32_t(r.phase_type[p]);
+        y.phase_bindings[p] = r.phase_bindings[p];
+        for (int b = 0; b < r.phase_bindings[p] && b < 8; ++b) {
+          y.phase_binding_types[p][b] = int32_t(r.binding_types[p][b]);
+          y.binding_bank[p][b] = int32_t(source.sources.at(p).at(b).bank);
+          y.binding_slot[p][b] = int32_t(source.sources.at(p).at(b).slot);
+        }
+      }
+      y.result_type = int32_t(plan.result_type);
+      y.state_count = int32_t(plan.state_types.size());
+      y.request_count = int32_t(plan.requests.size());
+      y.axis_count = int32_t(plan.coordinate_slots.size());
+      y.inclusive = plan.coordinate_endpoint == DomainEndpoint::Inclusive;
+      y.memoized = plan.memoized;
+      y.frames = plan.limits.frames; y.cells = plan.limits.cells; y.entry_fuel = plan.limits.entry_fuel;
+      for (std::size_t k = 0; k < plan.parameter_types.size() && k < 8; ++k)
+        y.parameter_types[k] = int32_t(plan.parameter_types[k]);
+      for (std::size_t q = 0; q < plan.requests.size() && q < 8; ++q)
+        for (std::size_t k = 0; k < plan.requests[q].states.size() && k < 4; ++k) {
+          const auto& t = plan.requests[q].states[k];
+          y.transition_kind[q][k] = int32_t(t.kind);  // CopyState 0, CoordinateOffset 1 (others are declined)
+          y.transition_source[q][k] = int32_t(t.source_state);
+          y.transition_offset[q][k] = t.offset;
+        }
+      for (std::size_t a = 0; a < plan.coordinate_slots.size() && a < 4; ++a) {
+        const auto& d = plan.coordinate_domains.at(a);
+        y.axis_slot[a] = int32_t(plan.coordinate_slots[a]);
+        y.lower_kind[a] = d.lower.kind == RegionBoundKind::Operand;
+        y.upper_kind[a] = d.upper.kind == RegionBoundKind::Operand;
+        y.lower[a] = d.lower.kind == RegionBoundKind::Operand ? int64_t(d.lower.operand) : d.lower.literal;
+        y.upper[a] = d.upper.kind == RegionBoundKind::Operand ? int64_t(d.upper.operand) : d.upper.literal;
+      }
+    }
   }
   const auto& nts = grammar.nonterminals()[layout.slots[0].nonterminal];
   gagp_grammar tables{};

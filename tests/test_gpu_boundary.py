@@ -32,6 +32,8 @@ TASKS = [
     ("poly4_generational", lambda: _with_search(W.poly4(population=200, generations=5, seed=8, cases=32,
                                                         max_nodes=40),
                                                 {"schedule": {"mode": "generational"}, "elitism": 2})),
+    ("list_statements", lambda: W.list_statements(population=128, generations=4, seed=9, cases=24)),
+    ("grid_paths", lambda: W.grid_paths(population=128, generations=4, seed=10, cases=30)),
 ]
 
 

@@ -84,11 +84,11 @@ def test_admission_declines_outside_the_resident_subset(poly_task):
         blob.expressions[_first(blob, W_KINDS["input"])].kind = 5  # an alias (template instance)
     assert _bytes(poly_task, template)[0] == 1  # GAGP_DECLINED
 
-    def region(blob):
+    def unknown_kind(blob):
         e = next(i for i in range(len(blob.tables.expressions))
                  if blob.expressions[i].kind == W_KINDS["operation"] and blob.expressions[i].arity > 0)
-        blob.expressions[e].node_kind = 15  # a bounded region
-    assert _bytes(poly_task, region)[0] == 1
+        blob.expressions[e].node_kind = 17  # a tree kind beyond the reference's
+    assert _bytes(poly_task, unknown_kind)[0] == 1
 
     # a statement belongs to a Program entry's phase: in a value phase the
     # tables are malformed

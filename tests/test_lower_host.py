@@ -3,7 +3,8 @@
 For every member of a generated population of each grammar in
 tests/golden/lower/ (list programs with forward, reverse and nested
 traversals, lets, statement programs with grammar locals, loops and
-branches, and the large scalar grammar), the reference's phase compiler
+branches, bounded regions with their records and phase code, and the
+large scalar grammar), the reference's phase compiler
 output and CPU fitness were recorded by ``ref_driver lower``.  The engine's
 own ``lower_program`` and ``run_program`` -- the functions its kernels run,
 compiled here for the host by tests/host_harness.py -- must emit the same
@@ -56,25 +57,26 @@ def test_lowering_and_vm_match_reference(name):
     penalty = int(abs(lt.settings.penalty))
     checked = 0
     for r, row in enumerate(fx["lower"]["rows"]):
-        got = H.lower(blob, row["origins"], row["constants"])
+        got = H.lower(blob, row["origins"], row["constants"], shape=True)
         if row["status"] != 0:
             assert got is None, (name, r)
             continue
         assert got is not None, (name, r, "rejected")
-        code, consts, n_locals, stack_bound = got
+        code, consts, n_locals, stack_bound, n_main, main_consts = got
         ref = row["code"]
-        # a value phase: the reference's code plus the RETURN that
-        # patch_whole_program appends; a statement program (Program entry)
+        # a value phase: the reference's main code plus the RETURN that
+        # patch_whole_program appends, then its bounded regions' records and
+        # phase code (op 255 onwards); a statement program (Program entry)
         # has no terminator
         statements = lt.tables.slot_type == G.TAG_STATEMENT
-        assert len(code) == len(ref) + (0 if statements else 1), (name, r)
-        for i, x in enumerate(ref):
+        ref_main = next((i for i, x in enumerate(ref) if x[0] == 255), len(ref))
+        want = ref[:ref_main] + ([] if statements else [[20, 0, 0, 0, 1]]) + ref[ref_main:]
+        assert len(code) == len(want) and n_main == ref_main + (0 if statements else 1), (name, r)
+        for i, x in enumerate(want):
             mine = [int(code[i][0]), int(code[i][1]) & 3, int(code[i][2]), int(code[i][3]), int(code[i][4])]
             assert mine == x, (name, r, i, mine, x)
-        if not statements:
-            assert list(code[-1]) == [20, 0, 0, 0, 1], (name, r)
         assert len(consts) == len(row["consts"]), (name, r)
-        for i, x in enumerate(code[:len(ref)]):
+        for i, x in enumerate(code[:ref_main]):
             if x[0] == 0:  # PUSH_CONST: the constant's tag and payload
                 tag, iv, bv = row["consts"][x[2]]
                 assert tag == (G.TAG_BOOL if x[1] & 4 else G.TAG_INT), (name, r, i)
@@ -82,7 +84,10 @@ def test_lowering_and_vm_match_reference(name):
         assert n_locals == row["n_locals"] and stack_bound == row["stack_bound"], (name, r)
         loss, wrong = 0, 0
         for c in range(len(cases.expected)):
-            ok, value, tag, _ = H.run(cases, lt.tables.local_types, fuel, code, consts, n_locals, c)
+            if n_main < len(code):
+                ok, value, tag, _ = H.run_regions(blob, cases, fuel, code, n_main, consts, main_consts, n_locals, c)
+            else:
+                ok, value, tag, _ = H.run(cases, lt.tables.local_types, fuel, code, consts, n_locals, c)
             if c < len(row["cases"]):
                 err, rtag, rvalue, _ = row["cases"][c]
                 assert ok == (err < 0), (name, r, c)
