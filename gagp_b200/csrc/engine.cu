@@ -960,6 +960,141 @@ bool import_rows(const gagp_grammar* g, const std::vector<gb::ExprInfo>& info, c
   return true;
 }
 
+// Whether two productions of one nonterminal may derive the same program:
+// their root expressions emit the same node (operations of one opcode and
+// shape, constants with overlapping domains, the same input or binder).
+// Only then can a program have two derivations.
+bool same_root_possible(const gagp_grammar* g, const gagp_expression& x, const gagp_expression& y) {
+  if (x.kind != y.kind) return false;
+  switch (x.kind) {
+    case gb::EK_INPUT: case gb::EK_BOUND: return x.operand == y.operand;
+    case gb::EK_CONSTANT: {
+      const gagp_domain& a = g->domains[x.target];
+      const gagp_domain& b = g->domains[y.target];
+      auto has = [&](const gagp_domain& d, int64_t v) {
+        if (d.integer_range) return d.minimum <= v && v <= d.maximum;
+        for (int k = 0; k < d.value_count; ++k)
+          if (g->values[d.value_offset + k].i == v) return true;
+        return false;
+      };
+      if (a.integer_range && b.integer_range) return std::max(a.minimum, b.minimum) <= std::min(a.maximum, b.maximum);
+      const gagp_domain& list = a.integer_range ? b : a;
+      const gagp_domain& other = a.integer_range ? a : b;
+      for (int k = 0; k < list.value_count; ++k)
+        if (has(other, g->values[list.value_offset + k].i)) return true;
+      return false;
+    }
+    case gb::EK_OPERATION:
+      return x.node_kind == y.node_kind && x.opcode == y.opcode && x.arity == y.arity && x.type == y.type &&
+             (x.operand == y.operand || x.node_kind == gb::TK_REGION || x.node_kind == gb::TK_LET ||
+              x.node_kind == gb::TK_TRAVERSE);
+    default: return true;
+  }
+}
+bool possibly_ambiguous(const gagp_grammar* g) {
+  for (int t = 0; t < g->nonterminal_count; ++t) {
+    const gagp_nonterminal& nt = g->nonterminals[t];
+    for (int a = 0; a < nt.production_count; ++a)
+      for (int b = a + 1; b < nt.production_count; ++b)
+        if (same_root_possible(g, g->expressions[g->productions[nt.production_offset + a].expression],
+                               g->expressions[g->productions[nt.production_offset + b].expression]))
+          return true;
+  }
+  return false;
+}
+
+// The derivation the reference's import gives a generated program
+// (reconstruct_derivation, cpp/src/evolution/grammar/membership.cpp:330-360):
+// at every nonterminal the first production, in production order, whose
+// expression matches the whole subtree.  `origins` and `value` (a constant
+// node's value) describe the program's nodes; out[i] receives node i's
+// expression.  Returns the subtree's end, or -1 (also past `budget` steps).
+int first_match(const gagp_grammar* g, int e, const int32_t* origins, const int64_t* value, int n, int i,
+                int32_t* out, long* budget) {
+  if (--*budget < 0 || i < 0) return -1;
+  const gagp_expression& x = g->expressions[e];
+  if (x.kind == gb::EK_REFERENCE) {
+    const gagp_nonterminal& nt = g->nonterminals[x.target];
+    for (int k = 0; k < nt.production_count; ++k) {
+      const int end = first_match(g, g->productions[nt.production_offset + k].expression, origins, value, n, i, out,
+                                  budget);
+      if (end >= 0) return end;
+    }
+    return -1;
+  }
+  if (i >= n) return -1;
+  const gagp_expression& y = g->expressions[origins[i]];
+  if (x.kind != y.kind) return -1;
+  if (x.kind == gb::EK_CONSTANT) {
+    const gagp_domain& d = g->domains[x.target];
+    bool in = d.integer_range && d.minimum <= value[i] && value[i] <= d.maximum;
+    for (int k = 0; !d.integer_range && k < d.value_count && !in; ++k) in = g->values[d.value_offset + k].i == value[i];
+    if (!in) return -1;
+  } else if (x.kind == gb::EK_OPERATION) {
+    if (x.node_kind != y.node_kind || x.opcode != y.opcode || x.operand != y.operand || x.arity != y.arity ||
+        x.type != y.type)
+      return -1;
+  } else if (x.operand != y.operand) {
+    return -1;
+  }
+  out[i] = e;
+  int j = i + 1;
+  for (int k = 0; k < (x.kind == gb::EK_OPERATION ? x.arity : 0); ++k) {
+    j = first_match(g, x.children[k], origins, value, n, j, out, budget);
+    if (j < 0) return -1;
+  }
+  return j;
+}
+
+// The device's initial population of a search whose grammar may be
+// ambiguous, re-derived as the reference's import re-derives its generated
+// programs: generated on the device (k_init_population), then each row's
+// first-match derivation annotated on the host (import_rows) and uploaded
+// as an imported population.
+gagp_status canonical_initial(gagp_engine* e, Search* s, const gagp_grammar* g, const std::vector<gb::ExprInfo>& info,
+                              gb::SearchDesc* d) {
+  const int P = s->P, S = s->stride;
+  gb::k_init_population<<<(P + 127) / 128, 128, 0, e->stream>>>(s->d_desc, s->d_off, 1);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  std::vector<uint64_t> node(size_t(P) * S);
+  std::vector<int64_t> cval(size_t(P) * S);
+  std::vector<int32_t> len(P);
+  CUDA_TRY(copy_d2h(e, node.data(), d->node, 8 * node.size()));
+  CUDA_TRY(copy_d2h(e, cval.data(), d->cval, 8 * cval.size()));
+  CUDA_TRY(copy_d2h(e, len.data(), d->len, 4 * len.size()));
+  std::vector<int32_t> origins(size_t(P) * S), counts(P), ccounts(P);
+  std::vector<int64_t> value(S);
+  for (int r = 0; r < P; ++r) {
+    const int n = gb::len_nodes(len[r]), nc = gb::len_consts(len[r]);
+    if (n < 1 || n > S) return fail(GAGP_DEVICE_ERROR, "initial population row length");
+    int32_t* o = origins.data() + size_t(r) * S;
+    for (int i = 0, k = 0; i < n; ++i) {
+      const uint64_t w = node[size_t(r) * S + i];
+      o[i] = gb::w_origin(w);
+      value[i] = gb::w_const(w) && k < nc ? cval[size_t(r) * S + k++] : 0;
+    }
+    std::vector<int32_t> canon(o, o + n);
+    long budget = 1 << 20;
+    if (first_match(g, g->root_expression, o, value.data(), n, 0, canon.data(), &budget) == n)
+      std::copy(canon.begin(), canon.end(), o);
+    counts[r] = n;
+    ccounts[r] = nc;
+  }
+  // the rows' constants are read while the annotated rows are written: separate buffers
+  const std::vector<int64_t> constants(cval);
+  gagp_rows rows{P, S, counts.data(), origins.data(), ccounts.data(), const_cast<int64_t*>(constants.data())};
+  std::string why;
+  if (!import_rows(g, info, &rows, P, S, &node, &cval, &len, &why))
+    return fail(GAGP_DEVICE_ERROR, "re-derived initial population: " + why);
+  CUDA_TRY(cudaMemcpyAsync(d->node, node.data(), 8 * node.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(d->cval, cval.data(), 8 * cval.size(), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(d->len, len.data(), 4 * len.size(), cudaMemcpyHostToDevice, e->stream));
+  d->imported = 1;
+  CUDA_TRY(copy_h2d(e, s->d_desc, d, sizeof(gb::SearchDesc)));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return GAGP_OK;
+}
+
 }  // namespace
 
 // ======================================================================= C ABI
@@ -1272,6 +1407,11 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   const int32_t off[4] = {0, s->P, 0, s->B};
   CUDA_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&s->d_off), sizeof(off), e->pool, e->stream));
   CUDA_TRY(copy_h2d(e, s->d_off, off, sizeof(off)));
+  if (!d.imported && possibly_ambiguous(g))
+    if (const gagp_status st = canonical_initial(e, s.get(), g, info, &d); st != GAGP_OK) {
+      cudaFreeAsync(s->block, e->stream);
+      return st;
+    }
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   s->id = e->next_id++;
   e->arena_used += s->bytes;

@@ -298,15 +298,16 @@ def _transition(kind: str, source: int, offset: int = 0) -> dict:
 
 
 def grid_paths_grammar(max_nodes: int = 48, max_depth: int = 12, fuel: int = 20000, frames: int = 16,
-                       cells: int = 64) -> dict:
+                       cells: int = 64, ambiguous: bool = False) -> dict:
     """A grammar with a bounded region: a memoized coordinate recurrence
     over (r, c) in [0, rows) x [0, columns) whose requests step to (r - 1, c)
     and (r, c - 1), and whose four phases are evolved: the base predicate
     (reads r and c), the base body (reads the captured input `columns`),
-    the combine (reads both request results) and the boundary value.  No
-    program has two derivations: the reference re-derives its generated
-    initial programs from their syntax trees, which picks one derivation of
-    an ambiguous program, while the device keeps the generated one."""
+    the combine (reads both request results) and the boundary value.
+    `ambiguous` adds a combine alternative add(Join, Join), which derives
+    add(up, left) a second way: the reference re-derives its generated
+    initial programs from their syntax trees, taking the first production
+    that matches."""
     ref = lambda n: {"ref": n}  # noqa: E731
     plan = {
         "version": 1, "state_types": ["Int", "Int"], "result_type": "Int", "parameter_types": ["Int"],
@@ -375,7 +376,9 @@ def grid_paths_grammar(max_nodes: int = 48, max_depth: int = 12, fuel: int = 200
                  {"id": "max", "weight": 1, "expression": {"signature": "max(Int,Int)->Int",
                                                            "args": [ref("Join"), ref("Join")]}},
                  {"id": "sub", "weight": 1, "expression": {"signature": "sub(Int,Int)->Int",
-                                                           "args": [ref("Join"), ref("Join")]}}]},
+                                                           "args": [ref("Join"), ref("Join")]}}] +
+             ([{"id": "sum", "weight": 1, "expression": {"signature": "add(Int,Int)->Int",
+                                                         "args": [ref("Join"), ref("Join")]}}] if ambiguous else [])},
             {"id": "Edge", "type": "Int", "scope": [], "alternatives": [
                 {"id": "k", "weight": 1, "expression": small(0, 1)}]},
         ],
@@ -383,7 +386,7 @@ def grid_paths_grammar(max_nodes: int = 48, max_depth: int = 12, fuel: int = 200
 
 
 def grid_paths(population: int = 1024, generations: int = 32, seed: int = 0, cases: int = 40,
-               size: int = 7) -> "TaskFiles":
+               size: int = 7, ambiguous: bool = False) -> "TaskFiles":
     """Lattice paths: C(row + column, row) for row, column in [0, size) on a
     size x size grid, searched with ``grid_paths_grammar``."""
     rng = random.Random(seed)
@@ -393,7 +396,7 @@ def grid_paths(population: int = 1024, generations: int = 32, seed: int = 0, cas
         train.append({"inputs": {"row": {"type": "int", "value": r}, "column": {"type": "int", "value": c},
                                  "rows": {"type": "int", "value": size}, "columns": {"type": "int", "value": size}},
                       "expected": {"type": "int", "value": math.comb(r + c, r)}})
-    return TaskFiles(name=f"grid-paths-s{seed}", grammar=grid_paths_grammar(), train=train,
+    return TaskFiles(name=f"grid-paths-s{seed}", grammar=grid_paths_grammar(ambiguous=ambiguous), train=train,
                      search=search_config(population, generations, seed))
 
 

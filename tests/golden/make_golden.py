@@ -97,6 +97,10 @@ LOWER_CASES = [
 REGION_CASES = [
     ("region_grid_paths_p256", dict(population=256, generations=6, seed=61, cases=30), True),
     ("region_grid_paths_p1024_g16", dict(population=1024, generations=16, seed=62, cases=49), False),
+    # an ambiguous grammar: the reference's initial rows are re-derived
+    # (first matching production) from the generated programs
+    ("region_grid_paths_ambiguous_p1024", dict(population=1024, generations=6, seed=62, cases=49, ambiguous=True),
+     False),
 ]
 
 
