@@ -771,8 +771,18 @@ int bytecode_bound(const gagp_grammar* g, int maxv) {
 // Whether a grammar's programs mostly need the exact VM: it holds
 // traversals or bound reads, or operations that can raise a runtime error
 // (modulo and division by zero, list builtins).
+// Whether every instruction a program of `g` can emit costs one unit of
+// fuel: the accumulator VM's timeout proof counts instructions.
+bool unit_fuel(const gagp_grammar* g) {
+  if (g->return_fuel != 1) return false;
+  for (int i = 0; i < g->expression_count; ++i)
+    if (g->expressions[i].fuel != 1 || g->expressions[i].merge_fuel != 1) return false;
+  return true;
+}
+
 bool exact_heavy(const gagp_grammar* g) {
   if (gb::is_statement_tag(g->slot_type)) return true;  // statement programs run on the exact VM only
+  if (!unit_fuel(g)) return true;                       // so do programs with fuel charges other than 1
   for (int i = 0; i < g->expression_count; ++i) {
     const gagp_expression& e = g->expressions[i];
     if (e.kind == gb::EK_BOUND) return true;
@@ -1330,6 +1340,7 @@ gagp_status gagp_b200_search_create(gagp_engine* e, const gagp_grammar* g, const
   d.depth_count = g->depth_count; d.logical_count = g->logical_depth_count; d.site_depth = g->site_depth;
   d.root_expression = g->root_expression; d.slot_max_depth = g->slot_max_depth; d.slot_type = g->slot_type;
   d.result_type = result_type_of(g);
+  d.unit_fuel = unit_fuel(g) ? 1 : 0;
   d.local_count = g->local_count; d.max_nodes = g->max_nodes; d.fixed_nodes = g->fixed_nodes;
   d.return_fuel = g->return_fuel;
   d.P = s->P; d.B = s->B; d.maxv = s->maxv; d.stride = p.stride;
@@ -2108,6 +2119,7 @@ gagp_status eval_rows_in(char* region, const EvalPlan& p, const gagp_grammar* g,
   d.n_ex = E;
   d.slot_type = g->slot_type;
   d.result_type = result_type_of(g);
+  d.unit_fuel = unit_fuel(g) ? 1 : 0;
   d.local_count = g->local_count;
   d.max_nodes = g->max_nodes;
   d.fixed_nodes = g->fixed_nodes;

@@ -982,7 +982,7 @@ __device__ inline int lower_accumulator_warp(const SearchDesc& s, const uint64_t
                                              int nc, uint2* code, int code_cap, int64_t* kpool, LowerScratch& m,
                                              int* temps_out) {
   const int lane = threadIdx.x & 31;
-  if (n <= 0 || n > kMaxLowerNodes) return -1;
+  if (n <= 0 || n > kMaxLowerNodes || !s.unit_fuel) return -1;
   const ExprInfo* __restrict__ info = s.info;
   bool total = true;
   int bytecode = 0, constants = 0;

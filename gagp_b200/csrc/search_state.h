@@ -191,6 +191,7 @@ struct SearchDesc {
   int32_t depth_count, logical_count, site_depth;
   int32_t root_expression, slot_max_depth, slot_type, local_count;
   int32_t result_type;                 // ValueTag a program returns (slot_type, or a statement program's return type)
+  int32_t unit_fuel;                   // every instruction costs 1 (else no program takes the accumulator VM)
   int32_t max_nodes, fixed_nodes;
   uint32_t return_fuel;
   // ---- config

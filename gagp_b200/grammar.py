@@ -452,9 +452,36 @@ class _Compiler:
         else:
             raise Declined("expression form outside the resident scalar subset")
         if "fuel_events" in value:
-            raise Declined("fuel profiles are outside the resident scalar subset")
+            self.fuel_events(e, value["fuel_events"])
         self.exprs.append(e)
         return len(self.exprs) - 1
+
+    @staticmethod
+    def fuel_events(e: "Expression", events: dict) -> None:
+        """Node-level fuel charges (fuel_charges and supports_fuel_event,
+        cpp/src/evolution/grammar/compiled.cpp:47-72, fuel_events.cpp:159-176,
+        as compile_phase_grammar places them, phase_grammar.hpp:386-395): an
+        operation's (a constant's, an input's, a bound read's) `operation`
+        charge and a value if's `branch_test` are its node's fuel, a value
+        if's `branch_merge` its merge fuel, a let's `bind` its STORE's fuel.
+        Traversal events are declined."""
+        if not isinstance(events, dict) or not events:
+            raise Declined("fuel_events must be a nonempty object")
+        for name, cost in events.items():
+            cost = int(cost)
+            if not 0 <= cost < 2 ** 31:
+                raise Declined("fuel event cost")
+            kind = e.node_kind if e.kind == EK_OPERATION else None
+            if name == "operation" and (e.kind in (EK_CONSTANT, EK_INPUT, EK_BOUND) or kind in (TK_OPERATION, TK_VAR)):
+                e.fuel = cost
+            elif name == "bind" and kind == TK_LET:
+                e.fuel = cost
+            elif name == "branch_test" and kind == TK_IF and e.type != TAG_STATEMENT:
+                e.fuel = cost
+            elif name == "branch_merge" and kind == TK_IF and e.type != TAG_STATEMENT:
+                e.merge_fuel = cost
+            else:
+                raise Declined(f"fuel event {name} outside the node-level charges")
 
     def bounded_region(self, value: dict, scope: List[Tuple[str, str]]) -> int:
         """A bounded structured expression (compiled.cpp:538-640) in the

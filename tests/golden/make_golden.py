@@ -88,6 +88,7 @@ LOWER_CASES = [
     ("lower_scalar_let", "scalar_let", dict(population=384, generations=1, seed=28, cases=32), None),
     ("lower_list_statements", "list_statements", dict(population=512, generations=1, seed=29, cases=24), None),
     ("lower_grid_paths", "grid_paths", dict(population=512, generations=1, seed=63, cases=30), None),
+    ("lower_scalar_fuel", "scalar_fuel", dict(population=384, generations=1, seed=30, cases=32), None),
 ]
 
 # Bounded regions (golden/region/): the lattice-path workload, whose
@@ -250,6 +251,21 @@ def scalar_let_grammar() -> dict:
                                                       "args": [{"ref": "Body"}, {"ref": "Body"}]}},
             {"id": "mul", "weight": 1, "expression": {"signature": "mul(Int,Int)->Int",
                                                       "args": [{"ref": "Body"}, {"ref": "Body"}]}}]})
+    return g
+
+
+def scalar_fuel_grammar() -> dict:
+    """The scalar let grammar with node-level fuel charges: input reads cost
+    2, constants 0, a let's bind 0, the body's mul 3, and the value if's test
+    2 and merge 0."""
+    g = scalar_let_grammar()
+    charges = {("Expr", "x"): {"operation": 2}, ("Expr", "c"): {"operation": 0},
+               ("Expr", "iflt"): {"branch_test": 2, "branch_merge": 0}, ("Expr", "let"): {"bind": 0},
+               ("Body", "mul"): {"operation": 3}}
+    for nt in g["nonterminals"]:
+        for alt in nt["alternatives"]:
+            if (nt["id"], alt["id"]) in charges:
+                alt["expression"]["fuel_events"] = charges[(nt["id"], alt["id"])]
     return g
 
 
@@ -613,6 +629,9 @@ def lower_fixtures() -> None:
         elif workload == "scalar_let":
             task = W.poly4(**kwargs)
             task.grammar = scalar_let_grammar()
+        elif workload == "scalar_fuel":
+            task = W.poly4(**kwargs)
+            task.grammar = scalar_fuel_grammar()
         else:
             task = W.make(workload, **kwargs)
         if variant:

@@ -34,7 +34,21 @@ TASKS = [
                                                 {"schedule": {"mode": "generational"}, "elitism": 2})),
     ("list_statements", lambda: W.list_statements(population=128, generations=4, seed=9, cases=24)),
     ("grid_paths", lambda: W.grid_paths(population=128, generations=4, seed=10, cases=30)),
+    ("poly4_fuel_charges", lambda: _with_fuel(W.poly4(population=192, generations=5, seed=11, cases=32,
+                                                      max_nodes=40))),
 ]
+
+
+def _with_fuel(files):
+    """Node-level fuel charges on the large scalar grammar: input reads cost
+    2, constants 0, mul 3, the value if's test 2 and merge 0."""
+    charges = {"x": {"operation": 2}, "c": {"operation": 0}, "mul": {"operation": 3},
+               "iflt": {"branch_test": 2, "branch_merge": 0}}
+    for nt in files.grammar["nonterminals"]:
+        for alt in nt["alternatives"]:
+            if alt["id"] in charges:
+                alt["expression"]["fuel_events"] = charges[alt["id"]]
+    return files
 
 
 def _with_search(files, extra):
