@@ -137,3 +137,29 @@ def test_list_requests_equal_alone():
     assert sorted(finished) == list(range(len(shapes)))
     for i, result in finished.items():
         assert result == alone[i], i
+
+
+def test_statement_and_region_requests_equal_alone():
+    """Statement programs and bounded regions through the server: each
+    request's tables (the bounded-region plans of the region table
+    included) are the server's copies, and the region kernel's workspace is
+    sized at admission, so a request runs the same search as alone."""
+    from gagp_b200 import build
+    from gagp_b200.engine import Engine, Server
+    build.build()
+    makers = [lambda: T.from_files(W.list_statements(population=128, generations=4, seed=31, cases=16)),
+              lambda: T.from_files(W.grid_paths(population=160, generations=5, seed=32, cases=30)),
+              lambda: T.from_files(W.grid_paths(population=96, generations=4, seed=33, cases=20, ambiguous=True))]
+    with Engine(0) as engine:
+        alone = []
+        for make in makers:
+            s = engine.admit(make())
+            s.run()
+            alone.append(s.result())
+            s.close()
+        with Server(engine, max_active=2, rounds_per_step=2) as server:
+            tickets = {i: server.submit(make()) for i, make in enumerate(makers)}
+            finished = _drain(server, tickets)
+    assert sorted(finished) == list(range(len(makers)))
+    for i, result in finished.items():
+        assert result == alone[i], i
