@@ -207,6 +207,10 @@ class GrammarBlob:
         for i, r in enumerate(t.regions):
             x = self.regions[i]
             x.traversal, x.ranged, x.fuel_profile, x.result_type = r.traversal, int(r.ranged), 0, r.result_type
+            if getattr(r, "event_cost", None):
+                x.fuel_profile = 1
+                for k, cost in enumerate(r.event_cost):
+                    x.event_cost[k] = cost
             for k in range(3):
                 x.binders[k], x.binding_types[k] = r.binders[k], r.binding_types[k]
             for k, tag in enumerate(r.operand_types[:6]):

@@ -362,7 +362,10 @@ gagp_status check_tables_and_cases(const gagp_grammar* g, const gagp_cases* c) {
     if (x.traversal != 1 && x.traversal != 2)
       return fail(GAGP_INVALID_ARGUMENT, "region table entry kind");
     if (x.ranged) return fail(GAGP_DECLINED, "ranged traversals are outside the resident subset");
-    if (x.fuel_profile) return fail(GAGP_DECLINED, "traversal fuel profiles are outside the resident subset");
+    if (x.fuel_profile)
+      for (int k = 0; k < 26; ++k)
+        if (x.event_cost[k] < 1 || x.event_cost[k] > 0x7fffffffu)
+          return fail(GAGP_DECLINED, "zero-cost traversal events are outside the resident subset");
     for (int k = 0; k < 3; ++k) {
       if (x.binders[k] < 0 || x.binders[k] >= gb::kLowerBinders) return fail(GAGP_INVALID_ARGUMENT, "traversal binder");
       if (!value_tag(x.binding_types[k])) return fail(GAGP_DECLINED, "traversal binding type");
@@ -775,6 +778,8 @@ int bytecode_bound(const gagp_grammar* g, int maxv) {
 // fuel: the accumulator VM's timeout proof counts instructions.
 bool unit_fuel(const gagp_grammar* g) {
   if (g->return_fuel != 1) return false;
+  for (int r = 0; r < g->region_count; ++r)
+    if (g->regions[r].fuel_profile) return false;
   for (int i = 0; i < g->expression_count; ++i)
     if (g->expressions[i].fuel != 1 || g->expressions[i].merge_fuel != 1) return false;
   return true;

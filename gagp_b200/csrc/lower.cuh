@@ -186,9 +186,20 @@ __host__ __device__ __noinline__ int lower_code(const LowerView& v, const uint64
     consts[nconst] = value;
     return nconst++;
   };
-  // a traversal's own instructions: unit fuel (no fuel profile)
+  // a traversal's own instructions, grouped by source fuel event: with a
+  // fuel profile the first instruction of an event carries its charge and
+  // the rest none, without one each costs 1 (phase_compile.cuh:422-432)
+  bool event_profile = false;
+  unsigned event_first = 1;
+  int event_count = 0;
+  auto event = [&](const RegionInfo& info, int which) {
+    event_profile = info.fuel_profile != 0;
+    event_first = event_profile ? info.event_cost[which] : 1u;
+    event_count = 0;
+  };
   auto put = [&](int op, int a, int b, int flags, int delta) -> bool {
-    if (!emit(op, 1u, a, b, flags)) return false;
+    const unsigned fuel = event_profile ? (event_count++ ? 0u : event_first) : 1u;
+    if (!emit(op, fuel, a, b, flags)) return false;
     if (delta > 0) grow(delta); else stack += delta;
     return true;
   };
@@ -268,31 +279,45 @@ __host__ __device__ __noinline__ int lower_code(const LowerView& v, const uint64
     const RegionInfo& info = v.regions[w.info];
     const bool reverse = info.traversal == 2;
     const int arity = info.arity;
-    if (c == 0 && !put_store(w.xs)) return false;                          // StoreSequence
+    if (c == 0) {
+      event(info, 4);                                                      // StoreSequence
+      if (!put_store(w.xs)) return false;
+    }
     if (c == 1) {
-      if (!put_store(w.start)) return false;                               // StoreStart
-      if (!put_load(w.start) || !put(OP_CHECK_INT, 0, 0, 0, 0) || !put_store(w.start)) return false;  // CheckStart
+      event(info, 5);                                                      // StoreStart
+      if (!put_store(w.start)) return false;
+      event(info, 8);                                                      // CheckStart
+      if (!put_load(w.start) || !put(OP_CHECK_INT, 0, 0, 0, 0) || !put_store(w.start)) return false;
+      event(info, 11);                                                     // ObserveSequence
       if (!put_load(w.xs) || !put(OP_CALL_BUILTIN, B_LEN, 1, kHasA | kHasB, 0) || !put_store(w.length))
-        return false;                                                      // ObserveSequence
-      if (!put_int(0) || !put_store(w.begin)) return false;                // SetBegin
-      if (!put_load(w.length) || !put_store(w.limit)) return false;        // SetEnd
+        return false;
+      event(info, 14);                                                     // SetBegin
+      if (!put_int(0) || !put_store(w.begin)) return false;
+      event(info, 15);                                                     // SetEnd
+      if (!put_load(w.length) || !put_store(w.limit)) return false;
     }
     if (c == arity - 2) {
-      if (!put_store(w.state)) return false;                               // InitializeState
-      if (!(reverse ? put_load(w.limit) : put_load(w.begin))) return false; // InitializeCursor
+      event(info, 16);                                                     // InitializeState
+      if (!put_store(w.state)) return false;
+      event(info, 17);                                                     // InitializeCursor
+      if (!(reverse ? put_load(w.limit) : put_load(w.begin))) return false;
       if (reverse && (!put_int(1) || !put(OP_SUB, 0, 0, 0, -1))) return false;
       if (!put_store(w.counter)) return false;
-      w.loop_head = count;                                                 // TestCursor
+      w.loop_head = count;
+      event(info, 18);                                                     // TestCursor
       if (!put_load(w.counter) || !(reverse ? put_load(w.begin) : put_load(w.limit)) ||
           !put(reverse ? OP_GE : OP_LT, 0, 0, 0, -1))
         return false;
       w.done_jump = count;
       if (!put(OP_JMP_IF_FALSE, 0, 0, kHasA, -1)) return false;
+      event(info, 19);                                                     // ReadElement
       if (!put_load(w.xs) || !put_load(w.counter) || !put(OP_CALL_BUILTIN, B_INDEX, 2, kHasA | kHasB, -1))
-        return false;                                                      // ReadElement
-      if (!put_store(w.element)) return false;                             // BindElement
+        return false;
+      event(info, 20);                                                     // BindElement
+      if (!put_store(w.element)) return false;
+      event(info, 21);                                                     // ComputeIndex
       if (!put_load(w.start) || !put_load(w.counter) || !put(OP_ADD, 0, 0, 0, -1) || !put_store(w.index))
-        return false;                                                      // ComputeIndex
+        return false;
       const int slots[3] = {w.element, w.index, w.state};
       for (int k = 0; k < 3; ++k) {
         const int b = info.binders[k];
@@ -308,14 +333,19 @@ __host__ __device__ __noinline__ int lower_code(const LowerView& v, const uint64
         env_slot[b] = w.saved_slot[k];
         env_type[b] = w.saved_type[k];
       }
-      if (!put_store(w.state)) return false;                               // UpdateState
+      event(info, 22);                                                     // UpdateState
+      if (!put_store(w.state)) return false;
+      event(info, 23);                                                     // AdvanceCursor
       if (!put_load(w.counter) || !put_int(1) || !put(reverse ? OP_SUB : OP_ADD, 0, 0, 0, -1) ||
           !put_store(w.counter))
-        return false;                                                      // AdvanceCursor
-      if (!put(OP_JMP, w.loop_head, 0, kHasA, 0)) return false;            // Repeat
+        return false;
+      event(info, 24);                                                     // Repeat
+      if (!put(OP_JMP, w.loop_head, 0, kHasA, 0)) return false;
       code[5 * w.done_jump + 2] = count;
-      if (!put_load(w.state)) return false;                                // Result
+      event(info, 25);                                                     // Result
+      if (!put_load(w.state)) return false;
     }
+    event_profile = false;
     return true;
   };
   for (;;) {

@@ -111,6 +111,10 @@ struct RegionInfo {
   int8_t transition_kind[8][4], transition_source[8][4];
   int8_t axis_slot[4], lower_kind[4], upper_kind[4];
   uint32_t frames, cells, entry_fuel;
+  // a traversal's fuel profile: each event's first instruction carries its
+  // charge, the rest none (PhaseFuelEvent numbering); off: every instruction costs 1
+  int32_t fuel_profile;
+  uint32_t event_cost[26];
   int64_t transition_offset[8][4];
   int64_t lower[4], upper[4];
 };
@@ -118,6 +122,8 @@ struct RegionInfo {
 // bounded region (a bounded one checked by the engine's admission).
 inline RegionInfo region_info_of(const gagp_region& x) {
   RegionInfo y{};
+  y.fuel_profile = x.fuel_profile ? 1 : 0;
+  for (int k = 0; k < 26; ++k) y.event_cost[k] = x.event_cost[k];
   y.traversal = int8_t(x.traversal);
   y.ranged = int8_t(x.ranged);
   y.arity = int8_t(x.ranged ? 6 : 4);

@@ -155,6 +155,7 @@ class Expression:
     category: str = "Expression"  # syntax category: Expression, or Program/Block/Statement
     label: str = ""               # the local or input an assign, a for_range or a local read names
     plan: Optional["BoundedPlan"] = None  # a bounded region's plan (front end only)
+    event_cost: Optional[List[int]] = None  # a traversal's fuel profile (26 PhaseFuelEvent charges)
 
 
 @dataclass
@@ -215,6 +216,8 @@ class Region:
     ranged: bool = False
     # a bounded region (traversal 0): its plan and phases (BoundedPlan)
     plan: Optional["BoundedPlan"] = None
+    # a traversal's fuel profile: 26 PhaseFuelEvent charges (None: every instruction costs 1)
+    event_cost: Optional[List[int]] = None
 
 
 # region slot banks (RegionSlotBank, cpp/include/gagp/core/region_plan.hpp:96)
@@ -456,6 +459,12 @@ class _Compiler:
         self.exprs.append(e)
         return len(self.exprs) - 1
 
+    # traversal fuel events by PhaseFuelEvent number (device/phase_compile.cuh:36-40)
+    TRAVERSAL_EVENTS = {"store_sequence": 4, "store_start": 5, "check_start": 8, "observe_sequence": 11,
+                        "set_begin": 14, "set_end": 15, "initialize_state": 16, "initialize_cursor": 17,
+                        "test_cursor": 18, "read_element": 19, "bind_element": 20, "compute_index": 21,
+                        "update_state": 22, "advance_cursor": 23, "repeat": 24, "result": 25}
+
     @staticmethod
     def fuel_events(e: "Expression", events: dict) -> None:
         """Node-level fuel charges (fuel_charges and supports_fuel_event,
@@ -467,6 +476,19 @@ class _Compiler:
         Traversal events are declined."""
         if not isinstance(events, dict) or not events:
             raise Declined("fuel_events must be a nonempty object")
+        if e.kind == EK_OPERATION and e.node_kind == TK_TRAVERSE:
+            # a traversal's profile: each event's first instruction carries
+            # its charge (unlisted events cost 1, phase_grammar.hpp:272-274);
+            # a zero charge lets the reference alias or skip instructions,
+            # which is not restated here
+            e.event_cost = [1] * 26
+            for name, cost in events.items():
+                if name not in _Compiler.TRAVERSAL_EVENTS:
+                    raise Declined(f"fuel event {name} outside a traversal's events")
+                if not 1 <= int(cost) < 2 ** 31:
+                    raise Declined("zero-cost traversal events are outside the resident subset")
+                e.event_cost[_Compiler.TRAVERSAL_EVENTS[name]] = int(cost)
+            return
         for name, cost in events.items():
             cost = int(cost)
             if not 0 <= cost < 2 ** 31:
@@ -773,7 +795,8 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
             x.operand = len(regions)
             regions.append(Region(traversal=e.operand, binders=[binder, binder + 1, binder + 2],
                                   operand_types=[c.exprs[k].type for k in e.children[:e.arity]],
-                                  binding_types=list(e.binding_types), result_type=e.type))
+                                  binding_types=list(e.binding_types), result_type=e.type,
+                                  event_cost=list(e.event_cost) if e.event_cost else None))
         if len(env) > 15:
             raise Declined("lexical environment capacity")
         if e.kind == EK_CONSTANT and e.target not in seen_dom:

@@ -89,6 +89,7 @@ LOWER_CASES = [
     ("lower_list_statements", "list_statements", dict(population=512, generations=1, seed=29, cases=24), None),
     ("lower_grid_paths", "grid_paths", dict(population=512, generations=1, seed=63, cases=30), None),
     ("lower_scalar_fuel", "scalar_fuel", dict(population=384, generations=1, seed=30, cases=32), None),
+    ("lower_list_fuel", "list", dict(population=256, generations=1, seed=31, cases=24), "fuel"),
 ]
 
 # Bounded regions (golden/region/): the lattice-path workload, whose
@@ -269,6 +270,17 @@ def scalar_fuel_grammar() -> dict:
     return g
 
 
+def list_fuel_grammar() -> dict:
+    """The list grammar whose traversal carries a fuel profile (every event
+    charged at least 1)."""
+    g = W.list_threshold_grammar()
+    top = next(r for r in g["nonterminals"] if r["id"] == "Top")
+    top["alternatives"][0]["expression"]["fuel_events"] = {
+        "store_sequence": 4, "test_cursor": 3, "read_element": 2, "compute_index": 2, "update_state": 2,
+        "repeat": 1, "result": 2}
+    return g
+
+
 def variant_grammar(variant):
     if variant == "let":
         return let_grammar()
@@ -280,6 +292,8 @@ def variant_grammar(variant):
         return deep_traversal_grammar()
     if variant == "statements":
         return W.list_statements_grammar()
+    if variant == "fuel":
+        return list_fuel_grammar()
     return None
 
 

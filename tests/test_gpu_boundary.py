@@ -36,7 +36,18 @@ TASKS = [
     ("grid_paths", lambda: W.grid_paths(population=128, generations=4, seed=10, cases=30)),
     ("poly4_fuel_charges", lambda: _with_fuel(W.poly4(population=192, generations=5, seed=11, cases=32,
                                                       max_nodes=40))),
+    ("list_traversal_fuel", lambda: _with_traversal_fuel(W.list_threshold(population=128, generations=4, seed=12,
+                                                                          cases=24))),
 ]
+
+
+def _with_traversal_fuel(files):
+    """A fuel profile on the list grammar's traversal (every event charged
+    at least 1)."""
+    top = next(r for r in files.grammar["nonterminals"] if r["id"] == "Top")
+    top["alternatives"][0]["expression"]["fuel_events"] = {"store_sequence": 2, "test_cursor": 3, "read_element": 2,
+                                                           "advance_cursor": 2, "result": 4}
+    return files
 
 
 def _with_fuel(files):
