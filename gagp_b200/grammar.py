@@ -15,7 +15,9 @@ subset of the grammar language, three reference steps:
 * the site-depth cost table (``phase_grammar.hpp:496-530``) and the static
   weight normalisation (``phase_grammar.hpp:48-67``).
 
-A construct outside the subset raises :class:`Declined`, which is the
+Beyond scalar expressions it admits lists, lets, traversals, statement
+programs, bounded regions and fuel charges (``allow_lists``).  A construct
+outside the subset raises :class:`Declined`, which is the
 reference's resident-admission decline (``std::invalid_argument`` at
 admission, ``cpp/src/evolution/evolve.cpp:45-49``).
 """
@@ -35,7 +37,7 @@ TAG_INT, TAG_FLOAT, TAG_BOOL, TAG_INTLIST, TAG_INVALID = 0, 1, 2, 5, 9
 # device/phase_compile.cuh:23)
 TAG_STATEMENT = 0xF0
 TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL}
-# with the list subset (tables only: the engine declines these grammars)
+# with the list subset
 LIST_TYPE_TAGS = {"Int": TAG_INT, "Bool": TAG_BOOL, "IntList": TAG_INTLIST}
 
 # PhaseExpressionKind (device/phase_generate.cuh:25)
@@ -674,11 +676,13 @@ def compile_tables(doc: dict, input_names: Optional[List[str]] = None, site_dept
                    allow_lists: bool = False) -> PhaseTables:
     """Admit ``doc`` and build the resident tables (one whole-program slot).
 
-    ``allow_lists`` builds the tables of the list subset too (IntList inputs,
-    len, forward traversals with their element/index/state binders, scoped
-    nonterminals and bound names), as compile_phase_grammar does
-    (``phase_grammar.hpp:94-300``); the engine still declines these grammars
-    at admission, so only the table builder's tests use it."""
+    ``allow_lists`` admits the engine's whole subset beyond scalar
+    expressions, as compile_phase_grammar builds it
+    (``phase_grammar.hpp:94-400``): IntList inputs, len and index, forward
+    and reverse traversals with their element/index/state binders, lets,
+    scoped nonterminals and bound names, statement programs with grammar
+    locals, bounded regions and fuel charges.  Task loading
+    (``task.assemble``) always passes it."""
     c = _Compiler(doc, allow_lists)
     c.compile()
     entry = doc["entry"]
