@@ -407,8 +407,8 @@ def _log_uniform_population(rng: random.Random, lo: int, hi: int) -> int:
 
 def mix_files(entry: dict) -> TaskFiles:
     """The task files of a mix entry: built with the mix for the scalar
-    entries, on demand for the list entries (their cases are the costly part
-    and this engine declines them at admission)."""
+    entries, on demand for the list entries (their cases, lists of up to 50
+    elements, are the costly part to build)."""
     if entry["files"] is None:
         entry["files"] = make(entry["workload"], **entry["args"])
     return entry["files"]

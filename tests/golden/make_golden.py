@@ -46,9 +46,9 @@ CASES = [
 ]
 
 
-# List programs (traversals over an IntList): the engine declines them, so
-# these fixtures pin the table builder's list subset and hold the reference's
-# runs for the list path.  They live in golden/list/.
+# List programs (traversals over an IntList, lets, statement programs):
+# the reference's tables, initial rows, one make_batch and whole runs of the
+# list path.  They live in golden/list/.
 LIST_CASES = [
     ("list_threshold_sum", dict(population=64, generations=3, seed=11, cases=12, target="threshold_sum"), None),
     ("list_threshold_count", dict(population=64, generations=3, seed=12, cases=12, target="threshold_count"), None),

@@ -24,8 +24,8 @@ def fixture(name: str) -> dict:
         return json.load(f)
 
 
-# list-program fixtures (golden/list/): the reference's tables and runs of
-# tasks this engine declines, which pin the table builder's list subset
+# list-program fixtures (golden/list/): the reference's tables, rows and runs
+# of list tasks (traversals, lets, statement programs)
 LIST_HERE = os.path.join(HERE, "list")
 
 
